@@ -1,0 +1,154 @@
+"""ctypes binding of ``libffx_core.so`` (declared in ``include/ffx.h``).
+
+The library is loaded from ``fluxfx_b200/_lib`` (built in place by
+``python -m fluxfx_b200.build``). There is no fallback: if the library is
+missing, every solver constructor raises ``NativeUnavailable``.
+"""
+import ctypes as C
+import os
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / '_lib' / 'libffx_core.so'
+
+FFX_OK, FFX_ERR_INVALID, FFX_ERR_LAUNCH, FFX_ERR_NOT_CONVERGED, FFX_ERR_TIMEOUT, FFX_ERR_CUDA = range(6)
+FFX_F32, FFX_BF16 = 0, 1
+STATUS_NAMES = {0: 'OK', 1: 'INVALID', 2: 'LAUNCH', 3: 'NOT_CONVERGED', 4: 'TIMEOUT', 5: 'CUDA'}
+
+vp = C.c_void_p
+i32 = C.c_int32
+f32 = C.c_float
+i64 = C.c_int64
+f3 = f32 * 3
+n3 = i32 * 3
+
+
+class NativeUnavailable(RuntimeError):
+    """libffx_core.so could not be loaded (not built, or no CUDA driver)."""
+
+
+class FfxError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class FfxGrid(C.Structure):
+    _fields_ = [('nx', i32), ('ny', i32), ('nz', i32), ('ex', f32), ('ey', f32), ('ez', f32),
+                ('ix', f32), ('iy', f32), ('iz', f32)]
+
+
+class FfxSolids(C.Structure):
+    _fields_ = [('solid', vp), ('halo', vp)]
+
+
+class FfxSources(C.Structure):
+    _fields_ = [('count', i32), ('single_solid_profile', i32), ('single_center', f3), ('single_start', f3),
+                ('single_radius', f32), ('single_jet', f3), ('single_coupling', f32), ('table', f32 * 128)]
+
+
+class FfxDeviceInfo(C.Structure):
+    _fields_ = [('device', i32), ('sm_count', i32), ('cc_major', i32), ('cc_minor', i32),
+                ('total_bytes', i64), ('name', C.c_char * 128)]
+
+
+class FfxScalarChannel(C.Structure):
+    _fields_ = [('field', vp), ('predictor', vp), ('reverse', vp), ('out', vp), ('rate', f32), ('decay', f32),
+                ('target', f32), ('channel', i32), ('table_target', i32)]
+
+
+class FfxGraphLevel(C.Structure):
+    _fields_ = [('nx', i32), ('ny', i32), ('nz', i32), ('edges', vp), ('solid', vp), ('w', f3)]
+
+
+P = C.POINTER
+_PROTOTYPES = {
+    'ffx_abi_version': (C.c_int, []),
+    'ffx_last_error': (C.c_char_p, []),
+    'ffx_device_info': (C.c_int, [C.c_int, P(FfxDeviceInfo)]),
+    'ffx_probe_3d': (C.c_int, [vp, vp]),
+    'ffx_seed_scalar': (C.c_int, [P(FfxGrid), C.c_int, f3, f32, f32, vp, vp]),
+    'ffx_seed_faces': (C.c_int, [P(FfxGrid), C.c_int, f3, f32, vp, vp, vp, vp]),
+    'ffx_raster_colliders': (C.c_int, [P(FfxGrid), C.c_double * 3, C.c_int, vp, vp, vp]),
+    'ffx_dilate_mask': (C.c_int, [P(FfxGrid), vp, vp, vp]),
+    'ffx_solid_clear': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp]),
+    'ffx_face_predictor': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
+    'ffx_advect_velocity': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, f32, C.c_int, f32,
+                                      P(FfxSources), vp, vp, f32, f32, C.c_int, vp, vp, vp, vp]),
+    'ffx_mac_advect_velocity': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
+    'ffx_buoyancy': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, f32, f32, vp, vp]),
+    'ffx_scalar_transport': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int, P(vp), P(vp), vp]),
+    'ffx_advect_scalars': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int, P(FfxSources),
+                                     C.c_int, P(FfxScalarChannel), vp, vp]),
+    'ffx_advect_open': (C.c_int, [P(FfxGrid), C.c_int, vp, f32, f3, f32, f3, f32, f32, f32, vp, vp]),
+    'ffx_mac_advect_density': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f3, f32, f32, f32, vp, vp]),
+    'ffx_walls': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp]),
+    'ffx_divergence': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp]),
+    'ffx_walls_divergence': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]),
+    'ffx_gradient': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, f32, vp, vp, vp, vp, vp, vp]),
+    'ffx_jacobi': (C.c_int, [n3, f3, vp, vp, vp, f32, f32, vp, vp]),
+    'ffx_scale': (C.c_int, [i64, vp, f32, vp, vp]),
+    'ffx_mg_residual': (C.c_int, [n3, f3, vp, vp, f32, vp, vp]),
+    'ffx_mg_restrict': (C.c_int, [n3, vp, vp, vp]),
+    'ffx_mg_residual_restrict': (C.c_int, [n3, f3, vp, vp, f32, vp, vp]),
+    'ffx_mg_prolong': (C.c_int, [n3, vp, vp, vp, vp]),
+    'ffx_direct_solve': (C.c_int, [i32, vp, vp, f32, vp, vp]),
+    'ffx_mg_residual_max': (C.c_int, [n3, f3, vp, vp, f32, vp, vp]),
+    'ffx_graph_smooth': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp]),
+    'ffx_graph_residual': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
+    'ffx_graph_residual_restrict': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
+    'ffx_graph_prolong': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
+    'ffx_graph_prolong_smooth': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, f32, vp, vp]),
+    'ffx_graph_residual_max': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
+    'ffx_graph_coarsen': (C.c_int, [P(FfxGraphLevel), vp, vp, vp]),
+    'ffx_graph_level0_edges': (C.c_int, [P(FfxGraphLevel), vp, vp]),
+    'ffx_max_abs': (C.c_int, [i64, C.c_int, vp, vp, vp]),
+    'ffx_divergence_stats_workspace': (C.c_size_t, [i64]),
+    'ffx_divergence_stats': (C.c_int, [i64, vp, vp, vp, vp, C.c_size_t, vp]),
+}
+
+_LIB = None
+
+
+def exported_symbols():
+    return tuple(_PROTOTYPES)
+
+
+def load(path=None):
+    """Load the library once and attach argument/return types."""
+    global _LIB
+    if _LIB is not None and path is None:
+        return _LIB
+    target = Path(path) if path else Path(os.environ.get('FFX_CORE_LIB', LIB_PATH))
+    if not target.exists():
+        raise NativeUnavailable(f"{target} is missing; build it with `python -m fluxfx_b200.build`")
+    try:
+        lib = C.CDLL(str(target))
+    except OSError as exc:
+        raise NativeUnavailable(f"cannot load {target}: {exc}") from exc
+    for name, (res, args) in _PROTOTYPES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    if lib.ffx_abi_version() != 1:
+        raise NativeUnavailable("libffx_core ABI version mismatch")
+    if path is None:
+        _LIB = lib
+    return lib
+
+
+def check(status):
+    if status != FFX_OK:
+        msg = load().ffx_last_error()
+        raise FfxError(status, msg.decode() if msg else '')
+
+
+def call(name, *args):
+    """Invoke an entry point and raise FfxError on a non-OK status."""
+    check(getattr(load(), name)(*args))
+
+
+def grid_struct(shape, extent):
+    """FfxGrid for a cell shape (nx, ny, nz) and an FP64 extent."""
+    nx, ny, nz = shape
+    inv = [1.0 / (e / n) for e, n in zip(extent, shape)]
+    return FfxGrid(nx, ny, nz, *[float(e) for e in extent], *inv)

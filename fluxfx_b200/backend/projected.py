@@ -1,0 +1,226 @@
+"""The dense smoke step: transport, buoyancy, projection, scalar transport.
+
+Drop-in for FluxFX ``fluxfx/backend/projected.py:13-229``
+(``DenseProjectedSmoke``): same constructor, step order and state machine
+(``faulted`` after a failed step until ``reset``). One step enqueues:
+
+1. ``ffx_face_predictor`` (MacCormack velocity only);
+2. ``ffx_advect_velocity`` -- transport of U, V, W, emitter coupling, buoyancy
+   on W from the previous density/temperature and the wall condition, written
+   straight into the projector's bounded faces;
+3. the projection (divergence, pressure solve, gradient + divergence after);
+4. ``ffx_scalar_transport`` x2 (MacCormack predictor and reverse of density and
+   temperature together) and ``ffx_advect_scalars`` (both channels, decay and
+   emission) -- one launch per pass for both scalars.
+
+Extensions: ``settings.storage == 'BF16'`` stores velocity and scalars in
+bfloat16 (FP32 arithmetic); ``heat_mode == 'TARGET'`` raises temperature to the
+emitter value instead of adding a rate.
+"""
+import ctypes as C
+
+import torch
+
+from .. import _native as N
+from ..physics.config import GridSpec, validate_dt
+from ..physics.emission import Emission, pack_sources, SOURCE_TABLE_SHAPE
+from ..physics.interaction import validate_live_update
+from ..physics.pressure import PressureSettings
+from .dense import SEED_CONSTANTS
+from .detail import DetailPasses
+from .device import ptr
+from .mac import FACE_CONSTANTS, VELOCITY_NAMES
+from .pressure import PressureProjector
+from .thermal import DenseThermalAdvection
+
+
+class DenseProjectedSmoke(DenseThermalAdvection):
+    def __init__(self, grid=None, settings=None, device=None, projector_class=None, *, colliders=()):
+        settings = settings or PressureSettings()
+        self._field_dtype = torch.bfloat16 if settings.storage == 'BF16' else torch.float32
+        self.combustion = None
+        self.solids = None
+        if colliders:
+            from .collision import SolidDevice, SolidPressureProjector
+            from .multigrid import use_multigrid
+            from .solid_multigrid import SolidMultigridProjector
+            grid = grid or GridSpec()
+            if settings.moving_colliders:
+                raise ValueError('Moving colliders are not part of this build; use static colliders')
+            device = self.solids = SolidDevice(grid, colliders, device)
+            projector_class = SolidMultigridProjector if use_multigrid(grid, settings) else SolidPressureProjector
+        if settings.combustion_enabled:
+            raise ValueError('Combustion is not part of this build')
+        if settings.turbulence_strength > 0 or settings.vorticity_strength > 0:
+            raise ValueError('Turbulence and vorticity confinement are not part of this build')
+        self.projector = None
+        self.detail = None
+        self.turbulence = None
+        self.faulted = False
+        self._source_data = None
+        self._sources = N.FfxSources()
+        self._sources.count = -1
+        super().__init__(grid, settings, device)
+        if projector_class is None:
+            from .multigrid import MultigridPressureProjector, use_multigrid
+            projector_class = MultigridPressureProjector if use_multigrid(self.grid, self.settings) else PressureProjector
+        self.projector = projector_class(self.grid, self.settings, self.device)
+        self.detail = DetailPasses(self.grid, self.device, self._field_dtype)
+        self._solids = N.FfxSolids(*(ptr(t) if t is not None else None
+                                     for t in ((self.solids.mask, self.solids.halo) if self.solids else (None, None))))
+        self._maxima = torch.zeros(3, dtype=torch.float32, device=self.device.device)
+        self.reset()
+
+    @property
+    def allocated_bytes(self):
+        extra = self.solids.allocated_bytes if self.solids else 0
+        return super().allocated_bytes + extra + self.projector.allocated_bytes + self.detail.allocated_bytes
+
+    def reset(self, seed=True):
+        super().reset(seed)
+        self.faulted = False
+        if self.solids is not None:
+            self.solids.clear_solid(self._front, self._back)
+            self._front, self._back = self._back, self._front
+            if self._temperature is not None:
+                self.solids.clear_solid(self._temperature, self._temperature_back)
+                self._temperature, self._temperature_back = self._temperature_back, self._temperature
+        if self.projector is not None:
+            self.projector.reset()
+            self.projector.enforce_walls(self._velocity, self._velocity_back)
+            self._velocity, self._velocity_back = self._velocity_back, self._velocity
+
+    def upload_velocity(self, components):
+        super().upload_velocity(components)
+        if self.solids is not None:
+            self.projector.enforce_walls(self._velocity, self._velocity_back)
+            self._velocity, self._velocity_back = self._velocity_back, self._velocity
+        self.projector.reset()
+
+    def upload(self, values):
+        super().upload(values)
+        if self.solids is not None:
+            self.solids.clear_solid(self._front, self._back)
+            self._front, self._back = self._back, self._front
+        self.projector.reset()
+
+    def upload_temperature(self, values):
+        super().upload_temperature(values)
+        if self.solids is not None:
+            self.solids.clear_solid(self._temperature, self._temperature_back)
+            self._temperature, self._temperature_back = self._temperature_back, self._temperature
+        self.projector.reset()
+
+    def update_settings(self, settings):
+        """Apply live parameters between steps, preserving all fields and pressure."""
+        validate_live_update(self.settings, settings)
+        self.settings = settings
+        self.projector.settings = settings
+
+    def move_colliders(self, colliders, dt):
+        raise ValueError('Enable Moving colliders and Reset first')
+
+    def measure_projection(self):
+        return self.projector.metrics() | {"step": self.steps, "simulation_time": self.time}
+
+    def step(self, dt=1.0 / 30.0, emission=None, sources=None):
+        validate_dt(dt)
+        if sources is not None:
+            self._prepare_sources(sources)
+        if self.faulted:
+            raise RuntimeError("Reset required after a failed GPU step")
+        try:
+            self._step(dt, emission or Emission(self.settings.source_center), sources)
+        except Exception:
+            self.faulted = True
+            self.projector.ready = False
+            raise
+
+    def _prepare_sources(self, sources):
+        data = pack_sources(sources)
+        if data != self._source_data:
+            self._source_data = data
+        self._source_count = len(sources)
+
+    def _fill_sources(self, emission, emitters):
+        src = self._sources
+        s = self.settings
+        if emitters is not None:
+            src.count = len(emitters)
+            for i, v in enumerate(self._source_data):
+                src.table[i] = v
+        else:
+            src.count = -1
+            src.single_solid_profile = int(s.source_profile == "SOLID")
+            src.single_center = N.f3(*s.source_center)
+            src.single_start = N.f3(*emission.start)
+            src.single_radius = s.source_radius
+            src.single_jet = N.f3(*emission.velocity)
+            src.single_coupling = emission.coupling
+        return src
+
+    def _step(self, dt, emission, emitters=None):
+        s = self.settings
+        dev = self.device
+        gp = C.byref(self._g)
+        sp = C.byref(self._solids)
+        st = dev.s
+        src = self._fill_sources(emission, emitters)
+        corrected_v = s.velocity_advection == "MACCORMACK"
+        vel = [ptr(f) for f in self._velocity]
+        if corrected_v:
+            self.detail.transport_velocity(self._velocity, dt)
+            pred = [ptr(f) for f in self.detail.face_predictor]
+        else:
+            pred = [None, None, None]
+        proj = self.projector
+        dev.call('ffx_advect_velocity', gp, sp, self._storage, *vel, *pred, dt, int(corrected_v), s.velocity_blend,
+                 C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift, s.density_weight, 1,
+                 *[ptr(b) for b in proj.bounded], st)
+        # The old velocity is consumed: the corrected field is written over it.
+        proj.project_bounded(self._velocity, dt)
+        corrected_s = s.scalar_advection == "MACCORMACK"
+        fields = [self._front, self._temperature]
+        if corrected_s:
+            preds, revs = self.detail.transport_many(fields, self._velocity, dt)
+        else:
+            preds = revs = fields
+        outs = [self._back, self._temperature_back]
+        density_target = s.source_rate if s.density_mode == "TARGET" else -1.0
+        heat_target = s.heat_source_rate if s.heat_mode == "TARGET" else -1.0
+        chans = (N.FfxScalarChannel * 2)(
+            N.FfxScalarChannel(ptr(fields[0]), ptr(preds[0]), ptr(revs[0]), ptr(outs[0]), s.source_rate,
+                               s.dissipation, density_target, 0, 0),
+            N.FfxScalarChannel(ptr(fields[1]), ptr(preds[1]), ptr(revs[1]), ptr(outs[1]), s.heat_source_rate,
+                               s.cooling, heat_target, 1, int(s.heat_mode == "TARGET")))
+        dev.call('ffx_advect_scalars', gp, sp, self._storage, *[ptr(f) for f in self._velocity], dt,
+                 int(corrected_s), C.byref(src), 2, chans, ptr(self._maxima), st)
+        self._front, self._back = self._back, self._front
+        self._temperature, self._temperature_back = self._temperature_back, self._temperature
+        self.time += dt
+        self.steps += 1
+
+    def scalar_maxima(self):
+        """max |density|, |temperature| of the last step (one readback)."""
+        return [float(v) for v in self._maxima[0:2].cpu()]
+
+    def preview_field(self, channel):
+        if channel == 'COLLISION':
+            if self.solids is None:
+                raise ValueError('Add a collider and Reset for collision display')
+            return self.solids.mask
+        if channel in {'FUEL', 'FLAME'}:
+            raise ValueError('Enable combustion and Reset for fuel/flame display')
+        return self.temperature if channel == 'TEMPERATURE' else self.density
+
+    def close(self):
+        if self.projector is not None:
+            self.projector.close()
+        self.projector = None
+        if self.detail is not None:
+            self.detail.close()
+        self.detail = None
+        super().close()
+        if self.solids is not None:
+            self.solids.close()
+        self.solids = None

@@ -1,0 +1,223 @@
+"""Topology-preserving aggregation V-cycles for static voxel colliders.
+
+Drop-in for FluxFX ``fluxfx/backend/solid_multigrid.py:7-93``. The Galerkin
+hierarchy of ``fluxfx/physics/solid_hierarchy.py:11-54`` is built on the device
+(``ffx_graph_coarsen`` per level, one flag readback per level at construction);
+level 0 reads the uint8 mask instead of storing conductances. The coarsest
+level (<= 256 cells) is solved with an FP64 graph pseudoinverse. Residual +
+restriction and prolongation + first post-smoothing sweep are fused passes
+with results identical to the separate passes.
+"""
+import ctypes as C
+from math import prod
+
+import numpy as np
+import torch
+
+from .. import _native as N
+from .collision import SolidPressureProjector
+from .device import KernelHandle, ptr
+
+DIRECT_LIMIT = 256
+
+
+class KernelTimer:
+    """CUDA events around every level-0 smoothing launch, on the solver's stream.
+
+    Set ``projector.timer = KernelTimer(stream)`` to time the dominant kernel of
+    the solve while the step runs; ``average_ms()`` synchronises and returns the
+    mean launch duration."""
+
+    def __init__(self, stream):
+        self.stream = stream
+        self.pairs = []
+
+    def begin(self):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        return e
+
+    def end(self, start):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        self.pairs.append((start, e))
+
+    @property
+    def count(self):
+        return len(self.pairs)
+
+    def average_ms(self):
+        if not self.pairs:
+            return None
+        self.pairs[-1][1].synchronize()
+        return sum(a.elapsed_time(b) for a, b in self.pairs) / len(self.pairs)
+
+
+def graph_pseudoinverse(shape, edges):
+    """FP64 pseudoinverse of the graph Laplacian with conductances ``edges``
+    ((nz, ny, nx, 4) host array), as ``solid_hierarchy.graph_inverse`` forms it."""
+    n = prod(shape)
+    if n > DIRECT_LIMIT:
+        raise ValueError('Direct coarse solve is limited to 256 cells')
+    e = np.asarray(edges, dtype=np.float64).reshape(n, 4)
+    m = np.zeros((n, n))
+    strides = (1, shape[0], shape[0] * shape[1])
+    for i in range(n):
+        for a, st in enumerate(strides):
+            w = e[i, a]
+            if w:
+                j = i + st
+                m[i, i] -= w
+                m[j, j] -= w
+                m[i, j] += w
+                m[j, i] += w
+    return np.linalg.pinv(m, rcond=1e-12, hermitian=True)
+
+
+class SolidMultigridProjector(SolidPressureProjector):
+    def __init__(self, grid, settings=None, device=None):
+        super().__init__(grid, settings, device)
+        s = self.settings
+        dev = self.device
+        self.levels = []
+        self.smooth_kernel = KernelHandle('solid_mg_smooth.glsl')
+        self.residual_kernel = KernelHandle('solid_mg_residual.glsl')
+        self.restrict_kernel = KernelHandle('mg_restrict.glsl')
+        self.prolong_kernel = KernelHandle('solid_mg_prolong.glsl')
+        shape = tuple(grid.shape)
+        weights = [float(np.float32((n / e) ** 2)) for n, e in zip(shape, grid.extent)]
+        level0 = N.FfxGraphLevel(*shape, None, ptr(self._mask), N.f3(*weights))
+        self.levels.append(dict(shape=shape, edges=None, graph=level0, p=self.pressure, q=self.spare,
+                                rhs=self.before))
+        flag = torch.zeros(1, dtype=torch.int32, device=dev.device)
+        while min(shape) >= 8 and all(n % 2 == 0 for n in shape):
+            if s.mg_max_levels and len(self.levels) >= s.mg_max_levels:
+                break
+            coarse_shape = tuple(n // 2 for n in shape)
+            cx, cy, cz = coarse_shape
+            edges = torch.empty((cz, cy, cx, 4), dtype=torch.float32, device=dev.device)
+            dev.call('ffx_graph_coarsen', C.byref(self.levels[-1]['graph']), ptr(edges), ptr(flag), dev.s)
+            if int(flag.item()):
+                break   # an aggregate would join disconnected children: stop here
+            graph = N.FfxGraphLevel(*coarse_shape, ptr(edges), None, N.f3(0.0, 0.0, 0.0))
+            self.levels.append(dict(shape=coarse_shape, edges=edges, graph=graph, p=dev.texture(coarse_shape),
+                                    q=dev.texture(coarse_shape), rhs=dev.texture(coarse_shape)))
+            shape = coarse_shape
+        self.coarse_matrix = self.coarse_kernel = None
+        last = self.levels[-1]
+        n = prod(last['shape'])
+        if n <= DIRECT_LIMIT and s.coarse_solver == 'DIRECT' and len(self.levels) > 1:
+            inv = graph_pseudoinverse(last['shape'], last['edges'].cpu().numpy())
+            self.coarse_matrix = torch.as_tensor(inv, dtype=torch.float64).to(dev.device)
+            self.coarse_kernel = KernelHandle('solid_mg_direct.glsl')
+        self.pre_sweeps = s.mg_pre_sweeps or 4
+        self.post_sweeps = s.mg_post_sweeps or 4
+        self.last_cycles = 0
+        self.timer = None
+        self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
+
+    @property
+    def allocated_bytes(self):
+        coarse = sum(4 * 7 * prod(v['shape']) for v in self.levels[1:])
+        direct = 8 * self.coarse_matrix.numel() if self.coarse_matrix is not None else 0
+        return super().allocated_bytes + coarse + direct
+
+    def smooth(self, level, count):
+        timer = self.timer if level is self.levels[0] else None
+        for _ in range(count):
+            started = timer.begin() if timer is not None else None
+            self.device.call('ffx_graph_smooth', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                             2.0 / 3.0, ptr(level['q']), self.device.s)
+            if timer is not None:
+                timer.end(started)
+            level['p'], level['q'] = level['q'], level['p']
+            self.last_iterations += 1
+
+    def cycle(self, index):
+        level = self.levels[index]
+        dev = self.device
+        if index == len(self.levels) - 1:
+            if self.coarse_matrix is not None:
+                dev.call('ffx_direct_solve', prod(level['shape']), ptr(self.coarse_matrix), ptr(level['rhs']), 1.0,
+                         ptr(level['q']), dev.s)
+                level['p'], level['q'] = level['q'], level['p']
+            else:
+                self.smooth(level, 80)
+            return
+        self.smooth(level, self.pre_sweeps)
+        coarse = self.levels[index + 1]
+        dev.call('ffx_graph_residual_restrict', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                 ptr(coarse['rhs']), dev.s)
+        coarse['p'].zero_()
+        self.cycle(index + 1)
+        if self.post_sweeps > 0:
+            dev.call('ffx_graph_prolong_smooth', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
+                     ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), dev.s)
+            level['p'], level['q'] = level['q'], level['p']
+            self.last_iterations += 1
+            self.smooth(level, self.post_sweeps - 1)
+        else:
+            dev.call('ffx_graph_prolong', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
+                     ptr(level['q']), dev.s)
+            level['p'], level['q'] = level['q'], level['p']
+
+    def _residual_max(self):
+        level = self.levels[0]
+        self.device.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                         ptr(self._rmax[0:1]), self.device.s)
+        return float(self._rmax[0].item())
+
+    def solve_pressure(self, dt, previous_dt):
+        s = self.settings
+        self.last_cycles = 0
+        if len(self.levels) == 1:
+            return super().solve_pressure(dt, previous_dt)
+        if not (s.solid_warm_start and previous_dt is not None):
+            self.pressure.zero_()
+        self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
+        self.last_iterations = 0
+        budget = s.pressure_cycles * (s.pressure_cold_multiplier if previous_dt is None else 1)
+        if s.pressure_tolerance <= 0:
+            for _ in range(budget):
+                self.cycle(0)
+                self.last_cycles += 1
+        else:
+            self.device.call('ffx_max_abs', self.before.numel(), N.FFX_F32, ptr(self.before),
+                             ptr(self._rmax[1:2]), self.device.s)
+            scale = float(self._rmax[1].item())
+            if scale == 0:
+                self.levels[0]['p'].zero_()
+            else:
+                while self.last_cycles < s.pressure_max_cycles and self._residual_max() > s.pressure_tolerance * scale:
+                    self.cycle(0)
+                    self.last_cycles += 1
+        self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
+
+    def reset(self):
+        super().reset()
+        self.last_cycles = 0
+        for level in self.levels[1:]:
+            for name in ('p', 'q', 'rhs'):
+                level[name].zero_()
+
+    def level_edges(self, index):
+        """Host copy of a level's (+x, +y, +z, active) records, x-fast."""
+        level = self.levels[index]
+        if level['edges'] is not None:
+            return level['edges'].cpu().numpy()
+        nz, ny, nx = self.levels[0]['p'].shape
+        out = torch.empty((nz, ny, nx, 4), dtype=torch.float32, device=self.device.device)
+        self.device.call('ffx_graph_level0_edges', C.byref(level['graph']), ptr(out), self.device.s)
+        return out.cpu().numpy()
+
+    def metrics(self):
+        return super().metrics() | {
+            'solver': 'SOLID_MULTIGRID' if self.last_cycles else 'SOLID_JACOBI',
+            'v_cycles': self.last_cycles, 'levels': [v['shape'] for v in self.levels],
+            'coarse_solver': 'graph_pseudoinverse' if self.coarse_matrix is not None else 'masked_smoothing',
+            'aggregation': 'connected_children_only'}
+
+    def close(self):
+        self.levels = []
+        self.coarse_matrix = self.coarse_kernel = None
+        super().close()

@@ -1,0 +1,665 @@
+// Transport kernels: MacCormack face predictor, fused velocity transport
+// (+ emitters, buoyancy, walls), closed scalar transport and the final scalar
+// pass, and the P0.2/P0.3 open-boundary forms.
+//
+// One thread per output sample. Face passes cover all three face grids in one
+// launch (a linear index over U, then V, then W). Gathers go through the
+// read-only path; the 8-corner stencils of neighbouring threads overlap, so
+// the L1/L2 hit rate is high and HBM traffic stays close to one read of each
+// field per pass.
+#include "ffx_host.cuh"
+
+namespace ffx {
+namespace {
+
+constexpr int kThreads = 256;
+
+__device__ __forceinline__ int floor_int(float v) {
+    return (int)fmaxf(fminf(floorf(v), 1.0e9f), -1.0e9f);
+}
+
+struct FaceIdx {
+    int axis, x, y, z, sx, sy, sz;
+    int64_t i;
+};
+
+__device__ __forceinline__ bool decode_face(const Dev& d, int64_t g, FaceIdx& f) {
+    int64_t nu = (int64_t)(d.nx + 1) * d.ny * d.nz, nv = (int64_t)d.nx * (d.ny + 1) * d.nz;
+    int64_t nw = (int64_t)d.nx * d.ny * (d.nz + 1);
+    if (g < nu) { f.axis = 0; f.sx = d.nx + 1; f.sy = d.ny; f.sz = d.nz; }
+    else if (g < nu + nv) { g -= nu; f.axis = 1; f.sx = d.nx; f.sy = d.ny + 1; f.sz = d.nz; }
+    else if (g < nu + nv + nw) { g -= nu + nv; f.axis = 2; f.sx = d.nx; f.sy = d.ny; f.sz = d.nz + 1; }
+    else return false;
+    f.i = g;
+    f.x = (int)(g % f.sx);
+    int64_t r = g / f.sx;
+    f.y = (int)(r % f.sy);
+    f.z = (int)(r / f.sy);
+    return true;
+}
+
+__host__ __device__ __forceinline__ int64_t total_faces(const Dev& d) {
+    return (int64_t)(d.nx + 1) * d.ny * d.nz + (int64_t)d.nx * (d.ny + 1) * d.nz + (int64_t)d.nx * d.ny * (d.nz + 1);
+}
+
+// Midpoint backtrace p -> departure (transport_face.glsl:8-17 and the same
+// lines of every advection shader); clipped at colliders when MASK.
+template <typename T, bool MASK>
+__device__ __forceinline__ F3 backtrace(const Dev& d, const Faces<T>& F, const uint8_t* solid, F3 p, F3 v0,
+                                        float dt) {
+    float s = 0.5f * dt;
+    F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
+    if (MASK) mid = clip_solid_trace(d, solid, p, mid);
+    F3 vm = velocity_at(d, F, mid);
+    F3 dep = {p.x - dt * vm.x, p.y - dt * vm.y, p.z - dt * vm.z};
+    if (MASK) dep = clip_solid_trace(d, solid, p, dep);
+    return dep;
+}
+
+// Closed scalar sample (closed_sample.glsl:7-29).
+template <typename T, bool MASK>
+__device__ __forceinline__ float sample_closed(const Dev& d, const uint8_t* solid, const T* __restrict__ f,
+                                               float qx, float qy, float qz) {
+    float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
+    float fx = qx - bx, fy = qy - by, fz = qz - bz;
+    int ix = floor_int(qx), iy = floor_int(qy), iz = floor_int(qz);
+    int x0 = min(max(ix, 0), d.nx - 1), x1 = min(max(ix + 1, 0), d.nx - 1);
+    int y0 = min(max(iy, 0), d.ny - 1), y1 = min(max(iy + 1, 0), d.ny - 1);
+    int z0 = min(max(iz, 0), d.nz - 1), z1 = min(max(iz + 1, 0), d.nz - 1);
+    if (MASK) {
+        int xs[2] = {x0, x1}, ys[2] = {y0, y1}, zs[2] = {z0, z1};
+        float value = 0.f, total = 0.f;
+        for (int oz = 0; oz < 2; ++oz) {
+            float wz = oz ? fz : 1.f - fz;
+            for (int oy = 0; oy < 2; ++oy) {
+                float wy = oy ? fy : 1.f - fy;
+                for (int ox = 0; ox < 2; ++ox) {
+                    float wx = ox ? fx : 1.f - fx;
+                    int64_t c = cidx(d, xs[ox], ys[oy], zs[oz]);
+                    if (__ldg(solid + c)) continue;
+                    float weight = wx * wy * wz;
+                    value = value + weight * Store<T>::ld(f, c);
+                    total = total + weight;
+                }
+            }
+        }
+        return total > 1e-8f ? value / total : 0.f;
+    }
+    float f000 = Store<T>::ld(f, cidx(d, x0, y0, z0)), f100 = Store<T>::ld(f, cidx(d, x1, y0, z0));
+    float f010 = Store<T>::ld(f, cidx(d, x0, y1, z0)), f110 = Store<T>::ld(f, cidx(d, x1, y1, z0));
+    float f001 = Store<T>::ld(f, cidx(d, x0, y0, z1)), f101 = Store<T>::ld(f, cidx(d, x1, y0, z1));
+    float f011 = Store<T>::ld(f, cidx(d, x0, y1, z1)), f111 = Store<T>::ld(f, cidx(d, x1, y1, z1));
+    float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
+    float a0 = f000 * gx + f100 * fx, a1 = f010 * gx + f110 * fx;
+    float b0 = f001 * gx + f101 * fx, b1 = f011 * gx + f111 * fx;
+    float zz0 = a0 * gy + a1 * fy, zz1 = b0 * gy + b1 * fy;
+    return zz0 * gz + zz1 * fz;
+}
+
+template <typename T>
+__device__ __forceinline__ float fetch_closed(const Dev& d, const T* __restrict__ f, int x, int y, int z) {
+    x = min(max(x, 0), d.nx - 1);
+    y = min(max(y, 0), d.ny - 1);
+    z = min(max(z, 0), d.nz - 1);
+    return Store<T>::ld(f, cidx(d, x, y, z));
+}
+
+// ------------------------------------------------------------ face predictor
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const uint8_t* __restrict__ solid,
+                                                                  Faces<T> F, float dt, T* pu, T* pv, T* pw) {
+    FaceIdx f;
+    if (!decode_face(d, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, f)) return;
+    T* out = f.axis == 0 ? pu : (f.axis == 1 ? pv : pw);
+    if (MASK && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
+        Store<T>::st(out, f.i, 0.f);
+        return;
+    }
+    float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
+    F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
+    F3 v0 = velocity_at(d, F, p);
+    F3 dep = backtrace<T, MASK>(d, F, solid, p, v0, dt);
+    const T* src = f.axis == 0 ? F.u : (f.axis == 1 ? F.v : F.w);
+    float value = sample_face(src, f.sx, f.sy, f.sz, dep.x / d.h[0] - ox, dep.y / d.h[1] - oy, dep.z / d.h[2] - oz);
+    Store<T>::st(out, f.i, value);
+}
+
+// ------------------------------------------------------- velocity transport
+template <typename T>
+struct VelParams {
+    Dev d;
+    const uint8_t* solid;
+    const uint8_t* halo;
+    Faces<T> F;       // velocity at the start of the step
+    Faces<T> P;       // MacCormack predictor
+    float dt, blend, lift, weight;
+    int corrected, apply_walls;
+    const T* density;
+    const T* temperature;
+    T* out[3];
+    SrcDev src;
+};
+
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
+    const Dev& d = P.d;
+    FaceIdx f;
+    if (!decode_face(d, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, f)) return;
+    const int axis = f.axis;
+    const float dt = P.dt;
+    bool blocked = MASK && solid_face(d, P.solid, f.x, f.y, f.z, axis);
+    float value = 0.f;
+    if (!blocked) {
+        float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
+        F3 p = {((float)f.x + off[0]) * d.e[0] / d.nf[0], ((float)f.y + off[1]) * d.e[1] / d.nf[1],
+                ((float)f.z + off[2]) * d.e[2] / d.nf[2]};
+        F3 v0 = velocity_at(d, P.F, p);
+        F3 dep = backtrace<T, MASK>(d, P.F, P.solid, p, v0, dt);
+        const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
+        const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
+        float qx = dep.x / d.h[0] - off[0], qy = dep.y / d.h[1] - off[1], qz = dep.z / d.h[2] - off[2];
+        float low = sample_face(orig, f.sx, f.sy, f.sz, qx, qy, qz);
+        value = low;
+        if (P.corrected) {
+            // correct_velocity_fused.glsl:5-27
+            float size[3] = {(float)(f.sx - 1), (float)(f.sy - 1), (float)(f.sz - 1)};
+            float lob[3], hib[3];
+            for (int k = 0; k < 3; ++k) {
+                lob[k] = off[k] * d.h[k];
+                hib[k] = (size[k] + off[k]) * d.h[k];
+            }
+            float s = 0.5f * dt;
+            F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
+            F3 vm2 = velocity_at(d, P.F, mid2);
+            F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
+            bool ok = !(dep.x < lob[0] || dep.y < lob[1] || dep.z < lob[2] || dep.x > hib[0] || dep.y > hib[1] ||
+                        dep.z > hib[2] || arr.x < lob[0] || arr.y < lob[1] || arr.z < lob[2] || arr.x > hib[0] ||
+                        arr.y > hib[1] || arr.z > hib[2]);
+            if (MASK && ok) ok = safe_solid_correction(d, P.solid, P.halo, p, dep, mid2, arr);
+            if (ok) {
+                float pa = sample_face(pred, f.sx, f.sy, f.sz, arr.x / d.h[0] - off[0], arr.y / d.h[1] - off[1],
+                                       arr.z / d.h[2] - off[2]);
+                float val = Store<T>::ld(pred, f.i) + 0.5f * (Store<T>::ld(orig, f.i) - pa);
+                int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
+                int64_t sxy = (int64_t)f.sx * f.sy;
+                float lo = 0.f, hi = 0.f;
+                bool first = true;
+                for (int oz = 0; oz < 2; ++oz)
+                    for (int oy = 0; oy < 2; ++oy)
+                        for (int ox = 0; ox < 2; ++ox) {
+                            int cx = min(max(bx + ox, 0), f.sx - 1), cy = min(max(by + oy, 0), f.sy - 1);
+                            int cz = min(max(bz + oz, 0), f.sz - 1);
+                            float v = Store<T>::ld(orig, (int64_t)cz * sxy + (int64_t)cy * f.sx + cx);
+                            if (first) { lo = hi = v; first = false; }
+                            else { lo = fminf(lo, v); hi = fmaxf(hi, v); }
+                        }
+                float cl = fminf(fmaxf(val, lo), hi);
+                value = low * (1.f - P.blend) + cl * P.blend;
+            }
+        }
+        const SrcDev& S = P.src;
+        if (S.count < 0) {
+            float w = emission_weight(p, S.center, S.start, S.radius, S.single_solid != 0);
+            float bl = 1.f - expf(-S.coupling * dt * w);
+            value = value * (1.f - bl) + comp(S.jet, axis) * bl;
+        } else if (S.count > 0) {
+            float total = 0.f, target = 0.f;
+            for (int i = 0; i < S.count; ++i) {
+                float rate = S.table[16 * i + 7] * table_weight(S, i, p);
+                total = total + rate;
+                target = target + rate * S.table[16 * i + 8 + axis];
+            }
+            if (total > 0.f) {
+                float bl = 1.f - expf(-dt * total);
+                value = value * (1.f - bl) + (target / total) * bl;
+            }
+        }
+    }
+    if (axis == 2 && P.density) {
+        // buoyancy.glsl:1-14 with the previous step's scalars
+        int below = min(max(f.z - 1, 0), d.nz - 1), above = min(max(f.z, 0), d.nz - 1);
+        int64_t ib = cidx(d, f.x, f.y, below), ia = cidx(d, f.x, f.y, above);
+        float rho = 0.5f * (Store<T>::ld(P.density, ib) + Store<T>::ld(P.density, ia));
+        float theta = 0.5f * (Store<T>::ld(P.temperature, ib) + Store<T>::ld(P.temperature, ia));
+        float a = P.lift * theta - P.weight * rho;
+        value = value + dt * a;
+    }
+    if (P.apply_walls) {
+        int c = axis == 0 ? f.x : (axis == 1 ? f.y : f.z);
+        int n = axis == 0 ? f.sx : (axis == 1 ? f.sy : f.sz);
+        if (c == 0 || c == n - 1 || blocked) value = 0.f;
+    }
+    Store<T>::st(P.out[axis], f.i, value);
+}
+
+// P0.3 plain face self-advection (mac_advect_velocity.glsl).
+template <typename T>
+__global__ void __launch_bounds__(kThreads) mac_advect_velocity_kernel(Dev d, Faces<T> F, float dt, T* ou, T* ov,
+                                                                       T* ow) {
+    FaceIdx f;
+    if (!decode_face(d, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, f)) return;
+    float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
+    F3 p = {((float)f.x + ox) * d.e[0] / d.nf[0], ((float)f.y + oy) * d.e[1] / d.nf[1],
+            ((float)f.z + oz) * d.e[2] / d.nf[2]};
+    F3 v0 = velocity_at(d, F, p);
+    F3 dep = backtrace<T, false>(d, F, nullptr, p, v0, dt);
+    F3 v = velocity_at(d, F, dep);
+    T* out = f.axis == 0 ? ou : (f.axis == 1 ? ov : ow);
+    Store<T>::st(out, f.i, comp(v, f.axis));
+}
+
+template <typename T>
+__global__ void buoyancy_kernel(Dev d, const T* w_in, const T* density, const T* temperature, float dt, float lift,
+                                float weight, T* w_out) {
+    int64_t n = (int64_t)d.nx * d.ny * (d.nz + 1);
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    int below = min(max(z - 1, 0), d.nz - 1), above = min(max(z, 0), d.nz - 1);
+    int64_t ib = cidx(d, x, y, below), ia = cidx(d, x, y, above);
+    float rho = 0.5f * (Store<T>::ld(density, ib) + Store<T>::ld(density, ia));
+    float theta = 0.5f * (Store<T>::ld(temperature, ib) + Store<T>::ld(temperature, ia));
+    float a = lift * theta - weight * rho;
+    Store<T>::st(w_out, i, Store<T>::ld(w_in, i) + dt * a);
+}
+
+// ------------------------------------------------------------- scalar passes
+template <typename T>
+struct ScalarXport {
+    Dev d;
+    const uint8_t* solid;
+    Faces<T> F;
+    float dt;
+    int count;
+    const T* in[3];
+    T* out[3];
+};
+
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
+    const Dev& d = P.d;
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    if (MASK && __ldg(P.solid + i)) {
+        for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, 0.f);
+        return;
+    }
+    F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
+    F3 v0 = velocity_at(d, P.F, p);
+    F3 dep = backtrace<T, MASK>(d, P.F, P.solid, p, v0, P.dt);
+    float qx = dep.x / d.h[0] - 0.5f, qy = dep.y / d.h[1] - 0.5f, qz = dep.z / d.h[2] - 0.5f;
+    for (int c = 0; c < P.count; ++c)
+        Store<T>::st(P.out[c], i, sample_closed<T, MASK>(d, P.solid, P.in[c], qx, qy, qz));
+}
+
+template <typename T>
+struct Channel {
+    const T* field;
+    const T* pred;
+    const T* rev;
+    T* out;
+    float rate, decay, target;
+    int channel, table_target;
+};
+
+template <typename T>
+struct ScalarFinal {
+    Dev d;
+    const uint8_t* solid;
+    const uint8_t* halo;
+    Faces<T> F;
+    float dt;
+    int corrected, count;
+    Channel<T> ch[3];
+    float* maxima;
+    SrcDev src;
+};
+
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
+    const Dev& d = P.d;
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float vmax[3] = {0.f, 0.f, 0.f};
+    if (i < n) {
+        int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+        if (MASK && __ldg(P.solid + i)) {
+            for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
+        } else {
+            const float dt = P.dt;
+            F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
+            F3 v0 = velocity_at(d, P.F, p);
+            F3 dep = backtrace<T, MASK>(d, P.F, P.solid, p, v0, dt);
+            float qx = dep.x / d.h[0] - 0.5f, qy = dep.y / d.h[1] - 0.5f, qz = dep.z / d.h[2] - 0.5f;
+            bool ok = false;
+            if (P.corrected) {
+                // correct_scalar.glsl:1-21
+                float s = 0.5f * dt;
+                F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
+                F3 vm2 = velocity_at(d, P.F, mid2);
+                F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
+                float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
+                float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
+                ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
+                       dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
+                       arr.y > hb[1] || arr.z > hb[2]);
+                if (MASK && ok) ok = safe_solid_correction(d, P.solid, P.halo, p, dep, mid2, arr);
+            }
+            int bx = 0, by = 0, bz = 0;
+            if (ok) { bx = (int)floorf(qx); by = (int)floorf(qy); bz = (int)floorf(qz); }
+            const SrcDev& S = P.src;
+            for (int c = 0; c < P.count; ++c) {
+                const Channel<T>& C = P.ch[c];
+                float value = sample_closed<T, MASK>(d, P.solid, C.field, qx, qy, qz);
+                if (ok) {
+                    float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
+                    float lo = fetch_closed(d, C.field, bx, by, bz), hi = lo;
+                    for (int oz = 0; oz < 2; ++oz)
+                        for (int oy = 0; oy < 2; ++oy)
+                            for (int ox = 0; ox < 2; ++ox) {
+                                float v = fetch_closed(d, C.field, bx + ox, by + oy, bz + oz);
+                                lo = fminf(lo, v);
+                                hi = fmaxf(hi, v);
+                            }
+                    value = fminf(fmaxf(val, lo), hi);
+                }
+                value = value * expf(-C.decay * dt);
+                if (S.count < 0) {
+                    float w = emission_weight(p, S.center, S.start, S.radius, S.single_solid != 0);
+                    value = C.target >= 0.f ? fmaxf(value, C.target * w) : value + dt * C.rate * w;
+                } else {
+                    float tgt = 0.f;
+                    for (int k = 0; k < S.count; ++k) {
+                        const float* row = S.table + 16 * k;
+                        float r = C.channel == 0 ? row[11] : (C.channel == 1 ? row[12] : row[15]);
+                        float w = table_weight(S, k, p);
+                        bool is_target = (C.channel == 0 && row[13] > 0.5f) || (C.channel == 1 && C.table_target);
+                        if (is_target) tgt = fmaxf(tgt, r * w);
+                        else value = value + dt * r * w;
+                    }
+                    if (C.channel == 0 || (C.channel == 1 && C.table_target)) value = fmaxf(value, tgt);
+                }
+                Store<T>::st(C.out, i, value);
+                vmax[c] = finite_abs(value);
+            }
+        }
+    }
+    if (P.maxima) {
+        for (int c = 0; c < P.count; ++c) {
+            block_max_to(P.maxima + c, vmax[c]);
+            __syncthreads();
+        }
+    }
+}
+
+// P0.2 open-boundary transport in an analytic flow (advect.glsl).
+__device__ __forceinline__ F3 analytic_velocity(const Dev& d, F3 p, F3 base, float w) {
+    float qx = p.x - 0.5f * d.e[0], qy = p.y - 0.5f * d.e[1];
+    F3 r = {base.x + (-w * qy), base.y + w * qx, base.z};
+    return r;
+}
+
+template <typename T>
+__device__ __forceinline__ float sample_zero(const Dev& d, const T* __restrict__ f, float qx, float qy, float qz) {
+    float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
+    float fx = qx - bx, fy = qy - by, fz = qz - bz;
+    int ix = floor_int(qx), iy = floor_int(qy), iz = floor_int(qz);
+    auto fz_ = [&](int ox, int oy, int oz) -> float {
+        int x = ix + ox, y = iy + oy, z = iz + oz;
+        if (x < 0 || y < 0 || z < 0 || x >= d.nx || y >= d.ny || z >= d.nz) return 0.f;
+        return Store<T>::ld(f, cidx(d, x, y, z));
+    };
+    float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
+    float a0 = fz_(0, 0, 0) * gx + fz_(1, 0, 0) * fx, a1 = fz_(0, 1, 0) * gx + fz_(1, 1, 0) * fx;
+    float b0 = fz_(0, 0, 1) * gx + fz_(1, 0, 1) * fx, b1 = fz_(0, 1, 1) * gx + fz_(1, 1, 1) * fx;
+    float z0 = a0 * gy + a1 * fy, z1 = b0 * gy + b1 * fy;
+    return z0 * gz + z1 * fz;
+}
+
+struct OpenParams {
+    Dev d;
+    float dt, angular, radius, rate, decay;
+    F3 base, center;
+};
+
+template <typename T>
+__global__ void advect_open_kernel(OpenParams P, const T* in, T* out) {
+    const Dev& d = P.d;
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
+    F3 v = analytic_velocity(d, p, P.base, P.angular);
+    float s = 0.5f * P.dt;
+    F3 mid = {p.x - s * v.x, p.y - s * v.y, p.z - s * v.z};
+    F3 vm = analytic_velocity(d, mid, P.base, P.angular);
+    F3 dep = {p.x - P.dt * vm.x, p.y - P.dt * vm.y, p.z - P.dt * vm.z};
+    float value = sample_zero(d, in, dep.x / d.h[0] - 0.5f, dep.y / d.h[1] - 0.5f, dep.z / d.h[2] - 0.5f) *
+                  expf(-P.decay * P.dt);
+    F3 off = {p.x - P.center.x, p.y - P.center.y, p.z - P.center.z};
+    float w = fmaxf(1.0f - dot3(off, off) / (P.radius * P.radius), 0.0f);
+    Store<T>::st(out, i, value + P.dt * P.rate * w * w);
+}
+
+template <typename T>
+__global__ void mac_advect_density_kernel(OpenParams P, Faces<T> F, const T* in, T* out) {
+    const Dev& d = P.d;
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
+    F3 v0 = velocity_at(d, F, p);
+    F3 dep = backtrace<T, false>(d, F, nullptr, p, v0, P.dt);
+    float value = sample_zero(d, in, dep.x / d.h[0] - 0.5f, dep.y / d.h[1] - 0.5f, dep.z / d.h[2] - 0.5f) *
+                  expf(-P.decay * P.dt);
+    F3 off = {p.x - P.center.x, p.y - P.center.y, p.z - P.center.z};
+    float w = fmaxf(1.0f - dot3(off, off) / (P.radius * P.radius), 0.0f);
+    Store<T>::st(out, i, value + P.dt * P.rate * w * w);
+}
+
+bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s->solid && s->halo); }
+bool has_mask(const FfxSolids* s) { return s && s->solid; }
+
+}  // namespace
+}  // namespace ffx
+
+using namespace ffx;
+
+extern "C" {
+
+int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                       const void* w, float dt, void* pu, void* pv, void* pw, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && pu && pv && pw,
+                "ffx_face_predictor: invalid arguments");
+    FFX_REQUIRE(pu != u && pv != v && pw != w, "ffx_face_predictor: outputs must not alias inputs");
+    Dev d = make_dev(*g);
+    unsigned blocks = blocks_for(total_faces(d), kThreads);
+    cudaStream_t st = as_stream(stream);
+    const uint8_t* solid = has_mask(s) ? s->solid : nullptr;
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        if (solid) face_predictor_kernel<T, true><<<blocks, kThreads, 0, st>>>(d, solid, F, dt, (T*)pu, (T*)pv, (T*)pw);
+        else face_predictor_kernel<T, false><<<blocks, kThreads, 0, st>>>(d, nullptr, F, dt, (T*)pu, (T*)pv, (T*)pw);
+    });
+    return launch_status("face_predictor_kernel");
+}
+
+int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                        const void* w, const void* pu, const void* pv, const void* pw, float dt, int corrected,
+                        float blend, const FfxSources* src, const void* density, const void* temperature,
+                        float lift, float weight, int apply_walls, void* ou, void* ov, void* ow, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && ou && ov && ow,
+                "ffx_advect_velocity: invalid arguments");
+    FFX_REQUIRE(!corrected || (pu && pv && pw), "ffx_advect_velocity: MacCormack needs the predictor faces");
+    FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_advect_velocity: outputs must not alias inputs");
+    FFX_REQUIRE(!src || src->count <= 8, "ffx_advect_velocity: at most eight sources");
+    FFX_REQUIRE((density == nullptr) == (temperature == nullptr), "ffx_advect_velocity: density and temperature "
+                "must both be given for buoyancy");
+    FFX_REQUIRE(blend >= 0.f && blend <= 1.f, "ffx_advect_velocity: blend must lie in [0, 1]");
+    Dev d = make_dev(*g);
+    unsigned blocks = blocks_for(total_faces(d), kThreads);
+    cudaStream_t st = as_stream(stream);
+    FFX_DISPATCH_STORAGE(storage, T, {
+        VelParams<T> P;
+        P.d = d;
+        P.solid = has_mask(s) ? s->solid : nullptr;
+        P.halo = has_mask(s) ? s->halo : nullptr;
+        P.F = {(const T*)u, (const T*)v, (const T*)w};
+        P.P = corrected ? Faces<T>{(const T*)pu, (const T*)pv, (const T*)pw} : P.F;
+        P.dt = dt;
+        P.blend = blend;
+        P.lift = lift;
+        P.weight = weight;
+        P.corrected = corrected;
+        P.apply_walls = apply_walls;
+        P.density = (const T*)density;
+        P.temperature = (const T*)temperature;
+        P.out[0] = (T*)ou; P.out[1] = (T*)ov; P.out[2] = (T*)ow;
+        P.src = make_src(src);
+        if (!src) P.src.count = 0;
+        if (P.solid) advect_velocity_kernel<T, true><<<blocks, kThreads, 0, st>>>(P);
+        else advect_velocity_kernel<T, false><<<blocks, kThreads, 0, st>>>(P);
+    });
+    return launch_status("advect_velocity_kernel");
+}
+
+int ffx_mac_advect_velocity(const FfxGrid* g, int storage, const void* u, const void* v, const void* w, float dt,
+                            void* ou, void* ov, void* ow, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && u && v && w && ou && ov && ow && ou != u && ov != v && ow != w,
+                "ffx_mac_advect_velocity: invalid arguments");
+    Dev d = make_dev(*g);
+    unsigned blocks = blocks_for(total_faces(d), kThreads);
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        mac_advect_velocity_kernel<T><<<blocks, kThreads, 0, as_stream(stream)>>>(d, F, dt, (T*)ou, (T*)ov, (T*)ow);
+    });
+    return launch_status("mac_advect_velocity_kernel");
+}
+
+int ffx_buoyancy(const FfxGrid* g, int storage, const void* w_in, const void* density, const void* temperature,
+                 float dt, float lift, float weight, void* w_out, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && w_in && density && temperature && w_out && w_in != w_out,
+                "ffx_buoyancy: invalid arguments");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * (g->nz + 1);
+    FFX_DISPATCH_STORAGE(storage, T,
+        buoyancy_kernel<T><<<blocks_for(n, kThreads), kThreads, 0, as_stream(stream)>>>(
+            d, (const T*)w_in, (const T*)density, (const T*)temperature, dt, lift, weight, (T*)w_out));
+    return launch_status("buoyancy_kernel");
+}
+
+int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                         const void* w, float dt, int count, const void* const* in, void* const* out, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 && in &&
+                out, "ffx_scalar_transport: invalid arguments");
+    for (int c = 0; c < count; ++c)
+        FFX_REQUIRE(in[c] && out[c] && in[c] != out[c], "ffx_scalar_transport: channel %d invalid or aliased", c);
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    cudaStream_t st = as_stream(stream);
+    FFX_DISPATCH_STORAGE(storage, T, {
+        ScalarXport<T> P;
+        P.d = d;
+        P.solid = has_mask(s) ? s->solid : nullptr;
+        P.F = {(const T*)u, (const T*)v, (const T*)w};
+        P.dt = dt;
+        P.count = count;
+        for (int c = 0; c < 3; ++c) {
+            P.in[c] = c < count ? (const T*)in[c] : nullptr;
+            P.out[c] = c < count ? (T*)out[c] : nullptr;
+        }
+        if (P.solid) scalar_transport_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
+        else scalar_transport_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
+    });
+    return launch_status("scalar_transport_kernel");
+}
+
+int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                       const void* w, float dt, int corrected, const FfxSources* src, int count,
+                       const FfxScalarChannel* channels, float* maxima, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 &&
+                channels && src && src->count <= 8, "ffx_advect_scalars: invalid arguments");
+    for (int c = 0; c < count; ++c) {
+        const FfxScalarChannel& C = channels[c];
+        FFX_REQUIRE(C.field && C.out && C.out != C.field, "ffx_advect_scalars: channel %d invalid or aliased", c);
+        FFX_REQUIRE(!corrected || (C.predictor && C.reverse), "ffx_advect_scalars: channel %d lacks predictor", c);
+    }
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    cudaStream_t st = as_stream(stream);
+    if (maxima) {
+        int e = cuda_status(cudaMemsetAsync(maxima, 0, sizeof(float) * count, st), "ffx_advect_scalars memset");
+        if (e) return e;
+    }
+    FFX_DISPATCH_STORAGE(storage, T, {
+        ScalarFinal<T> P;
+        P.d = d;
+        P.solid = has_mask(s) ? s->solid : nullptr;
+        P.halo = has_mask(s) ? s->halo : nullptr;
+        P.F = {(const T*)u, (const T*)v, (const T*)w};
+        P.dt = dt;
+        P.corrected = corrected;
+        P.count = count;
+        for (int c = 0; c < 3; ++c) {
+            Channel<T> C = {};
+            if (c < count) {
+                const FfxScalarChannel& H = channels[c];
+                C.field = (const T*)H.field;
+                C.pred = (const T*)(H.predictor ? H.predictor : H.field);
+                C.rev = (const T*)(H.reverse ? H.reverse : H.field);
+                C.out = (T*)H.out;
+                C.rate = H.rate;
+                C.decay = H.decay;
+                C.target = H.target;
+                C.channel = H.channel;
+                C.table_target = H.table_target;
+            }
+            P.ch[c] = C;
+        }
+        P.maxima = maxima;
+        P.src = make_src(src);
+        if (P.solid) advect_scalars_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
+        else advect_scalars_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
+    });
+    return launch_status("advect_scalars_kernel");
+}
+
+int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt, const float base[3], float angular,
+                    const float center[3], float radius, float rate, float decay, void* out, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && in && out && in != out && base && center && radius > 0.f,
+                "ffx_advect_open: invalid arguments");
+    OpenParams P;
+    P.d = make_dev(*g);
+    P.dt = dt; P.angular = angular; P.radius = radius; P.rate = rate; P.decay = decay;
+    P.base = {base[0], base[1], base[2]};
+    P.center = {center[0], center[1], center[2]};
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    FFX_DISPATCH_STORAGE(storage, T,
+        advect_open_kernel<T><<<blocks_for(n, kThreads), kThreads, 0, as_stream(stream)>>>(P, (const T*)in, (T*)out));
+    return launch_status("advect_open_kernel");
+}
+
+int ffx_mac_advect_density(const FfxGrid* g, int storage, const void* u, const void* v, const void* w, const void* in,
+                           float dt, const float center[3], float radius, float rate, float decay, void* out,
+                           void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && u && v && w && in && out && in != out && center && radius > 0.f,
+                "ffx_mac_advect_density: invalid arguments");
+    OpenParams P;
+    P.d = make_dev(*g);
+    P.dt = dt; P.angular = 0.f; P.radius = radius; P.rate = rate; P.decay = decay;
+    P.base = {0.f, 0.f, 0.f};
+    P.center = {center[0], center[1], center[2]};
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        mac_advect_density_kernel<T><<<blocks_for(n, kThreads), kThreads, 0, as_stream(stream)>>>(P, F, (const T*)in,
+                                                                                                (T*)out);
+    });
+    return launch_status("mac_advect_density_kernel");
+}
+
+}  // extern "C"

@@ -1,0 +1,279 @@
+// Shared device code of libffx_core: grid constants, storage loads/stores,
+// samplers, collider tests and emitter weights.
+//
+// Every expression keeps the evaluation order of the reference shaders
+// (fluxfx/shaders/*.glsl) and the library is compiled with --fmad=false, so a
+// float result and every discrete decision (floor, clamp, trace clipping,
+// MacCormack fallbacks) equal those of a strict IEEE FP32 evaluation.
+#pragma once
+#include <cuda_runtime.h>
+#include <cuda_bf16.h>
+#include <stdint.h>
+
+#include "../../include/ffx.h"
+
+namespace ffx {
+
+// ---------------------------------------------------------------- storage
+template <typename T> struct Store;
+template <> struct Store<float> {
+    static __device__ __forceinline__ float ld(const float* p, int64_t i) { return __ldg(p + i); }
+    static __device__ __forceinline__ void st(float* p, int64_t i, float v) { p[i] = v; }
+};
+template <> struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const __nv_bfloat16* p, int64_t i) {
+        return __bfloat162float(p[i]);
+    }
+    static __device__ __forceinline__ void st(__nv_bfloat16* p, int64_t i, float v) {
+        p[i] = __float2bfloat16_rn(v);
+    }
+};
+
+// ---------------------------------------------------------------- grid
+struct Dev {
+    int nx, ny, nz;          // cells
+    float nf[3];             // float(cell counts)
+    float e[3];              // extent
+    float h[3];              // e / n (FP32 division, as the shaders compute it)
+    float inv[3];            // host-side 1/h rounded to FP32 (the invCell uniform)
+};
+
+inline Dev make_dev(const FfxGrid& g) {
+    Dev d;
+    d.nx = g.nx; d.ny = g.ny; d.nz = g.nz;
+    int n[3] = {g.nx, g.ny, g.nz};
+    float e[3] = {g.ex, g.ey, g.ez};
+    double e64[3] = {g.ex, g.ey, g.ez};
+    float given[3] = {g.ix, g.iy, g.iz};
+    for (int i = 0; i < 3; ++i) {
+        d.nf[i] = (float)n[i];
+        d.e[i] = e[i];
+        d.h[i] = e[i] / (float)n[i];
+        d.inv[i] = given[i] != 0.f ? given[i] : (float)(1.0 / (e64[i] / (double)n[i]));
+    }
+    return d;
+}
+
+__device__ __forceinline__ int64_t cidx(const Dev& d, int x, int y, int z) {
+    return (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)d.ny * z);
+}
+
+struct F3 { float x, y, z; };
+__device__ __forceinline__ float comp(const F3& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
+__device__ __forceinline__ float dot3(const F3& a, const F3& b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
+
+// ---------------------------------------------------------------- samplers
+// Clamped trilinear sample of a face grid of size (sx, sy, sz)
+// (mac_sample.glsl:2-19).
+template <typename T>
+__device__ __forceinline__ float sample_face(const T* __restrict__ f, int sx, int sy, int sz,
+                                             float qx, float qy, float qz) {
+    qx = fminf(fmaxf(qx, 0.f), (float)(sx - 1));
+    qy = fminf(fmaxf(qy, 0.f), (float)(sy - 1));
+    qz = fminf(fmaxf(qz, 0.f), (float)(sz - 1));
+    float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
+    float fx = qx - bx, fy = qy - by, fz = qz - bz;
+    int ix = (int)bx, iy = (int)by, iz = (int)bz;
+    int ix1 = min(ix + 1, sx - 1), iy1 = min(iy + 1, sy - 1), iz1 = min(iz + 1, sz - 1);
+    int64_t sxy = (int64_t)sx * sy;
+    int64_t r00 = (int64_t)iz * sxy + (int64_t)iy * sx, r01 = (int64_t)iz * sxy + (int64_t)iy1 * sx;
+    int64_t r10 = (int64_t)iz1 * sxy + (int64_t)iy * sx, r11 = (int64_t)iz1 * sxy + (int64_t)iy1 * sx;
+    float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
+    float v = 0.f;
+    v = v + gx * gy * gz * Store<T>::ld(f, r00 + ix);
+    v = v + fx * gy * gz * Store<T>::ld(f, r00 + ix1);
+    v = v + gx * fy * gz * Store<T>::ld(f, r01 + ix);
+    v = v + fx * fy * gz * Store<T>::ld(f, r01 + ix1);
+    v = v + gx * gy * fz * Store<T>::ld(f, r10 + ix);
+    v = v + fx * gy * fz * Store<T>::ld(f, r10 + ix1);
+    v = v + gx * fy * fz * Store<T>::ld(f, r11 + ix);
+    v = v + fx * fy * fz * Store<T>::ld(f, r11 + ix1);
+    return v;
+}
+
+template <typename T>
+struct Faces {
+    const T* u; const T* v; const T* w;
+};
+
+// Staggered velocity at a physical point (mac_sample.glsl:20-26).
+template <typename T>
+__device__ __forceinline__ F3 velocity_at(const Dev& d, const Faces<T>& F, F3 p) {
+    float qx = p.x * d.nf[0] / d.e[0];
+    float qy = p.y * d.nf[1] / d.e[1];
+    float qz = p.z * d.nf[2] / d.e[2];
+    F3 r;
+    r.x = sample_face(F.u, d.nx + 1, d.ny, d.nz, qx, qy - 0.5f, qz - 0.5f);
+    r.y = sample_face(F.v, d.nx, d.ny + 1, d.nz, qx - 0.5f, qy, qz - 0.5f);
+    r.z = sample_face(F.w, d.nx, d.ny, d.nz + 1, qx - 0.5f, qy - 0.5f, qz);
+    return r;
+}
+
+// ---------------------------------------------------------------- colliders
+__device__ __forceinline__ bool solid_cell(const Dev& d, const uint8_t* __restrict__ solid,
+                                           int x, int y, int z) {
+    if (x < 0 || y < 0 || z < 0 || x >= d.nx || y >= d.ny || z >= d.nz) return true;
+    return __ldg(solid + cidx(d, x, y, z)) != 0;
+}
+
+__device__ __forceinline__ bool solid_face(const Dev& d, const uint8_t* __restrict__ solid,
+                                           int x, int y, int z, int axis) {
+    return solid_cell(d, solid, x, y, z) ||
+           solid_cell(d, solid, x - (axis == 0), y - (axis == 1), z - (axis == 2));
+}
+
+// Voxel DDA clip of the segment origin -> target at the first solid cell, at
+// most 384 crossings (solid_boundary.glsl:13-36).
+__device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __restrict__ solid,
+                                               F3 origin, F3 target) {
+    float cnt[3] = {d.nf[0], d.nf[1], d.nf[2]};
+    float o[3] = {origin.x, origin.y, origin.z}, t3[3] = {target.x, target.y, target.z};
+    float a[3], b[3], delta[3], crossing[3], stride[3];
+    int cell[3], dir[3];
+    for (int i = 0; i < 3; ++i) {
+        a[i] = fminf(fmaxf(o[i] / d.e[i] * cnt[i], 0.0001f), cnt[i] - 0.0001f);
+        b[i] = fminf(fmaxf(t3[i] / d.e[i] * cnt[i], 0.0001f), cnt[i] - 0.0001f);
+        delta[i] = b[i] - a[i];
+        cell[i] = (int)floorf(a[i]);
+        dir[i] = delta[i] > 0.f ? 1 : (delta[i] < 0.f ? -1 : 0);
+        crossing[i] = 1e20f;
+        stride[i] = 1e20f;
+    }
+    if (solid_cell(d, solid, cell[0], cell[1], cell[2])) return origin;
+    for (int i = 0; i < 3; ++i) {
+        if (fabsf(delta[i]) > 1e-10f) {
+            float edge = (float)(cell[i] + (dir[i] > 0 ? 1 : 0));
+            crossing[i] = (edge - a[i]) / delta[i];
+            stride[i] = 1.0f / fabsf(delta[i]);
+        }
+    }
+    float len = sqrtf((delta[0] * delta[0] + delta[1] * delta[1]) + delta[2] * delta[2]);
+    for (int it = 0; it < 384; ++it) {
+        int axis = (crossing[0] <= crossing[1] && crossing[0] <= crossing[2]) ? 0
+                   : (crossing[1] <= crossing[2] ? 1 : 2);
+        float t = crossing[axis];
+        if (t >= 1.0f) {
+            F3 r = {b[0] / cnt[0] * d.e[0], b[1] / cnt[1] * d.e[1], b[2] / cnt[2] * d.e[2]};
+            return r;
+        }
+        cell[axis] += dir[axis];
+        if (solid_cell(d, solid, cell[0], cell[1], cell[2])) {
+            float back = fmaxf(0.f, t - 0.0001f / fmaxf(len, 1.0f));
+            F3 r = {(a[0] + delta[0] * back) / cnt[0] * d.e[0], (a[1] + delta[1] * back) / cnt[1] * d.e[1],
+                    (a[2] + delta[2] * back) / cnt[2] * d.e[2]};
+            return r;
+        }
+        crossing[axis] += stride[axis];
+    }
+    return origin;
+}
+
+// Any solid (or out-of-domain) cell in the 3x3x3 block around p, read from the
+// precomputed dilated mask (solid_boundary.glsl:39-44).
+__device__ __forceinline__ bool solid_halo(const Dev& d, const uint8_t* __restrict__ halo, F3 p) {
+    int cx = (int)floorf(p.x / d.e[0] * d.nf[0]);
+    int cy = (int)floorf(p.y / d.e[1] * d.nf[1]);
+    int cz = (int)floorf(p.z / d.e[2] * d.nf[2]);
+    if (cx < 0 || cy < 0 || cz < 0 || cx >= d.nx || cy >= d.ny || cz >= d.nz) return true;
+    return __ldg(halo + cidx(d, cx, cy, cz)) != 0;
+}
+
+__device__ __forceinline__ float dist3(F3 a, F3 b) {
+    F3 c = {a.x - b.x, a.y - b.y, a.z - b.z};
+    return sqrtf(dot3(c, c));
+}
+
+__device__ __forceinline__ bool safe_solid_correction(const Dev& d, const uint8_t* solid,
+                                                      const uint8_t* halo, F3 p, F3 dep, F3 mid,
+                                                      F3 arr) {
+    if (solid_halo(d, halo, p) || solid_halo(d, halo, dep) || solid_halo(d, halo, arr)) return false;
+    if (!(dist3(clip_solid_trace(d, solid, p, dep), dep) < 1e-7f)) return false;
+    if (!(dist3(clip_solid_trace(d, solid, p, mid), mid) < 1e-7f)) return false;
+    return dist3(clip_solid_trace(d, solid, p, arr), arr) < 1e-7f;
+}
+
+// ---------------------------------------------------------------- emitters
+// Exact time average of the compact sphere profile along a linear sweep
+// (emission_weight.glsl:2-29).
+__device__ __forceinline__ float emission_weight(F3 p, F3 center, F3 start, float radius, bool solid) {
+    F3 seg = {center.x - start.x, center.y - start.y, center.z - start.z};
+    float l2 = dot3(seg, seg);
+    float r2 = radius * radius;
+    if (l2 < 1e-12f) {
+        F3 dd = {p.x - center.x, p.y - center.y, p.z - center.z};
+        float q = dot3(dd, dd);
+        float w = fmaxf(1.0f - q / r2, 0.0f);
+        return solid ? (q < r2 ? 1.0f : 0.0f) : w * w;
+    }
+    float lp = sqrtf(l2);
+    F3 ax = {seg.x / lp, seg.y / lp, seg.z / lp};
+    F3 off = {p.x - start.x, p.y - start.y, p.z - start.z};
+    float along = dot3(off, ax);
+    F3 perp = {off.x - along * ax.x, off.y - along * ax.y, off.z - along * ax.z};
+    float a = 1.0f - dot3(perp, perp) / r2;
+    if (a <= 0.0f) return 0.0f;
+    float half = radius * sqrtf(a);
+    float lo = fmaxf(-along, -half);
+    float hi = fminf(lp - along, half);
+    if (hi <= lo) return 0.0f;
+    if (solid) return (hi - lo) / lp;
+    float u = lo / half, v = hi / half;
+    float integral = (v - u) - (2.0f / 3.0f) * (v * v * v - u * u * u) + 0.2f * (v * v * v * v * v - u * u * u * u * u);
+    return fminf(fmaxf(a * a * half / lp * integral, 0.0f), 1.0f);
+}
+
+struct SrcDev {
+    int count;
+    int single_solid;
+    F3 center, start, jet;
+    float radius, coupling;
+    float table[128];
+};
+
+inline SrcDev make_src(const FfxSources* s) {
+    SrcDev r;
+    r.count = s ? s->count : -1;
+    r.single_solid = s ? s->single_solid_profile : 0;
+    r.center = {s ? s->single_center[0] : 0.f, s ? s->single_center[1] : 0.f, s ? s->single_center[2] : 0.f};
+    r.start = {s ? s->single_start[0] : 0.f, s ? s->single_start[1] : 0.f, s ? s->single_start[2] : 0.f};
+    r.jet = {s ? s->single_jet[0] : 0.f, s ? s->single_jet[1] : 0.f, s ? s->single_jet[2] : 0.f};
+    r.radius = s ? s->single_radius : 1.f;
+    r.coupling = s ? s->single_coupling : 0.f;
+    for (int i = 0; i < 128; ++i) r.table[i] = s ? s->table[i] : 0.f;
+    return r;
+}
+
+__device__ __forceinline__ float table_weight(const SrcDev& s, int i, F3 p) {
+    const float* row = s.table + 16 * i;
+    F3 c = {row[0], row[1], row[2]}, st = {row[4], row[5], row[6]};
+    return emission_weight(p, c, st, row[3], row[14] > 0.5f);
+}
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ float finite_abs(float v) {
+    return isfinite(v) ? fabsf(v) : 3.4e38f;
+}
+// Non-negative floats order like their bit patterns.
+__device__ __forceinline__ void atomic_max_nonneg(float* addr, float v) {
+    atomicMax(reinterpret_cast<unsigned int*>(addr), __float_as_uint(v));
+}
+__device__ __forceinline__ float warp_max(float v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
+    return v;
+}
+// Block-wide max then one atomic per block (blockDim.x multiple of 32, <= 1024).
+__device__ __forceinline__ void block_max_to(float* out, float v) {
+    __shared__ float part[32];
+    v = warp_max(v);
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    if (lane == 0) part[wid] = v;
+    __syncthreads();
+    if (wid == 0) {
+        int nw = (blockDim.x + 31) >> 5;
+        float m = lane < nw ? part[lane] : 0.f;
+        m = warp_max(m);
+        if (lane == 0 && m > 0.f) atomic_max_nonneg(out, m);
+    }
+}
+
+}  // namespace ffx

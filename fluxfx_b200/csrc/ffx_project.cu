@@ -1,0 +1,799 @@
+// Projection kernels: walls, divergence, gradient (fused cell-centric passes),
+// Jacobi, geometric multigrid operators, aggregation multigrid operators and
+// the FP64 direct coarse solve.
+//
+// The fused cell-centric passes give each thread one cell: it evaluates the
+// six faces of that cell, writes its three lower faces (and the upper face on
+// the far domain boundary), and forms the divergence from the six values, so
+// a face pass and the divergence that reads its result are one kernel and
+// one read of every face.
+#include "ffx_host.cuh"
+
+namespace ffx {
+namespace {
+
+constexpr int kThreads = 256;
+
+// Value after a round trip through storage type T.
+template <typename T>
+__device__ __forceinline__ float rt(float v);
+template <>
+__device__ __forceinline__ float rt<float>(float v) { return v; }
+template <>
+__device__ __forceinline__ float rt<__nv_bfloat16>(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
+
+__device__ __forceinline__ void cell_of(int64_t i, int nx, int ny, int& x, int& y, int& z) {
+    x = (int)(i % nx);
+    int64_t r = i / nx;
+    y = (int)(r % ny);
+    z = (int)(r / ny);
+}
+
+// ------------------------------------------------------ walls + divergence
+// pressure_walls.glsl + pressure_divergence.glsl. DIV = false: walls only.
+template <typename T, bool MASK, bool WRITE_FACES, bool DIV>
+__global__ void __launch_bounds__(kThreads) walls_div_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                            T* ou, T* ov, T* ow, float* div) {
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, d.nx, d.ny, x, y, z);
+    int64_t iu = (int64_t)x + (int64_t)(d.nx + 1) * ((int64_t)y + (int64_t)d.ny * z);
+    int64_t iv = (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)(d.ny + 1) * z);
+    int64_t iw = i;
+    int64_t su = 1, sv = d.nx, sw = (int64_t)d.nx * d.ny;
+    // lower / upper face values after the wall condition
+    auto bounded = [&](const T* f, int64_t idx, int c, int nf, int fx, int fy, int fz, int axis) -> float {
+        bool wall = c == 0 || c == nf - 1;
+        if (MASK) wall = wall || solid_face(d, solid, fx, fy, fz, axis);
+        return wall ? 0.f : Store<T>::ld(f, idx);
+    };
+    float ul = bounded(F.u, iu, x, d.nx + 1, x, y, z, 0);
+    float vl = bounded(F.v, iv, y, d.ny + 1, x, y, z, 1);
+    float wl = bounded(F.w, iw, z, d.nz + 1, x, y, z, 2);
+    if (WRITE_FACES) {
+        Store<T>::st(ou, iu, ul);
+        Store<T>::st(ov, iv, vl);
+        Store<T>::st(ow, iw, wl);
+    }
+    float uu = 0.f, vu = 0.f, wu = 0.f;
+    bool need_upper = DIV || WRITE_FACES;
+    if (need_upper) {
+        if (DIV || x == d.nx - 1) uu = bounded(F.u, iu + su, x + 1, d.nx + 1, x + 1, y, z, 0);
+        if (DIV || y == d.ny - 1) vu = bounded(F.v, iv + sv, y + 1, d.ny + 1, x, y + 1, z, 1);
+        if (DIV || z == d.nz - 1) wu = bounded(F.w, iw + sw, z + 1, d.nz + 1, x, y, z + 1, 2);
+    }
+    if (WRITE_FACES) {
+        if (x == d.nx - 1) Store<T>::st(ou, iu + su, uu);
+        if (y == d.ny - 1) Store<T>::st(ov, iv + sv, vu);
+        if (z == d.nz - 1) Store<T>::st(ow, iw + sw, wu);
+    }
+    if (DIV) {
+        float dv = (uu - ul) * d.inv[0] + (vu - vl) * d.inv[1] + (wu - wl) * d.inv[2];
+        if (MASK && __ldg(solid + i)) dv = 0.f;
+        div[i] = dv;
+    }
+}
+
+// Plain divergence of stored faces (pressure_divergence.glsl).
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(kThreads) divergence_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                             float* div) {
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (MASK && __ldg(solid + i)) { div[i] = 0.f; return; }
+    int x, y, z;
+    cell_of(i, d.nx, d.ny, x, y, z);
+    int64_t iu = (int64_t)x + (int64_t)(d.nx + 1) * ((int64_t)y + (int64_t)d.ny * z);
+    int64_t iv = (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)(d.ny + 1) * z);
+    int64_t sz = (int64_t)d.nx * d.ny;
+    div[i] = (Store<T>::ld(F.u, iu + 1) - Store<T>::ld(F.u, iu)) * d.inv[0] +
+             (Store<T>::ld(F.v, iv + d.nx) - Store<T>::ld(F.v, iv)) * d.inv[1] +
+             (Store<T>::ld(F.w, i + sz) - Store<T>::ld(F.w, i)) * d.inv[2];
+}
+
+// ------------------------------------------------- gradient + divergence
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(kThreads) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                           const float* __restrict__ p, float dt, T* ou, T* ov,
+                                                           T* ow, float* div, float* maxima) {
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float mx[3] = {0.f, 0.f, 0.f};
+    if (i < n) {
+        int x, y, z;
+        cell_of(i, d.nx, d.ny, x, y, z);
+        int64_t iu = (int64_t)x + (int64_t)(d.nx + 1) * ((int64_t)y + (int64_t)d.ny * z);
+        int64_t iv = (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)(d.ny + 1) * z);
+        int64_t iw = i;
+        int64_t sy = d.nx, sz = (int64_t)d.nx * d.ny;
+        float pc = __ldg(p + i);
+        // face value on axis `a` at face coordinate (fx, fy, fz); the face lies
+        // between cells c_lo = face - e_a and c_hi = face.
+        auto face_out = [&](const T* f, int64_t idx, int c, int nf, int fx, int fy, int fz, int axis, float phi,
+                            float plo) -> float {
+            bool open = c > 0 && c < nf - 1;
+            if (MASK) open = open && !solid_face(d, solid, fx, fy, fz, axis);
+            if (!open) return 0.f;
+            float gr = (phi - plo) * d.inv[axis];
+            return Store<T>::ld(f, idx) - dt * gr;
+        };
+        float p_xm = x > 0 ? __ldg(p + i - 1) : 0.f, p_xp = x + 1 < d.nx ? __ldg(p + i + 1) : 0.f;
+        float p_ym = y > 0 ? __ldg(p + i - sy) : 0.f, p_yp = y + 1 < d.ny ? __ldg(p + i + sy) : 0.f;
+        float p_zm = z > 0 ? __ldg(p + i - sz) : 0.f, p_zp = z + 1 < d.nz ? __ldg(p + i + sz) : 0.f;
+        float ul = rt<T>(face_out(F.u, iu, x, d.nx + 1, x, y, z, 0, pc, p_xm));
+        float vl = rt<T>(face_out(F.v, iv, y, d.ny + 1, x, y, z, 1, pc, p_ym));
+        float wl = rt<T>(face_out(F.w, iw, z, d.nz + 1, x, y, z, 2, pc, p_zm));
+        float uu = rt<T>(face_out(F.u, iu + 1, x + 1, d.nx + 1, x + 1, y, z, 0, p_xp, pc));
+        float vu = rt<T>(face_out(F.v, iv + d.nx, y + 1, d.ny + 1, x, y + 1, z, 1, p_yp, pc));
+        float wu = rt<T>(face_out(F.w, iw + sz, z + 1, d.nz + 1, x, y, z + 1, 2, p_zp, pc));
+        Store<T>::st(ou, iu, ul);
+        Store<T>::st(ov, iv, vl);
+        Store<T>::st(ow, iw, wl);
+        mx[0] = finite_abs(ul); mx[1] = finite_abs(vl); mx[2] = finite_abs(wl);
+        if (x == d.nx - 1) { Store<T>::st(ou, iu + 1, uu); mx[0] = fmaxf(mx[0], finite_abs(uu)); }
+        if (y == d.ny - 1) { Store<T>::st(ov, iv + d.nx, vu); mx[1] = fmaxf(mx[1], finite_abs(vu)); }
+        if (z == d.nz - 1) { Store<T>::st(ow, iw + sz, wu); mx[2] = fmaxf(mx[2], finite_abs(wu)); }
+        if (div) {
+            float dv = (uu - ul) * d.inv[0] + (vu - vl) * d.inv[1] + (wu - wl) * d.inv[2];
+            if (MASK && __ldg(solid + i)) dv = 0.f;
+            div[i] = dv;
+        }
+    }
+    if (maxima) {
+        for (int a = 0; a < 3; ++a) {
+            block_max_to(maxima + a, mx[a]);
+            __syncthreads();
+        }
+    }
+}
+
+// ---------------------------------------------------------------- Jacobi
+struct Lvl {
+    int nx, ny, nz;
+    float w[3];   // inv*inv per axis (FP32 product, as pressure_jacobi.glsl forms it)
+};
+
+inline Lvl make_lvl(const int32_t n[3], const float inv[3]) {
+    Lvl L;
+    L.nx = n[0]; L.ny = n[1]; L.nz = n[2];
+    for (int a = 0; a < 3; ++a) L.w[a] = inv[a] * inv[a];
+    return L;
+}
+
+// pressure_jacobi.glsl:1-34
+template <bool MASK>
+__global__ void __launch_bounds__(kThreads) jacobi_kernel(Lvl L, const uint8_t* __restrict__ solid,
+                                                         const float* __restrict__ p, const float* __restrict__ rhs,
+                                                         float dt, float omega, float* out) {
+    int64_t n = (int64_t)L.nx * L.ny * L.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    if (MASK && __ldg(solid + i)) { out[i] = 0.f; return; }
+    int c[3];
+    cell_of(i, L.nx, L.ny, c[0], c[1], c[2]);
+    int size[3] = {L.nx, L.ny, L.nz};
+    int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+    float nb = 0.f, diag = 0.f;
+    for (int a = 0; a < 3; ++a) {
+        float w = L.w[a];
+        bool lower = c[a] > 0, upper = c[a] + 1 < size[a];
+        if (MASK) {
+            lower = lower && !__ldg(solid + i - stride[a]);
+            upper = upper && !__ldg(solid + i + stride[a]);
+        }
+        if (lower) { nb = nb + w * __ldg(p + i - stride[a]); diag = diag + w; }
+        if (upper) { nb = nb + w * __ldg(p + i + stride[a]); diag = diag + w; }
+    }
+    if (diag == 0.f) { out[i] = 0.f; return; }
+    float cand = (nb - __ldg(rhs + i) / dt) / diag;
+    float old = __ldg(p + i);
+    out[i] = old * (1.f - omega) + cand * omega;
+}
+
+__global__ void scale_kernel(int64_t n, const float* in, float f, float* out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = in[i] * f;
+}
+
+// ---------------------------------------------------- geometric multigrid
+// Laplacian term of mg_residual.glsl at cell (x, y, z), index i.
+__device__ __forceinline__ float neumann_lap(const Lvl& L, const float* __restrict__ p, int64_t i, int x, int y,
+                                             int z) {
+    float c = __ldg(p + i);
+    float lap = 0.f;
+    int cc[3] = {x, y, z}, size[3] = {L.nx, L.ny, L.nz};
+    int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+    for (int a = 0; a < 3; ++a) {
+        float w = L.w[a];
+        if (cc[a] > 0) lap = lap + w * (__ldg(p + i - stride[a]) - c);
+        if (cc[a] + 1 < size[a]) lap = lap + w * (__ldg(p + i + stride[a]) - c);
+    }
+    return lap;
+}
+
+__global__ void __launch_bounds__(kThreads) mg_residual_kernel(Lvl L, const float* __restrict__ p,
+                                                              const float* __restrict__ rhs, float dt, float* r) {
+    int64_t n = (int64_t)L.nx * L.ny * L.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, L.nx, L.ny, x, y, z);
+    r[i] = __ldg(rhs + i) / dt - neumann_lap(L, p, i, x, y, z);
+}
+
+__global__ void __launch_bounds__(kThreads) mg_residual_max_kernel(Lvl L, const float* __restrict__ p,
+                                                                  const float* __restrict__ rhs, float dt,
+                                                                  float* out) {
+    int64_t n = (int64_t)L.nx * L.ny * L.nz;
+    float m = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        cell_of(i, L.nx, L.ny, x, y, z);
+        m = fmaxf(m, finite_abs(__ldg(rhs + i) / dt - neumann_lap(L, p, i, x, y, z)));
+    }
+    block_max_to(out, m);
+}
+
+// mg_restrict.glsl: coarse cell c averages fine cells 2c + {0,1}^3 (z, y, x order).
+__global__ void __launch_bounds__(kThreads) mg_restrict_kernel(int fx, int fy, int fz, const float* __restrict__ f,
+                                                              float* c) {
+    int cx = fx / 2, cy = fy / 2, cz = fz / 2;
+    int64_t n = (int64_t)cx * cy * cz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, cx, cy, x, y, z);
+    float v = 0.f;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx)
+                v = v + __ldg(f + (2 * x + dx) + (int64_t)fx * ((2 * y + dy) + (int64_t)fy * (2 * z + dz)));
+    c[i] = v / 8.0f;
+}
+
+__global__ void __launch_bounds__(kThreads) mg_residual_restrict_kernel(Lvl L, const float* __restrict__ p,
+                                                                       const float* __restrict__ rhs, float dt,
+                                                                       float* c) {
+    int cx = L.nx / 2, cy = L.ny / 2, cz = L.nz / 2;
+    int64_t n = (int64_t)cx * cy * cz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, cx, cy, x, y, z);
+    float v = 0.f;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+                int64_t fi = X + (int64_t)L.nx * (Y + (int64_t)L.ny * Z);
+                v = v + (__ldg(rhs + fi) / dt - neumann_lap(L, p, fi, X, Y, Z));
+            }
+    c[i] = v / 8.0f;
+}
+
+// mg_prolong.glsl: cell-centred trilinear interpolation, clamped at the edges.
+__global__ void __launch_bounds__(kThreads) mg_prolong_kernel(int nx, int ny, int nz, const float* __restrict__ p,
+                                                             const float* __restrict__ coarse, float* out) {
+    int64_t n = (int64_t)nx * ny * nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int c[3];
+    cell_of(i, nx, ny, c[0], c[1], c[2]);
+    int cs[3] = {nx / 2, ny / 2, nz / 2};
+    int b[3];
+    float fr[3];
+    for (int a = 0; a < 3; ++a) {
+        float q = ((float)c[a] + 0.5f) * 0.5f - 0.5f;
+        float fb = floorf(q);
+        fr[a] = q - fb;
+        b[a] = (int)fb;
+    }
+    float v = 0.f;
+    for (int oz = 0; oz < 2; ++oz) {
+        float wz = oz ? fr[2] : 1.f - fr[2];
+        int iz = min(max(b[2] + oz, 0), cs[2] - 1);
+        for (int oy = 0; oy < 2; ++oy) {
+            float wy = oy ? fr[1] : 1.f - fr[1];
+            int iy = min(max(b[1] + oy, 0), cs[1] - 1);
+            for (int ox = 0; ox < 2; ++ox) {
+                float wx = ox ? fr[0] : 1.f - fr[0];
+                int ix = min(max(b[0] + ox, 0), cs[0] - 1);
+                v = v + wx * wy * wz * __ldg(coarse + ix + (int64_t)cs[0] * (iy + (int64_t)cs[1] * iz));
+            }
+        }
+    }
+    out[i] = __ldg(p + i) + v;
+}
+
+// Dense FP64 mat-vec, one warp per row (coarse_pressure.glsl, solid_mg_direct.glsl).
+__global__ void direct_kernel(int n, const double* __restrict__ inv, const float* __restrict__ rhs, float dt,
+                              float* p) {
+    int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
+    if (warp >= n) return;
+    const double* row = inv + (int64_t)warp * n;
+    double s = 0.0;
+    for (int j = lane; j < n; j += 32) s += row[j] * (double)rhs[j];
+    for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+    if (lane == 0) p[warp] = (float)(s / (double)dt);
+}
+
+// ------------------------------------------------- aggregation multigrid
+struct GLvl {
+    int nx, ny, nz;
+    const float4* edges;     // NULL: derive from the mask
+    const uint8_t* solid;
+    float w[3];
+};
+
+inline GLvl make_glvl(const FfxGraphLevel* lv) {
+    GLvl g;
+    g.nx = lv->nx; g.ny = lv->ny; g.nz = lv->nz;
+    g.edges = reinterpret_cast<const float4*>(lv->edges);
+    g.solid = lv->solid;
+    for (int a = 0; a < 3; ++a) g.w[a] = lv->w[a];
+    return g;
+}
+
+__device__ __forceinline__ bool g_fluid(const GLvl& g, int64_t i) { return __ldg(g.solid + i) == 0; }
+
+// Record (+x, +y, +z, active) of cell i = (x, y, z)  (solid_hierarchy.py:16-25 for level 0).
+__device__ __forceinline__ float4 g_edge(const GLvl& g, int64_t i, int x, int y, int z) {
+    if (g.edges) return __ldg(g.edges + i);
+    float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (!g_fluid(g, i)) return e;
+    e.w = 1.f;
+    if (x + 1 < g.nx && g_fluid(g, i + 1)) e.x = g.w[0];
+    if (y + 1 < g.ny && g_fluid(g, i + g.nx)) e.y = g.w[1];
+    if (z + 1 < g.nz && g_fluid(g, i + (int64_t)g.nx * g.ny)) e.z = g.w[2];
+    return e;
+}
+
+__device__ __forceinline__ float comp4(const float4& e, int a) { return a == 0 ? e.x : (a == 1 ? e.y : e.z); }
+
+// Conductance of the edge between cell i and its +a neighbour.
+__device__ __forceinline__ float g_w_up(const GLvl& g, int64_t i, int x, int y, int z, int a) {
+    if (g.edges) return comp4(__ldg(g.edges + i), a);
+    int64_t s = a == 0 ? 1 : (a == 1 ? g.nx : (int64_t)g.nx * g.ny);
+    return (g_fluid(g, i) && g_fluid(g, i + s)) ? g.w[a] : 0.f;
+}
+
+// solid_mg_operator.glsl: diagonal and neighbour sums; `pv(j)` supplies p at j.
+template <typename PV>
+__device__ __forceinline__ void graph_terms(const GLvl& g, int64_t i, int x, int y, int z, PV pv, float& diag,
+                                            float& nb) {
+    diag = 0.f;
+    nb = 0.f;
+    int c[3] = {x, y, z}, size[3] = {g.nx, g.ny, g.nz};
+    int64_t stride[3] = {1, g.nx, (int64_t)g.nx * g.ny};
+    float4 here = g.edges ? __ldg(g.edges + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int a = 0; a < 3; ++a) {
+        if (c[a] > 0) {
+            int lc[3] = {x, y, z};
+            lc[a] -= 1;
+            float w = g_w_up(g, i - stride[a], lc[0], lc[1], lc[2], a);
+            diag = diag + w;
+            nb = nb + w * pv(i - stride[a], lc[0], lc[1], lc[2]);
+        }
+        if (c[a] + 1 < size[a]) {
+            float w = g.edges ? comp4(here, a) : g_w_up(g, i, x, y, z, a);
+            diag = diag + w;
+            int uc[3] = {x, y, z};
+            uc[a] += 1;
+            nb = nb + w * pv(i + stride[a], uc[0], uc[1], uc[2]);
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kThreads) graph_smooth_kernel(GLvl g, const float* __restrict__ p,
+                                                               const float* __restrict__ rhs, float omega,
+                                                               float* out) {
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, g.nx, g.ny, x, y, z);
+    float diag, nb;
+    graph_terms(g, i, x, y, z, [&](int64_t j, int, int, int) { return __ldg(p + j); }, diag, nb);
+    out[i] = diag > 0.f ? __ldg(p + i) * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
+}
+
+__device__ __forceinline__ float graph_res(const GLvl& g, const float* __restrict__ p, const float* __restrict__ rhs,
+                                           int64_t i, int x, int y, int z) {
+    float diag, nb;
+    graph_terms(g, i, x, y, z, [&](int64_t j, int, int, int) { return __ldg(p + j); }, diag, nb);
+    return diag > 0.f ? (__ldg(rhs + i) - nb) + diag * __ldg(p + i) : 0.f;
+}
+
+__global__ void __launch_bounds__(kThreads) graph_residual_kernel(GLvl g, const float* __restrict__ p,
+                                                                 const float* __restrict__ rhs, float* r) {
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, g.nx, g.ny, x, y, z);
+    r[i] = graph_res(g, p, rhs, i, x, y, z);
+}
+
+__global__ void __launch_bounds__(kThreads) graph_residual_max_kernel(GLvl g, const float* __restrict__ p,
+                                                                     const float* __restrict__ rhs, float* out) {
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    float m = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        int x, y, z;
+        cell_of(i, g.nx, g.ny, x, y, z);
+        m = fmaxf(m, finite_abs(graph_res(g, p, rhs, i, x, y, z)));
+    }
+    block_max_to(out, m);
+}
+
+__global__ void __launch_bounds__(kThreads) graph_residual_restrict_kernel(GLvl g, const float* __restrict__ p,
+                                                                          const float* __restrict__ rhs, float* c) {
+    int cx = g.nx / 2, cy = g.ny / 2, cz = g.nz / 2;
+    int64_t n = (int64_t)cx * cy * cz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, cx, cy, x, y, z);
+    float v = 0.f;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx) {
+                int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+                int64_t fi = X + (int64_t)g.nx * (Y + (int64_t)g.ny * Z);
+                v = v + graph_res(g, p, rhs, fi, X, Y, Z);
+            }
+    c[i] = v / 8.0f;
+}
+
+__device__ __forceinline__ bool g_active(const GLvl& g, int64_t i) {
+    return g.edges ? __ldg(g.edges + i).w > 0.f : g_fluid(g, i);
+}
+
+// solid_mg_prolong.glsl
+__device__ __forceinline__ float prolonged(const GLvl& g, const float* __restrict__ p,
+                                           const float* __restrict__ coarse, int64_t i, int x, int y, int z) {
+    if (!g_active(g, i)) return 0.f;
+    int cx = g.nx / 2, cy = g.ny / 2;
+    return __ldg(p + i) + __ldg(coarse + (x / 2) + (int64_t)cx * ((y / 2) + (int64_t)cy * (z / 2)));
+}
+
+__global__ void __launch_bounds__(kThreads) graph_prolong_kernel(GLvl g, const float* __restrict__ p,
+                                                                const float* __restrict__ coarse, float* out) {
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, g.nx, g.ny, x, y, z);
+    out[i] = prolonged(g, p, coarse, i, x, y, z);
+}
+
+__global__ void __launch_bounds__(kThreads) graph_prolong_smooth_kernel(GLvl g, const float* __restrict__ p,
+                                                                       const float* __restrict__ coarse,
+                                                                       const float* __restrict__ rhs, float omega,
+                                                                       float* out) {
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, g.nx, g.ny, x, y, z);
+    float diag, nb;
+    graph_terms(g, i, x, y, z, [&](int64_t j, int jx, int jy, int jz) { return prolonged(g, p, coarse, j, jx, jy, jz); },
+                diag, nb);
+    float pc = prolonged(g, p, coarse, i, x, y, z);
+    out[i] = diag > 0.f ? pc * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
+}
+
+// physics/solid_hierarchy.py:27-53 for one coarse cell.
+__global__ void __launch_bounds__(kThreads) graph_coarsen_kernel(GLvl g, float4* coarse, int* disconnected) {
+    int cx = g.nx / 2, cy = g.ny / 2, cz = g.nz / 2;
+    int64_t n = (int64_t)cx * cy * cz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, cx, cy, x, y, z);
+    float4 rec[8];
+    unsigned active = 0;
+    for (int j = 0; j < 8; ++j) {
+        int X = 2 * x + (j & 1), Y = 2 * y + ((j >> 1) & 1), Z = 2 * z + ((j >> 2) & 1);
+        int64_t fi = X + (int64_t)g.nx * (Y + (int64_t)g.ny * Z);
+        rec[j] = g_edge(g, fi, X, Y, Z);
+        if (rec[j].w > 0.f) active |= 1u << j;
+    }
+    if (active) {
+        unsigned seen = active & (~active + 1u);   // lowest active child
+        for (int it = 0; it < 8; ++it) {
+            unsigned grow = seen;
+            for (int j = 0; j < 8; ++j) {
+                if (!(seen >> j & 1u)) continue;
+                for (int a = 0; a < 3; ++a) {
+                    int k = j ^ (1 << a);
+                    int lower = (j >> a & 1) ? k : j;
+                    if ((active >> k & 1u) && comp4(rec[lower], a) > 0.f) grow |= 1u << k;
+                }
+            }
+            if (grow == seen) break;
+            seen = grow;
+        }
+        if (seen != active) atomicExch(disconnected, 1);
+    }
+    float4 out;
+    double s[3] = {0.0, 0.0, 0.0};
+    for (int a = 0; a < 3; ++a)
+        for (int j = 0; j < 8; ++j)
+            if (j >> a & 1) s[a] += (double)comp4(rec[j], a);
+    out.x = (float)(s[0] / 8.0);
+    out.y = (float)(s[1] / 8.0);
+    out.z = (float)(s[2] / 8.0);
+    out.w = active ? 1.f : 0.f;
+    coarse[i] = out;
+}
+
+__global__ void graph_level0_kernel(GLvl g, float4* out) {
+    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x, y, z;
+    cell_of(i, g.nx, g.ny, x, y, z);
+    out[i] = g_edge(g, i, x, y, z);
+}
+
+bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s->solid && s->halo); }
+bool has_mask(const FfxSolids* s) { return s && s->solid; }
+
+bool glvl_ok(const FfxGraphLevel* lv) {
+    if (!lv || lv->nx < 1 || lv->ny < 1 || lv->nz < 1) return false;
+    if ((int64_t)lv->nx * lv->ny * lv->nz >= (int64_t(1) << 31)) return false;
+    if (lv->edges) return ((uintptr_t)lv->edges & 15) == 0;
+    return lv->solid != nullptr;
+}
+
+unsigned reduce_blocks(int64_t n) {
+    int64_t b = (n + kThreads - 1) / kThreads;
+    return (unsigned)(b < 148 * 8 ? (b < 1 ? 1 : b) : 148 * 8);
+}
+
+}  // namespace
+}  // namespace ffx
+
+using namespace ffx;
+
+extern "C" {
+
+int ffx_walls(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
+              void* ou, void* ov, void* ow, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && ou && ov && ow,
+                "ffx_walls: invalid arguments");
+    FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_walls: outputs must not alias inputs");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    cudaStream_t st = as_stream(stream);
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        if (has_mask(s)) walls_div_kernel<T, true, true, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            d, s->solid, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
+        else walls_div_kernel<T, false, true, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
+    });
+    return launch_status("walls_kernel");
+}
+
+int ffx_divergence(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
+                   float* div, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && div,
+                "ffx_divergence: invalid arguments");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    cudaStream_t st = as_stream(stream);
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        if (has_mask(s)) divergence_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(d, s->solid, F, div);
+        else divergence_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(d, nullptr, F, div);
+    });
+    return launch_status("divergence_kernel");
+}
+
+int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                         const void* w, void* ou, void* ov, void* ow, float* div, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && ou && ov && ow && div,
+                "ffx_walls_divergence: invalid arguments");
+    FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_walls_divergence: outputs must not alias inputs");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    cudaStream_t st = as_stream(stream);
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        if (has_mask(s)) walls_div_kernel<T, true, true, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            d, s->solid, F, (T*)ou, (T*)ov, (T*)ow, div);
+        else walls_div_kernel<T, false, true, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, div);
+    });
+    return launch_status("walls_divergence_kernel");
+}
+
+int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
+                 const float* pressure, float dt, void* ou, void* ov, void* ow, float* div_after, float* maxima,
+                 void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && pressure && ou && ov && ow,
+                "ffx_gradient: invalid arguments");
+    FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_gradient: outputs must not alias inputs");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    cudaStream_t st = as_stream(stream);
+    if (maxima) {
+        int e = cuda_status(cudaMemsetAsync(maxima, 0, 3 * sizeof(float), st), "ffx_gradient memset");
+        if (e) return e;
+    }
+    FFX_DISPATCH_STORAGE(storage, T, {
+        Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
+        if (has_mask(s)) gradient_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            d, s->solid, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow, div_after, maxima);
+        else gradient_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
+            d, nullptr, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow, div_after, maxima);
+    });
+    return launch_status("gradient_kernel");
+}
+
+int ffx_jacobi(const int32_t n[3], const float inv[3], const uint8_t* solid, const float* p_in, const float* rhs,
+               float dt, float omega, float* p_out, void* stream) {
+    FFX_REQUIRE(shape_ok(n) && inv && p_in && rhs && p_out && p_in != p_out && dt != 0.f,
+                "ffx_jacobi: invalid arguments");
+    Lvl L = make_lvl(n, inv);
+    int64_t cnt = (int64_t)n[0] * n[1] * n[2];
+    cudaStream_t st = as_stream(stream);
+    if (solid) jacobi_kernel<true><<<blocks_for(cnt, kThreads), kThreads, 0, st>>>(L, solid, p_in, rhs, dt, omega, p_out);
+    else jacobi_kernel<false><<<blocks_for(cnt, kThreads), kThreads, 0, st>>>(L, nullptr, p_in, rhs, dt, omega, p_out);
+    return launch_status("jacobi_kernel");
+}
+
+int ffx_scale(int64_t count, const float* in, float factor, float* out, void* stream) {
+    FFX_REQUIRE(count >= 0 && (count == 0 || (in && out)), "ffx_scale: invalid arguments");
+    if (count == 0) return FFX_OK;
+    scale_kernel<<<blocks_for(count, kThreads), kThreads, 0, as_stream(stream)>>>(count, in, factor, out);
+    return launch_status("scale_kernel");
+}
+
+int ffx_mg_residual(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt, float* r,
+                    void* stream) {
+    FFX_REQUIRE(shape_ok(n) && inv && p && rhs && r && dt != 0.f, "ffx_mg_residual: invalid arguments");
+    Lvl L = make_lvl(n, inv);
+    int64_t cnt = (int64_t)n[0] * n[1] * n[2];
+    mg_residual_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(L, p, rhs, dt, r);
+    return launch_status("mg_residual_kernel");
+}
+
+int ffx_mg_restrict(const int32_t fine_n[3], const float* fine, float* coarse, void* stream) {
+    FFX_REQUIRE(shape_ok(fine_n) && fine && coarse && fine_n[0] % 2 == 0 && fine_n[1] % 2 == 0 && fine_n[2] % 2 == 0,
+                "ffx_mg_restrict: invalid arguments (even fine shape required)");
+    int64_t cnt = (int64_t)(fine_n[0] / 2) * (fine_n[1] / 2) * (fine_n[2] / 2);
+    mg_restrict_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(fine_n[0], fine_n[1], fine_n[2],
+                                                                                      fine, coarse);
+    return launch_status("mg_restrict_kernel");
+}
+
+int ffx_mg_residual_restrict(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt,
+                             float* coarse_rhs, void* stream) {
+    FFX_REQUIRE(shape_ok(n) && inv && p && rhs && coarse_rhs && dt != 0.f && n[0] % 2 == 0 && n[1] % 2 == 0 &&
+                n[2] % 2 == 0, "ffx_mg_residual_restrict: invalid arguments");
+    Lvl L = make_lvl(n, inv);
+    int64_t cnt = (int64_t)(n[0] / 2) * (n[1] / 2) * (n[2] / 2);
+    mg_residual_restrict_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(L, p, rhs, dt,
+                                                                                               coarse_rhs);
+    return launch_status("mg_residual_restrict_kernel");
+}
+
+int ffx_mg_prolong(const int32_t fine_n[3], const float* p, const float* coarse, float* p_out, void* stream) {
+    FFX_REQUIRE(shape_ok(fine_n) && p && coarse && p_out && p != p_out && fine_n[0] % 2 == 0 && fine_n[1] % 2 == 0 &&
+                fine_n[2] % 2 == 0, "ffx_mg_prolong: invalid arguments");
+    int64_t cnt = (int64_t)fine_n[0] * fine_n[1] * fine_n[2];
+    mg_prolong_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(fine_n[0], fine_n[1], fine_n[2],
+                                                                                     p, coarse, p_out);
+    return launch_status("mg_prolong_kernel");
+}
+
+int ffx_direct_solve(int32_t n, const double* inverse, const float* rhs, float dt, float* p, void* stream) {
+    FFX_REQUIRE(n >= 1 && n <= 1024 && inverse && rhs && p && rhs != p && dt != 0.f,
+                "ffx_direct_solve: invalid arguments (n in [1, 1024])");
+    int threads = 256;
+    int blocks = (n * 32 + threads - 1) / threads;
+    direct_kernel<<<blocks, threads, 0, as_stream(stream)>>>(n, inverse, rhs, dt, p);
+    return launch_status("direct_kernel");
+}
+
+int ffx_mg_residual_max(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt,
+                        float* out, void* stream) {
+    FFX_REQUIRE(shape_ok(n) && inv && p && rhs && out && dt != 0.f, "ffx_mg_residual_max: invalid arguments");
+    Lvl L = make_lvl(n, inv);
+    int64_t cnt = (int64_t)n[0] * n[1] * n[2];
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), st), "ffx_mg_residual_max memset");
+    if (e) return e;
+    mg_residual_max_kernel<<<reduce_blocks(cnt), kThreads, 0, st>>>(L, p, rhs, dt, out);
+    return launch_status("mg_residual_max_kernel");
+}
+
+int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega, float* p_out,
+                     void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p_in && rhs && p_out && p_in != p_out, "ffx_graph_smooth: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
+    graph_smooth_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p_in, rhs, omega, p_out);
+    return launch_status("graph_smooth_kernel");
+}
+
+int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && rhs && r && r != p, "ffx_graph_residual: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
+    graph_residual_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, rhs, r);
+    return launch_status("graph_residual_kernel");
+}
+
+int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse_rhs,
+                                void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && rhs && coarse_rhs && lv->nx % 2 == 0 && lv->ny % 2 == 0 && lv->nz % 2 == 0,
+                "ffx_graph_residual_restrict: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)(g.nx / 2) * (g.ny / 2) * (g.nz / 2);
+    graph_residual_restrict_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, rhs,
+                                                                                                  coarse_rhs);
+    return launch_status("graph_residual_restrict_kernel");
+}
+
+int ffx_graph_prolong(const FfxGraphLevel* lv, const float* p, const float* coarse, float* p_out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && coarse && p_out && p != p_out && lv->nx % 2 == 0 && lv->ny % 2 == 0 &&
+                lv->nz % 2 == 0, "ffx_graph_prolong: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
+    graph_prolong_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, coarse, p_out);
+    return launch_status("graph_prolong_kernel");
+}
+
+int ffx_graph_prolong_smooth(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                             float omega, float* p_out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && coarse && rhs && p_out && p != p_out && lv->nx % 2 == 0 && lv->ny % 2 == 0 &&
+                lv->nz % 2 == 0, "ffx_graph_prolong_smooth: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
+    graph_prolong_smooth_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, coarse, rhs,
+                                                                                               omega, p_out);
+    return launch_status("graph_prolong_smooth_kernel");
+}
+
+int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && rhs && out, "ffx_graph_residual_max: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), st), "ffx_graph_residual_max memset");
+    if (e) return e;
+    graph_residual_max_kernel<<<reduce_blocks(cnt), kThreads, 0, st>>>(g, p, rhs, out);
+    return launch_status("graph_residual_max_kernel");
+}
+
+int ffx_graph_coarsen(const FfxGraphLevel* fine, float* coarse_edges, int32_t* disconnected, void* stream) {
+    FFX_REQUIRE(glvl_ok(fine) && coarse_edges && disconnected && ((uintptr_t)coarse_edges & 15) == 0 &&
+                fine->nx % 2 == 0 && fine->ny % 2 == 0 && fine->nz % 2 == 0,
+                "ffx_graph_coarsen: invalid arguments (even shape, 16-byte aligned records)");
+    GLvl g = make_glvl(fine);
+    int64_t cnt = (int64_t)(g.nx / 2) * (g.ny / 2) * (g.nz / 2);
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(disconnected, 0, sizeof(int32_t), st), "ffx_graph_coarsen memset");
+    if (e) return e;
+    graph_coarsen_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, st>>>(g, reinterpret_cast<float4*>(coarse_edges),
+                                                                         disconnected);
+    return launch_status("graph_coarsen_kernel");
+}
+
+int ffx_graph_level0_edges(const FfxGraphLevel* lv, float* edges, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && !lv->edges && edges && ((uintptr_t)edges & 15) == 0,
+                "ffx_graph_level0_edges: invalid arguments");
+    GLvl g = make_glvl(lv);
+    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
+    graph_level0_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, reinterpret_cast<float4*>(edges));
+    return launch_status("graph_level0_kernel");
+}
+
+}  // extern "C"

@@ -1,0 +1,287 @@
+// Runtime entry points: error text, device query and probe, seeds, collider
+// masks and reductions.
+#include <cstring>
+
+#include "ffx_host.cuh"
+
+namespace ffx {
+
+std::string& last_error_buffer() {
+    static thread_local std::string buf;
+    return buf;
+}
+
+namespace {
+
+__global__ void probe_kernel(float* out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= 7 * 5 * 3) return;
+    int x = i % 7, y = (i / 7) % 5, z = i / 35;
+    out[i] = (float)(x + 10 * y + 100 * z);
+}
+
+// seed.glsl / temperature_seed.glsl
+template <typename T>
+__global__ void seed_scalar_kernel(Dev d, F3 center, float radius, float scale, int use_scale, T* out) {
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    F3 p = {((float)x + 0.5f) * d.e[0] / d.nf[0], ((float)y + 0.5f) * d.e[1] / d.nf[1],
+            ((float)z + 0.5f) * d.e[2] / d.nf[2]};
+    F3 off = {p.x - center.x, p.y - center.y, p.z - center.z};
+    float w = fmaxf(1.0f - dot3(off, off) / (radius * radius), 0.0f);
+    Store<T>::st(out, i, use_scale ? scale * w * w : w * w);
+}
+
+// mac_seed.glsl (all three components)
+template <typename T>
+__global__ void seed_faces_kernel(Dev d, F3 base, float angular, T* u, T* v, T* w) {
+    int64_t nu = (int64_t)(d.nx + 1) * d.ny * d.nz, nv = (int64_t)d.nx * (d.ny + 1) * d.nz;
+    int64_t nw = (int64_t)d.nx * d.ny * (d.nz + 1);
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int axis;
+    int sx, sy;
+    T* out;
+    if (i < nu) { axis = 0; sx = d.nx + 1; sy = d.ny; out = u; }
+    else if (i < nu + nv) { i -= nu; axis = 1; sx = d.nx; sy = d.ny + 1; out = v; }
+    else if (i < nu + nv + nw) { i -= nu + nv; axis = 2; sx = d.nx; sy = d.ny; out = w; }
+    else return;
+    int x = (int)(i % sx), y = (int)((i / sx) % sy), z = (int)(i / ((int64_t)sx * sy));
+    float ox = axis == 0 ? 0.f : 0.5f, oy = axis == 1 ? 0.f : 0.5f, oz = axis == 2 ? 0.f : 0.5f;
+    float px = ((float)x + ox) * d.e[0] / d.nf[0];
+    float py = ((float)y + oy) * d.e[1] / d.nf[1];
+    float qx = px - 0.5f * d.e[0], qy = py - 0.5f * d.e[1];
+    float val = axis == 0 ? base.x + (-angular * qy) : (axis == 1 ? base.y + angular * qx : base.z);
+    (void)oz;
+    Store<T>::st(out, i, val);
+}
+
+// FP64 voxelisation in the operation order of physics/collision.py:23-37.
+__global__ void raster_kernel(Dev d, double ex, double ey, double ez, int count, const double* __restrict__ rows, uint8_t* solid) {
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    double hx = ex / d.nx, hy = ey / d.ny, hz = ez / d.nz;
+    double px = (x + .5) * hx, py = (y + .5) * hy, pz = (z + .5) * hz;
+    uint8_t inside = 0;
+    for (int c = 0; c < count && !inside; ++c) {
+        const double* r = rows + 13 * c;
+        double q[3];
+        for (int k = 0; k < 3; ++k) {
+            const double* row = r + 4 * k;
+            q[k] = __dadd_rn(__dadd_rn(__dadd_rn(__dmul_rn(row[0], px), __dmul_rn(row[1], py)),
+                                       __dmul_rn(row[2], pz)), row[3]);
+        }
+        if (r[12] < 0.5) {
+            double s = __dadd_rn(__dadd_rn(__dmul_rn(q[0], q[0]), __dmul_rn(q[1], q[1])), __dmul_rn(q[2], q[2]));
+            inside = s <= 1.0;
+        } else {
+            double m = fmax(fmax(fabs(q[0]), fabs(q[1])), fabs(q[2]));
+            inside = m <= 1.0;
+        }
+    }
+    solid[i] = inside;
+}
+
+__global__ void dilate_kernel(Dev d, const uint8_t* __restrict__ solid, uint8_t* halo) {
+    int64_t n = (int64_t)d.nx * d.ny * d.nz;
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    uint8_t any = 0;
+    for (int dz = -1; dz <= 1 && !any; ++dz)
+        for (int dy = -1; dy <= 1 && !any; ++dy)
+            for (int dx = -1; dx <= 1 && !any; ++dx) any = solid_cell(d, solid, x + dx, y + dy, z + dz);
+    halo[i] = any;
+}
+
+template <typename T>
+__global__ void solid_clear_kernel(int64_t n, const uint8_t* __restrict__ solid, const T* in, T* out) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    Store<T>::st(out, i, solid[i] ? 0.f : Store<T>::ld(in, i));
+}
+
+template <typename T>
+__global__ void max_abs_kernel(int64_t n, const T* __restrict__ x, float* out) {
+    float m = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        m = fmaxf(m, finite_abs(Store<T>::ld(x, i)));
+    block_max_to(out, m);
+}
+
+// Deterministic divergence statistics: per-block FP64 partials in a fixed
+// order, then one block combines them in index order.
+constexpr int kStatsThreads = 256;
+constexpr int kStatsBlocks = 1184;   // 8 x 148 SMs
+
+__device__ __forceinline__ double warp_sum(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ double warp_maxd(double v) {
+    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
+    return v;
+}
+
+__global__ void stats_partial_kernel(int64_t n, const float* __restrict__ b, const float* __restrict__ a,
+                                     double* part) {
+    double s[6] = {0, 0, 0, 0, 0, 0};   // b2, a2, max b, max a, sum b, sum a
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        double vb = b[i], va = a[i];
+        s[0] += vb * vb; s[1] += va * va;
+        s[2] = fmax(s[2], fabs(vb)); s[3] = fmax(s[3], fabs(va));
+        s[4] += vb; s[5] += va;
+    }
+    __shared__ double sh[6][kStatsThreads / 32];
+    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    for (int k = 0; k < 6; ++k) {
+        double v = (k == 2 || k == 3) ? warp_maxd(s[k]) : warp_sum(s[k]);
+        if (lane == 0) sh[k][wid] = v;
+    }
+    __syncthreads();
+    if (threadIdx.x < 6) {
+        int k = threadIdx.x;
+        double v = sh[k][0];
+        for (int w = 1; w < kStatsThreads / 32; ++w) v = (k == 2 || k == 3) ? fmax(v, sh[k][w]) : v + sh[k][w];
+        part[(int64_t)blockIdx.x * 6 + k] = v;
+    }
+}
+
+__global__ void stats_final_kernel(int nblocks, const double* part, int64_t n, double* out) {
+    int k = threadIdx.x;
+    if (k >= 6) return;
+    double v = part[k];
+    for (int bidx = 1; bidx < nblocks; ++bidx) {
+        double x = part[(int64_t)bidx * 6 + k];
+        v = (k == 2 || k == 3) ? fmax(v, x) : v + x;
+    }
+    out[k] = v;
+    if (k == 0) { out[6] = (double)n; out[7] = 0.0; }
+}
+
+int stats_blocks(int64_t n) {
+    int64_t b = (n + kStatsThreads - 1) / kStatsThreads;
+    return (int)(b < kStatsBlocks ? (b < 1 ? 1 : b) : kStatsBlocks);
+}
+
+}  // namespace
+}  // namespace ffx
+
+using namespace ffx;
+
+extern "C" {
+
+int ffx_abi_version(void) { return FFX_ABI_VERSION; }
+
+const char* ffx_last_error(void) { return last_error_buffer().c_str(); }
+
+int ffx_device_info(int device, FfxDeviceInfo* out) {
+    FFX_REQUIRE(out, "ffx_device_info: out is NULL");
+    cudaDeviceProp prop;
+    int st = cuda_status(cudaGetDeviceProperties(&prop, device), "cudaGetDeviceProperties");
+    if (st) return st;
+    std::memset(out, 0, sizeof *out);
+    out->device = device;
+    out->sm_count = prop.multiProcessorCount;
+    out->cc_major = prop.major;
+    out->cc_minor = prop.minor;
+    out->total_bytes = (int64_t)prop.totalGlobalMem;
+    std::strncpy(out->name, prop.name, sizeof out->name - 1);
+    return FFX_OK;
+}
+
+int ffx_probe_3d(float* out, void* stream) {
+    FFX_REQUIRE(out, "ffx_probe_3d: out is NULL");
+    probe_kernel<<<1, 128, 0, as_stream(stream)>>>(out);
+    return launch_status("probe_kernel");
+}
+
+int ffx_seed_scalar(const FfxGrid* g, int storage, const float center[3], float radius, float scale,
+                    void* out, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && center && out && radius > 0.f,
+                "ffx_seed_scalar: invalid arguments");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    F3 c = {center[0], center[1], center[2]};
+    FFX_DISPATCH_STORAGE(storage, T,
+        seed_scalar_kernel<T><<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(d, c, radius, scale,
+                                                                                   scale != 1.0f, (T*)out));
+    return launch_status("seed_scalar_kernel");
+}
+
+int ffx_seed_faces(const FfxGrid* g, int storage, const float base[3], float angular, void* u, void* v,
+                   void* w, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && base && u && v && w, "ffx_seed_faces: invalid arguments");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)(g->nx + 1) * g->ny * g->nz + (int64_t)g->nx * (g->ny + 1) * g->nz +
+                (int64_t)g->nx * g->ny * (g->nz + 1);
+    F3 b = {base[0], base[1], base[2]};
+    FFX_DISPATCH_STORAGE(storage, T,
+        seed_faces_kernel<T><<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(d, b, angular, (T*)u, (T*)v,
+                                                                                  (T*)w));
+    return launch_status("seed_faces_kernel");
+}
+
+int ffx_raster_colliders(const FfxGrid* g, const double extent[3], int count, const double* rows13,
+                         uint8_t* solid, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && extent && solid && count >= 0 && count <= 64 && (count == 0 || rows13),
+                "ffx_raster_colliders: invalid arguments");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    raster_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(d, extent[0], extent[1], extent[2], count,
+                                                                          rows13, solid);
+    return launch_status("raster_kernel");
+}
+
+int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && solid && halo && solid != halo, "ffx_dilate_mask: invalid arguments");
+    Dev d = make_dev(*g);
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    dilate_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(d, solid, halo);
+    return launch_status("dilate_kernel");
+}
+
+int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const void* in, void* out,
+                    void* stream) {
+    FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solid && in && out, "ffx_solid_clear: invalid arguments");
+    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    FFX_DISPATCH_STORAGE(storage, T,
+        solid_clear_kernel<T><<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(n, solid, (const T*)in, (T*)out));
+    return launch_status("solid_clear_kernel");
+}
+
+int ffx_max_abs(int64_t count, int storage, const void* x, float* out, void* stream) {
+    FFX_REQUIRE(count >= 0 && storage_ok(storage) && out && (count == 0 || x), "ffx_max_abs: invalid arguments");
+    cudaStream_t s = as_stream(stream);
+    int st = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), s), "ffx_max_abs memset");
+    if (st || count == 0) return st;
+    int64_t b = (count + 255) / 256;
+    unsigned blocks = (unsigned)(b < 148 * 16 ? b : 148 * 16);
+    FFX_DISPATCH_STORAGE(storage, T, max_abs_kernel<T><<<blocks, 256, 0, s>>>(count, (const T*)x, out));
+    return launch_status("max_abs_kernel");
+}
+
+size_t ffx_divergence_stats_workspace(int64_t count) {
+    return (size_t)stats_blocks(count < 1 ? 1 : count) * 6 * sizeof(double);
+}
+
+int ffx_divergence_stats(int64_t count, const float* before, const float* after, double* out, void* workspace,
+                         size_t workspace_bytes, void* stream) {
+    FFX_REQUIRE(count >= 1 && before && after && out, "ffx_divergence_stats: invalid arguments");
+    size_t need = ffx_divergence_stats_workspace(count);
+    FFX_REQUIRE(workspace && workspace_bytes >= need,
+                "ffx_divergence_stats: workspace of %zu bytes required, %zu given", need, workspace_bytes);
+    FFX_REQUIRE(((uintptr_t)workspace & 7) == 0, "ffx_divergence_stats: workspace must be 8-byte aligned");
+    int nb = stats_blocks(count);
+    cudaStream_t s = as_stream(stream);
+    stats_partial_kernel<<<nb, kStatsThreads, 0, s>>>(count, before, after, (double*)workspace);
+    int st = launch_status("stats_partial_kernel");
+    if (st) return st;
+    stats_final_kernel<<<1, 32, 0, s>>>(nb, (const double*)workspace, count, out);
+    return launch_status("stats_final_kernel");
+}
+
+}  // extern "C"

@@ -1,0 +1,275 @@
+/*
+ * ffx.h -- C ABI of libffx_core.so, the B200 (sm_100a) kernels of the dense
+ * MAC-grid smoke step.
+ *
+ * Conventions
+ *   - Plain C: no exceptions cross this boundary. Every entry point returns an
+ *     FfxStatus; ffx_last_error() gives a thread-local message for the last
+ *     failure on the calling thread.
+ *   - All buffers are DEVICE pointers owned by the caller (allocated by any
+ *     allocator, e.g. torch). The library allocates nothing and frees nothing.
+ *     Work is enqueued on `stream` (a cudaStream_t passed as void*; NULL is the
+ *     legacy default stream); calls are asynchronous unless stated otherwise.
+ *   - Cell fields are x-fast: index x + nx*(y + ny*z). Face grids are
+ *     (nx+1, ny, nz), (nx, ny+1, nz), (nx, ny, nz+1) in the same order.
+ *   - `storage` selects the element type of velocity/scalar fields:
+ *     FFX_F32 (float) or FFX_BF16 (bfloat16). Arithmetic is always FP32;
+ *     pressure, divergence and multigrid buffers are always float.
+ *   - Colliders are two uint8 cell masks (FfxSolids): `solid` (1 = solid) and
+ *     `halo` (1 = a solid or out-of-domain cell lies in the 3x3x3 block), the
+ *     latter made by ffx_dilate_mask. Both NULL = no colliders.
+ *
+ * Each entry point names the reference interface it replaces
+ * (FluxFX, paths relative to the add-on package `fluxfx/`).
+ */
+#ifndef FFX_H
+#define FFX_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FFX_ABI_VERSION 1
+
+typedef enum FfxStatus {
+    FFX_OK = 0,
+    FFX_ERR_INVALID = 1,       /* bad argument (shape, pointer, range) */
+    FFX_ERR_LAUNCH = 2,        /* kernel launch failed */
+    FFX_ERR_NOT_CONVERGED = 3, /* iterative solve hit its cycle cap */
+    FFX_ERR_TIMEOUT = 4,       /* a bounded device wait gave up */
+    FFX_ERR_CUDA = 5           /* other CUDA runtime error */
+} FfxStatus;
+
+enum { FFX_F32 = 0, FFX_BF16 = 1 };
+
+typedef struct FfxGrid {
+    int32_t nx, ny, nz;   /* cells per axis */
+    float ex, ey, ez;     /* domain extent in metres */
+    float ix, iy, iz;     /* 1/h of divergence and gradient (the reference's
+                             invCell uniform: 1/(extent/n) in FP64, rounded);
+                             0 = derive it from ex..ez */
+} FfxGrid;
+
+typedef struct FfxSolids {
+    const uint8_t* solid; /* nx*ny*nz, 1 = solid cell; NULL = no colliders */
+    const uint8_t* halo;  /* nx*ny*nz dilated mask (ffx_dilate_mask) */
+} FfxSolids;
+
+/* Emitters. count < 0: one swept sphere described by the `single_*` fields
+ * (backend/projected.py:155-159, emission_weight.glsl). count in [0, 8]: rows
+ * of `table`, 16 floats per source in the layout of physics/emission.py:49-58
+ * (center.xyz, radius | start.xyz, coupling | jet.xyz, density_rate |
+ *  heat_rate, target_flag, solid_flag, fuel_rate). */
+typedef struct FfxSources {
+    int32_t count;
+    int32_t single_solid_profile;
+    float single_center[3];
+    float single_start[3];
+    float single_radius;
+    float single_jet[3];
+    float single_coupling;
+    float table[128];
+} FfxSources;
+
+typedef struct FfxDeviceInfo {
+    int32_t device, sm_count, cc_major, cc_minor;
+    int64_t total_bytes;
+    char name[128];
+} FfxDeviceInfo;
+
+/* ------------------------------------------------------------------ runtime */
+int ffx_abi_version(void);
+const char* ffx_last_error(void);
+/* Device capability query; replaces backend/device.py:15-28 (capability gate). */
+int ffx_device_info(int device, FfxDeviceInfo* out);
+/* Writes x + 10y + 100z over a 7x5x3 float buffer; replaces backend/device.py:83-96. */
+int ffx_probe_3d(float* out, void* stream);
+
+/* -------------------------------------------------------------- seeds/masks */
+/* Soft-sphere scalar seed * scale; replaces shaders/seed.glsl, temperature_seed.glsl. */
+int ffx_seed_scalar(const FfxGrid* g, int storage, const float center[3], float radius,
+                    float scale, void* out, void* stream);
+/* Analytic rotation + translation face seed; replaces shaders/mac_seed.glsl. */
+int ffx_seed_faces(const FfxGrid* g, int storage, const float base[3], float angular,
+                   void* u, void* v, void* w, void* stream);
+/* Voxelise `count` colliders (13 doubles each: 3x4 inverse rows, shape 0=sphere
+ * 1=box) at cell centres in FP64 using the FP64 `extent`; replaces backend/collision.py:22-41 +
+ * shaders/solid_mask.glsl, bit-exact with physics/collision.py:35-37. */
+int ffx_raster_colliders(const FfxGrid* g, const double extent[3], int count,
+                         const double* rows13, uint8_t* solid, void* stream);
+/* 3x3x3 dilation with out-of-domain = solid (precomputes solidHalo,
+ * shaders/solid_boundary.glsl:39-44). */
+int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void* stream);
+/* out = solid ? 0 : in; replaces shaders/solid_clear.glsl. */
+int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const void* in,
+                    void* out, void* stream);
+
+/* ---------------------------------------------------------- velocity passes */
+/* MacCormack predictor of all three face components in one launch; replaces
+ * backend/detail.py:27-37 + shaders/transport_face.glsl. */
+int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
+                       const void* u, const void* v, const void* w, float dt,
+                       void* pu, void* pv, void* pw, void* stream);
+/* Velocity transport (SL or MacCormack: corrected != 0, blended by `blend`),
+ * emitter coupling, and -- fused -- buoyancy on W from the previous density and
+ * temperature (NULL to skip) and the wall condition (apply_walls != 0). Replaces
+ * shaders/emitting_advect_velocity.glsl, multi_advect_velocity.glsl,
+ * correct_velocity_fused.glsl, buoyancy.glsl and pressure_walls.glsl as
+ * sequenced by backend/projected.py:150-177. Faces out must not alias faces in. */
+int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage,
+                        const void* u, const void* v, const void* w,
+                        const void* pu, const void* pv, const void* pw,
+                        float dt, int corrected, float blend, const FfxSources* src,
+                        const void* density, const void* temperature, float lift, float weight,
+                        int apply_walls, void* ou, void* ov, void* ow, void* stream);
+/* Plain face self-advection; replaces shaders/mac_advect_velocity.glsl. */
+int ffx_mac_advect_velocity(const FfxGrid* g, int storage, const void* u, const void* v,
+                            const void* w, float dt, void* ou, void* ov, void* ow, void* stream);
+/* w_out = w_in + dt (lift*T - weight*rho), face averaged; replaces shaders/buoyancy.glsl. */
+int ffx_buoyancy(const FfxGrid* g, int storage, const void* w_in, const void* density,
+                 const void* temperature, float dt, float lift, float weight, void* w_out,
+                 void* stream);
+
+/* ------------------------------------------------------------ scalar passes */
+typedef struct FfxScalarChannel {
+    const void* field;      /* current scalar */
+    const void* predictor;  /* MacCormack predictor (or == field) */
+    const void* reverse;    /* MacCormack reverse (or == field) */
+    void* out;
+    float rate, decay;      /* emission rate; exp(-decay dt) */
+    float target;           /* single-emitter form: >= 0 selects TARGET */
+    int32_t channel;        /* table form: 0 density, 1 heat, 2 fuel */
+    int32_t table_target;   /* table form: TARGET for this channel (heat extension) */
+} FfxScalarChannel;
+
+/* Closed (clamp-to-edge / collider-renormalised) semi-Lagrangian transport of
+ * up to 3 scalars sharing one backtrace; dt < 0 gives the MacCormack reverse.
+ * Replaces backend/detail.py:16-25 + shaders/transport_scalar.glsl. */
+int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage,
+                         const void* u, const void* v, const void* w, float dt, int count,
+                         const void* const* in, void* const* out, void* stream);
+/* Final scalar pass for up to 3 channels: MacCormack correction + clamp,
+ * decay, emission. Replaces shaders/closed_advect_scalar.glsl,
+ * multi_advect_scalar.glsl, correct_scalar.glsl (backend/projected.py:185-195).
+ * If maxima != NULL, atomically raises maxima[c] to max|out_c|. */
+int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage,
+                       const void* u, const void* v, const void* w, float dt, int corrected,
+                       const FfxSources* src, int count, const FfxScalarChannel* channels,
+                       float* maxima, void* stream);
+/* P0.2 open-boundary transport in an analytic flow; replaces shaders/advect.glsl. */
+int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt,
+                    const float base[3], float angular, const float center[3], float radius,
+                    float rate, float decay, void* out, void* stream);
+/* P0.3 open-boundary transport by MAC velocity; replaces shaders/mac_advect_density.glsl. */
+int ffx_mac_advect_density(const FfxGrid* g, int storage, const void* u, const void* v,
+                           const void* w, const void* in, float dt, const float center[3],
+                           float radius, float rate, float decay, void* out, void* stream);
+
+/* --------------------------------------------------------------- projection */
+/* Zero normal velocity on box walls and solid faces; replaces
+ * backend/pressure.py:49-51 + shaders/pressure_walls.glsl. */
+int ffx_walls(const FfxGrid* g, const FfxSolids* s, int storage, const void* u,
+              const void* v, const void* w, void* ou, void* ov, void* ow, void* stream);
+/* Cell divergence (0 in solids); replaces shaders/pressure_divergence.glsl. */
+int ffx_divergence(const FfxGrid* g, const FfxSolids* s, int storage, const void* u,
+                   const void* v, const void* w, float* div, void* stream);
+/* Fused walls + divergence in one pass (backend/pressure.py:61-62). */
+int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage,
+                         const void* u, const void* v, const void* w,
+                         void* ou, void* ov, void* ow, float* div, void* stream);
+/* out = bounded - dt grad p on open faces, 0 on walls/solid faces; fused with
+ * the divergence of the result (div_after, may be NULL) and the face maxima
+ * max|u|,|v|,|w| (maxima[0..2], atomically raised, may be NULL). Replaces
+ * backend/pressure.py:77-81 + shaders/pressure_gradient.glsl. */
+int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage,
+                 const void* u, const void* v, const void* w, const float* pressure, float dt,
+                 void* ou, void* ov, void* ow, float* div_after, float* maxima, void* stream);
+/* One weighted-Jacobi sweep of the (masked) Neumann Laplacian on a level of
+ * shape n[3] with 1/h = inv[3]; solid may be NULL. Replaces
+ * shaders/pressure_jacobi.glsl. p_out must not alias p_in. */
+int ffx_jacobi(const int32_t n[3], const float inv[3], const uint8_t* solid,
+               const float* p_in, const float* rhs, float dt, float omega, float* p_out,
+               void* stream);
+/* out[i] = in[i] * factor; replaces shaders/pressure_scale.glsl. */
+int ffx_scale(int64_t count, const float* in, float factor, float* out, void* stream);
+
+/* ------------------------------------------------- geometric multigrid (MG) */
+/* r = rhs/dt - L p; replaces shaders/mg_residual.glsl. */
+int ffx_mg_residual(const int32_t n[3], const float inv[3], const float* p, const float* rhs,
+                    float dt, float* r, void* stream);
+/* 2x2x2 average onto the coarse grid n/2; replaces shaders/mg_restrict.glsl. */
+int ffx_mg_restrict(const int32_t fine_n[3], const float* fine, float* coarse, void* stream);
+/* Fused residual + restriction (the fine residual is never stored). */
+int ffx_mg_residual_restrict(const int32_t n[3], const float inv[3], const float* p,
+                             const float* rhs, float dt, float* coarse_rhs, void* stream);
+/* p_out = p + trilinear(coarse); replaces shaders/mg_prolong.glsl. */
+int ffx_mg_prolong(const int32_t fine_n[3], const float* p, const float* coarse, float* p_out,
+                   void* stream);
+/* p = (inverse . rhs) / dt with an FP64 n x n pseudoinverse, FP64 accumulation;
+ * replaces shaders/coarse_pressure.glsl (4^3) and shaders/solid_mg_direct.glsl
+ * (dt = 1). n <= 1024. */
+int ffx_direct_solve(int32_t n, const double* inverse, const float* rhs, float dt, float* p,
+                     void* stream);
+/* max|rhs/dt - L p| raised into *out (zeroed by the call). */
+int ffx_mg_residual_max(const int32_t n[3], const float inv[3], const float* p,
+                        const float* rhs, float dt, float* out, void* stream);
+
+/* ------------------------------------- collider (aggregation) multigrid */
+/* A level of the graph Laplacian. Level 0 derives its conductances from the
+ * solid mask (edges == NULL): w[a] between two fluid cells, 0 otherwise. Coarse
+ * levels carry explicit float4 (+x, +y, +z conductance, active) records. */
+typedef struct FfxGraphLevel {
+    int32_t nx, ny, nz;
+    const float* edges;     /* 4 floats per cell, or NULL for level 0 */
+    const uint8_t* solid;   /* level-0 mask when edges == NULL */
+    float w[3];             /* level-0 conductances (n/extent)^2 */
+} FfxGraphLevel;
+
+/* omega-Jacobi on the graph Laplacian; replaces shaders/solid_mg_smooth.glsl
+ * (omega = 2/3 there). p_out must not alias p_in. */
+int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rhs,
+                     float omega, float* p_out, void* stream);
+/* r = rhs - L p on active cells; replaces shaders/solid_mg_residual.glsl. */
+int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r,
+                       void* stream);
+/* Fused residual + 2x2x2 average restriction (solid_multigrid.py:56-59). */
+int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs,
+                                float* coarse_rhs, void* stream);
+/* p_out = active ? p + coarse[c/2] : 0; replaces shaders/solid_mg_prolong.glsl. */
+int ffx_graph_prolong(const FfxGraphLevel* lv, const float* p, const float* coarse,
+                      float* p_out, void* stream);
+/* Fused prolongation + one smoothing sweep (the prolonged field is formed on the
+ * fly for the 7-point stencil and never stored). */
+int ffx_graph_prolong_smooth(const FfxGraphLevel* lv, const float* p, const float* coarse,
+                             const float* rhs, float omega, float* p_out, void* stream);
+/* max|rhs - L p| over active cells raised into *out (zeroed by the call). */
+int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs,
+                           float* out, void* stream);
+/* One Galerkin aggregation level (physics/solid_hierarchy.py:27-53): coarse
+ * edges = boundary sums / 8, active = any active child. *disconnected (int32,
+ * zeroed by the call) becomes nonzero if any aggregate joins children that are
+ * not connected inside it; the caller then discards the level. */
+int ffx_graph_coarsen(const FfxGraphLevel* fine, float* coarse_edges, int32_t* disconnected,
+                      void* stream);
+/* Materialise level-0 records (4 floats per cell) from the mask. */
+int ffx_graph_level0_edges(const FfxGraphLevel* lv, float* edges, void* stream);
+
+/* --------------------------------------------------------------- reductions */
+/* max|x| with NaN/Inf -> 3.4e38 into *out (zeroed by the call); replaces the
+ * shaders/max_reduce.glsl chains of backend/timestep.py:24-33. */
+int ffx_max_abs(int64_t count, int storage, const void* x, float* out, void* stream);
+/* Divergence statistics (physics/pressure.py:70-80) of two float fields:
+ * out[0..7] = sum(b^2), sum(a^2), max|b|, max|a|, sum(b), sum(a), n, 0 in FP64,
+ * deterministic (fixed-order two-pass reduction). Needs `workspace` of
+ * ffx_divergence_stats_workspace(count) bytes. */
+size_t ffx_divergence_stats_workspace(int64_t count);
+int ffx_divergence_stats(int64_t count, const float* before, const float* after,
+                         double* out, void* workspace, size_t workspace_bytes, void* stream);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FFX_H */
