@@ -290,7 +290,7 @@ def main():
     ap.add_argument('--size', type=int, default=256)
     ap.add_argument('--storage', default='FP32', choices=('FP32', 'BF16'))
     ap.add_argument('--seed', type=int, default=0)
-    ap.add_argument('--cpu-sample", type=int, default=64)
+    ap.add_argument('--cpu-sample', type=int, default=64)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     args = ap.parse_args()
     if args.impl == 'reference':
