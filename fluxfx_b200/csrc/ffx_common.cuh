@@ -171,9 +171,11 @@ __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __re
 // Any solid (or out-of-domain) cell in the 3x3x3 block around p, read from the
 // precomputed dilated mask (solid_boundary.glsl:39-44).
 __device__ __forceinline__ bool solid_halo(const Dev& d, const uint8_t* __restrict__ halo, F3 p) {
-    int cx = (int)floorf(p.x / d.e[0] * d.nf[0]);
-    int cy = (int)floorf(p.y / d.e[1] * d.nf[1]);
-    int cz = (int)floorf(p.z / d.e[2] * d.nf[2]);
+    // Clamp before the integer conversion so far-away (or non-finite) points
+    // land outside the grid, i.e. count as solid.
+    int cx = (int)fmaxf(fminf(floorf(p.x / d.e[0] * d.nf[0]), 1.0e9f), -1.0e9f);
+    int cy = (int)fmaxf(fminf(floorf(p.y / d.e[1] * d.nf[1]), 1.0e9f), -1.0e9f);
+    int cz = (int)fmaxf(fminf(floorf(p.z / d.e[2] * d.nf[2]), 1.0e9f), -1.0e9f);
     if (cx < 0 || cy < 0 || cz < 0 || cx >= d.nx || cy >= d.ny || cz >= d.nz) return true;
     return __ldg(halo + cidx(d, cx, cy, cz)) != 0;
 }
