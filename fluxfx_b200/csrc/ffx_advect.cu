@@ -3,10 +3,10 @@
 // pass, and the P0.2/P0.3 open-boundary forms.
 //
 // One thread per output sample. Face passes cover all three face grids in one
-// launch (a linear index over U, then V, then W). Gathers go through the
-// read-only path; the 8-corner stencils of neighbouring threads overlap, so
-// the L1/L2 hit rate is high and HBM traffic stays close to one read of each
-// field per pass.
+// launch (blockIdx.z enumerates axis and z; 32 x 8 threads over x and y).
+// Gathers go through the read-only path; the 8-corner stencils of
+// neighbouring threads overlap, so the L1/L2 hit rate is high and HBM traffic
+// stays close to one read of each field per pass.
 #include "ffx_host.cuh"
 
 namespace ffx {
@@ -20,26 +20,23 @@ __device__ __forceinline__ int floor_int(float v) {
 
 struct FaceIdx {
     int axis, x, y, z, sx, sy, sz;
-    int64_t i;
+    int i;
 };
 
-__device__ __forceinline__ bool decode_face(const Dev& d, int64_t g, FaceIdx& f) {
-    int64_t nu = (int64_t)(d.nx + 1) * d.ny * d.nz, nv = (int64_t)d.nx * (d.ny + 1) * d.nz;
-    int64_t nw = (int64_t)d.nx * d.ny * (d.nz + 1);
-    if (g < nu) { f.axis = 0; f.sx = d.nx + 1; f.sy = d.ny; f.sz = d.nz; }
-    else if (g < nu + nv) { g -= nu; f.axis = 1; f.sx = d.nx; f.sy = d.ny + 1; f.sz = d.nz; }
-    else if (g < nu + nv + nw) { g -= nu + nv; f.axis = 2; f.sx = d.nx; f.sy = d.ny; f.sz = d.nz + 1; }
-    else return false;
-    f.i = g;
-    f.x = (int)(g % f.sx);
-    int64_t r = g / f.sx;
-    f.y = (int)(r % f.sy);
-    f.z = (int)(r / f.sy);
+// Face of the launch thread (face_grid geometry): blockIdx.z = axis*(nz+1) + z.
+__device__ __forceinline__ bool face_coords(const Dev& d, FaceIdx& f) {
+    const int nz1 = d.nz + 1;
+    const int zz = blockIdx.z;
+    f.axis = zz >= 2 * nz1 ? 2 : (zz >= nz1 ? 1 : 0);
+    f.z = zz - f.axis * nz1;
+    f.sx = d.nx + (f.axis == 0);
+    f.sy = d.ny + (f.axis == 1);
+    f.sz = d.nz + (f.axis == 2);
+    f.x = blockIdx.x * kBX + threadIdx.x;
+    f.y = blockIdx.y * kBY + threadIdx.y;
+    if (f.x >= f.sx || f.y >= f.sy || f.z >= f.sz) return false;
+    f.i = f.x + f.sx * (f.y + f.sy * f.z);
     return true;
-}
-
-__host__ __device__ __forceinline__ int64_t total_faces(const Dev& d) {
-    return (int64_t)(d.nx + 1) * d.ny * d.nz + (int64_t)d.nx * (d.ny + 1) * d.nz + (int64_t)d.nx * d.ny * (d.nz + 1);
 }
 
 // Midpoint backtrace p -> departure (transport_face.glsl:8-17 and the same
@@ -75,7 +72,7 @@ __device__ __forceinline__ float sample_closed(const Dev& d, const uint8_t* soli
                 float wy = oy ? fy : 1.f - fy;
                 for (int ox = 0; ox < 2; ++ox) {
                     float wx = ox ? fx : 1.f - fx;
-                    int64_t c = cidx(d, xs[ox], ys[oy], zs[oz]);
+                    int c = cidx(d, xs[ox], ys[oy], zs[oz]);
                     if (__ldg(solid + c)) continue;
                     float weight = wx * wy * wz;
                     value = value + weight * Store<T>::ld(f, c);
@@ -109,7 +106,7 @@ template <typename T, bool MASK>
 __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const uint8_t* __restrict__ solid,
                                                                   Faces<T> F, float dt, T* pu, T* pv, T* pw) {
     FaceIdx f;
-    if (!decode_face(d, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, f)) return;
+    if (!face_coords(d, f)) return;
     T* out = f.axis == 0 ? pu : (f.axis == 1 ? pv : pw);
     if (MASK && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
         Store<T>::st(out, f.i, 0.f);
@@ -144,7 +141,7 @@ template <typename T, bool MASK>
 __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
     const Dev& d = P.d;
     FaceIdx f;
-    if (!decode_face(d, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, f)) return;
+    if (!face_coords(d, f)) return;
     const int axis = f.axis;
     const float dt = P.dt;
     bool blocked = MASK && solid_face(d, P.solid, f.x, f.y, f.z, axis);
@@ -181,7 +178,7 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
                                        arr.z / d.h[2] - off[2]);
                 float val = Store<T>::ld(pred, f.i) + 0.5f * (Store<T>::ld(orig, f.i) - pa);
                 int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
-                int64_t sxy = (int64_t)f.sx * f.sy;
+                int sxy = f.sx * f.sy;
                 float lo = 0.f, hi = 0.f;
                 bool first = true;
                 for (int oz = 0; oz < 2; ++oz)
@@ -189,7 +186,7 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
                         for (int ox = 0; ox < 2; ++ox) {
                             int cx = min(max(bx + ox, 0), f.sx - 1), cy = min(max(by + oy, 0), f.sy - 1);
                             int cz = min(max(bz + oz, 0), f.sz - 1);
-                            float v = Store<T>::ld(orig, (int64_t)cz * sxy + (int64_t)cy * f.sx + cx);
+                            float v = Store<T>::ld(orig, cz * sxy + cy * f.sx + cx);
                             if (first) { lo = hi = v; first = false; }
                             else { lo = fminf(lo, v); hi = fmaxf(hi, v); }
                         }
@@ -218,7 +215,7 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
     if (axis == 2 && P.density) {
         // buoyancy.glsl:1-14 with the previous step's scalars
         int below = min(max(f.z - 1, 0), d.nz - 1), above = min(max(f.z, 0), d.nz - 1);
-        int64_t ib = cidx(d, f.x, f.y, below), ia = cidx(d, f.x, f.y, above);
+        int ib = cidx(d, f.x, f.y, below), ia = cidx(d, f.x, f.y, above);
         float rho = 0.5f * (Store<T>::ld(P.density, ib) + Store<T>::ld(P.density, ia));
         float theta = 0.5f * (Store<T>::ld(P.temperature, ib) + Store<T>::ld(P.temperature, ia));
         float a = P.lift * theta - P.weight * rho;
@@ -237,7 +234,7 @@ template <typename T>
 __global__ void __launch_bounds__(kThreads) mac_advect_velocity_kernel(Dev d, Faces<T> F, float dt, T* ou, T* ov,
                                                                        T* ow) {
     FaceIdx f;
-    if (!decode_face(d, (int64_t)blockIdx.x * blockDim.x + threadIdx.x, f)) return;
+    if (!face_coords(d, f)) return;
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.e[0] / d.nf[0], ((float)f.y + oy) * d.e[1] / d.nf[1],
             ((float)f.z + oz) * d.e[2] / d.nf[2]};
@@ -251,12 +248,11 @@ __global__ void __launch_bounds__(kThreads) mac_advect_velocity_kernel(Dev d, Fa
 template <typename T>
 __global__ void buoyancy_kernel(Dev d, const T* w_in, const T* density, const T* temperature, float dt, float lift,
                                 float weight, T* w_out) {
-    int64_t n = (int64_t)d.nx * d.ny * (d.nz + 1);
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    int x, y, z;
+    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    const int i = cidx(d, x, y, z);
     int below = min(max(z - 1, 0), d.nz - 1), above = min(max(z, 0), d.nz - 1);
-    int64_t ib = cidx(d, x, y, below), ia = cidx(d, x, y, above);
+    int ib = cidx(d, x, y, below), ia = cidx(d, x, y, above);
     float rho = 0.5f * (Store<T>::ld(density, ib) + Store<T>::ld(density, ia));
     float theta = 0.5f * (Store<T>::ld(temperature, ib) + Store<T>::ld(temperature, ia));
     float a = lift * theta - weight * rho;
@@ -278,10 +274,9 @@ struct ScalarXport {
 template <typename T, bool MASK>
 __global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
     const Dev& d = P.d;
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    int x, y, z;
+    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    const int i = cidx(d, x, y, z);
     if (MASK && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, 0.f);
         return;
@@ -320,11 +315,10 @@ struct ScalarFinal {
 template <typename T, bool MASK>
 __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
     const Dev& d = P.d;
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    int x, y, z;
     float vmax[3] = {0.f, 0.f, 0.f};
-    if (i < n) {
-        int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    if (cell_coords(d.nx, d.ny, x, y, z)) {
+        const int i = cidx(d, x, y, z);
         if (MASK && __ldg(P.solid + i)) {
             for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
         } else {
@@ -427,10 +421,9 @@ struct OpenParams {
 template <typename T>
 __global__ void advect_open_kernel(OpenParams P, const T* in, T* out) {
     const Dev& d = P.d;
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    int x, y, z;
+    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    const int i = cidx(d, x, y, z);
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v = analytic_velocity(d, p, P.base, P.angular);
     float s = 0.5f * P.dt;
@@ -447,10 +440,9 @@ __global__ void advect_open_kernel(OpenParams P, const T* in, T* out) {
 template <typename T>
 __global__ void mac_advect_density_kernel(OpenParams P, Faces<T> F, const T* in, T* out) {
     const Dev& d = P.d;
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    int x = (int)(i % d.nx), y = (int)((i / d.nx) % d.ny), z = (int)(i / ((int64_t)d.nx * d.ny));
+    int x, y, z;
+    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    const int i = cidx(d, x, y, z);
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = velocity_at(d, F, p);
     F3 dep = backtrace<T, false>(d, F, nullptr, p, v0, P.dt);
@@ -477,13 +469,13 @@ int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const 
                 "ffx_face_predictor: invalid arguments");
     FFX_REQUIRE(pu != u && pv != v && pw != w, "ffx_face_predictor: outputs must not alias inputs");
     Dev d = make_dev(*g);
-    unsigned blocks = blocks_for(total_faces(d), kThreads);
+    dim3 blocks = face_grid(d.nx, d.ny, d.nz), threads = cell_block();
     cudaStream_t st = as_stream(stream);
     const uint8_t* solid = has_mask(s) ? s->solid : nullptr;
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (solid) face_predictor_kernel<T, true><<<blocks, kThreads, 0, st>>>(d, solid, F, dt, (T*)pu, (T*)pv, (T*)pw);
-        else face_predictor_kernel<T, false><<<blocks, kThreads, 0, st>>>(d, nullptr, F, dt, (T*)pu, (T*)pv, (T*)pw);
+        if (solid) face_predictor_kernel<T, true><<<blocks, threads, 0, st>>>(d, solid, F, dt, (T*)pu, (T*)pv, (T*)pw);
+        else face_predictor_kernel<T, false><<<blocks, threads, 0, st>>>(d, nullptr, F, dt, (T*)pu, (T*)pv, (T*)pw);
     });
     return launch_status("face_predictor_kernel");
 }
@@ -501,7 +493,7 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const
                 "must both be given for buoyancy");
     FFX_REQUIRE(blend >= 0.f && blend <= 1.f, "ffx_advect_velocity: blend must lie in [0, 1]");
     Dev d = make_dev(*g);
-    unsigned blocks = blocks_for(total_faces(d), kThreads);
+    dim3 blocks = face_grid(d.nx, d.ny, d.nz), threads = cell_block();
     cudaStream_t st = as_stream(stream);
     FFX_DISPATCH_STORAGE(storage, T, {
         VelParams<T> P;
@@ -521,8 +513,8 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const
         P.out[0] = (T*)ou; P.out[1] = (T*)ov; P.out[2] = (T*)ow;
         P.src = make_src(src);
         if (!src) P.src.count = 0;
-        if (P.solid) advect_velocity_kernel<T, true><<<blocks, kThreads, 0, st>>>(P);
-        else advect_velocity_kernel<T, false><<<blocks, kThreads, 0, st>>>(P);
+        if (P.solid) advect_velocity_kernel<T, true><<<blocks, threads, 0, st>>>(P);
+        else advect_velocity_kernel<T, false><<<blocks, threads, 0, st>>>(P);
     });
     return launch_status("advect_velocity_kernel");
 }
@@ -532,10 +524,10 @@ int ffx_mac_advect_velocity(const FfxGrid* g, int storage, const void* u, const 
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && u && v && w && ou && ov && ow && ou != u && ov != v && ow != w,
                 "ffx_mac_advect_velocity: invalid arguments");
     Dev d = make_dev(*g);
-    unsigned blocks = blocks_for(total_faces(d), kThreads);
+    dim3 blocks = face_grid(d.nx, d.ny, d.nz), threads = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        mac_advect_velocity_kernel<T><<<blocks, kThreads, 0, as_stream(stream)>>>(d, F, dt, (T*)ou, (T*)ov, (T*)ow);
+        mac_advect_velocity_kernel<T><<<blocks, threads, 0, as_stream(stream)>>>(d, F, dt, (T*)ou, (T*)ov, (T*)ow);
     });
     return launch_status("mac_advect_velocity_kernel");
 }
@@ -545,9 +537,9 @@ int ffx_buoyancy(const FfxGrid* g, int storage, const void* w_in, const void* de
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && w_in && density && temperature && w_out && w_in != w_out,
                 "ffx_buoyancy: invalid arguments");
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * (g->nz + 1);
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz + 1), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T,
-        buoyancy_kernel<T><<<blocks_for(n, kThreads), kThreads, 0, as_stream(stream)>>>(
+        buoyancy_kernel<T><<<grid, block, 0, as_stream(stream)>>>(
             d, (const T*)w_in, (const T*)density, (const T*)temperature, dt, lift, weight, (T*)w_out));
     return launch_status("buoyancy_kernel");
 }
@@ -559,7 +551,7 @@ int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, cons
     for (int c = 0; c < count; ++c)
         FFX_REQUIRE(in[c] && out[c] && in[c] != out[c], "ffx_scalar_transport: channel %d invalid or aliased", c);
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     cudaStream_t st = as_stream(stream);
     FFX_DISPATCH_STORAGE(storage, T, {
         ScalarXport<T> P;
@@ -572,8 +564,8 @@ int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, cons
             P.in[c] = c < count ? (const T*)in[c] : nullptr;
             P.out[c] = c < count ? (T*)out[c] : nullptr;
         }
-        if (P.solid) scalar_transport_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
-        else scalar_transport_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
+        if (P.solid) scalar_transport_kernel<T, true><<<grid, block, 0, st>>>(P);
+        else scalar_transport_kernel<T, false><<<grid, block, 0, st>>>(P);
     });
     return launch_status("scalar_transport_kernel");
 }
@@ -589,7 +581,7 @@ int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const 
         FFX_REQUIRE(!corrected || (C.predictor && C.reverse), "ffx_advect_scalars: channel %d lacks predictor", c);
     }
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     cudaStream_t st = as_stream(stream);
     if (maxima) {
         int e = cuda_status(cudaMemsetAsync(maxima, 0, sizeof(float) * count, st), "ffx_advect_scalars memset");
@@ -622,8 +614,8 @@ int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const 
         }
         P.maxima = maxima;
         P.src = make_src(src);
-        if (P.solid) advect_scalars_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
-        else advect_scalars_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(P);
+        if (P.solid) advect_scalars_kernel<T, true><<<grid, block, 0, st>>>(P);
+        else advect_scalars_kernel<T, false><<<grid, block, 0, st>>>(P);
     });
     return launch_status("advect_scalars_kernel");
 }
@@ -637,9 +629,9 @@ int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt, con
     P.dt = dt; P.angular = angular; P.radius = radius; P.rate = rate; P.decay = decay;
     P.base = {base[0], base[1], base[2]};
     P.center = {center[0], center[1], center[2]};
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T,
-        advect_open_kernel<T><<<blocks_for(n, kThreads), kThreads, 0, as_stream(stream)>>>(P, (const T*)in, (T*)out));
+        advect_open_kernel<T><<<grid, block, 0, as_stream(stream)>>>(P, (const T*)in, (T*)out));
     return launch_status("advect_open_kernel");
 }
 
@@ -653,10 +645,10 @@ int ffx_mac_advect_density(const FfxGrid* g, int storage, const void* u, const v
     P.dt = dt; P.angular = 0.f; P.radius = radius; P.rate = rate; P.decay = decay;
     P.base = {0.f, 0.f, 0.f};
     P.center = {center[0], center[1], center[2]};
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        mac_advect_density_kernel<T><<<blocks_for(n, kThreads), kThreads, 0, as_stream(stream)>>>(P, F, (const T*)in,
+        mac_advect_density_kernel<T><<<grid, block, 0, as_stream(stream)>>>(P, F, (const T*)in,
                                                                                                 (T*)out);
     });
     return launch_status("mac_advect_density_kernel");

@@ -54,8 +54,31 @@ inline Dev make_dev(const FfxGrid& g) {
     return d;
 }
 
-__device__ __forceinline__ int64_t cidx(const Dev& d, int x, int y, int z) {
-    return (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)d.ny * z);
+// Every field has fewer than 2^31 elements (checked at the entry points), so
+// 32-bit index arithmetic is exact.
+__device__ __forceinline__ int cidx(const Dev& d, int x, int y, int z) {
+    return x + d.nx * (y + d.ny * z);
+}
+
+// ------------------------------------------------------------ launch geometry
+// Cell-centric kernels run 32 x 8 thread blocks over (x, y) and one z slice per
+// blockIdx.z: coordinates come straight from the launch, with no integer
+// division, and each warp covers 32 consecutive x (coalesced rows).
+constexpr int kBX = 32, kBY = 8;
+inline dim3 cell_block() { return dim3(kBX, kBY, 1); }
+inline dim3 cell_grid(int nx, int ny, int nz) {
+    return dim3((unsigned)((nx + kBX - 1) / kBX), (unsigned)((ny + kBY - 1) / kBY), (unsigned)nz);
+}
+__device__ __forceinline__ bool cell_coords(int nx, int ny, int& x, int& y, int& z) {
+    x = blockIdx.x * kBX + threadIdx.x;
+    y = blockIdx.y * kBY + threadIdx.y;
+    z = blockIdx.z;
+    return x < nx && y < ny;
+}
+// Face kernels: blockIdx.z runs over (axis, z) for the three face grids, each
+// padded to the (nx+1, ny+1, nz+1) box.
+inline dim3 face_grid(int nx, int ny, int nz) {
+    return dim3((unsigned)((nx + 1 + kBX - 1) / kBX), (unsigned)((ny + 1 + kBY - 1) / kBY), (unsigned)(3 * (nz + 1)));
 }
 
 struct F3 { float x, y, z; };
@@ -75,9 +98,9 @@ __device__ __forceinline__ float sample_face(const T* __restrict__ f, int sx, in
     float fx = qx - bx, fy = qy - by, fz = qz - bz;
     int ix = (int)bx, iy = (int)by, iz = (int)bz;
     int ix1 = min(ix + 1, sx - 1), iy1 = min(iy + 1, sy - 1), iz1 = min(iz + 1, sz - 1);
-    int64_t sxy = (int64_t)sx * sy;
-    int64_t r00 = (int64_t)iz * sxy + (int64_t)iy * sx, r01 = (int64_t)iz * sxy + (int64_t)iy1 * sx;
-    int64_t r10 = (int64_t)iz1 * sxy + (int64_t)iy * sx, r11 = (int64_t)iz1 * sxy + (int64_t)iy1 * sx;
+    int sxy = sx * sy;
+    int r00 = iz * sxy + iy * sx, r01 = iz * sxy + iy1 * sx;
+    int r10 = iz1 * sxy + iy * sx, r11 = iz1 * sxy + iy1 * sx;
     float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
     float v = 0.f;
     v = v + gx * gy * gz * Store<T>::ld(f, r00 + ix);
@@ -263,15 +286,16 @@ __device__ __forceinline__ float warp_max(float v) {
     for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
     return v;
 }
-// Block-wide max then one atomic per block (blockDim.x multiple of 32, <= 1024).
+// Block-wide max then one atomic per block (block size a multiple of 32, <= 1024).
 __device__ __forceinline__ void block_max_to(float* out, float v) {
     __shared__ float part[32];
     v = warp_max(v);
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
+    int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    int lane = tid & 31, wid = tid >> 5;
     if (lane == 0) part[wid] = v;
     __syncthreads();
     if (wid == 0) {
-        int nw = (blockDim.x + 31) >> 5;
+        int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
         float m = lane < nw ? part[lane] : 0.f;
         m = warp_max(m);
         if (lane == 0 && m > 0.f) atomic_max_nonneg(out, m);

@@ -7,12 +7,14 @@
 // the far domain boundary), and forms the divergence from the six values, so
 // a face pass and the divergence that reads its result are one kernel and
 // one read of every face.
+//
+// All stencil kernels use the 32 x 8 (x, y) block / z-per-blockIdx.z launch of
+// ffx_common.cuh; reductions stride over z with a bounded number of blocks so
+// each block issues one atomic.
 #include "ffx_host.cuh"
 
 namespace ffx {
 namespace {
-
-constexpr int kThreads = 256;
 
 // Value after a round trip through storage type T.
 template <typename T>
@@ -22,29 +24,22 @@ __device__ __forceinline__ float rt<float>(float v) { return v; }
 template <>
 __device__ __forceinline__ float rt<__nv_bfloat16>(float v) { return __bfloat162float(__float2bfloat16_rn(v)); }
 
-__device__ __forceinline__ void cell_of(int64_t i, int nx, int ny, int& x, int& y, int& z) {
-    x = (int)(i % nx);
-    int64_t r = i / nx;
-    y = (int)(r % ny);
-    z = (int)(r / ny);
-}
+// Bounded z extent of reduction grids: (x, y) tiles x this many z blocks.
+inline unsigned reduce_z(int nz) { return (unsigned)(nz < 8 ? nz : 8); }
 
 // ------------------------------------------------------ walls + divergence
-// pressure_walls.glsl + pressure_divergence.glsl. DIV = false: walls only.
-template <typename T, bool MASK, bool WRITE_FACES, bool DIV>
-__global__ void __launch_bounds__(kThreads) walls_div_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
-                                                            T* ou, T* ov, T* ow, float* div) {
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+// pressure_walls.glsl + pressure_divergence.glsl (DIV = false: walls only).
+template <typename T, bool MASK, bool DIV>
+__global__ void __launch_bounds__(256) walls_div_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                       T* ou, T* ov, T* ow, float* div) {
     int x, y, z;
-    cell_of(i, d.nx, d.ny, x, y, z);
-    int64_t iu = (int64_t)x + (int64_t)(d.nx + 1) * ((int64_t)y + (int64_t)d.ny * z);
-    int64_t iv = (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)(d.ny + 1) * z);
-    int64_t iw = i;
-    int64_t su = 1, sv = d.nx, sw = (int64_t)d.nx * d.ny;
-    // lower / upper face values after the wall condition
-    auto bounded = [&](const T* f, int64_t idx, int c, int nf, int fx, int fy, int fz, int axis) -> float {
+    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    const int i = cidx(d, x, y, z);
+    const int iu = x + (d.nx + 1) * (y + d.ny * z);
+    const int iv = x + d.nx * (y + (d.ny + 1) * z);
+    const int iw = i;
+    const int sv = d.nx, sw = d.nx * d.ny;
+    auto bounded = [&](const T* f, int idx, int c, int nf, int fx, int fy, int fz, int axis) -> float {
         bool wall = c == 0 || c == nf - 1;
         if (MASK) wall = wall || solid_face(d, solid, fx, fy, fz, axis);
         return wall ? 0.f : Store<T>::ld(f, idx);
@@ -52,23 +47,16 @@ __global__ void __launch_bounds__(kThreads) walls_div_kernel(Dev d, const uint8_
     float ul = bounded(F.u, iu, x, d.nx + 1, x, y, z, 0);
     float vl = bounded(F.v, iv, y, d.ny + 1, x, y, z, 1);
     float wl = bounded(F.w, iw, z, d.nz + 1, x, y, z, 2);
-    if (WRITE_FACES) {
-        Store<T>::st(ou, iu, ul);
-        Store<T>::st(ov, iv, vl);
-        Store<T>::st(ow, iw, wl);
-    }
+    Store<T>::st(ou, iu, ul);
+    Store<T>::st(ov, iv, vl);
+    Store<T>::st(ow, iw, wl);
     float uu = 0.f, vu = 0.f, wu = 0.f;
-    bool need_upper = DIV || WRITE_FACES;
-    if (need_upper) {
-        if (DIV || x == d.nx - 1) uu = bounded(F.u, iu + su, x + 1, d.nx + 1, x + 1, y, z, 0);
-        if (DIV || y == d.ny - 1) vu = bounded(F.v, iv + sv, y + 1, d.ny + 1, x, y + 1, z, 1);
-        if (DIV || z == d.nz - 1) wu = bounded(F.w, iw + sw, z + 1, d.nz + 1, x, y, z + 1, 2);
-    }
-    if (WRITE_FACES) {
-        if (x == d.nx - 1) Store<T>::st(ou, iu + su, uu);
-        if (y == d.ny - 1) Store<T>::st(ov, iv + sv, vu);
-        if (z == d.nz - 1) Store<T>::st(ow, iw + sw, wu);
-    }
+    if (DIV || x == d.nx - 1) uu = bounded(F.u, iu + 1, x + 1, d.nx + 1, x + 1, y, z, 0);
+    if (DIV || y == d.ny - 1) vu = bounded(F.v, iv + sv, y + 1, d.ny + 1, x, y + 1, z, 1);
+    if (DIV || z == d.nz - 1) wu = bounded(F.w, iw + sw, z + 1, d.nz + 1, x, y, z + 1, 2);
+    if (x == d.nx - 1) Store<T>::st(ou, iu + 1, uu);
+    if (y == d.ny - 1) Store<T>::st(ov, iv + sv, vu);
+    if (z == d.nz - 1) Store<T>::st(ow, iw + sw, wu);
     if (DIV) {
         float dv = (uu - ul) * d.inv[0] + (vu - vl) * d.inv[1] + (wu - wl) * d.inv[2];
         if (MASK && __ldg(solid + i)) dv = 0.f;
@@ -78,17 +66,15 @@ __global__ void __launch_bounds__(kThreads) walls_div_kernel(Dev d, const uint8_
 
 // Plain divergence of stored faces (pressure_divergence.glsl).
 template <typename T, bool MASK>
-__global__ void __launch_bounds__(kThreads) divergence_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
-                                                             float* div) {
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
-    if (MASK && __ldg(solid + i)) { div[i] = 0.f; return; }
+__global__ void __launch_bounds__(256) divergence_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                        float* div) {
     int x, y, z;
-    cell_of(i, d.nx, d.ny, x, y, z);
-    int64_t iu = (int64_t)x + (int64_t)(d.nx + 1) * ((int64_t)y + (int64_t)d.ny * z);
-    int64_t iv = (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)(d.ny + 1) * z);
-    int64_t sz = (int64_t)d.nx * d.ny;
+    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    const int i = cidx(d, x, y, z);
+    if (MASK && __ldg(solid + i)) { div[i] = 0.f; return; }
+    const int iu = x + (d.nx + 1) * (y + d.ny * z);
+    const int iv = x + d.nx * (y + (d.ny + 1) * z);
+    const int sz = d.nx * d.ny;
     div[i] = (Store<T>::ld(F.u, iu + 1) - Store<T>::ld(F.u, iu)) * d.inv[0] +
              (Store<T>::ld(F.v, iv + d.nx) - Store<T>::ld(F.v, iv)) * d.inv[1] +
              (Store<T>::ld(F.w, i + sz) - Store<T>::ld(F.w, i)) * d.inv[2];
@@ -96,23 +82,20 @@ __global__ void __launch_bounds__(kThreads) divergence_kernel(Dev d, const uint8
 
 // ------------------------------------------------- gradient + divergence
 template <typename T, bool MASK>
-__global__ void __launch_bounds__(kThreads) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
-                                                           const float* __restrict__ p, float dt, T* ou, T* ov,
-                                                           T* ow, float* div, float* maxima) {
-    int64_t n = (int64_t)d.nx * d.ny * d.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+__global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                      const float* __restrict__ p, float dt, T* ou, T* ov, T* ow,
+                                                      float* div, float* maxima) {
+    int x, y, z;
     float mx[3] = {0.f, 0.f, 0.f};
-    if (i < n) {
-        int x, y, z;
-        cell_of(i, d.nx, d.ny, x, y, z);
-        int64_t iu = (int64_t)x + (int64_t)(d.nx + 1) * ((int64_t)y + (int64_t)d.ny * z);
-        int64_t iv = (int64_t)x + (int64_t)d.nx * ((int64_t)y + (int64_t)(d.ny + 1) * z);
-        int64_t iw = i;
-        int64_t sy = d.nx, sz = (int64_t)d.nx * d.ny;
+    if (cell_coords(d.nx, d.ny, x, y, z)) {
+        const int i = cidx(d, x, y, z);
+        const int iu = x + (d.nx + 1) * (y + d.ny * z);
+        const int iv = x + d.nx * (y + (d.ny + 1) * z);
+        const int iw = i;
+        const int sy = d.nx, sz = d.nx * d.ny;
         float pc = __ldg(p + i);
-        // face value on axis `a` at face coordinate (fx, fy, fz); the face lies
-        // between cells c_lo = face - e_a and c_hi = face.
-        auto face_out = [&](const T* f, int64_t idx, int c, int nf, int fx, int fy, int fz, int axis, float phi,
+        // face between cells (face - e_axis) and (face); phi / plo are their pressures
+        auto face_out = [&](const T* f, int idx, int c, int nf, int fx, int fy, int fz, int axis, float phi,
                             float plo) -> float {
             bool open = c > 0 && c < nf - 1;
             if (MASK) open = open && !solid_face(d, solid, fx, fy, fz, axis);
@@ -153,7 +136,7 @@ __global__ void __launch_bounds__(kThreads) gradient_kernel(Dev d, const uint8_t
 // ---------------------------------------------------------------- Jacobi
 struct Lvl {
     int nx, ny, nz;
-    float w[3];   // inv*inv per axis (FP32 product, as pressure_jacobi.glsl forms it)
+    float w[3];   // inv*inv per axis (the FP32 product pressure_jacobi.glsl forms)
 };
 
 inline Lvl make_lvl(const int32_t n[3], const float inv[3]) {
@@ -165,18 +148,17 @@ inline Lvl make_lvl(const int32_t n[3], const float inv[3]) {
 
 // pressure_jacobi.glsl:1-34
 template <bool MASK>
-__global__ void __launch_bounds__(kThreads) jacobi_kernel(Lvl L, const uint8_t* __restrict__ solid,
-                                                         const float* __restrict__ p, const float* __restrict__ rhs,
-                                                         float dt, float omega, float* out) {
-    int64_t n = (int64_t)L.nx * L.ny * L.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) jacobi_kernel(Lvl L, const uint8_t* __restrict__ solid,
+                                                    const float* __restrict__ p, const float* __restrict__ rhs,
+                                                    float dt, float omega, float* out) {
+    int x, y, z;
+    if (!cell_coords(L.nx, L.ny, x, y, z)) return;
+    const int i = x + L.nx * (y + L.ny * z);
     if (MASK && __ldg(solid + i)) { out[i] = 0.f; return; }
-    int c[3];
-    cell_of(i, L.nx, L.ny, c[0], c[1], c[2]);
-    int size[3] = {L.nx, L.ny, L.nz};
-    int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+    const int c[3] = {x, y, z}, size[3] = {L.nx, L.ny, L.nz};
+    const int stride[3] = {1, L.nx, L.nx * L.ny};
     float nb = 0.f, diag = 0.f;
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
         float w = L.w[a];
         bool lower = c[a] > 0, upper = c[a] + 1 < size[a];
@@ -200,12 +182,12 @@ __global__ void scale_kernel(int64_t n, const float* in, float f, float* out) {
 
 // ---------------------------------------------------- geometric multigrid
 // Laplacian term of mg_residual.glsl at cell (x, y, z), index i.
-__device__ __forceinline__ float neumann_lap(const Lvl& L, const float* __restrict__ p, int64_t i, int x, int y,
-                                             int z) {
+__device__ __forceinline__ float neumann_lap(const Lvl& L, const float* __restrict__ p, int i, int x, int y, int z) {
     float c = __ldg(p + i);
     float lap = 0.f;
-    int cc[3] = {x, y, z}, size[3] = {L.nx, L.ny, L.nz};
-    int64_t stride[3] = {1, L.nx, (int64_t)L.nx * L.ny};
+    const int cc[3] = {x, y, z}, size[3] = {L.nx, L.ny, L.nz};
+    const int stride[3] = {1, L.nx, L.nx * L.ny};
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
         float w = L.w[a];
         if (cc[a] > 0) lap = lap + w * (__ldg(p + i - stride[a]) - c);
@@ -214,77 +196,70 @@ __device__ __forceinline__ float neumann_lap(const Lvl& L, const float* __restri
     return lap;
 }
 
-__global__ void __launch_bounds__(kThreads) mg_residual_kernel(Lvl L, const float* __restrict__ p,
-                                                              const float* __restrict__ rhs, float dt, float* r) {
-    int64_t n = (int64_t)L.nx * L.ny * L.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) mg_residual_kernel(Lvl L, const float* __restrict__ p,
+                                                         const float* __restrict__ rhs, float dt, float* r) {
     int x, y, z;
-    cell_of(i, L.nx, L.ny, x, y, z);
+    if (!cell_coords(L.nx, L.ny, x, y, z)) return;
+    const int i = x + L.nx * (y + L.ny * z);
     r[i] = __ldg(rhs + i) / dt - neumann_lap(L, p, i, x, y, z);
 }
 
-__global__ void __launch_bounds__(kThreads) mg_residual_max_kernel(Lvl L, const float* __restrict__ p,
-                                                                  const float* __restrict__ rhs, float dt,
-                                                                  float* out) {
-    int64_t n = (int64_t)L.nx * L.ny * L.nz;
+__global__ void __launch_bounds__(256) mg_residual_max_kernel(Lvl L, const float* __restrict__ p,
+                                                             const float* __restrict__ rhs, float dt, float* out) {
+    int x = blockIdx.x * kBX + threadIdx.x, y = blockIdx.y * kBY + threadIdx.y;
     float m = 0.f;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        cell_of(i, L.nx, L.ny, x, y, z);
-        m = fmaxf(m, finite_abs(__ldg(rhs + i) / dt - neumann_lap(L, p, i, x, y, z)));
-    }
+    if (x < L.nx && y < L.ny)
+        for (int z = blockIdx.z; z < L.nz; z += gridDim.z) {
+            const int i = x + L.nx * (y + L.ny * z);
+            m = fmaxf(m, finite_abs(__ldg(rhs + i) / dt - neumann_lap(L, p, i, x, y, z)));
+        }
     block_max_to(out, m);
 }
 
 // mg_restrict.glsl: coarse cell c averages fine cells 2c + {0,1}^3 (z, y, x order).
-__global__ void __launch_bounds__(kThreads) mg_restrict_kernel(int fx, int fy, int fz, const float* __restrict__ f,
-                                                              float* c) {
-    int cx = fx / 2, cy = fy / 2, cz = fz / 2;
-    int64_t n = (int64_t)cx * cy * cz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) mg_restrict_kernel(int fx, int fy, int fz, const float* __restrict__ f,
+                                                         float* c) {
+    const int cx = fx / 2, cy = fy / 2;
     int x, y, z;
-    cell_of(i, cx, cy, x, y, z);
+    if (!cell_coords(cx, cy, x, y, z)) return;
     float v = 0.f;
+#pragma unroll
     for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
         for (int dy = 0; dy < 2; ++dy)
-            for (int dx = 0; dx < 2; ++dx)
-                v = v + __ldg(f + (2 * x + dx) + (int64_t)fx * ((2 * y + dy) + (int64_t)fy * (2 * z + dz)));
-    c[i] = v / 8.0f;
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) v = v + __ldg(f + (2 * x + dx) + fx * ((2 * y + dy) + fy * (2 * z + dz)));
+    c[x + cx * (y + cy * z)] = v / 8.0f;
 }
 
-__global__ void __launch_bounds__(kThreads) mg_residual_restrict_kernel(Lvl L, const float* __restrict__ p,
-                                                                       const float* __restrict__ rhs, float dt,
-                                                                       float* c) {
-    int cx = L.nx / 2, cy = L.ny / 2, cz = L.nz / 2;
-    int64_t n = (int64_t)cx * cy * cz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) mg_residual_restrict_kernel(Lvl L, const float* __restrict__ p,
+                                                                  const float* __restrict__ rhs, float dt, float* c) {
+    const int cx = L.nx / 2, cy = L.ny / 2;
     int x, y, z;
-    cell_of(i, cx, cy, x, y, z);
+    if (!cell_coords(cx, cy, x, y, z)) return;
     float v = 0.f;
+#pragma unroll
     for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
         for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
             for (int dx = 0; dx < 2; ++dx) {
-                int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
-                int64_t fi = X + (int64_t)L.nx * (Y + (int64_t)L.ny * Z);
+                const int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+                const int fi = X + L.nx * (Y + L.ny * Z);
                 v = v + (__ldg(rhs + fi) / dt - neumann_lap(L, p, fi, X, Y, Z));
             }
-    c[i] = v / 8.0f;
+    c[x + cx * (y + cy * z)] = v / 8.0f;
 }
 
 // mg_prolong.glsl: cell-centred trilinear interpolation, clamped at the edges.
-__global__ void __launch_bounds__(kThreads) mg_prolong_kernel(int nx, int ny, int nz, const float* __restrict__ p,
-                                                             const float* __restrict__ coarse, float* out) {
-    int64_t n = (int64_t)nx * ny * nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) mg_prolong_kernel(int nx, int ny, int nz, const float* __restrict__ p,
+                                                        const float* __restrict__ coarse, float* out) {
     int c[3];
-    cell_of(i, nx, ny, c[0], c[1], c[2]);
-    int cs[3] = {nx / 2, ny / 2, nz / 2};
+    if (!cell_coords(nx, ny, c[0], c[1], c[2])) return;
+    const int cs[3] = {nx / 2, ny / 2, nz / 2};
     int b[3];
     float fr[3];
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
         float q = ((float)c[a] + 0.5f) * 0.5f - 0.5f;
         float fb = floorf(q);
@@ -292,19 +267,23 @@ __global__ void __launch_bounds__(kThreads) mg_prolong_kernel(int nx, int ny, in
         b[a] = (int)fb;
     }
     float v = 0.f;
+#pragma unroll
     for (int oz = 0; oz < 2; ++oz) {
         float wz = oz ? fr[2] : 1.f - fr[2];
         int iz = min(max(b[2] + oz, 0), cs[2] - 1);
+#pragma unroll
         for (int oy = 0; oy < 2; ++oy) {
             float wy = oy ? fr[1] : 1.f - fr[1];
             int iy = min(max(b[1] + oy, 0), cs[1] - 1);
+#pragma unroll
             for (int ox = 0; ox < 2; ++ox) {
                 float wx = ox ? fr[0] : 1.f - fr[0];
                 int ix = min(max(b[0] + ox, 0), cs[0] - 1);
-                v = v + wx * wy * wz * __ldg(coarse + ix + (int64_t)cs[0] * (iy + (int64_t)cs[1] * iz));
+                v = v + wx * wy * wz * __ldg(coarse + ix + cs[0] * (iy + cs[1] * iz));
             }
         }
     }
+    const int i = c[0] + nx * (c[1] + ny * c[2]);
     out[i] = __ldg(p + i) + v;
 }
 
@@ -337,169 +316,170 @@ inline GLvl make_glvl(const FfxGraphLevel* lv) {
     return g;
 }
 
-__device__ __forceinline__ bool g_fluid(const GLvl& g, int64_t i) { return __ldg(g.solid + i) == 0; }
+__device__ __forceinline__ bool g_fluid(const GLvl& g, int i) { return __ldg(g.solid + i) == 0; }
+__device__ __forceinline__ float comp4(const float4& e, int a) { return a == 0 ? e.x : (a == 1 ? e.y : e.z); }
 
 // Record (+x, +y, +z, active) of cell i = (x, y, z)  (solid_hierarchy.py:16-25 for level 0).
-__device__ __forceinline__ float4 g_edge(const GLvl& g, int64_t i, int x, int y, int z) {
+__device__ __forceinline__ float4 g_edge(const GLvl& g, int i, int x, int y, int z) {
     if (g.edges) return __ldg(g.edges + i);
     float4 e = make_float4(0.f, 0.f, 0.f, 0.f);
     if (!g_fluid(g, i)) return e;
     e.w = 1.f;
     if (x + 1 < g.nx && g_fluid(g, i + 1)) e.x = g.w[0];
     if (y + 1 < g.ny && g_fluid(g, i + g.nx)) e.y = g.w[1];
-    if (z + 1 < g.nz && g_fluid(g, i + (int64_t)g.nx * g.ny)) e.z = g.w[2];
+    if (z + 1 < g.nz && g_fluid(g, i + g.nx * g.ny)) e.z = g.w[2];
     return e;
 }
 
-__device__ __forceinline__ float comp4(const float4& e, int a) { return a == 0 ? e.x : (a == 1 ? e.y : e.z); }
-
-// Conductance of the edge between cell i and its +a neighbour.
-__device__ __forceinline__ float g_w_up(const GLvl& g, int64_t i, int x, int y, int z, int a) {
-    if (g.edges) return comp4(__ldg(g.edges + i), a);
-    int64_t s = a == 0 ? 1 : (a == 1 ? g.nx : (int64_t)g.nx * g.ny);
-    return (g_fluid(g, i) && g_fluid(g, i + s)) ? g.w[a] : 0.f;
-}
-
-// solid_mg_operator.glsl: diagonal and neighbour sums; `pv(j)` supplies p at j.
+// solid_mg_operator.glsl: diagonal and neighbour sums. `pv(j, x, y, z)` supplies
+// the iterate at cell j. Level 0 (no records) reads each mask byte once.
 template <typename PV>
-__device__ __forceinline__ void graph_terms(const GLvl& g, int64_t i, int x, int y, int z, PV pv, float& diag,
+__device__ __forceinline__ void graph_terms(const GLvl& g, int i, int x, int y, int z, PV pv, float& diag,
                                             float& nb) {
     diag = 0.f;
     nb = 0.f;
-    int c[3] = {x, y, z}, size[3] = {g.nx, g.ny, g.nz};
-    int64_t stride[3] = {1, g.nx, (int64_t)g.nx * g.ny};
-    float4 here = g.edges ? __ldg(g.edges + i) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const int c[3] = {x, y, z}, size[3] = {g.nx, g.ny, g.nz};
+    const int stride[3] = {1, g.nx, g.nx * g.ny};
+    if (g.edges) {
+        const float4 here = __ldg(g.edges + i);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            if (c[a] > 0) {
+                int lc[3] = {x, y, z};
+                lc[a] -= 1;
+                float w = comp4(__ldg(g.edges + i - stride[a]), a);
+                diag = diag + w;
+                nb = nb + w * pv(i - stride[a], lc[0], lc[1], lc[2]);
+            }
+            if (c[a] + 1 < size[a]) {
+                int uc[3] = {x, y, z};
+                uc[a] += 1;
+                float w = comp4(here, a);
+                diag = diag + w;
+                nb = nb + w * pv(i + stride[a], uc[0], uc[1], uc[2]);
+            }
+        }
+        return;
+    }
+    const bool fluid = g_fluid(g, i);
+#pragma unroll
     for (int a = 0; a < 3; ++a) {
         if (c[a] > 0) {
             int lc[3] = {x, y, z};
             lc[a] -= 1;
-            float w = g_w_up(g, i - stride[a], lc[0], lc[1], lc[2], a);
+            float w = (fluid && g_fluid(g, i - stride[a])) ? g.w[a] : 0.f;
             diag = diag + w;
             nb = nb + w * pv(i - stride[a], lc[0], lc[1], lc[2]);
         }
         if (c[a] + 1 < size[a]) {
-            float w = g.edges ? comp4(here, a) : g_w_up(g, i, x, y, z, a);
-            diag = diag + w;
             int uc[3] = {x, y, z};
             uc[a] += 1;
+            float w = (fluid && g_fluid(g, i + stride[a])) ? g.w[a] : 0.f;
+            diag = diag + w;
             nb = nb + w * pv(i + stride[a], uc[0], uc[1], uc[2]);
         }
     }
 }
 
-__global__ void __launch_bounds__(kThreads) graph_smooth_kernel(GLvl g, const float* __restrict__ p,
-                                                               const float* __restrict__ rhs, float omega,
-                                                               float* out) {
-    int64_t n = (int64_t)g.nx * g.ny * g.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_smooth_kernel(GLvl g, const float* __restrict__ p,
+                                                          const float* __restrict__ rhs, float omega, float* out) {
     int x, y, z;
-    cell_of(i, g.nx, g.ny, x, y, z);
+    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    const int i = x + g.nx * (y + g.ny * z);
     float diag, nb;
-    graph_terms(g, i, x, y, z, [&](int64_t j, int, int, int) { return __ldg(p + j); }, diag, nb);
+    graph_terms(g, i, x, y, z, [&](int j, int, int, int) { return __ldg(p + j); }, diag, nb);
     out[i] = diag > 0.f ? __ldg(p + i) * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
 }
 
 __device__ __forceinline__ float graph_res(const GLvl& g, const float* __restrict__ p, const float* __restrict__ rhs,
-                                           int64_t i, int x, int y, int z) {
+                                           int i, int x, int y, int z) {
     float diag, nb;
-    graph_terms(g, i, x, y, z, [&](int64_t j, int, int, int) { return __ldg(p + j); }, diag, nb);
+    graph_terms(g, i, x, y, z, [&](int j, int, int, int) { return __ldg(p + j); }, diag, nb);
     return diag > 0.f ? (__ldg(rhs + i) - nb) + diag * __ldg(p + i) : 0.f;
 }
 
-__global__ void __launch_bounds__(kThreads) graph_residual_kernel(GLvl g, const float* __restrict__ p,
-                                                                 const float* __restrict__ rhs, float* r) {
-    int64_t n = (int64_t)g.nx * g.ny * g.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_residual_kernel(GLvl g, const float* __restrict__ p,
+                                                            const float* __restrict__ rhs, float* r) {
     int x, y, z;
-    cell_of(i, g.nx, g.ny, x, y, z);
+    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    const int i = x + g.nx * (y + g.ny * z);
     r[i] = graph_res(g, p, rhs, i, x, y, z);
 }
 
-__global__ void __launch_bounds__(kThreads) graph_residual_max_kernel(GLvl g, const float* __restrict__ p,
-                                                                     const float* __restrict__ rhs, float* out) {
-    int64_t n = (int64_t)g.nx * g.ny * g.nz;
+__global__ void __launch_bounds__(256) graph_residual_max_kernel(GLvl g, const float* __restrict__ p,
+                                                                const float* __restrict__ rhs, float* out) {
+    int x = blockIdx.x * kBX + threadIdx.x, y = blockIdx.y * kBY + threadIdx.y;
     float m = 0.f;
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        int x, y, z;
-        cell_of(i, g.nx, g.ny, x, y, z);
-        m = fmaxf(m, finite_abs(graph_res(g, p, rhs, i, x, y, z)));
-    }
+    if (x < g.nx && y < g.ny)
+        for (int z = blockIdx.z; z < g.nz; z += gridDim.z) {
+            const int i = x + g.nx * (y + g.ny * z);
+            m = fmaxf(m, finite_abs(graph_res(g, p, rhs, i, x, y, z)));
+        }
     block_max_to(out, m);
 }
 
-__global__ void __launch_bounds__(kThreads) graph_residual_restrict_kernel(GLvl g, const float* __restrict__ p,
-                                                                          const float* __restrict__ rhs, float* c) {
-    int cx = g.nx / 2, cy = g.ny / 2, cz = g.nz / 2;
-    int64_t n = (int64_t)cx * cy * cz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_residual_restrict_kernel(GLvl g, const float* __restrict__ p,
+                                                                     const float* __restrict__ rhs, float* c) {
+    const int cx = g.nx / 2, cy = g.ny / 2;
     int x, y, z;
-    cell_of(i, cx, cy, x, y, z);
+    if (!cell_coords(cx, cy, x, y, z)) return;
     float v = 0.f;
+#pragma unroll
     for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
         for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
             for (int dx = 0; dx < 2; ++dx) {
-                int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
-                int64_t fi = X + (int64_t)g.nx * (Y + (int64_t)g.ny * Z);
-                v = v + graph_res(g, p, rhs, fi, X, Y, Z);
+                const int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+                v = v + graph_res(g, p, rhs, X + g.nx * (Y + g.ny * Z), X, Y, Z);
             }
-    c[i] = v / 8.0f;
+    c[x + cx * (y + cy * z)] = v / 8.0f;
 }
 
-__device__ __forceinline__ bool g_active(const GLvl& g, int64_t i) {
+__device__ __forceinline__ bool g_active(const GLvl& g, int i) {
     return g.edges ? __ldg(g.edges + i).w > 0.f : g_fluid(g, i);
 }
 
 // solid_mg_prolong.glsl
 __device__ __forceinline__ float prolonged(const GLvl& g, const float* __restrict__ p,
-                                           const float* __restrict__ coarse, int64_t i, int x, int y, int z) {
+                                           const float* __restrict__ coarse, int i, int x, int y, int z) {
     if (!g_active(g, i)) return 0.f;
-    int cx = g.nx / 2, cy = g.ny / 2;
-    return __ldg(p + i) + __ldg(coarse + (x / 2) + (int64_t)cx * ((y / 2) + (int64_t)cy * (z / 2)));
+    const int cx = g.nx / 2, cy = g.ny / 2;
+    return __ldg(p + i) + __ldg(coarse + (x >> 1) + cx * ((y >> 1) + cy * (z >> 1)));
 }
 
-__global__ void __launch_bounds__(kThreads) graph_prolong_kernel(GLvl g, const float* __restrict__ p,
-                                                                const float* __restrict__ coarse, float* out) {
-    int64_t n = (int64_t)g.nx * g.ny * g.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_prolong_kernel(GLvl g, const float* __restrict__ p,
+                                                           const float* __restrict__ coarse, float* out) {
     int x, y, z;
-    cell_of(i, g.nx, g.ny, x, y, z);
+    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    const int i = x + g.nx * (y + g.ny * z);
     out[i] = prolonged(g, p, coarse, i, x, y, z);
 }
 
-__global__ void __launch_bounds__(kThreads) graph_prolong_smooth_kernel(GLvl g, const float* __restrict__ p,
-                                                                       const float* __restrict__ coarse,
-                                                                       const float* __restrict__ rhs, float omega,
-                                                                       float* out) {
-    int64_t n = (int64_t)g.nx * g.ny * g.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_prolong_smooth_kernel(GLvl g, const float* __restrict__ p,
+                                                                  const float* __restrict__ coarse,
+                                                                  const float* __restrict__ rhs, float omega,
+                                                                  float* out) {
     int x, y, z;
-    cell_of(i, g.nx, g.ny, x, y, z);
+    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    const int i = x + g.nx * (y + g.ny * z);
     float diag, nb;
-    graph_terms(g, i, x, y, z, [&](int64_t j, int jx, int jy, int jz) { return prolonged(g, p, coarse, j, jx, jy, jz); },
-                diag, nb);
+    graph_terms(g, i, x, y, z,
+                [&](int j, int jx, int jy, int jz) { return prolonged(g, p, coarse, j, jx, jy, jz); }, diag, nb);
     float pc = prolonged(g, p, coarse, i, x, y, z);
     out[i] = diag > 0.f ? pc * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
 }
 
 // physics/solid_hierarchy.py:27-53 for one coarse cell.
-__global__ void __launch_bounds__(kThreads) graph_coarsen_kernel(GLvl g, float4* coarse, int* disconnected) {
-    int cx = g.nx / 2, cy = g.ny / 2, cz = g.nz / 2;
-    int64_t n = (int64_t)cx * cy * cz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_coarsen_kernel(GLvl g, float4* coarse, int* disconnected) {
+    const int cx = g.nx / 2, cy = g.ny / 2;
     int x, y, z;
-    cell_of(i, cx, cy, x, y, z);
+    if (!cell_coords(cx, cy, x, y, z)) return;
     float4 rec[8];
     unsigned active = 0;
     for (int j = 0; j < 8; ++j) {
-        int X = 2 * x + (j & 1), Y = 2 * y + ((j >> 1) & 1), Z = 2 * z + ((j >> 2) & 1);
-        int64_t fi = X + (int64_t)g.nx * (Y + (int64_t)g.ny * Z);
-        rec[j] = g_edge(g, fi, X, Y, Z);
+        const int X = 2 * x + (j & 1), Y = 2 * y + ((j >> 1) & 1), Z = 2 * z + ((j >> 2) & 1);
+        rec[j] = g_edge(g, X + g.nx * (Y + g.ny * Z), X, Y, Z);
         if (rec[j].w > 0.f) active |= 1u << j;
     }
     if (active) {
@@ -509,8 +489,8 @@ __global__ void __launch_bounds__(kThreads) graph_coarsen_kernel(GLvl g, float4*
             for (int j = 0; j < 8; ++j) {
                 if (!(seen >> j & 1u)) continue;
                 for (int a = 0; a < 3; ++a) {
-                    int k = j ^ (1 << a);
-                    int lower = (j >> a & 1) ? k : j;
+                    const int k = j ^ (1 << a);
+                    const int lower = (j >> a & 1) ? k : j;
                     if ((active >> k & 1u) && comp4(rec[lower], a) > 0.f) grow |= 1u << k;
                 }
             }
@@ -519,24 +499,22 @@ __global__ void __launch_bounds__(kThreads) graph_coarsen_kernel(GLvl g, float4*
         }
         if (seen != active) atomicExch(disconnected, 1);
     }
-    float4 out;
     double s[3] = {0.0, 0.0, 0.0};
     for (int a = 0; a < 3; ++a)
         for (int j = 0; j < 8; ++j)
             if (j >> a & 1) s[a] += (double)comp4(rec[j], a);
+    float4 out;
     out.x = (float)(s[0] / 8.0);
     out.y = (float)(s[1] / 8.0);
     out.z = (float)(s[2] / 8.0);
     out.w = active ? 1.f : 0.f;
-    coarse[i] = out;
+    coarse[x + cx * (y + cy * z)] = out;
 }
 
-__global__ void graph_level0_kernel(GLvl g, float4* out) {
-    int64_t n = (int64_t)g.nx * g.ny * g.nz;
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= n) return;
+__global__ void __launch_bounds__(256) graph_level0_kernel(GLvl g, float4* out) {
     int x, y, z;
-    cell_of(i, g.nx, g.ny, x, y, z);
+    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    const int i = x + g.nx * (y + g.ny * z);
     out[i] = g_edge(g, i, x, y, z);
 }
 
@@ -544,16 +522,13 @@ bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s-
 bool has_mask(const FfxSolids* s) { return s && s->solid; }
 
 bool glvl_ok(const FfxGraphLevel* lv) {
-    if (!lv || lv->nx < 1 || lv->ny < 1 || lv->nz < 1) return false;
+    if (!lv || lv->nx < 1 || lv->ny < 1 || lv->nz < 1 || lv->nz > 65535) return false;
     if ((int64_t)lv->nx * lv->ny * lv->nz >= (int64_t(1) << 31)) return false;
     if (lv->edges) return ((uintptr_t)lv->edges & 15) == 0;
     return lv->solid != nullptr;
 }
 
-unsigned reduce_blocks(int64_t n) {
-    int64_t b = (n + kThreads - 1) / kThreads;
-    return (unsigned)(b < 148 * 8 ? (b < 1 ? 1 : b) : 148 * 8);
-}
+bool nz_ok(const int32_t n[3]) { return n[2] <= 65535; }
 
 }  // namespace
 }  // namespace ffx
@@ -568,14 +543,13 @@ int ffx_walls(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, 
                 "ffx_walls: invalid arguments");
     FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_walls: outputs must not alias inputs");
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
     cudaStream_t st = as_stream(stream);
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) walls_div_kernel<T, true, true, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            d, s->solid, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
-        else walls_div_kernel<T, false, true, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
+        if (has_mask(s)) walls_div_kernel<T, true, false><<<grid, block, 0, st>>>(d, s->solid, F, (T*)ou, (T*)ov,
+                                                                                  (T*)ow, nullptr);
+        else walls_div_kernel<T, false, false><<<grid, block, 0, st>>>(d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
     });
     return launch_status("walls_kernel");
 }
@@ -585,12 +559,12 @@ int ffx_divergence(const FfxGrid* g, const FfxSolids* s, int storage, const void
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && div,
                 "ffx_divergence: invalid arguments");
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
     cudaStream_t st = as_stream(stream);
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) divergence_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(d, s->solid, F, div);
-        else divergence_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(d, nullptr, F, div);
+        if (has_mask(s)) divergence_kernel<T, true><<<grid, block, 0, st>>>(d, s->solid, F, div);
+        else divergence_kernel<T, false><<<grid, block, 0, st>>>(d, nullptr, F, div);
     });
     return launch_status("divergence_kernel");
 }
@@ -601,14 +575,13 @@ int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage, cons
                 "ffx_walls_divergence: invalid arguments");
     FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_walls_divergence: outputs must not alias inputs");
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
     cudaStream_t st = as_stream(stream);
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) walls_div_kernel<T, true, true, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            d, s->solid, F, (T*)ou, (T*)ov, (T*)ow, div);
-        else walls_div_kernel<T, false, true, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, div);
+        if (has_mask(s)) walls_div_kernel<T, true, true><<<grid, block, 0, st>>>(d, s->solid, F, (T*)ou, (T*)ov,
+                                                                                 (T*)ow, div);
+        else walls_div_kernel<T, false, true><<<grid, block, 0, st>>>(d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, div);
     });
     return launch_status("walls_divergence_kernel");
 }
@@ -620,76 +593,72 @@ int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* 
                 "ffx_gradient: invalid arguments");
     FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_gradient: outputs must not alias inputs");
     Dev d = make_dev(*g);
-    int64_t n = (int64_t)g->nx * g->ny * g->nz;
     cudaStream_t st = as_stream(stream);
     if (maxima) {
         int e = cuda_status(cudaMemsetAsync(maxima, 0, 3 * sizeof(float), st), "ffx_gradient memset");
         if (e) return e;
     }
+    dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) gradient_kernel<T, true><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            d, s->solid, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow, div_after, maxima);
-        else gradient_kernel<T, false><<<blocks_for(n, kThreads), kThreads, 0, st>>>(
-            d, nullptr, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow, div_after, maxima);
+        if (has_mask(s)) gradient_kernel<T, true><<<grid, block, 0, st>>>(d, s->solid, F, pressure, dt, (T*)ou,
+                                                                          (T*)ov, (T*)ow, div_after, maxima);
+        else gradient_kernel<T, false><<<grid, block, 0, st>>>(d, nullptr, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow,
+                                                               div_after, maxima);
     });
     return launch_status("gradient_kernel");
 }
 
 int ffx_jacobi(const int32_t n[3], const float inv[3], const uint8_t* solid, const float* p_in, const float* rhs,
                float dt, float omega, float* p_out, void* stream) {
-    FFX_REQUIRE(shape_ok(n) && inv && p_in && rhs && p_out && p_in != p_out && dt != 0.f,
+    FFX_REQUIRE(shape_ok(n) && nz_ok(n) && inv && p_in && rhs && p_out && p_in != p_out && dt != 0.f,
                 "ffx_jacobi: invalid arguments");
     Lvl L = make_lvl(n, inv);
-    int64_t cnt = (int64_t)n[0] * n[1] * n[2];
     cudaStream_t st = as_stream(stream);
-    if (solid) jacobi_kernel<true><<<blocks_for(cnt, kThreads), kThreads, 0, st>>>(L, solid, p_in, rhs, dt, omega, p_out);
-    else jacobi_kernel<false><<<blocks_for(cnt, kThreads), kThreads, 0, st>>>(L, nullptr, p_in, rhs, dt, omega, p_out);
+    dim3 grid = cell_grid(n[0], n[1], n[2]), block = cell_block();
+    if (solid) jacobi_kernel<true><<<grid, block, 0, st>>>(L, solid, p_in, rhs, dt, omega, p_out);
+    else jacobi_kernel<false><<<grid, block, 0, st>>>(L, nullptr, p_in, rhs, dt, omega, p_out);
     return launch_status("jacobi_kernel");
 }
 
 int ffx_scale(int64_t count, const float* in, float factor, float* out, void* stream) {
     FFX_REQUIRE(count >= 0 && (count == 0 || (in && out)), "ffx_scale: invalid arguments");
     if (count == 0) return FFX_OK;
-    scale_kernel<<<blocks_for(count, kThreads), kThreads, 0, as_stream(stream)>>>(count, in, factor, out);
+    scale_kernel<<<blocks_for(count, 256), 256, 0, as_stream(stream)>>>(count, in, factor, out);
     return launch_status("scale_kernel");
 }
 
 int ffx_mg_residual(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt, float* r,
                     void* stream) {
-    FFX_REQUIRE(shape_ok(n) && inv && p && rhs && r && dt != 0.f, "ffx_mg_residual: invalid arguments");
+    FFX_REQUIRE(shape_ok(n) && nz_ok(n) && inv && p && rhs && r && dt != 0.f, "ffx_mg_residual: invalid arguments");
     Lvl L = make_lvl(n, inv);
-    int64_t cnt = (int64_t)n[0] * n[1] * n[2];
-    mg_residual_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(L, p, rhs, dt, r);
+    mg_residual_kernel<<<cell_grid(n[0], n[1], n[2]), cell_block(), 0, as_stream(stream)>>>(L, p, rhs, dt, r);
     return launch_status("mg_residual_kernel");
 }
 
 int ffx_mg_restrict(const int32_t fine_n[3], const float* fine, float* coarse, void* stream) {
-    FFX_REQUIRE(shape_ok(fine_n) && fine && coarse && fine_n[0] % 2 == 0 && fine_n[1] % 2 == 0 && fine_n[2] % 2 == 0,
-                "ffx_mg_restrict: invalid arguments (even fine shape required)");
-    int64_t cnt = (int64_t)(fine_n[0] / 2) * (fine_n[1] / 2) * (fine_n[2] / 2);
-    mg_restrict_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(fine_n[0], fine_n[1], fine_n[2],
-                                                                                      fine, coarse);
+    FFX_REQUIRE(shape_ok(fine_n) && nz_ok(fine_n) && fine && coarse && fine_n[0] % 2 == 0 && fine_n[1] % 2 == 0 &&
+                fine_n[2] % 2 == 0, "ffx_mg_restrict: invalid arguments (even fine shape required)");
+    mg_restrict_kernel<<<cell_grid(fine_n[0] / 2, fine_n[1] / 2, fine_n[2] / 2), cell_block(), 0,
+                         as_stream(stream)>>>(fine_n[0], fine_n[1], fine_n[2], fine, coarse);
     return launch_status("mg_restrict_kernel");
 }
 
 int ffx_mg_residual_restrict(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt,
                              float* coarse_rhs, void* stream) {
-    FFX_REQUIRE(shape_ok(n) && inv && p && rhs && coarse_rhs && dt != 0.f && n[0] % 2 == 0 && n[1] % 2 == 0 &&
-                n[2] % 2 == 0, "ffx_mg_residual_restrict: invalid arguments");
+    FFX_REQUIRE(shape_ok(n) && nz_ok(n) && inv && p && rhs && coarse_rhs && dt != 0.f && n[0] % 2 == 0 &&
+                n[1] % 2 == 0 && n[2] % 2 == 0, "ffx_mg_residual_restrict: invalid arguments");
     Lvl L = make_lvl(n, inv);
-    int64_t cnt = (int64_t)(n[0] / 2) * (n[1] / 2) * (n[2] / 2);
-    mg_residual_restrict_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(L, p, rhs, dt,
-                                                                                               coarse_rhs);
+    mg_residual_restrict_kernel<<<cell_grid(n[0] / 2, n[1] / 2, n[2] / 2), cell_block(), 0, as_stream(stream)>>>(
+        L, p, rhs, dt, coarse_rhs);
     return launch_status("mg_residual_restrict_kernel");
 }
 
 int ffx_mg_prolong(const int32_t fine_n[3], const float* p, const float* coarse, float* p_out, void* stream) {
-    FFX_REQUIRE(shape_ok(fine_n) && p && coarse && p_out && p != p_out && fine_n[0] % 2 == 0 && fine_n[1] % 2 == 0 &&
-                fine_n[2] % 2 == 0, "ffx_mg_prolong: invalid arguments");
-    int64_t cnt = (int64_t)fine_n[0] * fine_n[1] * fine_n[2];
-    mg_prolong_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(fine_n[0], fine_n[1], fine_n[2],
-                                                                                     p, coarse, p_out);
+    FFX_REQUIRE(shape_ok(fine_n) && nz_ok(fine_n) && p && coarse && p_out && p != p_out && fine_n[0] % 2 == 0 &&
+                fine_n[1] % 2 == 0 && fine_n[2] % 2 == 0, "ffx_mg_prolong: invalid arguments");
+    mg_prolong_kernel<<<cell_grid(fine_n[0], fine_n[1], fine_n[2]), cell_block(), 0, as_stream(stream)>>>(
+        fine_n[0], fine_n[1], fine_n[2], p, coarse, p_out);
     return launch_status("mg_prolong_kernel");
 }
 
@@ -704,13 +673,15 @@ int ffx_direct_solve(int32_t n, const double* inverse, const float* rhs, float d
 
 int ffx_mg_residual_max(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt,
                         float* out, void* stream) {
-    FFX_REQUIRE(shape_ok(n) && inv && p && rhs && out && dt != 0.f, "ffx_mg_residual_max: invalid arguments");
+    FFX_REQUIRE(shape_ok(n) && nz_ok(n) && inv && p && rhs && out && dt != 0.f,
+                "ffx_mg_residual_max: invalid arguments");
     Lvl L = make_lvl(n, inv);
-    int64_t cnt = (int64_t)n[0] * n[1] * n[2];
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), st), "ffx_mg_residual_max memset");
     if (e) return e;
-    mg_residual_max_kernel<<<reduce_blocks(cnt), kThreads, 0, st>>>(L, p, rhs, dt, out);
+    dim3 grid = cell_grid(n[0], n[1], 1);
+    grid.z = reduce_z(n[2]);
+    mg_residual_max_kernel<<<grid, cell_block(), 0, st>>>(L, p, rhs, dt, out);
     return launch_status("mg_residual_max_kernel");
 }
 
@@ -718,16 +689,15 @@ int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rh
                      void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p_in && rhs && p_out && p_in != p_out, "ffx_graph_smooth: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
-    graph_smooth_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p_in, rhs, omega, p_out);
+    graph_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, p_in, rhs, omega,
+                                                                                             p_out);
     return launch_status("graph_smooth_kernel");
 }
 
 int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && r && r != p, "ffx_graph_residual: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
-    graph_residual_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, rhs, r);
+    graph_residual_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, p, rhs, r);
     return launch_status("graph_residual_kernel");
 }
 
@@ -736,9 +706,8 @@ int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const f
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && coarse_rhs && lv->nx % 2 == 0 && lv->ny % 2 == 0 && lv->nz % 2 == 0,
                 "ffx_graph_residual_restrict: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)(g.nx / 2) * (g.ny / 2) * (g.nz / 2);
-    graph_residual_restrict_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, rhs,
-                                                                                                  coarse_rhs);
+    graph_residual_restrict_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0, as_stream(stream)>>>(
+        g, p, rhs, coarse_rhs);
     return launch_status("graph_residual_restrict_kernel");
 }
 
@@ -746,8 +715,7 @@ int ffx_graph_prolong(const FfxGraphLevel* lv, const float* p, const float* coar
     FFX_REQUIRE(glvl_ok(lv) && p && coarse && p_out && p != p_out && lv->nx % 2 == 0 && lv->ny % 2 == 0 &&
                 lv->nz % 2 == 0, "ffx_graph_prolong: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
-    graph_prolong_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, coarse, p_out);
+    graph_prolong_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, p, coarse, p_out);
     return launch_status("graph_prolong_kernel");
 }
 
@@ -756,20 +724,20 @@ int ffx_graph_prolong_smooth(const FfxGraphLevel* lv, const float* p, const floa
     FFX_REQUIRE(glvl_ok(lv) && p && coarse && rhs && p_out && p != p_out && lv->nx % 2 == 0 && lv->ny % 2 == 0 &&
                 lv->nz % 2 == 0, "ffx_graph_prolong_smooth: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
-    graph_prolong_smooth_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, p, coarse, rhs,
-                                                                                               omega, p_out);
+    graph_prolong_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(
+        g, p, coarse, rhs, omega, p_out);
     return launch_status("graph_prolong_smooth_kernel");
 }
 
 int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && out, "ffx_graph_residual_max: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), st), "ffx_graph_residual_max memset");
     if (e) return e;
-    graph_residual_max_kernel<<<reduce_blocks(cnt), kThreads, 0, st>>>(g, p, rhs, out);
+    dim3 grid = cell_grid(g.nx, g.ny, 1);
+    grid.z = reduce_z(g.nz);
+    graph_residual_max_kernel<<<grid, cell_block(), 0, st>>>(g, p, rhs, out);
     return launch_status("graph_residual_max_kernel");
 }
 
@@ -778,12 +746,11 @@ int ffx_graph_coarsen(const FfxGraphLevel* fine, float* coarse_edges, int32_t* d
                 fine->nx % 2 == 0 && fine->ny % 2 == 0 && fine->nz % 2 == 0,
                 "ffx_graph_coarsen: invalid arguments (even shape, 16-byte aligned records)");
     GLvl g = make_glvl(fine);
-    int64_t cnt = (int64_t)(g.nx / 2) * (g.ny / 2) * (g.nz / 2);
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(cudaMemsetAsync(disconnected, 0, sizeof(int32_t), st), "ffx_graph_coarsen memset");
     if (e) return e;
-    graph_coarsen_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, st>>>(g, reinterpret_cast<float4*>(coarse_edges),
-                                                                         disconnected);
+    graph_coarsen_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0, st>>>(
+        g, reinterpret_cast<float4*>(coarse_edges), disconnected);
     return launch_status("graph_coarsen_kernel");
 }
 
@@ -791,8 +758,8 @@ int ffx_graph_level0_edges(const FfxGraphLevel* lv, float* edges, void* stream) 
     FFX_REQUIRE(glvl_ok(lv) && !lv->edges && edges && ((uintptr_t)edges & 15) == 0,
                 "ffx_graph_level0_edges: invalid arguments");
     GLvl g = make_glvl(lv);
-    int64_t cnt = (int64_t)g.nx * g.ny * g.nz;
-    graph_level0_kernel<<<blocks_for(cnt, kThreads), kThreads, 0, as_stream(stream)>>>(g, reinterpret_cast<float4*>(edges));
+    graph_level0_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(
+        g, reinterpret_cast<float4*>(edges));
     return launch_status("graph_level0_kernel");
 }
 

@@ -20,6 +20,16 @@ def _cuda_available():
         return False
 
 
+@pytest.fixture(autouse=True)
+def _release_device_buffers():
+    yield
+    try:
+        from tests import gpu_helpers
+    except Exception:
+        return
+    gpu_helpers.release()
+
+
 def pytest_collection_modifyitems(config, items):
     if _cuda_available():
         return

@@ -15,8 +15,21 @@ def dev():
     return CudaDevice()
 
 
+# Tensors handed to the C ABI as raw pointers must outlive the (asynchronous)
+# launches that read them: t() parks every tensor here until the test ends.
+_KEEP = []
+
+
 def t(a, dtype=torch.float32):
-    return torch.as_tensor(np.ascontiguousarray(a)).to(dtype).cuda()
+    x = torch.as_tensor(np.ascontiguousarray(a)).to(dtype).cuda()
+    _KEEP.append(x)
+    return x
+
+
+def release():
+    if _KEEP:
+        torch.cuda.synchronize()
+        _KEEP.clear()
 
 
 def n(x):
