@@ -212,7 +212,10 @@ class OracleSmoke:
                 self.velocity = S.walls(g, self.velocity)
         self.projector.reset()
 
-    def step(self, dt, emission_start=None, sources=None):
+    def step(self, dt, emission=None, sources=None):
+        """One step. ``emission``: object with start/velocity/coupling (the
+        reference's ``Emission``), default a static emitter at the source
+        centre; ``sources``: (packed 128-float table, count)."""
         g, s = self.g, self.s
         vel = self.velocity
         detail = s.velocity_advection == 'MACCORMACK'
@@ -221,9 +224,11 @@ class OracleSmoke:
         if sources is not None:
             table = sources          # (128 floats, count)
         else:
-            start = emission_start if emission_start is not None else s.source_center
+            start = emission.start if emission is not None else s.source_center
+            jet = emission.velocity if emission is not None else (0.0, 0.0, 0.0)
+            coupling = emission.coupling if emission is not None else 0.0
             emitter = dict(center=s.source_center, start=start, radius=s.source_radius,
-                           solid=s.source_profile == 'SOLID', jet=(0.0, 0.0, 0.0), coupling=0.0)
+                           solid=s.source_profile == 'SOLID', jet=jet, coupling=coupling)
         preds = [S.face_predictor(g, vel, a, dt) for a in range(3)] if detail else list(vel)
         new = [S.advect_velocity_face(g, vel, preds[a], a, dt, detail, s.velocity_blend,
                                       emitter=emitter, sources=table) for a in range(3)]
