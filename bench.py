@@ -1,25 +1,34 @@
 """Benchmark: steps/s of the dense MAC smoke step at 256^3 with colliders.
 
-Workload (the precision-form scene, plain FP32 unless --storage BF16):
+Workload (the precision-form scene of the 256^3 configuration):
 256^3 cells, unit cube, closed free-slip walls; static colliders = a sphere of
 radius 40 cells at the centre and a box over cells [40:80, 100:160, 20:60]
 (uint8 mask, cell-centre inclusion); two seeded spherical emitters of radius
 8 cells in the lower third that set density and temperature to values drawn
 U(0.5, 1); buoyancy 1.0 T - 0.05 rho; MacCormack transport of U, V, W,
-density and temperature; aggregation multigrid projection cycled until the
-relative max-norm divergence is <= 1e-4; dt = min(0.02, 0.5 dx / max|u|).
-Initial velocity: zero plus seeded uniform +-1e-3 noise on every face.
+density and temperature; aggregation multigrid projection until the relative
+max-norm divergence is <= 1e-4; dt = min(0.02, 0.5 dx / max|u|). Initial
+velocity: zero plus seeded uniform +-1e-3 noise on every face.
 
 One "step" = one DenseProjectedSmoke.step plus the next-dt selection (one
-readback of three floats). `value` is whole-job steps/s (N GPUs each run their
-own replica domain: "weak" scaling, no collective on the step path). `e2e`
+readback of three floats). Solver variants, all to the same tolerance from the
+same seeded start after the same warm-up:
+
+* plain  -- the reference algorithm: stand-alone aggregation V-cycles (4/4
+            Jacobi sweeps), pressure cold-started every step, FP32 storage;
+* pcg    -- conjugate gradients preconditioned by the same V-cycle;
+* fast   -- pcg with the previous step's pressure as the initial guess
+            (--storage selects FP32 or BF16 field storage).
+
+The JSON `value` is the `--variant` run (default fast); the plain run is
+reported beside it. `value` is whole-job steps/s (N GPUs each run their own
+replica domain: "weak" scaling, no collective on the step path). `e2e`
 measures the same steps through the public API with each step's density field
 read back into pinned host memory (the bake/preview readback) inside the
-timed region. `--impl reference` times the CPU restatement of the reference
-on a bounded sample of the same scene.
-
-Inputs larger than L2 (every field of 256^3 is 64 MiB; the working set is
-~1.5 GB), so no L2 flush is needed between steps.
+timed region. Inputs are larger than L2 (each 256^3 field is 64 MiB; the
+working set is ~1.6 GB), so no L2 flush is needed between steps.
+`--impl reference` times the CPU restatement of the reference on a bounded
+sample of the same scene.
 """
 import argparse
 import json
@@ -34,8 +43,24 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-METRIC = "steps/s @256^3 to rel div 1e-4 (colliders, MacCormack, aggregation MG)"
+METRIC = "steps/s @256^3 to rel div 1e-4 (colliders, MacCormack)"
 UNIT = "steps/s"
+
+VARIANTS = {
+    'plain': dict(pressure_method='VCYCLE', solid_warm_start=False),
+    'pcg': dict(pressure_method='PCG', solid_warm_start=False),
+    'fast': dict(pressure_method='PCG', solid_warm_start=True),
+}
+
+# Algorithmic bytes per cell of each pass (inputs read once, outputs written
+# once; s = bytes per stored velocity/scalar value, masks 1 B each).
+def pass_bytes(s):
+    return {
+        'velocity_predictor': 3 * s + 2 + 3 * s,                  # U,V,W + solid,halo -> 3 predictor faces
+        'velocity_transport': 3 * s + 3 * s + 2 * s + 2 + 3 * s,  # U,V,W, predictors, rho,T, masks -> faces
+        'scalar_predictor_reverse': 2 * (3 * s + 2 * s + 2 + 2 * s),
+        'scalar_transport': 3 * s + 6 * s + 2 + 2 * s,            # U,V,W, 3 fields x 2 scalars, masks -> 2
+    }
 
 
 def peaks():
@@ -48,7 +73,7 @@ def peaks():
         return 6650.0, 'fallback'
 
 
-def scene(n, storage='FP32', seed=0):
+def scene(n, storage='FP32', seed=0, **overrides):
     """Grid, settings, colliders, emitters and the seeded initial velocity."""
     import numpy as np
     from fluxfx_b200.physics.collision import primitive
@@ -68,18 +93,19 @@ def scene(n, storage='FP32', seed=0):
         d, t = rng.uniform(0.5, 1.0, 2)
         pos = (cx + rng.uniform(-.05, .05), cy + rng.uniform(-.05, .05), cz)
         emitters.append(Source(pos, 8 * c * h, float(d), float(t), Emission(pos), 'TARGET', 'SOFT'))
-    settings = PressureSettings(velocity_advection='MACCORMACK', scalar_advection='MACCORMACK',
-                                thermal_lift=1.0, density_weight=0.05, dissipation=0.0, cooling=0.0,
-                                heat_mode='TARGET', pressure_tolerance=1e-4, pressure_max_cycles=200,
-                                storage=storage)
+    cfg = dict(velocity_advection='MACCORMACK', scalar_advection='MACCORMACK', thermal_lift=1.0,
+               density_weight=0.05, dissipation=0.0, cooling=0.0, heat_mode='TARGET', pressure_tolerance=1e-4,
+               pressure_max_cycles=200, storage=storage)
+    cfg.update(overrides)
+    settings = PressureSettings(**cfg)
     noise = [rng.uniform(-1e-3, 1e-3, (fs[2], fs[1], fs[0])).astype(np.float32) for fs in grid.face_shapes]
     return grid, settings, (sphere, box), emitters, noise
 
 
-def build_solver(n, storage, seed, device):
+def build_solver(n, storage, seed, device, **overrides):
     import torch
     from fluxfx_b200.backend.projected import DenseProjectedSmoke
-    grid, settings, colliders, emitters, noise = scene(n, storage, seed)
+    grid, settings, colliders, emitters, noise = scene(n, storage, seed, **overrides)
     solver = DenseProjectedSmoke(grid, settings, device, colliders=colliders)
     solver.upload(torch.zeros(grid.cells))
     solver.upload_temperature(torch.zeros(grid.cells))
@@ -127,19 +153,110 @@ class ClockSampler:
             self.thread.join(timeout=5)
         if not self.rows:
             return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
-        sm = [float(r[0]) for r in self.rows if r[0].replace('.', '', 1).isdigit()]
+
+        def num(v):
+            try:
+                return float(v)
+            except ValueError:
+                return None
+        sm = [v for v in (num(r[0]) for r in self.rows) if v is not None]
         names = ('hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap')
         reasons = sorted({names[k] for r in self.rows for k in range(4) if r[3 + k].lower() == 'active'})
-        return {"sm_mhz": statistics.median(sm) if sm else None,
-                "sm_max_mhz": float(self.rows[0][1]) if self.rows[0][1].replace('.', '', 1).isdigit() else None,
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": num(self.rows[0][1]),
                 "reasons": reasons, "samples": len(self.rows)}
+
+
+def max_over_ranks(values, world):
+    """Element-wise max of per-rank timings (every rank must call it)."""
+    import torch
+    import torch.distributed as dist
+    if world <= 1:
+        return [float(v) for v in values]
+    backend = dist.get_backend()
+    device = 'cuda' if backend == 'nccl' else 'cpu'
+    t = torch.tensor([float(v) for v in values], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return [float(v) for v in t.cpu()]
+
+
+def job_rate(world, steps, elapsed):
+    """Whole-job steps/s: every rank advances its own domain `steps` times."""
+    return world * steps / elapsed
+
+
+class Run:
+    """One solver variant on the bench scene: warm-up, timed steps, e2e steps."""
+
+    def __init__(self, args, device, rank, variant, storage):
+        self.args = args
+        self.device = device
+        self.variant = variant
+        self.storage = storage
+        self.solver, self.emitters = build_solver(args.size, storage, args.seed + rank, device, **VARIANTS[variant])
+        self.h = 1.0 / args.size
+        self.dt = 0.02
+
+    def next_dt(self):
+        umax = max(self.solver.projector.velocity_maxima())
+        return min(0.02, 0.5 * self.h / umax) if umax > 0 else 0.02
+
+    def step(self):
+        self.solver.step(self.dt, sources=self.emitters)
+        self.dt = self.next_dt()
+
+    def warm(self, count):
+        for _ in range(count):
+            self.step()
+
+    def timed(self, count, instrument=False):
+        import torch
+        from fluxfx_b200.backend import solid_multigrid as SM
+        from fluxfx_b200.backend.device import PassTimer
+        stream = self.device.stream
+        solver = self.solver
+        self.kernel_timer = SM.KernelTimer(stream) if instrument else None
+        self.pass_timer = PassTimer(stream) if instrument else None
+        solver.projector.timer = self.kernel_timer
+        solver.pass_timer = self.pass_timer
+        self.cycles = []
+        calls0 = self.device.calls
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for _ in range(count):
+            self.step()
+            self.cycles.append(solver.projector.last_cycles)
+        end.record(stream)
+        torch.cuda.synchronize()
+        self.launches = self.device.calls - calls0
+        solver.projector.timer = None
+        solver.pass_timer = None
+        return start.elapsed_time(end) / 1e3
+
+    def e2e(self, count):
+        import torch
+        stream = self.device.stream
+        solver = self.solver
+        host = torch.empty(solver.density.shape, dtype=solver.density.dtype, pin_memory=True)
+        torch.cuda.synchronize()
+        t0, t1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        t0.record(stream)
+        for _ in range(count):
+            self.step()
+            with torch.cuda.stream(stream):
+                host.copy_(solver.density, non_blocking=True)
+        t1.record(stream)
+        torch.cuda.synchronize()
+        return t0.elapsed_time(t1) / 1e3, host.numel() * host.element_size()
+
+    def close(self):
+        self.solver.close()
 
 
 def run_b200(args):
     import torch
     import torch.distributed as dist
     from fluxfx_b200.backend.device import CudaDevice
-    from fluxfx_b200.backend import solid_multigrid as SM
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
     rank = int(os.environ.get('RANK', '0'))
@@ -149,84 +266,83 @@ def run_b200(args):
         dist.init_process_group('nccl', timeout=__import__('datetime').timedelta(seconds=300))
     device = CudaDevice(local)
     n = args.size
-    solver, emitters = build_solver(n, args.storage, args.seed + rank, device)
-    stream = device.stream
-    h = 1.0 / n
+    cells = n ** 3
 
-    def next_dt():
-        umax = max(solver.projector.velocity_maxima())
-        return min(0.02, 0.5 * h / umax) if umax > 0 else 0.02
-
-    dt = 0.02
-    for _ in range(args.warmup):
-        solver.step(dt, sources=emitters)
-        dt = next_dt()
-    timer = SM.KernelTimer(stream)
-    solver.projector.timer = timer
-    cycles = []
-    torch.cuda.synchronize()
+    # --- headline variant -------------------------------------------------
+    run = Run(args, device, rank, args.variant, args.storage)
+    run.warm(args.warmup)
     if world > 1:
+        torch.cuda.synchronize()
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    start.record(stream)
-    for _ in range(args.steps):
-        solver.step(dt, sources=emitters)
-        cycles.append(solver.projector.last_cycles)
-        dt = next_dt()
-    end.record(stream)
-    torch.cuda.synchronize()
-    elapsed = start.elapsed_time(end) / 1e3
+    elapsed = run.timed(args.steps, instrument=True)
     clock_info = clocks.stop()
-    solver.projector.timer = None
-    rel_div = solver.measure_projection()['rel_div_inf']
-    # end to end: same steps through the public API, each step's density read back to pinned host memory
-    host = torch.empty(solver.density.shape, dtype=solver.density.dtype, pin_memory=True)
-    torch.cuda.synchronize()
+    passes = run.pass_timer.totals_ms()
+    smooth_ms = run.kernel_timer.average_ms()
+    smooth_launches = run.kernel_timer.count
+    rel_div = run.solver.measure_projection()['rel_div_inf']
     e2e_steps = max(1, args.steps // 2)
-    t0 = torch.cuda.Event(enable_timing=True)
-    t1 = torch.cuda.Event(enable_timing=True)
-    t0.record(stream)
-    for _ in range(e2e_steps):
-        solver.step(dt, sources=emitters)
-        with torch.cuda.stream(stream):
-            host.copy_(solver.density, non_blocking=True)
-        dt = next_dt()
-    t1.record(stream)
-    torch.cuda.synchronize()
-    e2e_time = t0.elapsed_time(t1) / 1e3
-    times = torch.tensor([elapsed, e2e_time], dtype=torch.float64, device='cuda')
-    if world > 1:
-        dist.all_reduce(times, op=dist.ReduceOp.MAX)
-    elapsed, e2e_time = float(times[0]), float(times[1])
+    e2e_time, d2h = run.e2e(e2e_steps)
+    head = dict(cycles=run.cycles, launches=run.launches)
+    run.close()
+
+    # --- plain FP32 reference algorithm, same scene and warm-up ----------------
+    plain = None
+    if args.compare_plain and args.variant != 'plain':
+        prun = Run(args, device, rank, 'plain', 'FP32')
+        prun.warm(args.warmup)
+        p_steps = max(2, args.steps // 2)
+        p_elapsed = prun.timed(p_steps)
+        plain = dict(elapsed=p_elapsed, steps=p_steps, cycles=prun.cycles,
+                     rel_div=prun.solver.measure_projection()['rel_div_inf'])
+        prun.close()
+
+    elapsed, e2e_time, p_el = max_over_ranks([elapsed, e2e_time, plain['elapsed'] if plain else 0.0], world)
     if rank == 0:
         hbm, peak_kind = peaks()
-        cells = n ** 3
-        avg_ms = timer.average_ms()
-        bytes_per_launch = 13 * cells   # p in + rhs in + mask in + p out, 4+4+1+4 bytes per cell
-        achieved = bytes_per_launch / (avg_ms / 1e3) / 1e9 if avg_ms else None
+        s = 4 if args.storage == 'FP32' else 2
+        bytes_per_launch = 13 * cells   # level-0 sweep: p in + rhs in + mask in + p out = 4+4+1+4 B per cell
+        achieved = bytes_per_launch / (smooth_ms / 1e3) / 1e9 if smooth_ms else None
+        pb = pass_bytes(s)
+        pass_report = {}
+        for name, ms in passes.items():
+            per_step = ms / args.steps
+            entry = {"ms_per_step": per_step}
+            if name in pb:
+                entry["algorithmic_bytes_per_cell"] = pb[name]
+                entry["achieved_GBps"] = pb[name] * cells / (per_step / 1e3) / 1e9
+                entry["frac_of_peak"] = entry["achieved_GBps"] / hbm
+            pass_report[name] = entry
         line = {
-            "metric": METRIC, "value": world * args.steps / elapsed, "unit": UNIT, "n_gpus": world,
+            "metric": METRIC, "value": job_rate(world, args.steps, elapsed), "unit": UNIT, "n_gpus": world,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * elapsed / args.steps,
             "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32" if args.storage == 'FP32' else "bf16-storage/f32-math",
             "data": "synthetic (seeded scene; no dataset)",
-            "config": {"workload": f"dense smoke step {n}^3, sphere r=40 + box colliders, 2 emitters r=8, "
-                                   f"MacCormack, aggregation MG to rel div<=1e-4, {args.storage} storage",
+            "config": {"workload": f"dense smoke step {n}^3, sphere r=40 + box colliders, 2 emitters r=8, MacCormack, "
+                                   f"projection to rel div<=1e-4; variant={args.variant} "
+                                   f"({VARIANTS[args.variant]}), {args.storage} storage",
                        "cells": cells, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}",
-                       "v_cycles_mean": statistics.mean(cycles), "v_cycles_max": max(cycles),
-                       "final_rel_div_inf": rel_div},
+                       "v_cycles_mean": statistics.mean(head['cycles']), "v_cycles_max": max(head['cycles']),
+                       "final_rel_div_inf": rel_div,
+                       "plain_fp32_mg": None if plain is None else {
+                           "steps_per_s": job_rate(world, plain['steps'], p_el), "steps": plain['steps'],
+                           "v_cycles_mean": statistics.mean(plain['cycles']),
+                           "final_rel_div_inf": plain['rel_div']},
+                       "speedup_vs_plain": None if plain is None else
+                       job_rate(world, args.steps, elapsed) / job_rate(world, plain['steps'], p_el)},
             "cell_updates_per_s": world * args.steps * cells / elapsed,
-            "e2e": {"value": world * e2e_steps / e2e_time, "unit": UNIT, "h2d_bytes_per_step": 512,
-                    "d2h_bytes_per_step": host.numel() * host.element_size()},
-            "gpu_launches": None,
-            "roofline": {"bound": "hbm", "kernel": "ffx graph_smooth_kernel (level-0 aggregation MG sweep)",
-                         "achieved": achieved, "peak": hbm, "peak_kind": peak_kind, "unit": "GB/s",
-                         "frac": (achieved / hbm) if achieved else None, "traffic": None,
-                         "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": avg_ms,
-                         "launches_timed": timer.count},
+            "passes": pass_report,
+            "e2e": {"value": job_rate(world, e2e_steps, e2e_time), "unit": UNIT, "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": head['launches'],
+            "roofline": {"bound": "hbm", "kernel": "graph_smooth_kernel (level-0 aggregation multigrid sweep)",
+                         "achieved": achieved, "peak": hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
+                         "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
+                         "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": smooth_ms,
+                         "launches_timed": smooth_launches},
             "clocks": clock_info,
         }
         if args.cpu_baseline:
@@ -239,13 +355,14 @@ def run_b200(args):
 
 def cpu_baseline(args, sample_n=None, sample_steps=1):
     """Time the NumPy restatement (one host thread) on a bounded sample of the
-    scene and express it as steps/s of the full 256^3 grid via cell updates/s."""
+    scene, the plain reference algorithm, and express it as steps/s of the
+    full grid through the cell-update rate."""
     import numpy as np
     from oracle.smoke import Grid, raster_mask
     from oracle.solver import OracleSmoke
     from fluxfx_b200.physics.emission import pack_sources
     n = sample_n or args.cpu_sample
-    grid, settings, colliders, emitters, noise = scene(n, 'FP32', args.seed)
+    grid, settings, colliders, emitters, noise = scene(n, 'FP32', args.seed, **VARIANTS['plain'])
     g = Grid(grid.shape, grid.extent, np.float32)
     mask = raster_mask(g, [(c.shape, c.inverse_rows) for c in colliders])
     ref = OracleSmoke(grid.shape, grid.extent, settings, np.float32, mask=mask)
@@ -257,27 +374,26 @@ def cpu_baseline(args, sample_n=None, sample_steps=1):
     dt = time.perf_counter() - t0
     rate = sample_steps * n ** 3 / dt
     return {"value": rate / args.size ** 3, "unit": UNIT, "cores": 1, "kind": "port",
-            "sample": f"{sample_steps} step(s) of the same scene at {n}^3 on the NumPy oracle "
-                      f"({dt:.1f} s, {ref.projector.last_cycles} V-cycles); cell-update rate scaled to {args.size}^3"}
+            "sample": f"{sample_steps} step(s) of the same scene at {n}^3 on the NumPy restatement of the "
+                      f"reference ({dt:.1f} s, {ref.projector.last_cycles} V-cycles); cell-update rate scaled "
+                      f"to {args.size}^3"}
 
 
 def run_reference(args):
     rank = int(os.environ.get('RANK', '0'))
     if rank != 0:
         return
-    samples = []
     for _ in range(args.warmup):
         cpu_baseline(args, args.cpu_sample, 1)
-    for _ in range(args.steps):
-        samples.append(cpu_baseline(args, args.cpu_sample, 1))
+    samples = [cpu_baseline(args, args.cpu_sample, 1) for _ in range(args.steps)]
     value = statistics.mean(s['value'] for s in samples)
-    base = samples[-1]
     print(json.dumps({
         "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": 1, "steps": args.steps,
         "warmup": args.warmup, "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded scene)",
-        "config": {"workload": f"dense smoke step {args.size}^3 scene, bounded CPU sample at {args.cpu_sample}^3"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": base['sample']},
+        "config": {"workload": f"dense smoke step {args.size}^3 scene, reference algorithm, "
+                               f"bounded CPU sample at {args.cpu_sample}^3"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": samples[-1]['sample']},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 
@@ -289,9 +405,11 @@ def main():
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--size', type=int, default=256)
     ap.add_argument('--storage', default='FP32', choices=('FP32', 'BF16'))
+    ap.add_argument('--variant', default='fast', choices=tuple(VARIANTS))
     ap.add_argument('--seed', type=int, default=0)
     ap.add_argument('--cpu-sample', type=int, default=64)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
+    ap.add_argument('--no-compare-plain', dest='compare_plain', action='store_false')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)

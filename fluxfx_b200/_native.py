@@ -101,6 +101,11 @@ _PROTOTYPES = {
     'ffx_graph_residual_max': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
     'ffx_graph_coarsen': (C.c_int, [P(FfxGraphLevel), vp, vp, vp]),
     'ffx_graph_level0_edges': (C.c_int, [P(FfxGraphLevel), vp, vp]),
+    'ffx_graph_smooth_zero': (C.c_int, [P(FfxGraphLevel), vp, f32, vp, vp]),
+    'ffx_graph_smooth_dot': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp, C.c_double, vp]),
+    'ffx_pcg_direction_apply': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp, vp, vp, vp, vp]),
+    'ffx_pcg_update': (C.c_int, [i64, vp, vp, vp, vp, vp, vp, vp, vp]),
+    'ffx_dot': (C.c_int, [i64, vp, vp, C.c_double, vp, vp]),
     'ffx_max_abs': (C.c_int, [i64, C.c_int, vp, vp, vp]),
     'ffx_divergence_stats_workspace': (C.c_size_t, [i64]),
     'ffx_divergence_stats': (C.c_int, [i64, vp, vp, vp, vp, C.c_size_t, vp]),

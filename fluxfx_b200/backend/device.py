@@ -66,6 +66,7 @@ class CudaDevice:
         self.sm_count = info.sm_count
         self.stream = stream if stream is not None else torch.cuda.current_stream(self.device)
         self.max_groups = (2 ** 31 - 1, 65535, 65535)
+        self.calls = 0
 
     # ------------------------------------------------------------------ basics
     @property
@@ -74,6 +75,9 @@ class CudaDevice:
         return C.c_void_p(self.stream.cuda_stream)
 
     def call(self, name, *args):
+        """Invoke a native entry point (each enqueues one kernel, two for the
+        divergence statistics) and count it in ``calls``."""
+        self.calls += 1
         N.check(getattr(self.lib, name)(*args))
 
     def synchronize(self):
@@ -126,6 +130,34 @@ class CudaDevice:
         if output is input_field or any(output is t for t in (sources or {}).values()):
             raise ValueError("Advection input/output textures must be distinct")
         _dispatch.run(self, shader, output, _shape3(shape), uniforms or {}, input_field, sources or {})
+
+
+class PassTimer:
+    """CUDA events between the passes of a step, on the solver's stream.
+
+    ``mark(name)`` closes the interval that started at the previous mark and
+    books it under ``name``; ``totals_ms()`` synchronises and returns the summed
+    milliseconds per name. Off unless a solver is given one."""
+
+    def __init__(self, stream):
+        self.stream = stream
+        self.events = []     # (name, event)
+
+    def mark(self, name):
+        e = torch.cuda.Event(enable_timing=True)
+        e.record(self.stream)
+        self.events.append((name, e))
+
+    def totals_ms(self):
+        if len(self.events) < 2:
+            return {}
+        self.events[-1][1].synchronize()
+        out = {}
+        for (_, a), (name, b) in zip(self.events, self.events[1:]):
+            if name == 'start':
+                continue
+            out[name] = out.get(name, 0.0) + a.elapsed_time(b)
+        return out
 
 
 def ptr(t):

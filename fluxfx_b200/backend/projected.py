@@ -56,6 +56,7 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         self.projector = None
         self.detail = None
         self.turbulence = None
+        self.pass_timer = None
         self.faulted = False
         self._source_data = None
         self._sources = N.FfxSources()
@@ -159,6 +160,10 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             src.single_coupling = emission.coupling
         return src
 
+    def _mark(self, name):
+        if self.pass_timer is not None:
+            self.pass_timer.mark(name)
+
     def _step(self, dt, emission, emitters=None):
         s = self.settings
         dev = self.device
@@ -168,21 +173,26 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         src = self._fill_sources(emission, emitters)
         corrected_v = s.velocity_advection == "MACCORMACK"
         vel = [ptr(f) for f in self._velocity]
+        self._mark('start')
         if corrected_v:
             self.detail.transport_velocity(self._velocity, dt)
             pred = [ptr(f) for f in self.detail.face_predictor]
+            self._mark('velocity_predictor')
         else:
             pred = [None, None, None]
         proj = self.projector
         dev.call('ffx_advect_velocity', gp, sp, self._storage, *vel, *pred, dt, int(corrected_v), s.velocity_blend,
                  C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift, s.density_weight, 1,
                  *[ptr(b) for b in proj.bounded], st)
+        self._mark('velocity_transport')
         # The old velocity is consumed: the corrected field is written over it.
         proj.project_bounded(self._velocity, dt)
+        self._mark('projection')
         corrected_s = s.scalar_advection == "MACCORMACK"
         fields = [self._front, self._temperature]
         if corrected_s:
             preds, revs = self.detail.transport_many(fields, self._velocity, dt)
+            self._mark('scalar_predictor_reverse')
         else:
             preds = revs = fields
         outs = [self._back, self._temperature_back]
@@ -195,6 +205,7 @@ class DenseProjectedSmoke(DenseThermalAdvection):
                                s.cooling, heat_target, 1, int(s.heat_mode == "TARGET")))
         dev.call('ffx_advect_scalars', gp, sp, self._storage, *[ptr(f) for f in self._velocity], dt,
                  int(corrected_s), C.byref(src), 2, chans, ptr(self._maxima), st)
+        self._mark('scalar_transport')
         self._front, self._back = self._back, self._front
         self._temperature, self._temperature_back = self._temperature_back, self._temperature
         self.time += dt

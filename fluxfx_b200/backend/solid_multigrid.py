@@ -133,7 +133,12 @@ class SolidMultigridProjector(SolidPressureProjector):
             level['p'], level['q'] = level['q'], level['p']
             self.last_iterations += 1
 
-    def cycle(self, index):
+    def cycle(self, index, zero_init=False, dot=None):
+        """One V-cycle from ``index`` down (``backend/solid_multigrid.py:46-65``).
+
+        ``zero_init``: the level's iterate is zero, so the first sweep reads none.
+        ``dot``: FP64 device slot receiving -rhs . result from the last sweep
+        (used by the Krylov solve)."""
         level = self.levels[index]
         dev = self.device
         if index == len(self.levels) - 1:
@@ -142,9 +147,23 @@ class SolidMultigridProjector(SolidPressureProjector):
                          ptr(level['q']), dev.s)
                 level['p'], level['q'] = level['q'], level['p']
             else:
+                if zero_init:
+                    level['p'].zero_()
                 self.smooth(level, 80)
+            if dot is not None:
+                dev.call('ffx_dot', level['p'].numel(), ptr(level['rhs']), ptr(level['p']), -1.0, ptr(dot), dev.s)
             return
-        self.smooth(level, self.pre_sweeps)
+        pre = self.pre_sweeps
+        if zero_init:
+            if pre > 0:
+                dev.call('ffx_graph_smooth_zero', C.byref(level['graph']), ptr(level['rhs']), 2.0 / 3.0,
+                         ptr(level['q']), dev.s)
+                level['p'], level['q'] = level['q'], level['p']
+                self.last_iterations += 1
+                pre -= 1
+            else:
+                level['p'].zero_()
+        self.smooth(level, pre)
         coarse = self.levels[index + 1]
         dev.call('ffx_graph_residual_restrict', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
                  ptr(coarse['rhs']), dev.s)
@@ -155,17 +174,89 @@ class SolidMultigridProjector(SolidPressureProjector):
                      ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), dev.s)
             level['p'], level['q'] = level['q'], level['p']
             self.last_iterations += 1
+            if dot is not None and self.post_sweeps > 1:
+                self.smooth(level, self.post_sweeps - 2)
+                dev.call('ffx_graph_smooth_dot', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                         2.0 / 3.0, ptr(level['q']), ptr(dot), -1.0, dev.s)
+                level['p'], level['q'] = level['q'], level['p']
+                self.last_iterations += 1
+                return
             self.smooth(level, self.post_sweeps - 1)
         else:
             dev.call('ffx_graph_prolong', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['q']), dev.s)
             level['p'], level['q'] = level['q'], level['p']
+        if dot is not None:
+            dev.call('ffx_dot', level['p'].numel(), ptr(level['rhs']), ptr(level['p']), -1.0, ptr(dot), dev.s)
 
     def _residual_max(self):
         level = self.levels[0]
         self.device.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
                          ptr(self._rmax[0:1]), self.device.s)
         return float(self._rmax[0].item())
+
+    # ------------------------------------------------------------ Krylov solve
+    def _krylov_buffers(self):
+        if getattr(self, '_kry', None) is None:
+            dev = self.device
+            shape = self.levels[0]['shape']
+            cap = self.settings.pressure_max_cycles + 8
+            self._kry = dict(res=dev.texture(shape), z=dev.texture(shape), z2=dev.texture(shape),
+                             p=[dev.texture(shape), dev.texture(shape)], q=dev.texture(shape),
+                             rz=torch.zeros(cap, dtype=torch.float64, device=dev.device),
+                             pq=torch.zeros(cap, dtype=torch.float64, device=dev.device),
+                             rmax=torch.zeros(1, dtype=torch.float32, device=dev.device))
+        return self._kry
+
+    def _precondition(self, res, bufs, rz_slot):
+        """z = V-cycle(res) from a zero iterate; rz_slot <- -res . z. Returns z."""
+        L0 = self.levels[0]
+        saved = (L0['p'], L0['q'], L0['rhs'])
+        L0['p'], L0['q'], L0['rhs'] = bufs['z'], bufs['z2'], res
+        self.cycle(0, zero_init=True, dot=rz_slot)
+        z = L0['p']
+        bufs['z'], bufs['z2'] = L0['p'], L0['q']
+        L0['p'], L0['q'], L0['rhs'] = saved
+        return z
+
+    def _solve_krylov(self, scale, budget):
+        """Conjugate gradients on A = -L preconditioned by the aggregation
+        V-cycle, until max|rhs - L x| <= tol * max|rhs| (or ``budget`` cycles)."""
+        s = self.settings
+        dev = self.device
+        B = self._krylov_buffers()
+        L0 = self.levels[0]
+        g = C.byref(L0['graph'])
+        x = self.pressure
+        n = x.numel()
+        tol = s.pressure_tolerance * scale if s.pressure_tolerance > 0 else -1.0
+        res = B['res']
+        for restart in range(2):
+            dev.call('ffx_graph_residual', g, ptr(x), ptr(self.before), ptr(res), dev.s)
+            dev.call('ffx_max_abs', n, N.FFX_F32, ptr(res), ptr(B['rmax']), dev.s)
+            if float(B['rmax'].item()) <= tol:
+                return
+            k = 0
+            p_old = None
+            while self.last_cycles < budget:
+                z = self._precondition(res, B, B['rz'][k:k + 1])
+                self.last_cycles += 1
+                p_new = B['p'][k % 2]
+                dev.call('ffx_pcg_direction_apply', g, ptr(z), ptr(p_old), ptr(B['rz'][k:k + 1]),
+                         ptr(B['rz'][k - 1:k]) if k > 0 else None, ptr(p_new), ptr(B['q']),
+                         ptr(B['pq'][k:k + 1]), dev.s)
+                dev.call('ffx_pcg_update', n, ptr(B['rz'][k:k + 1]), ptr(B['pq'][k:k + 1]), ptr(x), ptr(p_new),
+                         ptr(res), ptr(B['q']), ptr(B['rmax']), dev.s)
+                p_old = p_new
+                k += 1
+                if float(B['rmax'].item()) <= tol or k + 1 >= B['rz'].numel():
+                    break
+            if tol < 0 or self.last_cycles >= budget:
+                return
+            # the recursively updated residual drifts in FP32: confirm on the true one
+            dev.call('ffx_graph_residual_max', g, ptr(x), ptr(self.before), ptr(B['rmax']), dev.s)
+            if float(B['rmax'].item()) <= tol:
+                return
 
     def solve_pressure(self, dt, previous_dt):
         s = self.settings
@@ -177,6 +268,19 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
         self.last_iterations = 0
         budget = s.pressure_cycles * (s.pressure_cold_multiplier if previous_dt is None else 1)
+        if s.pressure_method == 'PCG':
+            scale = 0.0
+            if s.pressure_tolerance > 0:
+                self.device.call('ffx_max_abs', self.before.numel(), N.FFX_F32, ptr(self.before),
+                                 ptr(self._rmax[1:2]), self.device.s)
+                scale = float(self._rmax[1].item())
+                budget = s.pressure_max_cycles
+            if s.pressure_tolerance > 0 and scale == 0:
+                self.pressure.zero_()
+            else:
+                self._solve_krylov(scale, budget)
+            self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
+            return
         if s.pressure_tolerance <= 0:
             for _ in range(budget):
                 self.cycle(0)

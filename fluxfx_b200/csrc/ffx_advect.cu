@@ -42,14 +42,15 @@ __device__ __forceinline__ bool face_coords(const Dev& d, FaceIdx& f) {
 // Midpoint backtrace p -> departure (transport_face.glsl:8-17 and the same
 // lines of every advection shader); clipped at colliders when MASK.
 template <typename T, bool MASK>
-__device__ __forceinline__ F3 backtrace(const Dev& d, const Faces<T>& F, const uint8_t* solid, F3 p, F3 v0,
+__device__ __forceinline__ F3 backtrace(const Dev& d, const Faces<T>& F, const uint8_t* solid, const uint8_t* halo,
+                                        F3 p, F3 v0,
                                         float dt) {
     float s = 0.5f * dt;
     F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
-    if (MASK) mid = clip_solid_trace(d, solid, p, mid);
+    if (MASK) mid = clip_solid_trace(d, solid, halo, p, mid);
     F3 vm = velocity_at(d, F, mid);
     F3 dep = {p.x - dt * vm.x, p.y - dt * vm.y, p.z - dt * vm.z};
-    if (MASK) dep = clip_solid_trace(d, solid, p, dep);
+    if (MASK) dep = clip_solid_trace(d, solid, halo, p, dep);
     return dep;
 }
 
@@ -104,6 +105,7 @@ __device__ __forceinline__ float fetch_closed(const Dev& d, const T* __restrict_
 // ------------------------------------------------------------ face predictor
 template <typename T, bool MASK>
 __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const uint8_t* __restrict__ solid,
+                                                                  const uint8_t* __restrict__ halo,
                                                                   Faces<T> F, float dt, T* pu, T* pv, T* pw) {
     FaceIdx f;
     if (!face_coords(d, f)) return;
@@ -115,7 +117,7 @@ __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const u
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
     F3 v0 = velocity_at(d, F, p);
-    F3 dep = backtrace<T, MASK>(d, F, solid, p, v0, dt);
+    F3 dep = backtrace<T, MASK>(d, F, solid, halo, p, v0, dt);
     const T* src = f.axis == 0 ? F.u : (f.axis == 1 ? F.v : F.w);
     float value = sample_face(src, f.sx, f.sy, f.sz, dep.x / d.h[0] - ox, dep.y / d.h[1] - oy, dep.z / d.h[2] - oz);
     Store<T>::st(out, f.i, value);
@@ -151,7 +153,7 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
         F3 p = {((float)f.x + off[0]) * d.e[0] / d.nf[0], ((float)f.y + off[1]) * d.e[1] / d.nf[1],
                 ((float)f.z + off[2]) * d.e[2] / d.nf[2]};
         F3 v0 = velocity_at(d, P.F, p);
-        F3 dep = backtrace<T, MASK>(d, P.F, P.solid, p, v0, dt);
+        F3 dep = backtrace<T, MASK>(d, P.F, P.solid, P.halo, p, v0, dt);
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
         float qx = dep.x / d.h[0] - off[0], qy = dep.y / d.h[1] - off[1], qz = dep.z / d.h[2] - off[2];
@@ -239,7 +241,7 @@ __global__ void __launch_bounds__(kThreads) mac_advect_velocity_kernel(Dev d, Fa
     F3 p = {((float)f.x + ox) * d.e[0] / d.nf[0], ((float)f.y + oy) * d.e[1] / d.nf[1],
             ((float)f.z + oz) * d.e[2] / d.nf[2]};
     F3 v0 = velocity_at(d, F, p);
-    F3 dep = backtrace<T, false>(d, F, nullptr, p, v0, dt);
+    F3 dep = backtrace<T, false>(d, F, nullptr, nullptr, p, v0, dt);
     F3 v = velocity_at(d, F, dep);
     T* out = f.axis == 0 ? ou : (f.axis == 1 ? ov : ow);
     Store<T>::st(out, f.i, comp(v, f.axis));
@@ -264,6 +266,7 @@ template <typename T>
 struct ScalarXport {
     Dev d;
     const uint8_t* solid;
+    const uint8_t* halo;
     Faces<T> F;
     float dt;
     int count;
@@ -283,7 +286,7 @@ __global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = velocity_at(d, P.F, p);
-    F3 dep = backtrace<T, MASK>(d, P.F, P.solid, p, v0, P.dt);
+    F3 dep = backtrace<T, MASK>(d, P.F, P.solid, P.halo, p, v0, P.dt);
     float qx = dep.x / d.h[0] - 0.5f, qy = dep.y / d.h[1] - 0.5f, qz = dep.z / d.h[2] - 0.5f;
     for (int c = 0; c < P.count; ++c)
         Store<T>::st(P.out[c], i, sample_closed<T, MASK>(d, P.solid, P.in[c], qx, qy, qz));
@@ -325,7 +328,7 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
             const float dt = P.dt;
             F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
             F3 v0 = velocity_at(d, P.F, p);
-            F3 dep = backtrace<T, MASK>(d, P.F, P.solid, p, v0, dt);
+            F3 dep = backtrace<T, MASK>(d, P.F, P.solid, P.halo, p, v0, dt);
             float qx = dep.x / d.h[0] - 0.5f, qy = dep.y / d.h[1] - 0.5f, qz = dep.z / d.h[2] - 0.5f;
             bool ok = false;
             if (P.corrected) {
@@ -445,7 +448,7 @@ __global__ void mac_advect_density_kernel(OpenParams P, Faces<T> F, const T* in,
     const int i = cidx(d, x, y, z);
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = velocity_at(d, F, p);
-    F3 dep = backtrace<T, false>(d, F, nullptr, p, v0, P.dt);
+    F3 dep = backtrace<T, false>(d, F, nullptr, nullptr, p, v0, P.dt);
     float value = sample_zero(d, in, dep.x / d.h[0] - 0.5f, dep.y / d.h[1] - 0.5f, dep.z / d.h[2] - 0.5f) *
                   expf(-P.decay * P.dt);
     F3 off = {p.x - P.center.x, p.y - P.center.y, p.z - P.center.z};
@@ -474,8 +477,10 @@ int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const 
     const uint8_t* solid = has_mask(s) ? s->solid : nullptr;
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (solid) face_predictor_kernel<T, true><<<blocks, threads, 0, st>>>(d, solid, F, dt, (T*)pu, (T*)pv, (T*)pw);
-        else face_predictor_kernel<T, false><<<blocks, threads, 0, st>>>(d, nullptr, F, dt, (T*)pu, (T*)pv, (T*)pw);
+        if (solid) face_predictor_kernel<T, true><<<blocks, threads, 0, st>>>(d, solid, s->halo, F, dt, (T*)pu, (T*)pv,
+                                                                               (T*)pw);
+        else face_predictor_kernel<T, false><<<blocks, threads, 0, st>>>(d, nullptr, nullptr, F, dt, (T*)pu, (T*)pv,
+                                                                         (T*)pw);
     });
     return launch_status("face_predictor_kernel");
 }
@@ -557,6 +562,7 @@ int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, cons
         ScalarXport<T> P;
         P.d = d;
         P.solid = has_mask(s) ? s->solid : nullptr;
+        P.halo = has_mask(s) ? s->halo : nullptr;
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.dt = dt;
         P.count = count;

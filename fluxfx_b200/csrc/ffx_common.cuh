@@ -147,20 +147,33 @@ __device__ __forceinline__ bool solid_face(const Dev& d, const uint8_t* __restri
 
 // Voxel DDA clip of the segment origin -> target at the first solid cell, at
 // most 384 crossings (solid_boundary.glsl:13-36).
+//
+// Fast path (exact): when the 3x3x3 blocks around the start cell and the end
+// cell hold no solid (dilated mask `halo`) and the end cell is within one cell
+// of the start, every cell the traversal can visit -- including a one-cell
+// overshoot past the end from rounding of the crossing parameters -- is fluid,
+// so the loop would run to t >= 1 and return b / count * extent. That value is
+// returned directly; it is bit-identical to the loop's.
 __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __restrict__ solid,
-                                               F3 origin, F3 target) {
+                                               const uint8_t* __restrict__ halo, F3 origin, F3 target) {
     float cnt[3] = {d.nf[0], d.nf[1], d.nf[2]};
     float o[3] = {origin.x, origin.y, origin.z}, t3[3] = {target.x, target.y, target.z};
     float a[3], b[3], delta[3], crossing[3], stride[3];
-    int cell[3], dir[3];
+    int cell[3], dir[3], endc[3];
     for (int i = 0; i < 3; ++i) {
         a[i] = fminf(fmaxf(o[i] / d.e[i] * cnt[i], 0.0001f), cnt[i] - 0.0001f);
         b[i] = fminf(fmaxf(t3[i] / d.e[i] * cnt[i], 0.0001f), cnt[i] - 0.0001f);
         delta[i] = b[i] - a[i];
         cell[i] = (int)floorf(a[i]);
+        endc[i] = (int)floorf(b[i]);
         dir[i] = delta[i] > 0.f ? 1 : (delta[i] < 0.f ? -1 : 0);
         crossing[i] = 1e20f;
         stride[i] = 1e20f;
+    }
+    if (halo && abs(endc[0] - cell[0]) <= 1 && abs(endc[1] - cell[1]) <= 1 && abs(endc[2] - cell[2]) <= 1 &&
+        !__ldg(halo + cidx(d, cell[0], cell[1], cell[2])) && !__ldg(halo + cidx(d, endc[0], endc[1], endc[2]))) {
+        F3 r = {b[0] / cnt[0] * d.e[0], b[1] / cnt[1] * d.e[1], b[2] / cnt[2] * d.e[2]};
+        return r;
     }
     if (solid_cell(d, solid, cell[0], cell[1], cell[2])) return origin;
     for (int i = 0; i < 3; ++i) {
@@ -212,9 +225,9 @@ __device__ __forceinline__ bool safe_solid_correction(const Dev& d, const uint8_
                                                       const uint8_t* halo, F3 p, F3 dep, F3 mid,
                                                       F3 arr) {
     if (solid_halo(d, halo, p) || solid_halo(d, halo, dep) || solid_halo(d, halo, arr)) return false;
-    if (!(dist3(clip_solid_trace(d, solid, p, dep), dep) < 1e-7f)) return false;
-    if (!(dist3(clip_solid_trace(d, solid, p, mid), mid) < 1e-7f)) return false;
-    return dist3(clip_solid_trace(d, solid, p, arr), arr) < 1e-7f;
+    if (!(dist3(clip_solid_trace(d, solid, halo, p, dep), dep) < 1e-7f)) return false;
+    if (!(dist3(clip_solid_trace(d, solid, halo, p, mid), mid) < 1e-7f)) return false;
+    return dist3(clip_solid_trace(d, solid, halo, p, arr), arr) < 1e-7f;
 }
 
 // ---------------------------------------------------------------- emitters

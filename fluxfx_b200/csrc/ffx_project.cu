@@ -518,6 +518,98 @@ __global__ void __launch_bounds__(256) graph_level0_kernel(GLvl g, float4* out) 
     out[i] = g_edge(g, i, x, y, z);
 }
 
+// ------------------------------------------ Krylov acceleration (MG-PCG)
+// The projection solves L p = rhs with L the (negative semi-definite) graph
+// Laplacian. Conjugate gradients run on A = -L; `res` stores the residual in
+// the multigrid convention res = rhs - L x (= -(b - A x) for b = -rhs), so a
+// V-cycle applied to res approximates A^-1 r directly.
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+// Block-wide FP64 sum then one atomicAdd per block (block of 256 threads).
+__device__ __forceinline__ void block_sum_to(double* out, double v) {
+    __shared__ double part[8];
+    v = warp_sum_d(v);
+    const int tid = threadIdx.x + blockDim.x * threadIdx.y;
+    if ((tid & 31) == 0) part[tid >> 5] = v;
+    __syncthreads();
+    if (tid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < (int)(blockDim.x * blockDim.y) / 32; ++w) s += part[w];
+        if (s != 0.0) atomicAdd(out, s);
+    }
+}
+
+// Last sweep of the preconditioning V-cycle fused with dot += scale * rhs . out.
+__global__ void __launch_bounds__(256) graph_smooth_dot_kernel(GLvl g, const float* __restrict__ p,
+                                                              const float* __restrict__ rhs, float omega, float* out,
+                                                              double* dot, double scale) {
+    int x, y, z;
+    double acc = 0.0;
+    if (cell_coords(g.nx, g.ny, x, y, z)) {
+        const int i = x + g.nx * (y + g.ny * z);
+        float diag, nb;
+        graph_terms(g, i, x, y, z, [&](int j, int, int, int) { return __ldg(p + j); }, diag, nb);
+        const float r = __ldg(rhs + i);
+        const float v = diag > 0.f ? __ldg(p + i) * (1.f - omega) + ((nb - r) / diag) * omega : 0.f;
+        out[i] = v;
+        acc = scale * (double)r * (double)v;
+    }
+    block_sum_to(dot, acc);
+}
+
+// First sweep from a zero iterate: p_out = omega * (0 - rhs) / diag on active cells.
+__global__ void __launch_bounds__(256) graph_smooth_zero_kernel(GLvl g, const float* __restrict__ rhs, float omega,
+                                                               float* out) {
+    int x, y, z;
+    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    const int i = x + g.nx * (y + g.ny * z);
+    float diag, nb;
+    graph_terms(g, i, x, y, z, [&](int, int, int, int) { return 0.f; }, diag, nb);
+    out[i] = diag > 0.f ? 0.f * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
+}
+
+// New search direction p = z + beta p_old (beta = rz_new / rz_old; p = z when
+// rz_old is NULL), written out, and q = A p = diag p - nb(p), with pq += p . q.
+__global__ void __launch_bounds__(256) pcg_direction_apply_kernel(GLvl g, const float* __restrict__ zv,
+                                                                 const float* __restrict__ p_old,
+                                                                 const double* rz_new, const double* rz_old,
+                                                                 float* p_out, float* q, double* pq) {
+    int x, y, z;
+    const float beta = rz_old ? (float)(*rz_new / *rz_old) : 0.f;
+    double acc = 0.0;
+    if (cell_coords(g.nx, g.ny, x, y, z)) {
+        const int i = x + g.nx * (y + g.ny * z);
+        auto dir = [&](int j) { return rz_old ? __ldg(zv + j) + beta * __ldg(p_old + j) : __ldg(zv + j); };
+        float diag, nb;
+        graph_terms(g, i, x, y, z, [&](int j, int, int, int) { return dir(j); }, diag, nb);
+        const float pc = dir(i);
+        const float qc = diag > 0.f ? diag * pc - nb : 0.f;
+        p_out[i] = pc;
+        q[i] = qc;
+        acc = (double)pc * (double)qc;
+    }
+    block_sum_to(pq, acc);
+}
+
+// x += alpha p; res += alpha q; resmax = max|res| (alpha = rz / pq).
+__global__ void __launch_bounds__(256) pcg_update_kernel(int64_t n, const double* rz, const double* pq,
+                                                        float* __restrict__ xv, const float* __restrict__ p,
+                                                        float* __restrict__ res, const float* __restrict__ q,
+                                                        float* resmax) {
+    const double den = *pq;
+    const float alpha = den > 0.0 ? (float)(*rz / den) : 0.f;
+    float m = 0.f;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        xv[i] = xv[i] + alpha * p[i];
+        const float r = res[i] + alpha * q[i];
+        res[i] = r;
+        m = fmaxf(m, finite_abs(r));
+    }
+    block_max_to(resmax, m);
+}
+
 bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s->solid && s->halo); }
 bool has_mask(const FfxSolids* s) { return s && s->solid; }
 
@@ -761,6 +853,81 @@ int ffx_graph_level0_edges(const FfxGraphLevel* lv, float* edges, void* stream) 
     graph_level0_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(
         g, reinterpret_cast<float4*>(edges));
     return launch_status("graph_level0_kernel");
+}
+
+}  // extern "C"
+
+namespace ffx {
+namespace {
+
+__global__ void __launch_bounds__(256) dot_kernel(int64_t n, const float* __restrict__ a,
+                                                 const float* __restrict__ b, double scale, double* out) {
+    double acc = 0.0;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        acc += (double)a[i] * (double)b[i];
+    block_sum_to(out, scale * acc);
+}
+
+unsigned flat_blocks(int64_t n) {
+    int64_t b = (n + 255) / 256;
+    return (unsigned)(b < 148 * 8 ? (b < 1 ? 1 : b) : 148 * 8);
+}
+
+}  // namespace
+}  // namespace ffx
+
+extern "C" {
+
+int ffx_graph_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega, float* p_out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && rhs && p_out && rhs != p_out, "ffx_graph_smooth_zero: invalid arguments");
+    GLvl g = make_glvl(lv);
+    graph_smooth_zero_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, rhs, omega, p_out);
+    return launch_status("graph_smooth_zero_kernel");
+}
+
+int ffx_graph_smooth_dot(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega, float* p_out,
+                         double* dot, double scale, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p_in && rhs && p_out && dot && p_in != p_out,
+                "ffx_graph_smooth_dot: invalid arguments");
+    GLvl g = make_glvl(lv);
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(dot, 0, sizeof(double), st), "ffx_graph_smooth_dot memset");
+    if (e) return e;
+    graph_smooth_dot_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, st>>>(g, p_in, rhs, omega, p_out, dot,
+                                                                                 scale);
+    return launch_status("graph_smooth_dot_kernel");
+}
+
+int ffx_pcg_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old, const double* rz_new,
+                            const double* rz_old, float* p_out, float* q, double* pq, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && z && p_out && q && pq && (!rz_old || (rz_new && p_old)) && p_out != p_old &&
+                p_out != z && q != z, "ffx_pcg_direction_apply: invalid arguments");
+    GLvl g = make_glvl(lv);
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(pq, 0, sizeof(double), st), "ffx_pcg_direction_apply memset");
+    if (e) return e;
+    pcg_direction_apply_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, st>>>(g, z, p_old, rz_new, rz_old,
+                                                                                    p_out, q, pq);
+    return launch_status("pcg_direction_apply_kernel");
+}
+
+int ffx_pcg_update(int64_t count, const double* rz, const double* pq, float* x, const float* p, float* res,
+                   const float* q, float* resmax, void* stream) {
+    FFX_REQUIRE(count >= 1 && rz && pq && x && p && res && q && resmax, "ffx_pcg_update: invalid arguments");
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(resmax, 0, sizeof(float), st), "ffx_pcg_update memset");
+    if (e) return e;
+    pcg_update_kernel<<<flat_blocks(count), 256, 0, st>>>(count, rz, pq, x, p, res, q, resmax);
+    return launch_status("pcg_update_kernel");
+}
+
+int ffx_dot(int64_t count, const float* a, const float* b, double scale, double* out, void* stream) {
+    FFX_REQUIRE(count >= 1 && a && b && out, "ffx_dot: invalid arguments");
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(double), st), "ffx_dot memset");
+    if (e) return e;
+    dot_kernel<<<flat_blocks(count), 256, 0, st>>>(count, a, b, scale, out);
+    return launch_status("dot_kernel");
 }
 
 }  // extern "C"

@@ -17,7 +17,7 @@ _REFERENCE_LIVE = {
     "source_radius", "source_rate", "dissipation", "heat_source_rate", "cooling",
     "thermal_lift", "density_weight", "pressure_iterations", "pressure_cycles"}
 _EXTENSION_LIVE = {"pressure_tolerance", "pressure_max_cycles", "mg_pre_sweeps",
-                   "mg_post_sweeps", "velocity_blend", "heat_mode"}
+                   "mg_post_sweeps", "velocity_blend", "heat_mode", "pressure_method", "solid_warm_start"}
 LIVE_FIELDS = frozenset(_REFERENCE_LIVE | _EXTENSION_LIVE)
 
 

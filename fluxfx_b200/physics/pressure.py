@@ -19,6 +19,10 @@ Extensions (all default to the reference's behaviour):
   (arithmetic is FP32 either way).
 * ``solid_warm_start`` -- reuse the previous step's pressure with colliders
   instead of the reference's cold start.
+* ``pressure_method`` -- "VCYCLE" (reference: stand-alone V-cycles) or "PCG"
+  (conjugate gradients preconditioned by the same symmetric aggregation
+  V-cycle; collider multigrid only). Both solve the same system to the same
+  tolerance.
 """
 from dataclasses import dataclass
 from math import fsum, isfinite, sqrt
@@ -36,6 +40,7 @@ _CHOICES = {
     "pressure_solver": ({"AUTO", "JACOBI", "MULTIGRID"}, "Unknown pressure solver"),
     "heat_mode": ({"RATE", "TARGET"}, "Unknown heat emission mode"),
     "storage": ({"FP32", "BF16"}, "Unknown field storage"),
+    "pressure_method": ({"VCYCLE", "PCG"}, "Unknown pressure method"),
 }
 
 _TURBULENCE_RANGES = (
@@ -94,6 +99,7 @@ class PressureSettings(ThermalSettings):
     velocity_blend: float = 0.5
     storage: str = "FP32"
     solid_warm_start: bool = False
+    pressure_method: str = "VCYCLE"
 
     def __post_init__(self):
         super().__post_init__()

@@ -257,6 +257,28 @@ int ffx_graph_coarsen(const FfxGraphLevel* fine, float* coarse_edges, int32_t* d
 /* Materialise level-0 records (4 floats per cell) from the mask. */
 int ffx_graph_level0_edges(const FfxGraphLevel* lv, float* edges, void* stream);
 
+/* --------------------------------------- Krylov acceleration (MG-PCG) */
+/* Conjugate gradients on A = -L (L the graph Laplacian of `lv`) preconditioned
+ * by the aggregation V-cycle; an extension with no counterpart in the reference,
+ * which cycles plain V-cycles (backend/solid_multigrid.py:67-76). Residuals use
+ * the multigrid convention res = rhs - L x. FP64 scalars stay on the device. */
+/* First smoothing sweep from a zero iterate (reads no iterate). */
+int ffx_graph_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega, float* p_out,
+                          void* stream);
+/* Smoothing sweep fused with *dot = scale * sum(rhs * p_out) (FP64; zeroed by the call). */
+int ffx_graph_smooth_dot(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega,
+                         float* p_out, double* dot, double scale, void* stream);
+/* p_out = z + (*rz_new / *rz_old) p_old (p_out = z when rz_old is NULL), q = A p_out,
+ * *pq = sum(p_out * q) in FP64 (zeroed by the call). p_out must not alias p_old or z. */
+int ffx_pcg_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old,
+                            const double* rz_new, const double* rz_old, float* p_out, float* q,
+                            double* pq, void* stream);
+/* alpha = *rz / *pq; x += alpha p; res += alpha q; *resmax = max|res| (zeroed by the call). */
+int ffx_pcg_update(int64_t count, const double* rz, const double* pq, float* x, const float* p,
+                   float* res, const float* q, float* resmax, void* stream);
+/* *out = scale * sum(a * b), FP64 accumulation (zeroed by the call). */
+int ffx_dot(int64_t count, const float* a, const float* b, double scale, double* out, void* stream);
+
 /* --------------------------------------------------------------- reductions */
 /* max|x| with NaN/Inf -> 3.4e38 into *out (zeroed by the call); replaces the
  * shaders/max_reduce.glsl chains of backend/timestep.py:24-33. */

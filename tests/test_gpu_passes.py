@@ -376,3 +376,54 @@ def test_invalid_arguments_are_rejected_without_launch(D):
     bad = N.FfxGrid(0, 8, 8, 1, 1, 1, 0, 0, 0)
     assert D.lib.ffx_divergence(C.byref(bad), None, 0, ptr(x), ptr(x), ptr(x), ptr(x), D.s) == N.FFX_ERR_INVALID
     assert D.lib.ffx_direct_solve(2000, ptr(x), ptr(x), 1.0, ptr(x), D.s) == N.FFX_ERR_INVALID
+
+
+def test_krylov_kernels_match_numpy(D):
+    """MG-PCG building blocks: zero-start sweep, sweep + dot, direction + apply, update."""
+    from pathlib import Path
+    gold = np.load(Path(__file__).parent / 'golden' / 'solid_hierarchy.npz')
+    shape = tuple(int(v) for v in gold['sphere_shape'])
+    extent = tuple(float(v) for v in gold['sphere_extent'])
+    nx, ny, nz = shape
+    maskb = gold['sphere_mask'].reshape(nz, ny, nx) > .5
+    edges = S.level0_edges(shape, extent, maskb)
+    solid_t = t(maskb, torch.uint8)
+    w = [float(np.float32((c / e) ** 2)) for c, e in zip(shape, extent)]
+    lv = N.FfxGraphLevel(*shape, None, ptr(solid_t), N.f3(*w))
+    rng = np.random.default_rng(21)
+    cell = (nz, ny, nx)
+    rhs = rng.uniform(-1, 1, cell).astype(np.float32)
+    p = rng.uniform(-1, 1, cell).astype(np.float32)
+    out = t(np.zeros(cell))
+    D.call('ffx_graph_smooth_zero', C.byref(lv), ptr(t(rhs)), 2 / 3, ptr(out), D.s)
+    assert_close(n(out), S.graph_smooth(np.zeros_like(p), rhs, edges), rel=1e-6)
+    dot = torch.zeros(1, dtype=torch.float64, device='cuda')
+    D.call('ffx_graph_smooth_dot', C.byref(lv), ptr(t(p)), ptr(t(rhs)), 2 / 3, ptr(out), ptr(dot), -1.0, D.s)
+    sm = S.graph_smooth(p, rhs, edges)
+    assert_close(n(out), sm, rel=1e-6)
+    assert float(dot[0]) == pytest.approx(-(rhs.astype(np.float64) * sm).sum(), rel=1e-9)
+    # direction + apply: q = A p with A = -L = diag p - nb
+    z = rng.uniform(-1, 1, cell).astype(np.float32)
+    pold = rng.uniform(-1, 1, cell).astype(np.float32)
+    rz = torch.tensor([2.0, 4.0], dtype=torch.float64, device='cuda')   # beta = 2/4
+    pn, q = t(np.zeros(cell)), t(np.zeros(cell))
+    pq = torch.zeros(1, dtype=torch.float64, device='cuda')
+    D.call('ffx_pcg_direction_apply', C.byref(lv), ptr(t(z)), ptr(t(pold)), ptr(rz[0:1]), ptr(rz[1:2]), ptr(pn),
+           ptr(q), ptr(pq), D.s)
+    dirn = (z + np.float32(0.5) * pold).astype(np.float32)
+    diag, nb = S.graph_terms(dirn, edges)
+    qe = np.where(diag > 0, diag * dirn - nb, 0)
+    assert_close(n(pn), dirn, rel=1e-6)
+    assert_close(n(q), qe, rel=1e-5)
+    assert float(pq[0]) == pytest.approx((dirn.astype(np.float64) * qe).sum(), rel=1e-5)
+    # update: alpha = rz/pq
+    x0 = rng.uniform(-1, 1, cell).astype(np.float32)
+    r0 = rng.uniform(-1, 1, cell).astype(np.float32)
+    xs, rs = t(x0), t(r0)
+    rmax = torch.zeros(1, device='cuda')
+    D.call('ffx_pcg_update', x0.size, ptr(rz[0:1]), ptr(pq), ptr(xs), ptr(pn), ptr(rs), ptr(q), ptr(rmax), D.s)
+    alpha = np.float32(2.0 / float(pq[0]))
+    assert_close(n(xs), x0 + alpha * n(pn), rel=1e-6)
+    re = r0 + alpha * n(q)
+    assert_close(n(rs), re, rel=1e-6)
+    assert float(rmax[0]) == pytest.approx(np.abs(re).max(), rel=1e-6)

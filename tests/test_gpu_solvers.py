@@ -71,7 +71,7 @@ def test_multigrid_projector_matches_oracle(D, warm):
         eo, eb, ea = ref.project(vel, dt)
         for a in range(3):
             assert_close(n(outs[a]), eo[a], what=f'velocity {a}')
-        assert_close(n(proj.after), ea, rel=1e-4, what='after')
+        assert float(np.abs(n(proj.after) - ea).max()) <= 1e-5 * float(np.abs(eb).max()), 'after'
     m = proj.metrics()
     assert m['v_cycles'] == 3 and m['levels'][-1] == (4, 4, 4) and m['ratio'] < 0.05
 
@@ -173,7 +173,10 @@ def test_smoke_step_matches_oracle(D, case):
             assert_close(n(got), exp, rel=STEP_REL, what=f'step {k} {name}')
         for a in range(3):
             assert_close(n(solver._velocity[a]), ref.velocity[a], rel=STEP_REL, what=f'step {k} velocity {a}')
-        assert_close(n(solver.projector.after), ref.after, rel=1e-4, what=f'step {k} divergence after')
+        # the divergence after projection is a residual near zero: bound its
+        # error by the scale of the divergence before projection
+        err = float(np.abs(n(solver.projector.after) - ref.after).max())
+        assert err <= 1e-5 * float(np.abs(ref.before).max()), f'step {k} divergence after: {err:.3e}'
     m = solver.measure_projection()
     assert m['step'] == 3 and math.isfinite(m['rms_after'])
     if cols:
@@ -308,3 +311,32 @@ def test_thermal_and_mac_solvers_match_oracle(D):
         solver.upload([-1.0] * grid.cells)
     with pytest.raises(ValueError):
         solver.step(0.2)
+
+
+@pytest.mark.parametrize('warm', [False, True])
+def test_pcg_reaches_the_vcycle_solution_in_fewer_cycles(D, warm):
+    """MG-PCG (extension) solves the same collider system as the reference's
+    V-cycles: to the same tolerance it gives the same projected velocity."""
+    from fluxfx_b200.backend.collision import SolidDevice
+    from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
+    grid = GridSpec((32, 32, 32))
+    cols = sphere_box_mask(grid.shape, grid.extent)
+    sd = SolidDevice(grid, cols, D)
+    base = PressureSettings(pressure_tolerance=1e-6, pressure_max_cycles=200)
+    vproj = SolidMultigridProjector(grid, base, sd)
+    pproj = SolidMultigridProjector(grid, replace(base, pressure_method='PCG', solid_warm_start=warm), sd)
+    g = S.Grid(grid.shape, grid.extent, mask=n(sd.mask).astype(bool))
+    rng = np.random.default_rng(31)
+    vel = tuple(rng.uniform(-1, 1, fs).astype(np.float32) for fs in g.face_shapes)
+    fields = [D.texture(fs, v.ravel(), nonnegative=False) for fs, v in zip(grid.face_shapes, vel)]
+    outs_v = [D.texture(fs) for fs in grid.face_shapes]
+    outs_p = [D.texture(fs) for fs in grid.face_shapes]
+    for dt in (0.02, 0.02, 0.015):
+        vproj.project(fields, outs_v, dt)
+        pproj.project(fields, outs_p, dt)
+        mv, mp = vproj.metrics(), pproj.metrics()
+        assert mv['rel_div_inf'] <= 1.5e-6 and mp['rel_div_inf'] <= 1.5e-6, (mv['rel_div_inf'], mp['rel_div_inf'])
+        assert pproj.last_cycles < vproj.last_cycles, (pproj.last_cycles, vproj.last_cycles)
+        for a in range(3):
+            scale = float(np.abs(n(outs_v[a])).max())
+            assert float(np.abs(n(outs_v[a]) - n(outs_p[a])).max()) <= 2e-5 * scale

@@ -1,0 +1,39 @@
+"""Multi-rank host logic of bench.py on CPU: world size 2 over gloo. Each rank
+runs its own replica domain; the job rate is N x steps / (max over ranks of
+the device time), and every rank takes the same collective steps."""
+import os
+
+import pytest
+import torch.multiprocessing as mp
+
+
+def _worker(rank, world, port, out):
+    import torch.distributed as dist
+    import bench
+    os.environ.update(MASTER_ADDR='127.0.0.1', MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group('gloo', rank=rank, world_size=world)
+    try:
+        elapsed = [1.0 + rank, 0.5 + 2 * rank]       # rank 1 is the slow one
+        got = bench.max_over_ranks(elapsed, world)
+        out[rank] = (got, bench.job_rate(world, 10, got[0]))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_job_rate_world_size_2():
+    world = 2
+    port = 29500 + os.getpid() % 1000
+    manager = mp.Manager()
+    out = manager.dict()
+    mp.spawn(_worker, args=(world, port, out), nprocs=world, join=True)
+    for rank in range(world):
+        got, rate = out[rank]
+        assert got == [2.0, 2.5]
+        assert rate == pytest.approx(world * 10 / 2.0)
+
+
+def test_single_rank_needs_no_process_group():
+    import bench
+    assert bench.max_over_ranks([3.0, 4.0], 1) == [3.0, 4.0]
+    assert bench.job_rate(1, 20, 2.0) == 10.0
