@@ -391,6 +391,69 @@ __global__ void __launch_bounds__(256) graph_smooth_kernel(GLvl g, const float* 
     out[i] = diag > 0.f ? __ldg(p + i) * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
 }
 
+// Level-0 (mask-derived) sweep, streamed along z: each thread owns one (x, y)
+// column of kZ cells and carries p and the fluid flag of the z-1 / z / z+1
+// cells in registers, so every cell loads p and the mask once for its own z
+// neighbours; x/y neighbours come from the L1 lines its warp-mates load. The
+// operator terms are summed in the same order as graph_terms.
+constexpr int kZ = 8;
+__global__ void __launch_bounds__(256) graph_smooth_level0_kernel(GLvl g, const float* __restrict__ p,
+                                                                 const float* __restrict__ rhs, float omega,
+                                                                 float* out) {
+    const int x = blockIdx.x * kBX + threadIdx.x, y = blockIdx.y * kBY + threadIdx.y;
+    if (x >= g.nx || y >= g.ny) return;
+    const int z0 = blockIdx.z * kZ;
+    const int sy = g.nx, sz = g.nx * g.ny;
+    int i = x + g.nx * (y + g.ny * z0);
+    const float wx = g.w[0], wy = g.w[1], wz = g.w[2];
+    float p_lo = 0.f, p_c = __ldg(p + i);
+    bool f_lo = false, f_c = __ldg(g.solid + i) == 0;
+    if (z0 > 0) {
+        p_lo = __ldg(p + i - sz);
+        f_lo = __ldg(g.solid + i - sz) == 0;
+    }
+    const int zend = min(z0 + kZ, g.nz);
+    for (int z = z0; z < zend; ++z, i += sz) {
+        const bool up = z + 1 < g.nz;
+        const float p_hi = up ? __ldg(p + i + sz) : 0.f;
+        const bool f_hi = up && __ldg(g.solid + i + sz) == 0;
+        float diag = 0.f, nb = 0.f;
+        if (x > 0) {
+            const float w = (f_c && __ldg(g.solid + i - 1) == 0) ? wx : 0.f;
+            diag = diag + w;
+            nb = nb + w * __ldg(p + i - 1);
+        }
+        if (x + 1 < g.nx) {
+            const float w = (f_c && __ldg(g.solid + i + 1) == 0) ? wx : 0.f;
+            diag = diag + w;
+            nb = nb + w * __ldg(p + i + 1);
+        }
+        if (y > 0) {
+            const float w = (f_c && __ldg(g.solid + i - sy) == 0) ? wy : 0.f;
+            diag = diag + w;
+            nb = nb + w * __ldg(p + i - sy);
+        }
+        if (y + 1 < g.ny) {
+            const float w = (f_c && __ldg(g.solid + i + sy) == 0) ? wy : 0.f;
+            diag = diag + w;
+            nb = nb + w * __ldg(p + i + sy);
+        }
+        if (z > 0) {
+            const float w = (f_c && f_lo) ? wz : 0.f;
+            diag = diag + w;
+            nb = nb + w * p_lo;
+        }
+        if (up) {
+            const float w = (f_c && f_hi) ? wz : 0.f;
+            diag = diag + w;
+            nb = nb + w * p_hi;
+        }
+        out[i] = diag > 0.f ? p_c * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
+        p_lo = p_c; p_c = p_hi;
+        f_lo = f_c; f_c = f_hi;
+    }
+}
+
 __device__ __forceinline__ float graph_res(const GLvl& g, const float* __restrict__ p, const float* __restrict__ rhs,
                                            int i, int x, int y, int z) {
     float diag, nb;
@@ -781,6 +844,11 @@ int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rh
                      void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p_in && rhs && p_out && p_in != p_out, "ffx_graph_smooth: invalid arguments");
     GLvl g = make_glvl(lv);
+    if (!g.edges) {
+        dim3 grid = cell_grid(g.nx, g.ny, (g.nz + kZ - 1) / kZ);
+        graph_smooth_level0_kernel<<<grid, cell_block(), 0, as_stream(stream)>>>(g, p_in, rhs, omega, p_out);
+        return launch_status("graph_smooth_level0_kernel");
+    }
     graph_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, p_in, rhs, omega,
                                                                                              p_out);
     return launch_status("graph_smooth_kernel");
