@@ -208,15 +208,15 @@ class Run:
         for _ in range(count):
             self.step()
 
-    def timed(self, count, instrument=False):
+    def timed(self, count, passes=False):
+        """``count`` steps as the solver runs them (CUDA graphs on). With
+        ``passes`` an event is recorded between the passes of each step (a few
+        events per step, none inside the pressure solve)."""
         import torch
-        from fluxfx_b200.backend import solid_multigrid as SM
         from fluxfx_b200.backend.device import PassTimer
         stream = self.device.stream
         solver = self.solver
-        self.kernel_timer = SM.KernelTimer(stream) if instrument else None
-        self.pass_timer = PassTimer(stream) if instrument else None
-        solver.projector.timer = self.kernel_timer
+        self.pass_timer = PassTimer(stream) if passes else None
         solver.pass_timer = self.pass_timer
         self.cycles = []
         calls0 = self.device.calls
@@ -229,9 +229,22 @@ class Run:
         end.record(stream)
         torch.cuda.synchronize()
         self.launches = self.device.calls - calls0
-        solver.projector.timer = None
         solver.pass_timer = None
         return start.elapsed_time(end) / 1e3
+
+    def smoother_sample(self, count):
+        """Events around every level-0 smoother launch over ``count`` further
+        steps (these steps run eagerly, without graphs, so that each sweep can
+        be bracketed). Returns (average ms per launch, launches)."""
+        import torch
+        from fluxfx_b200.backend import solid_multigrid as SM
+        timer = SM.KernelTimer(self.device.stream)
+        self.solver.projector.timer = timer
+        for _ in range(count):
+            self.step()
+        torch.cuda.synchronize()
+        self.solver.projector.timer = None
+        return timer.average_ms(), timer.count
 
     def e2e(self, count):
         import torch
@@ -254,8 +267,10 @@ class Run:
 
 
 def run_b200(args):
+    import ctypes as C
     import torch
     import torch.distributed as dist
+    from fluxfx_b200 import _native as N
     from fluxfx_b200.backend.device import CudaDevice
 
     world = int(os.environ.get('WORLD_SIZE', '1'))
@@ -276,15 +291,15 @@ def run_b200(args):
         dist.barrier()
     clocks = ClockSampler(local)
     clocks.start()
-    elapsed = run.timed(args.steps, instrument=True)
+    elapsed = run.timed(args.steps, passes=True)
     clock_info = clocks.stop()
     passes = run.pass_timer.totals_ms()
-    smooth_ms = run.kernel_timer.average_ms()
-    smooth_launches = run.kernel_timer.count
+    head = dict(cycles=run.cycles, launches=run.launches)
     rel_div = run.solver.measure_projection()['rel_div_inf']
     e2e_steps = max(1, args.steps // 2)
     e2e_time, d2h = run.e2e(e2e_steps)
-    head = dict(cycles=run.cycles, launches=run.launches)
+    smooth_ms, smooth_launches = run.smoother_sample(min(args.steps, 4))
+    h2d = 2 * C.sizeof(N.FfxSources)   # the emitter table, passed with the two launches that emit
     run.close()
 
     # --- plain FP32 reference algorithm, same scene and warm-up ----------------
@@ -335,14 +350,19 @@ def run_b200(args):
                        job_rate(world, args.steps, elapsed) / job_rate(world, plain['steps'], p_el)},
             "cell_updates_per_s": world * args.steps * cells / elapsed,
             "passes": pass_report,
-            "e2e": {"value": job_rate(world, e2e_steps, e2e_time), "unit": UNIT, "h2d_bytes_per_step": 0,
-                    "d2h_bytes_per_step": d2h},
+            "e2e": {"value": job_rate(world, e2e_steps, e2e_time), "unit": UNIT, "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h,
+                    "path": "DenseProjectedSmoke.step with the emitter list each step (packed into the launch "
+                            "parameters of the two emitting passes) + the step's density field read back into "
+                            "pinned host memory"},
             "gpu_launches": head['launches'],
-            "roofline": {"bound": "hbm", "kernel": "graph_smooth_kernel (level-0 aggregation multigrid sweep)",
+            "roofline": {"bound": "hbm", "kernel": "graph_smooth_level0_kernel (level-0 aggregation multigrid sweep)",
                          "achieved": achieved, "peak": hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)",
                          "unit": "GB/s", "frac": (achieved / hbm) if achieved else None, "traffic": None,
                          "algorithmic_bytes_per_launch": bytes_per_launch, "avg_launch_ms": smooth_ms,
-                         "launches_timed": smooth_launches},
+                         "launches_timed": smooth_launches,
+                         "timing": "CUDA events around each level-0 sweep over an eager segment of "
+                                   "the same run after the timed steps"},
             "clocks": clock_info,
         }
         if args.cpu_baseline:

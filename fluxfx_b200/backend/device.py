@@ -83,6 +83,30 @@ class CudaDevice:
     def synchronize(self):
         self.stream.synchronize()
 
+    def capture(self, fn):
+        """Record the passes ``fn`` enqueues into a CUDA graph (not executed now).
+
+        Capture runs on a side stream: every native call made by ``fn`` goes to
+        ``self.stream``, which points at that stream for the duration, and torch
+        ops inside ``fn`` follow the capturing stream. ``fn`` must allocate
+        nothing and must not synchronise."""
+        graph = torch.cuda.CUDAGraph()
+        side = torch.cuda.Stream(self.device)
+        side.wait_stream(self.stream)
+        saved = self.stream
+        self.stream = side
+        try:
+            with torch.cuda.graph(graph, stream=side):
+                fn()
+        finally:
+            self.stream = saved
+        self.stream.wait_stream(side)
+        return graph
+
+    def replay(self, graph):
+        with torch.cuda.stream(self.stream):
+            graph.replay()
+
     def texture(self, shape, values=None, *, nonnegative=True, channels=1, dtype=torch.float32):
         if channels not in (1, 4):
             raise ValueError("Only scalar or four-channel fields are supported")

@@ -98,8 +98,7 @@ class MultigridPressureProjector(PressureProjector):
         if index == len(self.levels) - 1:
             if self.coarse_matrix is not None:
                 self.device.call('ffx_direct_solve', prod(level['shape']), ptr(self.coarse_matrix),
-                                 ptr(level['rhs']), dt, ptr(level['q']), s)
-                level['p'], level['q'] = level['q'], level['p']
+                                 ptr(level['rhs']), dt, ptr(level['p']), s)
                 self.last_coarse_solves += 1
             else:
                 self.smooth(level, dt, 80)

@@ -114,10 +114,10 @@ class PressureProjector:
         solve_dt = 1.0 if impulse else dt
         previous_solve_dt = (1.0 if previous_dt is not None else None) if impulse else previous_dt
         if impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
-            # The incremental pressure force scales with physical dt: rescale the guess.
+            # The incremental pressure force scales with physical dt: rescale the
+            # guess (in place, so the pressure keeps its buffer from step to step).
             self.device.call('ffx_scale', self.pressure.numel(), ptr(self.pressure), dt / previous_dt,
-                             ptr(self.spare), self.device.s)
-            self.pressure, self.spare = self.spare, self.pressure
+                             ptr(self.pressure), self.device.s)
         self.solve_pressure(solve_dt, previous_solve_dt)
         self.device.call('ffx_gradient', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
                          ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),

@@ -114,6 +114,8 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.post_sweeps = s.mg_post_sweeps or 4
         self.last_cycles = 0
         self.timer = None
+        self.use_graphs = True
+        self._graphs = {}
         self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
 
     @property
@@ -143,9 +145,10 @@ class SolidMultigridProjector(SolidPressureProjector):
         dev = self.device
         if index == len(self.levels) - 1:
             if self.coarse_matrix is not None:
+                # written straight into p (the iterate is replaced, not updated),
+                # so buffer roles repeat from one cycle to the next
                 dev.call('ffx_direct_solve', prod(level['shape']), ptr(self.coarse_matrix), ptr(level['rhs']), 1.0,
-                         ptr(level['q']), dev.s)
-                level['p'], level['q'] = level['q'], level['p']
+                         ptr(level['p']), dev.s)
             else:
                 if zero_init:
                     level['p'].zero_()
@@ -195,16 +198,36 @@ class SolidMultigridProjector(SolidPressureProjector):
                          ptr(self._rmax[0:1]), self.device.s)
         return float(self._rmax[0].item())
 
+    # ------------------------------------------------------------ graph replay
+    def _replayed(self, key, fn):
+        """Run ``fn`` (a fixed sequence of passes over fixed buffers) through a
+        CUDA graph captured on first use for this ``key``. Every level swaps its
+        p/q roles an even number of times per cycle, so the buffers a cycle
+        touches are the same every time it runs with the same level-0 roles."""
+        if not self.use_graphs or self.timer is not None:
+            fn()
+            return
+        dev = self.device
+        entry = self._graphs.get(key)
+        if entry is None:
+            sweeps, calls = self.last_iterations, dev.calls
+            graph = dev.capture(fn)
+            entry = (graph, self.last_iterations - sweeps, dev.calls - calls)
+            self.last_iterations, dev.calls = sweeps, calls
+            self._graphs[key] = entry
+        dev.replay(entry[0])
+        self.last_iterations += entry[1]
+        dev.calls += entry[2]   # the native passes the graph launches
+
     # ------------------------------------------------------------ Krylov solve
     def _krylov_buffers(self):
         if getattr(self, '_kry', None) is None:
             dev = self.device
             shape = self.levels[0]['shape']
-            cap = self.settings.pressure_max_cycles + 8
             self._kry = dict(res=dev.texture(shape), z=dev.texture(shape), z2=dev.texture(shape),
                              p=[dev.texture(shape), dev.texture(shape)], q=dev.texture(shape),
-                             rz=torch.zeros(cap, dtype=torch.float64, device=dev.device),
-                             pq=torch.zeros(cap, dtype=torch.float64, device=dev.device),
+                             rz=torch.zeros(2, dtype=torch.float64, device=dev.device),   # [current, previous]
+                             pq=torch.zeros(1, dtype=torch.float64, device=dev.device),
                              rmax=torch.zeros(1, dtype=torch.float32, device=dev.device))
         return self._kry
 
@@ -219,37 +242,43 @@ class SolidMultigridProjector(SolidPressureProjector):
         L0['p'], L0['q'], L0['rhs'] = saved
         return z
 
+    def _pcg_iteration(self, B, x, k):
+        """z = M res; p = z + beta p_old; q = A p; x += alpha p; res += alpha q."""
+        dev = self.device
+        g = C.byref(self.levels[0]['graph'])
+        z = self._precondition(B['res'], B, B['rz'][0:1])
+        p_new, p_old = B['p'][k % 2], B['p'][(k + 1) % 2]
+        first = k == 0
+        dev.call('ffx_pcg_direction_apply', g, ptr(z), None if first else ptr(p_old), ptr(B['rz'][0:1]),
+                 None if first else ptr(B['rz'][1:2]), ptr(p_new), ptr(B['q']), ptr(B['pq']), dev.s)
+        dev.call('ffx_pcg_update', x.numel(), ptr(B['rz'][0:1]), ptr(B['pq']), ptr(x), ptr(p_new), ptr(B['res']),
+                 ptr(B['q']), ptr(B['rmax']), dev.s)
+        B['rz'][1:2].copy_(B['rz'][0:1])
+
     def _solve_krylov(self, scale, budget):
         """Conjugate gradients on A = -L preconditioned by the aggregation
         V-cycle, until max|rhs - L x| <= tol * max|rhs| (or ``budget`` cycles)."""
         s = self.settings
         dev = self.device
         B = self._krylov_buffers()
-        L0 = self.levels[0]
-        g = C.byref(L0['graph'])
+        g = C.byref(self.levels[0]['graph'])
         x = self.pressure
         n = x.numel()
         tol = s.pressure_tolerance * scale if s.pressure_tolerance > 0 else -1.0
-        res = B['res']
-        for restart in range(2):
-            dev.call('ffx_graph_residual', g, ptr(x), ptr(self.before), ptr(res), dev.s)
-            dev.call('ffx_max_abs', n, N.FFX_F32, ptr(res), ptr(B['rmax']), dev.s)
+        for _restart in range(2):
+            dev.call('ffx_graph_residual', g, ptr(x), ptr(self.before), ptr(B['res']), dev.s)
+            dev.call('ffx_max_abs', n, N.FFX_F32, ptr(B['res']), ptr(B['rmax']), dev.s)
             if float(B['rmax'].item()) <= tol:
                 return
             k = 0
-            p_old = None
             while self.last_cycles < budget:
-                z = self._precondition(res, B, B['rz'][k:k + 1])
+                if k == 0:
+                    self._pcg_iteration(B, x, 0)
+                else:
+                    self._replayed(('pcg', x.data_ptr(), k % 2), lambda kk=k: self._pcg_iteration(B, x, kk))
                 self.last_cycles += 1
-                p_new = B['p'][k % 2]
-                dev.call('ffx_pcg_direction_apply', g, ptr(z), ptr(p_old), ptr(B['rz'][k:k + 1]),
-                         ptr(B['rz'][k - 1:k]) if k > 0 else None, ptr(p_new), ptr(B['q']),
-                         ptr(B['pq'][k:k + 1]), dev.s)
-                dev.call('ffx_pcg_update', n, ptr(B['rz'][k:k + 1]), ptr(B['pq'][k:k + 1]), ptr(x), ptr(p_new),
-                         ptr(res), ptr(B['q']), ptr(B['rmax']), dev.s)
-                p_old = p_new
                 k += 1
-                if float(B['rmax'].item()) <= tol or k + 1 >= B['rz'].numel():
+                if float(B['rmax'].item()) <= tol:
                     break
             if tol < 0 or self.last_cycles >= budget:
                 return
@@ -259,6 +288,10 @@ class SolidMultigridProjector(SolidPressureProjector):
                 return
 
     def solve_pressure(self, dt, previous_dt):
+        with torch.cuda.stream(self.device.stream):
+            self._solve(dt, previous_dt)
+
+    def _solve(self, dt, previous_dt):
         s = self.settings
         self.last_cycles = 0
         if len(self.levels) == 1:
@@ -281,9 +314,10 @@ class SolidMultigridProjector(SolidPressureProjector):
                 self._solve_krylov(scale, budget)
             self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
             return
+        one_cycle = lambda: self._replayed(('vcycle', self.levels[0]['p'].data_ptr()), lambda: self.cycle(0))
         if s.pressure_tolerance <= 0:
             for _ in range(budget):
-                self.cycle(0)
+                one_cycle()
                 self.last_cycles += 1
         else:
             self.device.call('ffx_max_abs', self.before.numel(), N.FFX_F32, ptr(self.before),
@@ -293,7 +327,7 @@ class SolidMultigridProjector(SolidPressureProjector):
                 self.levels[0]['p'].zero_()
             else:
                 while self.last_cycles < s.pressure_max_cycles and self._residual_max() > s.pressure_tolerance * scale:
-                    self.cycle(0)
+                    one_cycle()
                     self.last_cycles += 1
         self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
 
@@ -322,6 +356,8 @@ class SolidMultigridProjector(SolidPressureProjector):
             'aggregation': 'connected_children_only'}
 
     def close(self):
+        self._graphs = {}
+        self._kry = None
         self.levels = []
         self.coarse_matrix = self.coarse_kernel = None
         super().close()

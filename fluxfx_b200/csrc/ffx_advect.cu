@@ -41,16 +41,16 @@ __device__ __forceinline__ bool face_coords(const Dev& d, FaceIdx& f) {
 
 // Midpoint backtrace p -> departure (transport_face.glsl:8-17 and the same
 // lines of every advection shader); clipped at colliders when MASK.
-template <typename T, bool MASK>
+template <typename T, bool MASK, bool P2 = false>
 __device__ __forceinline__ F3 backtrace(const Dev& d, const Faces<T>& F, const uint8_t* solid, const uint8_t* halo,
                                         F3 p, F3 v0,
                                         float dt) {
     float s = 0.5f * dt;
     F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
-    if (MASK) mid = clip_solid_trace(d, solid, halo, p, mid);
-    F3 vm = velocity_at(d, F, mid);
+    if (MASK) mid = clip_solid_trace<P2>(d, solid, halo, p, mid);
+    F3 vm = velocity_at<T, P2>(d, F, mid);
     F3 dep = {p.x - dt * vm.x, p.y - dt * vm.y, p.z - dt * vm.z};
-    if (MASK) dep = clip_solid_trace(d, solid, halo, p, dep);
+    if (MASK) dep = clip_solid_trace<P2>(d, solid, halo, p, dep);
     return dep;
 }
 
@@ -103,7 +103,7 @@ __device__ __forceinline__ float fetch_closed(const Dev& d, const T* __restrict_
 }
 
 // ------------------------------------------------------------ face predictor
-template <typename T, bool MASK>
+template <typename T, bool MASK, bool P2>
 __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const uint8_t* __restrict__ solid,
                                                                   const uint8_t* __restrict__ halo,
                                                                   Faces<T> F, float dt, T* pu, T* pv, T* pw) {
@@ -116,10 +116,11 @@ __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const u
     }
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
-    F3 v0 = velocity_at(d, F, p);
-    F3 dep = backtrace<T, MASK>(d, F, solid, halo, p, v0, dt);
+    F3 v0 = velocity_at<T, P2>(d, F, p);
+    F3 dep = backtrace<T, MASK, P2>(d, F, solid, halo, p, v0, dt);
     const T* src = f.axis == 0 ? F.u : (f.axis == 1 ? F.v : F.w);
-    float value = sample_face(src, f.sx, f.sy, f.sz, dep.x / d.h[0] - ox, dep.y / d.h[1] - oy, dep.z / d.h[2] - oz);
+    float value = sample_face(src, f.sx, f.sy, f.sz, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
+                                dv_h<P2>(d, dep.z, 2) - oz);
     Store<T>::st(out, f.i, value);
 }
 
@@ -139,7 +140,7 @@ struct VelParams {
     SrcDev src;
 };
 
-template <typename T, bool MASK>
+template <typename T, bool MASK, bool P2>
 __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
     const Dev& d = P.d;
     FaceIdx f;
@@ -150,13 +151,14 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
     float value = 0.f;
     if (!blocked) {
         float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
-        F3 p = {((float)f.x + off[0]) * d.e[0] / d.nf[0], ((float)f.y + off[1]) * d.e[1] / d.nf[1],
-                ((float)f.z + off[2]) * d.e[2] / d.nf[2]};
-        F3 v0 = velocity_at(d, P.F, p);
-        F3 dep = backtrace<T, MASK>(d, P.F, P.solid, P.halo, p, v0, dt);
+        F3 p = {dv_n<P2>(d, ((float)f.x + off[0]) * d.e[0], 0), dv_n<P2>(d, ((float)f.y + off[1]) * d.e[1], 1),
+                dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
+        F3 v0 = velocity_at<T, P2>(d, P.F, p);
+        F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
-        float qx = dep.x / d.h[0] - off[0], qy = dep.y / d.h[1] - off[1], qz = dep.z / d.h[2] - off[2];
+        float qx = dv_h<P2>(d, dep.x, 0) - off[0], qy = dv_h<P2>(d, dep.y, 1) - off[1],
+              qz = dv_h<P2>(d, dep.z, 2) - off[2];
         float low = sample_face(orig, f.sx, f.sy, f.sz, qx, qy, qz);
         value = low;
         if (P.corrected) {
@@ -169,15 +171,15 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
             }
             float s = 0.5f * dt;
             F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
-            F3 vm2 = velocity_at(d, P.F, mid2);
+            F3 vm2 = velocity_at<T, P2>(d, P.F, mid2);
             F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
             bool ok = !(dep.x < lob[0] || dep.y < lob[1] || dep.z < lob[2] || dep.x > hib[0] || dep.y > hib[1] ||
                         dep.z > hib[2] || arr.x < lob[0] || arr.y < lob[1] || arr.z < lob[2] || arr.x > hib[0] ||
                         arr.y > hib[1] || arr.z > hib[2]);
-            if (MASK && ok) ok = safe_solid_correction(d, P.solid, P.halo, p, dep, mid2, arr);
+            if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
             if (ok) {
-                float pa = sample_face(pred, f.sx, f.sy, f.sz, arr.x / d.h[0] - off[0], arr.y / d.h[1] - off[1],
-                                       arr.z / d.h[2] - off[2]);
+                float pa = sample_face(pred, f.sx, f.sy, f.sz, dv_h<P2>(d, arr.x, 0) - off[0], dv_h<P2>(d, arr.y, 1) - off[1],
+                                       dv_h<P2>(d, arr.z, 2) - off[2]);
                 float val = Store<T>::ld(pred, f.i) + 0.5f * (Store<T>::ld(orig, f.i) - pa);
                 int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
                 int sxy = f.sx * f.sy;
@@ -198,7 +200,7 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
         }
         const SrcDev& S = P.src;
         if (S.count < 0) {
-            float w = emission_weight(p, S.center, S.start, S.radius, S.single_solid != 0);
+            float w = single_weight(S, p);
             float bl = 1.f - expf(-S.coupling * dt * w);
             value = value * (1.f - bl) + comp(S.jet, axis) * bl;
         } else if (S.count > 0) {
@@ -274,7 +276,7 @@ struct ScalarXport {
     T* out[3];
 };
 
-template <typename T, bool MASK>
+template <typename T, bool MASK, bool P2>
 __global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
     const Dev& d = P.d;
     int x, y, z;
@@ -285,9 +287,10 @@ __global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid
         return;
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-    F3 v0 = velocity_at(d, P.F, p);
-    F3 dep = backtrace<T, MASK>(d, P.F, P.solid, P.halo, p, v0, P.dt);
-    float qx = dep.x / d.h[0] - 0.5f, qy = dep.y / d.h[1] - 0.5f, qz = dep.z / d.h[2] - 0.5f;
+    F3 v0 = velocity_at<T, P2>(d, P.F, p);
+    F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, P.dt);
+    float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
+          qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     for (int c = 0; c < P.count; ++c)
         Store<T>::st(P.out[c], i, sample_closed<T, MASK>(d, P.solid, P.in[c], qx, qy, qz));
 }
@@ -315,7 +318,7 @@ struct ScalarFinal {
     SrcDev src;
 };
 
-template <typename T, bool MASK>
+template <typename T, bool MASK, bool P2>
 __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
     const Dev& d = P.d;
     int x, y, z;
@@ -327,22 +330,23 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
         } else {
             const float dt = P.dt;
             F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-            F3 v0 = velocity_at(d, P.F, p);
-            F3 dep = backtrace<T, MASK>(d, P.F, P.solid, P.halo, p, v0, dt);
-            float qx = dep.x / d.h[0] - 0.5f, qy = dep.y / d.h[1] - 0.5f, qz = dep.z / d.h[2] - 0.5f;
+            F3 v0 = velocity_at<T, P2>(d, P.F, p);
+            F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
+            float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
+                  qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
             bool ok = false;
             if (P.corrected) {
                 // correct_scalar.glsl:1-21
                 float s = 0.5f * dt;
                 F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
-                F3 vm2 = velocity_at(d, P.F, mid2);
+                F3 vm2 = velocity_at<T, P2>(d, P.F, mid2);
                 F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
                 float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
                 float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
                 ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
                        dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
                        arr.y > hb[1] || arr.z > hb[2]);
-                if (MASK && ok) ok = safe_solid_correction(d, P.solid, P.halo, p, dep, mid2, arr);
+                if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
             }
             int bx = 0, by = 0, bz = 0;
             if (ok) { bx = (int)floorf(qx); by = (int)floorf(qy); bz = (int)floorf(qz); }
@@ -364,7 +368,7 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
                 }
                 value = value * expf(-C.decay * dt);
                 if (S.count < 0) {
-                    float w = emission_weight(p, S.center, S.start, S.radius, S.single_solid != 0);
+                    float w = single_weight(S, p);
                     value = C.target >= 0.f ? fmaxf(value, C.target * w) : value + dt * C.rate * w;
                 } else {
                     float tgt = 0.f;
@@ -456,6 +460,18 @@ __global__ void mac_advect_density_kernel(OpenParams P, Faces<T> F, const T* in,
     Store<T>::st(out, i, value + P.dt * P.rate * w * w);
 }
 
+// Launch the (collider mask, power-of-two grid) instantiation of a kernel.
+#define FFX_DISPATCH_MASK_P2(mask, p2, M, P, ...)             \
+    do {                                                       \
+        if (mask) {                                            \
+            if (p2) { constexpr bool M = true, P = true; __VA_ARGS__; }   \
+            else { constexpr bool M = true, P = false; __VA_ARGS__; }     \
+        } else {                                               \
+            if (p2) { constexpr bool M = false, P = true; __VA_ARGS__; }  \
+            else { constexpr bool M = false, P = false; __VA_ARGS__; }    \
+        }                                                      \
+    } while (0)
+
 bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s->solid && s->halo); }
 bool has_mask(const FfxSolids* s) { return s && s->solid; }
 
@@ -477,10 +493,9 @@ int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const 
     const uint8_t* solid = has_mask(s) ? s->solid : nullptr;
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (solid) face_predictor_kernel<T, true><<<blocks, threads, 0, st>>>(d, solid, s->halo, F, dt, (T*)pu, (T*)pv,
-                                                                               (T*)pw);
-        else face_predictor_kernel<T, false><<<blocks, threads, 0, st>>>(d, nullptr, nullptr, F, dt, (T*)pu, (T*)pv,
-                                                                         (T*)pw);
+        const uint8_t* halo = solid ? s->halo : nullptr;
+        FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P, (face_predictor_kernel<T, M, P><<<blocks, threads, 0, st>>>(
+            d, solid, halo, F, dt, (T*)pu, (T*)pv, (T*)pw)));
     });
     return launch_status("face_predictor_kernel");
 }
@@ -516,10 +531,10 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const
         P.density = (const T*)density;
         P.temperature = (const T*)temperature;
         P.out[0] = (T*)ou; P.out[1] = (T*)ov; P.out[2] = (T*)ow;
-        P.src = make_src(src);
+        const float extent[3] = {g->ex, g->ey, g->ez};
+        P.src = make_src(src, extent);
         if (!src) P.src.count = 0;
-        if (P.solid) advect_velocity_kernel<T, true><<<blocks, threads, 0, st>>>(P);
-        else advect_velocity_kernel<T, false><<<blocks, threads, 0, st>>>(P);
+        FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_velocity_kernel<T, M, Q><<<blocks, threads, 0, st>>>(P)));
     });
     return launch_status("advect_velocity_kernel");
 }
@@ -570,8 +585,7 @@ int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, cons
             P.in[c] = c < count ? (const T*)in[c] : nullptr;
             P.out[c] = c < count ? (T*)out[c] : nullptr;
         }
-        if (P.solid) scalar_transport_kernel<T, true><<<grid, block, 0, st>>>(P);
-        else scalar_transport_kernel<T, false><<<grid, block, 0, st>>>(P);
+        FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (scalar_transport_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
     });
     return launch_status("scalar_transport_kernel");
 }
@@ -619,9 +633,9 @@ int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const 
             P.ch[c] = C;
         }
         P.maxima = maxima;
-        P.src = make_src(src);
-        if (P.solid) advect_scalars_kernel<T, true><<<grid, block, 0, st>>>(P);
-        else advect_scalars_kernel<T, false><<<grid, block, 0, st>>>(P);
+        const float extent[3] = {g->ex, g->ey, g->ez};
+        P.src = make_src(src, extent);
+        FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_scalars_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
     });
     return launch_status("advect_scalars_kernel");
 }

@@ -10,6 +10,8 @@
 #include <cuda_bf16.h>
 #include <stdint.h>
 
+#include <cmath>
+
 #include "../../include/ffx.h"
 
 namespace ffx {
@@ -36,7 +38,14 @@ struct Dev {
     float e[3];              // extent
     float h[3];              // e / n (FP32 division, as the shaders compute it)
     float inv[3];            // host-side 1/h rounded to FP32 (the invCell uniform)
+    float re[3], rn[3], rh[3];   // 1/e, 1/n, 1/h (exact when pow2)
+    int pow2;                // every e, n and h is a power of two
 };
+
+inline bool is_pow2f(float v) {
+    int ex = 0;
+    return v > 0.f && std::frexp(v, &ex) == 0.5f;
+}
 
 inline Dev make_dev(const FfxGrid& g) {
     Dev d;
@@ -45,13 +54,32 @@ inline Dev make_dev(const FfxGrid& g) {
     float e[3] = {g.ex, g.ey, g.ez};
     double e64[3] = {g.ex, g.ey, g.ez};
     float given[3] = {g.ix, g.iy, g.iz};
+    d.pow2 = 1;
     for (int i = 0; i < 3; ++i) {
         d.nf[i] = (float)n[i];
         d.e[i] = e[i];
         d.h[i] = e[i] / (float)n[i];
         d.inv[i] = given[i] != 0.f ? given[i] : (float)(1.0 / (e64[i] / (double)n[i]));
+        d.re[i] = 1.f / e[i];
+        d.rn[i] = 1.f / d.nf[i];
+        d.rh[i] = 1.f / d.h[i];
+        if (!(is_pow2f(e[i]) && is_pow2f(d.nf[i]) && is_pow2f(d.h[i]))) d.pow2 = 0;
     }
     return d;
+}
+
+// Division by the grid constants e, n and h. When every one of them is a power
+// of two (e.g. a 256^3 unit cube) dividing is an exact rescaling, so it is done
+// as a multiplication by the exact reciprocal -- bit-identical to the IEEE
+// division, and several times cheaper. P2 is chosen per launch from Dev::pow2.
+template <bool P2> __device__ __forceinline__ float dv_e(const Dev& d, float x, int i) {
+    return P2 ? x * d.re[i] : x / d.e[i];
+}
+template <bool P2> __device__ __forceinline__ float dv_n(const Dev& d, float x, int i) {
+    return P2 ? x * d.rn[i] : x / d.nf[i];
+}
+template <bool P2> __device__ __forceinline__ float dv_h(const Dev& d, float x, int i) {
+    return P2 ? x * d.rh[i] : x / d.h[i];
 }
 
 // Every field has fewer than 2^31 elements (checked at the entry points), so
@@ -120,11 +148,11 @@ struct Faces {
 };
 
 // Staggered velocity at a physical point (mac_sample.glsl:20-26).
-template <typename T>
+template <typename T, bool P2 = false>
 __device__ __forceinline__ F3 velocity_at(const Dev& d, const Faces<T>& F, F3 p) {
-    float qx = p.x * d.nf[0] / d.e[0];
-    float qy = p.y * d.nf[1] / d.e[1];
-    float qz = p.z * d.nf[2] / d.e[2];
+    float qx = dv_e<P2>(d, p.x * d.nf[0], 0);
+    float qy = dv_e<P2>(d, p.y * d.nf[1], 1);
+    float qz = dv_e<P2>(d, p.z * d.nf[2], 2);
     F3 r;
     r.x = sample_face(F.u, d.nx + 1, d.ny, d.nz, qx, qy - 0.5f, qz - 0.5f);
     r.y = sample_face(F.v, d.nx, d.ny + 1, d.nz, qx - 0.5f, qy, qz - 0.5f);
@@ -154,6 +182,7 @@ __device__ __forceinline__ bool solid_face(const Dev& d, const uint8_t* __restri
 // overshoot past the end from rounding of the crossing parameters -- is fluid,
 // so the loop would run to t >= 1 and return b / count * extent. That value is
 // returned directly; it is bit-identical to the loop's.
+template <bool P2 = false>
 __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __restrict__ solid,
                                                const uint8_t* __restrict__ halo, F3 origin, F3 target) {
     float cnt[3] = {d.nf[0], d.nf[1], d.nf[2]};
@@ -161,8 +190,8 @@ __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __re
     float a[3], b[3], delta[3], crossing[3], stride[3];
     int cell[3], dir[3], endc[3];
     for (int i = 0; i < 3; ++i) {
-        a[i] = fminf(fmaxf(o[i] / d.e[i] * cnt[i], 0.0001f), cnt[i] - 0.0001f);
-        b[i] = fminf(fmaxf(t3[i] / d.e[i] * cnt[i], 0.0001f), cnt[i] - 0.0001f);
+        a[i] = fminf(fmaxf(dv_e<P2>(d, o[i], i) * cnt[i], 0.0001f), cnt[i] - 0.0001f);
+        b[i] = fminf(fmaxf(dv_e<P2>(d, t3[i], i) * cnt[i], 0.0001f), cnt[i] - 0.0001f);
         delta[i] = b[i] - a[i];
         cell[i] = (int)floorf(a[i]);
         endc[i] = (int)floorf(b[i]);
@@ -172,7 +201,7 @@ __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __re
     }
     if (halo && abs(endc[0] - cell[0]) <= 1 && abs(endc[1] - cell[1]) <= 1 && abs(endc[2] - cell[2]) <= 1 &&
         !__ldg(halo + cidx(d, cell[0], cell[1], cell[2])) && !__ldg(halo + cidx(d, endc[0], endc[1], endc[2]))) {
-        F3 r = {b[0] / cnt[0] * d.e[0], b[1] / cnt[1] * d.e[1], b[2] / cnt[2] * d.e[2]};
+        F3 r = {dv_n<P2>(d, b[0], 0) * d.e[0], dv_n<P2>(d, b[1], 1) * d.e[1], dv_n<P2>(d, b[2], 2) * d.e[2]};
         return r;
     }
     if (solid_cell(d, solid, cell[0], cell[1], cell[2])) return origin;
@@ -189,14 +218,14 @@ __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __re
                    : (crossing[1] <= crossing[2] ? 1 : 2);
         float t = crossing[axis];
         if (t >= 1.0f) {
-            F3 r = {b[0] / cnt[0] * d.e[0], b[1] / cnt[1] * d.e[1], b[2] / cnt[2] * d.e[2]};
+            F3 r = {dv_n<P2>(d, b[0], 0) * d.e[0], dv_n<P2>(d, b[1], 1) * d.e[1], dv_n<P2>(d, b[2], 2) * d.e[2]};
             return r;
         }
         cell[axis] += dir[axis];
         if (solid_cell(d, solid, cell[0], cell[1], cell[2])) {
             float back = fmaxf(0.f, t - 0.0001f / fmaxf(len, 1.0f));
-            F3 r = {(a[0] + delta[0] * back) / cnt[0] * d.e[0], (a[1] + delta[1] * back) / cnt[1] * d.e[1],
-                    (a[2] + delta[2] * back) / cnt[2] * d.e[2]};
+            F3 r = {dv_n<P2>(d, a[0] + delta[0] * back, 0) * d.e[0], dv_n<P2>(d, a[1] + delta[1] * back, 1) * d.e[1],
+                    dv_n<P2>(d, a[2] + delta[2] * back, 2) * d.e[2]};
             return r;
         }
         crossing[axis] += stride[axis];
@@ -206,12 +235,13 @@ __device__ __forceinline__ F3 clip_solid_trace(const Dev& d, const uint8_t* __re
 
 // Any solid (or out-of-domain) cell in the 3x3x3 block around p, read from the
 // precomputed dilated mask (solid_boundary.glsl:39-44).
+template <bool P2 = false>
 __device__ __forceinline__ bool solid_halo(const Dev& d, const uint8_t* __restrict__ halo, F3 p) {
     // Clamp before the integer conversion so far-away (or non-finite) points
     // land outside the grid, i.e. count as solid.
-    int cx = (int)fmaxf(fminf(floorf(p.x / d.e[0] * d.nf[0]), 1.0e9f), -1.0e9f);
-    int cy = (int)fmaxf(fminf(floorf(p.y / d.e[1] * d.nf[1]), 1.0e9f), -1.0e9f);
-    int cz = (int)fmaxf(fminf(floorf(p.z / d.e[2] * d.nf[2]), 1.0e9f), -1.0e9f);
+    int cx = (int)fmaxf(fminf(floorf(dv_e<P2>(d, p.x, 0) * d.nf[0]), 1.0e9f), -1.0e9f);
+    int cy = (int)fmaxf(fminf(floorf(dv_e<P2>(d, p.y, 1) * d.nf[1]), 1.0e9f), -1.0e9f);
+    int cz = (int)fmaxf(fminf(floorf(dv_e<P2>(d, p.z, 2) * d.nf[2]), 1.0e9f), -1.0e9f);
     if (cx < 0 || cy < 0 || cz < 0 || cx >= d.nx || cy >= d.ny || cz >= d.nz) return true;
     return __ldg(halo + cidx(d, cx, cy, cz)) != 0;
 }
@@ -221,13 +251,14 @@ __device__ __forceinline__ float dist3(F3 a, F3 b) {
     return sqrtf(dot3(c, c));
 }
 
+template <bool P2 = false>
 __device__ __forceinline__ bool safe_solid_correction(const Dev& d, const uint8_t* solid,
                                                       const uint8_t* halo, F3 p, F3 dep, F3 mid,
                                                       F3 arr) {
-    if (solid_halo(d, halo, p) || solid_halo(d, halo, dep) || solid_halo(d, halo, arr)) return false;
-    if (!(dist3(clip_solid_trace(d, solid, halo, p, dep), dep) < 1e-7f)) return false;
-    if (!(dist3(clip_solid_trace(d, solid, halo, p, mid), mid) < 1e-7f)) return false;
-    return dist3(clip_solid_trace(d, solid, halo, p, arr), arr) < 1e-7f;
+    if (solid_halo<P2>(d, halo, p) || solid_halo<P2>(d, halo, dep) || solid_halo<P2>(d, halo, arr)) return false;
+    if (!(dist3(clip_solid_trace<P2>(d, solid, halo, p, dep), dep) < 1e-7f)) return false;
+    if (!(dist3(clip_solid_trace<P2>(d, solid, halo, p, mid), mid) < 1e-7f)) return false;
+    return dist3(clip_solid_trace<P2>(d, solid, halo, p, arr), arr) < 1e-7f;
 }
 
 // ---------------------------------------------------------------- emitters
@@ -260,15 +291,62 @@ __device__ __forceinline__ float emission_weight(F3 p, F3 center, F3 start, floa
     return fminf(fmaxf(a * a * half / lp * integral, 0.0f), 1.0f);
 }
 
+// Reach of an emitter: an axis-aligned box outside which emission_weight is
+// exactly 0.0f, so the weight need not be evaluated there.
+//
+// In real arithmetic the weight is non-zero only within distance r of the
+// segment start..center (a capsule; a sphere around center when the segment is
+// degenerate), and zero when the distance is >= r. Evaluated in FP32, the
+// perpendicular distance and the along-axis position of a point p carry
+// absolute errors of at most ~12 eps |p - start| (eps = 2^-24), and
+// |p - start| <= sqrt(3) * 2M for M = max(|extent|, |start|, |center|, r)
+// since grid positions lie in [0, extent]. So a point farther than
+// r + 1e-3 * 4M from the segment evaluates to exactly zero (the a <= 0 or
+// hi <= lo branch; both return +0.0f), and every point outside the box
+// [min(start, center) - r - 4e-3 M, max(start, center) + r + 4e-3 M] is that
+// far. The bounds are rounded outwards to float. A NaN anywhere leaves the
+// box unusable (comparisons are false), and the weight is then evaluated.
+struct Reach {
+    float lo[3], hi[3];
+};
+
+inline float round_down_f(double x) {
+    float f = (float)x;
+    return (double)f > x ? std::nextafter(f, -INFINITY) : f;
+}
+inline float round_up_f(double x) {
+    float f = (float)x;
+    return (double)f < x ? std::nextafter(f, INFINITY) : f;
+}
+
+inline Reach make_reach(const float* center, const float* start, float radius, const float* extent) {
+    double m = std::fabs((double)radius);
+    for (int a = 0; a < 3; ++a)
+        m = std::fmax(m, std::fmax(std::fabs((double)extent[a]),
+                                   std::fmax(std::fabs((double)center[a]), std::fabs((double)start[a]))));
+    double margin = std::fabs((double)radius) + 4e-3 * m;
+    Reach r;
+    for (int a = 0; a < 3; ++a) {
+        r.lo[a] = round_down_f(std::fmin((double)center[a], (double)start[a]) - margin);
+        r.hi[a] = round_up_f(std::fmax((double)center[a], (double)start[a]) + margin);
+    }
+    return r;
+}
+
+__device__ __forceinline__ bool outside(const Reach& r, F3 p) {
+    return p.x < r.lo[0] || p.x > r.hi[0] || p.y < r.lo[1] || p.y > r.hi[1] || p.z < r.lo[2] || p.z > r.hi[2];
+}
+
 struct SrcDev {
     int count;
     int single_solid;
     F3 center, start, jet;
     float radius, coupling;
     float table[128];
+    Reach reach[9];   // table rows 0..7, then the single emitter
 };
 
-inline SrcDev make_src(const FfxSources* s) {
+inline SrcDev make_src(const FfxSources* s, const float* extent) {
     SrcDev r;
     r.count = s ? s->count : -1;
     r.single_solid = s ? s->single_solid_profile : 0;
@@ -278,13 +356,25 @@ inline SrcDev make_src(const FfxSources* s) {
     r.radius = s ? s->single_radius : 1.f;
     r.coupling = s ? s->single_coupling : 0.f;
     for (int i = 0; i < 128; ++i) r.table[i] = s ? s->table[i] : 0.f;
+    for (int i = 0; i < 8; ++i) {
+        const float* row = r.table + 16 * i;
+        r.reach[i] = make_reach(row, row + 4, row[3], extent);
+    }
+    const float c[3] = {r.center.x, r.center.y, r.center.z}, st[3] = {r.start.x, r.start.y, r.start.z};
+    r.reach[8] = make_reach(c, st, r.radius, extent);
     return r;
 }
 
 __device__ __forceinline__ float table_weight(const SrcDev& s, int i, F3 p) {
+    if (outside(s.reach[i], p)) return 0.0f;
     const float* row = s.table + 16 * i;
     F3 c = {row[0], row[1], row[2]}, st = {row[4], row[5], row[6]};
     return emission_weight(p, c, st, row[3], row[14] > 0.5f);
+}
+
+__device__ __forceinline__ float single_weight(const SrcDev& s, F3 p) {
+    if (outside(s.reach[8], p)) return 0.0f;
+    return emission_weight(p, s.center, s.start, s.radius, s.single_solid != 0);
 }
 
 // ---------------------------------------------------------------- reductions

@@ -337,6 +337,39 @@ def test_pcg_reaches_the_vcycle_solution_in_fewer_cycles(D, warm):
         mv, mp = vproj.metrics(), pproj.metrics()
         assert mv['rel_div_inf'] <= 1.5e-6 and mp['rel_div_inf'] <= 1.5e-6, (mv['rel_div_inf'], mp['rel_div_inf'])
         assert pproj.last_cycles < vproj.last_cycles, (pproj.last_cycles, vproj.last_cycles)
+        # Two solutions with residuals <= 1e-6 max|div| can differ by low modes of
+        # size ~ tol * max|div| * L / pi in velocity (~4e-5 here): bound at 1e-4.
         for a in range(3):
             scale = float(np.abs(n(outs_v[a])).max())
-            assert float(np.abs(n(outs_v[a]) - n(outs_p[a])).max()) <= 2e-5 * scale
+            assert float(np.abs(n(outs_v[a]) - n(outs_p[a])).max()) <= 1e-4 * scale
+
+
+@pytest.mark.parametrize('method', ['VCYCLE', 'PCG'])
+def test_graph_replay_matches_eager_launches(D, method):
+    """The pressure solve replayed from captured CUDA graphs runs the same
+    kernels on the same buffers as eager launches: results are bit-identical,
+    and so are the cycle counts."""
+    from fluxfx_b200.backend.collision import SolidDevice
+    from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
+    grid = GridSpec((32, 24, 16))
+    sd = SolidDevice(grid, sphere_box_mask(grid.shape, grid.extent), D)
+    s = PressureSettings(pressure_tolerance=1e-5, pressure_max_cycles=60, pressure_method=method,
+                         solid_warm_start=method == 'PCG')
+    graphed, eager = SolidMultigridProjector(grid, s, sd), SolidMultigridProjector(grid, s, sd)
+    eager.use_graphs = False
+    rng = np.random.default_rng(7)
+    out_g = [D.texture(fs) for fs in grid.face_shapes]
+    out_e = [D.texture(fs) for fs in grid.face_shapes]
+    for dt in (0.02, 0.02, 0.01):
+        # fresh velocities each call, so a warm-started solve still has work to do
+        fields = [D.texture(fs, rng.uniform(-1, 1, fs[0] * fs[1] * fs[2]), nonnegative=False)
+                  for fs in grid.face_shapes]
+        graphed.project(fields, out_g, dt)
+        eager.project(fields, out_e, dt)
+        assert graphed.last_cycles == eager.last_cycles > 1
+        assert graphed.last_iterations == eager.last_iterations
+        for a in range(3):
+            assert np.array_equal(n(out_g[a]), n(out_e[a])), a
+    assert graphed._graphs and not eager._graphs
+    graphed.close()
+    eager.close()
