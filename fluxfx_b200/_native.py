@@ -109,6 +109,7 @@ _PROTOTYPES = {
     'ffx_max_abs': (C.c_int, [i64, C.c_int, vp, vp, vp]),
     'ffx_divergence_stats_workspace': (C.c_size_t, [i64]),
     'ffx_divergence_stats': (C.c_int, [i64, vp, vp, vp, vp, C.c_size_t, vp]),
+    'ffx_divergence_stats_static': (C.c_int, [i64, vp, vp, vp, vp]),
 }
 
 _LIB = None

@@ -290,6 +290,20 @@ int ffx_max_abs(int64_t count, int storage, const void* x, float* out, void* str
 size_t ffx_divergence_stats_workspace(int64_t count);
 int ffx_divergence_stats(int64_t count, const float* before, const float* after,
                          double* out, void* workspace, size_t workspace_bytes, void* stream);
+/* The same statistics for callers that cannot allocate device memory when they
+ * ask for them (a host whose device memory is all owned by its own pool, a
+ * real-time callback where cudaMalloc -- which may synchronise the device -- is
+ * not allowed, a C caller with no allocator). No counterpart in the reference.
+ * Allocates nothing: the block partials live in a fixed 56,832-byte array of
+ * the library, reserved on every GPU that loads it until the library is
+ * unloaded. count must lie in [1, 2^31 - 1]; larger counts are rejected with
+ * FFX_ERR_INVALID (use ffx_divergence_stats). The first call on a device looks
+ * up that array's device address (cudaGetSymbolAddress) with the device
+ * current; make that first call before any stream capture. All calls share the
+ * array: calls whose kernels overlap on the GPU race; calls ordered on one
+ * stream do not, since each call rewrites every partial it reads. */
+int ffx_divergence_stats_static(int64_t count, const float* before, const float* after,
+                                double* out, void* stream);
 
 #ifdef __cplusplus
 }
