@@ -219,6 +219,7 @@ class Run:
         self.pass_timer = PassTimer(stream) if passes else None
         solver.pass_timer = self.pass_timer
         self.cycles = []
+        graphs0 = len(getattr(solver.projector, '_graphs', ()))
         calls0 = self.device.calls
         torch.cuda.synchronize()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -229,6 +230,7 @@ class Run:
         end.record(stream)
         torch.cuda.synchronize()
         self.launches = self.device.calls - calls0
+        self.captures = len(getattr(solver.projector, '_graphs', ())) - graphs0
         solver.pass_timer = None
         return start.elapsed_time(end) / 1e3
 
@@ -294,7 +296,7 @@ def run_b200(args):
     elapsed = run.timed(args.steps, passes=True)
     clock_info = clocks.stop()
     passes = run.pass_timer.totals_ms()
-    head = dict(cycles=run.cycles, launches=run.launches)
+    head = dict(cycles=run.cycles, launches=run.launches, captures=run.captures)
     rel_div = run.solver.measure_projection()['rel_div_inf']
     e2e_steps = max(1, args.steps // 2)
     e2e_time, d2h = run.e2e(e2e_steps)
@@ -341,6 +343,7 @@ def run_b200(args):
                        "cells": cells, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}",
                        "v_cycles_mean": statistics.mean(head['cycles']), "v_cycles_max": max(head['cycles']),
+                       "graph_captures_in_timed_steps": head['captures'],
                        "final_rel_div_inf": rel_div,
                        "plain_fp32_mg": None if plain is None else {
                            "steps_per_s": job_rate(world, plain['steps'], p_el), "steps": plain['steps'],

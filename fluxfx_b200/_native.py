@@ -57,7 +57,19 @@ class FfxScalarChannel(C.Structure):
 
 
 class FfxGraphLevel(C.Structure):
-    _fields_ = [('nx', i32), ('ny', i32), ('nz', i32), ('edges', vp), ('solid', vp), ('w', f3)]
+    _fields_ = [('nx', i32), ('ny', i32), ('nz', i32), ('edges', vp), ('solid', vp), ('w', f3), ('links', vp)]
+
+
+TAIL_LEVELS = 8
+
+
+class FfxTailLevel(C.Structure):
+    _fields_ = [('level', FfxGraphLevel), ('p', vp), ('q', vp), ('rhs', vp)]
+
+
+class FfxGraphTail(C.Structure):
+    _fields_ = [('count', i32), ('pre', i32), ('post', i32), ('omega', f32), ('inverse', vp),
+                ('levels', FfxTailLevel * TAIL_LEVELS)]
 
 
 P = C.POINTER
@@ -101,6 +113,8 @@ _PROTOTYPES = {
     'ffx_graph_residual_max': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
     'ffx_graph_coarsen': (C.c_int, [P(FfxGraphLevel), vp, vp, vp]),
     'ffx_graph_level0_edges': (C.c_int, [P(FfxGraphLevel), vp, vp]),
+    'ffx_graph_links': (C.c_int, [P(FfxGraphLevel), vp, vp]),
+    'ffx_graph_tail': (C.c_int, [P(FfxGraphTail), vp]),
     'ffx_graph_smooth_zero': (C.c_int, [P(FfxGraphLevel), vp, f32, vp, vp]),
     'ffx_graph_smooth_dot': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp, C.c_double, vp]),
     'ffx_pcg_direction_apply': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp, vp, vp, vp, vp]),
@@ -135,7 +149,7 @@ def load(path=None):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.ffx_abi_version() != 1:
+    if lib.ffx_abi_version() != 2:
         raise NativeUnavailable("libffx_core ABI version mismatch")
     if path is None:
         _LIB = lib

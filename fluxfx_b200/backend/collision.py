@@ -55,6 +55,14 @@ class SolidDevice:
         self._rows = rows
         self.colliders = tuple(colliders)
 
+    @property
+    def calls(self):
+        return self.base.calls
+
+    @calls.setter
+    def calls(self, value):
+        self.base.calls = value
+
     def __getattr__(self, name):
         base = self.__dict__.get('base')
         if base is None:

@@ -3,7 +3,8 @@
 Drop-in for FluxFX ``fluxfx/backend/solid_multigrid.py:7-93``. The Galerkin
 hierarchy of ``fluxfx/physics/solid_hierarchy.py:11-54`` is built on the device
 (``ffx_graph_coarsen`` per level, one flag readback per level at construction);
-level 0 reads the uint8 mask instead of storing conductances. The coarsest
+level 0 stores one link byte per cell (``ffx_graph_links``) instead of
+conductances. The coarsest
 level (<= 256 cells) is solved with an FP64 graph pseudoinverse. Residual +
 restriction and prolongation + first post-smoothing sweep are fused passes
 with results identical to the separate passes.
@@ -19,6 +20,7 @@ from .collision import SolidPressureProjector
 from .device import KernelHandle, ptr
 
 DIRECT_LIMIT = 256
+TAIL_CELLS = 512   # coarse levels at most this size run in one single-block launch
 
 
 class KernelTimer:
@@ -87,6 +89,11 @@ class SolidMultigridProjector(SolidPressureProjector):
         shape = tuple(grid.shape)
         weights = [float(np.float32((n / e) ** 2)) for n, e in zip(shape, grid.extent)]
         level0 = N.FfxGraphLevel(*shape, None, ptr(self._mask), N.f3(*weights))
+        # one link byte per cell lets the level-0 passes run four cells per thread
+        nx, ny, nz = shape
+        self._links = torch.empty((nz, ny, nx), dtype=torch.uint8, device=dev.device)
+        dev.call('ffx_graph_links', C.byref(level0), ptr(self._links), dev.s)
+        level0.links = self._links.data_ptr()
         self.levels.append(dict(shape=shape, edges=None, graph=level0, p=self.pressure, q=self.spare,
                                 rhs=self.before))
         flag = torch.zeros(1, dtype=torch.int32, device=dev.device)
@@ -116,13 +123,37 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.timer = None
         self.use_graphs = True
         self._graphs = {}
+        self.use_tail = True
+        self._tail, self.tail_start = self._make_tail()
         self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
+
+    def _make_tail(self):
+        """Descriptor of the coarse levels run as one ``ffx_graph_tail`` launch:
+        the levels from the first one (below level 0) with at most TAIL_CELLS
+        cells down to the coarsest, at most eight of them. Needs an even number
+        of sweeps per level and cycle, so buffer roles repeat."""
+        if (self.pre_sweeps + self.post_sweeps) % 2 or len(self.levels) < 3:
+            return None, None
+        start = next((k for k in range(1, len(self.levels)) if prod(self.levels[k]['shape']) <= TAIL_CELLS), None)
+        if start is None or start == len(self.levels) - 1:
+            return None, None
+        start = max(start, len(self.levels) - N.TAIL_LEVELS)
+        tail = N.FfxGraphTail()
+        tail.count = len(self.levels) - start
+        tail.pre, tail.post, tail.omega = self.pre_sweeps, self.post_sweeps, 2.0 / 3.0
+        tail.inverse = self.coarse_matrix.data_ptr() if self.coarse_matrix is not None else None
+        for k, level in enumerate(self.levels[start:]):
+            slot = tail.levels[k]
+            slot.level = level['graph']
+            slot.p, slot.q, slot.rhs = level['p'].data_ptr(), level['q'].data_ptr(), level['rhs'].data_ptr()
+        return tail, start
 
     @property
     def allocated_bytes(self):
         coarse = sum(4 * 7 * prod(v['shape']) for v in self.levels[1:])
         direct = 8 * self.coarse_matrix.numel() if self.coarse_matrix is not None else 0
-        return super().allocated_bytes + coarse + direct
+        links = self._links.numel() if self._links is not None else 0
+        return super().allocated_bytes + coarse + direct + links
 
     def smooth(self, level, count):
         timer = self.timer if level is self.levels[0] else None
@@ -170,8 +201,13 @@ class SolidMultigridProjector(SolidPressureProjector):
         coarse = self.levels[index + 1]
         dev.call('ffx_graph_residual_restrict', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
                  ptr(coarse['rhs']), dev.s)
-        coarse['p'].zero_()
-        self.cycle(index + 1)
+        if self.use_tail and index + 1 == self.tail_start:
+            # every level below runs inside one launch (it zeroes coarse p itself)
+            dev.call('ffx_graph_tail', C.byref(self._tail), dev.s)
+            self.last_iterations += self._tail_sweeps()
+        else:
+            coarse['p'].zero_()
+            self.cycle(index + 1)
         if self.post_sweeps > 0:
             dev.call('ffx_graph_prolong_smooth', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), dev.s)
@@ -191,6 +227,10 @@ class SolidMultigridProjector(SolidPressureProjector):
             level['p'], level['q'] = level['q'], level['p']
         if dot is not None:
             dev.call('ffx_dot', level['p'].numel(), ptr(level['rhs']), ptr(level['p']), -1.0, ptr(dot), dev.s)
+
+    def _tail_sweeps(self):
+        n = len(self.levels) - self.tail_start - 1
+        return n * (self.pre_sweeps + self.post_sweeps) + (0 if self.coarse_matrix is not None else 80)
 
     def _residual_max(self):
         level = self.levels[0]
@@ -358,6 +398,8 @@ class SolidMultigridProjector(SolidPressureProjector):
     def close(self):
         self._graphs = {}
         self._kry = None
+        self._links = None
+        self._tail = None
         self.levels = []
         self.coarse_matrix = self.coarse_kernel = None
         super().close()

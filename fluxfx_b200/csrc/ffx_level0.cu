@@ -1,0 +1,445 @@
+// Level 0 of the collider (aggregation) multigrid, four cells per thread.
+//
+// Level 0 is the full-resolution grid and carries almost all of the solve's
+// memory traffic. These kernels replace the one-cell-per-thread versions in
+// ffx_project.cu when the level has a precomputed link field and the x extent
+// is a multiple of 4:
+//
+// * links: one byte per cell, bit 2a (2a+1) set when the face to the lower
+//   (upper) neighbour along axis a is open, i.e. both cells are fluid and the
+//   neighbour lies inside the domain; bit 6 = the cell itself is fluid. This is
+//   the level-0 conductance of solid_hierarchy.py:16-25 (weight (n/extent)^2
+//   on open faces, 0 elsewhere) packed into one load per cell.
+// * A thread owns four consecutive cells along x (float4 rows) and walks a
+//   column of kZ4 slices along z, carrying the iterate of slices z-1, z, z+1 in
+//   registers. The x neighbours of its four cells come from the neighbouring
+//   lanes by shuffle (a warp is one row of 128 cells); lanes 0 and 31 load the
+//   cell beyond the warp. y neighbours are float4 loads of the adjacent rows.
+//
+// Every cell is evaluated with the operations, and in the order, of the
+// scalar kernels (graph_terms: x-, x+, y-, y+, z-, z+), so both paths give
+// bit-identical fields. A term is added only where its link bit is set; the
+// scalar kernels instead add weight 0 for an in-domain neighbour that is not
+// linked, and diag + 0 == diag, nb + 0 * v == nb for finite v, so the sums are
+// the same (nb never holds -0: it starts at +0 and an exact cancellation
+// rounds to +0).
+#include "ffx_common.cuh"
+#include "ffx_host.cuh"
+#include "ffx_level0.cuh"
+
+namespace ffx {
+namespace {
+
+constexpr unsigned kXm = 1u, kXp = 2u, kYm = 4u, kYp = 8u, kZm = 16u, kZp = 32u, kFluid = 64u;
+constexpr int kZ4 = 8;           // slices per thread column (even: the restriction pairs slices)
+constexpr int kRows = 8;         // warps (rows) per block
+
+struct L0 {
+    int nx, ny, nz, nx4;
+    const uint8_t* links;
+    float wx, wy, wz;
+};
+
+inline L0 make_l0(const FfxGraphLevel* lv) {
+    L0 g;
+    g.nx = lv->nx; g.ny = lv->ny; g.nz = lv->nz; g.nx4 = lv->nx / 4;
+    g.links = lv->links;
+    g.wx = lv->w[0]; g.wy = lv->w[1]; g.wz = lv->w[2];
+    return g;
+}
+
+__device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
+__device__ __forceinline__ float4 ld4(const float* p, int i4) {
+    return __ldg(reinterpret_cast<const float4*>(p) + i4);
+}
+__device__ __forceinline__ float2 ld2(const float* p, int i2) {
+    return __ldg(reinterpret_cast<const float2*>(p) + i2);
+}
+__device__ __forceinline__ float el(const float4& v, int k) {
+    return k == 0 ? v.x : (k == 1 ? v.y : (k == 2 ? v.z : v.w));
+}
+__device__ __forceinline__ void set_el(float4& v, int k, float s) {
+    if (k == 0) v.x = s;
+    else if (k == 1) v.y = s;
+    else if (k == 2) v.z = s;
+    else v.w = s;
+}
+__device__ __forceinline__ uint32_t ld_links(const L0& g, int i4) {
+    return __ldg(reinterpret_cast<const uint32_t*>(g.links) + i4);
+}
+
+// Operator terms of the four cells of one row segment (byte k of `lk` is the
+// link byte of cell k). left/right: the iterate at x0-1 and x0+4.
+__device__ __forceinline__ void terms4(const L0& g, uint32_t lk, float left, const float4& c, float right,
+                                       const float4& ym, const float4& yp, const float4& lo, const float4& hi,
+                                       float diag[4], float nb[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const unsigned b = (lk >> (8 * k)) & 0xffu;
+        const float xm = k == 0 ? left : el(c, k - 1);
+        const float xp = k == 3 ? right : el(c, k + 1);
+        float d = 0.f, s = 0.f;
+        if (b & kXm) { d = d + g.wx; s = s + g.wx * xm; }
+        if (b & kXp) { d = d + g.wx; s = s + g.wx * xp; }
+        if (b & kYm) { d = d + g.wy; s = s + g.wy * el(ym, k); }
+        if (b & kYp) { d = d + g.wy; s = s + g.wy * el(yp, k); }
+        if (b & kZm) { d = d + g.wz; s = s + g.wz * el(lo, k); }
+        if (b & kZp) { d = d + g.wz; s = s + g.wz * el(hi, k); }
+        diag[k] = d;
+        nb[k] = s;
+    }
+}
+
+// ------------------------------------------------------------ iterates
+// The value the stencil reads at a cell: the iterate itself, the prolonged
+// iterate p + coarse (solid_mg_prolong.glsl, formed on the fly), or the new
+// search direction z + beta p_old.
+enum class It { Plain, Prolonged, Direction };
+
+struct ItArgs {
+    const float* a;        // p (Plain, Prolonged) or z (Direction)
+    const float* b;        // coarse correction (Prolonged) or p_old (Direction; NULL on the first iteration)
+    const double* rz_new;  // Direction: beta = rz_new / rz_old, read on the device
+    const double* rz_old;
+};
+
+template <It K>
+__device__ __forceinline__ float4 it4(const L0& g, const ItArgs& A, float beta, int i4, int x4, int y, int z) {
+    const float4 v = ld4(A.a, i4);
+    if constexpr (K == It::Plain) {
+        return v;
+    } else if constexpr (K == It::Prolonged) {
+        // coarse cell of (x, y, z) is (x/2, y/2, z/2); cells 4x4, 4x4+1 share
+        // coarse x = 2x4 and 4x4+2, 4x4+3 share 2x4+1: one float2.
+        const float2 c = ld2(A.b, x4 + g.nx4 * ((y >> 1) + (g.ny >> 1) * (z >> 1)));
+        return make_float4(v.x + c.x, v.y + c.x, v.z + c.y, v.w + c.y);
+    } else {
+        if (!A.b) return v;
+        const float4 q = ld4(A.b, i4);
+        return make_float4(v.x + beta * q.x, v.y + beta * q.y, v.z + beta * q.z, v.w + beta * q.w);
+    }
+}
+
+template <It K>
+__device__ __forceinline__ float it1(const L0& g, const ItArgs& A, float beta, int i, int x, int y, int z) {
+    const float v = __ldg(A.a + i);
+    if constexpr (K == It::Plain) {
+        return v;
+    } else if constexpr (K == It::Prolonged) {
+        return v + __ldg(A.b + (x >> 1) + (g.nx >> 1) * ((y >> 1) + (g.ny >> 1) * (z >> 1)));
+    } else {
+        return A.b ? v + beta * __ldg(A.b + i) : v;
+    }
+}
+
+// ------------------------------------------------------------ epilogues
+enum class Ep { Smooth, SmoothDot, Apply, Residual, ResidualMax };
+
+struct EpArgs {
+    const float* rhs;
+    float omega;
+    float* out;       // smoothed iterate, new direction (Apply) or residual
+    float* out2;      // q = A p (Apply)
+    double* dsum;     // SmoothDot: += scale * rhs . out; Apply: += p . q
+    double scale;
+    float* fmax;      // ResidualMax
+};
+
+__device__ __forceinline__ double warp_sum_d(double v) {
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+__device__ __forceinline__ void block_sum_d(double* out, double v) {
+    __shared__ double part[kRows];
+    v = warp_sum_d(v);
+    const int lane = threadIdx.x, wid = threadIdx.y;
+    if (lane == 0) part[wid] = v;
+    __syncthreads();
+    if (lane == 0 && wid == 0) {
+        double s = 0.0;
+        for (int w = 0; w < kRows; ++w) s += part[w];
+        if (s != 0.0) atomicAdd(out, s);
+    }
+}
+
+// One pass of the stencil over level 0: K selects the iterate, E what is
+// written. Block (32, kRows): lane = x4 within a 128-cell row segment, warp =
+// row; blockIdx.z = column of kZ4 slices. Threads outside the grid stay in the
+// loop (with zero data) so that shuffles and the block reduction see every lane.
+template <It K, Ep E>
+__global__ void __launch_bounds__(32 * kRows, 4) level0_kernel(L0 g, ItArgs A, EpArgs P) {
+    const int lane = threadIdx.x;
+    const int x4 = blockIdx.x * 32 + lane, y = blockIdx.y * kRows + threadIdx.y;
+    const bool active = x4 < g.nx4 && y < g.ny;
+    const int x0 = 4 * x4;
+    const int z0 = blockIdx.z * kZ4, zend = min(z0 + kZ4, g.nz);
+    const int row4 = g.nx4, slice4 = g.nx4 * g.ny;
+    int i4 = x4 + row4 * (y + g.ny * z0);
+    const float one_minus = 1.f - P.omega;
+    float beta = 0.f;
+    if constexpr (K == It::Direction) beta = A.b ? (float)(*A.rz_new / *A.rz_old) : 0.f;
+    double acc = 0.0;
+    float m = 0.f;
+    // Everything slice z needs from memory, fetched one slice ahead so that
+    // two slices' loads are in flight while one is computed. `edge` is the
+    // iterate beyond the warp (x0 - 1 on lane 0, x0 + 4 on lane 31).
+    struct Slice {
+        uint32_t lk;
+        float4 hi, ym, yp, r;
+        float edge;
+    };
+    auto fetch = [&](int z, int j4, Slice& s) {
+        s.lk = active ? ld_links(g, j4) : 0u;
+        s.hi = (active && z + 1 < g.nz) ? it4<K>(g, A, beta, j4 + slice4, x4, y, z + 1) : zero4();
+        s.ym = (active && y > 0) ? it4<K>(g, A, beta, j4 - row4, x4, y - 1, z) : zero4();
+        s.yp = (active && y + 1 < g.ny) ? it4<K>(g, A, beta, j4 + row4, x4, y + 1, z) : zero4();
+        if constexpr (E != Ep::Apply) s.r = active ? ld4(P.rhs, j4) : zero4();
+        s.edge = 0.f;
+        if (active && lane == 0 && x0 > 0) s.edge = it1<K>(g, A, beta, 4 * j4 - 1, x0 - 1, y, z);
+        if (active && lane == 31 && x0 + 4 < g.nx) s.edge = it1<K>(g, A, beta, 4 * j4 + 4, x0 + 4, y, z);
+    };
+    float4 lo = zero4(), c = zero4();
+    if (active) {
+        c = it4<K>(g, A, beta, i4, x4, y, z0);
+        if (z0 > 0) lo = it4<K>(g, A, beta, i4 - slice4, x4, y, z0 - 1);
+    }
+    Slice cur;
+    fetch(z0, i4, cur);
+    for (int z = z0; z < zend; ++z, i4 += slice4) {
+        Slice nxt;
+        if (z + 1 < zend) fetch(z + 1, i4 + slice4, nxt);
+        const uint32_t lk = cur.lk;
+        float left = __shfl_up_sync(0xffffffffu, c.w, 1);
+        float right = __shfl_down_sync(0xffffffffu, c.x, 1);
+        if (lane == 0) left = cur.edge;
+        if (lane == 31) right = cur.edge;
+        float diag[4], nb[4];
+        terms4(g, lk, left, c, right, cur.ym, cur.yp, lo, cur.hi, diag, nb);
+        if (active) {
+            if constexpr (E == Ep::Apply) {
+                float4 q;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float pc = el(c, k);
+                    const float qc = diag[k] > 0.f ? diag[k] * pc - nb[k] : 0.f;
+                    set_el(q, k, qc);
+                    acc += (double)pc * (double)qc;
+                }
+                reinterpret_cast<float4*>(P.out)[i4] = c;
+                reinterpret_cast<float4*>(P.out2)[i4] = q;
+            } else {
+                const float4 r = cur.r;
+                float4 o;
+#pragma unroll
+                for (int k = 0; k < 4; ++k) {
+                    const float rk = el(r, k), d = diag[k];
+                    float v;
+                    if constexpr (E == Ep::Residual || E == Ep::ResidualMax)
+                        v = d > 0.f ? (rk - nb[k]) + d * el(c, k) : 0.f;
+                    else
+                        v = d > 0.f ? el(c, k) * one_minus + ((nb[k] - rk) / d) * P.omega : 0.f;
+                    set_el(o, k, v);
+                    if constexpr (E == Ep::SmoothDot) acc += P.scale * (double)rk * (double)v;
+                    if constexpr (E == Ep::ResidualMax) m = fmaxf(m, finite_abs(v));
+                }
+                if constexpr (E != Ep::ResidualMax) reinterpret_cast<float4*>(P.out)[i4] = o;
+            }
+        }
+        lo = c;
+        c = cur.hi;
+        cur = nxt;
+    }
+    if constexpr (E == Ep::SmoothDot || E == Ep::Apply) block_sum_d(P.dsum, acc);
+    if constexpr (E == Ep::ResidualMax) block_max_to(P.fmax, m);
+}
+
+// First sweep from a zero iterate (graph_smooth_zero_kernel): no iterate is
+// read, so this is a plain stream over links and rhs.
+__global__ void __launch_bounds__(256) level0_smooth_zero_kernel(L0 g, const float* __restrict__ rhs, float omega,
+                                                                float* __restrict__ out, int n4) {
+    const int i4 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i4 >= n4) return;
+    const uint32_t lk = ld_links(g, i4);
+    const float4 r = ld4(rhs, i4);
+    const float4 z = zero4();
+    float diag[4], nb[4];
+    terms4(g, lk, 0.f, z, 0.f, z, z, z, z, diag, nb);
+    float4 o;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float d = diag[k];
+        set_el(o, k, d > 0.f ? 0.f * (1.f - omega) + ((nb[k] - el(r, k)) / d) * omega : 0.f);
+    }
+    reinterpret_cast<float4*>(out)[i4] = o;
+}
+
+// Fused residual + 2x2x2 average restriction (graph_residual_restrict_kernel):
+// a thread owns a 4 x 2 (x, y) patch, i.e. two coarse cells along x, and walks
+// pairs of slices; each coarse value sums its eight children's residuals in
+// the scalar kernel's order (dz, then dy, then dx) and divides by 8.
+__global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0 g, const float* __restrict__ p,
+                                                                             const float* __restrict__ rhs,
+                                                                             float* __restrict__ coarse) {
+    const int lane = threadIdx.x;
+    const int x4 = blockIdx.x * 32 + lane, ya = 2 * (blockIdx.y * kRows + threadIdx.y), yb = ya + 1;
+    const bool active = x4 < g.nx4 && ya < g.ny;
+    const int x0 = 4 * x4;
+    const int z0 = blockIdx.z * kZ4, zend = min(z0 + kZ4, g.nz);
+    const int row4 = g.nx4, slice4 = g.nx4 * g.ny;
+    int ia = x4 + row4 * (ya + g.ny * z0);
+    float4 lo_a = zero4(), c_a = zero4(), lo_b = zero4(), c_b = zero4();
+    if (active) {
+        c_a = ld4(p, ia);
+        c_b = ld4(p, ia + row4);
+        if (z0 > 0) {
+            lo_a = ld4(p, ia - slice4);
+            lo_b = ld4(p, ia + row4 - slice4);
+        }
+    }
+    float v0 = 0.f, v1 = 0.f;
+    for (int z = z0; z < zend; ++z, ia += slice4) {
+        const int ib = ia + row4;
+        const bool up = active && z + 1 < g.nz;
+        const float4 hi_a = up ? ld4(p, ia + slice4) : zero4();
+        const float4 hi_b = up ? ld4(p, ib + slice4) : zero4();
+        const float4 ym = (active && ya > 0) ? ld4(p, ia - row4) : zero4();
+        const float4 yp = (active && yb + 1 < g.ny) ? ld4(p, ib + row4) : zero4();
+        const uint32_t lka = active ? ld_links(g, ia) : 0u, lkb = active ? ld_links(g, ib) : 0u;
+        float left_a = __shfl_up_sync(0xffffffffu, c_a.w, 1), right_a = __shfl_down_sync(0xffffffffu, c_a.x, 1);
+        float left_b = __shfl_up_sync(0xffffffffu, c_b.w, 1), right_b = __shfl_down_sync(0xffffffffu, c_b.x, 1);
+        if (lane == 0) {
+            left_a = (lka & kXm) ? __ldg(p + 4 * ia - 1) : 0.f;
+            left_b = (lkb & kXm) ? __ldg(p + 4 * ib - 1) : 0.f;
+        }
+        if (lane == 31) {
+            right_a = ((lka >> 24) & kXp) ? __ldg(p + 4 * ia + 4) : 0.f;
+            right_b = ((lkb >> 24) & kXp) ? __ldg(p + 4 * ib + 4) : 0.f;
+        }
+        float da[4], na[4], db[4], nbb[4];
+        terms4(g, lka, left_a, c_a, right_a, ym, c_b, lo_a, hi_a, da, na);
+        terms4(g, lkb, left_b, c_b, right_b, c_a, yp, lo_b, hi_b, db, nbb);
+        if (active) {
+            const float4 ra = ld4(rhs, ia), rb = ld4(rhs, ib);
+            float res_a[4], res_b[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                res_a[k] = da[k] > 0.f ? (el(ra, k) - na[k]) + da[k] * el(c_a, k) : 0.f;
+                res_b[k] = db[k] > 0.f ? (el(rb, k) - nbb[k]) + db[k] * el(c_b, k) : 0.f;
+            }
+            if ((z & 1) == 0) {
+                v0 = 0.f;
+                v1 = 0.f;
+            }
+            v0 = v0 + res_a[0]; v0 = v0 + res_a[1]; v0 = v0 + res_b[0]; v0 = v0 + res_b[1];
+            v1 = v1 + res_a[2]; v1 = v1 + res_a[3]; v1 = v1 + res_b[2]; v1 = v1 + res_b[3];
+            if (z & 1)
+                reinterpret_cast<float2*>(coarse)[x4 + g.nx4 * ((ya >> 1) + (g.ny >> 1) * (z >> 1))] =
+                    make_float2(v0 / 8.0f, v1 / 8.0f);
+        }
+        lo_a = c_a; c_a = hi_a;
+        lo_b = c_b; c_b = hi_b;
+    }
+}
+
+__global__ void __launch_bounds__(256) links_kernel(int nx, int ny, int nz, const uint8_t* __restrict__ solid,
+                                                   uint8_t* __restrict__ links) {
+    int x, y, z;
+    if (!cell_coords(nx, ny, x, y, z)) return;
+    const int sy = nx, sz = nx * ny;
+    const int i = x + nx * (y + ny * z);
+    unsigned b = 0;
+    if (__ldg(solid + i) == 0) {
+        b = kFluid;
+        if (x > 0 && __ldg(solid + i - 1) == 0) b |= kXm;
+        if (x + 1 < nx && __ldg(solid + i + 1) == 0) b |= kXp;
+        if (y > 0 && __ldg(solid + i - sy) == 0) b |= kYm;
+        if (y + 1 < ny && __ldg(solid + i + sy) == 0) b |= kYp;
+        if (z > 0 && __ldg(solid + i - sz) == 0) b |= kZm;
+        if (z + 1 < nz && __ldg(solid + i + sz) == 0) b |= kZp;
+    }
+    links[i] = (uint8_t)b;
+}
+
+bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; }
+
+dim3 l0_grid(const L0& g) {
+    return dim3((unsigned)((g.nx4 + 31) / 32), (unsigned)((g.ny + kRows - 1) / kRows),
+                (unsigned)((g.nz + kZ4 - 1) / kZ4));
+}
+
+template <It K, Ep E>
+int launch(const L0& g, const ItArgs& A, const EpArgs& P, cudaStream_t st, const char* name) {
+    level0_kernel<K, E><<<l0_grid(g), dim3(32, kRows), 0, st>>>(g, A, P);
+    return launch_status(name);
+}
+
+}  // namespace
+
+bool level0_x4(const FfxGraphLevel* lv, std::initializer_list<const void*> f4) {
+    if (!lv || lv->edges || !lv->links || lv->nx % 4 != 0 || !aligned(lv->links, 4)) return false;
+    for (const void* p : f4)
+        if (p && !aligned(p, 16)) return false;
+    return true;
+}
+
+int level0_smooth(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega, float* out,
+                  cudaStream_t st) {
+    EpArgs P{rhs, omega, out, nullptr, nullptr, 0.0, nullptr};
+    return launch<It::Plain, Ep::Smooth>(make_l0(lv), ItArgs{p, nullptr, nullptr, nullptr}, P, st, "level0_smooth_kernel");
+}
+
+int level0_smooth_dot(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega, float* out,
+                      double* dot, double scale, cudaStream_t st) {
+    EpArgs P{rhs, omega, out, nullptr, dot, scale, nullptr};
+    return launch<It::Plain, Ep::SmoothDot>(make_l0(lv), ItArgs{p, nullptr, nullptr, nullptr}, P, st,
+                                            "level0_smooth_dot_kernel");
+}
+
+int level0_prolong_smooth(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                          float omega, float* out, cudaStream_t st) {
+    EpArgs P{rhs, omega, out, nullptr, nullptr, 0.0, nullptr};
+    return launch<It::Prolonged, Ep::Smooth>(make_l0(lv), ItArgs{p, coarse, nullptr, nullptr}, P, st,
+                                             "level0_prolong_smooth_kernel");
+}
+
+int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st) {
+    EpArgs P{rhs, 0.f, r, nullptr, nullptr, 0.0, nullptr};
+    return launch<It::Plain, Ep::Residual>(make_l0(lv), ItArgs{p, nullptr, nullptr, nullptr}, P, st, "level0_residual_kernel");
+}
+
+int level0_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, cudaStream_t st) {
+    EpArgs P{rhs, 0.f, nullptr, nullptr, nullptr, 0.0, out};
+    return launch<It::Plain, Ep::ResidualMax>(make_l0(lv), ItArgs{p, nullptr, nullptr, nullptr}, P, st,
+                                              "level0_residual_max_kernel");
+}
+
+int level0_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old, const double* rz_new,
+                           const double* rz_old, float* p_out, float* q, double* pq, cudaStream_t st) {
+    EpArgs P{nullptr, 0.f, p_out, q, pq, 0.0, nullptr};
+    const ItArgs A{z, rz_old ? p_old : nullptr, rz_new, rz_old};
+    return launch<It::Direction, Ep::Apply>(make_l0(lv), A, P, st,
+                                            "level0_direction_apply_kernel");
+}
+
+int level0_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega, float* out, cudaStream_t st) {
+    const L0 g = make_l0(lv);
+    const int n4 = g.nx4 * g.ny * g.nz;
+    level0_smooth_zero_kernel<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(g, rhs, omega, out, n4);
+    return launch_status("level0_smooth_zero_kernel");
+}
+
+int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse,
+                             cudaStream_t st) {
+    const L0 g = make_l0(lv);
+    const dim3 grid((unsigned)((g.nx4 + 31) / 32), (unsigned)((g.ny / 2 + kRows - 1) / kRows),
+                    (unsigned)((g.nz + kZ4 - 1) / kZ4));
+    level0_residual_restrict_kernel<<<grid, dim3(32, kRows), 0, st>>>(g, p, rhs, coarse);
+    return launch_status("level0_residual_restrict_kernel");
+}
+
+int level0_links(int nx, int ny, int nz, const uint8_t* solid, uint8_t* links, cudaStream_t st) {
+    links_kernel<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(nx, ny, nz, solid, links);
+    return launch_status("links_kernel");
+}
+
+}  // namespace ffx

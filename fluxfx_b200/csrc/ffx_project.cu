@@ -12,6 +12,7 @@
 // ffx_common.cuh; reductions stride over z with a bounded number of blocks so
 // each block issues one atomic.
 #include "ffx_host.cuh"
+#include "ffx_level0.cuh"
 
 namespace ffx {
 namespace {
@@ -581,6 +582,145 @@ __global__ void __launch_bounds__(256) graph_level0_kernel(GLvl g, float4* out) 
     out[i] = g_edge(g, i, x, y, z);
 }
 
+// ------------------------------------------------ coarse tail of a V-cycle
+// The small coarse levels (<= kTailCells cells each) of one V-cycle in a single
+// 1024-thread block: every pass of solid_multigrid.py:46-65 on those levels
+// (pre-smoothing, fused residual + restriction, the FP64 direct solve or the
+// 80 masked sweeps on the coarsest level, fused prolongation + smoothing,
+// post-smoothing), separated by __syncthreads instead of kernel launches. Each
+// cell is evaluated with the same operations and order as the per-level
+// kernels, and the direct solve sums its rows as direct_kernel does, so the
+// results are bit-identical. Fields written inside the kernel are read with
+// plain (coherent) loads, never the read-only path.
+constexpr int kTailThreads = 1024;
+constexpr int kTailCells = 32768;
+
+struct TailLvl {
+    GLvl g;
+    float* p;
+    float* q;
+    float* rhs;
+    int n;
+};
+struct TailArgs {
+    int count, pre, post;
+    float omega;
+    const double* inverse;
+    TailLvl lv[FFX_TAIL_LEVELS];
+};
+
+__device__ __forceinline__ void tail_xyz(const GLvl& g, int i, int& x, int& y, int& z) {
+    x = i % g.nx;
+    const int r = i / g.nx;
+    y = r % g.ny;
+    z = r / g.ny;
+}
+
+__device__ __forceinline__ void tail_smooth(const TailLvl& L, const float* p, float* out, float omega, bool zero) {
+    const GLvl& g = L.g;
+    for (int i = threadIdx.x; i < L.n; i += kTailThreads) {
+        int x, y, z;
+        tail_xyz(g, i, x, y, z);
+        float diag, nb;
+        graph_terms(g, i, x, y, z, [&](int j, int, int, int) { return zero ? 0.f : p[j]; }, diag, nb);
+        const float pc = zero ? 0.f : p[i];
+        out[i] = diag > 0.f ? pc * (1.f - omega) + ((nb - L.rhs[i]) / diag) * omega : 0.f;
+    }
+    __syncthreads();
+}
+
+__device__ __forceinline__ float tail_res(const TailLvl& L, const float* p, int i, int x, int y, int z) {
+    float diag, nb;
+    graph_terms(L.g, i, x, y, z, [&](int j, int, int, int) { return p[j]; }, diag, nb);
+    return diag > 0.f ? (L.rhs[i] - nb) + diag * p[i] : 0.f;
+}
+
+__global__ void __launch_bounds__(kTailThreads) graph_tail_kernel(const __grid_constant__ TailArgs A) {
+    float* cur[FFX_TAIL_LEVELS];
+    float* spare[FFX_TAIL_LEVELS];
+    for (int k = 0; k < A.count; ++k) {
+        cur[k] = A.lv[k].p;
+        spare[k] = A.lv[k].q;
+    }
+    const int last = A.count - 1;
+    // down: zero iterate, pre-smoothing, residual restricted to the next level
+    for (int k = 0; k < last; ++k) {
+        const TailLvl& L = A.lv[k];
+        for (int s = 0; s < A.pre; ++s) {
+            tail_smooth(L, cur[k], spare[k], A.omega, s == 0);
+            float* t = cur[k]; cur[k] = spare[k]; spare[k] = t;
+        }
+        if (A.pre == 0) {
+            for (int i = threadIdx.x; i < L.n; i += kTailThreads) cur[k][i] = 0.f;
+            __syncthreads();
+        }
+        const TailLvl& C = A.lv[k + 1];
+        const GLvl& g = L.g;
+        for (int c = threadIdx.x; c < C.n; c += kTailThreads) {
+            int x, y, z;
+            tail_xyz(C.g, c, x, y, z);
+            float v = 0.f;
+            for (int dz = 0; dz < 2; ++dz)
+                for (int dy = 0; dy < 2; ++dy)
+                    for (int dx = 0; dx < 2; ++dx) {
+                        const int X = 2 * x + dx, Y = 2 * y + dy, Z = 2 * z + dz;
+                        v = v + tail_res(L, cur[k], X + g.nx * (Y + g.ny * Z), X, Y, Z);
+                    }
+            C.rhs[c] = v / 8.0f;
+        }
+        __syncthreads();
+    }
+    // coarsest level: FP64 pseudoinverse (direct_kernel's summation order) or 80 sweeps
+    {
+        const TailLvl& L = A.lv[last];
+        if (A.inverse) {
+            const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+            for (int row = warp; row < L.n; row += kTailThreads / 32) {
+                const double* r = A.inverse + (int64_t)row * L.n;
+                double s = 0.0;
+                for (int j = lane; j < L.n; j += 32) s += r[j] * (double)L.rhs[j];
+                for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+                if (lane == 0) cur[last][row] = (float)(s / (double)1.0f);
+            }
+            __syncthreads();
+        } else {
+            for (int s = 0; s < 80; ++s) {
+                tail_smooth(L, cur[last], spare[last], A.omega, s == 0);
+                float* t = cur[last]; cur[last] = spare[last]; spare[last] = t;
+            }
+        }
+    }
+    // up: prolongation fused with the first post-sweep, then the other post-sweeps
+    for (int k = last - 1; k >= 0; --k) {
+        const TailLvl& L = A.lv[k];
+        const GLvl& g = L.g;
+        const float* p = cur[k];
+        const float* coarse = cur[k + 1];
+        const int cx = g.nx / 2, cy = g.ny / 2;
+        auto pro = [&](int j, int jx, int jy, int jz) {
+            return g_active(g, j) ? p[j] + coarse[(jx >> 1) + cx * ((jy >> 1) + cy * (jz >> 1))] : 0.f;
+        };
+        for (int i = threadIdx.x; i < L.n; i += kTailThreads) {
+            int x, y, z;
+            tail_xyz(g, i, x, y, z);
+            if (A.post > 0) {
+                float diag, nb;
+                graph_terms(g, i, x, y, z, pro, diag, nb);
+                const float pc = pro(i, x, y, z);
+                spare[k][i] = diag > 0.f ? pc * (1.f - A.omega) + ((nb - L.rhs[i]) / diag) * A.omega : 0.f;
+            } else {
+                spare[k][i] = pro(i, x, y, z);
+            }
+        }
+        __syncthreads();
+        float* t = cur[k]; cur[k] = spare[k]; spare[k] = t;
+        for (int s = 1; s < A.post; ++s) {
+            tail_smooth(L, cur[k], spare[k], A.omega, false);
+            float* u = cur[k]; cur[k] = spare[k]; spare[k] = u;
+        }
+    }
+}
+
 // ------------------------------------------ Krylov acceleration (MG-PCG)
 // The projection solves L p = rhs with L the (negative semi-definite) graph
 // Laplacian. Conjugate gradients run on A = -L; `res` stores the residual in
@@ -843,6 +983,7 @@ int ffx_mg_residual_max(const int32_t n[3], const float inv[3], const float* p, 
 int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega, float* p_out,
                      void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p_in && rhs && p_out && p_in != p_out, "ffx_graph_smooth: invalid arguments");
+    if (level0_x4(lv, {p_in, rhs, p_out})) return level0_smooth(lv, p_in, rhs, omega, p_out, as_stream(stream));
     GLvl g = make_glvl(lv);
     if (!g.edges) {
         dim3 grid = cell_grid(g.nx, g.ny, (g.nz + kZ - 1) / kZ);
@@ -856,6 +997,7 @@ int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rh
 
 int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && r && r != p, "ffx_graph_residual: invalid arguments");
+    if (level0_x4(lv, {p, rhs, r})) return level0_residual(lv, p, rhs, r, as_stream(stream));
     GLvl g = make_glvl(lv);
     graph_residual_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, p, rhs, r);
     return launch_status("graph_residual_kernel");
@@ -865,6 +1007,8 @@ int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const f
                                 void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && coarse_rhs && lv->nx % 2 == 0 && lv->ny % 2 == 0 && lv->nz % 2 == 0,
                 "ffx_graph_residual_restrict: invalid arguments");
+    if (level0_x4(lv, {p, rhs}) && ((uintptr_t)coarse_rhs & 7) == 0)
+        return level0_residual_restrict(lv, p, rhs, coarse_rhs, as_stream(stream));
     GLvl g = make_glvl(lv);
     graph_residual_restrict_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0, as_stream(stream)>>>(
         g, p, rhs, coarse_rhs);
@@ -883,6 +1027,8 @@ int ffx_graph_prolong_smooth(const FfxGraphLevel* lv, const float* p, const floa
                              float omega, float* p_out, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && coarse && rhs && p_out && p != p_out && lv->nx % 2 == 0 && lv->ny % 2 == 0 &&
                 lv->nz % 2 == 0, "ffx_graph_prolong_smooth: invalid arguments");
+    if (level0_x4(lv, {p, rhs, p_out}) && ((uintptr_t)coarse & 7) == 0)
+        return level0_prolong_smooth(lv, p, coarse, rhs, omega, p_out, as_stream(stream));
     GLvl g = make_glvl(lv);
     graph_prolong_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(
         g, p, coarse, rhs, omega, p_out);
@@ -895,6 +1041,7 @@ int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float*
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), st), "ffx_graph_residual_max memset");
     if (e) return e;
+    if (level0_x4(lv, {p, rhs})) return level0_residual_max(lv, p, rhs, out, st);
     dim3 grid = cell_grid(g.nx, g.ny, 1);
     grid.z = reduce_z(g.nz);
     graph_residual_max_kernel<<<grid, cell_block(), 0, st>>>(g, p, rhs, out);
@@ -912,6 +1059,42 @@ int ffx_graph_coarsen(const FfxGraphLevel* fine, float* coarse_edges, int32_t* d
     graph_coarsen_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0, st>>>(
         g, reinterpret_cast<float4*>(coarse_edges), disconnected);
     return launch_status("graph_coarsen_kernel");
+}
+
+int ffx_graph_tail(const FfxGraphTail* t, void* stream) {
+    FFX_REQUIRE(t && t->count >= 1 && t->count <= FFX_TAIL_LEVELS && t->pre >= 0 && t->post >= 0 &&
+                t->pre <= 64 && t->post <= 64, "ffx_graph_tail: invalid arguments");
+    TailArgs A;
+    A.count = t->count;
+    A.pre = t->pre;
+    A.post = t->post;
+    A.omega = t->omega;
+    A.inverse = t->inverse;
+    for (int k = 0; k < t->count; ++k) {
+        const FfxTailLevel& L = t->levels[k];
+        const FfxGraphLevel& lv = L.level;
+        FFX_REQUIRE(glvl_ok(&lv) && lv.edges && L.p && L.q && L.rhs && L.p != L.q && L.p != L.rhs &&
+                    L.q != L.rhs && (int64_t)lv.nx * lv.ny * lv.nz <= kTailCells,
+                    "ffx_graph_tail: level %d invalid (edges, distinct p/q/rhs, <= %d cells)", k, kTailCells);
+        if (k > 0) {
+            const FfxGraphLevel& up = t->levels[k - 1].level;
+            FFX_REQUIRE(up.nx == 2 * lv.nx && up.ny == 2 * lv.ny && up.nz == 2 * lv.nz,
+                        "ffx_graph_tail: level %d is not the 2x coarsening of level %d", k, k - 1);
+        }
+        A.lv[k].g = make_glvl(&lv);
+        A.lv[k].p = L.p;
+        A.lv[k].q = L.q;
+        A.lv[k].rhs = L.rhs;
+        A.lv[k].n = lv.nx * lv.ny * lv.nz;
+    }
+    FFX_REQUIRE(!t->inverse || A.lv[t->count - 1].n <= 1024, "ffx_graph_tail: direct solve limited to 1024 cells");
+    graph_tail_kernel<<<1, kTailThreads, 0, as_stream(stream)>>>(A);
+    return launch_status("graph_tail_kernel");
+}
+
+int ffx_graph_links(const FfxGraphLevel* lv, uint8_t* links, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && !lv->edges && lv->solid && links, "ffx_graph_links: invalid arguments");
+    return level0_links(lv->nx, lv->ny, lv->nz, lv->solid, links, as_stream(stream));
 }
 
 int ffx_graph_level0_edges(const FfxGraphLevel* lv, float* edges, void* stream) {
@@ -948,6 +1131,7 @@ extern "C" {
 
 int ffx_graph_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega, float* p_out, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && rhs && p_out && rhs != p_out, "ffx_graph_smooth_zero: invalid arguments");
+    if (level0_x4(lv, {rhs, p_out})) return level0_smooth_zero(lv, rhs, omega, p_out, as_stream(stream));
     GLvl g = make_glvl(lv);
     graph_smooth_zero_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, rhs, omega, p_out);
     return launch_status("graph_smooth_zero_kernel");
@@ -961,6 +1145,7 @@ int ffx_graph_smooth_dot(const FfxGraphLevel* lv, const float* p_in, const float
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(cudaMemsetAsync(dot, 0, sizeof(double), st), "ffx_graph_smooth_dot memset");
     if (e) return e;
+    if (level0_x4(lv, {p_in, rhs, p_out})) return level0_smooth_dot(lv, p_in, rhs, omega, p_out, dot, scale, st);
     graph_smooth_dot_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, st>>>(g, p_in, rhs, omega, p_out, dot,
                                                                                  scale);
     return launch_status("graph_smooth_dot_kernel");
@@ -974,6 +1159,8 @@ int ffx_pcg_direction_apply(const FfxGraphLevel* lv, const float* z, const float
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(cudaMemsetAsync(pq, 0, sizeof(double), st), "ffx_pcg_direction_apply memset");
     if (e) return e;
+    if (level0_x4(lv, {z, rz_old ? p_old : nullptr, p_out, q}))
+        return level0_direction_apply(lv, z, p_old, rz_new, rz_old, p_out, q, pq, st);
     pcg_direction_apply_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, st>>>(g, z, p_old, rz_new, rz_old,
                                                                                     p_out, q, pq);
     return launch_status("pcg_direction_apply_kernel");

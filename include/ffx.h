@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define FFX_ABI_VERSION 1
+#define FFX_ABI_VERSION 2
 
 typedef enum FfxStatus {
     FFX_OK = 0,
@@ -226,7 +226,46 @@ typedef struct FfxGraphLevel {
     const float* edges;     /* 4 floats per cell, or NULL for level 0 */
     const uint8_t* solid;   /* level-0 mask when edges == NULL */
     float w[3];             /* level-0 conductances (n/extent)^2 */
+    const uint8_t* links;   /* optional level-0 link bytes (ffx_graph_links); with
+                               nx % 4 == 0 and 16-byte aligned fields the level-0
+                               passes run four cells per thread. NULL: derive
+                               the links from `solid` in every pass. */
 } FfxGraphLevel;
+
+/* The small coarse levels of one V-cycle in one kernel launch (one 1024-thread
+ * block). Runs, on levels[0..count-1] (coarsest last), exactly the passes of
+ * solid_multigrid.py:46-65 below the level that restricted into levels[0]:
+ * levels[k].p is zeroed, `pre` sweeps, residual restricted into
+ * levels[k+1].rhs; on the coarsest level the FP64 pseudoinverse `inverse`
+ * (n x n, n <= 1024) is applied, or, with inverse == NULL, 80 sweeps from
+ * zero; going up, prolongation fused with the first of `post` sweeps. Results
+ * are bit-identical to the per-level entry points. Each sweep alternates a
+ * level's p and q; the final iterate of levels[k] is in p when the level saw
+ * an even number of sweeps (pre + post, or 80 / 0 on the coarsest), else in q.
+ * Every level needs edges (no level 0), at most 32768 cells, and halves the
+ * shape of the one before. Replaces that part of the per-level launch
+ * sequence; no counterpart shader. */
+#define FFX_TAIL_LEVELS 8
+typedef struct FfxTailLevel {
+    FfxGraphLevel level;
+    float* p;
+    float* q;
+    float* rhs;
+} FfxTailLevel;
+typedef struct FfxGraphTail {
+    int32_t count, pre, post;
+    float omega;
+    const double* inverse;
+    FfxTailLevel levels[FFX_TAIL_LEVELS];
+} FfxGraphTail;
+int ffx_graph_tail(const FfxGraphTail* tail, void* stream);
+
+/* Level-0 link bytes from the mask: bit 2a / 2a+1 = the face to the lower /
+ * upper neighbour along axis a joins two fluid cells inside the domain, bit 6
+ * = the cell is fluid. The level-0 conductances of
+ * physics/solid_hierarchy.py:16-25 (w[a] on linked faces), one byte per cell.
+ * Needs lv->solid and lv->edges == NULL; links holds nx*ny*nz bytes. */
+int ffx_graph_links(const FfxGraphLevel* lv, uint8_t* links, void* stream);
 
 /* omega-Jacobi on the graph Laplacian; replaces shaders/solid_mg_smooth.glsl
  * (omega = 2/3 there). p_out must not alias p_in. */

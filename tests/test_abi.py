@@ -26,7 +26,7 @@ def test_library_loads_and_exports_every_symbol():
     for name in header_functions():
         assert hasattr(lib, name), name
         assert ctypes.cast(getattr(lib, name), ctypes.c_void_p).value
-    assert lib.ffx_abi_version() == 1
+    assert lib.ffx_abi_version() == 2
 
 
 def test_struct_layouts_match_the_header():
@@ -35,7 +35,7 @@ def test_struct_layouts_match_the_header():
     assert ctypes.sizeof(N.FfxSolids) == 16
     assert ctypes.sizeof(N.FfxSources) == 4 * (2 + 3 + 3 + 1 + 3 + 1 + 128)
     assert ctypes.sizeof(N.FfxScalarChannel) == 4 * 8 + 4 * 5 + 4
-    assert ctypes.sizeof(N.FfxGraphLevel) == 12 + 4 + 8 + 8 + 12 + 4
+    assert ctypes.sizeof(N.FfxGraphLevel) == 12 + 4 + 8 + 8 + 12 + 4 + 8   # ..., w[3], pad, links
 
 
 def test_argument_errors_are_reported_without_a_device():

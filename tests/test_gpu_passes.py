@@ -427,3 +427,122 @@ def test_krylov_kernels_match_numpy(D):
     re = r0 + alpha * n(q)
     assert_close(n(rs), re, rel=1e-6)
     assert float(rmax[0]) == pytest.approx(np.abs(re).max(), rel=1e-6)
+
+
+def _links_numpy(mask):
+    """Link bytes of a (nz, ny, nx) solid mask: bit 2a / 2a+1 = open face to the
+    lower / upper neighbour along axis a (x, y, z), bit 6 = fluid."""
+    fluid = ~mask
+    out = np.where(fluid, 64, 0).astype(np.uint8)
+    for a, ax in enumerate((2, 1, 0)):
+        lo = np.zeros_like(fluid)
+        hi = np.zeros_like(fluid)
+        sl_a = [slice(None)] * 3
+        sl_b = [slice(None)] * 3
+        sl_a[ax], sl_b[ax] = slice(1, None), slice(None, -1)
+        lo[tuple(sl_a)] = fluid[tuple(sl_a)] & fluid[tuple(sl_b)]
+        hi[tuple(sl_b)] = fluid[tuple(sl_b)] & fluid[tuple(sl_a)]
+        out |= np.where(lo, 1 << (2 * a), 0).astype(np.uint8)
+        out |= np.where(hi, 1 << (2 * a + 1), 0).astype(np.uint8)
+    return out
+
+
+def _bits(x):
+    torch.cuda.synchronize()
+    return x.detach().cpu().numpy().view(np.uint32)
+
+
+@pytest.mark.parametrize('shape', [(64, 20, 12), (256, 10, 10), (40, 18, 8)])
+def test_level0_four_cell_kernels_equal_scalar_kernels(D, shape):
+    """With link bytes and nx % 4 == 0 the level-0 passes run four cells per
+    thread; every field they write is bit-identical to the one-cell kernels
+    (the dot products, summed in another order, agree to 1e-12)."""
+    nx, ny, nz = shape
+    rng = np.random.default_rng(nx + ny + nz)
+    from fluxfx_b200.physics.collision import raster_reference
+    from fluxfx_b200.physics.config import GridSpec
+    grid = GridSpec(shape, axis_limit=256)
+    mask = np.asarray(raster_reference(grid, sphere_box_mask(shape))).reshape(nz, ny, nx) > 0.5
+    assert 0 < mask.sum() < mask.size
+    mask |= rng.uniform(size=mask.shape) < 0.15
+    solid_t = t(mask, torch.uint8)
+    w = [float(np.float32(c ** 2)) for c in shape]
+    scalar = N.FfxGraphLevel(*shape, None, ptr(solid_t), N.f3(*w))
+    four = N.FfxGraphLevel(*shape, None, ptr(solid_t), N.f3(*w))
+    links = torch.zeros((nz, ny, nx), dtype=torch.uint8, device='cuda')
+    D.call('ffx_graph_links', C.byref(four), ptr(links), D.s)
+    torch.cuda.synchronize()
+    assert np.array_equal(links.cpu().numpy(), _links_numpy(mask))
+    four.links = links.data_ptr()
+    cell = (nz, ny, nx)
+    p, rhs, z, pold = (t(rng.uniform(-1, 1, cell)) for _ in range(4))
+    coarse = t(rng.uniform(-1, 1, (nz // 2, ny // 2, nx // 2)))
+    rz = torch.tensor([3.0, 5.0], dtype=torch.float64, device='cuda')
+
+    def both(fn):
+        outs = []
+        for lv in (scalar, four):
+            outs.append(fn(lv))
+        return outs
+
+    def smooth(lv):
+        o = t(np.full(cell, np.nan))
+        D.call('ffx_graph_smooth', C.byref(lv), ptr(p), ptr(rhs), 2 / 3, ptr(o), D.s)
+        return o
+    a, b = both(smooth)
+    assert np.array_equal(_bits(a), _bits(b))
+
+    def zero(lv):
+        o = t(np.full(cell, np.nan))
+        D.call('ffx_graph_smooth_zero', C.byref(lv), ptr(rhs), 2 / 3, ptr(o), D.s)
+        return o
+    a, b = both(zero)
+    assert np.array_equal(_bits(a), _bits(b))
+
+    def smooth_dot(lv):
+        o = t(np.full(cell, np.nan))
+        d = torch.zeros(1, dtype=torch.float64, device='cuda')
+        D.call('ffx_graph_smooth_dot', C.byref(lv), ptr(p), ptr(rhs), 2 / 3, ptr(o), ptr(d), -1.0, D.s)
+        return o, d
+    (a, da), (b, db) = both(smooth_dot)
+    assert np.array_equal(_bits(a), _bits(b))
+    assert float(db[0]) == pytest.approx(float(da[0]), rel=1e-12)
+
+    def prolong_smooth(lv):
+        o = t(np.full(cell, np.nan))
+        D.call('ffx_graph_prolong_smooth', C.byref(lv), ptr(p), ptr(coarse), ptr(rhs), 2 / 3, ptr(o), D.s)
+        return o
+    a, b = both(prolong_smooth)
+    assert np.array_equal(_bits(a), _bits(b))
+
+    def residual(lv):
+        o = t(np.full(cell, np.nan))
+        D.call('ffx_graph_residual', C.byref(lv), ptr(p), ptr(rhs), ptr(o), D.s)
+        return o
+    a, b = both(residual)
+    assert np.array_equal(_bits(a), _bits(b))
+
+    def residual_max(lv):
+        o = torch.full((1,), -1.0, device='cuda')
+        D.call('ffx_graph_residual_max', C.byref(lv), ptr(p), ptr(rhs), ptr(o), D.s)
+        return o
+    a, b = both(residual_max)
+    assert float(a[0]) == float(b[0]) > 0
+
+    def restrict(lv):
+        o = t(np.full((nz // 2, ny // 2, nx // 2), np.nan))
+        D.call('ffx_graph_residual_restrict', C.byref(lv), ptr(p), ptr(rhs), ptr(o), D.s)
+        return o
+    a, b = both(restrict)
+    assert np.array_equal(_bits(a), _bits(b))
+
+    for first in (True, False):
+        def direction(lv):
+            pn, q = t(np.full(cell, np.nan)), t(np.full(cell, np.nan))
+            pq = torch.zeros(1, dtype=torch.float64, device='cuda')
+            D.call('ffx_pcg_direction_apply', C.byref(lv), ptr(z), None if first else ptr(pold), ptr(rz[0:1]),
+                   None if first else ptr(rz[1:2]), ptr(pn), ptr(q), ptr(pq), D.s)
+            return pn, q, pq
+        (pa, qa, sa), (pb, qb, sb) = both(direction)
+        assert np.array_equal(_bits(pa), _bits(pb)) and np.array_equal(_bits(qa), _bits(qb))
+        assert float(sb[0]) == pytest.approx(float(sa[0]), rel=1e-12)

@@ -373,3 +373,34 @@ def test_graph_replay_matches_eager_launches(D, method):
     assert graphed._graphs and not eager._graphs
     graphed.close()
     eager.close()
+
+
+@pytest.mark.parametrize('method,coarse', [('VCYCLE', 'DIRECT'), ('PCG', 'DIRECT'), ('VCYCLE', 'SMOOTH')])
+def test_coarse_tail_matches_per_level_launches(D, method, coarse):
+    """The small coarse levels run as one single-block launch (ffx_graph_tail);
+    the solve is bit-identical to launching every pass of those levels."""
+    from fluxfx_b200.backend.collision import SolidDevice
+    from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
+    grid = GridSpec((32, 32, 32))
+    sd = SolidDevice(grid, sphere_box_mask(grid.shape, grid.extent), D)
+    s = PressureSettings(pressure_tolerance=1e-5, pressure_max_cycles=40, pressure_method=method,
+                         coarse_solver=coarse)
+    tail, plain = SolidMultigridProjector(grid, s, sd), SolidMultigridProjector(grid, s, sd)
+    plain.use_tail = False
+    assert [lv['shape'] for lv in tail.levels] == [(32, 32, 32), (16, 16, 16), (8, 8, 8), (4, 4, 4)]
+    assert tail.tail_start == 2
+    assert (tail.coarse_matrix is not None) == (coarse == 'DIRECT')
+    rng = np.random.default_rng(11)
+    out_t = [D.texture(fs) for fs in grid.face_shapes]
+    out_p = [D.texture(fs) for fs in grid.face_shapes]
+    for dt in (0.02, 0.01):
+        fields = [D.texture(fs, rng.uniform(-1, 1, fs[0] * fs[1] * fs[2]), nonnegative=False)
+                  for fs in grid.face_shapes]
+        tail.project(fields, out_t, dt)
+        plain.project(fields, out_p, dt)
+        assert tail.last_cycles == plain.last_cycles > 1
+        assert tail.last_iterations == plain.last_iterations
+        for a in range(3):
+            assert np.array_equal(n(out_t[a]), n(out_p[a])), a
+    tail.close()
+    plain.close()
