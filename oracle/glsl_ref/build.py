@@ -6,8 +6,9 @@ Reads the shader sources where they lie in the reference checkout, writes
 build inputs and the library only under ``oracle/_ref/``:
 
 * ``oracle/_ref/gen/*.glsl`` -- the shader files, unchanged except that GLSL
-  ``out`` parameters become C++ references (``out float x`` -> ``float& x``,
-  the only construct C++ cannot parse; used by solid_mg_operator.glsl);
+  ``out`` parameters become C++ references (``out float x`` -> ``float& x``;
+  used by solid_mg_operator.glsl) and the ``.xyz`` swizzle becomes a call
+  ``.xyz()`` (used by confinement.glsl) -- the two constructs C++ cannot parse;
 * ``oracle/_ref/libglsl_ref.so`` -- ``oracle/glsl_ref/kernels.cpp`` compiled
   with g++ -fsingle-precision-constant -ffp-contract=off -fopenmp.
 
@@ -25,6 +26,7 @@ GEN = OUT / 'gen'
 LIB = OUT / 'libglsl_ref.so'
 DEFAULT_SHADERS = Path('/root/reference/FluxFX_Source/fluxfx/shaders')
 OUT_PARAM = re.compile(r'\bout\s+(float|int|vec2|vec3|vec4|ivec3)\s+(\w+)')
+SWIZZLE_XYZ = re.compile(r'(?<!gl_GlobalInvocationID)\.xyz\b(?!\s*\()')
 
 
 def build(shaders=DEFAULT_SHADERS, force=False):
@@ -39,7 +41,7 @@ def build(shaders=DEFAULT_SHADERS, force=False):
     if LIB.exists() and not force and LIB.stat().st_mtime >= newest:
         return LIB
     for src in sources:
-        text = OUT_PARAM.sub(r'\1& \2', src.read_text())
+        text = SWIZZLE_XYZ.sub('.xyz()', OUT_PARAM.sub(r'\1& \2', src.read_text()))
         (GEN / src.name).write_text(text)
     cmd = ['g++', '-O2', '-std=c++17', '-fPIC', '-shared', '-fopenmp', '-fsingle-precision-constant',
            '-ffp-contract=off', '-fno-fast-math', '-w', '-I', str(HERE), '-I', str(GEN),

@@ -79,7 +79,7 @@ class GlslCpuDevice:
         return Texture(shape, channels, values)
 
     def kernel(self, filename, constants=(), sample_input=False, samplers=(), includes=(), output_format='R32F'):
-        collisions = int('solid_boundary.glsl' in includes)
+        collisions = 2 if 'moving_boundary.glsl' in includes else int('solid_boundary.glsl' in includes)
         kid = self.lib.glsl_ref_kernel(filename.encode(), collisions)
         return Shader(filename, kid)
 

@@ -62,6 +62,7 @@ struct vec4 {
     vec4(const vec3& p, float s) : x(p.x), y(p.y), z(p.z), w(s) {}
     float& operator[](int i) { return v[i]; }
     float operator[](int i) const { return v[i]; }
+    vec3 xyz() const { return vec3(x, y, z); }   // the build recipe rewrites `.xyz` reads to `.xyz()`
 };
 
 struct bvec3 { bool x, y, z; };
@@ -122,6 +123,9 @@ inline vec3 mix(const vec3& x, const vec3& y, float a) { return mix(x, y, vec3(a
 inline float dot(const vec3& a, const vec3& b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 inline float dot(const vec4& a, const vec4& b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
 inline float length(const vec3& a) { return sqrt(dot(a, a)); }
+inline vec3 cross(const vec3& a, const vec3& b) {
+    return vec3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x);
+}
 inline float distance(const vec3& a, const vec3& b) { return length(a - b); }
 
 inline bvec3 lessThan(const vec3& a, const vec3& b) { return {a.x < b.x, a.y < b.y, a.z < b.z}; }

@@ -31,11 +31,12 @@ vec3 domainExtent, cellCount, faceOffset, axisMask, invCell, sourceCenter, sourc
 vec4 row0, row1, row2;
 float dt, relaxation, componentAxis, factor, sourceRadius, sourceProfile, sourceRate, dissipation, targetDensity,
     correctedTransport, correctedVelocity, emissionCoupling, sourceCount, scalarChannel, thermalLift, densityWeight,
-    seedTemperature, angularSpeed, shapeKind;
+    seedTemperature, angularSpeed, shapeKind, curlStrength, forceLimit, ignitionTemperature, burnRate, yieldValue,
+    owner;
 // samplers and the output image
 sampler3D inputField, velocityU, velocityV, velocityW, divergenceField, pressureField, coarseField, inverseField,
     edgeField, solidField, densityField, temperatureField, predictorField, reverseField, originalFaceField,
-    facePredictor, sourceTable;
+    facePredictor, sourceTable, curlField, burnField, boundaryField, oldSolidField, wallTable;
 image3D outputField;
 }  // namespace glsl_state
 
@@ -149,6 +150,32 @@ FFX_KERNEL_BEGIN(k_solid_mg_direct)
 #include "solid_mg_direct.glsl"
 FFX_KERNEL_END
 
+// ------------------------------------------- fire-config passes (C5 rows)
+FFX_KERNEL_BEGIN(k_curl)
+#include "curl.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_confinement)
+#include "confinement.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_combustion_burn)
+#include "combustion_burn.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_combustion_apply)
+#include "combustion_apply.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_moving_mask)
+#include "moving_mask.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_moving_wall)
+#include "moving_wall.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_moving_remap_scalar)
+#include "moving_remap_scalar.glsl"
+FFX_KERNEL_END
+FFX_KERNEL_BEGIN(k_moving_remap_face)
+#include "moving_remap_face.glsl"
+FFX_KERNEL_END
+
 // ---------------------------------------------- collider-decorated variants
 // solid_boundary.glsl #defines FLUXFX_COLLISIONS; it is undefined again after
 // every variant so the next namespace starts clean.
@@ -220,6 +247,30 @@ FFX_KERNEL_BEGIN(ks_multi_advect_scalar)
 FFX_KERNEL_END
 #undef FLUXFX_COLLISIONS
 
+// Moving colliders (backend/moving_collision.py:23-37): walls and gradient get
+// solid_boundary.glsl + moving_boundary.glsl (FLUXFX_MOVING_COLLIDERS, wall
+// velocities from boundaryField; variant 2); the divergence gets
+// solid_boundary.glsl (variant 1).
+FFX_KERNEL_BEGIN(km_pressure_walls)
+#include "solid_boundary.glsl"
+#include "moving_boundary.glsl"
+#include "pressure_walls.glsl"
+FFX_KERNEL_END
+#undef FLUXFX_COLLISIONS
+#undef FLUXFX_MOVING_COLLIDERS
+FFX_KERNEL_BEGIN(km_pressure_gradient)
+#include "solid_boundary.glsl"
+#include "moving_boundary.glsl"
+#include "pressure_gradient.glsl"
+FFX_KERNEL_END
+#undef FLUXFX_COLLISIONS
+#undef FLUXFX_MOVING_COLLIDERS
+FFX_KERNEL_BEGIN(km_pressure_divergence)
+#include "solid_boundary.glsl"
+#include "pressure_divergence.glsl"
+FFX_KERNEL_END
+#undef FLUXFX_COLLISIONS
+
 // ------------------------------------------------------------------ tables
 namespace {
 using namespace glsl;
@@ -270,6 +321,17 @@ const KernelEntry kKernels[] = {
     {"emitting_advect_velocity.glsl", 1, ks_emitting_advect_velocity::main},
     {"multi_advect_velocity.glsl", 1, ks_multi_advect_velocity::main},
     {"multi_advect_scalar.glsl", 1, ks_multi_advect_scalar::main},
+    {"curl.glsl", 0, k_curl::main},
+    {"confinement.glsl", 0, k_confinement::main},
+    {"combustion_burn.glsl", 0, k_combustion_burn::main},
+    {"combustion_apply.glsl", 0, k_combustion_apply::main},
+    {"moving_mask.glsl", 0, k_moving_mask::main},
+    {"moving_wall.glsl", 0, k_moving_wall::main},
+    {"moving_remap_scalar.glsl", 0, k_moving_remap_scalar::main},
+    {"moving_remap_face.glsl", 0, k_moving_remap_face::main},
+    {"pressure_walls.glsl", 2, km_pressure_walls::main},
+    {"pressure_gradient.glsl", 2, km_pressure_gradient::main},
+    {"pressure_divergence.glsl", 1, km_pressure_divergence::main},
 };
 
 struct FloatSlot {
@@ -289,6 +351,9 @@ const FloatSlot kFloats[] = {
     {"emissionCoupling", &emissionCoupling, 1}, {"sourceCount", &sourceCount, 1},
     {"scalarChannel", &scalarChannel, 1}, {"thermalLift", &thermalLift, 1}, {"densityWeight", &densityWeight, 1},
     {"seedTemperature", &seedTemperature, 1}, {"angularSpeed", &angularSpeed, 1}, {"shapeKind", &shapeKind, 1},
+    {"curlStrength", &curlStrength, 1}, {"forceLimit", &forceLimit, 1},
+    {"ignitionTemperature", &ignitionTemperature, 1}, {"burnRate", &burnRate, 1}, {"yieldValue", &yieldValue, 1},
+    {"owner", &owner, 1},
 };
 
 struct SamplerSlot {
@@ -301,7 +366,8 @@ const SamplerSlot kSamplers[] = {
     {"inverseField", &inverseField}, {"edgeField", &edgeField}, {"solidField", &solidField},
     {"densityField", &densityField}, {"temperatureField", &temperatureField}, {"predictorField", &predictorField},
     {"reverseField", &reverseField}, {"originalFaceField", &originalFaceField}, {"facePredictor", &facePredictor},
-    {"sourceTable", &sourceTable},
+    {"sourceTable", &sourceTable}, {"curlField", &curlField}, {"burnField", &burnField},
+    {"boundaryField", &boundaryField}, {"oldSolidField", &oldSolidField}, {"wallTable", &wallTable},
 };
 
 long long g_total_out_of_range = 0;

@@ -58,6 +58,7 @@ class Grid:
         self.face_shapes = ((nz, ny, nx + 1), (nz, ny + 1, nx), (nz + 1, ny, nx))
         self.mask = None
         self.halo = None
+        self.boundary = None      # moving colliders: wall velocity per face grid (moving_wall.glsl)
         if mask is not None:
             self.set_mask(mask)
 
@@ -640,7 +641,9 @@ def walls(g, vel):
         wall = (c[axis] == 0) | (c[axis] == n - 1)
         if g.mask is not None:
             wall |= solid_face(g, x, y, z, axis)
-        out.append(np.where(wall, g.f(0), vel[axis]))
+        # moving colliders: walls take the wall velocity (FLUXFX_MOVING_COLLIDERS, pressure_walls.glsl:10-12)
+        wall_value = g.f(0) if g.boundary is None else g.boundary[axis]
+        out.append(np.where(wall, wall_value, vel[axis]))
     return tuple(out)
 
 
@@ -760,7 +763,9 @@ def gradient(g, bounded, p, dt):
         lo = list(hi)
         lo[axis] = np.clip(c[axis] - 1, 0, g.shape[axis] - 1)
         grad = (p[hi[2], hi[1], hi[0]] - p[lo[2], lo[1], lo[0]]) * g.inv[axis]
-        out.append(np.where(opened, bounded[axis] - dtf * grad, f(0)))
+        # moving colliders: closed faces take the wall velocity (pressure_gradient.glsl:11-13)
+        closed = f(0) if g.boundary is None else g.boundary[axis]
+        out.append(np.where(opened, bounded[axis] - dtf * grad, closed))
     return tuple(out)
 
 

@@ -21,6 +21,7 @@ from math import ceil
 
 import numpy as np
 
+from . import fire as F
 from . import smoke as S
 
 
@@ -168,8 +169,17 @@ def projector_kind(grid_shape, settings, has_mask):
 class OracleSmoke:
     """Field state and step sequence of ``DenseProjectedSmoke``."""
 
-    def __init__(self, shape, extent, settings, dtype=np.float32, mask=None, kind=None):
+    def __init__(self, shape, extent, settings, dtype=np.float32, mask=None, kind=None, colliders=None):
+        """``colliders``: ((shape, inverse_rows), ...) of moving colliders
+        (settings.moving_colliders); their FP32 owner mask replaces ``mask``."""
+        self.colliders = tuple(colliders) if colliders is not None else None
+        if self.colliders is not None:
+            g0 = S.Grid(shape, extent, dtype)
+            self.owners = F.moving_mask(g0, self.colliders)
+            mask = self.owners > 0.5
         self.g = S.Grid(shape, extent, dtype, mask)
+        if self.colliders is not None:
+            self.g.boundary = tuple(self.g.zeros(fs) for fs in self.g.face_shapes)
         self.s = settings
         self.kind = kind or projector_kind(tuple(shape), settings, mask is not None)
         self.projector = OracleProjector(self.g, settings, self.kind)
@@ -191,6 +201,8 @@ class OracleSmoke:
         if g.mask is not None:
             self.density = np.where(g.mask, g.f(0), self.density)
             self.temperature = np.where(g.mask, g.f(0), self.temperature)
+        self.fuel = g.zeros(g.cell_shape) if s.combustion_enabled else None
+        self.flame = g.zeros(g.cell_shape) if s.combustion_enabled else None
         self.projector.reset()
         self.velocity = S.walls(g, self.velocity)
         self.time = 0.0
@@ -233,6 +245,9 @@ class OracleSmoke:
         new = [S.advect_velocity_face(g, vel, preds[a], a, dt, detail, s.velocity_blend,
                                       emitter=emitter, sources=table) for a in range(3)]
         new[2] = S.buoyancy(g, new[2], self.density, self.temperature, dt, s.thermal_lift, s.density_weight)
+        if s.vorticity_strength > 0:
+            # confinement of the provisional (unwalled) velocity before projection (projected.py:172-175)
+            new = F.confine(g, new, F.curl(g, new), dt, s.vorticity_strength, s.vorticity_limit)
         out, self.before, self.after = self.projector.project(tuple(new), dt)
         self.velocity = out
         corrected = s.scalar_advection == 'MACCORMACK'
@@ -240,6 +255,8 @@ class OracleSmoke:
                      s.source_rate if s.density_mode == 'TARGET' else -1.0),
                     (1, self.temperature, s.heat_source_rate, s.cooling,
                      s.heat_source_rate if s.heat_mode == 'TARGET' else -1.0)]
+        if self.fuel is not None:
+            channels.append((2, self.fuel, s.fuel_source_rate, 0.0, -1.0))
         results = []
         for ch, field, rate, decay, target in channels:
             if corrected:
@@ -250,9 +267,34 @@ class OracleSmoke:
             results.append(S.advect_scalar(g, out, field, pred, rev, dt, corrected, rate, decay, target,
                                            emitter=emitter, sources=table, channel=ch,
                                            target_heat=s.heat_mode == 'TARGET'))
-        self.density, self.temperature = results
+        self.density, self.temperature = results[:2]
+        if self.fuel is not None:
+            # combustion after transport (backend/combustion.py:21-31)
+            self.fuel = results[2]
+            self.flame = F.burn(g, self.fuel, self.temperature, dt, s.ignition_temperature, s.burn_rate)
+            self.fuel = F.apply_burn(g, self.fuel, self.flame, dt, -1.0)
+            self.density = F.apply_burn(g, self.density, self.flame, dt, s.smoke_yield)
+            self.temperature = F.apply_burn(g, self.temperature, self.flame, dt, s.heat_yield)
         self.time += dt
         self.steps += 1
+
+    def move_colliders(self, colliders, dt):
+        """New collider poses before a step (backend/moving_collision.py:44-82):
+        owner mask, rigid wall velocities, remap of the fields."""
+        g = self.g
+        colliders = tuple(colliders)
+        old = self.owners
+        self.owners = F.moving_mask(g, colliders)
+        table = F.velocity_table([c[1] for c in self.colliders], [c[1] for c in colliders], dt)
+        g.boundary = F.moving_walls(g, self.owners, table)
+        self.colliders = colliders
+        g.set_mask(self.owners > 0.5)
+        self.density = F.remap_scalar(g, self.density, self.owners, old)
+        self.temperature = F.remap_scalar(g, self.temperature, self.owners, old)
+        self.velocity = F.remap_faces(g, self.velocity, self.owners, old, g.boundary)
+        if self.fuel is not None:
+            self.fuel = F.remap_scalar(g, self.fuel, self.owners, old)
+            self.flame = g.zeros(g.cell_shape)
 
     def rel_div(self):
         b = float(np.abs(self.before.astype(np.float64)).max())
