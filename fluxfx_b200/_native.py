@@ -38,7 +38,7 @@ class FfxGrid(C.Structure):
 
 
 class FfxSolids(C.Structure):
-    _fields_ = [('solid', vp), ('halo', vp)]
+    _fields_ = [('solid', vp), ('halo', vp), ('wall', vp * 3)]
 
 
 class FfxSources(C.Structure):
@@ -61,6 +61,7 @@ class FfxGraphLevel(C.Structure):
 
 
 TAIL_LEVELS = 8
+MOVING_MAX = 8
 
 
 class FfxTailLevel(C.Structure):
@@ -115,8 +116,15 @@ _PROTOTYPES = {
     'ffx_graph_level0_edges': (C.c_int, [P(FfxGraphLevel), vp, vp]),
     'ffx_graph_links': (C.c_int, [P(FfxGraphLevel), vp, vp]),
     'ffx_graph_tail': (C.c_int, [P(FfxGraphTail), vp]),
+    'ffx_curl': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, vp]),
+    'ffx_confine': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp]),
+    'ffx_combustion': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, f32, f32, f32, f32, vp, vp, vp, vp, vp]),
+    'ffx_moving_mask': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp]),
+    'ffx_moving_walls': (C.c_int, [P(FfxGrid), vp, C.c_int, vp, vp, vp, vp, vp]),
+    'ffx_moving_remap': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp, vp]),
     'ffx_graph_smooth_zero': (C.c_int, [P(FfxGraphLevel), vp, f32, vp, vp]),
     'ffx_graph_smooth_dot': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp, C.c_double, vp]),
+    'ffx_graph_prolong_smooth_dot': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, f32, vp, vp, C.c_double, vp]),
     'ffx_pcg_direction_apply': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp, vp, vp, vp, vp]),
     'ffx_pcg_update': (C.c_int, [i64, vp, vp, vp, vp, vp, vp, vp, vp]),
     'ffx_dot': (C.c_int, [i64, vp, vp, C.c_double, vp, vp]),
@@ -149,7 +157,7 @@ def load(path=None):
         fn = getattr(lib, name)
         fn.restype = res
         fn.argtypes = args
-    if lib.ffx_abi_version() != 2:
+    if lib.ffx_abi_version() != 3:
         raise NativeUnavailable("libffx_core ABI version mismatch")
     if path is None:
         _LIB = lib

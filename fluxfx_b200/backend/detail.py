@@ -12,7 +12,7 @@ from math import prod
 import torch
 
 from .. import _native as N
-from .device import ptr
+from .device import ptr, solids_struct
 from .mac import VELOCITY_NAMES
 
 
@@ -23,9 +23,7 @@ class DetailPasses:
         self.dtype = dtype
         self._storage = N.FFX_F32 if dtype == torch.float32 else N.FFX_BF16
         self._g = N.grid_struct(grid.shape, grid.extent)
-        mask = getattr(device, 'mask', None)
-        halo = getattr(device, 'halo', None)
-        self._solids = N.FfxSolids(ptr(mask) if mask is not None else None, ptr(halo) if halo is not None else None)
+        self._solids = solids_struct(device)
         self.predictor = self.reverse = None
         self.predictors = self.reverses = None
         self.face_predictor = None
@@ -36,7 +34,7 @@ class DetailPasses:
         size = 2 if self.dtype == torch.bfloat16 else 4
         scalar = sum(t.numel() for t in (self.predictors or []) + (self.reverses or [])) * size
         faces = size * sum(prod(s) for s in self.grid.face_shapes) if self.face_predictor is not None else 0
-        return scalar + faces
+        return scalar + faces + (self.curl.numel() * 4 if self.curl is not None else 0)
 
     def _ensure_scalar(self, count):
         if self.predictors is None or len(self.predictors) < count:
@@ -71,8 +69,18 @@ class DetailPasses:
                          *[ptr(f) for f in fields], dt, *[ptr(p) for p in self.face_predictor], self.device.s)
 
     def confine(self, fields, outputs, dt, strength, limit):
-        raise NotImplementedError("Vorticity confinement is not part of this build")
+        """Vorticity confinement (``backend/detail.py:39-49``): cell curl
+        (omega, |omega|) into ``self.curl``, then every face of ``outputs`` =
+        ``fields`` + dt * confinement force."""
+        if self.curl is None:
+            nx, ny, nz = self.grid.shape
+            self.curl = torch.zeros((nz, ny, nx, 4), dtype=torch.float32, device=self.device.device)
+        gp, s = C.byref(self._g), self.device.s
+        self.device.call('ffx_curl', gp, self._storage, *[ptr(f) for f in fields], ptr(self.curl), s)
+        self.device.call('ffx_confine', gp, self._storage, ptr(self.curl), *[ptr(f) for f in fields], dt, strength,
+                         limit, *[ptr(o) for o in outputs], s)
 
     def close(self):
         self.predictor = self.reverse = self.predictors = self.reverses = None
         self.face_predictor = None
+        self.curl = None

@@ -189,6 +189,20 @@ def ptr(t):
     return C.c_void_p(0 if t is None else t.data_ptr())
 
 
+def solids_struct(device):
+    """FfxSolids of a (collider) device: its mask and dilated mask, plus the
+    wall-velocity faces of moving colliders. The tensors are updated in place
+    when colliders move, so the struct stays valid."""
+    mask = getattr(device, 'mask', None)
+    halo = getattr(device, 'halo', None)
+    walls = getattr(device, 'walls', None)
+    s = N.FfxSolids(ptr(mask) if mask is not None else None, ptr(halo) if halo is not None else None)
+    if walls is not None:
+        for a in range(3):
+            s.wall[a] = walls[a].data_ptr()
+    return s
+
+
 def storage_code(dtype):
     if dtype == torch.float32:
         return N.FFX_F32

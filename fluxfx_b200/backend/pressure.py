@@ -15,7 +15,7 @@ import torch
 from .. import _native as N
 from ..physics.config import validate_dt
 from ..physics.pressure import PressureSettings
-from .device import CudaDevice, KernelHandle, ptr
+from .device import CudaDevice, KernelHandle, ptr, solids_struct
 
 
 class PressureProjector:
@@ -27,10 +27,8 @@ class PressureProjector:
         self._g = N.grid_struct(grid.shape, grid.extent)
         self._field_dtype = torch.bfloat16 if self.settings.storage == 'BF16' else torch.float32
         self._storage = N.FFX_F32 if self._field_dtype == torch.float32 else N.FFX_BF16
-        mask = getattr(self.device, 'mask', None)
-        halo = getattr(self.device, 'halo', None)
-        self._mask = mask
-        self._solids = N.FfxSolids(ptr(mask) if mask is not None else None, ptr(halo) if halo is not None else None)
+        self._mask = getattr(self.device, 'mask', None)
+        self._solids = solids_struct(self.device)
         self.wall = KernelHandle('pressure_walls.glsl')
         self.divergence = KernelHandle('pressure_divergence.glsl')
         self.jacobi = KernelHandle('pressure_jacobi.glsl')

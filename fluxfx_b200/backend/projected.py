@@ -13,6 +13,11 @@ Drop-in for FluxFX ``fluxfx/backend/projected.py:13-229``
    temperature together) and ``ffx_advect_scalars`` (both channels, decay and
    emission) -- one launch per pass for both scalars.
 
+Fire configuration (``projected.py:161-200``): vorticity confinement between
+buoyancy and projection (``ffx_curl`` + ``ffx_confine``), fuel as a third
+transported scalar and ``ffx_combustion`` after transport, moving colliders
+through ``move_colliders`` (``MovingSolidDevice``).
+
 Extensions: ``settings.storage == 'BF16'`` stores velocity and scalars in
 bfloat16 (FP32 arithmetic); ``heat_mode == 'TARGET'`` raises temperature to the
 emitter value instead of adding a rate.
@@ -28,7 +33,7 @@ from ..physics.interaction import validate_live_update
 from ..physics.pressure import PressureSettings
 from .dense import SEED_CONSTANTS
 from .detail import DetailPasses
-from .device import ptr
+from .device import ptr, solids_struct
 from .mac import FACE_CONSTANTS, VELOCITY_NAMES
 from .pressure import PressureProjector
 from .thermal import DenseThermalAdvection
@@ -46,13 +51,15 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             from .solid_multigrid import SolidMultigridProjector
             grid = grid or GridSpec()
             if settings.moving_colliders:
-                raise ValueError('Moving colliders are not part of this build; use static colliders')
-            device = self.solids = SolidDevice(grid, colliders, device)
-            projector_class = SolidMultigridProjector if use_multigrid(grid, settings) else SolidPressureProjector
-        if settings.combustion_enabled:
-            raise ValueError('Combustion is not part of this build')
-        if settings.turbulence_strength > 0 or settings.vorticity_strength > 0:
-            raise ValueError('Turbulence and vorticity confinement are not part of this build')
+                from .moving_collision import MovingSolidDevice
+                device = self.solids = MovingSolidDevice(grid, colliders, device)
+                # the reference projects moving-collider scenes with masked Jacobi (projected.py:28)
+                projector_class = projector_class or SolidPressureProjector
+            else:
+                device = self.solids = SolidDevice(grid, colliders, device)
+                projector_class = SolidMultigridProjector if use_multigrid(grid, settings) else SolidPressureProjector
+        if settings.turbulence_strength > 0:
+            raise ValueError('Turbulence is not part of this build')
         self.projector = None
         self.detail = None
         self.turbulence = None
@@ -67,19 +74,24 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             projector_class = MultigridPressureProjector if use_multigrid(self.grid, self.settings) else PressureProjector
         self.projector = projector_class(self.grid, self.settings, self.device)
         self.detail = DetailPasses(self.grid, self.device, self._field_dtype)
-        self._solids = N.FfxSolids(*(ptr(t) if t is not None else None
-                                     for t in ((self.solids.mask, self.solids.halo) if self.solids else (None, None))))
+        if self.settings.combustion_enabled:
+            from .combustion import CombustionPasses
+            self.combustion = CombustionPasses(self.grid, self.device, self._field_dtype)
+        self._solids = solids_struct(self.solids) if self.solids is not None else N.FfxSolids()
         self._maxima = torch.zeros(3, dtype=torch.float32, device=self.device.device)
         self.reset()
 
     @property
     def allocated_bytes(self):
-        extra = self.solids.allocated_bytes if self.solids else 0
+        extra = (self.solids.allocated_bytes if self.solids else 0) + (self.combustion.allocated_bytes
+                                                                       if self.combustion else 0)
         return super().allocated_bytes + extra + self.projector.allocated_bytes + self.detail.allocated_bytes
 
     def reset(self, seed=True):
         super().reset(seed)
         self.faulted = False
+        if self.combustion is not None:
+            self.combustion.reset()
         if self.solids is not None:
             self.solids.clear_solid(self._front, self._back)
             self._front, self._back = self._back, self._front
@@ -119,7 +131,19 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         self.projector.settings = settings
 
     def move_colliders(self, colliders, dt):
-        raise ValueError('Enable Moving colliders and Reset first')
+        """New collider poses before a step (``projected.py:103-115``)."""
+        if not self.settings.moving_colliders or self.solids is None:
+            raise ValueError('Enable Moving colliders and Reset first')
+        validate_dt(dt)
+        if self.faulted:
+            raise RuntimeError('Reset required after a failed GPU step')
+        try:
+            self.solids.update(colliders, dt)
+            self.solids.remap(self)
+            self.projector.ready = False
+        except Exception:
+            self.faulted = True
+            raise
 
     def measure_projection(self):
         return self.projector.metrics() | {"step": self.steps, "simulation_time": self.time}
@@ -181,15 +205,25 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         else:
             pred = [None, None, None]
         proj = self.projector
+        confine = s.vorticity_strength > 0
+        # with confinement the wall condition waits for the projection, as in
+        # the reference (confinement reads the provisional, unwalled faces)
         dev.call('ffx_advect_velocity', gp, sp, self._storage, *vel, *pred, dt, int(corrected_v), s.velocity_blend,
-                 C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift, s.density_weight, 1,
-                 *[ptr(b) for b in proj.bounded], st)
+                 C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift, s.density_weight,
+                 int(not confine), *[ptr(b) for b in proj.bounded], st)
         self._mark('velocity_transport')
         # The old velocity is consumed: the corrected field is written over it.
-        proj.project_bounded(self._velocity, dt)
+        if confine:
+            self.detail.confine(proj.bounded, self._velocity, dt, s.vorticity_strength, s.vorticity_limit)
+            self._mark('confinement')
+            proj.project(self._velocity, self._velocity, dt)
+        else:
+            proj.project_bounded(self._velocity, dt)
         self._mark('projection')
         corrected_s = s.scalar_advection == "MACCORMACK"
         fields = [self._front, self._temperature]
+        if self.combustion is not None:
+            fields.append(self.combustion.fuel)
         if corrected_s:
             preds, revs = self.detail.transport_many(fields, self._velocity, dt)
             self._mark('scalar_predictor_reverse')
@@ -198,16 +232,25 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         outs = [self._back, self._temperature_back]
         density_target = s.source_rate if s.density_mode == "TARGET" else -1.0
         heat_target = s.heat_source_rate if s.heat_mode == "TARGET" else -1.0
-        chans = (N.FfxScalarChannel * 2)(
-            N.FfxScalarChannel(ptr(fields[0]), ptr(preds[0]), ptr(revs[0]), ptr(outs[0]), s.source_rate,
-                               s.dissipation, density_target, 0, 0),
-            N.FfxScalarChannel(ptr(fields[1]), ptr(preds[1]), ptr(revs[1]), ptr(outs[1]), s.heat_source_rate,
-                               s.cooling, heat_target, 1, int(s.heat_mode == "TARGET")))
+        chans = [N.FfxScalarChannel(ptr(fields[0]), ptr(preds[0]), ptr(revs[0]), ptr(outs[0]), s.source_rate,
+                                    s.dissipation, density_target, 0, 0),
+                 N.FfxScalarChannel(ptr(fields[1]), ptr(preds[1]), ptr(revs[1]), ptr(outs[1]), s.heat_source_rate,
+                                    s.cooling, heat_target, 1, int(s.heat_mode == "TARGET"))]
+        if self.combustion is not None:
+            # fuel: third channel, additive emission (fuel_rate column / fuel_source_rate), no decay
+            chans.append(N.FfxScalarChannel(ptr(fields[2]), ptr(preds[2]), ptr(revs[2]), ptr(self.combustion.spare),
+                                            s.fuel_source_rate, 0.0, -1.0, 2, 0))
+        arr = (N.FfxScalarChannel * len(chans))(*chans)
         dev.call('ffx_advect_scalars', gp, sp, self._storage, *[ptr(f) for f in self._velocity], dt,
-                 int(corrected_s), C.byref(src), 2, chans, ptr(self._maxima), st)
+                 int(corrected_s), C.byref(src), len(chans), arr, ptr(self._maxima), st)
         self._mark('scalar_transport')
         self._front, self._back = self._back, self._front
         self._temperature, self._temperature_back = self._temperature_back, self._temperature
+        if self.combustion is not None:
+            c = self.combustion
+            c.fuel, c.spare = c.spare, c.fuel
+            c.react(self, dt)
+            self._mark('combustion')
         self.time += dt
         self.steps += 1
 
@@ -221,7 +264,9 @@ class DenseProjectedSmoke(DenseThermalAdvection):
                 raise ValueError('Add a collider and Reset for collision display')
             return self.solids.mask
         if channel in {'FUEL', 'FLAME'}:
-            raise ValueError('Enable combustion and Reset for fuel/flame display')
+            if self.combustion is None:
+                raise ValueError('Enable combustion and Reset for fuel/flame display')
+            return self.combustion.fuel if channel == 'FUEL' else self.combustion.flame
         return self.temperature if channel == 'TEMPERATURE' else self.density
 
     def close(self):
@@ -231,6 +276,9 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         if self.detail is not None:
             self.detail.close()
         self.detail = None
+        if self.combustion is not None:
+            self.combustion.close()
+        self.combustion = None
         super().close()
         if self.solids is not None:
             self.solids.close()

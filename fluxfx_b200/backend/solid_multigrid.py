@@ -208,6 +208,12 @@ class SolidMultigridProjector(SolidPressureProjector):
         else:
             coarse['p'].zero_()
             self.cycle(index + 1)
+        if self.post_sweeps == 1 and dot is not None:
+            dev.call('ffx_graph_prolong_smooth_dot', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
+                     ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), ptr(dot), -1.0, dev.s)
+            level['p'], level['q'] = level['q'], level['p']
+            self.last_iterations += 1
+            return
         if self.post_sweeps > 0:
             dev.call('ffx_graph_prolong_smooth', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), dev.s)

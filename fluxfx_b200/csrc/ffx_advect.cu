@@ -116,7 +116,8 @@ __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const u
     }
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
-    F3 v0 = velocity_at<T, P2>(d, F, p);
+    F3 v0 = velocity_at_start<T, P2>(d, F, p, 2 * f.x + (f.axis != 0), 2 * f.y + (f.axis != 1),
+                                       2 * f.z + (f.axis != 2));
     F3 dep = backtrace<T, MASK, P2>(d, F, solid, halo, p, v0, dt);
     const T* src = f.axis == 0 ? F.u : (f.axis == 1 ? F.v : F.w);
     float value = sample_face(src, f.sx, f.sy, f.sz, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
@@ -137,6 +138,7 @@ struct VelParams {
     const T* density;
     const T* temperature;
     T* out[3];
+    Walls walls;      // wall velocities of the fused wall condition (moving colliders)
     SrcDev src;
 };
 
@@ -153,7 +155,8 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
         float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
         F3 p = {dv_n<P2>(d, ((float)f.x + off[0]) * d.e[0], 0), dv_n<P2>(d, ((float)f.y + off[1]) * d.e[1], 1),
                 dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
-        F3 v0 = velocity_at<T, P2>(d, P.F, p);
+        F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * f.x + (axis != 0), 2 * f.y + (axis != 1),
+                                         2 * f.z + (axis != 2));
         F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
@@ -228,7 +231,7 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
     if (P.apply_walls) {
         int c = axis == 0 ? f.x : (axis == 1 ? f.y : f.z);
         int n = axis == 0 ? f.sx : (axis == 1 ? f.sy : f.sz);
-        if (c == 0 || c == n - 1 || blocked) value = 0.f;
+        if (c == 0 || c == n - 1 || blocked) value = wall_value(P.walls, axis, f.i);
     }
     Store<T>::st(P.out[axis], f.i, value);
 }
@@ -287,7 +290,7 @@ __global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid
         return;
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-    F3 v0 = velocity_at<T, P2>(d, P.F, p);
+    F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
     F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, P.dt);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
@@ -330,7 +333,7 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
         } else {
             const float dt = P.dt;
             F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-            F3 v0 = velocity_at<T, P2>(d, P.F, p);
+            F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
             F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
             float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
                   qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
@@ -472,7 +475,12 @@ __global__ void mac_advect_density_kernel(OpenParams P, Faces<T> F, const T* in,
         }                                                      \
     } while (0)
 
-bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s->solid && s->halo); }
+bool solids_ok(const FfxSolids* s) {
+    if (!s) return true;
+    const bool walls = s->wall[0] || s->wall[1] || s->wall[2];
+    if (walls && !(s->wall[0] && s->wall[1] && s->wall[2] && s->solid)) return false;   // all three, with a mask
+    return (!s->solid && !s->halo) || (s->solid && s->halo);
+}
 bool has_mask(const FfxSolids* s) { return s && s->solid; }
 
 }  // namespace
@@ -531,6 +539,7 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const
         P.density = (const T*)density;
         P.temperature = (const T*)temperature;
         P.out[0] = (T*)ou; P.out[1] = (T*)ov; P.out[2] = (T*)ow;
+        P.walls = make_walls(s);
         const float extent[3] = {g->ex, g->ey, g->ez};
         P.src = make_src(src, extent);
         if (!src) P.src.count = 0;

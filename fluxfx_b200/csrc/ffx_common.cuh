@@ -160,6 +160,80 @@ __device__ __forceinline__ F3 velocity_at(const Dev& d, const Faces<T>& F, F3 p)
     return r;
 }
 
+// sample_face at a point whose grid coordinates are exact integers or
+// half-integers, given doubled: q = (qx2, qy2, qz2) / 2. Each fraction is then
+// 0 or 1/2, every weight a power of two, and a term of zero weight adds a
+// signed zero, which leaves the running sum unchanged (it starts at +0 and
+// cannot become -0). Summing only the terms of nonzero weight, in
+// sample_face's order and with its weight products, therefore gives
+// sample_face's value for finite fields, with 1, 2, 4 or 8 loads instead of 8.
+template <typename T>
+__device__ __forceinline__ float sample_face_half(const T* __restrict__ f, int sx, int sy, int sz, int qx2, int qy2,
+                                                  int qz2) {
+    qx2 = min(max(qx2, 0), 2 * (sx - 1));
+    qy2 = min(max(qy2, 0), 2 * (sy - 1));
+    qz2 = min(max(qz2, 0), 2 * (sz - 1));
+    const int ix = qx2 >> 1, iy = qy2 >> 1, iz = qz2 >> 1;
+    const bool hx = qx2 & 1, hy = qy2 & 1, hz = qz2 & 1;
+    const int ix1 = min(ix + 1, sx - 1), iy1 = min(iy + 1, sy - 1), iz1 = min(iz + 1, sz - 1);
+    // every term present has the same weight: 1/2 per axis with a half fraction
+    const float w = (hx ? 0.5f : 1.f) * (hy ? 0.5f : 1.f) * (hz ? 0.5f : 1.f);
+    const int sxy = sx * sy;
+    const int r00 = iz * sxy + iy * sx, r01 = iz * sxy + iy1 * sx, r10 = iz1 * sxy + iy * sx,
+              r11 = iz1 * sxy + iy1 * sx;
+    float v = 0.f;
+    v = v + w * Store<T>::ld(f, r00 + ix);
+    if (hx) v = v + w * Store<T>::ld(f, r00 + ix1);
+    if (hy) {
+        v = v + w * Store<T>::ld(f, r01 + ix);
+        if (hx) v = v + w * Store<T>::ld(f, r01 + ix1);
+    }
+    if (hz) {
+        v = v + w * Store<T>::ld(f, r10 + ix);
+        if (hx) v = v + w * Store<T>::ld(f, r10 + ix1);
+        if (hy) {
+            v = v + w * Store<T>::ld(f, r11 + ix);
+            if (hx) v = v + w * Store<T>::ld(f, r11 + ix1);
+        }
+    }
+    return v;
+}
+
+// Staggered velocity at a point with doubled cell coordinates (X2, Y2, Z2)
+// (a face centre or cell centre): velocity_at's value, exact when the grid's
+// positions round-trip exactly (power-of-two extent, cells and spacing).
+template <typename T>
+__device__ __forceinline__ F3 velocity_at_node(const Dev& d, const Faces<T>& F, int X2, int Y2, int Z2) {
+    F3 r;
+    r.x = sample_face_half(F.u, d.nx + 1, d.ny, d.nz, X2, Y2 - 1, Z2 - 1);
+    r.y = sample_face_half(F.v, d.nx, d.ny + 1, d.nz, X2 - 1, Y2, Z2 - 1);
+    r.z = sample_face_half(F.w, d.nx, d.ny, d.nz + 1, X2 - 1, Y2 - 1, Z2);
+    return r;
+}
+
+// Velocity at the node p = (X2, Y2, Z2) / 2 cells of the launch thread.
+template <typename T, bool P2>
+__device__ __forceinline__ F3 velocity_at_start(const Dev& d, const Faces<T>& F, F3 p, int X2, int Y2, int Z2) {
+    if constexpr (P2) return velocity_at_node(d, F, X2, Y2, Z2);
+    else return velocity_at<T, false>(d, F, p);
+}
+
+// Velocity of wall and solid faces: 0 for static walls, the moving colliders'
+// rigid-body velocity when the FfxSolids carry wall fields (the
+// FLUXFX_MOVING_COLLIDERS variant of pressure_walls.glsl / pressure_gradient.glsl).
+struct Walls {
+    const float* f[3];
+};
+inline Walls make_walls(const FfxSolids* s) {
+    Walls w;
+    for (int a = 0; a < 3; ++a) w.f[a] = s ? s->wall[a] : nullptr;
+    return w;
+}
+__device__ __forceinline__ float wall_value(const Walls& w, int axis, int i) {
+    const float* p = w.f[axis];
+    return p ? __ldg(p + i) : 0.f;
+}
+
 // ---------------------------------------------------------------- colliders
 __device__ __forceinline__ bool solid_cell(const Dev& d, const uint8_t* __restrict__ solid,
                                            int x, int y, int z) {

@@ -402,6 +402,13 @@ int level0_prolong_smooth(const FfxGraphLevel* lv, const float* p, const float* 
                                              "level0_prolong_smooth_kernel");
 }
 
+int level0_prolong_smooth_dot(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                              float omega, float* out, double* dot, double scale, cudaStream_t st) {
+    EpArgs P{rhs, omega, out, nullptr, dot, scale, nullptr};
+    return launch<It::Prolonged, Ep::SmoothDot>(make_l0(lv), ItArgs{p, coarse, nullptr, nullptr}, P, st,
+                                                "level0_prolong_smooth_dot_kernel");
+}
+
 int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st) {
     EpArgs P{rhs, 0.f, r, nullptr, nullptr, 0.0, nullptr};
     return launch<It::Plain, Ep::Residual>(make_l0(lv), ItArgs{p, nullptr, nullptr, nullptr}, P, st, "level0_residual_kernel");

@@ -31,8 +31,8 @@ inline unsigned reduce_z(int nz) { return (unsigned)(nz < 8 ? nz : 8); }
 // ------------------------------------------------------ walls + divergence
 // pressure_walls.glsl + pressure_divergence.glsl (DIV = false: walls only).
 template <typename T, bool MASK, bool DIV>
-__global__ void __launch_bounds__(256) walls_div_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
-                                                       T* ou, T* ov, T* ow, float* div) {
+__global__ void __launch_bounds__(256) walls_div_kernel(Dev d, const uint8_t* __restrict__ solid, Walls W,
+                                                       Faces<T> F, T* ou, T* ov, T* ow, float* div) {
     int x, y, z;
     if (!cell_coords(d.nx, d.ny, x, y, z)) return;
     const int i = cidx(d, x, y, z);
@@ -43,7 +43,7 @@ __global__ void __launch_bounds__(256) walls_div_kernel(Dev d, const uint8_t* __
     auto bounded = [&](const T* f, int idx, int c, int nf, int fx, int fy, int fz, int axis) -> float {
         bool wall = c == 0 || c == nf - 1;
         if (MASK) wall = wall || solid_face(d, solid, fx, fy, fz, axis);
-        return wall ? 0.f : Store<T>::ld(f, idx);
+        return wall ? wall_value(W, axis, idx) : Store<T>::ld(f, idx);
     };
     float ul = bounded(F.u, iu, x, d.nx + 1, x, y, z, 0);
     float vl = bounded(F.v, iv, y, d.ny + 1, x, y, z, 1);
@@ -83,9 +83,9 @@ __global__ void __launch_bounds__(256) divergence_kernel(Dev d, const uint8_t* _
 
 // ------------------------------------------------- gradient + divergence
 template <typename T, bool MASK>
-__global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
-                                                      const float* __restrict__ p, float dt, T* ou, T* ov, T* ow,
-                                                      float* div, float* maxima) {
+__global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Walls W,
+                                                      Faces<T> F, const float* __restrict__ p, float dt, T* ou,
+                                                      T* ov, T* ow, float* div, float* maxima) {
     int x, y, z;
     float mx[3] = {0.f, 0.f, 0.f};
     if (cell_coords(d.nx, d.ny, x, y, z)) {
@@ -100,7 +100,7 @@ __global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __r
                             float plo) -> float {
             bool open = c > 0 && c < nf - 1;
             if (MASK) open = open && !solid_face(d, solid, fx, fy, fz, axis);
-            if (!open) return 0.f;
+            if (!open) return wall_value(W, axis, idx);
             float gr = (phi - plo) * d.inv[axis];
             return Store<T>::ld(f, idx) - dt * gr;
         };
@@ -762,6 +762,28 @@ __global__ void __launch_bounds__(256) graph_smooth_dot_kernel(GLvl g, const flo
     block_sum_to(dot, acc);
 }
 
+// Prolongation + first post-sweep fused with dot += scale * rhs . out (the
+// last sweep of a preconditioning V-cycle with one post-sweep).
+__global__ void __launch_bounds__(256) graph_prolong_smooth_dot_kernel(GLvl g, const float* __restrict__ p,
+                                                                      const float* __restrict__ coarse,
+                                                                      const float* __restrict__ rhs, float omega,
+                                                                      float* out, double* dot, double scale) {
+    int x, y, z;
+    double acc = 0.0;
+    if (cell_coords(g.nx, g.ny, x, y, z)) {
+        const int i = x + g.nx * (y + g.ny * z);
+        float diag, nb;
+        graph_terms(g, i, x, y, z,
+                    [&](int j, int jx, int jy, int jz) { return prolonged(g, p, coarse, j, jx, jy, jz); }, diag, nb);
+        const float pc = prolonged(g, p, coarse, i, x, y, z);
+        const float r = __ldg(rhs + i);
+        const float v = diag > 0.f ? pc * (1.f - omega) + ((nb - r) / diag) * omega : 0.f;
+        out[i] = v;
+        acc = scale * (double)r * (double)v;
+    }
+    block_sum_to(dot, acc);
+}
+
 // First sweep from a zero iterate: p_out = omega * (0 - rhs) / diag on active cells.
 __global__ void __launch_bounds__(256) graph_smooth_zero_kernel(GLvl g, const float* __restrict__ rhs, float omega,
                                                                float* out) {
@@ -813,7 +835,12 @@ __global__ void __launch_bounds__(256) pcg_update_kernel(int64_t n, const double
     block_max_to(resmax, m);
 }
 
-bool solids_ok(const FfxSolids* s) { return !s || (!s->solid && !s->halo) || (s->solid && s->halo); }
+bool solids_ok(const FfxSolids* s) {
+    if (!s) return true;
+    const bool walls = s->wall[0] || s->wall[1] || s->wall[2];
+    if (walls && !(s->wall[0] && s->wall[1] && s->wall[2] && s->solid)) return false;   // all three, with a mask
+    return (!s->solid && !s->halo) || (s->solid && s->halo);
+}
 bool has_mask(const FfxSolids* s) { return s && s->solid; }
 
 bool glvl_ok(const FfxGraphLevel* lv) {
@@ -842,9 +869,9 @@ int ffx_walls(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, 
     dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) walls_div_kernel<T, true, false><<<grid, block, 0, st>>>(d, s->solid, F, (T*)ou, (T*)ov,
+        if (has_mask(s)) walls_div_kernel<T, true, false><<<grid, block, 0, st>>>(d, s->solid, make_walls(s), F, (T*)ou, (T*)ov,
                                                                                   (T*)ow, nullptr);
-        else walls_div_kernel<T, false, false><<<grid, block, 0, st>>>(d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
+        else walls_div_kernel<T, false, false><<<grid, block, 0, st>>>(d, nullptr, Walls{}, F, (T*)ou, (T*)ov, (T*)ow, nullptr);
     });
     return launch_status("walls_kernel");
 }
@@ -874,9 +901,9 @@ int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage, cons
     dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) walls_div_kernel<T, true, true><<<grid, block, 0, st>>>(d, s->solid, F, (T*)ou, (T*)ov,
+        if (has_mask(s)) walls_div_kernel<T, true, true><<<grid, block, 0, st>>>(d, s->solid, make_walls(s), F, (T*)ou, (T*)ov,
                                                                                  (T*)ow, div);
-        else walls_div_kernel<T, false, true><<<grid, block, 0, st>>>(d, nullptr, F, (T*)ou, (T*)ov, (T*)ow, div);
+        else walls_div_kernel<T, false, true><<<grid, block, 0, st>>>(d, nullptr, Walls{}, F, (T*)ou, (T*)ov, (T*)ow, div);
     });
     return launch_status("walls_divergence_kernel");
 }
@@ -896,9 +923,9 @@ int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* 
     dim3 grid = cell_grid(g->nx, g->ny, g->nz), block = cell_block();
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
-        if (has_mask(s)) gradient_kernel<T, true><<<grid, block, 0, st>>>(d, s->solid, F, pressure, dt, (T*)ou,
+        if (has_mask(s)) gradient_kernel<T, true><<<grid, block, 0, st>>>(d, s->solid, make_walls(s), F, pressure, dt, (T*)ou,
                                                                           (T*)ov, (T*)ow, div_after, maxima);
-        else gradient_kernel<T, false><<<grid, block, 0, st>>>(d, nullptr, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow,
+        else gradient_kernel<T, false><<<grid, block, 0, st>>>(d, nullptr, Walls{}, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow,
                                                                div_after, maxima);
     });
     return launch_status("gradient_kernel");
@@ -1149,6 +1176,21 @@ int ffx_graph_smooth_dot(const FfxGraphLevel* lv, const float* p_in, const float
     graph_smooth_dot_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, st>>>(g, p_in, rhs, omega, p_out, dot,
                                                                                  scale);
     return launch_status("graph_smooth_dot_kernel");
+}
+
+int ffx_graph_prolong_smooth_dot(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                                 float omega, float* p_out, double* dot, double scale, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && coarse && rhs && p_out && dot && p != p_out && lv->nx % 2 == 0 &&
+                lv->ny % 2 == 0 && lv->nz % 2 == 0, "ffx_graph_prolong_smooth_dot: invalid arguments");
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(dot, 0, sizeof(double), st), "ffx_graph_prolong_smooth_dot memset");
+    if (e) return e;
+    if (level0_x4(lv, {p, rhs, p_out}) && ((uintptr_t)coarse & 7) == 0)
+        return level0_prolong_smooth_dot(lv, p, coarse, rhs, omega, p_out, dot, scale, st);
+    GLvl g = make_glvl(lv);
+    graph_prolong_smooth_dot_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, st>>>(g, p, coarse, rhs, omega,
+                                                                                         p_out, dot, scale);
+    return launch_status("graph_prolong_smooth_dot_kernel");
 }
 
 int ffx_pcg_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old, const double* rz_new,

@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define FFX_ABI_VERSION 2
+#define FFX_ABI_VERSION 3
 
 typedef enum FfxStatus {
     FFX_OK = 0,
@@ -54,9 +54,14 @@ typedef struct FfxGrid {
 } FfxGrid;
 
 typedef struct FfxSolids {
-    const uint8_t* solid; /* nx*ny*nz, 1 = solid cell; NULL = no colliders */
+    const uint8_t* solid; /* nx*ny*nz, nonzero = solid cell; NULL = no colliders */
     const uint8_t* halo;  /* nx*ny*nz dilated mask (ffx_dilate_mask) */
+    const float* wall[3]; /* moving colliders: velocity of every wall and solid face
+                             (face grids, ffx_moving_walls); NULL = 0 (static walls) */
 } FfxSolids;
+
+/* Moving colliders per solver (the reference's wall table holds 8). */
+#define FFX_MOVING_MAX 8
 
 /* Emitters. count < 0: one swept sphere described by the `single_*` fields
  * (backend/projected.py:155-159, emission_weight.glsl). count in [0, 8]: rows
@@ -307,6 +312,12 @@ int ffx_graph_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega
 /* Smoothing sweep fused with *dot = scale * sum(rhs * p_out) (FP64; zeroed by the call). */
 int ffx_graph_smooth_dot(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega,
                          float* p_out, double* dot, double scale, void* stream);
+/* ffx_graph_prolong_smooth fused with *dot = scale * (rhs . p_out) (FP64,
+ * zeroed by the call): the last sweep of a preconditioning V-cycle that has
+ * one post-sweep. No counterpart shader (MG-PCG extension). */
+int ffx_graph_prolong_smooth_dot(const FfxGraphLevel* lv, const float* p, const float* coarse,
+                                 const float* rhs, float omega, float* p_out, double* dot,
+                                 double scale, void* stream);
 /* p_out = z + (*rz_new / *rz_old) p_old (p_out = z when rz_old is NULL), q = A p_out,
  * *pq = sum(p_out * q) in FP64 (zeroed by the call). p_out must not alias p_old or z. */
 int ffx_pcg_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old,
@@ -343,6 +354,47 @@ int ffx_divergence_stats(int64_t count, const float* before, const float* after,
  * stream do not, since each call rewrites every partial it reads. */
 int ffx_divergence_stats_static(int64_t count, const float* before, const float* after,
                                 double* out, void* stream);
+
+/* ------------------------------------------------------ fire configuration */
+/* Cell vorticity (omega.xyz, |omega|) as float4 per cell, central differences of
+ * the cell-centred velocity with clamped reads; replaces shaders/curl.glsl
+ * (backend/detail.py:39-49). */
+int ffx_curl(const FfxGrid* g, int storage, const void* u, const void* v, const void* w,
+             float* curl4, void* stream);
+/* Vorticity confinement on every face: out = in + dt * (force(c) + force(c - e_a)) / 2 . e_a,
+ * force = strength * h * normalize(grad|omega|) x omega capped at `limit`; replaces
+ * shaders/confinement.glsl. Outputs must not alias inputs. */
+int ffx_confine(const FfxGrid* g, int storage, const float* curl4, const void* u, const void* v,
+                const void* w, float dt, float strength, float limit, void* ou, void* ov,
+                void* ow, void* stream);
+/* Combustion in one pass (backend/combustion.py:21-31, combustion_burn.glsl,
+ * combustion_apply.glsl): flame = (T >= ignition ? max(fuel,0)(1 - exp(-rate dt)) : 0)/dt;
+ * fuel -= dt flame (clamped at 0), density += dt smoke_yield flame, temperature +=
+ * dt heat_yield flame. Outputs may alias their inputs (elementwise). */
+int ffx_combustion(const FfxGrid* g, int storage, const void* fuel, const void* temperature,
+                   const void* density, float dt, float ignition, float burn_rate,
+                   float smoke_yield, float heat_yield, float* flame, void* fuel_out,
+                   void* density_out, void* temperature_out, void* stream);
+/* Owner mask of moving colliders: 1-based index of the first collider holding
+ * each cell centre (FP32 test of 12 inverse-affine coefficients per collider,
+ * sphere or box), 0 = fluid; replaces shaders/moving_mask.glsl
+ * (backend/moving_collision.py:44-58). count <= FFX_MOVING_MAX. rows12 and
+ * is_box are HOST arrays (passed to the kernel by value). */
+int ffx_moving_mask(const FfxGrid* g, int count, const float* rows12, const int32_t* is_box,
+                    uint8_t* owners, void* stream);
+/* Rigid wall velocity (row . (p, 1), 3 rows of 4 per collider in the HOST array
+ * `table`) on every interior face next to a solid cell, 0 elsewhere; replaces
+ * shaders/moving_wall.glsl. */
+int ffx_moving_walls(const FfxGrid* g, const uint8_t* owners, int count, const float* table,
+                     float* wu, float* wv, float* ww, void* stream);
+/* In-place remap after a move (backend/moving_collision.py:64-80,
+ * moving_remap_scalar.glsl, moving_remap_face.glsl): scalars (scalar1, scalar2
+ * may be NULL) zeroed in cells solid now or before; faces take the wall velocity
+ * where blocked, 0 where just uncovered, 0 on domain walls. */
+int ffx_moving_remap(const FfxGrid* g, int storage, const uint8_t* owners,
+                     const uint8_t* old_owners, void* scalar0, void* scalar1, void* scalar2,
+                     void* u, void* v, void* w, const float* wu, const float* wv,
+                     const float* ww, void* stream);
 
 #ifdef __cplusplus
 }

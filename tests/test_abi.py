@@ -26,13 +26,13 @@ def test_library_loads_and_exports_every_symbol():
     for name in header_functions():
         assert hasattr(lib, name), name
         assert ctypes.cast(getattr(lib, name), ctypes.c_void_p).value
-    assert lib.ffx_abi_version() == 2
+    assert lib.ffx_abi_version() == 3
 
 
 def test_struct_layouts_match_the_header():
     # sizes of the C structs (natural alignment, 64-bit pointers)
     assert ctypes.sizeof(N.FfxGrid) == 36
-    assert ctypes.sizeof(N.FfxSolids) == 16
+    assert ctypes.sizeof(N.FfxSolids) == 16 + 24   # solid, halo, wall[3]
     assert ctypes.sizeof(N.FfxSources) == 4 * (2 + 3 + 3 + 1 + 3 + 1 + 128)
     assert ctypes.sizeof(N.FfxScalarChannel) == 4 * 8 + 4 * 5 + 4
     assert ctypes.sizeof(N.FfxGraphLevel) == 12 + 4 + 8 + 8 + 12 + 4 + 8   # ..., w[3], pad, links

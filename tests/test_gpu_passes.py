@@ -515,6 +515,18 @@ def test_level0_four_cell_kernels_equal_scalar_kernels(D, shape):
     a, b = both(prolong_smooth)
     assert np.array_equal(_bits(a), _bits(b))
 
+    def prolong_smooth_dot(lv):
+        o = t(np.full(cell, np.nan))
+        d = torch.zeros(1, dtype=torch.float64, device='cuda')
+        D.call('ffx_graph_prolong_smooth_dot', C.byref(lv), ptr(p), ptr(coarse), ptr(rhs), 2 / 3, ptr(o), ptr(d),
+               -1.0, D.s)
+        return o, d
+    (a, da), (b, db) = both(prolong_smooth_dot)
+    assert np.array_equal(_bits(a), _bits(b))
+    assert np.array_equal(_bits(a), _bits(both(prolong_smooth)[0]))
+    expect = -(n(rhs).astype(np.float64) * n(a)).sum()
+    assert float(da[0]) == pytest.approx(expect, rel=1e-9) and float(db[0]) == pytest.approx(expect, rel=1e-9)
+
     def residual(lv):
         o = t(np.full(cell, np.nan))
         D.call('ffx_graph_residual', C.byref(lv), ptr(p), ptr(rhs), ptr(o), D.s)

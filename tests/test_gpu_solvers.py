@@ -344,6 +344,33 @@ def test_pcg_reaches_the_vcycle_solution_in_fewer_cycles(D, warm):
             assert float(np.abs(n(outs_v[a]) - n(outs_p[a])).max()) <= 1e-4 * scale
 
 
+@pytest.mark.parametrize('sweeps', [(1, 1), (2, 2)])
+def test_pcg_with_short_preconditioner_reaches_tolerance(D, sweeps):
+    """PCG preconditioned by V(1,1) / V(2,2) aggregation cycles (the last
+    sweep fused with the FP64 dot) converges to the tolerance and to the same
+    projected velocity as the reference's V(4,4) cycles."""
+    from fluxfx_b200.backend.collision import SolidDevice
+    from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
+    grid = GridSpec((32, 32, 32))
+    sd = SolidDevice(grid, sphere_box_mask(grid.shape, grid.extent), D)
+    base = PressureSettings(pressure_tolerance=1e-6, pressure_max_cycles=200)
+    vproj = SolidMultigridProjector(grid, base, sd)
+    pproj = SolidMultigridProjector(grid, replace(base, pressure_method='PCG', solid_warm_start=True,
+                                                  mg_pre_sweeps=sweeps[0], mg_post_sweeps=sweeps[1]), sd)
+    rng = np.random.default_rng(5)
+    outs_v = [D.texture(fs) for fs in grid.face_shapes]
+    outs_p = [D.texture(fs) for fs in grid.face_shapes]
+    for dt in (0.02, 0.015):
+        fields = [D.texture(fs, rng.uniform(-1, 1, fs[0] * fs[1] * fs[2]), nonnegative=False)
+                  for fs in grid.face_shapes]
+        vproj.project(fields, outs_v, dt)
+        pproj.project(fields, outs_p, dt)
+        assert pproj.metrics()['rel_div_inf'] <= 1.5e-6 and pproj.last_cycles < 200
+        for a in range(3):
+            scale = float(np.abs(n(outs_v[a])).max())
+            assert float(np.abs(n(outs_v[a]) - n(outs_p[a])).max()) <= 1e-4 * scale
+
+
 @pytest.mark.parametrize('method', ['VCYCLE', 'PCG'])
 def test_graph_replay_matches_eager_launches(D, method):
     """The pressure solve replayed from captured CUDA graphs runs the same

@@ -155,3 +155,34 @@ def test_combustion_kinetics():
     assert react(1.0, 100, 0.1, 150, 4.0) == 0
     with pytest.raises(ValueError):
         react(-1.0, 200, 0.1, 150, 4.0)
+
+
+def test_rigid_collider_motion_rows():
+    """Wall velocity rows of a moved collider (physics/collider_motion.py:107-118):
+    translation gives the linear velocity everywhere, a rotation about the
+    centre gives omega x (p - c); shape or size changes are rejected."""
+    from fluxfx_b200.physics.collider_motion import velocity_rows, validate_motion
+    from fluxfx_b200.physics.collision import Collider
+    a = primitive('BOX', (0.4, 0.5, 0.5), (0.1, 0.2, 0.1))
+    b = primitive('BOX', (0.42, 0.49, 0.5), (0.1, 0.2, 0.1))
+    rows = velocity_rows(a, b, 0.02)
+    for p in ((0.1, 0.2, 0.3), (0.9, 0.4, 0.2)):
+        v = [r[0] * p[0] + r[1] * p[1] + r[2] * p[2] + r[3] for r in rows]
+        assert v == pytest.approx([1.0, -0.5, 0.0], abs=1e-12)
+    theta, c = 0.1, (0.5, 0.5, 0.5)
+    ct, st = math.cos(theta), math.sin(theta)
+    rot = ((ct, -st, 0.0), (st, ct, 0.0), (0.0, 0.0, 1.0))       # columns = rotated axes
+    size = (0.1, 0.2, 0.1)
+    rrows = []
+    for i in range(3):
+        r = [rot[k][i] / size[i] for k in range(3)]
+        rrows.append(tuple(r + [-sum(r[k] * c[k] for k in range(3))]))
+    rows = velocity_rows(primitive('BOX', c, size), Collider('BOX', tuple(rrows)), 0.02)
+    w = theta / 0.02
+    p = (0.7, 0.45, 0.3)
+    v = [r[0] * p[0] + r[1] * p[1] + r[2] * p[2] + r[3] for r in rows]
+    assert v == pytest.approx([-w * (p[1] - c[1]), w * (p[0] - c[0]), 0.0], abs=1e-9)
+    with pytest.raises(ValueError):
+        validate_motion((a,), (primitive('BOX', (0.4, 0.5, 0.5), (0.1, 0.3, 0.1)),))
+    with pytest.raises(ValueError):
+        validate_motion((a,), (a, b))
