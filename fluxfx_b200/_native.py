@@ -73,6 +73,18 @@ class FfxGraphTail(C.Structure):
                 ('levels', FfxTailLevel * TAIL_LEVELS)]
 
 
+class FfxTensorView(C.Structure):
+    _fields_ = [('data', vp), ('pitch', i32), ('offset', i32)]
+
+
+class FfxConv(C.Structure):
+    _fields_ = [('batch', i32), ('in_dims', i32 * 3), ('out_dims', i32 * 3), ('c1', i32), ('c2', i32),
+                ('cout', i32), ('ksize', i32), ('stride', i32), ('pad', i32), ('transposed', i32),
+                ('in1', FfxTensorView), ('in2', FfxTensorView), ('weight', vp), ('bias', vp), ('relu', i32),
+                ('accumulate', i32), ('out', vp), ('out_pitch', i32), ('out_offset', i32), ('out_f32', vp),
+                ('out_f32_pitch', i32)]
+
+
 P = C.POINTER
 _PROTOTYPES = {
     'ffx_abi_version': (C.c_int, []),
@@ -116,6 +128,14 @@ _PROTOTYPES = {
     'ffx_graph_level0_edges': (C.c_int, [P(FfxGraphLevel), vp, vp]),
     'ffx_graph_links': (C.c_int, [P(FfxGraphLevel), vp, vp]),
     'ffx_graph_tail': (C.c_int, [P(FfxGraphTail), vp]),
+    'ffx_conv_forward': (C.c_int, [P(FfxConv), vp]),
+    'ffx_conv_weight_grad': (C.c_int, [P(FfxConv), vp, i32, vp, vp]),
+    'ffx_relu_backward': (C.c_int, [i64, i32, vp, i32, vp, i32, i32, vp]),
+    'ffx_bias_grad': (C.c_int, [i64, i32, vp, i32, vp, vp]),
+    'ffx_weight_transpose': (C.c_int, [i32, i32, i32, i32, vp, vp, vp]),
+    'ffx_adam': (C.c_int, [i64, vp, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp]),
+    'ffx_pack_input': (C.c_int, [i64, vp, vp, f32, vp, vp]),
+    'ffx_mse_grad': (C.c_int, [i64, vp, i32, vp, vp, f32, vp, vp, vp]),
     'ffx_curl': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, vp]),
     'ffx_confine': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp]),
     'ffx_combustion': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, f32, f32, f32, f32, vp, vp, vp, vp, vp]),

@@ -1,0 +1,562 @@
+// Learned pressure warm start: BF16 implicit-GEMM 3D convolutions (forward,
+// data gradient, weight gradient), ReLU backward, Adam, and the loss.
+//
+// Activations are NDHWC bfloat16 (a voxel's channels are contiguous); a tensor
+// is addressed through a view (pointer, elements per voxel, first channel), so
+// the decoder's concatenation of the upsampled path and the skip connection is
+// one buffer that both producers write into and every consumer reads a channel
+// range of, without copies.
+//
+// Forward convolution as a GEMM: rows = output voxels, columns = output
+// channels, reduction k = (tap, input channel), A gathered from the input with
+// zero padding (implicit im2col), B = weights [k][cout]. Tiles of 128 x 64 x 16
+// per block of four warps, a three-stage cp.async pipeline (zero-fill for
+// padding and ragged edges), and BF16 tensor-core MMAs (m16n8k16, FP32
+// accumulation, fragments via ldmatrix). The transposed 2^3 stride-2
+// convolution (decoder up-sampling, and the data gradient of the stride-2
+// down-sampling) maps each output voxel 2q + j to tap j of input voxel q: one
+// GEMM per parity class j (blockIdx.z). Weight gradients reduce over voxels:
+// dW[k][n] = sum_m A[m][k] G[m][n], split over voxel chunks with FP32 atomics.
+#include <cuda_bf16.h>
+
+#include <algorithm>
+
+#include "ffx_host.cuh"
+
+namespace ffx {
+namespace {
+
+using bf16 = __nv_bfloat16;
+
+constexpr int kBM = 128, kBN = 64, kStages = 3, kGemmThreads = 128;
+constexpr int kAStride = 24;    // bf16 per A row in shared memory (16 + 8 pad: 48 B, conflict-free ldmatrix)
+constexpr int kBStride = 72;    // bf16 per B row (64 + 8 pad: 144 B)
+constexpr int kWStride = 136;   // bf16 per A row of the weight-gradient tile (128 + 8 pad: 272 B)
+
+struct View {
+    const bf16* p;
+    int pitch, offset;
+};
+
+struct Conv {
+    int batch, id, ih, iw, od, oh, ow;
+    int c1, c2, cin, cout, ks, stride, pad, transposed;
+    int taps, units_per_tap, k_units;   // reduction in units of 8 channels
+    long long rows;                      // GEMM rows: output voxels, or input voxels per parity class
+    View in1, in2;
+    const bf16* w;
+    const float* bias;
+    int relu, accumulate;
+    bf16* out;
+    int out_pitch, out_offset;
+    float* out_f32;
+    int out_f32_pitch;
+};
+
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem, bool valid) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    const int size = valid ? 16 : 0;
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16, %2;\n" ::"r"(s), "l"(gmem), "r"(size));
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N)); }
+
+__device__ __forceinline__ void ldmatrix_x4(unsigned r[4], const void* smem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(s));
+}
+__device__ __forceinline__ void ldmatrix_x4_trans(unsigned r[4], const void* smem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];\n"
+                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
+                 : "r"(s));
+}
+__device__ __forceinline__ void mma_bf16(float c[4], const unsigned a[4], unsigned b0, unsigned b1) {
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};\n"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b0), "r"(b1));
+}
+
+// Position of GEMM row m: the output voxel (convolution) or the input voxel q
+// of a parity class (transposed).
+struct RowPos {
+    int b, z, y, x;
+};
+__device__ __forceinline__ RowPos decode(long long m, int d, int h, int w) {
+    RowPos r;
+    r.x = (int)(m % w);
+    long long t = m / w;
+    r.y = (int)(t % h);
+    t /= h;
+    r.z = (int)(t % d);
+    r.b = (int)(t / d);
+    return r;
+}
+
+// Address of unit u (8 channels) of GEMM row `pos` in the gathered input, or
+// nullptr where the tap falls outside the input (zero padding).
+__device__ __forceinline__ const bf16* gather(const Conv& a, const RowPos& pos, int u) {
+    const int tap = u / a.units_per_tap;
+    const int c = (u - tap * a.units_per_tap) * 8;
+    long long vox;
+    if (a.transposed) {
+        vox = (((long long)pos.b * a.id + pos.z) * a.ih + pos.y) * a.iw + pos.x;
+    } else {
+        const int ks = a.ks;
+        const int dz = tap / (ks * ks), dy = (tap / ks) % ks, dx = tap % ks;
+        const int zz = pos.z * a.stride - a.pad + dz, yy = pos.y * a.stride - a.pad + dy,
+                  xx = pos.x * a.stride - a.pad + dx;
+        if ((unsigned)zz >= (unsigned)a.id || (unsigned)yy >= (unsigned)a.ih || (unsigned)xx >= (unsigned)a.iw)
+            return nullptr;
+        vox = (((long long)pos.b * a.id + zz) * a.ih + yy) * a.iw + xx;
+    }
+    if (c < a.c1) return a.in1.p + vox * a.in1.pitch + a.in1.offset + c;
+    return a.in2.p + vox * a.in2.pitch + a.in2.offset + (c - a.c1);
+}
+
+// Output voxel index of GEMM row m (class j for the transposed form).
+__device__ __forceinline__ long long out_voxel(const Conv& a, long long m, int cls) {
+    if (!a.transposed) return m;
+    const RowPos q = decode(m, a.id, a.ih, a.iw);
+    const int z = 2 * q.z + (cls >> 2), y = 2 * q.y + ((cls >> 1) & 1), x = 2 * q.x + (cls & 1);
+    return (((long long)q.b * a.od + z) * a.oh + y) * a.ow + x;
+}
+
+// ------------------------------------------------------------ forward GEMM
+__global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_constant__ Conv a) {
+    __shared__ __align__(128) bf16 sA[kStages][kBM * kAStride];
+    __shared__ __align__(128) bf16 sB[kStages][16 * kBStride];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long m0 = (long long)blockIdx.x * kBM;
+    const int n0 = blockIdx.y * kBN;
+    const int cls = blockIdx.z;
+    const bf16* W = a.w + (a.transposed ? (size_t)cls * a.cin * a.cout : 0);
+    const long long my_row = m0 + tid;
+    const bool row_ok = my_row < a.rows;
+    const RowPos pos = row_ok ? (a.transposed ? decode(my_row, a.id, a.ih, a.iw) : decode(my_row, a.od, a.oh, a.ow))
+                              : RowPos{0, 0, 0, 0};
+    const int k_elems = a.k_units * 8;
+    const int nk = (a.k_units + 1) / 2;
+
+    auto load = [&](int stage, int kstep) {
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int u = kstep * 2 + h;
+            const bf16* src = (row_ok && u < a.k_units) ? gather(a, pos, u) : nullptr;
+            cp_async16(&sA[stage][tid * kAStride + h * 8], src ? src : a.in1.p, src != nullptr);
+        }
+        const int kr = tid >> 3, nu = (tid & 7) * 8;
+        const int k = kstep * 16 + kr, n = n0 + nu;
+        const bool ok = k < k_elems && n < a.cout;
+        cp_async16(&sB[stage][kr * kBStride + nu], ok ? W + (size_t)k * a.cout + n : W, ok);
+    };
+
+    float acc[2][8][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nk) load(s, s);
+        cp_async_commit();
+    }
+    for (int ks = 0; ks < nk; ++ks) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        const int pf = ks + kStages - 1;
+        if (pf < nk) load(pf % kStages, pf);
+        cp_async_commit();
+        const int st = ks % kStages;
+        unsigned af[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt)
+            ldmatrix_x4(af[mt], &sA[st][(warp * 32 + mt * 16 + (lane & 15)) * kAStride + (lane >> 4) * 8]);
+#pragma unroll
+        for (int np = 0; np < 4; ++np) {
+            unsigned bf[4];
+            ldmatrix_x4_trans(bf, &sB[st][((lane & 7) + ((lane >> 3) & 1) * 8) * kBStride + np * 16 + (lane >> 4) * 8]);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                mma_bf16(acc[mt][2 * np], af[mt], bf[0], bf[1]);
+                mma_bf16(acc[mt][2 * np + 1], af[mt], bf[2], bf[3]);
+            }
+        }
+    }
+    cp_async_wait<0>();
+
+    // epilogue: bias, ReLU, optional accumulation, BF16 and/or FP32 stores
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const long long m = m0 + warp * 32 + mt * 16 + (lane >> 2) + half * 8;
+            if (m >= a.rows) continue;
+            const long long vox = out_voxel(a, m, cls);
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int n = n0 + nt * 8 + (lane & 3) * 2;
+                if (n >= a.cout) continue;
+                float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
+                if (a.bias) {
+                    v0 += a.bias[n];
+                    v1 += a.bias[n + 1];
+                }
+                if (a.relu) {
+                    v0 = fmaxf(v0, 0.f);
+                    v1 = fmaxf(v1, 0.f);
+                }
+                if (a.out) {
+                    __nv_bfloat162* o =
+                        reinterpret_cast<__nv_bfloat162*>(a.out + vox * a.out_pitch + a.out_offset + n);
+                    if (a.accumulate) {
+                        const float2 prev = __bfloat1622float2(*o);
+                        v0 += prev.x;
+                        v1 += prev.y;
+                    }
+                    *o = __floats2bfloat162_rn(v0, v1);
+                }
+                if (a.out_f32) {
+                    float* o = a.out_f32 + vox * a.out_f32_pitch + n;
+                    o[0] = v0;
+                    o[1] = v1;
+                }
+            }
+        }
+}
+
+// ------------------------------------------------------ weight gradient GEMM
+// dW[k][n] += sum over the block's voxel chunk of A[m][k] G[m][n]; A^T
+// fragments come from the [m][k] tile through ldmatrix.trans.
+__global__ void __launch_bounds__(kGemmThreads) conv_wgrad_kernel(const __grid_constant__ Conv a, const bf16* g,
+                                                                 int g_pitch, float* dw, long long chunk) {
+    __shared__ __align__(128) bf16 sA[kStages][16 * kWStride];
+    __shared__ __align__(128) bf16 sG[kStages][16 * kBStride];
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const int k0 = blockIdx.x * 128, n0 = blockIdx.y * kBN;
+    const int cls = a.transposed ? (int)(blockIdx.z % 8) : 0;
+    const long long split = a.transposed ? blockIdx.z / 8 : blockIdx.z;
+    const long long mb = split * chunk;
+    const long long me = min(a.rows, mb + chunk);
+    const int nsteps = (int)((me - mb + 15) / 16);
+    const int u0 = k0 / 8;
+
+    auto load = [&](int stage, int step) {
+        const int ml = tid >> 3;
+        const long long m = mb + (long long)step * 16 + ml;
+        const bool row_ok = m < me;
+        RowPos pos = {0, 0, 0, 0};
+        if (row_ok) pos = a.transposed ? decode(m, a.id, a.ih, a.iw) : decode(m, a.od, a.oh, a.ow);
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            const int ul = (tid & 7) * 2 + h;
+            const int u = u0 + ul;
+            const bf16* src = (row_ok && u < a.k_units) ? gather(a, pos, u) : nullptr;
+            cp_async16(&sA[stage][ml * kWStride + ul * 8], src ? src : a.in1.p, src != nullptr);
+        }
+        const int nu = (tid & 7) * 8, n = n0 + nu;
+        const bool ok = row_ok && n < a.cout;
+        const bf16* src = ok ? g + out_voxel(a, m, cls) * g_pitch + n : g;
+        cp_async16(&sG[stage][ml * kBStride + nu], src, ok);
+    };
+
+    float acc[2][8][4];
+#pragma unroll
+    for (int i = 0; i < 2; ++i)
+#pragma unroll
+        for (int j = 0; j < 8; ++j)
+#pragma unroll
+            for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
+
+#pragma unroll
+    for (int s = 0; s < kStages - 1; ++s) {
+        if (s < nsteps) load(s, s);
+        cp_async_commit();
+    }
+    for (int step = 0; step < nsteps; ++step) {
+        cp_async_wait<kStages - 2>();
+        __syncthreads();
+        const int pf = step + kStages - 1;
+        if (pf < nsteps) load(pf % kStages, pf);
+        cp_async_commit();
+        const int st = step % kStages;
+        unsigned af[2][4];
+#pragma unroll
+        for (int mt = 0; mt < 2; ++mt) {
+            const int kt = warp * 2 + mt;
+            ldmatrix_x4_trans(af[mt], &sA[st][((lane & 7) + ((lane >> 4) << 3)) * kWStride + kt * 16 +
+                                              ((lane >> 3) & 1) * 8]);
+        }
+#pragma unroll
+        for (int np = 0; np < 4; ++np) {
+            unsigned bf[4];
+            ldmatrix_x4_trans(bf, &sG[st][((lane & 7) + ((lane >> 3) & 1) * 8) * kBStride + np * 16 + (lane >> 4) * 8]);
+#pragma unroll
+            for (int mt = 0; mt < 2; ++mt) {
+                mma_bf16(acc[mt][2 * np], af[mt], bf[0], bf[1]);
+                mma_bf16(acc[mt][2 * np + 1], af[mt], bf[2], bf[3]);
+            }
+        }
+    }
+    cp_async_wait<0>();
+    const int k_elems = a.k_units * 8;
+    float* base = dw + (a.transposed ? (size_t)cls * a.cin * a.cout : 0);
+#pragma unroll
+    for (int mt = 0; mt < 2; ++mt)
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int k = k0 + warp * 32 + mt * 16 + (lane >> 2) + half * 8;
+            if (k >= k_elems) continue;
+#pragma unroll
+            for (int nt = 0; nt < 8; ++nt) {
+                const int n = n0 + nt * 8 + (lane & 3) * 2;
+                if (n >= a.cout) continue;
+                atomicAdd(base + (size_t)k * a.cout + n, acc[mt][nt][half * 2]);
+                atomicAdd(base + (size_t)k * a.cout + n + 1, acc[mt][nt][half * 2 + 1]);
+            }
+        }
+}
+
+// ------------------------------------------------------------ elementwise
+// dy *= (y > 0): the ReLU derivative, in place.
+__global__ void relu_backward_kernel(long long voxels, int channels, bf16* dy, int dy_pitch, const bf16* y,
+                                     int y_pitch, int y_offset) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= voxels * channels) return;
+    const long long v = i / channels;
+    const int c = (int)(i - v * channels);
+    if (!(__bfloat162float(y[v * y_pitch + y_offset + c]) > 0.f)) dy[v * dy_pitch + c] = __float2bfloat16_rn(0.f);
+}
+
+// db[c] += sum over voxels of g[v][c] (block-local FP32 sums, one atomic per channel and block).
+__global__ void bias_grad_kernel(long long voxels, int channels, const bf16* g, int pitch, float* db) {
+    __shared__ float part[128];
+    for (int c = threadIdx.x; c < channels; c += blockDim.x) part[c] = 0.f;
+    __syncthreads();
+    const long long per = (voxels + gridDim.x - 1) / gridDim.x;
+    const long long vb = blockIdx.x * per, ve = min(voxels, vb + per);
+    for (int c = threadIdx.x % channels; c < channels; c += channels) {
+        float s = 0.f;
+        for (long long v = vb + threadIdx.x / channels; v < ve; v += blockDim.x / channels)
+            s += __bfloat162float(g[v * pitch + c]);
+        atomicAdd(&part[c], s);
+    }
+    __syncthreads();
+    for (int c = threadIdx.x; c < channels; c += blockDim.x) atomicAdd(db + c, part[c]);
+}
+
+// Adam on FP32 master weights, refreshing their BF16 copy.
+__global__ void adam_kernel(long long n, float* w, float* m, float* v, const float* g, bf16* w16, float lr, float b1,
+                            float b2, float eps, float c1, float c2) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float gi = g[i];
+    const float mi = b1 * m[i] + (1.f - b1) * gi;
+    const float vi = b2 * v[i] + (1.f - b2) * gi * gi;
+    m[i] = mi;
+    v[i] = vi;
+    const float wi = w[i] - lr * (mi / c1) / (sqrtf(vi / c2) + eps);
+    w[i] = wi;
+    if (w16) w16[i] = __float2bfloat16_rn(wi);
+}
+
+// Network input: channel 0 = scale * divergence, channel 1 = solid mask,
+// channels 2..7 = 0 (the first convolution reads 8 channels).
+__global__ void pack_input_kernel(long long voxels, const float* div, const uint8_t* mask, float scale, bf16* out) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (v >= voxels) return;
+    __align__(16) bf16 c[8];
+    c[0] = __float2bfloat16_rn(scale * div[v]);
+    c[1] = __float2bfloat16_rn(mask && mask[v] ? 1.f : 0.f);
+#pragma unroll
+    for (int k = 2; k < 8; ++k) c[k] = __float2bfloat16_rn(0.f);
+    *reinterpret_cast<uint4*>(out + v * 8) = *reinterpret_cast<const uint4*>(c);
+}
+
+// Loss sum_v (pred - target)^2 / count over fluid voxels and its gradient,
+// written into channel 0 of an 8-channel BF16 tensor (the head's input gradient
+// is formed from it by the head's data-gradient convolution).
+__global__ void mse_kernel(long long voxels, const float* pred, int pred_pitch, const float* target,
+                           const uint8_t* mask, float inv_count, bf16* grad, double* loss) {
+    const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    double e = 0.0;
+    if (v < voxels) {
+        const bool fluid = !(mask && mask[v]);
+        const float d = fluid ? pred[v * pred_pitch] - target[v] : 0.f;
+        e = (double)d * d * inv_count;
+        __align__(16) bf16 c[8];
+        c[0] = __float2bfloat16_rn(2.f * d * inv_count);
+#pragma unroll
+        for (int k = 1; k < 8; ++k) c[k] = __float2bfloat16_rn(0.f);
+        *reinterpret_cast<uint4*>(grad + v * 8) = *reinterpret_cast<const uint4*>(c);
+    }
+    for (int o = 16; o > 0; o >>= 1) e += __shfl_xor_sync(0xffffffffu, e, o);
+    if ((threadIdx.x & 31) == 0 && e != 0.0) atomicAdd(loss, e);
+}
+
+// dst[t][co][ci] = src[flip ? taps - 1 - t : t][ci][co]: the weights of the
+// data-gradient convolution (transposed per tap; taps reversed for a padded
+// convolution whose gradient correlates with the mirrored kernel).
+__global__ void weight_transpose_kernel(int taps, int cin, int cout, int flip, const bf16* src, bf16* dst) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    const long long n = (long long)taps * cin * cout;
+    if (i >= n) return;
+    const int ci = (int)(i % cin);
+    const long long r = i / cin;
+    const int co = (int)(r % cout);
+    const int t = (int)(r / cout);
+    const int ts = flip ? taps - 1 - t : t;
+    dst[i] = src[((long long)ts * cin + ci) * cout + co];
+}
+
+bool view_ok(const FfxTensorView& t, int channels) {
+    return t.data && t.pitch >= t.offset + channels && t.pitch % 8 == 0 && t.offset % 8 == 0 &&
+           ((uintptr_t)t.data & 15) == 0;
+}
+
+int make_conv(const FfxConv* c, Conv& a) {
+    FFX_REQUIRE(c && c->batch >= 1 && c->c1 >= 8 && c->c1 % 8 == 0 && c->c2 >= 0 && c->c2 % 8 == 0 &&
+                    c->cout >= 8 && c->cout % 8 == 0 && c->weight && ((uintptr_t)c->weight & 15) == 0,
+                "ffx_conv: invalid arguments (channels multiples of 8, 16-byte aligned weights)");
+    for (int i = 0; i < 3; ++i)
+        FFX_REQUIRE(c->in_dims[i] >= 1 && c->out_dims[i] >= 1 && c->in_dims[i] <= 4096 && c->out_dims[i] <= 4096,
+                    "ffx_conv: invalid dimensions");
+    FFX_REQUIRE(view_ok(c->in1, c->c1) && (c->c2 == 0 || view_ok(c->in2, c->c2)),
+                "ffx_conv: input views need 16-byte aligned data, pitch and offset multiples of 8");
+    if (c->transposed) {
+        FFX_REQUIRE(c->ksize == 2 && c->stride == 2 && c->pad == 0 && c->out_dims[0] == 2 * c->in_dims[0] &&
+                        c->out_dims[1] == 2 * c->in_dims[1] && c->out_dims[2] == 2 * c->in_dims[2],
+                    "ffx_conv: the transposed form is 2^3 with stride 2 onto a grid twice as large");
+    } else {
+        FFX_REQUIRE(c->ksize >= 1 && c->ksize <= 3 && c->stride >= 1 && c->stride <= 2 && c->pad >= 0 &&
+                        c->pad < c->ksize,
+                    "ffx_conv: kernel size 1..3, stride 1..2, pad < kernel size");
+        for (int i = 0; i < 3; ++i)
+            FFX_REQUIRE(c->out_dims[i] == (c->in_dims[i] + 2 * c->pad - c->ksize) / c->stride + 1,
+                        "ffx_conv: output dimensions do not follow from input, kernel, stride and pad");
+    }
+    if (c->out)
+        FFX_REQUIRE(c->out_pitch >= c->out_offset + c->cout && c->out_pitch % 8 == 0 && c->out_offset % 8 == 0 &&
+                        ((uintptr_t)c->out & 15) == 0,
+                    "ffx_conv: output view");
+    if (c->out_f32) FFX_REQUIRE(c->out_f32_pitch >= c->cout && c->out_f32_pitch % 2 == 0, "ffx_conv: FP32 output pitch");
+    a.batch = c->batch;
+    a.id = c->in_dims[0]; a.ih = c->in_dims[1]; a.iw = c->in_dims[2];
+    a.od = c->out_dims[0]; a.oh = c->out_dims[1]; a.ow = c->out_dims[2];
+    a.c1 = c->c1; a.c2 = c->c2; a.cin = c->c1 + c->c2; a.cout = c->cout;
+    a.ks = c->ksize; a.stride = c->stride; a.pad = c->pad; a.transposed = c->transposed;
+    a.taps = c->transposed ? 1 : c->ksize * c->ksize * c->ksize;
+    a.units_per_tap = a.cin / 8;
+    a.k_units = a.taps * a.units_per_tap;
+    const long long in_vox = (long long)a.batch * a.id * a.ih * a.iw;
+    a.rows = c->transposed ? in_vox : (long long)a.batch * a.od * a.oh * a.ow;
+    FFX_REQUIRE(a.rows < (1LL << 40), "ffx_conv: too many voxels");
+    a.in1 = View{(const bf16*)c->in1.data, c->in1.pitch, c->in1.offset};
+    a.in2 = View{(const bf16*)(c->c2 ? c->in2.data : c->in1.data), c->c2 ? c->in2.pitch : 8,
+                 c->c2 ? c->in2.offset : 0};
+    a.w = (const bf16*)c->weight;
+    a.bias = c->bias;
+    a.relu = c->relu;
+    a.accumulate = c->accumulate;
+    a.out = (bf16*)c->out;
+    a.out_pitch = c->out_pitch;
+    a.out_offset = c->out_offset;
+    a.out_f32 = c->out_f32;
+    a.out_f32_pitch = c->out_f32_pitch;
+    return FFX_OK;
+}
+
+}  // namespace
+}  // namespace ffx
+
+using namespace ffx;
+
+extern "C" {
+
+int ffx_conv_forward(const FfxConv* c, void* stream) {
+    Conv a;
+    int e = make_conv(c, a);
+    if (e) return e;
+    FFX_REQUIRE(a.out || a.out_f32, "ffx_conv_forward: no output");
+    const dim3 grid((unsigned)((a.rows + kBM - 1) / kBM), (unsigned)((a.cout + kBN - 1) / kBN), a.transposed ? 8 : 1);
+    FFX_REQUIRE(grid.x < (1u << 31), "ffx_conv_forward: grid too large");
+    conv_fwd_kernel<<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    return launch_status("conv_fwd_kernel");
+}
+
+int ffx_conv_weight_grad(const FfxConv* c, const void* grad, int32_t grad_pitch, float* dweight, void* stream) {
+    Conv a;
+    int e = make_conv(c, a);
+    if (e) return e;
+    FFX_REQUIRE(grad && dweight && grad_pitch >= c->cout && grad_pitch % 8 == 0 && ((uintptr_t)grad & 15) == 0,
+                "ffx_conv_weight_grad: invalid gradient view");
+    const long long chunk = 8192;
+    const long long splits = (a.rows + chunk - 1) / chunk;
+    FFX_REQUIRE(splits * (a.transposed ? 8 : 1) < 65536, "ffx_conv_weight_grad: too many voxels for one launch");
+    const dim3 grid((unsigned)((a.k_units * 8 + 127) / 128), (unsigned)((a.cout + kBN - 1) / kBN),
+                    (unsigned)(splits * (a.transposed ? 8 : 1)));
+    conv_wgrad_kernel<<<grid, kGemmThreads, 0, as_stream(stream)>>>(a, (const bf16*)grad, grad_pitch, dweight, chunk);
+    return launch_status("conv_wgrad_kernel");
+}
+
+int ffx_relu_backward(int64_t voxels, int32_t channels, void* dy, int32_t dy_pitch, const void* y, int32_t y_pitch,
+                      int32_t y_offset, void* stream) {
+    FFX_REQUIRE(voxels >= 1 && channels >= 1 && dy && y && dy_pitch >= channels && y_pitch >= y_offset + channels,
+                "ffx_relu_backward: invalid arguments");
+    const long long n = voxels * channels;
+    relu_backward_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(voxels, channels, (bf16*)dy, dy_pitch,
+                                                                             (const bf16*)y, y_pitch, y_offset);
+    return launch_status("relu_backward_kernel");
+}
+
+int ffx_bias_grad(int64_t voxels, int32_t channels, const void* g, int32_t pitch, float* dbias, void* stream) {
+    FFX_REQUIRE(voxels >= 1 && channels >= 1 && channels <= 128 && 256 % channels == 0 && g && dbias &&
+                    pitch >= channels,
+                "ffx_bias_grad: invalid arguments (channels divide 256, at most 128)");
+    const long long blocks = std::min<long long>(1184, (voxels + 255) / 256);
+    bias_grad_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(voxels, channels, (const bf16*)g, pitch, dbias);
+    return launch_status("bias_grad_kernel");
+}
+
+int ffx_adam(int64_t n, float* w, float* m, float* v, const float* g, void* w_bf16, float lr, float beta1,
+             float beta2, float eps, int32_t step, void* stream) {
+    FFX_REQUIRE(n >= 1 && w && m && v && g && step >= 1 && lr > 0.f, "ffx_adam: invalid arguments");
+    const float c1 = 1.f - powf(beta1, (float)step), c2 = 1.f - powf(beta2, (float)step);
+    adam_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(n, w, m, v, g, (bf16*)w_bf16, lr, beta1, beta2,
+                                                                    eps, c1, c2);
+    return launch_status("adam_kernel");
+}
+
+int ffx_weight_transpose(int32_t taps, int32_t cin, int32_t cout, int32_t flip, const void* src, void* dst,
+                         void* stream) {
+    FFX_REQUIRE(taps >= 1 && cin >= 1 && cout >= 1 && src && dst && src != dst, "ffx_weight_transpose: invalid arguments");
+    const long long n = (long long)taps * cin * cout;
+    weight_transpose_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(taps, cin, cout, flip, (const bf16*)src,
+                                                                                (bf16*)dst);
+    return launch_status("weight_transpose_kernel");
+}
+
+int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float scale, void* out, void* stream) {
+    FFX_REQUIRE(voxels >= 1 && div && out && ((uintptr_t)out & 15) == 0, "ffx_pack_input: invalid arguments");
+    pack_input_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, div, mask, scale, (bf16*)out);
+    return launch_status("pack_input_kernel");
+}
+
+int ffx_mse_grad(int64_t voxels, const float* pred, int32_t pred_pitch, const float* target, const uint8_t* mask,
+                 float inv_count, void* grad, double* loss, void* stream) {
+    FFX_REQUIRE(voxels >= 1 && pred && target && grad && loss && pred_pitch >= 1 && ((uintptr_t)grad & 15) == 0,
+                "ffx_mse_grad: invalid arguments");
+    mse_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, pred, pred_pitch, target, mask,
+                                                                        inv_count, (bf16*)grad, loss);
+    return launch_status("mse_kernel");
+}
+
+}  // extern "C"

@@ -396,6 +396,56 @@ int ffx_moving_remap(const FfxGrid* g, int storage, const uint8_t* owners,
                      void* u, void* v, void* w, const float* wu, const float* wv,
                      const float* ww, void* stream);
 
+/* ------------------------------------------------- learned warm start (a18) */
+/* No counterpart in the reference: a 3D U-Net predicts the pressure from the
+ * divergence and the collider mask. Activations are NDHWC bfloat16 addressed
+ * through views (data, elements per voxel, first channel); every channel
+ * count, pitch and offset is a multiple of 8 and data is 16-byte aligned. */
+typedef struct FfxTensorView {
+    const void* data;
+    int32_t pitch, offset;
+} FfxTensorView;
+typedef struct FfxConv {
+    int32_t batch;
+    int32_t in_dims[3];      /* d, h, w of the input grid */
+    int32_t out_dims[3];     /* d, h, w of the output grid */
+    int32_t c1, c2, cout;    /* input channels read from in1, then in2 (concatenated; c2 may be 0) */
+    int32_t ksize, stride, pad;
+    int32_t transposed;      /* 1: 2^3 stride-2 transposed convolution onto the doubled grid */
+    FfxTensorView in1, in2;
+    const void* weight;      /* bf16 [taps][c1 + c2][cout] (transposed: taps = 8 parity classes) */
+    const float* bias;       /* optional, FP32 [cout] */
+    int32_t relu, accumulate; /* ReLU on the result; add to the existing BF16 output */
+    void* out; int32_t out_pitch, out_offset;   /* optional BF16 output view */
+    float* out_f32; int32_t out_f32_pitch;      /* optional FP32 output */
+} FfxConv;
+/* Convolution as an implicit GEMM on the BF16 tensor cores (FP32 accumulation). */
+int ffx_conv_forward(const FfxConv* conv, void* stream);
+/* dweight[k][cout] += sum over output voxels of input(k) * grad (FP32, caller zeroes);
+ * `grad` is the BF16 gradient of the convolution's output (ReLU already applied). */
+int ffx_conv_weight_grad(const FfxConv* conv, const void* grad, int32_t grad_pitch, float* dweight,
+                         void* stream);
+/* dy *= (y > 0) in place. */
+int ffx_relu_backward(int64_t voxels, int32_t channels, void* dy, int32_t dy_pitch, const void* y,
+                      int32_t y_pitch, int32_t y_offset, void* stream);
+/* dbias[c] += sum over voxels of g[v][c] (channels <= 128, dividing 256). */
+int ffx_bias_grad(int64_t voxels, int32_t channels, const void* g, int32_t pitch, float* dbias,
+                  void* stream);
+/* Weights of the data-gradient convolution: dst[t][co][ci] = src[flip ? taps-1-t : t][ci][co]. */
+int ffx_weight_transpose(int32_t taps, int32_t cin, int32_t cout, int32_t flip, const void* src,
+                         void* dst, void* stream);
+/* Adam step on FP32 master weights w (moments m, v) with gradient g; w_bf16 (optional)
+ * receives the rounded weights. */
+int ffx_adam(int64_t n, float* w, float* m, float* v, const float* g, void* w_bf16, float lr,
+             float beta1, float beta2, float eps, int32_t step, void* stream);
+/* Network input, 8 BF16 channels per voxel: scale * div, solid mask, zeros. */
+int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float scale, void* out,
+                   void* stream);
+/* *loss += sum over fluid voxels of (pred - target)^2 * inv_count; grad (8 BF16
+ * channels per voxel) = its derivative in channel 0. */
+int ffx_mse_grad(int64_t voxels, const float* pred, int32_t pred_pitch, const float* target,
+                 const uint8_t* mask, float inv_count, void* grad, double* loss, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -1,0 +1,228 @@
+"""The learned warm start's kernels: BF16 implicit-GEMM convolutions (every
+form the U-Net uses) against torch FP64 on the same BF16 values, weight
+gradients, Adam, and the whole network's forward and backward against the
+FP64 oracle (oracle/unet_ref.py)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+import torch.nn.functional as F
+
+from fluxfx_b200 import _native as N
+from oracle import unet_ref as U
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def lib():
+    return N.load()
+
+
+def bf(x):
+    return x.to(torch.bfloat16)
+
+
+def rel_l2(a, b):
+    a = a.detach().double().cpu()
+    b = b.detach().double().cpu()
+    return float((a - b).norm() / max(float(b.norm()), 1e-30))
+
+
+def rel_err(a, b):
+    a = a.detach().double().cpu()
+    b = b.detach().double().cpu()
+    return float((a - b).abs().max() / max(float(b.abs().max()), 1e-30))
+
+
+def conv_struct(batch, ind, outd, c1, c2, cout, ks, stride, pad, transposed, in1, p1, o1, in2, p2, o2, w, bias,
+                relu, out, op, oo, out32, p32, accumulate=0):
+    c = N.FfxConv()
+    c.batch = batch
+    c.in_dims = (N.i32 * 3)(*ind)
+    c.out_dims = (N.i32 * 3)(*outd)
+    c.c1, c.c2, c.cout = c1, c2, cout
+    c.ksize, c.stride, c.pad, c.transposed = ks, stride, pad, transposed
+    c.in1 = N.FfxTensorView(in1.data_ptr(), p1, o1)
+    c.in2 = N.FfxTensorView(in2.data_ptr() if in2 is not None else None, p2, o2)
+    c.weight = w.data_ptr()
+    c.bias = bias.data_ptr() if bias is not None else None
+    c.relu, c.accumulate = relu, accumulate
+    c.out = out.data_ptr() if out is not None else None
+    c.out_pitch, c.out_offset = op, oo
+    c.out_f32 = out32.data_ptr() if out32 is not None else None
+    c.out_f32_pitch = p32
+    return c
+
+
+@pytest.mark.parametrize('kind', ['conv3', 'conv3_concat', 'down', 'up', 'head'])
+def test_convolution_forms_match_torch(lib, kind):
+    g = torch.Generator().manual_seed(1)
+    B, D, H, W = 2, 12, 8, 16
+    c1, c2, cout = {'conv3': (16, 0, 32), 'conv3_concat': (16, 24, 40), 'down': (16, 0, 32), 'up': (32, 0, 16),
+                    'head': (16, 0, 8)}[kind]
+    cin = c1 + c2
+    ind = (D // 2, H // 2, W // 2) if kind == 'up' else (D, H, W)
+    outd = {'down': (D // 2, H // 2, W // 2), 'up': (D, H, W)}.get(kind, (D, H, W))
+    taps = {'down': 8, 'up': 8, 'head': 1}.get(kind, 27)
+    x1 = bf(torch.randn((B, *ind, c1 + 8), generator=g))        # pitch c1 + 8, offset 8 (a view)
+    x2 = bf(torch.randn((B, *ind, c2), generator=g)) if c2 else None
+    w = bf(torch.randn((taps, cin, cout), generator=g) / (taps * cin) ** 0.5)
+    bias = torch.randn(cout, generator=g)
+    dx1, dx2, dw, db = x1.cuda(), (x2.cuda() if x2 is not None else None), w.cuda(), bias.cuda()
+    out32 = torch.zeros((B, *outd, cout), device='cuda')
+    out16 = torch.zeros((B, *outd, cout + 16), dtype=torch.bfloat16, device='cuda')
+    ks, stride, pad = {'conv3': (3, 1, 1), 'conv3_concat': (3, 1, 1), 'down': (2, 2, 0), 'up': (2, 2, 0),
+                       'head': (1, 1, 0)}[kind]
+    c = conv_struct(B, ind, outd, c1, c2, cout, ks, stride, pad, int(kind == 'up'), dx1, c1 + 8, 8, dx2, c2, 0, dw,
+                    db, 1, out16, cout + 16, 8, out32, cout)
+    N.check(lib.ffx_conv_forward(C.byref(c), None))
+    torch.cuda.synchronize()
+    # torch FP64 on the same BF16 values
+    xin = x1[..., 8:].double()
+    if x2 is not None:
+        xin = torch.cat([xin, x2.double()], -1)
+    xt = xin.permute(0, 4, 1, 2, 3)
+    wt = U.torch_weight('up' if kind == 'up' else {'head': 'head', 'down': 'down'}.get(kind, 'conv3'), w.double())
+    if kind == 'up':
+        ref = F.conv_transpose3d(xt, wt, bias.double(), stride=2)
+    else:
+        ref = F.conv3d(xt, wt, bias.double(), stride=stride, padding=pad)
+    ref = torch.relu(ref).permute(0, 2, 3, 4, 1)
+    assert rel_err(out32, ref) < 1e-5, rel_err(out32, ref)
+    assert rel_err(out16[..., 8:8 + cout].float(), ref) < 8e-3
+    assert float(out16[..., :8].abs().max()) == 0 and float(out16[..., 8 + cout:].abs().max()) == 0
+
+
+@pytest.mark.parametrize('kind', ['conv3', 'down', 'up'])
+def test_weight_gradients_match_torch(lib, kind):
+    g = torch.Generator().manual_seed(2)
+    B, D, H, W = 2, 8, 12, 8
+    cin, cout = (16, 32) if kind != 'up' else (32, 16)
+    ind = (D // 2, H // 2, W // 2) if kind == 'up' else (D, H, W)
+    outd = (D // 2, H // 2, W // 2) if kind == 'down' else (D, H, W)
+    taps = 27 if kind == 'conv3' else 8
+    x = bf(torch.randn((B, *ind, cin), generator=g))
+    gy = bf(torch.randn((B, *outd, cout), generator=g))
+    w = bf(torch.randn((taps, cin, cout), generator=g))
+    dw = torch.zeros((taps, cin, cout), device='cuda')
+    ks, stride, pad = (3, 1, 1) if kind == 'conv3' else (2, 2, 0)
+    xcu, wcu, gcu = x.cuda(), w.cuda(), gy.cuda()     # kept alive until the kernels have run
+    c = conv_struct(B, ind, outd, cin, 0, cout, ks, stride, pad, int(kind == 'up'), xcu, cin, 0, None, 0, 0,
+                    wcu, None, 0, None, 0, 0, None, 0)
+    N.check(lib.ffx_conv_weight_grad(C.byref(c), C.c_void_p(gcu.data_ptr()), cout, C.c_void_p(dw.data_ptr()), None))
+    db = torch.zeros(cout, device='cuda')
+    N.check(lib.ffx_bias_grad(B * outd[0] * outd[1] * outd[2], cout, C.c_void_p(gcu.data_ptr()), cout,
+                              C.c_void_p(db.data_ptr()), None))
+    torch.cuda.synchronize()
+    wl = w.double().requires_grad_(True)
+    bl = torch.zeros(cout, dtype=torch.float64, requires_grad=True)
+    xt = x.double().permute(0, 4, 1, 2, 3)
+    wt = U.torch_weight('up' if kind == 'up' else ('down' if kind == 'down' else 'conv3'), wl)
+    y = F.conv_transpose3d(xt, wt, bl, stride=2) if kind == 'up' else F.conv3d(xt, wt, bl, stride=stride, padding=pad)
+    (y * gy.double().permute(0, 4, 1, 2, 3)).sum().backward()
+    assert rel_err(dw, wl.grad) < 1e-4, rel_err(dw, wl.grad)
+    assert rel_err(db, bl.grad) < 1e-4
+
+
+def test_adam_matches_formula(lib):
+    n = 1000
+    g = torch.Generator().manual_seed(3)
+    w, m, v, gr = (torch.randn(n, generator=g) for _ in range(4))
+    v = v.abs()
+    dw, dm, dv, dg = w.cuda(), m.cuda(), v.cuda(), gr.cuda()
+    w16 = torch.zeros(n, dtype=torch.bfloat16, device='cuda')
+    ptr = lambda t: C.c_void_p(t.data_ptr())
+    N.check(lib.ffx_adam(n, ptr(dw), ptr(dm), ptr(dv), ptr(dg), ptr(w16), 1e-3, 0.9, 0.999, 1e-8, 3, None))
+    torch.cuda.synchronize()
+    m2 = 0.9 * m + 0.1 * gr
+    v2 = 0.999 * v + 0.001 * gr * gr
+    w2 = w - 1e-3 * (m2 / (1 - 0.9 ** 3)) / ((v2 / (1 - 0.999 ** 3)).sqrt() + 1e-8)
+    assert rel_err(dw, w2) < 1e-6 and rel_err(dm, m2) < 1e-6 and rel_err(dv, v2) < 1e-6
+    assert rel_err(w16.float(), w2) < 1e-2
+
+
+def test_unet_forward_and_gradients_match_oracle():
+    from fluxfx_b200.learned.unet import UNet
+    dev = torch.device('cuda')
+    net = UNet(dev, seed=4)
+    g = torch.Generator().manual_seed(5)
+    B, D = 2, 16
+    div = torch.randn((B, D, D, D), generator=g)
+    mask = (torch.rand((B, D, D, D), generator=g) < 0.1).to(torch.uint8)
+    target = torch.randn((B, D, D, D), generator=g)
+    stream = torch.cuda.current_stream().cuda_stream
+    pred = net.forward(div.cuda(), mask.cuda(), 0.5, stream)
+    loss = net.loss_backward(target.cuda(), mask.cuda(), stream)
+    torch.cuda.synchronize()
+    x = torch.zeros((B, 8, D, D, D), dtype=torch.float64)
+    x[:, 0] = (0.5 * div).to(torch.bfloat16).double()
+    x[:, 1] = mask.double()
+    rpred, rloss, _ = U.loss_and_grads(net.layers, x, target.double(), mask.bool())
+    # BF16 activations: the device and the oracle round the same values, but
+    # FP32-vs-FP64 accumulation can flip a rounding, which then propagates.
+    assert rel_err(pred, rpred) < 3e-2, rel_err(pred, rpred)
+    assert float(loss[0]) == pytest.approx(rloss, rel=5e-2)
+    # A rounding flip next to zero also flips a ReLU, which zeroes or keeps a
+    # whole gradient element; with a fraction f of flipped voxels the L2 error
+    # of every gradient upstream grows like sqrt(f). So the gradients are
+    # checked with the device's own ReLU pattern, leaving only the BF16
+    # rounding of activations and of their gradients (both modelled).
+    masks = {l.name: (net.activation(l.name) > 0).permute(0, 4, 1, 2, 3).cpu() for l in net.layers if l.relu}
+    _, _, grads = U.loss_and_grads(net.layers, x, target.double(), mask.bool(), relu_masks=masks)
+    errs = {l.name: (rel_l2(l.gw, grads[l.name][0]), rel_l2(l.gb, grads[l.name][1])) for l in net.layers}
+    for name, (ew, eb) in errs.items():
+        assert ew < 2e-2 and eb < 2e-2, (name, errs)
+
+
+@pytest.mark.parametrize('kind', ['conv3', 'down', 'up', 'head'])
+def test_data_gradients_match_torch(lib, kind):
+    """The backward-data convolutions as the network issues them: the flipped
+    transpose of a 3^3 kernel, the transposed 2^3 stride-2 form for a
+    down-sampling, the 2^3 stride-2 form for an up-sampling, and the head."""
+    from fluxfx_b200.learned.unet import Layer
+    g = torch.Generator().manual_seed(8)
+    B, D, H, W = 2, 8, 8, 16
+    cin, cout = {'conv3': (16, 32), 'down': (16, 32), 'up': (32, 16), 'head': (16, 8)}[kind]
+    layer = Layer('t', kind, cin, cout, True, 'cuda', g)
+    ind = (D // 2, H // 2, W // 2) if kind == 'up' else (D, H, W)
+    outd = (D // 2, H // 2, W // 2) if kind == 'down' else (D, H, W)
+    gy = bf(torch.randn((B, *outd, cout), generator=g))
+    gcu = gy.cuda()
+    gin = torch.zeros((B, *ind, cin + 8), dtype=torch.bfloat16, device='cuda')   # a view at offset 8
+    flip = int(kind == 'conv3')
+    N.check(lib.ffx_weight_transpose(layer.taps, cin, cout, flip, C.c_void_p(layer.w16.data_ptr()),
+                                     C.c_void_p(layer.wt16.data_ptr()), None))
+    ks, stride, pad, tr = {'conv3': (3, 1, 1, 0), 'down': (2, 2, 0, 1), 'up': (2, 2, 0, 0), 'head': (1, 1, 0, 0)}[kind]
+    c = conv_struct(B, outd, ind, cout, 0, cin, ks, stride, pad, tr, gcu, cout, 0, None, 0, 0, layer.wt16, None, 0,
+                    gin, cin + 8, 8, None, 0)
+    N.check(lib.ffx_conv_forward(C.byref(c), None))
+    torch.cuda.synchronize()
+    x = torch.zeros((B, cin, *ind), dtype=torch.float64, requires_grad=True)
+    wt = U.torch_weight(kind, layer.w16.double().cpu())
+    if kind == 'up':
+        y = F.conv_transpose3d(x, wt, stride=2)
+    else:
+        y = F.conv3d(x, wt, stride=stride, padding=pad)
+    (y * gy.double().permute(0, 4, 1, 2, 3)).sum().backward()
+    ref = x.grad.permute(0, 2, 3, 4, 1)
+    assert rel_err(gin[..., 8:].float(), ref) < 8e-3, rel_err(gin[..., 8:].float(), ref)
+    assert float(gin[..., :8].abs().max()) == 0
+
+
+def test_training_steps_reduce_the_loss():
+    from fluxfx_b200.learned.unet import UNet
+    dev = torch.device('cuda')
+    net = UNet(dev, seed=6)
+    g = torch.Generator().manual_seed(7)
+    B, D = 2, 16
+    div = torch.randn((B, D, D, D), generator=g).cuda()
+    target = (0.3 * div).contiguous()
+    stream = torch.cuda.current_stream().cuda_stream
+    losses = []
+    for _ in range(30):
+        net.forward(div, None, 1.0, stream)
+        losses.append(float(net.loss_backward(target, None, stream)[0]))
+        net.adam_step(3e-3, stream)
+    assert losses[-1] < 0.5 * losses[0], losses
