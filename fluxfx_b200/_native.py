@@ -85,6 +85,36 @@ class FfxConv(C.Structure):
                 ('out_f32_pitch', i32)]
 
 
+BATCH_MAX = 64
+BATCH_LEVELS = 8
+(PASS_PREDICTOR, PASS_VELOCITY, PASS_DIVERGENCE, PASS_SCALE, PASS_GRADIENT, PASS_SCALAR_PREDICTOR,
+ PASS_SCALAR_REVERSE, PASS_SCALAR_FINAL, PASS_RESIDUAL_MAX, PASS_SMOOTH, PASS_RESIDUAL_RESTRICT, PASS_PROLONG_SMOOTH,
+ PASS_DIRECT, PASS_KINDS) = range(14)
+PASS_NAMES = ('predictor', 'velocity', 'divergence', 'scale', 'gradient', 'scalar_predictor', 'scalar_reverse',
+              'scalar_final', 'residual_max', 'smooth', 'residual_restrict', 'prolong_smooth', 'direct')
+
+
+class FfxBatchLevel(C.Structure):
+    _fields_ = [('level', FfxGraphLevel), ('p', vp), ('q', vp), ('rhs', vp)]
+
+
+class FfxBatchDomain(C.Structure):
+    _fields_ = [('grid', FfxGrid), ('solid', vp), ('halo', vp), ('u', vp), ('v', vp), ('w', vp), ('pu', vp),
+                ('pv', vp), ('pw', vp), ('bu', vp), ('bv', vp), ('bw', vp), ('density', vp * 2),
+                ('temperature', vp * 2), ('predictor', vp * 2), ('reverse', vp * 2), ('after', vp),
+                ('sources', FfxSources), ('velocity_corrected', i32), ('scalar_corrected', i32), ('blend', f32),
+                ('lift', f32), ('weight', f32), ('density_channel', FfxScalarChannel),
+                ('heat_channel', FfxScalarChannel), ('cell', C.c_double), ('cfl', C.c_double),
+                ('dt_max', C.c_double), ('dt0', f32), ('levels', i32), ('level', FfxBatchLevel * BATCH_LEVELS),
+                ('tail_start', i32), ('inverse', vp), ('pre', i32), ('post', i32), ('max_cycles', i32),
+                ('tolerance', C.c_double)]
+
+
+class FfxBatchStats(C.Structure):
+    _fields_ = [('dt', f32), ('last_dt', f32), ('last_cycles', i32), ('total_cycles', i32), ('steps', i32),
+                ('maxima', f3), ('time', C.c_double)]
+
+
 P = C.POINTER
 _PROTOTYPES = {
     'ffx_abi_version': (C.c_int, []),
@@ -152,6 +182,16 @@ _PROTOTYPES = {
     'ffx_divergence_stats_workspace': (C.c_size_t, [i64]),
     'ffx_divergence_stats': (C.c_int, [i64, vp, vp, vp, vp, C.c_size_t, vp]),
     'ffx_divergence_stats_static': (C.c_int, [i64, vp, vp, vp, vp]),
+    'ffx_batch_workspace_bytes': (C.c_int, [P(FfxBatchDomain), i32, P(i64)]),
+    'ffx_batch_create': (C.c_int, [P(FfxBatchDomain), i32, vp, i64, P(vp)]),
+    'ffx_batch_set_config': (C.c_int, [vp, i32, i32, i32]),
+    'ffx_batch_tune_pass': (C.c_int, [vp, i32, vp]),
+    'ffx_batch_graph': (C.c_int, [vp, i32, P(vp)]),
+    'ffx_batch_launch': (C.c_int, [vp, vp, i32, vp]),
+    'ffx_batch_graph_free': (C.c_int, [vp]),
+    'ffx_batch_stats': (C.c_int, [vp, P(FfxBatchStats), vp]),
+    'ffx_batch_parity': (C.c_int, [vp]),
+    'ffx_batch_destroy': (C.c_int, [vp]),
 }
 
 _LIB = None

@@ -8,6 +8,7 @@
 // neighbouring threads overlap, so the L1/L2 hit rate is high and HBM traffic
 // stays close to one read of each field per pass.
 #include "ffx_host.cuh"
+#include "ffx_batch.cuh"
 
 namespace ffx {
 namespace {
@@ -23,17 +24,17 @@ struct FaceIdx {
     int i;
 };
 
-// Face of the launch thread (face_grid geometry): blockIdx.z = axis*(nz+1) + z.
-__device__ __forceinline__ bool face_coords(const Dev& d, FaceIdx& f) {
+// Face of the thread (face_grid geometry): block z = axis*(nz+1) + z.
+__device__ __forceinline__ bool face_coords(const Blk& b, const Dev& d, FaceIdx& f) {
     const int nz1 = d.nz + 1;
-    const int zz = blockIdx.z;
+    const int zz = b.z;
     f.axis = zz >= 2 * nz1 ? 2 : (zz >= nz1 ? 1 : 0);
     f.z = zz - f.axis * nz1;
     f.sx = d.nx + (f.axis == 0);
     f.sy = d.ny + (f.axis == 1);
     f.sz = d.nz + (f.axis == 2);
-    f.x = blockIdx.x * kBX + threadIdx.x;
-    f.y = blockIdx.y * kBY + threadIdx.y;
+    f.x = b.x * b.bw + b.ox;
+    f.y = b.y * b.bh + b.oy;
     if (f.x >= f.sx || f.y >= f.sy || f.z >= f.sz) return false;
     f.i = f.x + f.sx * (f.y + f.sy * f.z);
     return true;
@@ -103,13 +104,26 @@ __device__ __forceinline__ float fetch_closed(const Dev& d, const T* __restrict_
 }
 
 // ------------------------------------------------------------ face predictor
+template <typename T>
+struct PredParams {
+    Dev d;
+    const uint8_t* solid;
+    const uint8_t* halo;
+    Faces<T> F;
+    float dt;
+    T* out[3];
+};
+
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const uint8_t* __restrict__ solid,
-                                                                  const uint8_t* __restrict__ halo,
-                                                                  Faces<T> F, float dt, T* pu, T* pv, T* pw) {
+__device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, const Blk& b) {
+    const Dev& d = P.d;
+    const uint8_t* __restrict__ solid = P.solid;
+    const uint8_t* __restrict__ halo = P.halo;
+    const Faces<T>& F = P.F;
+    const float dt = P.dt;
     FaceIdx f;
-    if (!face_coords(d, f)) return;
-    T* out = f.axis == 0 ? pu : (f.axis == 1 ? pv : pw);
+    if (!face_coords(b, d, f)) return;
+    T* out = P.out[f.axis];
     if (MASK && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
         Store<T>::st(out, f.i, 0.f);
         return;
@@ -123,6 +137,11 @@ __global__ void __launch_bounds__(kThreads) face_predictor_kernel(Dev d, const u
     float value = sample_face(src, f.sx, f.sy, f.sz, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
                                 dv_h<P2>(d, dep.z, 2) - oz);
     Store<T>::st(out, f.i, value);
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(kThreads) face_predictor_kernel(const __grid_constant__ PredParams<T> P) {
+    face_predictor_body<T, MASK, P2>(P, hw_blk());
 }
 
 // ------------------------------------------------------- velocity transport
@@ -143,10 +162,10 @@ struct VelParams {
 };
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
+__device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, const Blk& b) {
     const Dev& d = P.d;
     FaceIdx f;
-    if (!face_coords(d, f)) return;
+    if (!face_coords(b, d, f)) return;
     const int axis = f.axis;
     const float dt = P.dt;
     bool blocked = MASK && solid_face(d, P.solid, f.x, f.y, f.z, axis);
@@ -236,12 +255,17 @@ __global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_
     Store<T>::st(P.out[axis], f.i, value);
 }
 
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
+    advect_velocity_body<T, MASK, P2>(P, hw_blk());
+}
+
 // P0.3 plain face self-advection (mac_advect_velocity.glsl).
 template <typename T>
 __global__ void __launch_bounds__(kThreads) mac_advect_velocity_kernel(Dev d, Faces<T> F, float dt, T* ou, T* ov,
                                                                        T* ow) {
     FaceIdx f;
-    if (!face_coords(d, f)) return;
+    if (!face_coords(hw_blk(), d, f)) return;
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.e[0] / d.nf[0], ((float)f.y + oy) * d.e[1] / d.nf[1],
             ((float)f.z + oz) * d.e[2] / d.nf[2]};
@@ -280,10 +304,10 @@ struct ScalarXport {
 };
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
+__device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, const Blk& b) {
     const Dev& d = P.d;
     int x, y, z;
-    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    if (!cell_coords(b, d.nx, d.ny, x, y, z)) return;
     const int i = cidx(d, x, y, z);
     if (MASK && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, 0.f);
@@ -296,6 +320,11 @@ __global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     for (int c = 0; c < P.count; ++c)
         Store<T>::st(P.out[c], i, sample_closed<T, MASK>(d, P.solid, P.in[c], qx, qy, qz));
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
+    scalar_transport_body<T, MASK, P2>(P, hw_blk());
 }
 
 template <typename T>
@@ -322,11 +351,11 @@ struct ScalarFinal {
 };
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
+__device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, const Blk& b) {
     const Dev& d = P.d;
     int x, y, z;
     float vmax[3] = {0.f, 0.f, 0.f};
-    if (cell_coords(d.nx, d.ny, x, y, z)) {
+    if (cell_coords(b, d.nx, d.ny, x, y, z)) {
         const int i = cidx(d, x, y, z);
         if (MASK && __ldg(P.solid + i)) {
             for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
@@ -396,6 +425,11 @@ __global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_c
             __syncthreads();
         }
     }
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
+    advect_scalars_body<T, MASK, P2>(P, hw_blk());
 }
 
 // P0.2 open-boundary transport in an analytic flow (advect.glsl).
@@ -502,8 +536,14 @@ int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const 
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
         const uint8_t* halo = solid ? s->halo : nullptr;
-        FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P, (face_predictor_kernel<T, M, P><<<blocks, threads, 0, st>>>(
-            d, solid, halo, F, dt, (T*)pu, (T*)pv, (T*)pw)));
+        PredParams<T> Q;
+        Q.d = d;
+        Q.solid = solid;
+        Q.halo = halo;
+        Q.F = F;
+        Q.dt = dt;
+        Q.out[0] = (T*)pu; Q.out[1] = (T*)pv; Q.out[2] = (T*)pw;
+        FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P, (face_predictor_kernel<T, M, P><<<blocks, threads, 0, st>>>(Q)));
     });
     return launch_status("face_predictor_kernel");
 }
@@ -684,3 +724,194 @@ int ffx_mac_advect_density(const FfxGrid* g, int storage, const void* u, const v
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------- batched passes
+// Persistent launches over the tiles of many domains (ffx_batch.cuh). Every
+// domain is on the collider path; pow2 (exact reciprocal division) is chosen
+// per domain, as the single-domain launch chooses it per launch.
+namespace ffx {
+namespace {
+
+// prep: the descriptor's time step is the domain's device dt (times `sign`).
+struct DeviceDt {
+    const BatchState* state;
+    float sign;
+    template <class D>
+    __device__ __forceinline__ void operator()(D& sh, int slot) const { sh.dt = sign * state[slot].dt; }
+};
+
+__global__ void __launch_bounds__(kBatchThreads) batch_predictor_kernel(const __grid_constant__ BatchMap M,
+                                                                        const PredParams<float>* descs,
+                                                                        const BatchState* state) {
+    for_tiles(M, descs, state, false, DeviceDt{state, 1.f}, [](const PredParams<float>& P, const Blk& b, int) {
+        if (P.d.pow2) face_predictor_body<float, true, true>(P, b);
+        else face_predictor_body<float, true, false>(P, b);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_velocity_kernel(const __grid_constant__ BatchMap M,
+                                                                       const VelParams<float>* descs,
+                                                                       const BatchState* state) {
+    for_tiles(M, descs, state, false, DeviceDt{state, 1.f}, [](const VelParams<float>& P, const Blk& b, int) {
+        if (P.d.pow2) advect_velocity_body<float, true, true>(P, b);
+        else advect_velocity_body<float, true, false>(P, b);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_scalar_transport_kernel(const __grid_constant__ BatchMap M,
+                                                                               const ScalarXport<float>* descs,
+                                                                               const BatchState* state, float sign) {
+    for_tiles(M, descs, state, false, DeviceDt{state, sign}, [](const ScalarXport<float>& P, const Blk& b, int) {
+        if (P.d.pow2) scalar_transport_body<float, true, true>(P, b);
+        else scalar_transport_body<float, true, false>(P, b);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_scalars_kernel(const __grid_constant__ BatchMap M,
+                                                                      const ScalarFinal<float>* descs,
+                                                                      const BatchState* state) {
+    for_tiles(M, descs, state, false, DeviceDt{state, 1.f}, [](const ScalarFinal<float>& P, const Blk& b, int) {
+        if (P.d.pow2) advect_scalars_body<float, true, true>(P, b);
+        else advect_scalars_body<float, true, false>(P, b);
+    });
+}
+
+template <class K>
+int occupancy(K kernel) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBatchThreads, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+unsigned grid_of(const BatchMap& M, int grid) { return (unsigned)(grid > 0 && grid < M.total ? grid : M.total); }
+
+}  // namespace
+
+namespace batch {
+
+size_t predictor_desc(const FfxBatchDomain& D, void* out) {
+    if (out) {
+        PredParams<float> P;
+        P.d = make_dev(D.grid);
+        P.solid = D.solid;
+        P.halo = D.halo;
+        P.F = {D.u, D.v, D.w};
+        P.dt = 0.f;
+        P.out[0] = D.pu; P.out[1] = D.pv; P.out[2] = D.pw;
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(PredParams<float>);
+}
+
+size_t velocity_desc(const FfxBatchDomain& D, int parity, void* out) {
+    if (out) {
+        VelParams<float> P;
+        memset(&P, 0, sizeof P);
+        P.d = make_dev(D.grid);
+        P.solid = D.solid;
+        P.halo = D.halo;
+        P.F = {D.u, D.v, D.w};
+        P.P = D.velocity_corrected ? Faces<float>{D.pu, D.pv, D.pw} : P.F;
+        P.dt = 0.f;
+        P.blend = D.blend;
+        P.lift = D.lift;
+        P.weight = D.weight;
+        P.corrected = D.velocity_corrected;
+        P.apply_walls = 1;
+        P.density = D.density[parity];
+        P.temperature = D.temperature[parity];
+        P.out[0] = D.bu; P.out[1] = D.bv; P.out[2] = D.bw;
+        P.walls = make_walls(nullptr);
+        const float extent[3] = {D.grid.ex, D.grid.ey, D.grid.ez};
+        P.src = make_src(&D.sources, extent);
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(VelParams<float>);
+}
+
+size_t scalar_xport_desc(const FfxBatchDomain& D, int parity, int reverse, void* out) {
+    if (out) {
+        ScalarXport<float> P;
+        memset(&P, 0, sizeof P);
+        P.d = make_dev(D.grid);
+        P.solid = D.solid;
+        P.halo = D.halo;
+        P.F = {D.u, D.v, D.w};
+        P.dt = 0.f;
+        P.count = 2;
+        P.in[0] = reverse ? D.predictor[0] : D.density[parity];
+        P.in[1] = reverse ? D.predictor[1] : D.temperature[parity];
+        P.out[0] = reverse ? D.reverse[0] : D.predictor[0];
+        P.out[1] = reverse ? D.reverse[1] : D.predictor[1];
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(ScalarXport<float>);
+}
+
+size_t scalar_final_desc(const FfxBatchDomain& D, int parity, void* out) {
+    if (out) {
+        ScalarFinal<float> P;
+        memset(&P, 0, sizeof P);
+        P.d = make_dev(D.grid);
+        P.solid = D.solid;
+        P.halo = D.halo;
+        P.F = {D.u, D.v, D.w};
+        P.dt = 0.f;
+        P.corrected = D.scalar_corrected;
+        P.count = 2;
+        const FfxScalarChannel* H[2] = {&D.density_channel, &D.heat_channel};
+        const float* field[2] = {D.density[parity], D.temperature[parity]};
+        float* dst[2] = {D.density[1 - parity], D.temperature[1 - parity]};
+        for (int c = 0; c < 2; ++c) {
+            Channel<float> C = {};
+            C.field = field[c];
+            C.pred = D.scalar_corrected ? D.predictor[c] : field[c];
+            C.rev = D.scalar_corrected ? D.reverse[c] : field[c];
+            C.out = dst[c];
+            C.rate = H[c]->rate;
+            C.decay = H[c]->decay;
+            C.target = H[c]->target;
+            C.channel = H[c]->channel;
+            C.table_target = H[c]->table_target;
+            P.ch[c] = C;
+        }
+        P.maxima = nullptr;
+        const float extent[3] = {D.grid.ex, D.grid.ey, D.grid.ez};
+        P.src = make_src(&D.sources, extent);
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(ScalarFinal<float>);
+}
+
+cudaError_t face_predictor(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_predictor_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(M, (const PredParams<float>*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t advect_velocity(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_velocity_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(M, (const VelParams<float>*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t scalar_transport(const BatchMap& M, const void* descs, BatchState* state, int reverse, int grid,
+                             cudaStream_t st) {
+    batch_scalar_transport_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(
+        M, (const ScalarXport<float>*)descs, state, reverse ? -1.f : 1.f);
+    return cudaGetLastError();
+}
+cudaError_t advect_scalars(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_scalars_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(M, (const ScalarFinal<float>*)descs, state);
+    return cudaGetLastError();
+}
+
+int advect_resident_blocks(int kind) {
+    switch (kind) {
+        case kPredictor: return occupancy(batch_predictor_kernel);
+        case kVelocity: return occupancy(batch_velocity_kernel);
+        case kScalarPredictor:
+        case kScalarReverse: return occupancy(batch_scalar_transport_kernel);
+        case kScalarFinal: return occupancy(batch_scalars_kernel);
+        default: return 0;
+    }
+}
+
+}  // namespace batch
+}  // namespace ffx

@@ -97,11 +97,26 @@ inline dim3 cell_block() { return dim3(kBX, kBY, 1); }
 inline dim3 cell_grid(int nx, int ny, int nz) {
     return dim3((unsigned)((nx + kBX - 1) / kBX), (unsigned)((ny + kBY - 1) / kBY), (unsigned)nz);
 }
-__device__ __forceinline__ bool cell_coords(int nx, int ny, int& x, int& y, int& z) {
-    x = blockIdx.x * kBX + threadIdx.x;
-    y = blockIdx.y * kBY + threadIdx.y;
-    z = blockIdx.z;
+// The block a thread works on: the hardware block of a single-domain launch,
+// or a tile of one domain inside a batched persistent launch. (x, y, z) index
+// tiles of bw x bh threads; (ox, oy) is the thread's place in its tile; gz is
+// the number of z tiles (the stride of z-strided reductions).
+struct Blk {
+    int x, y, z, gz;
+    int bw, bh, ox, oy;
+};
+__device__ __forceinline__ Blk hw_blk() {
+    return Blk{(int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)gridDim.z, kBX, kBY, (int)threadIdx.x,
+               (int)threadIdx.y};
+}
+__device__ __forceinline__ bool cell_coords(const Blk& b, int nx, int ny, int& x, int& y, int& z) {
+    x = b.x * b.bw + b.ox;
+    y = b.y * b.bh + b.oy;
+    z = b.z;
     return x < nx && y < ny;
+}
+__device__ __forceinline__ bool cell_coords(int nx, int ny, int& x, int& y, int& z) {
+    return cell_coords(hw_blk(), nx, ny, x, y, z);
 }
 // Face kernels: blockIdx.z runs over (axis, z) for the three face grids, each
 // padded to the (nx+1, ny+1, nz+1) box.

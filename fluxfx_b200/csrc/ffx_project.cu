@@ -12,6 +12,7 @@
 // ffx_common.cuh; reductions stride over z with a bounded number of blocks so
 // each block issues one atomic.
 #include "ffx_host.cuh"
+#include "ffx_batch.cuh"
 #include "ffx_level0.cuh"
 
 namespace ffx {
@@ -66,11 +67,22 @@ __global__ void __launch_bounds__(256) walls_div_kernel(Dev d, const uint8_t* __
 }
 
 // Plain divergence of stored faces (pressure_divergence.glsl).
+template <typename T>
+struct DivDesc {
+    Dev d;
+    const uint8_t* solid;
+    Faces<T> F;
+    float* div;
+};
+
 template <typename T, bool MASK>
-__global__ void __launch_bounds__(256) divergence_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
-                                                        float* div) {
+__device__ __forceinline__ void divergence_body(const DivDesc<T>& P, const Blk& b) {
+    const Dev& d = P.d;
+    const uint8_t* __restrict__ solid = P.solid;
+    const Faces<T>& F = P.F;
+    float* div = P.div;
     int x, y, z;
-    if (!cell_coords(d.nx, d.ny, x, y, z)) return;
+    if (!cell_coords(b, d.nx, d.ny, x, y, z)) return;
     const int i = cidx(d, x, y, z);
     if (MASK && __ldg(solid + i)) { div[i] = 0.f; return; }
     const int iu = x + (d.nx + 1) * (y + d.ny * z);
@@ -81,14 +93,40 @@ __global__ void __launch_bounds__(256) divergence_kernel(Dev d, const uint8_t* _
              (Store<T>::ld(F.w, i + sz) - Store<T>::ld(F.w, i)) * d.inv[2];
 }
 
-// ------------------------------------------------- gradient + divergence
 template <typename T, bool MASK>
-__global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Walls W,
-                                                      Faces<T> F, const float* __restrict__ p, float dt, T* ou,
-                                                      T* ov, T* ow, float* div, float* maxima) {
+__global__ void __launch_bounds__(256) divergence_kernel(Dev d, const uint8_t* __restrict__ solid, Faces<T> F,
+                                                        float* div) {
+    divergence_body<T, MASK>(DivDesc<T>{d, solid, F, div}, hw_blk());
+}
+
+// ------------------------------------------------- gradient + divergence
+template <typename T>
+struct GradDesc {
+    Dev d;
+    const uint8_t* solid;
+    Walls W;
+    Faces<T> F;
+    const float* p;
+    float dt;
+    T* out[3];
+    float* div;
+};
+
+template <typename T, bool MASK>
+__device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b, float* maxima) {
+    const Dev& d = P.d;
+    const uint8_t* __restrict__ solid = P.solid;
+    const Walls& W = P.W;
+    const Faces<T>& F = P.F;
+    const float* __restrict__ p = P.p;
+    const float dt = P.dt;
+    T* ou = P.out[0];
+    T* ov = P.out[1];
+    T* ow = P.out[2];
+    float* div = P.div;
     int x, y, z;
     float mx[3] = {0.f, 0.f, 0.f};
-    if (cell_coords(d.nx, d.ny, x, y, z)) {
+    if (cell_coords(b, d.nx, d.ny, x, y, z)) {
         const int i = cidx(d, x, y, z);
         const int iu = x + (d.nx + 1) * (y + d.ny * z);
         const int iv = x + d.nx * (y + (d.ny + 1) * z);
@@ -132,6 +170,13 @@ __global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __r
             __syncthreads();
         }
     }
+}
+
+template <typename T, bool MASK>
+__global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Walls W,
+                                                      Faces<T> F, const float* __restrict__ p, float dt, T* ou,
+                                                      T* ov, T* ow, float* div, float* maxima) {
+    gradient_body<T, MASK>(GradDesc<T>{d, solid, W, F, p, dt, {ou, ov, ow}, div}, hw_blk(), maxima);
 }
 
 // ---------------------------------------------------------------- Jacobi
@@ -382,14 +427,20 @@ __device__ __forceinline__ void graph_terms(const GLvl& g, int i, int x, int y, 
     }
 }
 
-__global__ void __launch_bounds__(256) graph_smooth_kernel(GLvl g, const float* __restrict__ p,
-                                                          const float* __restrict__ rhs, float omega, float* out) {
+__device__ __forceinline__ void graph_smooth_body(const GLvl& g, const float* __restrict__ p,
+                                                  const float* __restrict__ rhs, float omega, float* out,
+                                                  const Blk& b) {
     int x, y, z;
-    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    if (!cell_coords(b, g.nx, g.ny, x, y, z)) return;
     const int i = x + g.nx * (y + g.ny * z);
     float diag, nb;
     graph_terms(g, i, x, y, z, [&](int j, int, int, int) { return __ldg(p + j); }, diag, nb);
     out[i] = diag > 0.f ? __ldg(p + i) * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
+}
+
+__global__ void __launch_bounds__(256) graph_smooth_kernel(GLvl g, const float* __restrict__ p,
+                                                          const float* __restrict__ rhs, float omega, float* out) {
+    graph_smooth_body(g, p, rhs, omega, out, hw_blk());
 }
 
 // Level-0 (mask-derived) sweep, streamed along z: each thread owns one (x, y)
@@ -470,23 +521,29 @@ __global__ void __launch_bounds__(256) graph_residual_kernel(GLvl g, const float
     r[i] = graph_res(g, p, rhs, i, x, y, z);
 }
 
-__global__ void __launch_bounds__(256) graph_residual_max_kernel(GLvl g, const float* __restrict__ p,
-                                                                const float* __restrict__ rhs, float* out) {
-    int x = blockIdx.x * kBX + threadIdx.x, y = blockIdx.y * kBY + threadIdx.y;
+__device__ __forceinline__ void graph_residual_max_body(const GLvl& g, const float* __restrict__ p,
+                                                        const float* __restrict__ rhs, float* out, const Blk& b) {
+    int x = b.x * b.bw + b.ox, y = b.y * b.bh + b.oy;
     float m = 0.f;
     if (x < g.nx && y < g.ny)
-        for (int z = blockIdx.z; z < g.nz; z += gridDim.z) {
+        for (int z = b.z; z < g.nz; z += b.gz) {
             const int i = x + g.nx * (y + g.ny * z);
             m = fmaxf(m, finite_abs(graph_res(g, p, rhs, i, x, y, z)));
         }
     block_max_to(out, m);
 }
 
-__global__ void __launch_bounds__(256) graph_residual_restrict_kernel(GLvl g, const float* __restrict__ p,
-                                                                     const float* __restrict__ rhs, float* c) {
+__global__ void __launch_bounds__(256) graph_residual_max_kernel(GLvl g, const float* __restrict__ p,
+                                                                const float* __restrict__ rhs, float* out) {
+    graph_residual_max_body(g, p, rhs, out, hw_blk());
+}
+
+__device__ __forceinline__ void graph_residual_restrict_body(const GLvl& g, const float* __restrict__ p,
+                                                             const float* __restrict__ rhs, float* c,
+                                                             float* zero, const Blk& b) {
     const int cx = g.nx / 2, cy = g.ny / 2;
     int x, y, z;
-    if (!cell_coords(cx, cy, x, y, z)) return;
+    if (!cell_coords(b, cx, cy, x, y, z)) return;
     float v = 0.f;
 #pragma unroll
     for (int dz = 0; dz < 2; ++dz)
@@ -498,6 +555,12 @@ __global__ void __launch_bounds__(256) graph_residual_restrict_kernel(GLvl g, co
                 v = v + graph_res(g, p, rhs, X + g.nx * (Y + g.ny * Z), X, Y, Z);
             }
     c[x + cx * (y + cy * z)] = v / 8.0f;
+    if (zero) zero[x + cx * (y + cy * z)] = 0.f;
+}
+
+__global__ void __launch_bounds__(256) graph_residual_restrict_kernel(GLvl g, const float* __restrict__ p,
+                                                                     const float* __restrict__ rhs, float* c) {
+    graph_residual_restrict_body(g, p, rhs, c, nullptr, hw_blk());
 }
 
 __device__ __forceinline__ bool g_active(const GLvl& g, int i) {
@@ -520,18 +583,25 @@ __global__ void __launch_bounds__(256) graph_prolong_kernel(GLvl g, const float*
     out[i] = prolonged(g, p, coarse, i, x, y, z);
 }
 
-__global__ void __launch_bounds__(256) graph_prolong_smooth_kernel(GLvl g, const float* __restrict__ p,
-                                                                  const float* __restrict__ coarse,
-                                                                  const float* __restrict__ rhs, float omega,
-                                                                  float* out) {
+__device__ __forceinline__ void graph_prolong_smooth_body(const GLvl& g, const float* __restrict__ p,
+                                                          const float* __restrict__ coarse,
+                                                          const float* __restrict__ rhs, float omega, float* out,
+                                                          const Blk& b) {
     int x, y, z;
-    if (!cell_coords(g.nx, g.ny, x, y, z)) return;
+    if (!cell_coords(b, g.nx, g.ny, x, y, z)) return;
     const int i = x + g.nx * (y + g.ny * z);
     float diag, nb;
     graph_terms(g, i, x, y, z,
                 [&](int j, int jx, int jy, int jz) { return prolonged(g, p, coarse, j, jx, jy, jz); }, diag, nb);
     float pc = prolonged(g, p, coarse, i, x, y, z);
     out[i] = diag > 0.f ? pc * (1.f - omega) + ((nb - __ldg(rhs + i)) / diag) * omega : 0.f;
+}
+
+__global__ void __launch_bounds__(256) graph_prolong_smooth_kernel(GLvl g, const float* __restrict__ p,
+                                                                  const float* __restrict__ coarse,
+                                                                  const float* __restrict__ rhs, float omega,
+                                                                  float* out) {
+    graph_prolong_smooth_body(g, p, coarse, rhs, omega, out, hw_blk());
 }
 
 // physics/solid_hierarchy.py:27-53 for one coarse cell.
@@ -635,7 +705,7 @@ __device__ __forceinline__ float tail_res(const TailLvl& L, const float* p, int 
     return diag > 0.f ? (L.rhs[i] - nb) + diag * p[i] : 0.f;
 }
 
-__global__ void __launch_bounds__(kTailThreads) graph_tail_kernel(const __grid_constant__ TailArgs A) {
+__device__ __forceinline__ void graph_tail_body(const TailArgs& A) {
     float* cur[FFX_TAIL_LEVELS];
     float* spare[FFX_TAIL_LEVELS];
     for (int k = 0; k < A.count; ++k) {
@@ -719,6 +789,10 @@ __global__ void __launch_bounds__(kTailThreads) graph_tail_kernel(const __grid_c
             float* u = cur[k]; cur[k] = spare[k]; spare[k] = u;
         }
     }
+}
+
+__global__ void __launch_bounds__(kTailThreads) graph_tail_kernel(const __grid_constant__ TailArgs A) {
+    graph_tail_body(A);
 }
 
 // ------------------------------------------ Krylov acceleration (MG-PCG)
@@ -1228,3 +1302,261 @@ int ffx_dot(int64_t count, const float* a, const float* b, double scale, double*
 }
 
 }  // extern "C"
+
+// ----------------------------------------------------------- batched passes
+// Persistent launches over the tiles of many domains (ffx_batch.cuh) running
+// the bodies of the single-domain kernels above on the collider path.
+namespace ffx {
+namespace {
+
+constexpr float kOmega = (float)(2.0 / 3.0);   // the weighted-Jacobi factor the host passes
+
+struct ScaleDesc {        // max |rhs| into the state, iterate zeroed
+    int n;
+    const float* rhs;
+    float* p;
+};
+struct GDesc {            // one multigrid level
+    GLvl g;
+    const float* p;
+    float* q;
+    const float* rhs;
+    float* coarse;
+    float* zero;
+};
+struct DirectDesc {
+    int n;
+    const double* inverse;
+    const float* rhs;
+    float* p;
+};
+
+__global__ void __launch_bounds__(kBatchThreads) batch_divergence_kernel(const __grid_constant__ BatchMap M,
+                                                                         const DivDesc<float>* descs,
+                                                                         const BatchState* state) {
+    for_tiles(M, descs, state, false, NoPrep{},
+              [](const DivDesc<float>& P, const Blk& b, int) { divergence_body<float, true>(P, b); });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_scale_kernel(const __grid_constant__ BatchMap M,
+                                                                    const ScaleDesc* descs, BatchState* state) {
+    for_tiles(M, descs, state, false, NoPrep{}, [state](const ScaleDesc& P, const Blk& b, int slot) {
+        const int i = b.x * kBatchThreads + (int)threadIdx.x;
+        float v = 0.f;
+        if (i < P.n) {
+            v = finite_abs(__ldg(P.rhs + i));
+            P.p[i] = 0.f;
+        }
+        block_max_to(&state[slot].scale, v);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_gradient_kernel(const __grid_constant__ BatchMap M,
+                                                                       const GradDesc<float>* descs,
+                                                                       BatchState* state) {
+    for_tiles(M, descs, state, false, NoPrep{}, [state](const GradDesc<float>& P, const Blk& b, int slot) {
+        gradient_body<float, true>(P, b, state[slot].maxima);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_residual_max_kernel(const __grid_constant__ BatchMap M,
+                                                                           const GDesc* descs, BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [state](const GDesc& P, const Blk& b, int slot) {
+        graph_residual_max_body(P.g, P.p, P.rhs, &state[slot].res, b);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_smooth_kernel(const __grid_constant__ BatchMap M,
+                                                                     const GDesc* descs, const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{},
+              [](const GDesc& P, const Blk& b, int) { graph_smooth_body(P.g, P.p, P.rhs, kOmega, P.q, b); });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_residual_restrict_kernel(const __grid_constant__ BatchMap M,
+                                                                                const GDesc* descs,
+                                                                                const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [](const GDesc& P, const Blk& b, int) {
+        graph_residual_restrict_body(P.g, P.p, P.rhs, P.coarse, P.zero, b);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_prolong_smooth_kernel(const __grid_constant__ BatchMap M,
+                                                                             const GDesc* descs,
+                                                                             const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [](const GDesc& P, const Blk& b, int) {
+        graph_prolong_smooth_body(P.g, P.p, P.coarse, P.rhs, kOmega, P.q, b);
+    });
+}
+
+// direct_kernel's rows, eight per tile (one warp each).
+__global__ void __launch_bounds__(kBatchThreads) batch_direct_kernel(const __grid_constant__ BatchMap M,
+                                                                     const DirectDesc* descs,
+                                                                     const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [](const DirectDesc& P, const Blk& b, int) {
+        const int row = b.x * (kBatchThreads / 32) + (int)(threadIdx.x >> 5), lane = threadIdx.x & 31;
+        if (row >= P.n) return;
+        const double* r = P.inverse + (int64_t)row * P.n;
+        double s = 0.0;
+        for (int j = lane; j < P.n; j += 32) s += r[j] * (double)P.rhs[j];
+        for (int o = 16; o > 0; o >>= 1) s += __shfl_down_sync(0xffffffffu, s, o);
+        if (lane == 0) P.p[row] = (float)(s / (double)1.0f);
+    });
+}
+
+// One 1024-thread block per domain with a tail.
+__global__ void __launch_bounds__(kTailThreads) batch_tail_kernel(const __grid_constant__ BatchMap M,
+                                                                  const TailArgs* descs, const BatchState* state) {
+    __shared__ __align__(16) unsigned char raw[sizeof(TailArgs)];
+    const int k = blockIdx.x;
+    if (k >= M.count || state[M.dom[k]].done) return;
+    const int* src = reinterpret_cast<const int*>(descs + k);
+    int* dst = reinterpret_cast<int*>(raw);
+    for (int i = threadIdx.x; i < (int)(sizeof(TailArgs) / sizeof(int)); i += blockDim.x) dst[i] = __ldg(src + i);
+    __syncthreads();
+    graph_tail_body(*reinterpret_cast<const TailArgs*>(raw));
+}
+
+template <class K>
+int occupancy_of(K kernel) {
+    int n = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBatchThreads, 0) != cudaSuccess) return 1;
+    return n > 0 ? n : 1;
+}
+
+unsigned persistent(const BatchMap& M, int grid) {
+    return (unsigned)(grid > 0 && grid < M.total ? grid : M.total);
+}
+
+GLvl batch_glvl(const FfxGraphLevel& lv) { return make_glvl(&lv); }
+
+}  // namespace
+
+namespace batch {
+
+size_t divergence_desc(const FfxBatchDomain& D, void* out) {
+    if (out) {
+        DivDesc<float> P = {make_dev(D.grid), D.solid, {D.bu, D.bv, D.bw}, D.level[0].rhs};
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(DivDesc<float>);
+}
+
+size_t scale_zero_desc(const FfxBatchDomain& D, void* out) {
+    if (out) {
+        ScaleDesc P = {D.grid.nx * D.grid.ny * D.grid.nz, D.level[0].rhs, D.level[0].p};
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(ScaleDesc);
+}
+
+size_t gradient_desc(const FfxBatchDomain& D, float* u, float* v, float* w, void* out) {
+    if (out) {
+        GradDesc<float> P;
+        memset(&P, 0, sizeof P);
+        P.d = make_dev(D.grid);
+        P.solid = D.solid;
+        P.W = make_walls(nullptr);
+        P.F = {D.bu, D.bv, D.bw};
+        P.p = D.level[0].p;
+        P.dt = 1.0f;   // impulse form: the solve used dt = 1
+        P.out[0] = u; P.out[1] = v; P.out[2] = w;
+        P.div = D.after;
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(GradDesc<float>);
+}
+
+size_t level_desc(const FfxGraphLevel& lv, const float* p, float* q, const float* rhs, float* coarse, float* zero,
+                  void* out) {
+    if (out) {
+        GDesc P = {batch_glvl(lv), p, q, rhs, coarse, zero};
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(GDesc);
+}
+
+size_t tail_desc(const FfxBatchDomain& D, int pre, int post, void* out) {
+    if (out) {
+        TailArgs A;
+        memset(&A, 0, sizeof A);
+        const int start = D.tail_start;
+        A.count = D.levels - start;
+        A.pre = pre;
+        A.post = post;
+        A.omega = kOmega;
+        A.inverse = D.inverse;
+        for (int k = 0; k < A.count; ++k) {
+            const FfxBatchLevel& L = D.level[start + k];
+            A.lv[k].g = batch_glvl(L.level);
+            A.lv[k].p = L.p;
+            A.lv[k].q = L.q;
+            A.lv[k].rhs = L.rhs;
+            A.lv[k].n = L.level.nx * L.level.ny * L.level.nz;
+        }
+        memcpy(out, &A, sizeof A);
+    }
+    return sizeof(TailArgs);
+}
+
+size_t direct_desc(const FfxBatchDomain& D, float* p, void* out) {
+    if (out) {
+        const FfxBatchLevel& L = D.level[D.levels - 1];
+        DirectDesc P = {L.level.nx * L.level.ny * L.level.nz, D.inverse, L.rhs, p};
+        memcpy(out, &P, sizeof P);
+    }
+    return sizeof(DirectDesc);
+}
+
+cudaError_t divergence(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_divergence_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const DivDesc<float>*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t scale_zero(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_scale_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const ScaleDesc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t gradient(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_gradient_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const GradDesc<float>*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t residual_max(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_residual_max_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const GDesc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_smooth_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const GDesc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t residual_restrict(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_residual_restrict_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const GDesc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t prolong_smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_prolong_smooth_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const GDesc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t direct(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_direct_kernel<<<persistent(M, grid), kBatchThreads, 0, st>>>(M, (const DirectDesc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t tail(const BatchMap& M, const void* descs, BatchState* state, cudaStream_t st) {
+    batch_tail_kernel<<<(unsigned)M.count, kTailThreads, 0, st>>>(M, (const TailArgs*)descs, state);
+    return cudaGetLastError();
+}
+
+int project_resident_blocks(int kind) {
+    switch (kind) {
+        case kDivergence: return occupancy_of(batch_divergence_kernel);
+        case kScaleZero: return occupancy_of(batch_scale_kernel);
+        case kGradient: return occupancy_of(batch_gradient_kernel);
+        case kResidualMax: return occupancy_of(batch_residual_max_kernel);
+        case kSmooth: return occupancy_of(batch_smooth_kernel);
+        case kResidualRestrict: return occupancy_of(batch_residual_restrict_kernel);
+        case kProlongSmooth: return occupancy_of(batch_prolong_smooth_kernel);
+        case kDirect: return occupancy_of(batch_direct_kernel);
+        default: return 0;
+    }
+}
+
+}  // namespace batch
+}  // namespace ffx

@@ -396,6 +396,90 @@ int ffx_moving_remap(const FfxGrid* g, int storage, const uint8_t* owners,
                      void* u, void* v, void* w, const float* wu, const float* wv,
                      const float* ww, void* stream);
 
+/* ------------------------------------------------ batched domains (a19) */
+/* No counterpart in the reference (it runs one domain per solver object): many
+ * independent FP32 collider-path smoke domains of uneven sizes advance
+ * together, one persistent launch per pass over all of them. Each domain
+ * follows exactly the single-domain step of backend/projected.py:149-202 with
+ * static colliders, MacCormack (or semi-Lagrangian) transport, buoyancy,
+ * table emitters, the aggregation multigrid of backend/solid_multigrid.py:46-76
+ * run as stand-alone V-cycles until max|rhs - L p| <= tolerance * max|rhs|
+ * (pressure from zero every step), and the time step
+ * dt = min(dt_max, cfl * cell / max|u|) computed on the device from the
+ * projection's velocity maxima. Results are bit-identical to running each
+ * domain alone through the single-domain entry points. */
+#define FFX_BATCH_MAX 64
+#define FFX_BATCH_LEVELS 8
+typedef struct FfxBatchLevel {
+    FfxGraphLevel level;   /* level 0: edges NULL, solid = the collider mask */
+    float* p;              /* iterate (level 0: the pressure) */
+    float* q;              /* sweep partner (level 0: the spare pressure) */
+    float* rhs;            /* right-hand side (level 0: the divergence) */
+} FfxBatchLevel;
+typedef struct FfxBatchDomain {
+    FfxGrid grid;
+    const uint8_t* solid;  /* collider mask (all zero for a domain without colliders) */
+    const uint8_t* halo;   /* its dilation (ffx_dilate_mask) */
+    float* u; float* v; float* w;      /* velocity faces, updated in place every step */
+    float* pu; float* pv; float* pw;   /* face predictor scratch */
+    float* bu; float* bv; float* bw;   /* walled (bounded) faces scratch */
+    float* density[2];                 /* [front, back]: front holds the field before an even step */
+    float* temperature[2];
+    float* predictor[2];               /* scalar MacCormack predictor scratch (density, temperature) */
+    float* reverse[2];
+    float* after;                      /* divergence after the projection */
+    FfxSources sources;                /* emitter table (count 0..8) or single emitter (count < 0) */
+    int32_t velocity_corrected, scalar_corrected;   /* MacCormack (1) or semi-Lagrangian (0) */
+    float blend, lift, weight;
+    FfxScalarChannel density_channel;  /* rate, decay, target, channel, table_target (pointers unused) */
+    FfxScalarChannel heat_channel;
+    double cell, cfl, dt_max;          /* time step rule */
+    float dt0;                         /* time step of the first step */
+    int32_t levels;                    /* multigrid hierarchy, finest first */
+    FfxBatchLevel level[FFX_BATCH_LEVELS];
+    int32_t tail_start;                /* first level run by the single-block tail, or -1 */
+    const double* inverse;             /* FP64 pseudoinverse of the coarsest level, or NULL */
+    int32_t pre, post, max_cycles;     /* sweeps per V-cycle (both >= 1), cycle cap per solve */
+    double tolerance;                  /* relative max-norm residual target (> 0) */
+} FfxBatchDomain;
+typedef struct FfxBatchStats {
+    float dt, last_dt;                 /* dt of the next step, of the last step */
+    int32_t last_cycles, total_cycles, steps;
+    float maxima[3];
+    double time;
+} FfxBatchStats;
+typedef struct FfxBatchPlan FfxBatchPlan;
+/* Device bytes the plan of these domains needs (descriptors and state). */
+int ffx_batch_workspace_bytes(const FfxBatchDomain* domains, int32_t count, int64_t* bytes);
+/* Build a plan in the caller's device workspace (synchronous upload). */
+int ffx_batch_create(const FfxBatchDomain* domains, int32_t count, void* workspace, int64_t bytes,
+                     FfxBatchPlan** plan);
+/* Pass kinds of a batched step (the autotuner's keys). */
+enum {
+    FFX_PASS_PREDICTOR = 0, FFX_PASS_VELOCITY, FFX_PASS_DIVERGENCE, FFX_PASS_SCALE, FFX_PASS_GRADIENT,
+    FFX_PASS_SCALAR_PREDICTOR, FFX_PASS_SCALAR_REVERSE, FFX_PASS_SCALAR_FINAL, FFX_PASS_RESIDUAL_MAX,
+    FFX_PASS_SMOOTH, FFX_PASS_RESIDUAL_RESTRICT, FFX_PASS_PROLONG_SMOOTH, FFX_PASS_DIRECT, FFX_PASS_KINDS
+};
+/* Tile shape (0: 32x8, 1: 64x4, 2: 128x2, 3: 16x16 threads) and persistent grid
+ * (0: one block per tile; m >= 1: m x the resident blocks of the GPU) of one
+ * pass kind. Takes effect for graphs captured afterwards. */
+int ffx_batch_set_config(FfxBatchPlan* plan, int32_t kind, int32_t shape, int32_t grid);
+/* Launch one pass kind alone over the plan's buffers (autotuning; the pass only
+ * writes scratch fields that the step recomputes, the gradient pass writes the
+ * predictor faces instead of the velocity). */
+int ffx_batch_tune_pass(FfxBatchPlan* plan, int32_t kind, void* stream);
+/* Capture `steps` steps (starting from the plan's current parity) into an
+ * instantiated CUDA graph with one conditional WHILE node per solve. */
+int ffx_batch_graph(FfxBatchPlan* plan, int32_t steps, void** graph_exec);
+/* Launch such a graph; advances the plan's parity by its step count. */
+int ffx_batch_launch(FfxBatchPlan* plan, void* graph_exec, int32_t steps, void* stream);
+int ffx_batch_graph_free(void* graph_exec);
+/* Host copy of every domain's FfxBatchStats (synchronises `stream`). */
+int ffx_batch_stats(const FfxBatchPlan* plan, FfxBatchStats* out, void* stream);
+/* Current parity: 0 = density[0]/temperature[0] hold the fields. */
+int ffx_batch_parity(const FfxBatchPlan* plan);
+int ffx_batch_destroy(FfxBatchPlan* plan);
+
 /* ------------------------------------------------- learned warm start (a18) */
 /* No counterpart in the reference: a 3D U-Net predicts the pressure from the
  * divergence and the collider mask. Activations are NDHWC bfloat16 addressed
