@@ -112,7 +112,7 @@ class FfxBatchDomain(C.Structure):
 
 class FfxBatchStats(C.Structure):
     _fields_ = [('dt', f32), ('last_dt', f32), ('last_cycles', i32), ('total_cycles', i32), ('steps', i32),
-                ('maxima', f3), ('time', C.c_double)]
+                ('maxima', f3), ('time', C.c_double), ('loop_iterations', i64)]
 
 
 P = C.POINTER
@@ -151,6 +151,7 @@ _PROTOTYPES = {
     'ffx_graph_smooth': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp]),
     'ffx_graph_residual': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
     'ffx_graph_residual_restrict': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
+    'ffx_graph_residual_restrict_zero': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp, vp]),
     'ffx_graph_prolong': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
     'ffx_graph_prolong_smooth': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, f32, vp, vp]),
     'ffx_graph_residual_max': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),

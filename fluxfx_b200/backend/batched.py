@@ -162,7 +162,8 @@ class BatchedSmoke:
         out = (N.FfxBatchStats * len(self.solvers))()
         N.check(self.lib.ffx_batch_stats(self.plan, out, self.stream))
         return [dict(dt=o.dt, last_dt=o.last_dt, last_cycles=o.last_cycles, total_cycles=o.total_cycles,
-                     steps=o.steps, maxima=tuple(o.maxima), time=o.time) for o in out]
+                     steps=o.steps, maxima=tuple(o.maxima), time=o.time, loop_iterations=o.loop_iterations)
+                for o in out]
 
     def fields(self, i):
         """(density, temperature, (u, v, w)) tensors of domain ``i`` now."""

@@ -199,14 +199,16 @@ class SolidMultigridProjector(SolidPressureProjector):
                 level['p'].zero_()
         self.smooth(level, pre)
         coarse = self.levels[index + 1]
-        dev.call('ffx_graph_residual_restrict', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
-                 ptr(coarse['rhs']), dev.s)
-        if self.use_tail and index + 1 == self.tail_start:
-            # every level below runs inside one launch (it zeroes coarse p itself)
+        tail = self.use_tail and index + 1 == self.tail_start
+        # the coarse iterate starts from zero: the restriction pass clears it
+        # (the tail clears its own levels)
+        dev.call('ffx_graph_residual_restrict_zero', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                 ptr(coarse['rhs']), None if tail else ptr(coarse['p']), dev.s)
+        if tail:
+            # every level below runs inside one launch
             dev.call('ffx_graph_tail', C.byref(self._tail), dev.s)
             self.last_iterations += self._tail_sweeps()
         else:
-            coarse['p'].zero_()
             self.cycle(index + 1)
         if self.post_sweeps == 1 and dot is not None:
             dev.call('ffx_graph_prolong_smooth_dot', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),

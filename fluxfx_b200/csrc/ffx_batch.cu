@@ -28,7 +28,7 @@ struct FfxBatchPlan {
     ffx::BatchState* state = nullptr;
     struct Solve { double tol; int max_cycles; int pad; }* solve = nullptr;
     const void* rules = nullptr;
-    struct Guard { int iterations; int tripped; }* guard = nullptr;   // solve-loop bound (device)
+    struct Guard { int iterations; int tripped; long long total; }* guard = nullptr;   // solve-loop bound (device)
     struct Entry { int slot, X, Y, Z; };
     struct Launch {
         int kind;             // ffx::BatchKind, or kTail
@@ -58,7 +58,10 @@ constexpr int kLoopCap = 300;
 __global__ void batch_decide_kernel(BatchState* state, const FfxBatchPlan::Solve* solve, int count,
                                     FfxBatchPlan::Guard* guard, cudaGraphConditionalHandle handle) {
     __shared__ int iteration;
-    if (threadIdx.x == 0) iteration = ++guard->iterations;
+    if (threadIdx.x == 0) {
+        iteration = ++guard->iterations;
+        guard->total += 1;
+    }
     __syncthreads();
     int open = 0;
     for (int d = threadIdx.x; d < count; d += blockDim.x) {
@@ -668,7 +671,7 @@ int ffx_batch_graph_free(void* graph_exec) {
 int ffx_batch_stats(const FfxBatchPlan* plan, FfxBatchStats* out, void* stream) {
     FFX_REQUIRE(plan && out, "ffx_batch_stats: invalid arguments");
     std::vector<BatchState> S(plan->count);
-    FfxBatchPlan::Guard G = {0, 0};
+    FfxBatchPlan::Guard G = {0, 0, 0};
     cudaStream_t st = as_stream(stream);
     int rc = cuda_status(cudaMemcpyAsync(S.data(), plan->state, sizeof(BatchState) * plan->count,
                                          cudaMemcpyDeviceToHost, st), "ffx_batch_stats: copy");
@@ -684,6 +687,7 @@ int ffx_batch_stats(const FfxBatchPlan* plan, FfxBatchStats* out, void* stream) 
         out[d].steps = S[d].steps;
         for (int a = 0; a < 3; ++a) out[d].maxima[a] = S[d].last_maxima[a];
         out[d].time = S[d].time;
+        out[d].loop_iterations = G.total;
     }
     if (G.tripped) return fail(FFX_ERR_TIMEOUT, "ffx_batch_stats: a solve loop reached %d iterations", kLoopCap);
     return FFX_OK;

@@ -279,7 +279,8 @@ __global__ void __launch_bounds__(256) level0_smooth_zero_kernel(L0 g, const flo
 // the scalar kernel's order (dz, then dy, then dx) and divides by 8.
 __global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0 g, const float* __restrict__ p,
                                                                              const float* __restrict__ rhs,
-                                                                             float* __restrict__ coarse) {
+                                                                             float* __restrict__ coarse,
+                                                                             float* __restrict__ zero) {
     const int lane = threadIdx.x;
     const int x4 = blockIdx.x * 32 + lane, ya = 2 * (blockIdx.y * kRows + threadIdx.y), yb = ya + 1;
     const bool active = x4 < g.nx4 && ya < g.ny;
@@ -332,9 +333,11 @@ __global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0
             }
             v0 = v0 + res_a[0]; v0 = v0 + res_a[1]; v0 = v0 + res_b[0]; v0 = v0 + res_b[1];
             v1 = v1 + res_a[2]; v1 = v1 + res_a[3]; v1 = v1 + res_b[2]; v1 = v1 + res_b[3];
-            if (z & 1)
-                reinterpret_cast<float2*>(coarse)[x4 + g.nx4 * ((ya >> 1) + (g.ny >> 1) * (z >> 1))] =
-                    make_float2(v0 / 8.0f, v1 / 8.0f);
+            if (z & 1) {
+                const int c2 = x4 + g.nx4 * ((ya >> 1) + (g.ny >> 1) * (z >> 1));
+                reinterpret_cast<float2*>(coarse)[c2] = make_float2(v0 / 8.0f, v1 / 8.0f);
+                if (zero) reinterpret_cast<float2*>(zero)[c2] = make_float2(0.f, 0.f);
+            }
         }
         lo_a = c_a; c_a = hi_a;
         lo_b = c_b; c_b = hi_b;
@@ -436,11 +439,11 @@ int level0_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega, f
 }
 
 int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse,
-                             cudaStream_t st) {
+                             float* zero, cudaStream_t st) {
     const L0 g = make_l0(lv);
     const dim3 grid((unsigned)((g.nx4 + 31) / 32), (unsigned)((g.ny / 2 + kRows - 1) / kRows),
                     (unsigned)((g.nz + kZ4 - 1) / kZ4));
-    level0_residual_restrict_kernel<<<grid, dim3(32, kRows), 0, st>>>(g, p, rhs, coarse);
+    level0_residual_restrict_kernel<<<grid, dim3(32, kRows), 0, st>>>(g, p, rhs, coarse, zero);
     return launch_status("level0_residual_restrict_kernel");
 }
 

@@ -24,7 +24,7 @@ int level0_prolong_smooth_dot(const FfxGraphLevel* lv, const float* p, const flo
 int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st);
 int level0_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, cudaStream_t st);
 int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse,
-                             cudaStream_t st);
+                             float* zero, cudaStream_t st);
 int level0_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old, const double* rz_new,
                            const double* rz_old, float* p_out, float* q, double* pq, cudaStream_t st);
 int level0_links(int nx, int ny, int nz, const uint8_t* solid, uint8_t* links, cudaStream_t st);

@@ -558,9 +558,10 @@ __device__ __forceinline__ void graph_residual_restrict_body(const GLvl& g, cons
     if (zero) zero[x + cx * (y + cy * z)] = 0.f;
 }
 
-__global__ void __launch_bounds__(256) graph_residual_restrict_kernel(GLvl g, const float* __restrict__ p,
-                                                                     const float* __restrict__ rhs, float* c) {
-    graph_residual_restrict_body(g, p, rhs, c, nullptr, hw_blk());
+__global__ void __launch_bounds__(256) graph_residual_restrict_zero_kernel(GLvl g, const float* __restrict__ p,
+                                                                          const float* __restrict__ rhs, float* c,
+                                                                          float* zero) {
+    graph_residual_restrict_body(g, p, rhs, c, zero, hw_blk());
 }
 
 __device__ __forceinline__ bool g_active(const GLvl& g, int i) {
@@ -1104,16 +1105,22 @@ int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs
     return launch_status("graph_residual_kernel");
 }
 
-int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse_rhs,
-                                void* stream) {
+int ffx_graph_residual_restrict_zero(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse_rhs,
+                                     float* coarse_p, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && coarse_rhs && lv->nx % 2 == 0 && lv->ny % 2 == 0 && lv->nz % 2 == 0,
                 "ffx_graph_residual_restrict: invalid arguments");
-    if (level0_x4(lv, {p, rhs}) && ((uintptr_t)coarse_rhs & 7) == 0)
-        return level0_residual_restrict(lv, p, rhs, coarse_rhs, as_stream(stream));
+    FFX_REQUIRE(coarse_p != coarse_rhs || !coarse_p, "ffx_graph_residual_restrict: coarse iterate aliases its rhs");
+    if (level0_x4(lv, {p, rhs}) && ((uintptr_t)coarse_rhs & 7) == 0 && ((uintptr_t)coarse_p & 7) == 0)
+        return level0_residual_restrict(lv, p, rhs, coarse_rhs, coarse_p, as_stream(stream));
     GLvl g = make_glvl(lv);
-    graph_residual_restrict_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0, as_stream(stream)>>>(
-        g, p, rhs, coarse_rhs);
+    graph_residual_restrict_zero_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0,
+                                          as_stream(stream)>>>(g, p, rhs, coarse_rhs, coarse_p);
     return launch_status("graph_residual_restrict_kernel");
+}
+
+int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse_rhs,
+                                void* stream) {
+    return ffx_graph_residual_restrict_zero(lv, p, rhs, coarse_rhs, nullptr, stream);
 }
 
 int ffx_graph_prolong(const FfxGraphLevel* lv, const float* p, const float* coarse, float* p_out, void* stream) {

@@ -286,3 +286,64 @@ class UNet:
             l.w.copy_(w.to(l.w.device))
             l.b.copy_(b.to(l.b.device))
             l.w16.copy_(l.w.to(torch.bfloat16))
+
+    def forward_flops(self, batch, dims):
+        """Multiply-add FLOPs (2 per MAC) of one forward pass."""
+        D, H, W = dims
+        total = 0
+        level_of = {'e0a': 0, 'e0b': 0, 'd0': 1, 'e1a': 1, 'e1b': 1, 'd1': 2, 'e2a': 2, 'e2b': 2, 'd2': 3, 'e3a': 3,
+                    'e3b': 3, 'u2': 2, 'c2a': 2, 'c2b': 2, 'u1': 1, 'c1a': 1, 'c1b': 1, 'u0': 0, 'c0a': 0, 'c0b': 0,
+                    'head': 0}
+        for l in self.layers:
+            out_vox = batch * (D >> level_of[l.name]) * (H >> level_of[l.name]) * (W >> level_of[l.name])
+            per = l.cin * l.cout * (l.taps if l.kind != 'up' else 1)   # a transposed 2^3 tap feeds one output
+            total += 2 * per * out_vox
+        return total
+
+
+def main():
+    """Time the forward pass and a training step on synthetic input:
+    python -m fluxfx_b200.learned.unet --size 128 --batch 1 --repeat 5"""
+    import argparse
+    import json
+    ap = argparse.ArgumentParser(description='U-Net timing on synthetic input')
+    ap.add_argument('--size', type=int, default=128)
+    ap.add_argument('--batch', type=int, default=1)
+    ap.add_argument('--repeat', type=int, default=5)
+    ap.add_argument('--train', action='store_true', help='also time forward + backward + Adam')
+    args = ap.parse_args()
+    dev = torch.device('cuda')
+    net = UNet(dev, seed=0)
+    g = torch.Generator(device='cuda').manual_seed(0)
+    n = args.size
+    div = torch.randn((args.batch, n, n, n), device=dev, generator=g)
+    mask = (torch.rand((args.batch, n, n, n), device=dev, generator=g) < 0.05).to(torch.uint8)
+    target = torch.randn((args.batch, n, n, n), device=dev, generator=g)
+    stream = torch.cuda.current_stream().cuda_stream
+    for _ in range(2):
+        net.forward(div, mask, 1.0, stream)
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(args.repeat):
+        net.forward(div, mask, 1.0, stream)
+    end.record()
+    end.synchronize()
+    fwd = start.elapsed_time(end) / args.repeat
+    flops = net.forward_flops(args.batch, (n, n, n))
+    out = {'size': n, 'batch': args.batch, 'forward_ms': fwd, 'forward_gflop': flops / 1e9,
+           'forward_tflops': flops / (fwd * 1e-3) / 1e12}
+    if args.train:
+        start.record()
+        for _ in range(args.repeat):
+            net.forward(div, mask, 1.0, stream)
+            net.loss_backward(target, mask, stream)
+            net.adam_step(1e-4, stream)
+        end.record()
+        end.synchronize()
+        step = start.elapsed_time(end) / args.repeat
+        out.update(train_step_ms=step, train_tflops=3 * flops / (step * 1e-3) / 1e12)
+    print(json.dumps(out))
+
+
+if __name__ == '__main__':
+    main()

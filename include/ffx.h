@@ -282,6 +282,10 @@ int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs
 /* Fused residual + 2x2x2 average restriction (solid_multigrid.py:56-59). */
 int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs,
                                 float* coarse_rhs, void* stream);
+/* The same, and coarse_p (the coarse level's iterate, may be NULL) set to zero
+ * in the same pass: the next level of the V-cycle starts from it. */
+int ffx_graph_residual_restrict_zero(const FfxGraphLevel* lv, const float* p, const float* rhs,
+                                     float* coarse_rhs, float* coarse_p, void* stream);
 /* p_out = active ? p + coarse[c/2] : 0; replaces shaders/solid_mg_prolong.glsl. */
 int ffx_graph_prolong(const FfxGraphLevel* lv, const float* p, const float* coarse,
                       float* p_out, void* stream);
@@ -447,6 +451,7 @@ typedef struct FfxBatchStats {
     int32_t last_cycles, total_cycles, steps;
     float maxima[3];
     double time;
+    int64_t loop_iterations;           /* solve-loop iterations of the whole batch since creation */
 } FfxBatchStats;
 typedef struct FfxBatchPlan FfxBatchPlan;
 /* Device bytes the plan of these domains needs (descriptors and state). */
