@@ -52,6 +52,7 @@ VARIANTS = {
     'plain': dict(pressure_method='VCYCLE', solid_warm_start=False),
     'pcg': dict(pressure_method='PCG', solid_warm_start=False),
     'fast': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
+    'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
 }
 
 # Algorithmic bytes per cell of each pass (inputs read once, outputs written
@@ -109,6 +110,9 @@ def build_solver(n, storage, seed, device, **overrides):
     from fluxfx_b200.backend.projected import DenseProjectedSmoke
     grid, settings, colliders, emitters, noise = scene(n, storage, seed, **overrides)
     solver = DenseProjectedSmoke(grid, settings, device, colliders=colliders)
+    if settings.learned_warm_start:
+        from fluxfx_b200.learned import attach
+        attach(solver, colliders)
     solver.upload(torch.zeros(grid.cells))
     solver.upload_temperature(torch.zeros(grid.cells))
     solver.upload_velocity([torch.as_tensor(v) for v in noise])
@@ -194,7 +198,10 @@ class Run:
         self.device = device
         self.variant = variant
         self.storage = storage
-        self.solver, self.emitters = build_solver(args.size, storage, args.seed + rank, device, **VARIANTS[variant])
+        overrides = dict(VARIANTS[variant])
+        if variant == args.variant and args.coarse_scale is not None:
+            overrides['mg_coarse_scale'] = args.coarse_scale
+        self.solver, self.emitters = build_solver(args.size, storage, args.seed + rank, device, **overrides)
         self.h = 1.0 / args.size
         self.dt = 0.02
 
@@ -302,7 +309,19 @@ def run_b200(args):
                      rel_div=prun.solver.measure_projection()['rel_div_inf'])
         prun.close()
 
-    elapsed, e2e_time, p_el = max_over_ranks([elapsed, e2e_time, plain['elapsed'] if plain else 0.0], world)
+    # --- the plain algorithm started from the learned guess -------------------
+    learned = None
+    if args.compare_learned and args.variant != 'learned':
+        lrun = Run(args, device, rank, 'learned', args.storage)
+        lrun.warm(args.warmup)
+        l_steps = max(2, args.steps // 2)
+        l_elapsed = lrun.timed(l_steps)
+        learned = dict(elapsed=l_elapsed, steps=l_steps, cycles=lrun.cycles,
+                       rel_div=lrun.solver.measure_projection()['rel_div_inf'])
+        lrun.close()
+
+    elapsed, e2e_time, p_el, l_el = max_over_ranks(
+        [elapsed, e2e_time, plain['elapsed'] if plain else 0.0, learned['elapsed'] if learned else 0.0], world)
     if rank == 0:
         hbm, peak_kind = peaks()
         s = 4 if args.storage == 'FP32' else 2
@@ -324,7 +343,9 @@ def run_b200(args):
             "data": "synthetic (seeded scene; no dataset)",
             "config": {"workload": f"dense smoke step {n}^3, sphere r=40 + box colliders, 2 emitters r=8, MacCormack, "
                                    f"projection to rel div<=1e-4; variant={args.variant} "
-                                   f"({VARIANTS[args.variant]}), {args.storage} storage",
+                                   f"({VARIANTS[args.variant]}"
+                                   f"{'' if args.coarse_scale is None else f', mg_coarse_scale={args.coarse_scale}'}), "
+                                   f"{args.storage} storage",
                        "cells": cells, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}",
                        "v_cycles_mean": statistics.mean(head['cycles']), "v_cycles_max": max(head['cycles']),
@@ -335,7 +356,13 @@ def run_b200(args):
                            "v_cycles_mean": statistics.mean(plain['cycles']),
                            "final_rel_div_inf": plain['rel_div']},
                        "speedup_vs_plain": None if plain is None else
-                       job_rate(world, args.steps, elapsed) / job_rate(world, plain['steps'], p_el)},
+                       job_rate(world, args.steps, elapsed) / job_rate(world, plain['steps'], p_el),
+                       "learned_warm_start_mg": None if learned is None else {
+                           "steps_per_s": job_rate(world, learned['steps'], l_el), "steps": learned['steps'],
+                           "v_cycles_mean": statistics.mean(learned['cycles']),
+                           "final_rel_div_inf": learned['rel_div'], "storage": args.storage,
+                           "method": "stand-alone V(4,4) cycles from the U-Net's guess (net on the 128^3 "
+                                     "restriction, trilinear prolongation)"}},
             "cell_updates_per_s": world * args.steps * cells / elapsed,
             "passes": pass_report,
             "e2e": {"value": job_rate(world, e2e_steps, e2e_time), "unit": UNIT, "h2d_bytes_per_step": h2d,
@@ -537,6 +564,9 @@ def main():
     ap.add_argument('--cpu-sample', type=int, default=64)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--no-compare-plain', dest='compare_plain', action='store_false')
+    ap.add_argument('--no-compare-learned', dest='compare_learned', action='store_false')
+    ap.add_argument('--coarse-scale', type=float, default=None,
+                    help='over-correction factor of the headline variant\'s prolongation (default: the variant\'s)')
     ap.add_argument('--workload', default='single256', choices=('single256', 'batched48'),
                     help='single256: the 256^3 collider scene (default); batched48: 48 uneven domains')
     args = ap.parse_args()

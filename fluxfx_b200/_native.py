@@ -57,7 +57,8 @@ class FfxScalarChannel(C.Structure):
 
 
 class FfxGraphLevel(C.Structure):
-    _fields_ = [('nx', i32), ('ny', i32), ('nz', i32), ('edges', vp), ('solid', vp), ('w', f3), ('links', vp)]
+    _fields_ = [('nx', i32), ('ny', i32), ('nz', i32), ('edges', vp), ('solid', vp), ('w', f3),
+                ('coarse_scale', f32), ('links', vp)]
 
 
 TAIL_LEVELS = 8
@@ -167,6 +168,7 @@ _PROTOTYPES = {
     'ffx_adam': (C.c_int, [i64, vp, vp, vp, vp, vp, f32, f32, f32, f32, i32, vp]),
     'ffx_pack_input': (C.c_int, [i64, vp, vp, f32, vp, vp]),
     'ffx_mse_grad': (C.c_int, [i64, vp, i32, vp, vp, f32, vp, vp, vp]),
+    'ffx_unpack_channel': (C.c_int, [i64, vp, i32, f32, vp, vp]),
     'ffx_curl': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, vp]),
     'ffx_confine': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp]),
     'ffx_combustion': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, f32, f32, f32, f32, vp, vp, vp, vp, vp]),

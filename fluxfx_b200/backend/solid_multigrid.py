@@ -89,6 +89,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         shape = tuple(grid.shape)
         weights = [float(np.float32((n / e) ** 2)) for n, e in zip(shape, grid.extent)]
         level0 = N.FfxGraphLevel(*shape, None, ptr(self._mask), N.f3(*weights))
+        level0.coarse_scale = s.mg_coarse_scale   # over-correction of the prolongation (1: the reference's)
         # one link byte per cell lets the level-0 passes run four cells per thread
         nx, ny, nz = shape
         self._links = torch.empty((nz, ny, nx), dtype=torch.uint8, device=dev.device)
@@ -107,6 +108,7 @@ class SolidMultigridProjector(SolidPressureProjector):
             if int(flag.item()):
                 break   # an aggregate would join disconnected children: stop here
             graph = N.FfxGraphLevel(*coarse_shape, ptr(edges), None, N.f3(0.0, 0.0, 0.0))
+            graph.coarse_scale = s.mg_coarse_scale
             self.levels.append(dict(shape=coarse_shape, edges=edges, graph=graph, p=dev.texture(coarse_shape),
                                     q=dev.texture(coarse_shape), rhs=dev.texture(coarse_shape)))
             shape = coarse_shape
@@ -121,6 +123,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.post_sweeps = s.mg_post_sweeps or 4
         self.last_cycles = 0
         self.timer = None
+        self.learned = None
         self.use_graphs = True
         self._graphs = {}
         self.use_tail = True
@@ -344,7 +347,11 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.last_cycles = 0
         if len(self.levels) == 1:
             return super().solve_pressure(dt, previous_dt)
-        if not (s.solid_warm_start and previous_dt is not None):
+        if s.learned_warm_start and not (s.solid_warm_start and previous_dt is not None):
+            if self.learned is None:
+                raise ValueError('learned_warm_start needs a model: projector.attach_learned(LearnedWarmStart(...))')
+            self.learned.guess(self.before, self.pressure)
+        elif not (s.solid_warm_start and previous_dt is not None):
             self.pressure.zero_()
         self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
         self.last_iterations = 0
@@ -379,6 +386,11 @@ class SolidMultigridProjector(SolidPressureProjector):
                     self.last_cycles += 1
         self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
 
+    def attach_learned(self, model):
+        """Pressure guess used when ``learned_warm_start`` is set
+        (``fluxfx_b200.learned.LearnedWarmStart``)."""
+        self.learned = model
+
     def reset(self):
         super().reset()
         self.last_cycles = 0
@@ -406,6 +418,9 @@ class SolidMultigridProjector(SolidPressureProjector):
     def close(self):
         self._graphs = {}
         self._kry = None
+        if self.learned is not None:
+            self.learned.close()
+        self.learned = None
         self._links = None
         self._tail = None
         self.levels = []

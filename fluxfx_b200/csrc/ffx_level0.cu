@@ -38,6 +38,7 @@ struct L0 {
     int nx, ny, nz, nx4;
     const uint8_t* links;
     float wx, wy, wz;
+    float cs;              // coarse-correction factor of the prolongation (1: plain)
 };
 
 inline L0 make_l0(const FfxGraphLevel* lv) {
@@ -45,6 +46,7 @@ inline L0 make_l0(const FfxGraphLevel* lv) {
     g.nx = lv->nx; g.ny = lv->ny; g.nz = lv->nz; g.nx4 = lv->nx / 4;
     g.links = lv->links;
     g.wx = lv->w[0]; g.wy = lv->w[1]; g.wz = lv->w[2];
+    g.cs = lv->coarse_scale != 0.f ? lv->coarse_scale : 1.f;
     return g;
 }
 
@@ -112,7 +114,7 @@ __device__ __forceinline__ float4 it4(const L0& g, const ItArgs& A, float beta, 
         // coarse cell of (x, y, z) is (x/2, y/2, z/2); cells 4x4, 4x4+1 share
         // coarse x = 2x4 and 4x4+2, 4x4+3 share 2x4+1: one float2.
         const float2 c = ld2(A.b, x4 + g.nx4 * ((y >> 1) + (g.ny >> 1) * (z >> 1)));
-        return make_float4(v.x + c.x, v.y + c.x, v.z + c.y, v.w + c.y);
+        return make_float4(v.x + g.cs * c.x, v.y + g.cs * c.x, v.z + g.cs * c.y, v.w + g.cs * c.y);
     } else {
         if (!A.b) return v;
         const float4 q = ld4(A.b, i4);
@@ -126,7 +128,7 @@ __device__ __forceinline__ float it1(const L0& g, const ItArgs& A, float beta, i
     if constexpr (K == It::Plain) {
         return v;
     } else if constexpr (K == It::Prolonged) {
-        return v + __ldg(A.b + (x >> 1) + (g.nx >> 1) * ((y >> 1) + (g.ny >> 1) * (z >> 1)));
+        return v + g.cs * __ldg(A.b + (x >> 1) + (g.nx >> 1) * ((y >> 1) + (g.ny >> 1) * (z >> 1)));
     } else {
         return A.b ? v + beta * __ldg(A.b + i) : v;
     }

@@ -351,6 +351,7 @@ struct GLvl {
     const float4* edges;     // NULL: derive from the mask
     const uint8_t* solid;
     float w[3];
+    float cs;                // coarse-correction factor of the prolongation into this level (1: plain)
 };
 
 inline GLvl make_glvl(const FfxGraphLevel* lv) {
@@ -359,6 +360,7 @@ inline GLvl make_glvl(const FfxGraphLevel* lv) {
     g.edges = reinterpret_cast<const float4*>(lv->edges);
     g.solid = lv->solid;
     for (int a = 0; a < 3; ++a) g.w[a] = lv->w[a];
+    g.cs = lv->coarse_scale != 0.f ? lv->coarse_scale : 1.f;
     return g;
 }
 
@@ -573,7 +575,7 @@ __device__ __forceinline__ float prolonged(const GLvl& g, const float* __restric
                                            const float* __restrict__ coarse, int i, int x, int y, int z) {
     if (!g_active(g, i)) return 0.f;
     const int cx = g.nx / 2, cy = g.ny / 2;
-    return __ldg(p + i) + __ldg(coarse + (x >> 1) + cx * ((y >> 1) + cy * (z >> 1)));
+    return __ldg(p + i) + g.cs * __ldg(coarse + (x >> 1) + cx * ((y >> 1) + cy * (z >> 1)));
 }
 
 __global__ void __launch_bounds__(256) graph_prolong_kernel(GLvl g, const float* __restrict__ p,
@@ -769,7 +771,7 @@ __device__ __forceinline__ void graph_tail_body(const TailArgs& A) {
         const float* coarse = cur[k + 1];
         const int cx = g.nx / 2, cy = g.ny / 2;
         auto pro = [&](int j, int jx, int jy, int jz) {
-            return g_active(g, j) ? p[j] + coarse[(jx >> 1) + cx * ((jy >> 1) + cy * (jz >> 1))] : 0.f;
+            return g_active(g, j) ? p[j] + g.cs * coarse[(jx >> 1) + cx * ((jy >> 1) + cy * (jz >> 1))] : 0.f;
         };
         for (int i = threadIdx.x; i < L.n; i += kTailThreads) {
             int x, y, z;

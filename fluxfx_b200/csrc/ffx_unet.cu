@@ -370,6 +370,12 @@ __global__ void adam_kernel(long long n, float* w, float* m, float* v, const flo
 
 // Network input: channel 0 = scale * divergence, channel 1 = solid mask,
 // channels 2..7 = 0 (the first convolution reads 8 channels).
+__global__ void unpack_channel_kernel(long long voxels, const float* __restrict__ src, int pitch, float scale,
+                                      float* __restrict__ out) {
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < voxels) out[i] = src[i * pitch] * scale;
+}
+
 __global__ void pack_input_kernel(long long voxels, const float* div, const uint8_t* mask, float scale, bf16* out) {
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= voxels) return;
@@ -548,6 +554,12 @@ int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float 
     FFX_REQUIRE(voxels >= 1 && div && out && ((uintptr_t)out & 15) == 0, "ffx_pack_input: invalid arguments");
     pack_input_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, div, mask, scale, (bf16*)out);
     return launch_status("pack_input_kernel");
+}
+
+int ffx_unpack_channel(int64_t voxels, const float* src, int32_t pitch, float scale, float* out, void* stream) {
+    FFX_REQUIRE(voxels >= 1 && src && out && pitch >= 1, "ffx_unpack_channel: invalid arguments");
+    unpack_channel_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, src, pitch, scale, out);
+    return launch_status("unpack_channel_kernel");
 }
 
 int ffx_mse_grad(int64_t voxels, const float* pred, int32_t pred_pitch, const float* target, const uint8_t* mask,

@@ -1,0 +1,92 @@
+"""The trained U-Net as the pressure solver's initial guess.
+
+``LearnedWarmStart(grid, colliders, device)`` predicts the impulse pressure of
+a projection from its divergence (``projector.before``) and the collider
+mask. Grids up to 128 cells per axis run the network at their own
+resolution; larger grids (dimensions divisible by 16) run it on the 2x2x2
+average of the divergence over a half-resolution grid whose collider mask is
+rasterised at that resolution, and the prediction is prolonged trilinearly.
+Every pass is a library kernel (``ffx_mg_restrict``, ``ffx_max_abs``,
+``ffx_pack_input`` + the convolutions, ``ffx_unpack_channel``,
+``ffx_mg_prolong``); torch only allocates.
+
+Attach it with ``projector.attach_learned(model)`` and set
+``learned_warm_start=True``: the solve then starts from the prediction when it
+would otherwise start from zero (every step without ``solid_warm_start``; the
+first step after a reset with it). The multigrid still iterates to the same
+tolerance, so the plain method stays both the fallback and the judge.
+"""
+import ctypes as C
+from pathlib import Path
+
+import torch
+
+from .. import _native as N
+from ..backend.device import ptr
+from .unet import HEAD_CHANNELS, UNet
+
+WEIGHTS = Path(__file__).resolve().parent / 'weights' / 'unet128.pt'
+MAX_NATIVE = 128
+
+
+def weight_of(shape, extent):
+    """Largest Laplacian conductance (n / extent)^2 of a grid."""
+    return max((n / e) ** 2 for n, e in zip(shape, extent))
+
+
+class LearnedWarmStart:
+    def __init__(self, grid, colliders, device, weights=None, net=None):
+        from ..backend.collision import SolidDevice
+        from ..physics.config import GridSpec
+        base = getattr(device, 'base', device)
+        self.device = base
+        self.grid = grid
+        self.factor = 1 if max(grid.shape) <= MAX_NATIVE else 2
+        shape = tuple(n // self.factor for n in grid.shape)
+        if any(n % 8 for n in shape) or any(n % self.factor for n in grid.shape):
+            raise ValueError('the network needs grid dimensions divisible by 8 (by 16 above 128 cells)')
+        self.shape = shape
+        coarse = GridSpec(shape, extent=grid.extent, axis_limit=max(128, max(shape)))
+        if colliders:
+            self._solids = SolidDevice(coarse, colliders, base)
+            self.mask = self._solids.mask
+        else:
+            self._solids = None
+            self.mask = torch.zeros(shape[::-1], dtype=torch.uint8, device=base.device)
+        self.weight = weight_of(shape, grid.extent)
+        self.net = net or UNet(base.device, seed=0)
+        if net is None:
+            state = torch.load(weights or WEIGHTS)
+            self.net.load_state_dict(state)
+        dev = base.device
+        nx, ny, nz = shape
+        self.div = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev) if self.factor > 1 else None
+        self.coarse = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev) if self.factor > 1 else None
+        self.zero = torch.zeros(tuple(grid.shape[::-1]), dtype=torch.float32, device=dev) if self.factor > 1 else None
+        self._max = torch.zeros(1, dtype=torch.float32, device=dev)
+
+    def guess(self, before, out):
+        """Write the predicted pressure for the divergence ``before`` into ``out``."""
+        dev = self.device
+        s = dev.s
+        src = before
+        if self.factor > 1:
+            dev.call('ffx_mg_restrict', N.n3(*self.grid.shape), ptr(before), ptr(self.div), s)
+            src = self.div
+        dev.call('ffx_max_abs', src.numel(), N.FFX_F32, ptr(src), ptr(self._max), s)
+        m = float(self._max.item())
+        if m == 0.0:
+            out.zero_()
+            return
+        scale = 1.0 / m
+        pred = self.net.forward(src.unsqueeze(0), self.mask.unsqueeze(0), scale, s.value or 0)
+        target = self.coarse if self.factor > 1 else out
+        dev.call('ffx_unpack_channel', src.numel(), ptr(self.net.pred), HEAD_CHANNELS, 1.0 / (scale * self.weight),
+                 ptr(target), s)
+        if self.factor > 1:
+            dev.call('ffx_mg_prolong', N.n3(*self.grid.shape), ptr(self.zero), ptr(self.coarse), ptr(out), s)
+        return pred
+
+    def close(self):
+        self.net = None
+        self._solids = None

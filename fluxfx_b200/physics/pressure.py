@@ -100,6 +100,8 @@ class PressureSettings(ThermalSettings):
     storage: str = "FP32"
     solid_warm_start: bool = False
     pressure_method: str = "VCYCLE"
+    learned_warm_start: bool = False
+    mg_coarse_scale: float = 1.0
 
     def __post_init__(self):
         super().__post_init__()
@@ -138,6 +140,10 @@ class PressureSettings(ThermalSettings):
             raise ValueError("Velocity blend must lie in [0, 1]")
         if type(self.solid_warm_start) is not bool:
             raise ValueError("Collider warm start must be boolean")
+        if type(self.learned_warm_start) is not bool:
+            raise ValueError("Learned warm start must be boolean")
+        if not isfinite(self.mg_coarse_scale) or not 0 < self.mg_coarse_scale < 2:
+            raise ValueError("Coarse-correction factor must lie in (0, 2)")
 
 
 def divergence_stats(before, after):

@@ -231,6 +231,8 @@ typedef struct FfxGraphLevel {
     const float* edges;     /* 4 floats per cell, or NULL for level 0 */
     const uint8_t* solid;   /* level-0 mask when edges == NULL */
     float w[3];             /* level-0 conductances (n/extent)^2 */
+    float coarse_scale;     /* factor of the coarse correction prolonged into this level
+                               (over-correction); 0 or 1 = the plain prolongation */
     const uint8_t* links;   /* optional level-0 link bytes (ffx_graph_links); with
                                nx % 4 == 0 and 16-byte aligned fields the level-0
                                passes run four cells per thread. NULL: derive
@@ -530,6 +532,9 @@ int ffx_adam(int64_t n, float* w, float* m, float* v, const float* g, void* w_bf
 /* Network input, 8 BF16 channels per voxel: scale * div, solid mask, zeros. */
 int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float scale, void* out,
                    void* stream);
+/* out[v] = src[v * pitch] * scale: one channel of the FP32 network output as a cell field. */
+int ffx_unpack_channel(int64_t voxels, const float* src, int32_t pitch, float scale, float* out,
+                       void* stream);
 /* *loss += sum over fluid voxels of (pred - target)^2 * inv_count; grad (8 BF16
  * channels per voxel) = its derivative in channel 0. */
 int ffx_mse_grad(int64_t voxels, const float* pred, int32_t pred_pitch, const float* target,

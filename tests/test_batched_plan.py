@@ -55,7 +55,7 @@ def fake_domain(shape, tail=True, pre=4, post=4, base=0x10000):
     levels.append(tuple(n))
     D.levels = len(levels)
     for k, (nx, ny, nz) in enumerate(levels):
-        lv = N.FfxGraphLevel(nx, ny, nz, None if k == 0 else p(), D.solid if k == 0 else None, N.f3(1, 1, 1), None)
+        lv = N.FfxGraphLevel(nx, ny, nz, None if k == 0 else p(), D.solid if k == 0 else None, N.f3(1, 1, 1))
         D.level[k].level = lv
         D.level[k].p, D.level[k].q, D.level[k].rhs = p(), p(), p()
     small = [k for k in range(1, len(levels)) if np.prod(levels[k]) <= 512]
