@@ -14,13 +14,16 @@ One "step" = one DenseProjectedSmoke.step plus the next-dt selection (one
 readback of three floats). Solver variants, all to the same tolerance from the
 same seeded start after the same warm-up:
 
-* plain  -- the reference algorithm: stand-alone aggregation V-cycles (4/4
-            Jacobi sweeps), pressure cold-started every step, FP32 storage;
-* pcg    -- conjugate gradients preconditioned by the same V-cycle;
-* fast   -- pcg with the previous step's pressure as the initial guess and a
-            V(1,1) preconditioner (one Jacobi sweep down, one up: more
-            iterations than V(4,4) but less time)
-            (--storage selects FP32 or BF16 field storage).
+* plain   -- the reference algorithm: stand-alone aggregation V-cycles (4/4
+             Jacobi sweeps), pressure cold-started every step, FP32 storage;
+* fast    -- the same V(4,4) cycles started from the previous step's pressure
+             (scaled by dt / previous dt) with the coarse correction
+             over-corrected by 1.8 at every prolongation (default);
+* pcg     -- conjugate gradients preconditioned by a V(1,1) cycle, warm start;
+* learned -- plain, started from the U-Net's prediction (network on the
+             128^3 restriction, trilinear prolongation)
+             (--storage selects FP32 or BF16 field storage; --set overrides
+             any solver setting of the headline variant).
 
 The JSON `value` is the `--variant` run (default fast); the plain run is
 reported beside it. `value` is whole-job steps/s (N GPUs each run their own
@@ -50,8 +53,8 @@ UNIT = "steps/s"
 
 VARIANTS = {
     'plain': dict(pressure_method='VCYCLE', solid_warm_start=False),
-    'pcg': dict(pressure_method='PCG', solid_warm_start=False),
-    'fast': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
+    'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.8),
+    'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
     'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
 }
 
@@ -199,8 +202,10 @@ class Run:
         self.variant = variant
         self.storage = storage
         overrides = dict(VARIANTS[variant])
-        if variant == args.variant and args.coarse_scale is not None:
-            overrides['mg_coarse_scale'] = args.coarse_scale
+        if variant == args.variant:
+            if args.coarse_scale is not None:
+                overrides['mg_coarse_scale'] = args.coarse_scale
+            overrides.update(parse_settings(args.set))
         self.solver, self.emitters = build_solver(args.size, storage, args.seed + rank, device, **overrides)
         self.h = 1.0 / args.size
         self.dt = 0.02
@@ -344,7 +349,8 @@ def run_b200(args):
             "config": {"workload": f"dense smoke step {n}^3, sphere r=40 + box colliders, 2 emitters r=8, MacCormack, "
                                    f"projection to rel div<=1e-4; variant={args.variant} "
                                    f"({VARIANTS[args.variant]}"
-                                   f"{'' if args.coarse_scale is None else f', mg_coarse_scale={args.coarse_scale}'}), "
+                                   f"{'' if args.coarse_scale is None else f', mg_coarse_scale={args.coarse_scale}'}"
+                                   f"{''.join(', ' + x for x in args.set)}), "
                                    f"{args.storage} storage",
                        "cells": cells, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}",
@@ -462,7 +468,10 @@ def run_batched(args):
     from fluxfx_b200.backend.device import CudaDevice
     device = CudaDevice()
     graph_steps = 32
-    scenes = batched_scenes(48, seed=args.seed)
+    opts = parse_settings(args.set)
+    warm = bool(opts.get('solid_warm_start', True))
+    alpha = float(opts.get('mg_coarse_scale', 1.8))
+    scenes = batched_scenes(48, seed=args.seed, warm_start=warm, coarse_scale=alpha)
     solvers, sources = build_solvers(scenes, device)
     cells = cell_updates(solvers)
     batch = BatchedSmoke(solvers, sources)
@@ -531,6 +540,7 @@ def run_batched(args):
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
         "config": {"workload": "48 uneven FP32 smoke domains, axes from {32,48,64,96,128}, 1-3 emitters, "
                                "0-2 sphere colliders, multigrid to rel div 1e-4, 32 steps per CUDA graph",
+                   "solver": f"aggregation V(4,4) cycles, warm start {warm}, coarse-correction factor {alpha}",
                    "cells": cells, "domains": len(solvers), "l2": "working set > L2 (no flush)"},
         "cell_updates_per_s": cells * rate, "v_cycles_per_domain_step": cycles,
         "solve_loop_iterations_per_step": iterations / steps,
@@ -551,6 +561,25 @@ def run_batched(args):
 SHAPES_NAMES = ((32, 8), (64, 4), (128, 2), (16, 16))
 
 
+def parse_settings(items):
+    """--set name=value pairs as PressureSettings overrides (ints, floats, booleans, strings)."""
+    out = {}
+    for item in items or ():
+        name, _, text = item.partition('=')
+        if text in ('True', 'False'):
+            value = text == 'True'
+        else:
+            try:
+                value = int(text)
+            except ValueError:
+                try:
+                    value = float(text)
+                except ValueError:
+                    value = text
+        out[name.strip()] = value
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split('\n')[0])
     ap.add_argument('--gpus', type=int, default=1)
@@ -565,6 +594,8 @@ def main():
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--no-compare-plain', dest='compare_plain', action='store_false')
     ap.add_argument('--no-compare-learned', dest='compare_learned', action='store_false')
+    ap.add_argument('--set', action='append', default=[], metavar='NAME=VALUE',
+                    help='settings override of the headline variant (repeatable)')
     ap.add_argument('--coarse-scale', type=float, default=None,
                     help='over-correction factor of the headline variant\'s prolongation (default: the variant\'s)')
     ap.add_argument('--workload', default='single256', choices=('single256', 'batched48'),

@@ -9,8 +9,9 @@ pressure solve as a conditional WHILE node of a CUDA graph that stops when
 every domain has converged, and each domain's next time step
 ``min(dt_max, cfl * cell / max|u|)`` computed on the device, so a run of many
 steps is one graph launch with no host round trip. Each domain's fields after
-a batched run are bit-identical to stepping that solver alone with the same
-time-step rule.
+a batched run are bit-identical to stepping that solver alone (from a reset)
+with the same time-step rule. The solve starts from zero, or with
+``solid_warm_start`` from the previous pressure times dt / previous dt.
 
 A domain without colliders takes the collider path with an empty mask (the
 reference's collider path with its collider outside the domain).
@@ -51,8 +52,8 @@ def _check_solver(i, s):
         problems.append('needs the collider multigrid with at least two levels')
     elif not p.uses_impulse:
         problems.append('needs the impulse pressure form')
-    if st.pressure_method != 'VCYCLE' or st.solid_warm_start:
-        problems.append('stand-alone V-cycles from a zero pressure required')
+    if st.pressure_method != 'VCYCLE' or st.learned_warm_start:
+        problems.append('stand-alone V-cycles required (from zero or the previous pressure)')
     if not st.pressure_tolerance > 0:
         problems.append('a pressure tolerance is required')
     if st.moving_colliders or st.vorticity_strength > 0 or s.combustion is not None:
@@ -133,6 +134,7 @@ class BatchedSmoke:
         D.inverse = p.coarse_matrix.data_ptr() if p.coarse_matrix is not None else None
         D.pre, D.post = p.pre_sweeps, p.post_sweeps
         D.max_cycles = st.pressure_max_cycles
+        D.warm_start = int(st.solid_warm_start)
         D.tolerance = st.pressure_tolerance
 
     # ------------------------------------------------------------ running
@@ -257,12 +259,15 @@ class BatchedSmoke:
             pass
 
 
-def batched_scenes(count=48, seed=0, sizes=(32, 48, 64, 96, 128), cell=1.0 / 64.0):
+def batched_scenes(count=48, seed=0, sizes=(32, 48, 64, 96, 128), cell=1.0 / 64.0, warm_start=False,
+                   coarse_scale=1.0):
     """Seeded uneven domains: each axis from ``sizes``; 1-3 spherical emitters
     (radius 3-8 cells, density and temperature U(0.5, 1), in the lower third);
     0-2 static sphere colliders (radius 4-16 cells, above the emitters). A
     domain without colliders gets one sphere outside the domain (an empty
-    mask). Returns [(grid, settings, colliders, emitters, noise)]."""
+    mask). ``warm_start`` and ``coarse_scale`` select the solver (previous
+    pressure as the start; over-correction of the prolongation). Returns
+    [(grid, settings, colliders, emitters, noise)]."""
     import numpy as np
     from ..physics.collision import primitive
     from ..physics.config import GridSpec
@@ -291,7 +296,8 @@ def batched_scenes(count=48, seed=0, sizes=(32, 48, 64, 96, 128), cell=1.0 / 64.
             colliders.append(primitive('SPHERE', (-1.0, -1.0, -1.0), (cell, cell, cell)))
         settings = PressureSettings(velocity_advection='MACCORMACK', scalar_advection='MACCORMACK', thermal_lift=1.0,
                                     density_weight=0.05, dissipation=0.0, cooling=0.0, heat_mode='TARGET',
-                                    pressure_tolerance=1e-4, pressure_max_cycles=200)
+                                    pressure_tolerance=1e-4, pressure_max_cycles=200, solid_warm_start=warm_start,
+                                    mg_coarse_scale=coarse_scale)
         noise = [rng.uniform(-1e-3, 1e-3, (fs[2], fs[1], fs[0])).astype(np.float32) for fs in grid.face_shapes]
         out.append((grid, settings, tuple(colliders), emitters, noise))
     return out

@@ -26,7 +26,7 @@ struct FfxBatchPlan {
     char* ws = nullptr;
     int64_t ws_bytes = 0;
     ffx::BatchState* state = nullptr;
-    struct Solve { double tol; int max_cycles; int pad; }* solve = nullptr;
+    struct Solve { double tol; int max_cycles; int warm; }* solve = nullptr;
     const void* rules = nullptr;
     struct Guard { int iterations; int tripped; long long total; }* guard = nullptr;   // solve-loop bound (device)
     struct Entry { int slot, X, Y, Z; };
@@ -86,8 +86,8 @@ __global__ void batch_decide_kernel(BatchState* state, const FfxBatchPlan::Solve
 
 struct StepRule { double cell, cfl, dt_max; };
 
-__global__ void batch_step_end_kernel(BatchState* state, const StepRule* rule, int count,
-                                      FfxBatchPlan::Guard* guard) {
+__global__ void batch_step_end_kernel(BatchState* state, const StepRule* rule, const FfxBatchPlan::Solve* solve,
+                                      int count, FfxBatchPlan::Guard* guard) {
     if (threadIdx.x == 0) guard->iterations = 0;
     for (int d = threadIdx.x; d < count; d += blockDim.x) {
         BatchState& S = state[d];
@@ -97,11 +97,17 @@ __global__ void batch_step_end_kernel(BatchState* state, const StepRule* rule, i
         S.last_maxima[2] = S.maxima[2];
         S.total_cycles += S.cycles;
         S.steps += 1;
-        S.time += (double)S.dt;
+        S.time += S.dtd;
         S.last_dt = S.dt;
+        S.last_dtd = S.dtd;
         const float umax = fmaxf(fmaxf(S.maxima[0], S.maxima[1]), S.maxima[2]);
         const double r = rule[d].cfl * rule[d].cell / (double)umax;
-        S.dt = (float)(umax > 0.f ? (r < rule[d].dt_max ? r : rule[d].dt_max) : rule[d].dt_max);
+        S.dtd = umax > 0.f ? (r < rule[d].dt_max ? r : rule[d].dt_max) : rule[d].dt_max;
+        S.dt = (float)S.dtd;
+        // impulse warm start: the previous pressure times dt / previous dt when they differ
+        const double ratio = S.dtd / S.last_dtd;
+        S.pfactor = (float)ratio;
+        S.pmode = solve[d].warm ? (fabs(ratio - 1.0) > 1e-6 ? 2 : 1) : 0;
         S.scale = 0.f;
         S.res = 0.f;
         S.cycles = 0;
@@ -322,7 +328,9 @@ void build_cycle(Builder& B) {
     auto other = [&](int d, int k) { const FfxBatchLevel& L = P.dom[d].level[k]; return role[d][k] ? L.p : L.q; };
     auto level_entry = [&](int kind, int d, int k) {
         const FfxGraphLevel& lv = P.dom[d].level[k].level;
-        return entry_for(kind, d, lv.nx, lv.ny, lv.nz);
+        FfxBatchPlan::Entry e = entry_for(kind, d, lv.nx, lv.ny, lv.nz);
+        if (kind == kSmooth && k == 0) e.Z = (lv.nz + kBatchZ0 - 1) / kBatchZ0;   // streamed along z
+        return e;
     };
     auto smooth_at = [&](int k, const std::vector<int>& slots) {
         P.cycle.push_back(B.launch(kSmooth, slots, [&](int d, char* out, FfxBatchPlan::Entry& e) {
@@ -410,8 +418,10 @@ int build(FfxBatchPlan& P, std::vector<char>& host) {
         BatchState S;
         memset(&S, 0, sizeof S);
         S.dt = D.dt0;
+        S.dtd = D.dt0;
+        S.pmode = 0;
         memcpy(B.host.data() + state_off + d * sizeof(BatchState), &S, sizeof S);
-        FfxBatchPlan::Solve V = {D.tolerance, D.max_cycles, 0};
+        FfxBatchPlan::Solve V = {D.tolerance, D.max_cycles, D.warm_start ? 1 : 0};
         memcpy(B.host.data() + solve_off + d * sizeof V, &V, sizeof V);
         StepRule R = {D.cell, D.cfl, D.dt_max};
         memcpy(B.host.data() + rule_off + d * sizeof R, &R, sizeof R);
@@ -555,7 +565,7 @@ int capture_step(FfxBatchPlan& P, int par, cudaStream_t st, cudaStream_t side) {
     if (e != cudaSuccess) return cuda_status(e, "ffx_batch_graph: capture dependencies");
     e = issue_list(P, P.post[par], st);
     if (e != cudaSuccess) return cuda_status(e, "ffx_batch_graph: passes after the solve");
-    batch_step_end_kernel<<<1, 64, 0, st>>>(P.state, rules_of(P), P.count, P.guard);
+    batch_step_end_kernel<<<1, 64, 0, st>>>(P.state, rules_of(P), P.solve, P.count, P.guard);
     return cuda_status(cudaGetLastError(), "ffx_batch_graph: step end");
 }
 

@@ -18,6 +18,7 @@ namespace ffx {
 
 constexpr int kBatchMax = 64;       // domains per batch
 constexpr int kBatchThreads = 256;  // threads per block of every batched tile kernel
+constexpr int kBatchZ0 = 8;         // z cells per thread of the level-0 sweeps
 
 struct BatchMap {
     int count;                // entries (domains) in this launch
@@ -45,6 +46,10 @@ struct BatchState {
     float last_dt;     // dt of the previous step
     float last_maxima[3];   // maxima of the previous step
     double time;       // simulated time
+    double dtd;        // the time step in FP64 (as the host rule computes it); dt is its FP32 rounding
+    double last_dtd;
+    float pfactor;     // warm start: factor of the previous pressure (dt / previous dt)
+    int pmode;         // pressure at the start of the solve: 0 zero, 1 previous, 2 previous x pfactor
 };
 
 __device__ __forceinline__ int batch_entry(const BatchMap& M, int t) {

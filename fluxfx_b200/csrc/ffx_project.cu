@@ -451,12 +451,13 @@ __global__ void __launch_bounds__(256) graph_smooth_kernel(GLvl g, const float* 
 // neighbours; x/y neighbours come from the L1 lines its warp-mates load. The
 // operator terms are summed in the same order as graph_terms.
 constexpr int kZ = 8;
-__global__ void __launch_bounds__(256) graph_smooth_level0_kernel(GLvl g, const float* __restrict__ p,
-                                                                 const float* __restrict__ rhs, float omega,
-                                                                 float* out) {
-    const int x = blockIdx.x * kBX + threadIdx.x, y = blockIdx.y * kBY + threadIdx.y;
+static_assert(kZ == kBatchZ0, "batched level-0 sweeps tile z like the single-domain ones");
+__device__ __forceinline__ void graph_smooth_level0_body(const GLvl& g, const float* __restrict__ p,
+                                                         const float* __restrict__ rhs, float omega, float* out,
+                                                         const Blk& b) {
+    const int x = b.x * b.bw + b.ox, y = b.y * b.bh + b.oy;
     if (x >= g.nx || y >= g.ny) return;
-    const int z0 = blockIdx.z * kZ;
+    const int z0 = b.z * kZ;
     const int sy = g.nx, sz = g.nx * g.ny;
     int i = x + g.nx * (y + g.ny * z0);
     const float wx = g.w[0], wy = g.w[1], wz = g.w[2];
@@ -506,6 +507,12 @@ __global__ void __launch_bounds__(256) graph_smooth_level0_kernel(GLvl g, const 
         p_lo = p_c; p_c = p_hi;
         f_lo = f_c; f_c = f_hi;
     }
+}
+
+__global__ void __launch_bounds__(256) graph_smooth_level0_kernel(GLvl g, const float* __restrict__ p,
+                                                                 const float* __restrict__ rhs, float omega,
+                                                                 float* out) {
+    graph_smooth_level0_body(g, p, rhs, omega, out, hw_blk());
 }
 
 __device__ __forceinline__ float graph_res(const GLvl& g, const float* __restrict__ p, const float* __restrict__ rhs,
@@ -1351,10 +1358,13 @@ __global__ void __launch_bounds__(kBatchThreads) batch_scale_kernel(const __grid
                                                                     const ScaleDesc* descs, BatchState* state) {
     for_tiles(M, descs, state, false, NoPrep{}, [state](const ScaleDesc& P, const Blk& b, int slot) {
         const int i = b.x * kBatchThreads + (int)threadIdx.x;
+        const int mode = state[slot].pmode;
+        const float f = state[slot].pfactor;
         float v = 0.f;
         if (i < P.n) {
             v = finite_abs(__ldg(P.rhs + i));
-            P.p[i] = 0.f;
+            if (mode == 0) P.p[i] = 0.f;
+            else if (mode == 2) P.p[i] = P.p[i] * f;   // ffx_scale's product
         }
         block_max_to(&state[slot].scale, v);
     });
@@ -1371,14 +1381,24 @@ __global__ void __launch_bounds__(kBatchThreads) batch_gradient_kernel(const __g
 __global__ void __launch_bounds__(kBatchThreads) batch_residual_max_kernel(const __grid_constant__ BatchMap M,
                                                                            const GDesc* descs, BatchState* state) {
     for_tiles(M, descs, state, true, NoPrep{}, [state](const GDesc& P, const Blk& b, int slot) {
+        if (state[slot].scale == 0.f) {
+            // rhs == 0: the solve's result is the zero pressure (and no cycle runs)
+            int x, y, z;
+            if (cell_coords(b, P.g.nx, P.g.ny, x, y, z))
+                for (int zz = z; zz < P.g.nz; zz += b.gz) const_cast<float*>(P.p)[x + P.g.nx * (y + P.g.ny * zz)] = 0.f;
+            return;
+        }
         graph_residual_max_body(P.g, P.p, P.rhs, &state[slot].res, b);
     });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batch_smooth_kernel(const __grid_constant__ BatchMap M,
                                                                      const GDesc* descs, const BatchState* state) {
-    for_tiles(M, descs, state, true, NoPrep{},
-              [](const GDesc& P, const Blk& b, int) { graph_smooth_body(P.g, P.p, P.rhs, kOmega, P.q, b); });
+    // level 0 (mask-derived terms) streams kBatchZ0 cells along z per thread
+    for_tiles(M, descs, state, true, NoPrep{}, [](const GDesc& P, const Blk& b, int) {
+        if (P.g.edges) graph_smooth_body(P.g, P.p, P.rhs, kOmega, P.q, b);
+        else graph_smooth_level0_body(P.g, P.p, P.rhs, kOmega, P.q, b);
+    });
 }
 
 __global__ void __launch_bounds__(kBatchThreads) batch_residual_restrict_kernel(const __grid_constant__ BatchMap M,

@@ -128,12 +128,16 @@ __device__ __forceinline__ long long out_voxel(const Conv& a, long long m, int c
 }
 
 // ------------------------------------------------------------ forward GEMM
+// BN output channels per block (16, 32 or 64, chosen from cout so that narrow
+// layers do not multiply padded channels).
+template <int BN>
 __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_constant__ Conv a) {
+    constexpr int BS = BN + 8;   // bf16 per B row in shared memory (8 pad: conflict-free ldmatrix)
     __shared__ __align__(128) bf16 sA[kStages][kBM * kAStride];
-    __shared__ __align__(128) bf16 sB[kStages][16 * kBStride];
+    __shared__ __align__(128) bf16 sB[kStages][16 * BS];
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
     const long long m0 = (long long)blockIdx.x * kBM;
-    const int n0 = blockIdx.y * kBN;
+    const int n0 = blockIdx.y * BN;
     const int cls = blockIdx.z;
     const bf16* W = a.w + (a.transposed ? (size_t)cls * a.cin * a.cout : 0);
     const long long my_row = m0 + tid;
@@ -150,17 +154,19 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_con
             const bf16* src = (row_ok && u < a.k_units) ? gather(a, pos, u) : nullptr;
             cp_async16(&sA[stage][tid * kAStride + h * 8], src ? src : a.in1.p, src != nullptr);
         }
-        const int kr = tid >> 3, nu = (tid & 7) * 8;
-        const int k = kstep * 16 + kr, n = n0 + nu;
-        const bool ok = k < k_elems && n < a.cout;
-        cp_async16(&sB[stage][kr * kBStride + nu], ok ? W + (size_t)k * a.cout + n : W, ok);
+        if (tid < 2 * BN) {   // 16 rows x BN / 8 units of 8 channels
+            const int kr = tid / (BN / 8), nu = (tid % (BN / 8)) * 8;
+            const int k = kstep * 16 + kr, n = n0 + nu;
+            const bool ok = k < k_elems && n < a.cout;
+            cp_async16(&sB[stage][kr * BS + nu], ok ? W + (size_t)k * a.cout + n : W, ok);
+        }
     };
 
-    float acc[2][8][4];
+    float acc[2][BN / 8][4];
 #pragma unroll
     for (int i = 0; i < 2; ++i)
 #pragma unroll
-        for (int j = 0; j < 8; ++j)
+        for (int j = 0; j < BN / 8; ++j)
 #pragma unroll
             for (int e = 0; e < 4; ++e) acc[i][j][e] = 0.f;
 
@@ -181,9 +187,9 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_con
         for (int mt = 0; mt < 2; ++mt)
             ldmatrix_x4(af[mt], &sA[st][(warp * 32 + mt * 16 + (lane & 15)) * kAStride + (lane >> 4) * 8]);
 #pragma unroll
-        for (int np = 0; np < 4; ++np) {
+        for (int np = 0; np < BN / 16; ++np) {
             unsigned bf[4];
-            ldmatrix_x4_trans(bf, &sB[st][((lane & 7) + ((lane >> 3) & 1) * 8) * kBStride + np * 16 + (lane >> 4) * 8]);
+            ldmatrix_x4_trans(bf, &sB[st][((lane & 7) + ((lane >> 3) & 1) * 8) * BS + np * 16 + (lane >> 4) * 8]);
 #pragma unroll
             for (int mt = 0; mt < 2; ++mt) {
                 mma_bf16(acc[mt][2 * np], af[mt], bf[0], bf[1]);
@@ -202,7 +208,7 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_con
             if (m >= a.rows) continue;
             const long long vox = out_voxel(a, m, cls);
 #pragma unroll
-            for (int nt = 0; nt < 8; ++nt) {
+            for (int nt = 0; nt < BN / 8; ++nt) {
                 const int n = n0 + nt * 8 + (lane & 3) * 2;
                 if (n >= a.cout) continue;
                 float v0 = acc[mt][nt][half * 2], v1 = acc[mt][nt][half * 2 + 1];
@@ -492,9 +498,12 @@ int ffx_conv_forward(const FfxConv* c, void* stream) {
     int e = make_conv(c, a);
     if (e) return e;
     FFX_REQUIRE(a.out || a.out_f32, "ffx_conv_forward: no output");
-    const dim3 grid((unsigned)((a.rows + kBM - 1) / kBM), (unsigned)((a.cout + kBN - 1) / kBN), a.transposed ? 8 : 1);
+    const int bn = a.cout <= 16 ? 16 : (a.cout <= 32 ? 32 : 64);
+    const dim3 grid((unsigned)((a.rows + kBM - 1) / kBM), (unsigned)((a.cout + bn - 1) / bn), a.transposed ? 8 : 1);
     FFX_REQUIRE(grid.x < (1u << 31), "ffx_conv_forward: grid too large");
-    conv_fwd_kernel<<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    if (bn == 16) conv_fwd_kernel<16><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    else if (bn == 32) conv_fwd_kernel<32><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    else conv_fwd_kernel<64><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
     return launch_status("conv_fwd_kernel");
 }
 

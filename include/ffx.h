@@ -410,7 +410,7 @@ int ffx_moving_remap(const FfxGrid* g, int storage, const uint8_t* owners,
  * static colliders, MacCormack (or semi-Lagrangian) transport, buoyancy,
  * table emitters, the aggregation multigrid of backend/solid_multigrid.py:46-76
  * run as stand-alone V-cycles until max|rhs - L p| <= tolerance * max|rhs|
- * (pressure from zero every step), and the time step
+ * (pressure from zero every step, or warm-started), and the time step
  * dt = min(dt_max, cfl * cell / max|u|) computed on the device from the
  * projection's velocity maxima. Results are bit-identical to running each
  * domain alone through the single-domain entry points. */
@@ -446,6 +446,8 @@ typedef struct FfxBatchDomain {
     int32_t tail_start;                /* first level run by the single-block tail, or -1 */
     const double* inverse;             /* FP64 pseudoinverse of the coarsest level, or NULL */
     int32_t pre, post, max_cycles;     /* sweeps per V-cycle (both >= 1), cycle cap per solve */
+    int32_t warm_start;                /* 1: start each solve from the previous step's pressure scaled by
+                                          dt / previous dt (backend/pressure.py:63-75), 0: from zero */
     double tolerance;                  /* relative max-norm residual target (> 0) */
 } FfxBatchDomain;
 typedef struct FfxBatchStats {

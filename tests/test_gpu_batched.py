@@ -77,3 +77,16 @@ def test_multi_step_graph_with_tuned_passes(tmp_path):
     compare(batch, ref, 4)
     assert batch.launches_per_step(ref[0]['cycles'][-1] + 1) > 10
     batch.close()
+
+
+def test_warm_started_batch_matches_single_domain_steps():
+    """Solves from the previous pressure (rescaled by dt / previous dt) take
+    the same cycles and give the same fields as the single-domain solver with
+    solid_warm_start."""
+    scenes = batched_scenes(4, seed=13, sizes=(32, 48, 64), warm_start=True)
+    ref = stepped_alone(scenes, 5)
+    solvers, sources = build_solvers(scenes, device())
+    batch = BatchedSmoke(solvers, sources)
+    batch.run(5)
+    compare(batch, ref, 5)
+    batch.close()
