@@ -18,7 +18,7 @@ same seeded start after the same warm-up:
              Jacobi sweeps), pressure cold-started every step, FP32 storage;
 * fast    -- the same V(4,4) cycles started from the previous step's pressure
              (scaled by dt / previous dt) with the coarse correction
-             over-corrected by 1.8 at every prolongation (default);
+             over-corrected by 1.9 at every prolongation (default);
 * pcg     -- conjugate gradients preconditioned by a V(1,1) cycle, warm start;
 * learned -- plain, started from the U-Net's prediction (network on the
              128^3 restriction, trilinear prolongation)
@@ -53,7 +53,7 @@ UNIT = "steps/s"
 
 VARIANTS = {
     'plain': dict(pressure_method='VCYCLE', solid_warm_start=False),
-    'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.8),
+    'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9),
     'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
     'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
 }
@@ -470,7 +470,7 @@ def run_batched(args):
     graph_steps = 32
     opts = parse_settings(args.set)
     warm = bool(opts.get('solid_warm_start', True))
-    alpha = float(opts.get('mg_coarse_scale', 1.8))
+    alpha = float(opts.get('mg_coarse_scale', 1.9))
     scenes = batched_scenes(48, seed=args.seed, warm_start=warm, coarse_scale=alpha)
     solvers, sources = build_solvers(scenes, device)
     cells = cell_updates(solvers)

@@ -63,7 +63,8 @@ def test_fp32_and_mixed_forms_against_fp64():
     fp32, mixed = gpu_run('FP32'), gpu_run('BF16')
     grid, base, colliders, emitters, noise = scene()
     ref = O.OracleSmoke(grid.shape, grid.extent, PressureSettings(**base), np.float64, mask=fp32['mask'])
-    ref.upload(velocity=tuple(v.astype(np.float64) for v in noise))
+    zeros = np.zeros(grid.shape[::-1])
+    ref.upload(density=zeros, temperature=zeros, velocity=tuple(v.astype(np.float64) for v in noise))
     table = (pack_sources(emitters), len(emitters))
     for _ in range(STEPS):
         ref.step(DT, sources=table)
