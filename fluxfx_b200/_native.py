@@ -128,13 +128,21 @@ _PROTOTYPES = {
     'ffx_dilate_mask': (C.c_int, [P(FfxGrid), vp, vp, vp]),
     'ffx_solid_clear': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp]),
     'ffx_face_predictor': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
+    'ffx_face_predictor_trace': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, P(vp),
+                                           vp]),
     'ffx_advect_velocity': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, f32, C.c_int, f32,
                                       P(FfxSources), vp, vp, f32, f32, C.c_int, vp, vp, vp, vp]),
+    'ffx_advect_velocity_trace': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, f32, C.c_int,
+                                            f32, P(FfxSources), vp, vp, f32, f32, C.c_int, vp, vp, vp, P(vp), vp]),
     'ffx_mac_advect_velocity': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
     'ffx_buoyancy': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, f32, f32, f32, vp, vp]),
     'ffx_scalar_transport': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int, P(vp), P(vp), vp]),
+    'ffx_scalar_transport_trace': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int, P(vp),
+                                             P(vp), vp, vp]),
     'ffx_advect_scalars': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int, P(FfxSources),
                                      C.c_int, P(FfxScalarChannel), vp, vp]),
+    'ffx_advect_scalars_trace': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int,
+                                           P(FfxSources), C.c_int, P(FfxScalarChannel), vp, vp, vp]),
     'ffx_advect_open': (C.c_int, [P(FfxGrid), C.c_int, vp, f32, f3, f32, f3, f32, f32, f32, vp, vp]),
     'ffx_mac_advect_density': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f3, f32, f32, f32, vp, vp]),
     'ffx_walls': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp]),
@@ -243,3 +251,22 @@ def grid_struct(shape, extent):
     nx, ny, nz = shape
     inv = [1.0 / (e / n) for e, n in zip(extent, shape)]
     return FfxGrid(nx, ny, nz, *[float(e) for e in extent], *inv)
+
+
+def grid_pow2(shape, extent):
+    """True when every FP32 extent, cell count and spacing (extent / count in
+    FP32) is a power of two: the kernels then divide by exact reciprocals and
+    the two transport passes form the same start points."""
+    import math
+
+    import numpy as np
+
+    def pow2(v):
+        v = float(v)
+        return v > 0 and math.frexp(v)[0] == 0.5
+    for n, e in zip(shape, extent):
+        e32 = np.float32(e)
+        h32 = np.float32(e32 / np.float32(n))
+        if not (pow2(e32) and pow2(n) and pow2(h32)):
+            return False
+    return True

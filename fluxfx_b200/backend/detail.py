@@ -28,13 +28,21 @@ class DetailPasses:
         self.predictors = self.reverses = None
         self.face_predictor = None
         self.curl = None
+        # departure points of the predictor passes, reused by the correction passes
+        # (faces only on power-of-two grids, where both passes trace the same point)
+        self.reuse_traces = True
+        self.face_trace = None
+        self.cell_trace = None
+        self._pow2 = N.grid_pow2(grid.shape, grid.extent)
 
     @property
     def allocated_bytes(self):
         size = 2 if self.dtype == torch.bfloat16 else 4
         scalar = sum(t.numel() for t in (self.predictors or []) + (self.reverses or [])) * size
         faces = size * sum(prod(s) for s in self.grid.face_shapes) if self.face_predictor is not None else 0
-        return scalar + faces + (self.curl.numel() * 4 if self.curl is not None else 0)
+        traces = sum(4 * t.numel() for t in (self.face_trace or [])) + (
+            4 * self.cell_trace.numel() if self.cell_trace is not None else 0)
+        return scalar + faces + traces + (self.curl.numel() * 4 if self.curl is not None else 0)
 
     def _ensure_scalar(self, count):
         if self.predictors is None or len(self.predictors) < count:
@@ -53,7 +61,10 @@ class DetailPasses:
         preds = (C.c_void_p * count)(*[p.data_ptr() for p in self.predictors[:count]])
         revs = (C.c_void_p * count)(*[r.data_ptr() for r in self.reverses[:count]])
         gp, sp, s = C.byref(self._g), C.byref(self._solids), self.device.s
-        self.device.call('ffx_scalar_transport', gp, sp, self._storage, *vel, dt, count, ins, preds, s)
+        if self.reuse_traces and self.cell_trace is None:
+            self.cell_trace = torch.empty(3 * prod(self.grid.shape), dtype=torch.float32, device=self.device.device)
+        trace = ptr(self.cell_trace) if self.reuse_traces else None
+        self.device.call('ffx_scalar_transport_trace', gp, sp, self._storage, *vel, dt, count, ins, preds, trace, s)
         self.device.call('ffx_scalar_transport', gp, sp, self._storage, *vel, -dt, count, preds, revs, s)
         return self.predictors[:count], self.reverses[:count]
 
@@ -65,8 +76,21 @@ class DetailPasses:
         """Predict each signed face component; the reverse sample is fused with the correction."""
         if self.face_predictor is None:
             self.face_predictor = [self.device.texture(s, dtype=self.dtype) for s in self.grid.face_shapes]
-        self.device.call('ffx_face_predictor', C.byref(self._g), C.byref(self._solids), self._storage,
-                         *[ptr(f) for f in fields], dt, *[ptr(p) for p in self.face_predictor], self.device.s)
+        if self.reuse_traces and self._pow2 and self.face_trace is None:
+            self.face_trace = [torch.empty(3 * prod(s), dtype=torch.float32, device=self.device.device)
+                               for s in self.grid.face_shapes]
+        self.device.call('ffx_face_predictor_trace', C.byref(self._g), C.byref(self._solids), self._storage,
+                         *[ptr(f) for f in fields], dt, *[ptr(p) for p in self.face_predictor],
+                         self.face_traces(), self.device.s)
+
+    def face_traces(self):
+        """The face departure points as a C array of three pointers, or NULL."""
+        if not (self.reuse_traces and self._pow2 and self.face_trace is not None):
+            return None
+        return (C.c_void_p * 3)(*[t.data_ptr() for t in self.face_trace])
+
+    def cell_traces(self):
+        return ptr(self.cell_trace) if (self.reuse_traces and self.cell_trace is not None) else None
 
     def confine(self, fields, outputs, dt, strength, limit):
         """Vorticity confinement (``backend/detail.py:39-49``): cell curl
@@ -83,4 +107,5 @@ class DetailPasses:
     def close(self):
         self.predictor = self.reverse = self.predictors = self.reverses = None
         self.face_predictor = None
+        self.face_trace = self.cell_trace = None
         self.curl = None

@@ -208,9 +208,10 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         confine = s.vorticity_strength > 0
         # with confinement the wall condition waits for the projection, as in
         # the reference (confinement reads the provisional, unwalled faces)
-        dev.call('ffx_advect_velocity', gp, sp, self._storage, *vel, *pred, dt, int(corrected_v), s.velocity_blend,
-                 C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift, s.density_weight,
-                 int(not confine), *[ptr(b) for b in proj.bounded], st)
+        dev.call('ffx_advect_velocity_trace', gp, sp, self._storage, *vel, *pred, dt, int(corrected_v),
+                 s.velocity_blend, C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift,
+                 s.density_weight, int(not confine), *[ptr(b) for b in proj.bounded],
+                 self.detail.face_traces() if corrected_v else None, st)
         self._mark('velocity_transport')
         # The old velocity is consumed: the corrected field is written over it.
         if confine:
@@ -241,8 +242,9 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             chans.append(N.FfxScalarChannel(ptr(fields[2]), ptr(preds[2]), ptr(revs[2]), ptr(self.combustion.spare),
                                             s.fuel_source_rate, 0.0, -1.0, 2, 0))
         arr = (N.FfxScalarChannel * len(chans))(*chans)
-        dev.call('ffx_advect_scalars', gp, sp, self._storage, *[ptr(f) for f in self._velocity], dt,
-                 int(corrected_s), C.byref(src), len(chans), arr, ptr(self._maxima), st)
+        dev.call('ffx_advect_scalars_trace', gp, sp, self._storage, *[ptr(f) for f in self._velocity], dt,
+                 int(corrected_s), C.byref(src), len(chans), arr, ptr(self._maxima),
+                 self.detail.cell_traces() if corrected_s else None, st)
         self._mark('scalar_transport')
         self._front, self._back = self._back, self._front
         self._temperature, self._temperature_back = self._temperature_back, self._temperature

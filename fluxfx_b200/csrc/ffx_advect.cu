@@ -112,6 +112,8 @@ struct PredParams {
     Faces<T> F;
     float dt;
     T* out[3];
+    float* dep[3];    // optional: departure points per face grid (three planes of nf floats), for reuse
+    int nf[3];
 };
 
 template <typename T, bool MASK, bool P2>
@@ -137,6 +139,12 @@ __device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, cons
     float value = sample_face(src, f.sx, f.sy, f.sz, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
                                 dv_h<P2>(d, dep.z, 2) - oz);
     Store<T>::st(out, f.i, value);
+    if (float* D = P.dep[f.axis]) {
+        const int nf = P.nf[f.axis];
+        D[f.i] = dep.x;
+        D[f.i + nf] = dep.y;
+        D[f.i + 2 * nf] = dep.z;
+    }
 }
 
 template <typename T, bool MASK, bool P2>
@@ -158,6 +166,8 @@ struct VelParams {
     const T* temperature;
     T* out[3];
     Walls walls;      // wall velocities of the fused wall condition (moving colliders)
+    const float* dep[3];   // optional: the predictor's departure points (reused on power-of-two grids,
+    int nf[3];             // where both passes form the same start point)
     SrcDev src;
 };
 
@@ -176,12 +186,23 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
                 dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
         F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * f.x + (axis != 0), 2 * f.y + (axis != 1),
                                          2 * f.z + (axis != 2));
-        F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
+        // The predictor pass traced the same start point on power-of-two grids
+        // (there (x + o) h and (x + o) e / n are the same exact product), so its
+        // departure point, and in FP32 storage its sample, are this pass's.
+        const bool reuse = P2 && P.corrected && P.dep[axis] != nullptr;
+        F3 dep;
+        if (reuse) {
+            const float* D = P.dep[axis];
+            const int nf = P.nf[axis];
+            dep = {__ldg(D + f.i), __ldg(D + f.i + nf), __ldg(D + f.i + 2 * nf)};
+        } else {
+            dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
+        }
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
         float qx = dv_h<P2>(d, dep.x, 0) - off[0], qy = dv_h<P2>(d, dep.y, 1) - off[1],
               qz = dv_h<P2>(d, dep.z, 2) - off[2];
-        float low = sample_face(orig, f.sx, f.sy, f.sz, qx, qy, qz);
+        float low = (reuse && sizeof(T) == 4) ? Store<T>::ld(pred, f.i) : sample_face(orig, f.sx, f.sy, f.sz, qx, qy, qz);
         value = low;
         if (P.corrected) {
             // correct_velocity_fused.glsl:5-27
@@ -301,6 +322,8 @@ struct ScalarXport {
     int count;
     const T* in[3];
     T* out[3];
+    float* dep;       // optional: departure points (three planes of n floats) for the final pass
+    int n;
 };
 
 template <typename T, bool MASK, bool P2>
@@ -320,6 +343,11 @@ __device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, c
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     for (int c = 0; c < P.count; ++c)
         Store<T>::st(P.out[c], i, sample_closed<T, MASK>(d, P.solid, P.in[c], qx, qy, qz));
+    if (P.dep) {
+        P.dep[i] = dep.x;
+        P.dep[i + P.n] = dep.y;
+        P.dep[i + 2 * P.n] = dep.z;
+    }
 }
 
 template <typename T, bool MASK, bool P2>
@@ -347,6 +375,8 @@ struct ScalarFinal {
     int corrected, count;
     Channel<T> ch[3];
     float* maxima;
+    const float* dep;   // optional: the forward predictor's departure points (same start point, reused)
+    int n;
     SrcDev src;
 };
 
@@ -363,7 +393,12 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
             const float dt = P.dt;
             F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
             F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
-            F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
+            // the forward predictor traced this cell's start point with the same
+            // velocity: its departure point, and in FP32 storage its samples, are this pass's
+            const bool reuse = P.corrected && P.dep != nullptr;
+            F3 dep;
+            if (reuse) dep = {__ldg(P.dep + i), __ldg(P.dep + i + P.n), __ldg(P.dep + i + 2 * P.n)};
+            else dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
             float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
                   qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
             bool ok = false;
@@ -385,7 +420,8 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
             const SrcDev& S = P.src;
             for (int c = 0; c < P.count; ++c) {
                 const Channel<T>& C = P.ch[c];
-                float value = sample_closed<T, MASK>(d, P.solid, C.field, qx, qy, qz);
+                float value = (reuse && sizeof(T) == 4) ? Store<T>::ld(C.pred, i)
+                                                        : sample_closed<T, MASK>(d, P.solid, C.field, qx, qy, qz);
                 if (ok) {
                     float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
                     float lo = fetch_closed(d, C.field, bx, by, bz), hi = lo;
@@ -524,8 +560,9 @@ using namespace ffx;
 
 extern "C" {
 
-int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                       const void* w, float dt, void* pu, void* pv, void* pw, void* stream) {
+int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                             const void* w, float dt, void* pu, void* pv, void* pw, float* const dep[3],
+                             void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && pu && pv && pw,
                 "ffx_face_predictor: invalid arguments");
     FFX_REQUIRE(pu != u && pv != v && pw != w, "ffx_face_predictor: outputs must not alias inputs");
@@ -543,15 +580,25 @@ int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const 
         Q.F = F;
         Q.dt = dt;
         Q.out[0] = (T*)pu; Q.out[1] = (T*)pv; Q.out[2] = (T*)pw;
+        for (int a = 0; a < 3; ++a) {
+            Q.dep[a] = dep ? dep[a] : nullptr;
+            Q.nf[a] = (d.nx + (a == 0)) * (d.ny + (a == 1)) * (d.nz + (a == 2));
+        }
         FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P, (face_predictor_kernel<T, M, P><<<blocks, threads, 0, st>>>(Q)));
     });
     return launch_status("face_predictor_kernel");
 }
 
-int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                        const void* w, const void* pu, const void* pv, const void* pw, float dt, int corrected,
-                        float blend, const FfxSources* src, const void* density, const void* temperature,
-                        float lift, float weight, int apply_walls, void* ou, void* ov, void* ow, void* stream) {
+int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                       const void* w, float dt, void* pu, void* pv, void* pw, void* stream) {
+    return ffx_face_predictor_trace(g, s, storage, u, v, w, dt, pu, pv, pw, nullptr, stream);
+}
+
+int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                              const void* w, const void* pu, const void* pv, const void* pw, float dt,
+                              int corrected, float blend, const FfxSources* src, const void* density,
+                              const void* temperature, float lift, float weight, int apply_walls, void* ou,
+                              void* ov, void* ow, const float* const dep[3], void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && ou && ov && ow,
                 "ffx_advect_velocity: invalid arguments");
     FFX_REQUIRE(!corrected || (pu && pv && pw), "ffx_advect_velocity: MacCormack needs the predictor faces");
@@ -580,12 +627,24 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const
         P.temperature = (const T*)temperature;
         P.out[0] = (T*)ou; P.out[1] = (T*)ov; P.out[2] = (T*)ow;
         P.walls = make_walls(s);
+        for (int a = 0; a < 3; ++a) {
+            P.dep[a] = (dep && corrected) ? dep[a] : nullptr;
+            P.nf[a] = (d.nx + (a == 0)) * (d.ny + (a == 1)) * (d.nz + (a == 2));
+        }
         const float extent[3] = {g->ex, g->ey, g->ez};
         P.src = make_src(src, extent);
         if (!src) P.src.count = 0;
         FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_velocity_kernel<T, M, Q><<<blocks, threads, 0, st>>>(P)));
     });
     return launch_status("advect_velocity_kernel");
+}
+
+int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                        const void* w, const void* pu, const void* pv, const void* pw, float dt, int corrected,
+                        float blend, const FfxSources* src, const void* density, const void* temperature,
+                        float lift, float weight, int apply_walls, void* ou, void* ov, void* ow, void* stream) {
+    return ffx_advect_velocity_trace(g, s, storage, u, v, w, pu, pv, pw, dt, corrected, blend, src, density,
+                                     temperature, lift, weight, apply_walls, ou, ov, ow, nullptr, stream);
 }
 
 int ffx_mac_advect_velocity(const FfxGrid* g, int storage, const void* u, const void* v, const void* w, float dt,
@@ -613,8 +672,9 @@ int ffx_buoyancy(const FfxGrid* g, int storage, const void* w_in, const void* de
     return launch_status("buoyancy_kernel");
 }
 
-int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                         const void* w, float dt, int count, const void* const* in, void* const* out, void* stream) {
+int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                               const void* w, float dt, int count, const void* const* in, void* const* out,
+                               float* dep, void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 && in &&
                 out, "ffx_scalar_transport: invalid arguments");
     for (int c = 0; c < count; ++c)
@@ -634,14 +694,21 @@ int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, cons
             P.in[c] = c < count ? (const T*)in[c] : nullptr;
             P.out[c] = c < count ? (T*)out[c] : nullptr;
         }
+        P.dep = dep;
+        P.n = g->nx * g->ny * g->nz;
         FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (scalar_transport_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
     });
     return launch_status("scalar_transport_kernel");
 }
 
-int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                       const void* w, float dt, int corrected, const FfxSources* src, int count,
-                       const FfxScalarChannel* channels, float* maxima, void* stream) {
+int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                         const void* w, float dt, int count, const void* const* in, void* const* out, void* stream) {
+    return ffx_scalar_transport_trace(g, s, storage, u, v, w, dt, count, in, out, nullptr, stream);
+}
+
+int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                             const void* w, float dt, int corrected, const FfxSources* src, int count,
+                             const FfxScalarChannel* channels, float* maxima, const float* dep, void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 &&
                 channels && src && src->count <= 8, "ffx_advect_scalars: invalid arguments");
     for (int c = 0; c < count; ++c) {
@@ -682,11 +749,20 @@ int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const 
             P.ch[c] = C;
         }
         P.maxima = maxima;
+        P.dep = corrected ? dep : nullptr;
+        P.n = g->nx * g->ny * g->nz;
         const float extent[3] = {g->ex, g->ey, g->ez};
         P.src = make_src(src, extent);
         FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_scalars_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
     });
     return launch_status("advect_scalars_kernel");
+}
+
+int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                       const void* w, float dt, int corrected, const FfxSources* src, int count,
+                       const FfxScalarChannel* channels, float* maxima, void* stream) {
+    return ffx_advect_scalars_trace(g, s, storage, u, v, w, dt, corrected, src, count, channels, maxima, nullptr,
+                                    stream);
 }
 
 int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt, const float base[3], float angular,
@@ -792,6 +868,7 @@ namespace batch {
 size_t predictor_desc(const FfxBatchDomain& D, void* out) {
     if (out) {
         PredParams<float> P;
+        memset(&P, 0, sizeof P);   // no departure output in the batched pass
         P.d = make_dev(D.grid);
         P.solid = D.solid;
         P.halo = D.halo;

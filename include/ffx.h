@@ -118,6 +118,11 @@ int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const v
 int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
                        const void* u, const void* v, const void* w, float dt,
                        void* pu, void* pv, void* pw, void* stream);
+/* The same, also storing each open face's departure point in dep[axis] (three
+ * planes of (nx+a0)(ny+a1)(nz+a2) floats: x, y, z) for ffx_advect_velocity_trace. */
+int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage,
+                             const void* u, const void* v, const void* w, float dt,
+                             void* pu, void* pv, void* pw, float* const dep[3], void* stream);
 /* Velocity transport (SL or MacCormack: corrected != 0, blended by `blend`),
  * emitter coupling, and -- fused -- buoyancy on W from the previous density and
  * temperature (NULL to skip) and the wall condition (apply_walls != 0). Replaces
@@ -130,6 +135,18 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage,
                         float dt, int corrected, float blend, const FfxSources* src,
                         const void* density, const void* temperature, float lift, float weight,
                         int apply_walls, void* ou, void* ov, void* ow, void* stream);
+/* The same, reusing the predictor's departure points `dep` (ffx_face_predictor_trace
+ * of the same faces and dt) instead of tracing again; used on grids whose extent, cell
+ * count and spacing are powers of two, where both passes form the same start point, so
+ * the result is unchanged (and in FP32 storage the semi-Lagrangian sample is the
+ * predictor's value). dep == NULL or other grids: ffx_advect_velocity. */
+int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
+                              const void* u, const void* v, const void* w,
+                              const void* pu, const void* pv, const void* pw,
+                              float dt, int corrected, float blend, const FfxSources* src,
+                              const void* density, const void* temperature, float lift, float weight,
+                              int apply_walls, void* ou, void* ov, void* ow,
+                              const float* const dep[3], void* stream);
 /* Plain face self-advection; replaces shaders/mac_advect_velocity.glsl. */
 int ffx_mac_advect_velocity(const FfxGrid* g, int storage, const void* u, const void* v,
                             const void* w, float dt, void* ou, void* ov, void* ow, void* stream);
@@ -156,6 +173,11 @@ typedef struct FfxScalarChannel {
 int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage,
                          const void* u, const void* v, const void* w, float dt, int count,
                          const void* const* in, void* const* out, void* stream);
+/* The same, also storing each fluid cell's departure point in dep (three planes of
+ * nx*ny*nz floats) for ffx_advect_scalars_trace (use it on the forward, +dt, pass). */
+int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage,
+                               const void* u, const void* v, const void* w, float dt, int count,
+                               const void* const* in, void* const* out, float* dep, void* stream);
 /* Final scalar pass for up to 3 channels: MacCormack correction + clamp,
  * decay, emission. Replaces shaders/closed_advect_scalar.glsl,
  * multi_advect_scalar.glsl, correct_scalar.glsl (backend/projected.py:185-195).
@@ -164,6 +186,13 @@ int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage,
                        const void* u, const void* v, const void* w, float dt, int corrected,
                        const FfxSources* src, int count, const FfxScalarChannel* channels,
                        float* maxima, void* stream);
+/* The same, reusing the forward predictor's departure points (same cells, velocity
+ * and dt: the same start point), so the result is unchanged; in FP32 storage the
+ * semi-Lagrangian samples are the predictor's values. */
+int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage,
+                             const void* u, const void* v, const void* w, float dt, int corrected,
+                             const FfxSources* src, int count, const FfxScalarChannel* channels,
+                             float* maxima, const float* dep, void* stream);
 /* P0.2 open-boundary transport in an analytic flow; replaces shaders/advect.glsl. */
 int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt,
                     const float base[3], float angular, const float center[3], float radius,
