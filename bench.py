@@ -60,12 +60,16 @@ VARIANTS = {
 
 # Algorithmic bytes per cell of each pass (inputs read once, outputs written
 # once; s = bytes per stored velocity/scalar value, masks 1 B each).
-def pass_bytes(s):
+def pass_bytes(s, face_trace=True):
+    """Per cell; the departure points the predictor passes store and the
+    correction passes read are 3 FP32 values per face (3 faces per cell, on
+    power-of-two grids) and per cell."""
+    ft = 36 if face_trace else 0
     return {
-        'velocity_predictor': 3 * s + 2 + 3 * s,                  # U,V,W + solid,halo -> 3 predictor faces
-        'velocity_transport': 3 * s + 3 * s + 2 * s + 2 + 3 * s,  # U,V,W, predictors, rho,T, masks -> faces
-        'scalar_predictor_reverse': 2 * (3 * s + 2 * s + 2 + 2 * s),
-        'scalar_transport': 3 * s + 6 * s + 2 + 2 * s,            # U,V,W, 3 fields x 2 scalars, masks -> 2
+        'velocity_predictor': 3 * s + 2 + 3 * s + ft,             # U,V,W + solid,halo -> 3 predictor faces (+trace)
+        'velocity_transport': 3 * s + 3 * s + 2 * s + 2 + 3 * s + ft,  # U,V,W, predictors, rho,T, masks (+trace) -> faces
+        'scalar_predictor_reverse': 2 * (3 * s + 2 * s + 2 + 2 * s) + 12,
+        'scalar_transport': 3 * s + 6 * s + 2 + 2 * s + 12,       # U,V,W, 3 fields x 2 scalars, masks, trace -> 2
     }
 
 
@@ -330,7 +334,8 @@ def run_b200(args):
     if rank == 0:
         hbm, peak_kind = peaks()
         s = 4 if args.storage == 'FP32' else 2
-        pb = pass_bytes(s)
+        ft = N.grid_pow2((n, n, n), (1.0, 1.0, 1.0))
+        pb = pass_bytes(s, ft)
         pass_report = {}
         for name, ms in passes.items():
             per_step = ms / args.steps
@@ -377,7 +382,7 @@ def run_b200(args):
                             "parameters of the two emitting passes) + the step's density field read back into "
                             "pinned host memory"},
             "gpu_launches": head['launches'],
-            "roofline": roofline(passes, args.steps, cells, s, hbm, peak_kind),
+            "roofline": roofline(passes, args.steps, cells, s, hbm, peak_kind, ft),
             "clocks": clock_info,
         }
         if args.cpu_baseline:
@@ -393,7 +398,7 @@ def run_b200(args):
 MEASURED_TRAFFIC = {(256, 4): 1.237e9}
 
 
-def roofline(passes, steps, cells, s, hbm, peak_kind):
+def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True):
     """The dominant kernel of the step, advect_velocity_kernel (one launch per
     step; its time comes from the events bracketing that launch in the timed
     steps): algorithmic bytes per launch / launch time against the measured
@@ -401,7 +406,7 @@ def roofline(passes, steps, cells, s, hbm, peak_kind):
     (about 2000 instructions per face: three trilinear velocity samples per
     trace, two traces, trace clipping), hence the low fraction."""
     ms = passes.get('velocity_transport', 0.0) / steps
-    per_cell = pass_bytes(s)['velocity_transport']
+    per_cell = pass_bytes(s, face_trace)['velocity_transport']
     achieved = per_cell * cells / (ms / 1e3) / 1e9 if ms else None
     return {"bound": "hbm", "kernel": "advect_velocity_kernel (MacCormack velocity transport + emission + "
                                       "buoyancy + walls, one launch per step)",

@@ -15,6 +15,21 @@ namespace {
 
 constexpr int kThreads = 256;
 
+// Minimum resident blocks per SM asked of the compiler for the transport
+// kernels (register budget vs warps resident to hide the gathers' latency).
+#ifndef FFX_MINB_PREDICTOR
+#define FFX_MINB_PREDICTOR 1
+#endif
+#ifndef FFX_MINB_VELOCITY
+#define FFX_MINB_VELOCITY 1
+#endif
+#ifndef FFX_MINB_SCALAR_PREDICTOR
+#define FFX_MINB_SCALAR_PREDICTOR 1
+#endif
+#ifndef FFX_MINB_SCALARS
+#define FFX_MINB_SCALARS 1
+#endif
+
 __device__ __forceinline__ int floor_int(float v) {
     return (int)fmaxf(fminf(floorf(v), 1.0e9f), -1.0e9f);
 }
@@ -148,7 +163,7 @@ __device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, cons
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) face_predictor_kernel(const __grid_constant__ PredParams<T> P) {
+__global__ void __launch_bounds__(kThreads, FFX_MINB_PREDICTOR) face_predictor_kernel(const __grid_constant__ PredParams<T> P) {
     face_predictor_body<T, MASK, P2>(P, hw_blk());
 }
 
@@ -277,7 +292,7 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
+__global__ void __launch_bounds__(kThreads, FFX_MINB_VELOCITY) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
     advect_velocity_body<T, MASK, P2>(P, hw_blk());
 }
 
@@ -351,7 +366,7 @@ __device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, c
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
+__global__ void __launch_bounds__(kThreads, FFX_MINB_SCALAR_PREDICTOR) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
     scalar_transport_body<T, MASK, P2>(P, hw_blk());
 }
 
@@ -464,7 +479,7 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
+__global__ void __launch_bounds__(kThreads, FFX_MINB_SCALARS) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
     advect_scalars_body<T, MASK, P2>(P, hw_blk());
 }
 
