@@ -16,20 +16,41 @@ namespace {
 constexpr int kThreads = 256;
 
 // Minimum resident blocks per SM asked of the compiler for the transport
-// kernels (register budget vs warps resident to hide the gathers' latency).
+// kernels: the register budget against the warps resident to hide the
+// gathers' latency, chosen by measurement at 256^3 (a build can override
+// each with -DFFX_MINB_<KERNEL>=n; 0 leaves the choice to the compiler).
 #ifndef FFX_MINB_PREDICTOR
-#define FFX_MINB_PREDICTOR 1
+#define FFX_MINB_PREDICTOR 8
 #endif
 #ifndef FFX_MINB_VELOCITY
-#define FFX_MINB_VELOCITY 1
+#define FFX_MINB_VELOCITY 5
 #endif
 #ifndef FFX_MINB_SCALAR_PREDICTOR
-#define FFX_MINB_SCALAR_PREDICTOR 1
+#define FFX_MINB_SCALAR_PREDICTOR 0
 #endif
 #ifndef FFX_MINB_SCALARS
-#define FFX_MINB_SCALARS 1
+#define FFX_MINB_SCALARS 4
 #endif
-
+#if FFX_MINB_PREDICTOR > 0
+#define FFX_LB_PREDICTOR __launch_bounds__(kThreads, FFX_MINB_PREDICTOR)
+#else
+#define FFX_LB_PREDICTOR __launch_bounds__(kThreads)
+#endif
+#if FFX_MINB_VELOCITY > 0
+#define FFX_LB_VELOCITY __launch_bounds__(kThreads, FFX_MINB_VELOCITY)
+#else
+#define FFX_LB_VELOCITY __launch_bounds__(kThreads)
+#endif
+#if FFX_MINB_SCALAR_PREDICTOR > 0
+#define FFX_LB_SCALAR_PREDICTOR __launch_bounds__(kThreads, FFX_MINB_SCALAR_PREDICTOR)
+#else
+#define FFX_LB_SCALAR_PREDICTOR __launch_bounds__(kThreads)
+#endif
+#if FFX_MINB_SCALARS > 0
+#define FFX_LB_SCALARS __launch_bounds__(kThreads, FFX_MINB_SCALARS)
+#else
+#define FFX_LB_SCALARS __launch_bounds__(kThreads)
+#endif
 __device__ __forceinline__ int floor_int(float v) {
     return (int)fmaxf(fminf(floorf(v), 1.0e9f), -1.0e9f);
 }
@@ -163,7 +184,7 @@ __device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, cons
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads, FFX_MINB_PREDICTOR) face_predictor_kernel(const __grid_constant__ PredParams<T> P) {
+__global__ void FFX_LB_PREDICTOR face_predictor_kernel(const __grid_constant__ PredParams<T> P) {
     face_predictor_body<T, MASK, P2>(P, hw_blk());
 }
 
@@ -292,7 +313,7 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads, FFX_MINB_VELOCITY) advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
+__global__ void FFX_LB_VELOCITY advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
     advect_velocity_body<T, MASK, P2>(P, hw_blk());
 }
 
@@ -366,7 +387,7 @@ __device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, c
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads, FFX_MINB_SCALAR_PREDICTOR) scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
+__global__ void FFX_LB_SCALAR_PREDICTOR scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
     scalar_transport_body<T, MASK, P2>(P, hw_blk());
 }
 
@@ -479,7 +500,7 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
 }
 
 template <typename T, bool MASK, bool P2>
-__global__ void __launch_bounds__(kThreads, FFX_MINB_SCALARS) advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
+__global__ void FFX_LB_SCALARS advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
     advect_scalars_body<T, MASK, P2>(P, hw_blk());
 }
 
