@@ -140,6 +140,9 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         try:
             self.solids.update(colliders, dt)
             self.solids.remap(self)
+            refresh = getattr(self.projector, 'refresh_hierarchy', None)
+            if refresh is not None:
+                refresh()            # multigrid with moving colliders (extension): follow the new mask
             self.projector.ready = False
         except Exception:
             self.faulted = True

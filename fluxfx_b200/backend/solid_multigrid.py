@@ -86,22 +86,47 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.residual_kernel = KernelHandle('solid_mg_residual.glsl')
         self.restrict_kernel = KernelHandle('mg_restrict.glsl')
         self.prolong_kernel = KernelHandle('solid_mg_prolong.glsl')
-        shape = tuple(grid.shape)
-        weights = [float(np.float32((n / e) ** 2)) for n, e in zip(shape, grid.extent)]
+        self.pre_sweeps = s.mg_pre_sweeps or 4
+        self.post_sweeps = s.mg_post_sweeps or 4
+        self.last_cycles = 0
+        self.timer = None
+        self.learned = None
+        self.use_graphs = True
+        self.use_tail = True
+        self._build_hierarchy()
+        self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
+
+    def _shapes(self):
+        """Level shapes the grid allows (halving while all dims are even and >= 8)."""
+        s = self.settings
+        shapes = [tuple(self.grid.shape)]
+        while min(shapes[-1]) >= 8 and all(n % 2 == 0 for n in shapes[-1]):
+            if s.mg_max_levels and len(shapes) >= s.mg_max_levels:
+                break
+            shapes.append(tuple(n // 2 for n in shapes[-1]))
+        return shapes
+
+    def _build_hierarchy(self):
+        """Aggregation hierarchy of the current mask (``physics/solid_hierarchy.py:11-54``)
+        built on the device: level-0 links, coarse records level by level (one
+        flag readback each), the coarse pseudoinverse, the single-block tail."""
+        s = self.settings
+        dev = self.device
+        self.levels = []
+        shape = tuple(self.grid.shape)
+        weights = [float(np.float32((n / e) ** 2)) for n, e in zip(shape, self.grid.extent)]
         level0 = N.FfxGraphLevel(*shape, None, ptr(self._mask), N.f3(*weights))
         level0.coarse_scale = s.mg_coarse_scale   # over-correction of the prolongation (1: the reference's)
         # one link byte per cell lets the level-0 passes run four cells per thread
         nx, ny, nz = shape
-        self._links = torch.empty((nz, ny, nx), dtype=torch.uint8, device=dev.device)
+        if getattr(self, '_links', None) is None:
+            self._links = torch.empty((nz, ny, nx), dtype=torch.uint8, device=dev.device)
         dev.call('ffx_graph_links', C.byref(level0), ptr(self._links), dev.s)
         level0.links = self._links.data_ptr()
         self.levels.append(dict(shape=shape, edges=None, graph=level0, p=self.pressure, q=self.spare,
                                 rhs=self.before))
         flag = torch.zeros(1, dtype=torch.int32, device=dev.device)
-        while min(shape) >= 8 and all(n % 2 == 0 for n in shape):
-            if s.mg_max_levels and len(self.levels) >= s.mg_max_levels:
-                break
-            coarse_shape = tuple(n // 2 for n in shape)
+        for coarse_shape in self._shapes()[1:]:
             cx, cy, cz = coarse_shape
             edges = torch.empty((cz, cy, cx, 4), dtype=torch.float32, device=dev.device)
             dev.call('ffx_graph_coarsen', C.byref(self.levels[-1]['graph']), ptr(edges), ptr(flag), dev.s)
@@ -111,24 +136,45 @@ class SolidMultigridProjector(SolidPressureProjector):
             graph.coarse_scale = s.mg_coarse_scale
             self.levels.append(dict(shape=coarse_shape, edges=edges, graph=graph, p=dev.texture(coarse_shape),
                                     q=dev.texture(coarse_shape), rhs=dev.texture(coarse_shape)))
-            shape = coarse_shape
+        self._coarse_solve()
+        self._graphs = {}
+        self._tail, self.tail_start = self._make_tail()
+
+    def _coarse_solve(self):
+        s = self.settings
         self.coarse_matrix = self.coarse_kernel = None
         last = self.levels[-1]
-        n = prod(last['shape'])
-        if n <= DIRECT_LIMIT and s.coarse_solver == 'DIRECT' and len(self.levels) > 1:
+        if prod(last['shape']) <= DIRECT_LIMIT and s.coarse_solver == 'DIRECT' and len(self.levels) > 1:
             inv = graph_pseudoinverse(last['shape'], last['edges'].cpu().numpy())
-            self.coarse_matrix = torch.as_tensor(inv, dtype=torch.float64).to(dev.device)
+            self.coarse_matrix = torch.as_tensor(inv, dtype=torch.float64).to(self.device.device)
             self.coarse_kernel = KernelHandle('solid_mg_direct.glsl')
-        self.pre_sweeps = s.mg_pre_sweeps or 4
-        self.post_sweeps = s.mg_post_sweeps or 4
-        self.last_cycles = 0
-        self.timer = None
-        self.learned = None
-        self.use_graphs = True
-        self._graphs = {}
-        self.use_tail = True
-        self._tail, self.tail_start = self._make_tail()
-        self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
+
+    def refresh_hierarchy(self):
+        """Follow a collider mask that changed in place (moving colliders): the
+        level-0 links and every coarse level's records are recomputed into the
+        same buffers (one pass per level, one flag readback), so captured graphs
+        stay valid; if the coarsening would now stop at another depth, the
+        hierarchy is rebuilt. An extension: the reference keeps masked Jacobi
+        for moving colliders."""
+        dev = self.device
+        shapes = self._shapes()
+        n = len(self.levels)
+        probe = n < len(shapes)           # the hierarchy stopped early: could it go deeper now?
+        flags = torch.zeros(n + 1, dtype=torch.int32, device=dev.device)
+        dev.call('ffx_graph_links', C.byref(self.levels[0]['graph']), ptr(self._links), dev.s)
+        for k in range(1, n):
+            dev.call('ffx_graph_coarsen', C.byref(self.levels[k - 1]['graph']), ptr(self.levels[k]['edges']),
+                     ptr(flags[k:k + 1]), dev.s)
+        if probe:
+            cx, cy, cz = shapes[n]
+            scratch = torch.empty((cz, cy, cx, 4), dtype=torch.float32, device=dev.device)
+            dev.call('ffx_graph_coarsen', C.byref(self.levels[n - 1]['graph']), ptr(scratch), ptr(flags[n:n + 1]),
+                     dev.s)
+        f = flags.cpu().tolist()
+        if any(f[1:n]) or (probe and not f[n]):
+            self._build_hierarchy()
+        elif self.coarse_matrix is not None:
+            self._coarse_solve()
 
     def _make_tail(self):
         """Descriptor of the coarse levels run as one ``ffx_graph_tail`` launch:

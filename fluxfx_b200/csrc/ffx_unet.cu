@@ -382,6 +382,22 @@ __global__ void unpack_channel_kernel(long long voxels, const float* __restrict_
     if (i < voxels) out[i] = src[i * pitch] * scale;
 }
 
+// Coarse collider mask: a coarse cell is solid when at least `threshold` of its
+// eight children are.
+__global__ void mask_restrict_kernel(int cx, int cy, int cz, const uint8_t* __restrict__ fine, int threshold,
+                                     uint8_t* __restrict__ coarse) {
+    const long long c = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (c >= (long long)cx * cy * cz) return;
+    const int x = (int)(c % cx), y = (int)((c / cx) % cy), z = (int)(c / ((long long)cx * cy));
+    const int fx = 2 * cx, fy = 2 * cy;
+    int n = 0;
+    for (int dz = 0; dz < 2; ++dz)
+        for (int dy = 0; dy < 2; ++dy)
+            for (int dx = 0; dx < 2; ++dx)
+                n += fine[(2 * x + dx) + (long long)fx * ((2 * y + dy) + (long long)fy * (2 * z + dz))] != 0;
+    coarse[c] = n >= threshold ? 1 : 0;
+}
+
 __global__ void pack_input_kernel(long long voxels, const float* div, const uint8_t* mask, float scale, bf16* out) {
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= voxels) return;
@@ -563,6 +579,18 @@ int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float 
     FFX_REQUIRE(voxels >= 1 && div && out && ((uintptr_t)out & 15) == 0, "ffx_pack_input: invalid arguments");
     pack_input_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, div, mask, scale, (bf16*)out);
     return launch_status("pack_input_kernel");
+}
+
+int ffx_mask_restrict(const int32_t coarse_n[3], const uint8_t* fine, int32_t threshold, uint8_t* coarse,
+                      void* stream) {
+    FFX_REQUIRE(coarse_n && coarse_n[0] >= 1 && coarse_n[1] >= 1 && coarse_n[2] >= 1 && fine && coarse &&
+                threshold >= 1 && threshold <= 8 &&
+                (int64_t)coarse_n[0] * coarse_n[1] * coarse_n[2] * 8 < (int64_t(1) << 40),
+                "ffx_mask_restrict: invalid arguments");
+    const int64_t n = (int64_t)coarse_n[0] * coarse_n[1] * coarse_n[2];
+    mask_restrict_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(coarse_n[0], coarse_n[1], coarse_n[2],
+                                                                            fine, threshold, coarse);
+    return launch_status("mask_restrict_kernel");
 }
 
 int ffx_unpack_channel(int64_t voxels, const float* src, int32_t pitch, float scale, float* out, void* stream) {

@@ -5,8 +5,10 @@ a projection from its divergence (``projector.before``) and the collider
 mask. Grids up to 128 cells per axis run the network at their own
 resolution; larger grids (dimensions divisible by 16) run it on the 2x2x2
 average of the divergence over a half-resolution grid whose collider mask is
-rasterised at that resolution, and the prediction is prolonged trilinearly.
-Every pass is a library kernel (``ffx_mg_restrict``, ``ffx_max_abs``,
+restricted from the solver's (a coarse cell is solid when at least four of its
+children are, so moving colliders are followed at every guess), and the
+prediction is prolonged trilinearly. Every pass is a library kernel
+(``ffx_mg_restrict``, ``ffx_mask_restrict``, ``ffx_max_abs``,
 ``ffx_pack_input`` + the convolutions, ``ffx_unpack_channel``,
 ``ffx_mg_prolong``); torch only allocates.
 
@@ -35,9 +37,10 @@ def weight_of(shape, extent):
 
 
 class LearnedWarmStart:
+    """``device`` is the solver's device: a ``SolidDevice`` (its ``mask`` is
+    read at every guess) or a plain device (no colliders)."""
+
     def __init__(self, grid, colliders, device, weights=None, net=None):
-        from ..backend.collision import SolidDevice
-        from ..physics.config import GridSpec
         base = getattr(device, 'base', device)
         self.device = base
         self.grid = grid
@@ -46,12 +49,10 @@ class LearnedWarmStart:
         if any(n % 8 for n in shape) or any(n % self.factor for n in grid.shape):
             raise ValueError('the network needs grid dimensions divisible by 8 (by 16 above 128 cells)')
         self.shape = shape
-        coarse = GridSpec(shape, extent=grid.extent, axis_limit=max(128, max(shape)))
-        if colliders:
-            self._solids = SolidDevice(coarse, colliders, base)
-            self.mask = self._solids.mask
+        self.fine_mask = getattr(device, 'mask', None) if colliders else None
+        if self.fine_mask is not None and self.factor == 1:
+            self.mask = self.fine_mask
         else:
-            self._solids = None
             self.mask = torch.zeros(shape[::-1], dtype=torch.uint8, device=base.device)
         self.weight = weight_of(shape, grid.extent)
         self.net = net or UNet(base.device, seed=0)
@@ -73,6 +74,8 @@ class LearnedWarmStart:
         if self.factor > 1:
             dev.call('ffx_mg_restrict', N.n3(*self.grid.shape), ptr(before), ptr(self.div), s)
             src = self.div
+            if self.fine_mask is not None:
+                dev.call('ffx_mask_restrict', N.n3(*self.shape), ptr(self.fine_mask), 4, ptr(self.mask), s)
         dev.call('ffx_max_abs', src.numel(), N.FFX_F32, ptr(src), ptr(self._max), s)
         m = float(self._max.item())
         if m == 0.0:
@@ -89,4 +92,4 @@ class LearnedWarmStart:
 
     def close(self):
         self.net = None
-        self._solids = None
+        self.fine_mask = self.mask = None

@@ -563,6 +563,10 @@ int ffx_adam(int64_t n, float* w, float* m, float* v, const float* g, void* w_bf
 /* Network input, 8 BF16 channels per voxel: scale * div, solid mask, zeros. */
 int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float scale, void* out,
                    void* stream);
+/* Collider mask of the 2x coarser grid (dims coarse_n): 1 where at least `threshold`
+ * of the eight children are nonzero. */
+int ffx_mask_restrict(const int32_t coarse_n[3], const uint8_t* fine, int32_t threshold, uint8_t* coarse,
+                      void* stream);
 /* out[v] = src[v * pitch] * scale: one channel of the FP32 network output as a cell field. */
 int ffx_unpack_channel(int64_t voxels, const float* src, int32_t pitch, float scale, float* out,
                        void* stream);

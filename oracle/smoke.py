@@ -949,18 +949,22 @@ def graph_residual(p, rhs, edges):
     return np.where(diag > 0, rhs - nb + diag * p, p.dtype.type(0))
 
 
-def graph_prolong(p, coarse, edges):
-    """Piecewise-constant injection on active cells (``solid_mg_prolong.glsl``)."""
+def graph_prolong(p, coarse, edges, alpha=1.0):
+    """Piecewise-constant injection on active cells (``solid_mg_prolong.glsl``);
+    ``alpha`` over-corrects (an extension: p + alpha * coarse; 1 is the reference)."""
     up = coarse.repeat(2, 0).repeat(2, 1).repeat(2, 2)[:p.shape[0], :p.shape[1], :p.shape[2]]
+    if alpha != 1.0:
+        up = (p.dtype.type(alpha) * up).astype(p.dtype)
     return np.where(edges[..., 3] > 0, p + up, p.dtype.type(0))
 
 
 class SolidMG:
     """Aggregation V-cycle (``backend/solid_multigrid.py:7-76``)."""
 
-    def __init__(self, levels, pre=4, post=4, coarse_solver='DIRECT', dtype=np.float32):
+    def __init__(self, levels, pre=4, post=4, coarse_solver='DIRECT', dtype=np.float32, alpha=1.0):
         self.levels = levels
         self.pre, self.post = pre, post
+        self.alpha = alpha
         self.dtype = np.dtype(dtype)
         shape, edges = levels[-1]
         self.inverse = None
@@ -986,7 +990,7 @@ class SolidMG:
         r = graph_residual(p, rhs, edges)
         crhs = restrict(r)
         cp = self.cycle(level + 1, np.zeros_like(crhs), crhs)
-        p = graph_prolong(p, cp, edges)
+        p = graph_prolong(p, cp, edges, self.alpha)
         return self.smooth(level, p, rhs, self.post)
 
 

@@ -47,9 +47,18 @@ class OracleProjector:
             self.mg = S.GeometricMG(g, s.mg_pre_sweeps or 3, s.mg_post_sweeps or 3, s.mg_max_levels,
                                     inverse, s.coarse_solver)
         elif kind == 'SOLID_MULTIGRID':
+            self.refresh()
+
+    def refresh(self):
+        """(Re)build the aggregation hierarchy from the grid's current mask (at
+        construction, and after a collider move: the multigrid-with-moving-
+        colliders extension of the fire configuration)."""
+        g, s = self.g, self.s
+        if self.kind == 'SOLID_MULTIGRID':
             hier = S.build_hierarchy(g.shape, g.extent64, g.mask, s.mg_max_levels)
             self.levels = [h[0] for h in hier]
-            self.mg = S.SolidMG(hier, s.mg_pre_sweeps or 4, s.mg_post_sweeps or 4, s.coarse_solver, g.dt)
+            self.mg = S.SolidMG(hier, s.mg_pre_sweeps or 4, s.mg_post_sweeps or 4, s.coarse_solver, g.dt,
+                                getattr(s, 'mg_coarse_scale', 1.0))
 
     @property
     def uses_impulse(self):
@@ -289,6 +298,7 @@ class OracleSmoke:
         g.boundary = F.moving_walls(g, self.owners, table)
         self.colliders = colliders
         g.set_mask(self.owners > 0.5)
+        self.projector.refresh()
         self.density = F.remap_scalar(g, self.density, self.owners, old)
         self.temperature = F.remap_scalar(g, self.temperature, self.owners, old)
         self.velocity = F.remap_faces(g, self.velocity, self.owners, old, g.boundary)
