@@ -567,6 +567,125 @@ def run_batched(args):
 SHAPES_NAMES = ((32, 8), (64, 4), (128, 2), (16, 16))
 
 
+def fire_scene(storage, seed, fast):
+    """The fire configuration: 192 x 192 x 320 cells (cells of 1/192, z up), a
+    fuel emitter of radius 10 cells (fuel 1.0, temperature 0.4), combustion
+    (burn rate 0.75, ignition 0.3, heat yield 1.0, smoke yield 0.5), vorticity
+    confinement 0.3, a sphere collider of radius 20 cells moving +x by half a
+    cell per step; multigrid to relative divergence 1e-4. ``fast``: BF16 or FP32
+    storage as given, warm start, over-correction 1.9, the learned guess for
+    cold starts; otherwise the plain FP32 multigrid (V(4,4) from zero)."""
+    import numpy as np
+    from fluxfx_b200.physics.collision import primitive
+    from fluxfx_b200.physics.config import GridSpec
+    from fluxfx_b200.physics.pressure import PressureSettings
+    shape = (192, 192, 320)
+    h = 1.0 / 192
+    grid = GridSpec(shape, extent=(1.0, 1.0, 320 * h), axis_limit=320)
+    rng = np.random.default_rng(seed)
+    x0 = 0.25 + rng.uniform(-0.02, 0.02)
+    pose = lambda k: (primitive('SPHERE', (x0 + 0.5 * h * k, 0.5, 0.9), (20 * h,) * 3),)
+    cfg = dict(velocity_advection='MACCORMACK', scalar_advection='MACCORMACK', combustion_enabled=True,
+               fuel_source_rate=1.0, heat_source_rate=0.4, heat_mode='TARGET', source_rate=0.0,
+               source_radius=10 * h, source_center=(0.5 + rng.uniform(-0.02, 0.02), 0.5, 0.25),
+               ignition_temperature=0.3, burn_rate=0.75, heat_yield=1.0, smoke_yield=0.5, vorticity_strength=0.3,
+               thermal_lift=1.0, density_weight=0.05, moving_colliders=True, pressure_tolerance=1e-4,
+               pressure_max_cycles=200, storage=storage if fast else 'FP32')
+    if fast:
+        cfg.update(solid_warm_start=True, mg_coarse_scale=1.9, learned_warm_start=True)
+    noise = [rng.uniform(-1e-3, 1e-3, (fs[2], fs[1], fs[0])).astype(np.float32) for fs in grid.face_shapes]
+    return grid, PressureSettings(**cfg), pose, noise
+
+
+def run_fire(args):
+    """Four fire domains stepped in turn on one GPU (the batched plan covers the
+    static-collider step only), fast form against the plain FP32 multigrid form
+    on the same dt sequence; error of the fast fields against the plain ones."""
+    import torch
+    from fluxfx_b200.backend.device import CudaDevice
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
+    from fluxfx_b200.learned import attach
+    device = CudaDevice()
+    domains, steps = 4, args.steps
+    h = 1.0 / 192
+
+    def build(fast):
+        out = []
+        for d in range(domains):
+            grid, settings, pose, noise = fire_scene(args.storage, args.seed + d, fast)
+            s = DenseProjectedSmoke(grid, settings, device, projector_class=SolidMultigridProjector, colliders=pose(0))
+            if fast:
+                attach(s, pose(0))
+            s.upload(torch.zeros(grid.cells))
+            s.upload_temperature(torch.zeros(grid.cells))
+            s.upload_velocity([torch.as_tensor(v) for v in noise])
+            out.append((s, pose))
+        return out
+
+    def run(solvers, dts=None):
+        record = []
+        cycles = 0
+        stream = device.stream
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        for k in range(steps):
+            row = []
+            for d, (s, pose) in enumerate(solvers):
+                dt = dts[k][d] if dts else (record[-1][d] if record else 0.02)
+                s.move_colliders(pose(k + 1), dt)
+                s.step(dt)
+                cycles += s.projector.last_cycles
+                umax = max(s.projector.velocity_maxima())
+                row.append(min(0.02, 0.5 * h / umax) if umax > 0 else 0.02)
+            record.append(row)
+        b.record(stream)
+        torch.cuda.synchronize()
+        used = [[0.02] * domains] + record[:-1] if dts is None else dts
+        return a.elapsed_time(b) / 1e3, cycles / (steps * domains), used
+
+    plain = build(False)
+    p_time, p_cycles, dts = run(plain)
+    fields = [(s.density.float().clone(), s.temperature.float().clone(), s.combustion.fuel.float().clone(),
+               [v.float().clone() for v in s._velocity]) for s, _ in plain]
+    rel = [s.measure_projection()['rel_div_inf'] for s, _ in plain]
+    for s, _ in plain:
+        s.close()
+    fast = build(True)
+    clocks = ClockSampler(torch.cuda.current_device())
+    clocks.start()
+    f_time, f_cycles, _ = run(fast, dts)
+    clock_info = clocks.stop()
+    err = {}
+    for (s, _), (rho, t, fuel, vel) in zip(fast, fields):
+        pairs = (('density', s.density, rho), ('temperature', s.temperature, t), ('fuel', s.combustion.fuel, fuel),
+                 *[(f'velocity_{a}', s._velocity[a], vel[a]) for a in range(3)])
+        for name, got, want in pairs:
+            scale = max(float(want.abs().max()), 1e-30)
+            err[name] = max(err.get(name, 0.0), float((got.float() - want).abs().max()) / scale)
+    f_rel = [s.measure_projection()['rel_div_inf'] for s, _ in fast]
+    for s, _ in fast:
+        s.close()
+    cells = 192 * 192 * 320 * domains
+    line = {
+        "metric": "fire steps/s, 4 domains of 192x192x320 (all domains advance one step)",
+        "value": steps / f_time, "unit": "steps/s", "n_gpus": 1, "steps": steps, "warmup": 0,
+        "ms_per_step": 1e3 * f_time / steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "bf16-storage/f32-math" if args.storage == 'BF16' else "f32", "data": "synthetic",
+        "config": {"workload": "fire: fuel emitter r=10, combustion, confinement 0.3, moving sphere r=20 "
+                               "(+0.5 cells/step), multigrid to rel div 1e-4 after every move, 4 domains in turn",
+                   "fast": f"{args.storage} storage, warm start, over-correction 1.9, learned guess on cold starts",
+                   "cells": cells},
+        "cell_updates_per_s": cells * steps / f_time, "v_cycles_per_domain_step": f_cycles,
+        "plain_fp32_mg": {"steps_per_s": steps / p_time, "v_cycles_per_domain_step": p_cycles,
+                          "final_rel_div_inf_max": max(rel)},
+        "speedup_vs_plain": p_time / f_time, "final_rel_div_inf_max": max(f_rel),
+        "max_rel_error_vs_plain_fp32": err, "clocks": clock_info,
+    }
+    print(json.dumps(line), flush=True)
+
+
 def parse_settings(items):
     """--set name=value pairs as PressureSettings overrides (ints, floats, booleans, strings)."""
     out = {}
@@ -604,13 +723,16 @@ def main():
                     help='settings override of the headline variant (repeatable)')
     ap.add_argument('--coarse-scale', type=float, default=None,
                     help='over-correction factor of the headline variant\'s prolongation (default: the variant\'s)')
-    ap.add_argument('--workload', default='single256', choices=('single256', 'batched48'),
-                    help='single256: the 256^3 collider scene (default); batched48: 48 uneven domains')
+    ap.add_argument('--workload', default='single256', choices=('single256', 'batched48', 'fire'),
+                    help='single256: the 256^3 collider scene (default); batched48: 48 uneven domains; '
+                         'fire: four 192x192x320 fire domains with a moving collider')
     args = ap.parse_args()
     if args.impl == 'reference':
         run_reference(args)
     elif args.workload == 'batched48':
         run_batched(args)
+    elif args.workload == 'fire':
+        run_fire(args)
     else:
         run_b200(args)
 

@@ -184,7 +184,9 @@ class SolidMultigridProjector(SolidPressureProjector):
         if (self.pre_sweeps + self.post_sweeps) % 2 or len(self.levels) < 3:
             return None, None
         start = next((k for k in range(1, len(self.levels)) if prod(self.levels[k]['shape']) <= TAIL_CELLS), None)
-        if start is None or start == len(self.levels) - 1:
+        if start is None or (start == len(self.levels) - 1 and self.coarse_matrix is not None):
+            # (a coarsest level alone is worth a launch only for its 80 sweeps; a
+            # direct solve is one launch already)
             return None, None
         start = max(start, len(self.levels) - N.TAIL_LEVELS)
         tail = N.FfxGraphTail()

@@ -196,7 +196,7 @@ bool domain_ok(const FfxBatchDomain& D, int i, int D_first_pre, int D_first_post
     if (D.inverse && cells_of(D.level[last].level) > 1024)
         return fail(FFX_ERR_INVALID, "ffx_batch: domain %d: direct solve limited to 1024 cells", i), false;
     if (D.tail_start >= 0) {
-        if (D.tail_start < 1 || D.tail_start >= last || D.levels - D.tail_start > FFX_TAIL_LEVELS)
+        if (D.tail_start < 1 || D.tail_start > last || D.levels - D.tail_start > FFX_TAIL_LEVELS)
             return fail(FFX_ERR_INVALID, "ffx_batch: domain %d: tail start", i), false;
         for (int k = D.tail_start; k < D.levels; ++k)
             if (cells_of(D.level[k].level) > 32768)
