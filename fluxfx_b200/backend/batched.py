@@ -136,6 +136,19 @@ class BatchedSmoke:
         D.max_cycles = st.pressure_max_cycles
         D.warm_start = int(st.solid_warm_start)
         D.tolerance = st.pressure_tolerance
+        # departure points of the predictor passes, reused by the correction passes
+        # (faces on power-of-two grids only), as the single-domain step does
+        dev = s.device.device
+        if D.velocity_corrected and det.reuse_traces and det._pow2:
+            if det.face_trace is None:
+                det.face_trace = [torch.empty(3 * prod(sh), dtype=torch.float32, device=dev)
+                                  for sh in s.grid.face_shapes]
+            for a in range(3):
+                D.face_trace[a] = det.face_trace[a].data_ptr()
+        if D.scalar_corrected and det.reuse_traces:
+            if det.cell_trace is None:
+                det.cell_trace = torch.empty(3 * prod(s.grid.shape), dtype=torch.float32, device=dev)
+            D.cell_trace = det.cell_trace.data_ptr()
 
     # ------------------------------------------------------------ running
     @property

@@ -844,6 +844,33 @@ int ffx_mac_advect_density(const FfxGrid* g, int storage, const void* u, const v
 namespace ffx {
 namespace {
 
+// Occupancy targets of the batched transport kernels (their loops carry both
+// the power-of-two and the general body; 0: the compiler's choice).
+#ifndef FFX_MINB_BATCH_PREDICTOR
+#define FFX_MINB_BATCH_PREDICTOR 0
+#endif
+#ifndef FFX_MINB_BATCH_VELOCITY
+#define FFX_MINB_BATCH_VELOCITY 0
+#endif
+#ifndef FFX_MINB_BATCH_SCALARS
+#define FFX_MINB_BATCH_SCALARS 0
+#endif
+#if FFX_MINB_BATCH_PREDICTOR > 0
+#define FFX_LB_BATCH_PREDICTOR __launch_bounds__(kBatchThreads, FFX_MINB_BATCH_PREDICTOR)
+#else
+#define FFX_LB_BATCH_PREDICTOR __launch_bounds__(kBatchThreads)
+#endif
+#if FFX_MINB_BATCH_VELOCITY > 0
+#define FFX_LB_BATCH_VELOCITY __launch_bounds__(kBatchThreads, FFX_MINB_BATCH_VELOCITY)
+#else
+#define FFX_LB_BATCH_VELOCITY __launch_bounds__(kBatchThreads)
+#endif
+#if FFX_MINB_BATCH_SCALARS > 0
+#define FFX_LB_BATCH_SCALARS __launch_bounds__(kBatchThreads, FFX_MINB_BATCH_SCALARS)
+#else
+#define FFX_LB_BATCH_SCALARS __launch_bounds__(kBatchThreads)
+#endif
+
 // prep: the descriptor's time step is the domain's device dt (times `sign`).
 struct DeviceDt {
     const BatchState* state;
@@ -852,7 +879,7 @@ struct DeviceDt {
     __device__ __forceinline__ void operator()(D& sh, int slot) const { sh.dt = sign * state[slot].dt; }
 };
 
-__global__ void __launch_bounds__(kBatchThreads) batch_predictor_kernel(const __grid_constant__ BatchMap M,
+__global__ void FFX_LB_BATCH_PREDICTOR batch_predictor_kernel(const __grid_constant__ BatchMap M,
                                                                         const PredParams<float>* descs,
                                                                         const BatchState* state) {
     for_tiles(M, descs, state, false, DeviceDt{state, 1.f}, [](const PredParams<float>& P, const Blk& b, int) {
@@ -861,7 +888,7 @@ __global__ void __launch_bounds__(kBatchThreads) batch_predictor_kernel(const __
     });
 }
 
-__global__ void __launch_bounds__(kBatchThreads) batch_velocity_kernel(const __grid_constant__ BatchMap M,
+__global__ void FFX_LB_BATCH_VELOCITY batch_velocity_kernel(const __grid_constant__ BatchMap M,
                                                                        const VelParams<float>* descs,
                                                                        const BatchState* state) {
     for_tiles(M, descs, state, false, DeviceDt{state, 1.f}, [](const VelParams<float>& P, const Blk& b, int) {
@@ -879,7 +906,7 @@ __global__ void __launch_bounds__(kBatchThreads) batch_scalar_transport_kernel(c
     });
 }
 
-__global__ void __launch_bounds__(kBatchThreads) batch_scalars_kernel(const __grid_constant__ BatchMap M,
+__global__ void FFX_LB_BATCH_SCALARS batch_scalars_kernel(const __grid_constant__ BatchMap M,
                                                                       const ScalarFinal<float>* descs,
                                                                       const BatchState* state) {
     for_tiles(M, descs, state, false, DeviceDt{state, 1.f}, [](const ScalarFinal<float>& P, const Blk& b, int) {
@@ -911,6 +938,11 @@ size_t predictor_desc(const FfxBatchDomain& D, void* out) {
         P.F = {D.u, D.v, D.w};
         P.dt = 0.f;
         P.out[0] = D.pu; P.out[1] = D.pv; P.out[2] = D.pw;
+        const int nx = D.grid.nx, ny = D.grid.ny, nz = D.grid.nz;
+        for (int a = 0; a < 3; ++a) {
+            P.dep[a] = D.face_trace[a];
+            P.nf[a] = (nx + (a == 0)) * (ny + (a == 1)) * (nz + (a == 2));
+        }
         memcpy(out, &P, sizeof P);
     }
     return sizeof(PredParams<float>);
@@ -935,6 +967,11 @@ size_t velocity_desc(const FfxBatchDomain& D, int parity, void* out) {
         P.temperature = D.temperature[parity];
         P.out[0] = D.bu; P.out[1] = D.bv; P.out[2] = D.bw;
         P.walls = make_walls(nullptr);
+        const int nx = D.grid.nx, ny = D.grid.ny, nz = D.grid.nz;
+        for (int a = 0; a < 3; ++a) {
+            P.dep[a] = D.velocity_corrected ? D.face_trace[a] : nullptr;
+            P.nf[a] = (nx + (a == 0)) * (ny + (a == 1)) * (nz + (a == 2));
+        }
         const float extent[3] = {D.grid.ex, D.grid.ey, D.grid.ez};
         P.src = make_src(&D.sources, extent);
         memcpy(out, &P, sizeof P);
@@ -956,6 +993,8 @@ size_t scalar_xport_desc(const FfxBatchDomain& D, int parity, int reverse, void*
         P.in[1] = reverse ? D.predictor[1] : D.temperature[parity];
         P.out[0] = reverse ? D.reverse[0] : D.predictor[0];
         P.out[1] = reverse ? D.reverse[1] : D.predictor[1];
+        P.dep = reverse ? nullptr : D.cell_trace;     // the forward pass stores its departure points
+        P.n = D.grid.nx * D.grid.ny * D.grid.nz;
         memcpy(out, &P, sizeof P);
     }
     return sizeof(ScalarXport<float>);
@@ -989,6 +1028,8 @@ size_t scalar_final_desc(const FfxBatchDomain& D, int parity, void* out) {
             P.ch[c] = C;
         }
         P.maxima = nullptr;
+        P.dep = D.scalar_corrected ? D.cell_trace : nullptr;
+        P.n = D.grid.nx * D.grid.ny * D.grid.nz;
         const float extent[3] = {D.grid.ex, D.grid.ey, D.grid.ez};
         P.src = make_src(&D.sources, extent);
         memcpy(out, &P, sizeof P);

@@ -478,6 +478,11 @@ typedef struct FfxBatchDomain {
     int32_t warm_start;                /* 1: start each solve from the previous step's pressure scaled by
                                           dt / previous dt (backend/pressure.py:63-75), 0: from zero */
     double tolerance;                  /* relative max-norm residual target (> 0) */
+    float* face_trace[3];              /* optional departure points of the face predictor (three planes
+                                          per face grid; power-of-two grids only), reused by the
+                                          velocity pass as in ffx_advect_velocity_trace */
+    float* cell_trace;                 /* optional departure points of the scalar predictor (three
+                                          planes of cells), reused by the final scalar pass */
 } FfxBatchDomain;
 typedef struct FfxBatchStats {
     float dt, last_dt;                 /* dt of the next step, of the last step */
