@@ -169,6 +169,8 @@ _PROTOTYPES = {
     'ffx_graph_links': (C.c_int, [P(FfxGraphLevel), vp, vp]),
     'ffx_graph_tail': (C.c_int, [P(FfxGraphTail), vp]),
     'ffx_conv_forward': (C.c_int, [P(FfxConv), vp]),
+    'ffx_conv_forward_tc': (C.c_int, [P(FfxConv), vp]),
+    'ffx_conv_timeouts': (C.c_int, [P(i32), i32]),
     'ffx_conv_weight_grad': (C.c_int, [P(FfxConv), vp, i32, vp, vp]),
     'ffx_relu_backward': (C.c_int, [i64, i32, vp, i32, vp, i32, i32, vp]),
     'ffx_bias_grad': (C.c_int, [i64, i32, vp, i32, vp, vp]),

@@ -239,6 +239,212 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_con
         }
 }
 
+// ------------------------------------------------- forward GEMM, tcgen05
+// The same implicit GEMM on the 5th-generation tensor cores: one elected
+// thread issues tcgen05.mma (kind::f16, M = 128, N = BN, K = 16, BF16 in, FP32
+// accumulated in tensor memory) from shared-memory operand descriptors, the
+// accumulator tile lives in TMEM for the whole reduction, and the epilogue
+// reads it back with tcgen05.ld (one row per thread). Operands are staged by
+// cp.async in the canonical no-swizzle core-matrix layouts: A (voxels x k)
+// K-major, 8 rows x 16 B per core matrix; B (k x channels) MN-major straight
+// from the [k][cout] weights, 8 k-rows x 8 channels per core matrix. A stage
+// holds K = 32 (two MMAs); a single mbarrier tracks MMA completion through
+// tcgen05.commit. Every wait is bounded: on timeout the kernel records it in
+// g_conv_timeouts, stops issuing, and still frees its TMEM.
+__device__ int g_conv_timeouts;
+
+constexpr int kTcStages = 3;
+constexpr int kTcStageK = 32;                    // two MMA k-steps of 16
+constexpr int kTcSpin = 1 << 22;                 // bounded mbarrier polling
+
+__device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+// Shared-memory matrix descriptor (no swizzle): start, leading- and stride-
+// dimension byte offsets (16-byte units), descriptor version 1.
+__device__ __forceinline__ uint64_t umma_desc(uint32_t addr, uint32_t lbo, uint32_t sbo) {
+    uint64_t d = 0;
+    d |= (uint64_t)((addr >> 4) & 0x3FFF);
+    d |= (uint64_t)((lbo >> 4) & 0x3FFF) << 16;
+    d |= (uint64_t)((sbo >> 4) & 0x3FFF) << 32;
+    d |= (uint64_t)1 << 46;                      // version
+    return d;                                    // base offset 0, layout type 0 (no swizzle)
+}
+
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
+    for (int i = 0; i < kTcSpin; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_constant__ Conv a) {
+    static_assert(BN == 16 || BN == 32 || BN == 64, "BN");
+    constexpr int kAStep = kBM * 16 * 2;             // bytes of A per MMA k-step (128 rows x 16 k)
+    constexpr int kBStep = 16 * BN * 2;              // bytes of B per MMA k-step (16 k x BN)
+    constexpr int kTmemCols = BN < 32 ? 32 : BN;
+    __shared__ __align__(128) unsigned char sA[kTcStages][2 * kAStep];
+    __shared__ __align__(128) unsigned char sB[kTcStages][2 * kBStep];
+    __shared__ __align__(8) uint64_t mbar;
+    __shared__ uint32_t tmem_base;
+    __shared__ int abort_flag;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    const long long m0 = (long long)blockIdx.x * kBM;
+    const int n0 = blockIdx.y * BN;
+    const int cls = blockIdx.z;
+    const bf16* W = a.w + (a.transposed ? (size_t)cls * a.cin * a.cout : 0);
+    const long long my_row = m0 + tid;
+    const bool row_ok = my_row < a.rows;
+    const RowPos pos = row_ok ? (a.transposed ? decode(my_row, a.id, a.ih, a.iw) : decode(my_row, a.od, a.oh, a.ow))
+                              : RowPos{0, 0, 0, 0};
+    const int k_elems = a.k_units * 8;
+    const int nk = (a.k_units + 3) / 4;              // stages of 4 units (K = 32)
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(kTmemCols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (tid == 0) {
+        abort_flag = 0;
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+    const uint32_t bar = smem_u32(&mbar);
+
+    // A: row `tid`, units u (8 channels) of the stage -> core (row/8, chunk)
+    // B: k-row r (0..31) x channel chunk h (BN/8) -> MN-major core matrices
+    auto load = [&](int stage, int kstep) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const int u = kstep * 4 + c;
+            const bf16* src = (row_ok && u < a.k_units) ? gather(a, pos, u) : nullptr;
+            unsigned char* dst = sA[stage] + (c >> 1) * kAStep + (tid >> 3) * 256 + (c & 1) * 128 + (tid & 7) * 16;
+            cp_async16(dst, src ? src : a.in1.p, src != nullptr);
+        }
+        constexpr int kBLoads = kTcStageK * (BN / 8);       // 16-byte chunks of B per stage
+        for (int q = tid; q < kBLoads; q += kGemmThreads) {
+            const int r = q / (BN / 8), h = q % (BN / 8);
+            const int k = kstep * kTcStageK + r, n = n0 + h * 8;
+            const bool ok = k < k_elems && n < a.cout;
+            unsigned char* dst = sB[stage] + (r >> 4) * kBStep + h * 256 + ((r & 15) >> 3) * 128 + (r & 7) * 16;
+            cp_async16(dst, ok ? W + (size_t)k * a.cout + n : W, ok);
+        }
+    };
+    // kind::f16, D = F32, A = B = BF16, A K-major, B MN-major, N = BN, M = 128
+    const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(BN >> 3) << 17) |
+                           ((uint32_t)(kBM >> 4) << 24);
+
+#pragma unroll
+    for (int st = 0; st < kTcStages - 1; ++st) {
+        if (st < nk) load(st, st);
+        cp_async_commit();
+    }
+    bool ok = true;
+    for (int ks = 0; ks < nk && ok; ++ks) {
+        // the MMAs of the previous stage read the buffer the prefetch overwrites
+        if (ks > 0) {
+            if (!mbar_wait(bar, (uint32_t)((ks - 1) & 1))) ok = false;
+            if (__syncthreads_or(!ok)) { ok = false; break; }
+        }
+        const int pf = ks + kTcStages - 1;
+        if (pf < nk) load(pf % kTcStages, pf);
+        cp_async_commit();
+        cp_async_wait<kTcStages - 1>();
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (tid == 0) {
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const int st = ks % kTcStages;
+#pragma unroll
+            for (int j = 0; j < 2; ++j) {
+                const uint64_t da = umma_desc(smem_u32(sA[st] + j * kAStep), 128, 256);
+                const uint64_t db = umma_desc(smem_u32(sB[st] + j * kBStep), 128, 256);
+                const uint32_t acc = (ks > 0 || j > 0) ? 1u : 0u;
+                asm volatile(
+                    "{\n\t.reg .pred p;\n\t"
+                    "setp.ne.b32 p, %4, 0;\n\t"
+                    "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
+                    ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u));
+            }
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar));
+        }
+    }
+    cp_async_wait<0>();
+    // the last commit covers every MMA issued
+    if (ok && nk > 0 && !mbar_wait(bar, (uint32_t)((nk - 1) & 1))) ok = false;
+    if (!ok && tid == 0) atomicAdd(&g_conv_timeouts, 1);
+    if (__syncthreads_or(!ok)) {
+        // give MMAs possibly still in flight a bounded grace period before freeing TMEM
+        if (nk > 0) mbar_wait(bar, (uint32_t)((nk - 1) & 1));
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        // epilogue: warp w holds TMEM lanes 32w..32w+31 = rows of the tile
+        const long long m = m0 + warp * 32 + lane;
+        const uint32_t taddr = tmem + ((uint32_t)(warp * 32) << 16);
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(taddr + (uint32_t)c0));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (m < a.rows) {
+                const long long vox = out_voxel(a, m, cls);
+#pragma unroll
+                for (int e = 0; e < 16; e += 2) {
+                    const int n = n0 + c0 + e;
+                    if (n >= a.cout) continue;
+                    float v0 = __uint_as_float(r[e]), v1 = __uint_as_float(r[e + 1]);
+                    if (a.bias) {
+                        v0 += a.bias[n];
+                        v1 += a.bias[n + 1];
+                    }
+                    if (a.relu) {
+                        v0 = fmaxf(v0, 0.f);
+                        v1 = fmaxf(v1, 0.f);
+                    }
+                    if (a.out) {
+                        __nv_bfloat162* o =
+                            reinterpret_cast<__nv_bfloat162*>(a.out + vox * a.out_pitch + a.out_offset + n);
+                        if (a.accumulate) {
+                            const float2 prev = __bfloat1622float2(*o);
+                            v0 += prev.x;
+                            v1 += prev.y;
+                        }
+                        *o = __floats2bfloat162_rn(v0, v1);
+                    }
+                    if (a.out_f32) {
+                        float* o = a.out_f32 + vox * a.out_f32_pitch + n;
+                        o[0] = v0;
+                        o[1] = v1;
+                    }
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
+}
+
 // ------------------------------------------------------ weight gradient GEMM
 // dW[k][n] += sum over the block's voxel chunk of A[m][k] G[m][n]; A^T
 // fragments come from the [m][k] tile through ldmatrix.trans.
@@ -521,6 +727,31 @@ int ffx_conv_forward(const FfxConv* c, void* stream) {
     else if (bn == 32) conv_fwd_kernel<32><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
     else conv_fwd_kernel<64><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
     return launch_status("conv_fwd_kernel");
+}
+
+int ffx_conv_forward_tc(const FfxConv* c, void* stream) {
+    Conv a;
+    int e = make_conv(c, a);
+    if (e) return e;
+    FFX_REQUIRE(a.out || a.out_f32, "ffx_conv_forward_tc: no output");
+    const int bn = a.cout <= 16 ? 16 : (a.cout <= 32 ? 32 : 64);
+    const dim3 grid((unsigned)((a.rows + kBM - 1) / kBM), (unsigned)((a.cout + bn - 1) / bn), a.transposed ? 8 : 1);
+    FFX_REQUIRE(grid.x < (1u << 31), "ffx_conv_forward_tc: grid too large");
+    if (bn == 16) conv_fwd_tc_kernel<16><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    else if (bn == 32) conv_fwd_tc_kernel<32><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    else conv_fwd_tc_kernel<64><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    return launch_status("conv_fwd_tc_kernel");
+}
+
+int ffx_conv_timeouts(int32_t* out, int32_t reset) {
+    FFX_REQUIRE(out, "ffx_conv_timeouts: invalid arguments");
+    int e = cuda_status(cudaMemcpyFromSymbol(out, g_conv_timeouts, sizeof(int32_t)), "ffx_conv_timeouts: read");
+    if (e) return e;
+    if (reset) {
+        const int32_t zero = 0;
+        e = cuda_status(cudaMemcpyToSymbol(g_conv_timeouts, &zero, sizeof(int32_t)), "ffx_conv_timeouts: reset");
+    }
+    return e;
 }
 
 int ffx_conv_weight_grad(const FfxConv* c, const void* grad, int32_t grad_pitch, float* dweight, void* stream) {

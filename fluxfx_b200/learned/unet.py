@@ -83,6 +83,9 @@ class UNet:
         self.by_name = {l.name: l for l in self.layers}
         self.shape = None
         self.step_count = 0
+        # forward and data-gradient convolutions: tcgen05 (accumulator in tensor
+        # memory) or the mma.sync form
+        self.conv_entry = 'ffx_conv_forward_tc'
 
     # ------------------------------------------------------------- buffers
     def _buffers(self, batch, dims):
@@ -196,7 +199,7 @@ class UNet:
                 c = self._conv(layer, lin, ins[0], lout, None, 0, 0, out_f32=self.pred, f32_pitch=HEAD_CHANNELS)
             else:
                 c = self._conv(layer, lin, ins[0], lout, out, pitch, offset)
-            self._call('ffx_conv_forward', C.byref(c), s)
+            self._call(self.conv_entry, C.byref(c), s)
         return self.pred[..., 0]
 
     def activation(self, name):
@@ -261,7 +264,7 @@ class UNet:
             else:   # up: its data gradient is a 2^3 stride-2 convolution of the fine gradient
                 c = self._conv(layer, lout, g_view, lin, gin, ipitch, ioff, weight=layer.wt16, transposed=0,
                                ks=2, stride=2, pad=0, cout=layer.cin, bias=False, relu=False)
-            self._call('ffx_conv_forward', C.byref(c), s)
+            self._call(self.conv_entry, C.byref(c), s)
         return self.loss_acc
 
     def _voxels(self, level):
@@ -311,9 +314,12 @@ def main():
     ap.add_argument('--batch', type=int, default=1)
     ap.add_argument('--repeat', type=int, default=5)
     ap.add_argument('--train', action='store_true', help='also time forward + backward + Adam')
+    ap.add_argument('--mma-sync', action='store_true', help='the mma.sync convolutions instead of tcgen05')
     args = ap.parse_args()
     dev = torch.device('cuda')
     net = UNet(dev, seed=0)
+    if args.mma_sync:
+        net.conv_entry = 'ffx_conv_forward'
     g = torch.Generator(device='cuda').manual_seed(0)
     n = args.size
     div = torch.randn((args.batch, n, n, n), device=dev, generator=g)

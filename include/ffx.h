@@ -548,6 +548,12 @@ typedef struct FfxConv {
 } FfxConv;
 /* Convolution as an implicit GEMM on the BF16 tensor cores (FP32 accumulation). */
 int ffx_conv_forward(const FfxConv* conv, void* stream);
+/* The same on the 5th-generation tensor cores (tcgen05.mma, accumulator in tensor
+ * memory, bounded completion waits). */
+int ffx_conv_forward_tc(const FfxConv* conv, void* stream);
+/* Number of tcgen05 convolution launches that gave up waiting (synchronous; reset != 0
+ * clears it). */
+int ffx_conv_timeouts(int32_t* out, int32_t reset);
 /* dweight[k][cout] += sum over output voxels of input(k) * grad (FP32, caller zeroes);
  * `grad` is the BF16 gradient of the convolution's output (ReLU already applied). */
 int ffx_conv_weight_grad(const FfxConv* conv, const void* grad, int32_t grad_pitch, float* dweight,

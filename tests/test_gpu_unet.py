@@ -95,6 +95,48 @@ def test_convolution_forms_match_torch(lib, kind):
     assert float(out16[..., :8].abs().max()) == 0 and float(out16[..., 8 + cout:].abs().max()) == 0
 
 
+@pytest.mark.parametrize('entry', ['ffx_conv_forward', 'ffx_conv_forward_tc'])
+@pytest.mark.parametrize('kind', ['conv3', 'conv3_concat', 'down', 'up', 'head', 'wide'])
+def test_forward_entries_match_torch(lib, kind, entry):
+    """Both forward implementations (mma.sync and tcgen05 with the accumulator
+    in tensor memory) against torch FP64 on the same BF16 values, for every
+    form and each output tile width (16, 32, 64 channels; 'wide' spans two
+    column tiles), with a ragged voxel count."""
+    g = torch.Generator().manual_seed(11)
+    B, D, H, W = 1, 6, 10, 12          # 720 voxels: not a multiple of the 128-row tile
+    c1, c2, cout = {'conv3': (16, 0, 16), 'conv3_concat': (16, 16, 32), 'down': (32, 0, 64), 'up': (64, 0, 32),
+                    'head': (16, 0, 8), 'wide': (24, 0, 72)}[kind]
+    cin = c1 + c2
+    ind = (D // 2, H // 2, W // 2) if kind == 'up' else (D, H, W)
+    outd = {'down': (D // 2, H // 2, W // 2), 'up': (D, H, W)}.get(kind, (D, H, W))
+    taps = {'down': 8, 'up': 8, 'head': 1}.get(kind, 27)
+    x1 = bf(torch.randn((B, *ind, c1), generator=g))
+    x2 = bf(torch.randn((B, *ind, c2), generator=g)) if c2 else None
+    w = bf(torch.randn((taps, cin, cout), generator=g) / (taps * cin) ** 0.5)
+    bias = torch.randn(cout, generator=g)
+    dx1, dx2, dw, db = x1.cuda(), (x2.cuda() if x2 is not None else None), w.cuda(), bias.cuda()
+    out32 = torch.zeros((B, *outd, cout), device='cuda')
+    ks, stride, pad = {'down': (2, 2, 0), 'up': (2, 2, 0), 'head': (1, 1, 0)}.get(kind, (3, 1, 1))
+    c = conv_struct(B, ind, outd, c1, c2, cout, ks, stride, pad, int(kind == 'up'), dx1, c1, 0, dx2, c2, 0, dw,
+                    db, 0, None, 0, 0, out32, cout)
+    N.check(getattr(lib, entry)(C.byref(c), None))
+    torch.cuda.synchronize()
+    count = C.c_int32(0)
+    N.check(lib.ffx_conv_timeouts(C.byref(count), 1))
+    assert count.value == 0
+    xin = x1.double()
+    if x2 is not None:
+        xin = torch.cat([xin, x2.double()], -1)
+    xt = xin.permute(0, 4, 1, 2, 3)
+    wt = U.torch_weight('up' if kind == 'up' else {'head': 'head', 'down': 'down'}.get(kind, 'conv3'), w.double())
+    if kind == 'up':
+        ref = F.conv_transpose3d(xt, wt, bias.double(), stride=2)
+    else:
+        ref = F.conv3d(xt, wt, bias.double(), stride=stride, padding=pad)
+    ref = ref.permute(0, 2, 3, 4, 1)
+    assert rel_err(out32, ref) < 1e-5, rel_err(out32, ref)
+
+
 @pytest.mark.parametrize('kind', ['conv3', 'down', 'up'])
 def test_weight_gradients_match_torch(lib, kind):
     g = torch.Generator().manual_seed(2)
