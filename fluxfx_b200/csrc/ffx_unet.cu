@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_con
 // g_conv_timeouts, stops issuing, and still frees its TMEM.
 __device__ int g_conv_timeouts;
 
-constexpr int kTcStages = 3;
+constexpr int kTcStages = 4;                     // ring of operand stages; loads run two ahead
 constexpr int kTcStageK = 32;                    // two MMA k-steps of 16
 constexpr int kTcSpin = 1 << 22;                 // bounded mbarrier polling
 
@@ -286,14 +286,19 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
 }
 
 template <int BN>
+constexpr int tc_smem_bytes() { return kTcStages * (2 * kBM * 16 * 2 + 2 * 16 * BN * 2); }
+
+template <int BN>
 __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_constant__ Conv a) {
     static_assert(BN == 16 || BN == 32 || BN == 64, "BN");
     constexpr int kAStep = kBM * 16 * 2;             // bytes of A per MMA k-step (128 rows x 16 k)
     constexpr int kBStep = 16 * BN * 2;              // bytes of B per MMA k-step (16 k x BN)
     constexpr int kTmemCols = BN < 32 ? 32 : BN;
-    __shared__ __align__(128) unsigned char sA[kTcStages][2 * kAStep];
-    __shared__ __align__(128) unsigned char sB[kTcStages][2 * kBStep];
-    __shared__ __align__(8) uint64_t mbar;
+    extern __shared__ __align__(128) unsigned char tc_smem[];
+    unsigned char (*sA)[2 * kAStep] = reinterpret_cast<unsigned char (*)[2 * kAStep]>(tc_smem);
+    unsigned char (*sB)[2 * kBStep] =
+        reinterpret_cast<unsigned char (*)[2 * kBStep]>(tc_smem + kTcStages * 2 * kAStep);
+    __shared__ __align__(8) uint64_t mbar[kTcStages];   // one per stage: its MMAs completed
     __shared__ uint32_t tmem_base;
     __shared__ int abort_flag;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
@@ -315,14 +320,14 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
     }
     if (tid == 0) {
         abort_flag = 0;
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar)));
+        for (int st = 0; st < kTcStages; ++st)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&mbar[st])));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
-    const uint32_t bar = smem_u32(&mbar);
 
     // A: row `tid`, units u (8 channels) of the stage -> core (row/8, chunk)
     // B: k-row r (0..31) x channel chunk h (BN/8) -> MN-major core matrices
@@ -347,22 +352,25 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(kBM >> 4) << 24);
 
+    constexpr int kAhead = 2;                         // stages loaded ahead of the MMAs
 #pragma unroll
-    for (int st = 0; st < kTcStages - 1; ++st) {
+    for (int st = 0; st < kAhead; ++st) {
         if (st < nk) load(st, st);
         cp_async_commit();
     }
     bool ok = true;
     for (int ks = 0; ks < nk && ok; ++ks) {
-        // the MMAs of the previous stage read the buffer the prefetch overwrites
-        if (ks > 0) {
-            if (!mbar_wait(bar, (uint32_t)((ks - 1) & 1))) ok = false;
-            if (__syncthreads_or(!ok)) { ok = false; break; }
+        // the prefetch overwrites the stage whose MMAs were issued two iterations ago:
+        // wait for that stage's use (kTcStages - kAhead = 2 MMA groups may stay in flight)
+        const int pf = ks + kAhead;
+        const int ps = pf % kTcStages;
+        if (pf < nk && pf >= kTcStages) {
+            if (!mbar_wait(smem_u32(&mbar[ps]), (uint32_t)(((pf - kTcStages) / kTcStages) & 1))) ok = false;
         }
-        const int pf = ks + kTcStages - 1;
-        if (pf < nk) load(pf % kTcStages, pf);
+        if (__syncthreads_or(!ok)) { ok = false; break; }
+        if (pf < nk) load(ps, pf);
         cp_async_commit();
-        cp_async_wait<kTcStages - 1>();
+        cp_async_wait<kAhead>();
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (tid == 0) {
@@ -379,16 +387,19 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
                     "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, {%5, %5, %5, %5}, p;\n\t}\n"
                     ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc), "r"(0u));
             }
-            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar));
+            asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];"
+                         ::"r"(smem_u32(&mbar[st])));
         }
     }
     cp_async_wait<0>();
-    // the last commit covers every MMA issued
-    if (ok && nk > 0 && !mbar_wait(bar, (uint32_t)((nk - 1) & 1))) ok = false;
+    // the last commit covers every MMA issued (its stage's barrier, last use)
+    const uint32_t last_bar = nk > 0 ? smem_u32(&mbar[(nk - 1) % kTcStages]) : 0u;
+    const uint32_t last_parity = nk > 0 ? (uint32_t)(((nk - 1) / kTcStages) & 1) : 0u;
+    if (ok && nk > 0 && !mbar_wait(last_bar, last_parity)) ok = false;
     if (!ok && tid == 0) atomicAdd(&g_conv_timeouts, 1);
     if (__syncthreads_or(!ok)) {
         // give MMAs possibly still in flight a bounded grace period before freeing TMEM
-        if (nk > 0) mbar_wait(bar, (uint32_t)((nk - 1) & 1));
+        if (nk > 0) mbar_wait(last_bar, last_parity);
     } else {
         asm volatile("tcgen05.fence::after_thread_sync;");
         // epilogue: warp w holds TMEM lanes 32w..32w+31 = rows of the tile
@@ -737,9 +748,17 @@ int ffx_conv_forward_tc(const FfxConv* c, void* stream) {
     const int bn = a.cout <= 16 ? 16 : (a.cout <= 32 ? 32 : 64);
     const dim3 grid((unsigned)((a.rows + kBM - 1) / kBM), (unsigned)((a.cout + bn - 1) / bn), a.transposed ? 8 : 1);
     FFX_REQUIRE(grid.x < (1u << 31), "ffx_conv_forward_tc: grid too large");
-    if (bn == 16) conv_fwd_tc_kernel<16><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
-    else if (bn == 32) conv_fwd_tc_kernel<32><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
-    else conv_fwd_tc_kernel<64><<<grid, kGemmThreads, 0, as_stream(stream)>>>(a);
+    static bool configured = false;     // dynamic shared memory above 48 KB, once per process
+    if (!configured) {
+        cudaFuncSetAttribute(conv_fwd_tc_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<16>());
+        cudaFuncSetAttribute(conv_fwd_tc_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<32>());
+        cudaFuncSetAttribute(conv_fwd_tc_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, tc_smem_bytes<64>());
+        configured = true;
+    }
+    cudaStream_t st = as_stream(stream);
+    if (bn == 16) conv_fwd_tc_kernel<16><<<grid, kGemmThreads, tc_smem_bytes<16>(), st>>>(a);
+    else if (bn == 32) conv_fwd_tc_kernel<32><<<grid, kGemmThreads, tc_smem_bytes<32>(), st>>>(a);
+    else conv_fwd_tc_kernel<64><<<grid, kGemmThreads, tc_smem_bytes<64>(), st>>>(a);
     return launch_status("conv_fwd_tc_kernel");
 }
 
