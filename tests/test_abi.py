@@ -66,3 +66,10 @@ def test_reference_shader_library_exports(tmp_path):
     assert lib.glsl_ref_kernel_count() >= 30
     assert lib.glsl_ref_kernel(b'pressure_jacobi.glsl', 1) >= 0
     assert lib.glsl_ref_kernel(b'volume.frag.glsl', 0) == -1
+
+
+def test_build_entry_compiles_and_loads():
+    """The build entry point (nvcc for sm_100a, in place; incremental) imports
+    the package and finds every bound symbol."""
+    import __graft_entry__ as entry
+    entry.build()
