@@ -253,7 +253,7 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_kernel(const __grid_con
 // g_conv_timeouts, stops issuing, and still frees its TMEM.
 __device__ int g_conv_timeouts;
 
-constexpr int kTcStages = 4;                     // ring of operand stages; loads run two ahead
+constexpr int kTcStages = 3;                     // ring of operand stages (36 KB at BN = 64: six blocks per SM)
 constexpr int kTcStageK = 32;                    // two MMA k-steps of 16
 constexpr int kTcSpin = 1 << 22;                 // bounded mbarrier polling
 
@@ -352,7 +352,7 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
     const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(BN >> 3) << 17) |
                            ((uint32_t)(kBM >> 4) << 24);
 
-    constexpr int kAhead = 2;                         // stages loaded ahead of the MMAs
+    constexpr int kAhead = 1;                         // stages loaded ahead of the MMAs
 #pragma unroll
     for (int st = 0; st < kAhead; ++st) {
         if (st < nk) load(st, st);
@@ -361,7 +361,7 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
     bool ok = true;
     for (int ks = 0; ks < nk && ok; ++ks) {
         // the prefetch overwrites the stage whose MMAs were issued two iterations ago:
-        // wait for that stage's use (kTcStages - kAhead = 2 MMA groups may stay in flight)
+        // wait for that stage's use (kTcStages - kAhead MMA groups may stay in flight)
         const int pf = ks + kAhead;
         const int ps = pf % kTcStages;
         if (pf < nk && pf >= kTcStages) {

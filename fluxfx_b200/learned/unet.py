@@ -83,9 +83,9 @@ class UNet:
         self.by_name = {l.name: l for l in self.layers}
         self.shape = None
         self.step_count = 0
-        # forward and data-gradient convolutions: tcgen05 (accumulator in tensor
-        # memory) or the mma.sync form
-        self.conv_entry = 'ffx_conv_forward_tc'
+        # forward and data-gradient convolutions: the mma.sync form (faster on
+        # these narrow layers, whose operand gather dominates) or the tcgen05 form
+        self.conv_entry = 'ffx_conv_forward'
 
     # ------------------------------------------------------------- buffers
     def _buffers(self, batch, dims):
@@ -314,12 +314,12 @@ def main():
     ap.add_argument('--batch', type=int, default=1)
     ap.add_argument('--repeat', type=int, default=5)
     ap.add_argument('--train', action='store_true', help='also time forward + backward + Adam')
-    ap.add_argument('--mma-sync', action='store_true', help='the mma.sync convolutions instead of tcgen05')
+    ap.add_argument('--tcgen05', action='store_true', help='the tcgen05 convolutions instead of mma.sync')
     args = ap.parse_args()
     dev = torch.device('cuda')
     net = UNet(dev, seed=0)
-    if args.mma_sync:
-        net.conv_entry = 'ffx_conv_forward'
+    if args.tcgen05:
+        net.conv_entry = 'ffx_conv_forward_tc'
     g = torch.Generator(device='cuda').manual_seed(0)
     n = args.size
     div = torch.randn((args.batch, n, n, n), device=dev, generator=g)

@@ -185,10 +185,12 @@ def test_adam_matches_formula(lib):
     assert rel_err(w16.float(), w2) < 1e-2
 
 
-def test_unet_forward_and_gradients_match_oracle():
+@pytest.mark.parametrize('entry', ['ffx_conv_forward', 'ffx_conv_forward_tc'])
+def test_unet_forward_and_gradients_match_oracle(entry):
     from fluxfx_b200.learned.unet import UNet
     dev = torch.device('cuda')
     net = UNet(dev, seed=4)
+    net.conv_entry = entry
     g = torch.Generator().manual_seed(5)
     B, D = 2, 16
     div = torch.randn((B, D, D, D), generator=g)
