@@ -131,14 +131,6 @@ __device__ __forceinline__ float sample_closed(const Dev& d, const uint8_t* soli
     return zz0 * gz + zz1 * fz;
 }
 
-template <typename T>
-__device__ __forceinline__ float fetch_closed(const Dev& d, const T* __restrict__ f, int x, int y, int z) {
-    x = min(max(x, 0), d.nx - 1);
-    y = min(max(y, 0), d.ny - 1);
-    z = min(max(z, 0), d.nz - 1);
-    return Store<T>::ld(f, cidx(d, x, y, z));
-}
-
 // ------------------------------------------------------------ face predictor
 template <typename T>
 struct PredParams {
@@ -260,19 +252,21 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
                 float pa = sample_face(pred, f.sx, f.sy, f.sz, dv_h<P2>(d, arr.x, 0) - off[0], dv_h<P2>(d, arr.y, 1) - off[1],
                                        dv_h<P2>(d, arr.z, 2) - off[2]);
                 float val = Store<T>::ld(pred, f.i) + 0.5f * (Store<T>::ld(orig, f.i) - pa);
-                int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
-                int sxy = f.sx * f.sy;
-                float lo = 0.f, hi = 0.f;
-                bool first = true;
-                for (int oz = 0; oz < 2; ++oz)
-                    for (int oy = 0; oy < 2; ++oy)
-                        for (int ox = 0; ox < 2; ++ox) {
-                            int cx = min(max(bx + ox, 0), f.sx - 1), cy = min(max(by + oy, 0), f.sy - 1);
-                            int cz = min(max(bz + oz, 0), f.sz - 1);
-                            float v = Store<T>::ld(orig, cz * sxy + cy * f.sx + cx);
-                            if (first) { lo = hi = v; first = false; }
-                            else { lo = fminf(lo, v); hi = fmaxf(hi, v); }
-                        }
+                // min / max of the 8 corners around the departure point, clamped to the grid
+                const int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
+                const int cx0 = min(max(bx, 0), f.sx - 1), cx1 = min(max(bx + 1, 0), f.sx - 1);
+                const int cy0 = min(max(by, 0), f.sy - 1), cy1 = min(max(by + 1, 0), f.sy - 1);
+                const int cz0 = min(max(bz, 0), f.sz - 1), cz1 = min(max(bz + 1, 0), f.sz - 1);
+                const int sxy = f.sx * f.sy;
+                const int rows[4] = {cz0 * sxy + cy0 * f.sx, cz0 * sxy + cy1 * f.sx, cz1 * sxy + cy0 * f.sx,
+                                     cz1 * sxy + cy1 * f.sx};
+                float lo = Store<T>::ld(orig, rows[0] + cx0), hi = lo;
+#pragma unroll
+                for (int k = 1; k < 8; ++k) {
+                    const float v = Store<T>::ld(orig, rows[k >> 1] + ((k & 1) ? cx1 : cx0));
+                    lo = fminf(lo, v);
+                    hi = fmaxf(hi, v);
+                }
                 float cl = fminf(fmaxf(val, lo), hi);
                 value = low * (1.f - P.blend) + cl * P.blend;
             }
@@ -280,8 +274,13 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
         const SrcDev& S = P.src;
         if (S.count < 0) {
             float w = single_weight(S, p);
-            float bl = 1.f - expf(-S.coupling * dt * w);
-            value = value * (1.f - bl) + comp(S.jet, axis) * bl;
+            if (w != 0.f) {
+                float bl = 1.f - expf(-S.coupling * dt * w);
+                value = value * (1.f - bl) + comp(S.jet, axis) * bl;
+            } else {
+                // expf(+-0) = 1, so bl = 0 and the blend is value * 1 + jet * 0
+                value = value + comp(S.jet, axis) * 0.f;
+            }
         } else if (S.count > 0) {
             float total = 0.f, target = 0.f;
             for (int i = 0; i < S.count; ++i) {
@@ -451,8 +450,19 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
                        arr.y > hb[1] || arr.z > hb[2]);
                 if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
             }
-            int bx = 0, by = 0, bz = 0;
-            if (ok) { bx = (int)floorf(qx); by = (int)floorf(qy); bz = (int)floorf(qz); }
+            // corners of the departure cell clamped to the grid (closed boundary), shared by the channels
+            int rows[4] = {0, 0, 0, 0}, cx0 = 0, cx1 = 0;
+            if (ok) {
+                const int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
+                cx0 = min(max(bx, 0), d.nx - 1);
+                cx1 = min(max(bx + 1, 0), d.nx - 1);
+                const int cy0 = min(max(by, 0), d.ny - 1), cy1 = min(max(by + 1, 0), d.ny - 1);
+                const int cz0 = min(max(bz, 0), d.nz - 1), cz1 = min(max(bz + 1, 0), d.nz - 1);
+                rows[0] = cidx(d, 0, cy0, cz0);
+                rows[1] = cidx(d, 0, cy1, cz0);
+                rows[2] = cidx(d, 0, cy0, cz1);
+                rows[3] = cidx(d, 0, cy1, cz1);
+            }
             const SrcDev& S = P.src;
             for (int c = 0; c < P.count; ++c) {
                 const Channel<T>& C = P.ch[c];
@@ -460,14 +470,13 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
                                                         : sample_closed<T, MASK>(d, P.solid, C.field, qx, qy, qz);
                 if (ok) {
                     float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
-                    float lo = fetch_closed(d, C.field, bx, by, bz), hi = lo;
-                    for (int oz = 0; oz < 2; ++oz)
-                        for (int oy = 0; oy < 2; ++oy)
-                            for (int ox = 0; ox < 2; ++ox) {
-                                float v = fetch_closed(d, C.field, bx + ox, by + oy, bz + oz);
-                                lo = fminf(lo, v);
-                                hi = fmaxf(hi, v);
-                            }
+                    float lo = Store<T>::ld(C.field, rows[0] + cx0), hi = lo;
+#pragma unroll
+                    for (int k = 1; k < 8; ++k) {
+                        const float v = Store<T>::ld(C.field, rows[k >> 1] + ((k & 1) ? cx1 : cx0));
+                        lo = fminf(lo, v);
+                        hi = fmaxf(hi, v);
+                    }
                     value = fminf(fmaxf(val, lo), hi);
                 }
                 value = value * expf(-C.decay * dt);

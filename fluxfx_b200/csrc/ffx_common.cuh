@@ -340,14 +340,72 @@ __device__ __forceinline__ float dist3(F3 a, F3 b) {
     return sqrtf(dot3(c, c));
 }
 
+// dist3(a, b) < 1e-7f without the square root: sqrtf is correctly rounded and
+// monotone, so sqrtf(q) < 1e-7f holds exactly when q < 1e-14f (the float
+// nearest 1e-14, 0x1.6849b8p-47), for every q including NaN and infinity.
+__device__ __forceinline__ bool within_1e7(F3 a, F3 b) {
+    F3 c = {a.x - b.x, a.y - b.y, a.z - b.z};
+    return dot3(c, c) < 0x1.6849b8p-47f;
+}
+
+// Grid coordinates q = t / e * n of a point and the cell floor(q), clamped
+// before the integer conversion as in solid_halo.
+struct Probe {
+    float q[3];
+    int c[3];
+};
+template <bool P2>
+__device__ __forceinline__ bool probe_inside(const Dev& d, F3 t, Probe& r) {
+    const float tt[3] = {t.x, t.y, t.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        r.q[i] = dv_e<P2>(d, tt[i], i) * d.nf[i];
+        r.c[i] = (int)fmaxf(fminf(floorf(r.q[i]), 1.0e9f), -1.0e9f);
+    }
+    return r.c[0] >= 0 && r.c[1] >= 0 && r.c[2] >= 0 && r.c[0] < d.nx && r.c[1] < d.ny && r.c[2] < d.nz;
+}
+
+// Whether the MacCormack correction may be applied near colliders
+// (correct_velocity_fused.glsl / correct_scalar.glsl: no solid in the 3x3x3
+// blocks around the start, departure and arrival points, and none of the
+// three segments from the start clipped by a collider). Evaluated as
+//   !solid_halo(p) && !solid_halo(dep) && !solid_halo(arr) &&
+//   dist3(clip_solid_trace(p, t), t) < 1e-7f for t = dep, mid, arr
+// with the shared work done once: solid_halo's cell of an in-grid point is
+// the clip's start / end cell (floor(clamp(q, 1e-4, n - 1e-4)) = floor(q) for
+// q in [0, n)), so its halo tests stand for the clip's, and the clip's
+// fast-path value is formed here; a segment the fast path does not cover
+// takes the full clip.
 template <bool P2 = false>
 __device__ __forceinline__ bool safe_solid_correction(const Dev& d, const uint8_t* solid,
                                                       const uint8_t* halo, F3 p, F3 dep, F3 mid,
                                                       F3 arr) {
-    if (solid_halo<P2>(d, halo, p) || solid_halo<P2>(d, halo, dep) || solid_halo<P2>(d, halo, arr)) return false;
-    if (!(dist3(clip_solid_trace<P2>(d, solid, halo, p, dep), dep) < 1e-7f)) return false;
-    if (!(dist3(clip_solid_trace<P2>(d, solid, halo, p, mid), mid) < 1e-7f)) return false;
-    return dist3(clip_solid_trace<P2>(d, solid, halo, p, arr), arr) < 1e-7f;
+    Probe pp, pd, pa;
+    if (!probe_inside<P2>(d, p, pp) || __ldg(halo + cidx(d, pp.c[0], pp.c[1], pp.c[2]))) return false;
+    if (!probe_inside<P2>(d, dep, pd) || __ldg(halo + cidx(d, pd.c[0], pd.c[1], pd.c[2]))) return false;
+    if (!probe_inside<P2>(d, arr, pa) || __ldg(halo + cidx(d, pa.c[0], pa.c[1], pa.c[2]))) return false;
+    // clip_solid_trace(p, t) where t's halo cell is known (known_clear) or not
+    auto clipped_ok = [&](F3 t, const Probe& pt, bool known_clear) -> bool {
+        float b[3];
+        int e[3];
+        bool near = true;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) {
+            b[i] = fminf(fmaxf(pt.q[i], 0.0001f), d.nf[i] - 0.0001f);
+            e[i] = known_clear ? pt.c[i] : (int)floorf(b[i]);
+            near = near && abs(e[i] - pp.c[i]) <= 1;
+        }
+        if (near && (known_clear || !__ldg(halo + cidx(d, e[0], e[1], e[2])))) {
+            const F3 r = {dv_n<P2>(d, b[0], 0) * d.e[0], dv_n<P2>(d, b[1], 1) * d.e[1], dv_n<P2>(d, b[2], 2) * d.e[2]};
+            return within_1e7(r, t);
+        }
+        return within_1e7(clip_solid_trace<P2>(d, solid, halo, p, t), t);
+    };
+    if (!clipped_ok(dep, pd, true)) return false;
+    Probe pm;
+    probe_inside<P2>(d, mid, pm);
+    if (!clipped_ok(mid, pm, false)) return false;
+    return clipped_ok(arr, pa, true);
 }
 
 // ---------------------------------------------------------------- emitters
