@@ -171,6 +171,9 @@ _PROTOTYPES = {
     'ffx_conv_forward': (C.c_int, [P(FfxConv), vp]),
     'ffx_conv_forward_tc': (C.c_int, [P(FfxConv), vp]),
     'ffx_conv_timeouts': (C.c_int, [P(i32), i32]),
+    'ffx_conv_packed_bytes': (C.c_int, [P(FfxConv), P(i64)]),
+    'ffx_conv_pack_weights': (C.c_int, [P(FfxConv), vp, vp]),
+    'ffx_conv_forward_tma': (C.c_int, [P(FfxConv), vp, vp]),
     'ffx_conv_weight_grad': (C.c_int, [P(FfxConv), vp, i32, vp, vp]),
     'ffx_relu_backward': (C.c_int, [i64, i32, vp, i32, vp, i32, i32, vp]),
     'ffx_bias_grad': (C.c_int, [i64, i32, vp, i32, vp, vp]),

@@ -17,9 +17,11 @@
 // down-sampling) maps each output voxel 2q + j to tap j of input voxel q: one
 // GEMM per parity class j (blockIdx.z). Weight gradients reduce over voxels:
 // dW[k][n] = sum_m A[m][k] G[m][n], split over voxel chunks with FP32 atomics.
+#include <cuda.h>
 #include <cuda_bf16.h>
 
 #include <algorithm>
+#include <cstring>
 
 #include "ffx_host.cuh"
 
@@ -456,6 +458,264 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(kTmemCols));
 }
 
+// ------------------------------- 3^3 convolution: TMA halo tile + tcgen05
+// Stride-1, pad-1 3x3x3 layers without a gather. A block owns an output tile
+// of 8 (x) x 16 (y) x bz (z) voxels; its input footprint, a 10 x 18 x (bz + 2)
+// halo tile, comes in by one TMA tensor load per 8-channel plane (zero-filled
+// outside the grid, which is the padding). In shared memory a plane is laid
+// out [z][y][x][8 channels], 16 bytes per voxel, so for every tap (dz, dy, dx)
+// the 128 rows (8 x-voxels x 16 y-rows) of the A operand are the canonical
+// no-swizzle K-major core matrices of a shifted window: start = the tap's
+// first voxel, 8-row groups one halo row (160 B) apart, the two 8-channel
+// halves of K = 16 one plane apart. No data moves per tap: a K = 16 channel
+// group costs 27 x bz MMAs (M = 128, N = BN) on one staged tile. The weights
+// of a group, pre-packed into the MN-major core-matrix image of all 27 taps,
+// arrive by one bulk copy. A producer thread (TMA) and an MMA thread hand the
+// stages over through mbarriers (full: loads landed; empty: the stage's MMAs
+// completed, via tcgen05.commit); the bz accumulators (128 x BN FP32 each)
+// stay in tensor memory until the epilogue. Every wait is bounded; on timeout
+// the block counts it in g_conv_timeouts, lets its copies and MMAs drain
+// (bounded), frees its tensor memory and returns.
+constexpr int kTmX = 8, kTmY = 16;                   // output tile in x, y (M = 128)
+constexpr int kTmHX = kTmX + 2, kTmHY = kTmY + 2;    // halo tile
+constexpr int kTmThreads = 128;
+constexpr int kTmMaxStages = 4;
+constexpr int kTmSmemLimit = 200 * 1024;             // dynamic shared memory attribute of the kernels
+
+struct TmaConv {
+    CUtensorMap act;          // input: (channel, x, y, z, batch), box (8, 10, 18, bz + 2, 1)
+    const bf16* wpack;        // packed weights: [cout / BN][groups][27][BN / 8][16][8]
+    int batch, d, h, w;       // grid (input = output)
+    int cin, cout, groups;    // groups = ceil(cin / 16) channel groups of K = 16
+    int bz, tiles_x, tiles_y, tiles_z;
+    int stages, planes;       // planes loaded per group (1 when cin == 8)
+    uint32_t plane;           // bytes of one plane in shared memory (multiple of 128)
+    uint32_t stage;           // bytes of one stage: 2 planes + 27 weight tiles
+    uint32_t tx;              // bytes a stage's loads deliver
+    const float* bias;
+    int relu, accumulate;
+    bf16* out;
+    int out_pitch, out_offset;
+    float* out_f32;
+    int out_f32_pitch;
+};
+
+__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
+}
+
+// The halo planes of group g (channels 16g .. 16g + 15) and its packed weights.
+template <int BN>
+__device__ __forceinline__ void tm_issue_loads(const TmaConv& P, uint32_t st, uint32_t bar, int g, int b, int x0,
+                                               int y0, int z0, int nb) {
+    mbar_expect_tx(bar, P.tx);
+    const uint64_t map = reinterpret_cast<uint64_t>(&P.act);
+    for (int h = 0; h < P.planes; ++h)
+        asm volatile(
+            "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
+            "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
+            ::"r"(st + h * P.plane), "l"(map), "r"(16 * g + 8 * h), "r"(x0 - 1), "r"(y0 - 1), "r"(z0 - 1), "r"(b),
+              "r"(bar)
+            : "memory");
+    constexpr uint32_t kWBytes = 27u * 32u * BN;
+    const bf16* src = P.wpack + ((size_t)nb * P.groups + g) * (kWBytes / 2);
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 ::"r"(st + 2 * P.plane), "l"(src), "r"(kWBytes), "r"(bar)
+                 : "memory");
+}
+
+__device__ __forceinline__ void tm_mma(uint32_t tmem, uint64_t da, uint64_t db, uint32_t idesc, uint32_t acc) {
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "setp.ne.b32 p, %4, 0;\n\t"
+        "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n"
+        ::"r"(tmem), "l"(da), "l"(db), "r"(idesc), "r"(acc));
+}
+
+__device__ __forceinline__ void tm_commit(uint32_t bar) {
+    asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(bar)
+                 : "memory");
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kTmThreads) conv3_tma_kernel(const __grid_constant__ TmaConv P) {
+    static_assert(BN == 16 || BN == 32 || BN == 64, "BN");
+    extern __shared__ __align__(128) unsigned char tm_smem[];
+    __shared__ __align__(8) uint64_t full[kTmMaxStages], empty[kTmMaxStages], done;
+    __shared__ uint32_t tmem_base;
+    const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+    int t = blockIdx.x;
+    const int tx = t % P.tiles_x;
+    t /= P.tiles_x;
+    const int ty = t % P.tiles_y;
+    t /= P.tiles_y;
+    const int tz = t % P.tiles_z;
+    const int b = t / P.tiles_z;
+    const int x0 = tx * kTmX, y0 = ty * kTmY, z0 = tz * P.bz;
+    const int nb = blockIdx.y;
+    const uint32_t base = (smem_u32(tm_smem) + 127u) & ~127u;
+    const uint32_t cols = P.bz * BN <= 32 ? 32u : (P.bz * BN <= 64 ? 64u : (P.bz * BN <= 128 ? 128u : 256u));
+
+    if (warp == 0) {
+        asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
+                     ::"r"(smem_u32(&tmem_base)), "r"(cols));
+        asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
+    }
+    if (P.planes == 1) {
+        // cin == 8: the second channel half of K is zero (one group, one stage)
+        for (uint32_t i = tid * 16; i < P.plane; i += kTmThreads * 16)
+            asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(base + P.plane + i), "r"(0u) : "memory");
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    }
+    if (tid == 0) {
+        for (int s = 0; s < P.stages; ++s) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done)));
+        asm volatile("fence.mbarrier_init.release.cluster;");
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    asm volatile("tcgen05.fence::after_thread_sync;");
+    const uint32_t tmem = tmem_base;
+
+    bool ok = true;
+    int issued = 0;
+    if (warp == 0 && lane == 0) {
+        // producer
+        for (int g = 0; g < P.groups; ++g) {
+            const int s = g % P.stages;
+            if (g >= P.stages && !mbar_wait(smem_u32(&empty[s]), (uint32_t)(((g / P.stages) - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            tm_issue_loads<BN>(P, base + s * P.stage, smem_u32(&full[s]), g, b, x0, y0, z0, nb);
+            ++issued;
+        }
+    } else if (warp == 1 && lane == 0) {
+        // MMA issuer: D[j] += A(tap, z-slice j) x B(tap) over 27 taps and bz slices per group
+        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(BN >> 3) << 17) |
+                               ((uint32_t)(128 >> 4) << 24);
+        for (int g = 0; g < P.groups; ++g) {
+            const int s = g % P.stages;
+            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((g / P.stages) & 1))) {
+                ok = false;
+                break;
+            }
+            asm volatile("tcgen05.fence::after_thread_sync;");
+            const uint32_t st = base + s * P.stage;
+            const uint32_t wt = st + 2 * P.plane;
+            for (int j = 0; j < P.bz; ++j) {
+#pragma unroll 3
+                for (int tap = 0; tap < 27; ++tap) {
+                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                    const uint32_t a = st + (uint32_t)((((j + dz) * kTmHY + dy) * kTmHX + dx) * 16);
+                    const uint64_t da = umma_desc(a, P.plane, kTmHX * 16);
+                    const uint64_t db = umma_desc(wt + (uint32_t)(tap * 32 * BN), 128, 256);
+                    tm_mma(tmem + (uint32_t)(j * BN), da, db, idesc, (g > 0 || tap > 0) ? 1u : 0u);
+                }
+            }
+            tm_commit(smem_u32(&empty[s]));
+        }
+        tm_commit(smem_u32(&done));   // tracks every MMA this thread issued
+    }
+    __syncwarp();
+    const bool failed = __syncthreads_or(!ok);
+    const bool finished = mbar_wait(smem_u32(&done), 0);
+    if (failed || !finished) {
+        if (tid == 0) {
+            atomicAdd(&g_conv_timeouts, 1);
+            // let the loads this block issued land before its shared memory is released
+            for (int g = issued > P.stages ? issued - P.stages : 0; g < issued; ++g)
+                mbar_wait(smem_u32(&full[g % P.stages]), (uint32_t)((g / P.stages) & 1));
+        }
+    } else {
+        asm volatile("tcgen05.fence::after_thread_sync;");
+        const int m = warp * 32 + lane;
+        const int x = x0 + (m & 7), y = y0 + (m >> 3);
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        for (int j = 0; j < P.bz; ++j) {
+            const int z = z0 + j;
+            const bool in = x < P.w && y < P.h && z < P.d;
+            const long long vox = (((long long)b * P.d + z) * P.h + y) * P.w + x;
+#pragma unroll
+            for (int c0 = 0; c0 < BN; c0 += 16) {
+                uint32_t r[16];
+                asm volatile(
+                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                    "[%16];"
+                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
+                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
+                      "=r"(r[14]), "=r"(r[15])
+                    : "r"(lane_addr + (uint32_t)(j * BN + c0)));
+                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+                if (!in) continue;
+                const int n = nb * BN + c0;
+                float v[16];
+#pragma unroll
+                for (int e = 0; e < 16; ++e) {
+                    v[e] = __uint_as_float(r[e]);
+                    if (P.bias) v[e] += __ldg(P.bias + n + e);
+                    if (P.relu) v[e] = fmaxf(v[e], 0.f);
+                }
+                if (P.out) {
+                    uint4* o = reinterpret_cast<uint4*>(P.out + vox * P.out_pitch + P.out_offset + n);
+#pragma unroll
+                    for (int q = 0; q < 2; ++q) {
+                        if (P.accumulate) {
+                            const uint4 prev = o[q];
+                            const __nv_bfloat162* pv = reinterpret_cast<const __nv_bfloat162*>(&prev);
+#pragma unroll
+                            for (int e = 0; e < 4; ++e) {
+                                const float2 f = __bfloat1622float2(pv[e]);
+                                v[8 * q + 2 * e] += f.x;
+                                v[8 * q + 2 * e + 1] += f.y;
+                            }
+                        }
+                        uint4 pk;
+                        __nv_bfloat162* pp = reinterpret_cast<__nv_bfloat162*>(&pk);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) pp[e] = __floats2bfloat162_rn(v[8 * q + 2 * e], v[8 * q + 2 * e + 1]);
+                        o[q] = pk;
+                    }
+                }
+                if (P.out_f32) {
+                    float* o = P.out_f32 + vox * P.out_f32_pitch + n;
+#pragma unroll
+                    for (int e = 0; e < 16; ++e) o[e] = v[e];
+                }
+            }
+        }
+    }
+    asm volatile("tcgen05.fence::before_thread_sync;");
+    __syncthreads();
+    if (warp == 0)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols));
+}
+
+// Packed weights of the TMA convolution: w[k = tap * cin + c][cout] ->
+// [cout / BN][groups][27][BN / 8][16][8] (channels >= cin zero), the
+// MN-major core-matrix image a stage copies into shared memory as it is.
+__global__ void conv3_pack_kernel(const bf16* __restrict__ w, int cin, int cout, int bn, int groups,
+                                  bf16* __restrict__ packed) {
+    const long long n = (long long)(cout / bn) * groups * 27 * bn * 16;
+    const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int e = (int)(i % 8);
+    long long r = i / 8;
+    const int row = (int)(r % 16);
+    r /= 16;
+    const int j = (int)(r % (bn / 8));
+    r /= bn / 8;
+    const int tap = (int)(r % 27);
+    r /= 27;
+    const int g = (int)(r % groups);
+    const int nb = (int)(r / groups);
+    const int c = 16 * g + row, co = nb * bn + 8 * j + e;
+    packed[i] = c < cin ? w[((long long)tap * cin + c) * cout + co] : __float2bfloat16(0.f);
+}
+
 // ------------------------------------------------------ weight gradient GEMM
 // dW[k][n] += sum over the block's voxel chunk of A[m][k] G[m][n]; A^T
 // fragments come from the [m][k] tile through ldmatrix.trans.
@@ -719,6 +979,47 @@ int make_conv(const FfxConv* c, Conv& a) {
     return FFX_OK;
 }
 
+// ---------------------------------------------- TMA convolution, host side
+using EncodeTiled = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*, const cuuint64_t*,
+                                 const cuuint64_t*, const cuuint32_t*, const cuuint32_t*, CUtensorMapInterleave,
+                                 CUtensorMapSwizzle, CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+// cuTensorMapEncodeTiled from the driver the runtime loaded (no link-time libcuda).
+EncodeTiled tensor_map_encoder() {
+    static EncodeTiled fn = nullptr;
+    static bool tried = false;
+    if (!tried) {
+        tried = true;
+        void* p = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) == cudaSuccess &&
+            q == cudaDriverEntryPointSuccess)
+            fn = reinterpret_cast<EncodeTiled>(p);
+    }
+    return fn;
+}
+
+// 3x3x3, stride 1, pad 1, one input view, channels the kernel tiles.
+bool tma_eligible(const Conv& a) {
+    return !a.transposed && a.ks == 3 && a.stride == 1 && a.pad == 1 && a.c2 == 0 &&
+           (a.cin % 16 == 0 || a.cin == 8) && a.cin <= 512 && a.cout % 16 == 0 && a.od == a.id && a.oh == a.ih &&
+           a.ow == a.iw;
+}
+int tma_bn(int cout) { return cout % 64 == 0 ? 64 : (cout % 32 == 0 ? 32 : 16); }
+int tma_groups(int cin) { return (cin + 15) / 16; }
+long long tma_packed_elems(const Conv& a) { return (long long)tma_groups(a.cin) * 27 * 16 * a.cout; }
+
+int sm_count() {
+    static int n = 0;
+    if (n == 0) {
+        int dev = 0;
+        if (cudaGetDevice(&dev) != cudaSuccess || cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) !=
+                                                     cudaSuccess || n <= 0)
+            n = 148;
+    }
+    return n;
+}
+
 }  // namespace
 }  // namespace ffx
 
@@ -760,6 +1061,100 @@ int ffx_conv_forward_tc(const FfxConv* c, void* stream) {
     else if (bn == 32) conv_fwd_tc_kernel<32><<<grid, kGemmThreads, tc_smem_bytes<32>(), st>>>(a);
     else conv_fwd_tc_kernel<64><<<grid, kGemmThreads, tc_smem_bytes<64>(), st>>>(a);
     return launch_status("conv_fwd_tc_kernel");
+}
+
+int ffx_conv_packed_bytes(const FfxConv* c, int64_t* bytes) {
+    FFX_REQUIRE(bytes, "ffx_conv_packed_bytes: invalid arguments");
+    Conv a;
+    int e = make_conv(c, a);
+    if (e) return e;
+    *bytes = tma_eligible(a) ? tma_packed_elems(a) * 2 : 0;
+    return FFX_OK;
+}
+
+int ffx_conv_pack_weights(const FfxConv* c, void* packed, void* stream) {
+    Conv a;
+    int e = make_conv(c, a);
+    if (e) return e;
+    FFX_REQUIRE(tma_eligible(a), "ffx_conv_pack_weights: not a 3x3x3 stride-1 pad-1 convolution the TMA kernel tiles");
+    FFX_REQUIRE(packed && ((uintptr_t)packed & 15) == 0, "ffx_conv_pack_weights: packed buffer (16-byte aligned)");
+    const long long n = tma_packed_elems(a);
+    conv3_pack_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(a.w, a.cin, a.cout, tma_bn(a.cout),
+                                                                        tma_groups(a.cin), (bf16*)packed);
+    return launch_status("conv3_pack_kernel");
+}
+
+int ffx_conv_forward_tma(const FfxConv* c, const void* packed, void* stream) {
+    Conv a;
+    int e = make_conv(c, a);
+    if (e) return e;
+    if (!tma_eligible(a)) return ffx_conv_forward(c, stream);   // other shapes: the mma.sync kernel
+    FFX_REQUIRE(a.out || a.out_f32, "ffx_conv_forward_tma: no output");
+    FFX_REQUIRE(packed && ((uintptr_t)packed & 15) == 0,
+                "ffx_conv_forward_tma: packed weights (ffx_conv_pack_weights, 16-byte aligned)");
+    FFX_REQUIRE(!a.out_f32 || a.out_f32_pitch >= a.cout, "ffx_conv_forward_tma: FP32 output pitch");
+    EncodeTiled encode = tensor_map_encoder();
+    FFX_REQUIRE(encode, "ffx_conv_forward_tma: cuTensorMapEncodeTiled is not available from the driver");
+    const int bn = tma_bn(a.cout);
+    TmaConv P;
+    std::memset(&P, 0, sizeof(P));
+    P.wpack = (const bf16*)packed;
+    P.batch = a.batch;
+    P.d = a.id; P.h = a.ih; P.w = a.iw;
+    P.cin = a.cin; P.cout = a.cout; P.groups = tma_groups(a.cin);
+    P.planes = a.cin == 8 ? 1 : 2;
+    P.tiles_x = (a.iw + kTmX - 1) / kTmX;
+    P.tiles_y = (a.ih + kTmY - 1) / kTmY;
+    // deepest tile (z slices sharing one halo) that still gives every SM two blocks
+    const long long nblocks = a.cout / bn;
+    const long long want = 2LL * sm_count();
+    P.bz = 1;
+    for (int bz = 4; bz >= 1; bz >>= 1) {
+        const long long blocks = (long long)P.tiles_x * P.tiles_y * ((a.id + bz - 1) / bz) * a.batch * nblocks;
+        if (blocks >= want || bz == 1) { P.bz = bz; break; }
+    }
+    P.tiles_z = (a.id + P.bz - 1) / P.bz;
+    const uint32_t box_bytes = 8u * kTmHX * kTmHY * (uint32_t)(P.bz + 2) * 2u;
+    P.plane = (box_bytes + 127u) & ~127u;
+    P.stage = 2 * P.plane + 27u * 32u * (uint32_t)bn;
+    P.tx = (uint32_t)P.planes * box_bytes + 27u * 32u * (uint32_t)bn;
+    P.stages = std::max(1, std::min({P.groups, kTmMaxStages, (int)((110u * 1024u) / P.stage)}));
+    const size_t smem = (size_t)P.stages * P.stage + 128;
+    FFX_REQUIRE(smem <= (size_t)kTmSmemLimit, "ffx_conv_forward_tma: stage does not fit in shared memory");
+    const long long blocks = (long long)P.tiles_x * P.tiles_y * P.tiles_z * a.batch;
+    FFX_REQUIRE(blocks < (1LL << 31) && nblocks < 65536, "ffx_conv_forward_tma: grid too large");
+    P.bias = a.bias;
+    P.relu = a.relu;
+    P.accumulate = a.accumulate;
+    P.out = a.out;
+    P.out_pitch = a.out_pitch;
+    P.out_offset = a.out_offset;
+    P.out_f32 = a.out_f32;
+    P.out_f32_pitch = a.out_f32_pitch;
+    // input activations as a (channel, x, y, z, batch) tensor, zero outside
+    const cuuint64_t pitch = (cuuint64_t)a.in1.pitch * 2;
+    const cuuint64_t dims[5] = {(cuuint64_t)a.cin, (cuuint64_t)a.iw, (cuuint64_t)a.ih, (cuuint64_t)a.id,
+                                (cuuint64_t)a.batch};
+    const cuuint64_t strides[4] = {pitch, pitch * a.iw, pitch * a.iw * a.ih, pitch * a.iw * a.ih * a.id};
+    const cuuint32_t box[5] = {8, kTmHX, kTmHY, (cuuint32_t)(P.bz + 2), 1};
+    const cuuint32_t estride[5] = {1, 1, 1, 1, 1};
+    const CUresult r = encode(&P.act, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, (void*)(a.in1.p + a.in1.offset), dims,
+                              strides, box, estride, CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE,
+                              CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+    FFX_REQUIRE(r == CUDA_SUCCESS, "ffx_conv_forward_tma: cuTensorMapEncodeTiled rejected the input view");
+    static bool configured = false;
+    if (!configured) {
+        cudaFuncSetAttribute(conv3_tma_kernel<16>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmSmemLimit);
+        cudaFuncSetAttribute(conv3_tma_kernel<32>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmSmemLimit);
+        cudaFuncSetAttribute(conv3_tma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmSmemLimit);
+        configured = true;
+    }
+    const dim3 grid((unsigned)blocks, (unsigned)nblocks, 1);
+    cudaStream_t st = as_stream(stream);
+    if (bn == 16) conv3_tma_kernel<16><<<grid, kTmThreads, smem, st>>>(P);
+    else if (bn == 32) conv3_tma_kernel<32><<<grid, kTmThreads, smem, st>>>(P);
+    else conv3_tma_kernel<64><<<grid, kTmThreads, smem, st>>>(P);
+    return launch_status("conv3_tma_kernel");
 }
 
 int ffx_conv_timeouts(int32_t* out, int32_t reset) {

@@ -1,9 +1,9 @@
 """3D U-Net pressure warm start on the library's BF16 tensor-core convolutions.
 
-No counterpart in the reference: the network maps (divergence,
-solid mask) to a pressure that replaces the zero initial guess of the
-multigrid solve; the solver still iterates to the same tolerance, so the plain
-method stays both the fallback and the judge of the prediction.
+No counterpart in the reference: the network maps (divergence, solid mask)
+to a pressure that replaces the zero initial guess of the multigrid solve;
+the solver still iterates to the same tolerance, so the plain method stays
+both the fallback and the arbiter of the prediction.
 
 Architecture (4 levels, channels 16/32/64/128): per level two 3^3 convolutions
 with ReLU; 2^3 stride-2 convolutions (+ReLU) down; 2^3 stride-2 transposed
@@ -14,10 +14,13 @@ The decoder's concatenation buffers are written in place by both producers
 (up-sampling into channels [0, C), the encoder's second convolution into
 [C, 2C)), and their gradients likewise, so no copies are made.
 
-All work runs through ``libffx_core`` (``ffx_conv_forward``,
-``ffx_conv_weight_grad``, ``ffx_relu_backward``, ``ffx_bias_grad``,
-``ffx_weight_transpose``, ``ffx_adam``, ``ffx_pack_input``,
-``ffx_mse_grad``); torch only allocates.
+All work runs through ``libffx_core`` (``ffx_conv_forward_tma`` with
+``ffx_conv_pack_weights``, ``ffx_conv_forward``, ``ffx_conv_weight_grad``,
+``ffx_relu_backward``, ``ffx_bias_grad``, ``ffx_weight_transpose``,
+``ffx_adam``, ``ffx_pack_input``, ``ffx_mse_grad``); torch only allocates.
+The 3^3 layers (forward and data gradient) run on the TMA-staged tcgen05
+convolution by default; the stride-2, transposed and 1^3 layers on the
+mma.sync implicit GEMM.
 """
 import ctypes as C
 
@@ -83,9 +86,13 @@ class UNet:
         self.by_name = {l.name: l for l in self.layers}
         self.shape = None
         self.step_count = 0
-        # forward and data-gradient convolutions: the mma.sync form (faster on
-        # these narrow layers, whose operand gather dominates) or the tcgen05 form
-        self.conv_entry = 'ffx_conv_forward'
+        # forward and data-gradient convolutions: 'ffx_conv_forward' (mma.sync,
+        # gathered operands), 'ffx_conv_forward_tc' (tcgen05, gathered operands)
+        # or 'ffx_conv_forward_tma' (3x3x3 layers as TMA halo tiles + tcgen05 on
+        # pre-packed weights, the other shapes on the mma.sync kernel; the default)
+        self.conv_entry = 'ffx_conv_forward_tma'
+        self.weight_version = 0      # bumped when the weights change (repacks the TMA weights)
+        self._packs = {}
 
     # ------------------------------------------------------------- buffers
     def _buffers(self, batch, dims):
@@ -185,6 +192,27 @@ class UNet:
     def _call(self, name, *args):
         N.check(getattr(self.lib, name)(*args))
 
+    def _run_conv(self, key, c, s):
+        """One convolution through the selected entry; the TMA entry gets the
+        weights packed once per weight version (and per role: forward weights
+        or the transposed data-gradient weights)."""
+        if self.conv_entry != 'ffx_conv_forward_tma':
+            self._call(self.conv_entry, C.byref(c), s)
+            return
+        n = N.i64(0)
+        self._call('ffx_conv_packed_bytes', C.byref(c), C.byref(n))
+        packed = None
+        if n.value:
+            entry = self._packs.get(key)
+            if entry is None or entry[0].numel() * 2 < n.value:
+                entry = [torch.empty(n.value // 2, dtype=torch.bfloat16, device=self.device), -1]
+                self._packs[key] = entry
+            if entry[1] != self.weight_version:
+                self._call('ffx_conv_pack_weights', C.byref(c), _p(entry[0]), s)
+                entry[1] = self.weight_version
+            packed = entry[0]
+        self._call('ffx_conv_forward_tma', C.byref(c), _p(packed), s)
+
     # ------------------------------------------------------------ forward
     def forward(self, div, mask, scale, stream):
         """div: (B, D, H, W) float32, mask: uint8 or None; returns the FP32
@@ -199,7 +227,7 @@ class UNet:
                 c = self._conv(layer, lin, ins[0], lout, None, 0, 0, out_f32=self.pred, f32_pitch=HEAD_CHANNELS)
             else:
                 c = self._conv(layer, lin, ins[0], lout, out, pitch, offset)
-            self._call(self.conv_entry, C.byref(c), s)
+            self._run_conv((name, 'forward'), c, s)
         return self.pred[..., 0]
 
     def activation(self, name):
@@ -264,7 +292,7 @@ class UNet:
             else:   # up: its data gradient is a 2^3 stride-2 convolution of the fine gradient
                 c = self._conv(layer, lout, g_view, lin, gin, ipitch, ioff, weight=layer.wt16, transposed=0,
                                ks=2, stride=2, pad=0, cout=layer.cin, bias=False, relu=False)
-            self._call(self.conv_entry, C.byref(c), s)
+            self._run_conv((name, 'data'), c, s)
         return self.loss_acc
 
     def _voxels(self, level):
@@ -273,6 +301,7 @@ class UNet:
 
     def adam_step(self, lr, stream, beta1=0.9, beta2=0.999, eps=1e-8):
         self.step_count += 1
+        self.weight_version += 1
         s = C.c_void_p(stream)
         for l in self.layers:
             for w, m, v, g, w16 in l.params():
@@ -289,6 +318,7 @@ class UNet:
             l.w.copy_(w.to(l.w.device))
             l.b.copy_(b.to(l.b.device))
             l.w16.copy_(l.w.to(torch.bfloat16))
+        self.weight_version += 1
 
     def forward_flops(self, batch, dims):
         """Multiply-add FLOPs (2 per MAC) of one forward pass."""
@@ -314,12 +344,16 @@ def main():
     ap.add_argument('--batch', type=int, default=1)
     ap.add_argument('--repeat', type=int, default=5)
     ap.add_argument('--train', action='store_true', help='also time forward + backward + Adam')
-    ap.add_argument('--tcgen05', action='store_true', help='the tcgen05 convolutions instead of mma.sync')
+    ap.add_argument('--tcgen05', action='store_true', help='the gathered-operand tcgen05 convolutions')
+    ap.add_argument('--mma-sync', action='store_true', help='the gathered-operand mma.sync convolutions')
+    ap.add_argument('--tma', action='store_true', help='3x3x3 layers as TMA halo tiles on tcgen05 (default)')
     args = ap.parse_args()
     dev = torch.device('cuda')
     net = UNet(dev, seed=0)
     if args.tcgen05:
         net.conv_entry = 'ffx_conv_forward_tc'
+    if args.mma_sync:
+        net.conv_entry = 'ffx_conv_forward'
     g = torch.Generator(device='cuda').manual_seed(0)
     n = args.size
     div = torch.randn((args.batch, n, n, n), device=dev, generator=g)

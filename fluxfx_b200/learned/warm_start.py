@@ -16,7 +16,7 @@ Attach it with ``projector.attach_learned(model)`` and set
 ``learned_warm_start=True``: the solve then starts from the prediction when it
 would otherwise start from zero (every step without ``solid_warm_start``; the
 first step after a reset with it). The multigrid still iterates to the same
-tolerance, so the plain method stays both the fallback and the judge.
+tolerance, so the plain method stays both the fallback and the arbiter.
 """
 import ctypes as C
 from pathlib import Path

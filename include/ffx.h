@@ -551,6 +551,15 @@ int ffx_conv_forward(const FfxConv* conv, void* stream);
 /* The same on the 5th-generation tensor cores (tcgen05.mma, accumulator in tensor
  * memory, bounded completion waits). */
 int ffx_conv_forward_tc(const FfxConv* conv, void* stream);
+/* 3x3x3 stride-1 pad-1 convolutions without an operand gather: each block stages its
+ * input halo tile by TMA tensor loads (cp.async.bulk.tensor, zero fill = padding) and runs
+ * every tap as a shifted shared-memory descriptor into tcgen05.mma (accumulators in tensor
+ * memory). The weights come pre-packed (ffx_conv_pack_weights, `packed_bytes` from
+ * ffx_conv_packed_bytes; 0 for shapes the kernel does not tile). Other shapes (2^3
+ * stride 2, transposed, 1x1) run the ffx_conv_forward kernel and ignore `packed`. */
+int ffx_conv_packed_bytes(const FfxConv* conv, int64_t* packed_bytes);
+int ffx_conv_pack_weights(const FfxConv* conv, void* packed, void* stream);
+int ffx_conv_forward_tma(const FfxConv* conv, const void* packed, void* stream);
 /* Number of tcgen05 convolution launches that gave up waiting (synchronous; reset != 0
  * clears it). */
 int ffx_conv_timeouts(int32_t* out, int32_t reset);

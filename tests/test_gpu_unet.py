@@ -137,6 +137,79 @@ def test_forward_entries_match_torch(lib, kind, entry):
     assert rel_err(out32, ref) < 1e-5, rel_err(out32, ref)
 
 
+@pytest.mark.parametrize('case', [
+    # (batch, (D, H, W), cin, cout, view, bf16 output, accumulate)
+    (1, (5, 20, 12), 8, 16, False, False, 0),      # cin 8: one plane, ragged tiles in every axis
+    (2, (6, 10, 12), 16, 16, True, True, 1),       # input and output views, ReLU, accumulate
+    (1, (8, 16, 16), 32, 32, False, True, 0),
+    (1, (4, 16, 8), 64, 64, False, False, 0),      # four channel groups through the stage ring
+    (1, (8, 8, 8), 128, 128, True, True, 0),       # two 64-channel column blocks, eight groups
+    (2, (3, 7, 9), 32, 48, False, False, 0),       # 16-channel columns, grid smaller than one tile
+])
+def test_tma_convolution_matches_torch(lib, case):
+    """The 3x3x3 TMA-staged tcgen05 convolution against torch FP64 on the
+    same BF16 values: every channel width it tiles, ragged grids smaller and
+    larger than the 8 x 16 x bz tile, channel views, and the BF16 epilogue
+    (bias, ReLU, accumulation into the existing output)."""
+    B, (D, H, W), cin, cout, view, out_bf16, acc = case
+    g = torch.Generator().manual_seed(cin * 7 + cout)
+    pitch, off = (cin + 16, 8) if view else (cin, 0)
+    x = bf(torch.randn((B, D, H, W, pitch), generator=g))
+    w = bf(torch.randn((27, cin, cout), generator=g) / (27 * cin) ** 0.5)
+    bias = torch.randn(cout, generator=g)
+    dx, dw, db = x.cuda(), w.cuda(), bias.cuda()
+    opitch, ooff = (cout + 16, 8) if view else (cout, 0)
+    prior = bf(torch.randn((B, D, H, W, opitch), generator=g))
+    out16 = prior.clone().cuda()
+    out32 = torch.zeros((B, D, H, W, cout), device='cuda')
+    relu = int(out_bf16)
+    c = conv_struct(B, (D, H, W), (D, H, W), cin, 0, cout, 3, 1, 1, 0, dx, pitch, off, None, 0, 0, dw, db, relu,
+                    out16 if out_bf16 else None, opitch, ooff, None if out_bf16 else out32, cout, accumulate=acc)
+    nbytes = N.i64(0)
+    N.check(lib.ffx_conv_packed_bytes(C.byref(c), C.byref(nbytes)))
+    assert nbytes.value == ((cin + 15) // 16) * 27 * 16 * cout * 2
+    packed = torch.zeros(nbytes.value // 2, dtype=torch.bfloat16, device='cuda')
+    N.check(lib.ffx_conv_pack_weights(C.byref(c), C.c_void_p(packed.data_ptr()), None))
+    N.check(lib.ffx_conv_forward_tma(C.byref(c), C.c_void_p(packed.data_ptr()), None))
+    torch.cuda.synchronize()
+    count = C.c_int32(0)
+    N.check(lib.ffx_conv_timeouts(C.byref(count), 1))
+    assert count.value == 0
+    xt = x[..., off:off + cin].double().permute(0, 4, 1, 2, 3)
+    ref = F.conv3d(xt, U.torch_weight('conv3', w.double()), bias.double(), padding=1).permute(0, 2, 3, 4, 1)
+    if relu:
+        ref = torch.relu(ref)
+    if not out_bf16:
+        assert rel_err(out32, ref) < 1e-5, rel_err(out32, ref)
+        return
+    if acc:
+        ref = ref + prior[..., ooff:ooff + cout].double()
+    got = out16.cpu()
+    assert rel_err(got[..., ooff:ooff + cout].float(), ref) < 8e-3, rel_err(got[..., ooff:ooff + cout].float(), ref)
+    # channels outside the output view are untouched
+    assert torch.equal(got[..., :ooff], prior[..., :ooff]) and torch.equal(got[..., ooff + cout:],
+                                                                            prior[..., ooff + cout:])
+
+
+def test_tma_convolution_other_shapes_use_the_gather_kernel(lib):
+    """Shapes the TMA kernel does not tile report no packed size and run the
+    mma.sync kernel through the same entry (packed pointer ignored)."""
+    g = torch.Generator().manual_seed(3)
+    x = bf(torch.randn((1, 8, 8, 8, 16), generator=g)).cuda()
+    w = bf(torch.randn((8, 16, 32), generator=g) / 11.0).cuda()
+    out32 = torch.zeros((1, 4, 4, 4, 32), device='cuda')
+    c = conv_struct(1, (8, 8, 8), (4, 4, 4), 16, 0, 32, 2, 2, 0, 0, x, 16, 0, None, 0, 0, w, None, 0, None, 0, 0,
+                    out32, 32)
+    nbytes = N.i64(-1)
+    N.check(lib.ffx_conv_packed_bytes(C.byref(c), C.byref(nbytes)))
+    assert nbytes.value == 0
+    assert lib.ffx_conv_pack_weights(C.byref(c), None, None) != 0
+    N.check(lib.ffx_conv_forward_tma(C.byref(c), None, None))
+    torch.cuda.synchronize()
+    ref = F.conv3d(x.double().cpu().permute(0, 4, 1, 2, 3), U.torch_weight('down', w.double().cpu()), stride=2)
+    assert rel_err(out32, ref.permute(0, 2, 3, 4, 1)) < 1e-5
+
+
 @pytest.mark.parametrize('kind', ['conv3', 'down', 'up'])
 def test_weight_gradients_match_torch(lib, kind):
     g = torch.Generator().manual_seed(2)
@@ -185,7 +258,7 @@ def test_adam_matches_formula(lib):
     assert rel_err(w16.float(), w2) < 1e-2
 
 
-@pytest.mark.parametrize('entry', ['ffx_conv_forward', 'ffx_conv_forward_tc'])
+@pytest.mark.parametrize('entry', ['ffx_conv_forward', 'ffx_conv_forward_tc', 'ffx_conv_forward_tma'])
 def test_unet_forward_and_gradients_match_oracle(entry):
     from fluxfx_b200.learned.unet import UNet
     dev = torch.device('cuda')
