@@ -16,17 +16,21 @@ same seeded start after the same warm-up:
 
 * plain   -- the reference algorithm: stand-alone aggregation V-cycles (4/4
              Jacobi sweeps), pressure cold-started every step, FP32 storage;
-* fast    -- the same V(4,4) cycles started from the previous step's pressure
-             (scaled by dt / previous dt) with the coarse correction
-             over-corrected by 1.9 at every prolongation (default);
-* pcg     -- conjugate gradients preconditioned by a V(1,1) cycle, warm start;
-* learned -- plain, started from the U-Net's prediction (network on the
-             128^3 restriction, trilinear prolongation)
+* learned -- the same V(4,4) cycles started every step from the U-Net's
+             prediction (network on the 128^3 restriction, trilinear
+             prolongation), with the coarse correction over-corrected by 1.9
+             at every prolongation (default: the learned-warm-start step);
+* fast    -- the same over-corrected cycles started from the previous step's
+             pressure (scaled by dt / previous dt) instead of the network;
+* learned_plain -- the plain cycles from the network's prediction (the
+             V-cycles the network alone saves);
+* pcg     -- conjugate gradients preconditioned by a V(1,1) cycle, warm start
              (--storage selects FP32 or BF16 field storage; --set overrides
              any solver setting of the headline variant).
 
-The JSON `value` is the `--variant` run (default fast); the plain run is
-reported beside it. `value` is whole-job steps/s (N GPUs each run their own
+The JSON `value` is the `--variant` run (default learned); the plain run,
+the fast run and the plain-cycles-from-the-network run are reported beside
+it. `value` is whole-job steps/s (N GPUs each run their own
 replica domain: "weak" scaling, no collective on the step path). `e2e`
 measures the same steps through the public API with each step's density field
 read back into pinned host memory (the bake/preview readback) inside the
@@ -48,14 +52,15 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
-METRIC = "steps/s @256^3 to rel div 1e-4 (colliders, MacCormack)"
+METRIC = "steps/s @256^3 to rel div 1e-4: learned warm start vs plain FP32 MG (colliders, MacCormack)"
 UNIT = "steps/s"
 
 VARIANTS = {
     'plain': dict(pressure_method='VCYCLE', solid_warm_start=False),
+    'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True, mg_coarse_scale=1.9),
     'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9),
+    'learned_plain': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
     'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
-    'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
 }
 
 # Algorithmic bytes per cell of each pass (inputs read once, outputs written
@@ -318,19 +323,26 @@ def run_b200(args):
                      rel_div=prun.solver.measure_projection()['rel_div_inf'])
         prun.close()
 
-    # --- the plain algorithm started from the learned guess -------------------
-    learned = None
-    if args.compare_learned and args.variant != 'learned':
-        lrun = Run(args, device, rank, 'learned', args.storage)
-        lrun.warm(args.warmup)
-        l_steps = max(2, args.steps // 2)
-        l_elapsed = lrun.timed(l_steps)
-        learned = dict(elapsed=l_elapsed, steps=l_steps, cycles=lrun.cycles,
-                       rel_div=lrun.solver.measure_projection()['rel_div_inf'])
-        lrun.close()
+    # --- comparison variants: the previous pressure instead of the network, and
+    # the plain cycles from the network's guess -----------------------------------
+    def compare(variant, enabled):
+        if not enabled or args.variant == variant:
+            return None
+        crun = Run(args, device, rank, variant, args.storage)
+        crun.warm(args.warmup)
+        c_steps = max(2, args.steps // 2)
+        c_elapsed = crun.timed(c_steps)
+        out = dict(elapsed=c_elapsed, steps=c_steps, cycles=crun.cycles,
+                   rel_div=crun.solver.measure_projection()['rel_div_inf'])
+        crun.close()
+        return out
 
-    elapsed, e2e_time, p_el, l_el = max_over_ranks(
-        [elapsed, e2e_time, plain['elapsed'] if plain else 0.0, learned['elapsed'] if learned else 0.0], world)
+    fast = compare('fast', args.compare_fast)
+    learned = compare('learned_plain', args.compare_learned)
+
+    elapsed, e2e_time, p_el, f_el, l_el = max_over_ranks(
+        [elapsed, e2e_time, plain['elapsed'] if plain else 0.0, fast['elapsed'] if fast else 0.0,
+         learned['elapsed'] if learned else 0.0], world)
     if rank == 0:
         hbm, peak_kind = peaks()
         s = 4 if args.storage == 'FP32' else 2
@@ -368,11 +380,16 @@ def run_b200(args):
                            "final_rel_div_inf": plain['rel_div']},
                        "speedup_vs_plain": None if plain is None else
                        job_rate(world, args.steps, elapsed) / job_rate(world, plain['steps'], p_el),
-                       "learned_warm_start_mg": None if learned is None else {
+                       "fast_previous_pressure_mg": None if fast is None else {
+                           "steps_per_s": job_rate(world, fast['steps'], f_el), "steps": fast['steps'],
+                           "v_cycles_mean": statistics.mean(fast['cycles']),
+                           "final_rel_div_inf": fast['rel_div'], "storage": args.storage,
+                           "method": "over-corrected V(4,4) cycles from the previous step's pressure"},
+                       "plain_cycles_from_network": None if learned is None else {
                            "steps_per_s": job_rate(world, learned['steps'], l_el), "steps": learned['steps'],
                            "v_cycles_mean": statistics.mean(learned['cycles']),
                            "final_rel_div_inf": learned['rel_div'], "storage": args.storage,
-                           "method": "stand-alone V(4,4) cycles from the U-Net's guess (net on the 128^3 "
+                           "method": "the reference's V(4,4) cycles from the U-Net's guess (net on the 128^3 "
                                      "restriction, trilinear prolongation)"}},
             "cell_updates_per_s": world * args.steps * cells / elapsed,
             "passes": pass_report,
@@ -735,12 +752,13 @@ def main():
     ap.add_argument('--impl', default='b200', choices=('b200', 'reference'))
     ap.add_argument('--size', type=int, default=256)
     ap.add_argument('--storage', default='FP32', choices=('FP32', 'BF16'))
-    ap.add_argument('--variant', default='fast', choices=tuple(VARIANTS))
+    ap.add_argument('--variant', default='learned', choices=tuple(VARIANTS))
     ap.add_argument('--seed', type=int, default=0)
     ap.add_argument('--cpu-sample', type=int, default=64)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')
     ap.add_argument('--no-compare-plain', dest='compare_plain', action='store_false')
     ap.add_argument('--no-compare-learned', dest='compare_learned', action='store_false')
+    ap.add_argument('--no-compare-fast', dest='compare_fast', action='store_false')
     ap.add_argument('--set', action='append', default=[], metavar='NAME=VALUE',
                     help='settings override of the headline variant (repeatable)')
     ap.add_argument('--coarse-scale', type=float, default=None,

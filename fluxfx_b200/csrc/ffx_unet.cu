@@ -459,26 +459,34 @@ __global__ void __launch_bounds__(kGemmThreads) conv_fwd_tc_kernel(const __grid_
 }
 
 // ------------------------------- 3^3 convolution: TMA halo tile + tcgen05
-// Stride-1, pad-1 3x3x3 layers without a gather. A block owns an output tile
-// of 8 (x) x 16 (y) x bz (z) voxels; its input footprint, a 10 x 18 x (bz + 2)
-// halo tile, comes in by one TMA tensor load per 8-channel plane (zero-filled
-// outside the grid, which is the padding). In shared memory a plane is laid
-// out [z][y][x][8 channels], 16 bytes per voxel, so for every tap (dz, dy, dx)
-// the 128 rows (8 x-voxels x 16 y-rows) of the A operand are the canonical
-// no-swizzle K-major core matrices of a shifted window: start = the tap's
-// first voxel, 8-row groups one halo row (160 B) apart, the two 8-channel
-// halves of K = 16 one plane apart. No data moves per tap: a K = 16 channel
-// group costs 27 x bz MMAs (M = 128, N = BN) on one staged tile. The weights
-// of a group, pre-packed into the MN-major core-matrix image of all 27 taps,
-// arrive by one bulk copy. A producer thread (TMA) and an MMA thread hand the
-// stages over through mbarriers (full: loads landed; empty: the stage's MMAs
-// completed, via tcgen05.commit); the bz accumulators (128 x BN FP32 each)
-// stay in tensor memory until the epilogue. Every wait is bounded; on timeout
-// the block counts it in g_conv_timeouts, lets its copies and MMAs drain
-// (bounded), frees its tensor memory and returns.
+// Stride-1, pad-1 3x3x3 layers without a gather. A work tile is an output
+// block of 8 (x) x 16 (y) x bz (z) voxels and BN output channels; its input
+// footprint, a 10 x 18 x (bz + 2) halo tile, comes in by one TMA tensor load
+// per 8-channel plane (zero-filled outside the grid, which is the padding).
+// In shared memory a plane is laid out [z][y][x][8 channels], 16 bytes per
+// voxel, so for every tap (dz, dy, dx) the 128 rows (8 x-voxels x 16 y-rows)
+// of the A operand are the canonical no-swizzle K-major core matrices of a
+// shifted window: start = the tap's first voxel, 8-row groups one halo row
+// (160 B) apart, the two 8-channel halves of K = 16 one plane apart. No data
+// moves per tap: a K = 16 channel group costs 27 x bz MMAs (M = 128, N = BN)
+// on one staged tile. The weights of a group, pre-packed into the MN-major
+// core-matrix image of all 27 taps, arrive by one bulk copy with the planes.
+//
+// The kernel is persistent and warp-specialised: warp 4 (one thread) issues
+// the loads of tile after tile into a ring of stages, warp 5 (one thread)
+// issues the MMAs into one of two accumulator sets in tensor memory (bz x BN
+// FP32 columns each), and warps 0-3 drain the other set (tcgen05.ld, bias,
+// ReLU, accumulation, BF16 or FP32 stores), so a tile's loads, its MMAs and
+// the previous tile's epilogue overlap. mbarriers hand over stages (full: the
+// loads landed; empty: the stage's MMAs completed, by tcgen05.commit) and
+// accumulator sets (acc_full by tcgen05.commit, acc_empty by the four
+// epilogue warps). Every wait is bounded and also ends when another role has
+// given up (a shared abort flag); the block then counts a timeout in
+// g_conv_timeouts, lets its copies and MMAs drain (bounded), frees its tensor
+// memory and returns.
 constexpr int kTmX = 8, kTmY = 16;                   // output tile in x, y (M = 128)
 constexpr int kTmHX = kTmX + 2, kTmHY = kTmY + 2;    // halo tile
-constexpr int kTmThreads = 128;
+constexpr int kTmThreads = 192;                      // warps 0-3 epilogue, 4 loads, 5 MMAs
 constexpr int kTmMaxStages = 4;
 constexpr int kTmSmemLimit = 200 * 1024;             // dynamic shared memory attribute of the kernels
 
@@ -487,11 +495,13 @@ struct TmaConv {
     const bf16* wpack;        // packed weights: [cout / BN][groups][27][BN / 8][16][8]
     int batch, d, h, w;       // grid (input = output)
     int cin, cout, groups;    // groups = ceil(cin / 16) channel groups of K = 16
-    int bz, tiles_x, tiles_y, tiles_z;
+    int bz, tiles_x, tiles_y, tiles_z, nblocks;
+    int tiles;                // work tiles: tiles_x * tiles_y * tiles_z * batch * nblocks
     int stages, planes;       // planes loaded per group (1 when cin == 8)
     uint32_t plane;           // bytes of one plane in shared memory (multiple of 128)
     uint32_t stage;           // bytes of one stage: 2 planes + 27 weight tiles
     uint32_t tx;              // bytes a stage's loads deliver
+    uint32_t cols;            // tensor-memory columns allocated (2 accumulator sets)
     const float* bias;
     int relu, accumulate;
     bf16* out;
@@ -500,25 +510,57 @@ struct TmaConv {
     int out_f32_pitch;
 };
 
+struct TmTile {
+    int nb, x0, y0, z0, b;
+};
+__device__ __forceinline__ TmTile tm_tile(const TmaConv& P, int t) {
+    TmTile r;
+    r.nb = t % P.nblocks;
+    t /= P.nblocks;
+    r.x0 = (t % P.tiles_x) * kTmX;
+    t /= P.tiles_x;
+    r.y0 = (t % P.tiles_y) * kTmY;
+    t /= P.tiles_y;
+    r.z0 = (t % P.tiles_z) * P.bz;
+    r.b = t / P.tiles_z;
+    return r;
+}
+
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
 
+// Bounded wait that also gives up once another role has set `abort`.
+__device__ __forceinline__ bool tm_wait(uint32_t bar, uint32_t parity, const volatile int* abort) {
+    for (int i = 0; i < kTcSpin; ++i) {
+        uint32_t done;
+        asm volatile(
+            "{\n\t.reg .pred p;\n\t"
+            "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+            "selp.u32 %0, 1, 0, p;\n\t}\n"
+            : "=r"(done)
+            : "r"(bar), "r"(parity)
+            : "memory");
+        if (done) return true;
+        if ((i & 255) == 255 && *abort) return false;
+    }
+    return false;
+}
+
 // The halo planes of group g (channels 16g .. 16g + 15) and its packed weights.
 template <int BN>
-__device__ __forceinline__ void tm_issue_loads(const TmaConv& P, uint32_t st, uint32_t bar, int g, int b, int x0,
-                                               int y0, int z0, int nb) {
+__device__ __forceinline__ void tm_issue_loads(const TmaConv& P, uint32_t st, uint32_t bar, int g, const TmTile& T) {
     mbar_expect_tx(bar, P.tx);
     const uint64_t map = reinterpret_cast<uint64_t>(&P.act);
     for (int h = 0; h < P.planes; ++h)
         asm volatile(
             "cp.async.bulk.tensor.5d.shared::cluster.global.tile.mbarrier::complete_tx::bytes "
             "[%0], [%1, {%2, %3, %4, %5, %6}], [%7];"
-            ::"r"(st + h * P.plane), "l"(map), "r"(16 * g + 8 * h), "r"(x0 - 1), "r"(y0 - 1), "r"(z0 - 1), "r"(b),
-              "r"(bar)
+            ::"r"(st + h * P.plane), "l"(map), "r"(16 * g + 8 * h), "r"(T.x0 - 1), "r"(T.y0 - 1), "r"(T.z0 - 1),
+              "r"(T.b), "r"(bar)
             : "memory");
     constexpr uint32_t kWBytes = 27u * 32u * BN;
-    const bf16* src = P.wpack + ((size_t)nb * P.groups + g) * (kWBytes / 2);
+    const bf16* src = P.wpack + ((size_t)T.nb * P.groups + g) * (kWBytes / 2);
     asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
                  ::"r"(st + 2 * P.plane), "l"(src), "r"(kWBytes), "r"(bar)
                  : "memory");
@@ -537,42 +579,105 @@ __device__ __forceinline__ void tm_commit(uint32_t bar) {
                  : "memory");
 }
 
+// Epilogue of one tile: warp w reads tensor-memory lanes 32w .. 32w + 31 (the
+// tile's rows m = 8 y + x) of accumulator set `acc`.
 template <int BN>
-__global__ void __launch_bounds__(kTmThreads) conv3_tma_kernel(const __grid_constant__ TmaConv P) {
+__device__ __forceinline__ void tm_epilogue(const TmaConv& P, const TmTile& T, uint32_t acc, int warp, int lane) {
+    const int m = warp * 32 + lane;
+    const int x = T.x0 + (m & 7), y = T.y0 + (m >> 3);
+    const uint32_t lane_addr = acc + ((uint32_t)(warp * 32) << 16);
+    for (int j = 0; j < P.bz; ++j) {
+        const int z = T.z0 + j;
+        const bool in = x < P.w && y < P.h && z < P.d;
+        const long long vox = (((long long)T.b * P.d + z) * P.h + y) * P.w + x;
+#pragma unroll
+        for (int c0 = 0; c0 < BN; c0 += 16) {
+            uint32_t r[16];
+            asm volatile(
+                "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
+                "[%16];"
+                : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+                  "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),
+                  "=r"(r[15])
+                : "r"(lane_addr + (uint32_t)(j * BN + c0)));
+            asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+            if (!in) continue;
+            const int n = T.nb * BN + c0;
+            float v[16];
+#pragma unroll
+            for (int e = 0; e < 16; ++e) {
+                v[e] = __uint_as_float(r[e]);
+                if (P.bias) v[e] += __ldg(P.bias + n + e);
+                if (P.relu) v[e] = fmaxf(v[e], 0.f);
+            }
+            if (P.out) {
+                uint4* o = reinterpret_cast<uint4*>(P.out + vox * P.out_pitch + P.out_offset + n);
+#pragma unroll
+                for (int q = 0; q < 2; ++q) {
+                    if (P.accumulate) {
+                        const uint4 prev = o[q];
+                        const __nv_bfloat162* pv = reinterpret_cast<const __nv_bfloat162*>(&prev);
+#pragma unroll
+                        for (int e = 0; e < 4; ++e) {
+                            const float2 f = __bfloat1622float2(pv[e]);
+                            v[8 * q + 2 * e] += f.x;
+                            v[8 * q + 2 * e + 1] += f.y;
+                        }
+                    }
+                    uint4 pk;
+                    __nv_bfloat162* pp = reinterpret_cast<__nv_bfloat162*>(&pk);
+#pragma unroll
+                    for (int e = 0; e < 4; ++e) pp[e] = __floats2bfloat162_rn(v[8 * q + 2 * e], v[8 * q + 2 * e + 1]);
+                    o[q] = pk;
+                }
+            }
+            if (P.out_f32) {
+                float* o = P.out_f32 + vox * P.out_f32_pitch + n;
+#pragma unroll
+                for (int e = 0; e < 16; ++e) o[e] = v[e];
+            }
+        }
+    }
+}
+
+template <int BN>
+__global__ void __launch_bounds__(kTmThreads, 1) conv3_tma_kernel(const __grid_constant__ TmaConv P) {
     static_assert(BN == 16 || BN == 32 || BN == 64, "BN");
     extern __shared__ __align__(128) unsigned char tm_smem[];
-    __shared__ __align__(8) uint64_t full[kTmMaxStages], empty[kTmMaxStages], done;
+    __shared__ __align__(8) uint64_t full[kTmMaxStages], empty[kTmMaxStages], acc_full[2], acc_empty[2], drained;
     __shared__ uint32_t tmem_base;
+    __shared__ int abort_word;
+    volatile int* abort_flag = &abort_word;
     const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-    int t = blockIdx.x;
-    const int tx = t % P.tiles_x;
-    t /= P.tiles_x;
-    const int ty = t % P.tiles_y;
-    t /= P.tiles_y;
-    const int tz = t % P.tiles_z;
-    const int b = t / P.tiles_z;
-    const int x0 = tx * kTmX, y0 = ty * kTmY, z0 = tz * P.bz;
-    const int nb = blockIdx.y;
     const uint32_t base = (smem_u32(tm_smem) + 127u) & ~127u;
-    const uint32_t cols = P.bz * BN <= 32 ? 32u : (P.bz * BN <= 64 ? 64u : (P.bz * BN <= 128 ? 128u : 256u));
+    const uint32_t acc_cols = (uint32_t)(P.bz * BN);
+    const int S = P.stages;
 
-    if (warp == 0) {
+    if (warp == 5) {
         asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;"
-                     ::"r"(smem_u32(&tmem_base)), "r"(cols));
+                     ::"r"(smem_u32(&tmem_base)), "r"(P.cols));
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;");
     }
     if (P.planes == 1) {
-        // cin == 8: the second channel half of K is zero (one group, one stage)
-        for (uint32_t i = tid * 16; i < P.plane; i += kTmThreads * 16)
-            asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(base + P.plane + i), "r"(0u) : "memory");
+        // cin == 8: the second channel half of K is zero in every stage
+        for (int s = 0; s < S; ++s)
+            for (uint32_t i = tid * 16; i < P.plane; i += kTmThreads * 16)
+                asm volatile("st.shared.v4.u32 [%0], {%1, %1, %1, %1};" ::"r"(base + s * P.stage + P.plane + i),
+                             "r"(0u)
+                             : "memory");
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
     }
     if (tid == 0) {
-        for (int s = 0; s < P.stages; ++s) {
+        abort_word = 0;
+        for (int s = 0; s < S; ++s) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&full[s])));
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&empty[s])));
         }
-        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&done)));
+        for (int a = 0; a < 2; ++a) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&acc_full[a])));
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 4;" ::"r"(smem_u32(&acc_empty[a])));
+        }
+        asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(smem_u32(&drained)));
         asm volatile("fence.mbarrier_init.release.cluster;");
     }
     asm volatile("tcgen05.fence::before_thread_sync;");
@@ -580,118 +685,95 @@ __global__ void __launch_bounds__(kTmThreads) conv3_tma_kernel(const __grid_cons
     asm volatile("tcgen05.fence::after_thread_sync;");
     const uint32_t tmem = tmem_base;
 
-    bool ok = true;
-    int issued = 0;
-    if (warp == 0 && lane == 0) {
-        // producer
-        for (int g = 0; g < P.groups; ++g) {
-            const int s = g % P.stages;
-            if (g >= P.stages && !mbar_wait(smem_u32(&empty[s]), (uint32_t)(((g / P.stages) - 1) & 1))) {
-                ok = false;
-                break;
+    if (warp == 4) {
+        if (lane == 0) {
+            // loads: tile after tile, group after group, into the stage ring
+            int q = 0;
+            for (int t = blockIdx.x; t < P.tiles && !*abort_flag; t += gridDim.x) {
+                const TmTile T = tm_tile(P, t);
+                for (int g = 0; g < P.groups; ++g, ++q) {
+                    const int s = q % S;
+                    if (q >= S && !tm_wait(smem_u32(&empty[s]), (uint32_t)(((q / S) - 1) & 1), abort_flag)) {
+                        *abort_flag = 1;
+                        break;
+                    }
+                    tm_issue_loads<BN>(P, base + s * P.stage, smem_u32(&full[s]), g, T);
+                }
             }
-            tm_issue_loads<BN>(P, base + s * P.stage, smem_u32(&full[s]), g, b, x0, y0, z0, nb);
-            ++issued;
+            // the last load of every stage has landed before the block may exit
+            for (int k = q > S ? q - S : 0; k < q; ++k) mbar_wait(smem_u32(&full[k % S]), (uint32_t)((k / S) & 1));
         }
-    } else if (warp == 1 && lane == 0) {
-        // MMA issuer: D[j] += A(tap, z-slice j) x B(tap) over 27 taps and bz slices per group
-        const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(BN >> 3) << 17) |
-                               ((uint32_t)(128 >> 4) << 24);
-        for (int g = 0; g < P.groups; ++g) {
-            const int s = g % P.stages;
-            if (!mbar_wait(smem_u32(&full[s]), (uint32_t)((g / P.stages) & 1))) {
-                ok = false;
+    } else if (warp == 5) {
+        if (lane == 0) {
+            // MMAs: D[set][j] += A(tap, z slice j) x B(tap), 27 taps x bz slices per group
+            const uint32_t idesc = (1u << 4) | (1u << 7) | (1u << 10) | (1u << 16) | ((uint32_t)(BN >> 3) << 17) |
+                                   ((uint32_t)(128 >> 4) << 24);
+            int q = 0, it = 0;
+            for (int t = blockIdx.x; t < P.tiles && !*abort_flag; t += gridDim.x, ++it) {
+                const int a = it & 1;
+                if (it >= 2 && !tm_wait(smem_u32(&acc_empty[a]), (uint32_t)(((it >> 1) - 1) & 1), abort_flag)) {
+                    *abort_flag = 1;
+                    break;
+                }
+                asm volatile("tcgen05.fence::after_thread_sync;");
+                const uint32_t d0 = tmem + (uint32_t)a * acc_cols;
+                bool ok = true;
+                for (int g = 0; g < P.groups; ++g, ++q) {
+                    const int s = q % S;
+                    if (!tm_wait(smem_u32(&full[s]), (uint32_t)((q / S) & 1), abort_flag)) {
+                        ok = false;
+                        break;
+                    }
+                    asm volatile("tcgen05.fence::after_thread_sync;");
+                    const uint32_t st = base + s * P.stage;
+                    const uint64_t da0 = umma_desc(st, P.plane, kTmHX * 16);
+                    const uint64_t db0 = umma_desc(st + 2 * P.plane, 128, 256);
+                    for (int j = 0; j < P.bz; ++j) {
+                        // descriptor start addresses advance in 16-byte units (no carry: shared memory < 256 KB)
+                        const uint64_t daj = da0 + (uint64_t)(j * kTmHY * kTmHX);
+#pragma unroll
+                        for (int tap = 0; tap < 27; ++tap) {
+                            const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
+                            tm_mma(d0 + (uint32_t)(j * BN), daj + (uint64_t)((dz * kTmHY + dy) * kTmHX + dx),
+                                   db0 + (uint64_t)(tap * 2 * BN), idesc, (g > 0 || tap > 0) ? 1u : 0u);
+                        }
+                    }
+                    tm_commit(smem_u32(&empty[s]));
+                }
+                if (!ok) {
+                    *abort_flag = 1;
+                    break;
+                }
+                tm_commit(smem_u32(&acc_full[a]));
+            }
+            // every MMA issued has completed before tensor memory is freed
+            tm_commit(smem_u32(&drained));
+            mbar_wait(smem_u32(&drained), 0);
+        }
+    } else {
+        // epilogue warps 0-3
+        int it = 0;
+        for (int t = blockIdx.x; t < P.tiles; t += gridDim.x, ++it) {
+            const int a = it & 1;
+            const bool ok = !*abort_flag && tm_wait(smem_u32(&acc_full[a]), (uint32_t)((it >> 1) & 1), abort_flag);
+            if (!__all_sync(0xffffffffu, ok)) {
+                *abort_flag = 1;
                 break;
             }
             asm volatile("tcgen05.fence::after_thread_sync;");
-            const uint32_t st = base + s * P.stage;
-            const uint32_t wt = st + 2 * P.plane;
-            for (int j = 0; j < P.bz; ++j) {
-#pragma unroll 3
-                for (int tap = 0; tap < 27; ++tap) {
-                    const int dz = tap / 9, dy = (tap / 3) % 3, dx = tap % 3;
-                    const uint32_t a = st + (uint32_t)((((j + dz) * kTmHY + dy) * kTmHX + dx) * 16);
-                    const uint64_t da = umma_desc(a, P.plane, kTmHX * 16);
-                    const uint64_t db = umma_desc(wt + (uint32_t)(tap * 32 * BN), 128, 256);
-                    tm_mma(tmem + (uint32_t)(j * BN), da, db, idesc, (g > 0 || tap > 0) ? 1u : 0u);
-                }
-            }
-            tm_commit(smem_u32(&empty[s]));
+            tm_epilogue<BN>(P, tm_tile(P, t), tmem + (uint32_t)a * acc_cols, warp, lane);
+            asm volatile("tcgen05.fence::before_thread_sync;");
+            __syncwarp();
+            if (lane == 0)
+                asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(&acc_empty[a])) : "memory");
         }
-        tm_commit(smem_u32(&done));   // tracks every MMA this thread issued
     }
     __syncwarp();
-    const bool failed = __syncthreads_or(!ok);
-    const bool finished = mbar_wait(smem_u32(&done), 0);
-    if (failed || !finished) {
-        if (tid == 0) {
-            atomicAdd(&g_conv_timeouts, 1);
-            // let the loads this block issued land before its shared memory is released
-            for (int g = issued > P.stages ? issued - P.stages : 0; g < issued; ++g)
-                mbar_wait(smem_u32(&full[g % P.stages]), (uint32_t)((g / P.stages) & 1));
-        }
-    } else {
-        asm volatile("tcgen05.fence::after_thread_sync;");
-        const int m = warp * 32 + lane;
-        const int x = x0 + (m & 7), y = y0 + (m >> 3);
-        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
-        for (int j = 0; j < P.bz; ++j) {
-            const int z = z0 + j;
-            const bool in = x < P.w && y < P.h && z < P.d;
-            const long long vox = (((long long)b * P.d + z) * P.h + y) * P.w + x;
-#pragma unroll
-            for (int c0 = 0; c0 < BN; c0 += 16) {
-                uint32_t r[16];
-                asm volatile(
-                    "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15}, "
-                    "[%16];"
-                    : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]),
-                      "=r"(r[7]), "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]),
-                      "=r"(r[14]), "=r"(r[15])
-                    : "r"(lane_addr + (uint32_t)(j * BN + c0)));
-                asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
-                if (!in) continue;
-                const int n = nb * BN + c0;
-                float v[16];
-#pragma unroll
-                for (int e = 0; e < 16; ++e) {
-                    v[e] = __uint_as_float(r[e]);
-                    if (P.bias) v[e] += __ldg(P.bias + n + e);
-                    if (P.relu) v[e] = fmaxf(v[e], 0.f);
-                }
-                if (P.out) {
-                    uint4* o = reinterpret_cast<uint4*>(P.out + vox * P.out_pitch + P.out_offset + n);
-#pragma unroll
-                    for (int q = 0; q < 2; ++q) {
-                        if (P.accumulate) {
-                            const uint4 prev = o[q];
-                            const __nv_bfloat162* pv = reinterpret_cast<const __nv_bfloat162*>(&prev);
-#pragma unroll
-                            for (int e = 0; e < 4; ++e) {
-                                const float2 f = __bfloat1622float2(pv[e]);
-                                v[8 * q + 2 * e] += f.x;
-                                v[8 * q + 2 * e + 1] += f.y;
-                            }
-                        }
-                        uint4 pk;
-                        __nv_bfloat162* pp = reinterpret_cast<__nv_bfloat162*>(&pk);
-#pragma unroll
-                        for (int e = 0; e < 4; ++e) pp[e] = __floats2bfloat162_rn(v[8 * q + 2 * e], v[8 * q + 2 * e + 1]);
-                        o[q] = pk;
-                    }
-                }
-                if (P.out_f32) {
-                    float* o = P.out_f32 + vox * P.out_f32_pitch + n;
-#pragma unroll
-                    for (int e = 0; e < 16; ++e) o[e] = v[e];
-                }
-            }
-        }
-    }
     asm volatile("tcgen05.fence::before_thread_sync;");
     __syncthreads();
-    if (warp == 0)
-        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(cols));
+    if (tid == 0 && abort_word) atomicAdd(&g_conv_timeouts, 1);
+    if (warp == 5)
+        asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.cols));
 }
 
 // Packed weights of the TMA convolution: w[k = tap * cin + c][cout] ->
@@ -1105,7 +1187,7 @@ int ffx_conv_forward_tma(const FfxConv* c, const void* packed, void* stream) {
     P.planes = a.cin == 8 ? 1 : 2;
     P.tiles_x = (a.iw + kTmX - 1) / kTmX;
     P.tiles_y = (a.ih + kTmY - 1) / kTmY;
-    // deepest tile (z slices sharing one halo) that still gives every SM two blocks
+    // deepest tile (z slices sharing one halo) that still gives every SM two tiles
     const long long nblocks = a.cout / bn;
     const long long want = 2LL * sm_count();
     P.bz = 1;
@@ -1114,15 +1196,23 @@ int ffx_conv_forward_tma(const FfxConv* c, const void* packed, void* stream) {
         if (blocks >= want || bz == 1) { P.bz = bz; break; }
     }
     P.tiles_z = (a.id + P.bz - 1) / P.bz;
+    P.nblocks = (int)nblocks;
+    const long long tiles = (long long)P.tiles_x * P.tiles_y * P.tiles_z * a.batch * nblocks;
+    FFX_REQUIRE(tiles < (1LL << 31), "ffx_conv_forward_tma: too many tiles");
+    P.tiles = (int)tiles;
     const uint32_t box_bytes = 8u * kTmHX * kTmHY * (uint32_t)(P.bz + 2) * 2u;
     P.plane = (box_bytes + 127u) & ~127u;
     P.stage = 2 * P.plane + 27u * 32u * (uint32_t)bn;
     P.tx = (uint32_t)P.planes * box_bytes + 27u * 32u * (uint32_t)bn;
-    P.stages = std::max(1, std::min({P.groups, kTmMaxStages, (int)((110u * 1024u) / P.stage)}));
+    // as many stages as fit (the ring runs across tiles), at most four
+    P.stages = std::min(kTmMaxStages, (int)((kTmSmemLimit - 128u) / P.stage));
+    FFX_REQUIRE(P.stages >= 1, "ffx_conv_forward_tma: a stage does not fit in shared memory");
     const size_t smem = (size_t)P.stages * P.stage + 128;
-    FFX_REQUIRE(smem <= (size_t)kTmSmemLimit, "ffx_conv_forward_tma: stage does not fit in shared memory");
-    const long long blocks = (long long)P.tiles_x * P.tiles_y * P.tiles_z * a.batch;
-    FFX_REQUIRE(blocks < (1LL << 31) && nblocks < 65536, "ffx_conv_forward_tma: grid too large");
+    const uint32_t need = 2u * (uint32_t)P.bz * (uint32_t)bn;    // two accumulator sets
+    P.cols = need <= 32 ? 32u : (need <= 64 ? 64u : (need <= 128 ? 128u : (need <= 256 ? 256u : 512u)));
+    FFX_REQUIRE(need <= 512, "ffx_conv_forward_tma: accumulators exceed tensor memory");
+    // persistent: one block per SM (the stage ring fills its shared memory)
+    const long long blocks = std::min<long long>(tiles, sm_count());
     P.bias = a.bias;
     P.relu = a.relu;
     P.accumulate = a.accumulate;
@@ -1149,7 +1239,7 @@ int ffx_conv_forward_tma(const FfxConv* c, const void* packed, void* stream) {
         cudaFuncSetAttribute(conv3_tma_kernel<64>, cudaFuncAttributeMaxDynamicSharedMemorySize, kTmSmemLimit);
         configured = true;
     }
-    const dim3 grid((unsigned)blocks, (unsigned)nblocks, 1);
+    const dim3 grid((unsigned)blocks, 1, 1);
     cudaStream_t st = as_stream(stream);
     if (bn == 16) conv3_tma_kernel<16><<<grid, kTmThreads, smem, st>>>(P);
     else if (bn == 32) conv3_tma_kernel<32><<<grid, kTmThreads, smem, st>>>(P);

@@ -92,6 +92,7 @@ class UNet:
         # pre-packed weights, the other shapes on the mma.sync kernel; the default)
         self.conv_entry = 'ffx_conv_forward_tma'
         self.weight_version = 0      # bumped when the weights change (repacks the TMA weights)
+        self.calls = 0               # library calls issued (each launches one kernel)
         self._packs = {}
 
     # ------------------------------------------------------------- buffers
@@ -191,6 +192,7 @@ class UNet:
 
     def _call(self, name, *args):
         N.check(getattr(self.lib, name)(*args))
+        self.calls += 1
 
     def _run_conv(self, key, c, s):
         """One convolution through the selected entry; the TMA entry gets the
@@ -200,7 +202,7 @@ class UNet:
             self._call(self.conv_entry, C.byref(c), s)
             return
         n = N.i64(0)
-        self._call('ffx_conv_packed_bytes', C.byref(c), C.byref(n))
+        N.check(self.lib.ffx_conv_packed_bytes(C.byref(c), C.byref(n)))    # a host query, no launch
         packed = None
         if n.value:
             entry = self._packs.get(key)

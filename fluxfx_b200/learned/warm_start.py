@@ -82,7 +82,9 @@ class LearnedWarmStart:
             out.zero_()
             return
         scale = 1.0 / m
+        calls = self.net.calls
         pred = self.net.forward(src.unsqueeze(0), self.mask.unsqueeze(0), scale, s.value or 0)
+        dev.calls += self.net.calls - calls     # the network's launches count with the solver's
         target = self.coarse if self.factor > 1 else out
         dev.call('ffx_unpack_channel', src.numel(), ptr(self.net.pred), HEAD_CHANNELS, 1.0 / (scale * self.weight),
                  ptr(target), s)
