@@ -182,6 +182,8 @@ _PROTOTYPES = {
     'ffx_pack_input': (C.c_int, [i64, vp, vp, f32, vp, vp]),
     'ffx_mse_grad': (C.c_int, [i64, vp, i32, vp, vp, f32, vp, vp, vp]),
     'ffx_unpack_channel': (C.c_int, [i64, vp, i32, f32, vp, vp]),
+    'ffx_unpack_channel_scaled': (C.c_int, [i64, vp, i32, vp, C.c_double, vp, vp]),
+    'ffx_pack_input_scaled': (C.c_int, [i64, vp, vp, vp, vp, vp]),
     'ffx_mask_restrict': (C.c_int, [n3, vp, i32, vp, vp]),
     'ffx_curl': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, vp]),
     'ffx_confine': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f32, f32, vp, vp, vp, vp]),

@@ -935,9 +935,15 @@ __global__ void adam_kernel(long long n, float* w, float* m, float* v, const flo
 
 // Network input: channel 0 = scale * divergence, channel 1 = solid mask,
 // channels 2..7 = 0 (the first convolution reads 8 channels).
+// out = src * scale; with `max_abs`, scale = 1 / (input_scale * weight) in
+// FP64 (0 for a zero input), the factor that undoes the input normalisation.
 __global__ void unpack_channel_kernel(long long voxels, const float* __restrict__ src, int pitch, float scale,
-                                      float* __restrict__ out) {
+                                      const float* max_abs, double weight, float* __restrict__ out) {
     const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (max_abs) {
+        const float m = *max_abs;
+        scale = m > 0.f ? (float)(1.0 / ((1.0 / (double)m) * weight)) : 0.f;
+    }
     if (i < voxels) out[i] = src[i * pitch] * scale;
 }
 
@@ -957,9 +963,19 @@ __global__ void mask_restrict_kernel(int cx, int cy, int cz, const uint8_t* __re
     coarse[c] = n >= threshold ? 1 : 0;
 }
 
-__global__ void pack_input_kernel(long long voxels, const float* div, const uint8_t* mask, float scale, bf16* out) {
+// Scale of the network's input from max |div| on the device: 1 / max (0 when
+// the field is zero), the FP32 rounding of the FP64 quotient, as a host would
+// form it.
+__device__ __forceinline__ float input_scale(const float* max_abs) {
+    const float m = *max_abs;
+    return m > 0.f ? (float)(1.0 / (double)m) : 0.f;
+}
+
+__global__ void pack_input_kernel(long long voxels, const float* div, const uint8_t* mask, float scale,
+                                  const float* max_abs, bf16* out) {
     const long long v = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     if (v >= voxels) return;
+    if (max_abs) scale = input_scale(max_abs);
     __align__(16) bf16 c[8];
     c[0] = __float2bfloat16_rn(scale * div[v]);
     c[1] = __float2bfloat16_rn(mask && mask[v] ? 1.f : 0.f);
@@ -1312,7 +1328,17 @@ int ffx_weight_transpose(int32_t taps, int32_t cin, int32_t cout, int32_t flip, 
 
 int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float scale, void* out, void* stream) {
     FFX_REQUIRE(voxels >= 1 && div && out && ((uintptr_t)out & 15) == 0, "ffx_pack_input: invalid arguments");
-    pack_input_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, div, mask, scale, (bf16*)out);
+    pack_input_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, div, mask, scale, nullptr,
+                                                                            (bf16*)out);
+    return launch_status("pack_input_kernel");
+}
+
+int ffx_pack_input_scaled(int64_t voxels, const float* div, const uint8_t* mask, const float* max_abs, void* out,
+                          void* stream) {
+    FFX_REQUIRE(voxels >= 1 && div && max_abs && out && ((uintptr_t)out & 15) == 0,
+                "ffx_pack_input_scaled: invalid arguments");
+    pack_input_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, div, mask, 0.f, max_abs,
+                                                                            (bf16*)out);
     return launch_status("pack_input_kernel");
 }
 
@@ -1330,7 +1356,16 @@ int ffx_mask_restrict(const int32_t coarse_n[3], const uint8_t* fine, int32_t th
 
 int ffx_unpack_channel(int64_t voxels, const float* src, int32_t pitch, float scale, float* out, void* stream) {
     FFX_REQUIRE(voxels >= 1 && src && out && pitch >= 1, "ffx_unpack_channel: invalid arguments");
-    unpack_channel_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, src, pitch, scale, out);
+    unpack_channel_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, src, pitch, scale, nullptr,
+                                                                                0.0, out);
+    return launch_status("unpack_channel_kernel");
+}
+
+int ffx_unpack_channel_scaled(int64_t voxels, const float* src, int32_t pitch, const float* max_abs, double weight,
+                              float* out, void* stream) {
+    FFX_REQUIRE(voxels >= 1 && src && max_abs && out && pitch >= 1, "ffx_unpack_channel_scaled: invalid arguments");
+    unpack_channel_kernel<<<blocks_for(voxels, 256), 256, 0, as_stream(stream)>>>(voxels, src, pitch, 0.f, max_abs,
+                                                                                weight, out);
     return launch_status("unpack_channel_kernel");
 }
 

@@ -216,13 +216,18 @@ class UNet:
         self._call('ffx_conv_forward_tma', C.byref(c), _p(packed), s)
 
     # ------------------------------------------------------------ forward
-    def forward(self, div, mask, scale, stream):
+    def forward(self, div, mask, scale, stream, max_abs=None):
         """div: (B, D, H, W) float32, mask: uint8 or None; returns the FP32
-        prediction view (B, D, H, W) (channel 0 of the head output)."""
+        prediction view (B, D, H, W) (channel 0 of the head output). The input
+        is div * scale, or div / max|div| read on the device from `max_abs` (a
+        one-element FP32 tensor) when it is given."""
         batch, D, H, W = div.shape
         self._buffers(batch, (D, H, W))
         s = C.c_void_p(stream)
-        self._call('ffx_pack_input', div.numel(), _p(div), _p(mask), float(scale), _p(self.x), s)
+        if max_abs is not None:
+            self._call('ffx_pack_input_scaled', div.numel(), _p(div), _p(mask), _p(max_abs), _p(self.x), s)
+        else:
+            self._call('ffx_pack_input', div.numel(), _p(div), _p(mask), float(scale), _p(self.x), s)
         for name, lin, ins, lout, out, pitch, offset in self.graph:
             layer = self.by_name[name]
             if name == 'head':

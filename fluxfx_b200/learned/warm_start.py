@@ -76,18 +76,15 @@ class LearnedWarmStart:
             src = self.div
             if self.fine_mask is not None:
                 dev.call('ffx_mask_restrict', N.n3(*self.shape), ptr(self.fine_mask), 4, ptr(self.mask), s)
+        # the input scale 1 / max|div| stays on the device (no readback in the step);
+        # a zero divergence gives a zero guess through the zero unpacking factor
         dev.call('ffx_max_abs', src.numel(), N.FFX_F32, ptr(src), ptr(self._max), s)
-        m = float(self._max.item())
-        if m == 0.0:
-            out.zero_()
-            return
-        scale = 1.0 / m
         calls = self.net.calls
-        pred = self.net.forward(src.unsqueeze(0), self.mask.unsqueeze(0), scale, s.value or 0)
+        pred = self.net.forward(src.unsqueeze(0), self.mask.unsqueeze(0), None, s.value or 0, max_abs=self._max)
         dev.calls += self.net.calls - calls     # the network's launches count with the solver's
         target = self.coarse if self.factor > 1 else out
-        dev.call('ffx_unpack_channel', src.numel(), ptr(self.net.pred), HEAD_CHANNELS, 1.0 / (scale * self.weight),
-                 ptr(target), s)
+        dev.call('ffx_unpack_channel_scaled', src.numel(), ptr(self.net.pred), HEAD_CHANNELS, ptr(self._max),
+                 float(self.weight), ptr(target), s)
         if self.factor > 1:
             dev.call('ffx_mg_prolong', N.n3(*self.grid.shape), ptr(self.zero), ptr(self.coarse), ptr(out), s)
         return pred

@@ -583,6 +583,10 @@ int ffx_adam(int64_t n, float* w, float* m, float* v, const float* g, void* w_bf
 /* Network input, 8 BF16 channels per voxel: scale * div, solid mask, zeros. */
 int ffx_pack_input(int64_t voxels, const float* div, const uint8_t* mask, float scale, void* out,
                    void* stream);
+/* The same with scale = 1 / *max_abs (0 when *max_abs is 0) formed on the device, so the
+ * caller need not read max |div| back (max_abs: ffx_max_abs of div). */
+int ffx_pack_input_scaled(int64_t voxels, const float* div, const uint8_t* mask, const float* max_abs,
+                          void* out, void* stream);
 /* Collider mask of the 2x coarser grid (dims coarse_n): 1 where at least `threshold`
  * of the eight children are nonzero. */
 int ffx_mask_restrict(const int32_t coarse_n[3], const uint8_t* fine, int32_t threshold, uint8_t* coarse,
@@ -590,6 +594,10 @@ int ffx_mask_restrict(const int32_t coarse_n[3], const uint8_t* fine, int32_t th
 /* out[v] = src[v * pitch] * scale: one channel of the FP32 network output as a cell field. */
 int ffx_unpack_channel(int64_t voxels, const float* src, int32_t pitch, float scale, float* out,
                        void* stream);
+/* The same with scale = 1 / ((1 / *max_abs) * weight) formed on the device in FP64 (0 when
+ * *max_abs is 0): the factor that undoes ffx_pack_input_scaled's normalisation. */
+int ffx_unpack_channel_scaled(int64_t voxels, const float* src, int32_t pitch, const float* max_abs,
+                              double weight, float* out, void* stream);
 /* *loss += sum over fluid voxels of (pred - target)^2 * inv_count; grad (8 BF16
  * channels per voxel) = its derivative in channel 0. */
 int ffx_mse_grad(int64_t voxels, const float* pred, int32_t pred_pitch, const float* target,

@@ -241,6 +241,40 @@ def test_weight_gradients_match_torch(lib, kind):
     assert rel_err(db, bl.grad) < 1e-4
 
 
+@pytest.mark.parametrize('zero', [False, True])
+def test_device_scaled_input_and_output_match_host_scaling(lib, zero):
+    """The network's input packing and output unpacking with the scale read on
+    the device from max|div| give the host-scaled results bit for bit (and a
+    zero guess for a zero divergence)."""
+    g = torch.Generator().manual_seed(9)
+    n = 4096
+    div = torch.zeros(n) if zero else torch.randn(n, generator=g) * 3.0
+    mask = (torch.rand(n, generator=g) < 0.2).to(torch.uint8)
+    ddiv, dmask = div.cuda(), mask.cuda()
+    mx = torch.zeros(1, device='cuda')
+    N.check(lib.ffx_max_abs(n, N.FFX_F32, C.c_void_p(ddiv.data_ptr()), C.c_void_p(mx.data_ptr()), None))
+    torch.cuda.synchronize()
+    m = float(mx.item())
+    a = torch.zeros((n, 8), dtype=torch.bfloat16, device='cuda')
+    b = torch.zeros_like(a)
+    N.check(lib.ffx_pack_input(n, C.c_void_p(ddiv.data_ptr()), C.c_void_p(dmask.data_ptr()),
+                               (1.0 / m) if m else 0.0, C.c_void_p(a.data_ptr()), None))
+    N.check(lib.ffx_pack_input_scaled(n, C.c_void_p(ddiv.data_ptr()), C.c_void_p(dmask.data_ptr()),
+                                      C.c_void_p(mx.data_ptr()), C.c_void_p(b.data_ptr()), None))
+    src = torch.randn((n, 8), generator=g).cuda()
+    weight = 16384.0
+    u1, u2 = torch.full((n,), 7.0, device='cuda'), torch.full((n,), 7.0, device='cuda')
+    N.check(lib.ffx_unpack_channel(n, C.c_void_p(src.data_ptr()), 8, (1.0 / ((1.0 / m) * weight)) if m else 0.0,
+                                   C.c_void_p(u1.data_ptr()), None))
+    N.check(lib.ffx_unpack_channel_scaled(n, C.c_void_p(src.data_ptr()), 8, C.c_void_p(mx.data_ptr()), weight,
+                                          C.c_void_p(u2.data_ptr()), None))
+    torch.cuda.synchronize()
+    assert torch.equal(a, b)
+    assert torch.equal(u1, u2)
+    if zero:
+        assert float(u2.abs().max()) == 0.0
+
+
 def test_adam_matches_formula(lib):
     n = 1000
     g = torch.Generator().manual_seed(3)
