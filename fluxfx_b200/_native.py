@@ -90,9 +90,13 @@ BATCH_MAX = 64
 BATCH_LEVELS = 8
 (PASS_PREDICTOR, PASS_VELOCITY, PASS_DIVERGENCE, PASS_SCALE, PASS_GRADIENT, PASS_SCALAR_PREDICTOR,
  PASS_SCALAR_REVERSE, PASS_SCALAR_FINAL, PASS_RESIDUAL_MAX, PASS_SMOOTH, PASS_RESIDUAL_RESTRICT, PASS_PROLONG_SMOOTH,
- PASS_DIRECT, PASS_KINDS) = range(14)
+ PASS_DIRECT, PASS_L0_SMOOTH, PASS_L0_PROLONG_SMOOTH, PASS_L0_RESIDUAL_RESTRICT, PASS_L0_RESIDUAL_MAX,
+ PASS_KINDS) = range(18)
 PASS_NAMES = ('predictor', 'velocity', 'divergence', 'scale', 'gradient', 'scalar_predictor', 'scalar_reverse',
-              'scalar_final', 'residual_max', 'smooth', 'residual_restrict', 'prolong_smooth', 'direct')
+              'scalar_final', 'residual_max', 'smooth', 'residual_restrict', 'prolong_smooth', 'direct',
+              'l0_smooth', 'l0_prolong_smooth', 'l0_residual_restrict', 'l0_residual_max')
+# pass kinds with a fixed tile (the level-0 four-cell kernels' 32 x 8 block): only the grid is tuned
+FIXED_TILE_PASSES = (PASS_L0_SMOOTH, PASS_L0_PROLONG_SMOOTH, PASS_L0_RESIDUAL_RESTRICT, PASS_L0_RESIDUAL_MAX)
 
 
 class FfxBatchLevel(C.Structure):

@@ -37,7 +37,7 @@ SHAPES = ((32, 8), (64, 4), (128, 2), (16, 16))
 GRIDS = (0, 1, 2, 4)
 TUNABLE = (N.PASS_PREDICTOR, N.PASS_VELOCITY, N.PASS_DIVERGENCE, N.PASS_SCALE, N.PASS_GRADIENT,
            N.PASS_SCALAR_PREDICTOR, N.PASS_SCALAR_REVERSE, N.PASS_SCALAR_FINAL, N.PASS_RESIDUAL_MAX, N.PASS_SMOOTH,
-           N.PASS_RESIDUAL_RESTRICT, N.PASS_PROLONG_SMOOTH)
+           N.PASS_RESIDUAL_RESTRICT, N.PASS_PROLONG_SMOOTH) + N.FIXED_TILE_PASSES
 
 
 def _check_solver(i, s):
@@ -230,7 +230,7 @@ class BatchedSmoke:
         best = {}
         for kind in TUNABLE:
             results = []
-            for shape in range(len(SHAPES)):
+            for shape in ((0,) if kind in N.FIXED_TILE_PASSES else range(len(SHAPES))):
                 for grid in GRIDS:
                     N.check(self.lib.ffx_batch_set_config(self.plan, kind, shape, grid))
                     N.check(self.lib.ffx_batch_tune_pass(self.plan, kind, self.stream))

@@ -144,6 +144,10 @@ size_t desc_size(int kind) {
         case kScalarFinal: return batch::scalar_final_desc(z, 0, nullptr);
         case kDirect: return batch::direct_desc(z, nullptr, nullptr);
         case kTail: return batch::tail_desc(z, 0, 0, nullptr);
+        case kL0Smooth:
+        case kL0ProlongSmooth:
+        case kL0ResidualRestrict:
+        case kL0ResidualMax: return batch::l0_desc(FfxGraphLevel{}, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
         default: return batch::level_desc(FfxGraphLevel{}, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr);
     }
 }
@@ -211,6 +215,11 @@ FfxBatchPlan::Entry entry_for(int kind, int slot, int nx, int ny, int nz) {
         case kPredictor:
         case kVelocity: return {slot, nx + 1, ny + 1, 3 * (nz + 1)};
         case kResidualRestrict: return {slot, nx / 2, ny / 2, nz / 2};
+        // level 0, four cells per thread: x in units of 4 cells, kL0Slices z per thread
+        case kL0Smooth:
+        case kL0ProlongSmooth:
+        case kL0ResidualMax: return {slot, nx / kL0Cells, ny, (nz + kL0Slices - 1) / kL0Slices};
+        case kL0ResidualRestrict: return {slot, nx / kL0Cells, ny / 2, (nz + kL0Slices - 1) / kL0Slices};
         case kScaleZero: return {slot, nx * ny * nz, 1, 1};
         case kDirect: return {slot, nx * ny * nz, 1, 1};
         default: return {slot, nx, ny, nz};
@@ -223,6 +232,10 @@ BatchMap make_map(const FfxBatchPlan& P, const FfxBatchPlan::Launch& L) {
     memset(&M, 0, sizeof M);
     const int kind = L.kind;
     int bw = kShapes[P.shape[kind < kBatchKinds ? kind : 0]][0], bh = kShapes[P.shape[kind < kBatchKinds ? kind : 0]][1];
+    if (is_l0_kind(kind)) {   // the four-cell kernels' block: 32 lanes x kL0Rows rows
+        bw = 32;
+        bh = kL0Rows;
+    }
     M.count = (int)L.entries.size();
     int64_t total = 0;
     for (int k = 0; k < M.count; ++k) {
@@ -248,6 +261,7 @@ BatchMap make_map(const FfxBatchPlan& P, const FfxBatchPlan::Launch& L) {
 int resident(int kind) {
     int r = batch::advect_resident_blocks(kind);
     if (!r) r = batch::project_resident_blocks(kind);
+    if (!r) r = batch::level0_resident_blocks(kind);
     return r > 0 ? r : 1;
 }
 
@@ -273,6 +287,10 @@ cudaError_t issue(FfxBatchPlan& P, const FfxBatchPlan::Launch& L, cudaStream_t s
         case kResidualRestrict: return batch::residual_restrict(M, d, P.state, g, st);
         case kProlongSmooth: return batch::prolong_smooth(M, d, P.state, g, st);
         case kDirect: return batch::direct(M, d, P.state, g, st);
+        case kL0Smooth: return batch::l0_smooth(M, d, P.state, g, st);
+        case kL0ProlongSmooth: return batch::l0_prolong_smooth(M, d, P.state, g, st);
+        case kL0ResidualRestrict: return batch::l0_residual_restrict(M, d, P.state, g, st);
+        case kL0ResidualMax: return batch::l0_residual_max(M, d, P.state, g, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -303,6 +321,17 @@ struct Builder {
     }
 };
 
+// Level 0 of a domain qualifies for the four-cell kernels: link field, x a
+// multiple of 4, 16-byte aligned fields, even y and z, and a level below it
+// (whose rhs and iterate the restriction and prolongation address as float2).
+bool l0_domain(const FfxBatchDomain& D) {
+    if (D.levels < 2) return false;
+    const FfxBatchLevel& L = D.level[0];
+    const FfxBatchLevel& C = D.level[1];
+    return batch::l0_eligible(L.level, {L.p, L.q, L.rhs}) && L.level.ny % 2 == 0 && L.level.nz % 2 == 0 &&
+           ((uintptr_t)C.rhs & 7) == 0 && ((uintptr_t)C.p & 7) == 0 && ((uintptr_t)C.q & 7) == 0;
+}
+
 std::vector<int> all_slots(const FfxBatchPlan& P) {
     std::vector<int> s;
     for (int d = 0; d < P.count; ++d) s.push_back(d);
@@ -332,12 +361,31 @@ void build_cycle(Builder& B) {
         if (kind == kSmooth && k == 0) e.Z = (lv.nz + kBatchZ0 - 1) / kBatchZ0;   // streamed along z
         return e;
     };
+    // level 0 runs four cells per thread when every domain of the launch qualifies
+    auto x4 = [&](int k, const std::vector<int>& slots) {
+        if (k != 0) return false;
+        for (int d : slots)
+            if (!l0_domain(P.dom[d])) return false;
+        return true;
+    };
+    auto l0_entry = [&](int kind, int d) {
+        const FfxGraphLevel& lv = P.dom[d].level[0].level;
+        return entry_for(kind, d, lv.nx, lv.ny, lv.nz);
+    };
     auto smooth_at = [&](int k, const std::vector<int>& slots) {
-        P.cycle.push_back(B.launch(kSmooth, slots, [&](int d, char* out, FfxBatchPlan::Entry& e) {
-            const FfxBatchLevel& L = P.dom[d].level[k];
-            batch::level_desc(L.level, cur(d, k), other(d, k), L.rhs, nullptr, nullptr, out);
-            e = level_entry(kSmooth, d, k);
-        }));
+        if (x4(k, slots)) {
+            P.cycle.push_back(B.launch(kL0Smooth, slots, [&](int d, char* out, FfxBatchPlan::Entry& e) {
+                const FfxBatchLevel& L = P.dom[d].level[0];
+                batch::l0_desc(L.level, cur(d, 0), nullptr, L.rhs, other(d, 0), nullptr, out);
+                e = l0_entry(kL0Smooth, d);
+            }));
+        } else {
+            P.cycle.push_back(B.launch(kSmooth, slots, [&](int d, char* out, FfxBatchPlan::Entry& e) {
+                const FfxBatchLevel& L = P.dom[d].level[k];
+                batch::level_desc(L.level, cur(d, k), other(d, k), L.rhs, nullptr, nullptr, out);
+                e = level_entry(kSmooth, d, k);
+            }));
+        }
         for (int d : slots) role[d][k] ^= 1;
     };
     // down
@@ -346,13 +394,20 @@ void build_cycle(Builder& B) {
         for (int d = 0; d < n; ++d)
             if (k < top[d]) act.push_back(d);
         for (int s = 0; s < P.dom[act[0]].pre; ++s) smooth_at(k, act);
-        P.cycle.push_back(B.launch(kResidualRestrict, act, [&](int d, char* out, FfxBatchPlan::Entry& e) {
+        const bool four = x4(k, act);
+        P.cycle.push_back(B.launch(four ? kL0ResidualRestrict : kResidualRestrict, act,
+                                   [&](int d, char* out, FfxBatchPlan::Entry& e) {
             const FfxBatchDomain& D = P.dom[d];
             const FfxBatchLevel& L = D.level[k];
             const bool tail_next = D.tail_start == k + 1;
-            batch::level_desc(L.level, cur(d, k), nullptr, L.rhs, D.level[k + 1].rhs,
-                              tail_next ? nullptr : cur(d, k + 1), out);
-            e = level_entry(kResidualRestrict, d, k);
+            float* zero = tail_next ? nullptr : cur(d, k + 1);
+            if (four) {
+                batch::l0_desc(L.level, cur(d, 0), nullptr, L.rhs, D.level[1].rhs, zero, out);
+                e = l0_entry(kL0ResidualRestrict, d);
+            } else {
+                batch::level_desc(L.level, cur(d, k), nullptr, L.rhs, D.level[k + 1].rhs, zero, out);
+                e = level_entry(kResidualRestrict, d, k);
+            }
         }));
     }
     // coarse stage
@@ -396,10 +451,17 @@ void build_cycle(Builder& B) {
         std::vector<int> act;
         for (int d = 0; d < n; ++d)
             if (k < top[d]) act.push_back(d);
-        P.cycle.push_back(B.launch(kProlongSmooth, act, [&](int d, char* out, FfxBatchPlan::Entry& e) {
+        const bool four = x4(k, act);
+        P.cycle.push_back(B.launch(four ? kL0ProlongSmooth : kProlongSmooth, act,
+                                   [&](int d, char* out, FfxBatchPlan::Entry& e) {
             const FfxBatchLevel& L = P.dom[d].level[k];
-            batch::level_desc(L.level, cur(d, k), other(d, k), L.rhs, cur(d, k + 1), nullptr, out);
-            e = level_entry(kProlongSmooth, d, k);
+            if (four) {
+                batch::l0_desc(L.level, cur(d, 0), cur(d, 1), L.rhs, other(d, 0), nullptr, out);
+                e = l0_entry(kL0ProlongSmooth, d);
+            } else {
+                batch::level_desc(L.level, cur(d, k), other(d, k), L.rhs, cur(d, k + 1), nullptr, out);
+                e = level_entry(kProlongSmooth, d, k);
+            }
         }));
         for (int d : act) role[d][k] ^= 1;
         for (int s = 1; s < P.dom[act[0]].post; ++s) smooth_at(k, act);
@@ -475,10 +537,17 @@ int build(FfxBatchPlan& P, std::vector<char>& host) {
             e = cells(kScalarFinal, d);
         }));
     }
-    P.resmax = B.launch(kResidualMax, all, [&](int d, char* out, FfxBatchPlan::Entry& e) {
+    bool four = true;
+    for (int d = 0; d < P.count; ++d) four = four && l0_domain(P.dom[d]);
+    P.resmax = B.launch(four ? kL0ResidualMax : kResidualMax, all, [&](int d, char* out, FfxBatchPlan::Entry& e) {
         const FfxBatchLevel& L = P.dom[d].level[0];
-        batch::level_desc(L.level, L.p, nullptr, L.rhs, nullptr, nullptr, out);
-        e = cells(kResidualMax, d);
+        if (four) {
+            batch::l0_desc(L.level, L.p, nullptr, L.rhs, nullptr, nullptr, out);
+            e = entry_for(kL0ResidualMax, d, L.level.nx, L.level.ny, L.level.nz);
+        } else {
+            batch::level_desc(L.level, L.p, nullptr, L.rhs, nullptr, nullptr, out);
+            e = cells(kResidualMax, d);
+        }
     });
     build_cycle(B);
     // tuning launches: each kind once over every domain, writing scratch only
@@ -493,7 +562,7 @@ int build(FfxBatchPlan& P, std::vector<char>& host) {
         for (auto* list : {&P.pre[0], &P.post[0], &P.cycle})
             for (auto& L : *list)
                 if (L.kind == kind && (!found || volume(L) > volume(*found))) found = &L;
-        if (kind == kResidualMax) found = &P.resmax;
+        if ((kind == kResidualMax || kind == kL0ResidualMax) && P.resmax.kind == kind) found = &P.resmax;
         if (kind == kGradient) {
             P.tune[kind] = B.launch(kGradient, all, [&](int d, char* out, FfxBatchPlan::Entry& e) {
                 const FfxBatchDomain& D = P.dom[d];
@@ -635,7 +704,7 @@ int ffx_batch_tune_pass(FfxBatchPlan* plan, int32_t kind, void* stream) {
     cudaStream_t st = as_stream(stream);
     int e = cuda_status(issue(*plan, plan->tune[kind], st), "ffx_batch_tune_pass");
     if (e) return e;
-    if (kind == kScaleZero || kind == kGradient || kind == kResidualMax) {
+    if (kind == kScaleZero || kind == kGradient || kind == kResidualMax || kind == kL0ResidualMax) {
         batch_clear_kernel<<<1, 64, 0, st>>>(plan->state, plan->count);
         return launch_status("ffx_batch_tune_pass: clear");
     }

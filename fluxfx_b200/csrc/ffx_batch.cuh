@@ -11,6 +11,7 @@
 // solver's convergence state) live in BatchState.
 #pragma once
 #include <cstring>
+#include <initializer_list>
 
 #include "ffx_common.cuh"
 
@@ -110,8 +111,12 @@ struct NoPrep {
 // Pass kinds (the autotuner's keys; FFX_PASS_* in ffx.h).
 enum BatchKind {
     kPredictor = 0, kVelocity, kDivergence, kScaleZero, kGradient, kScalarPredictor, kScalarReverse, kScalarFinal,
-    kResidualMax, kSmooth, kResidualRestrict, kProlongSmooth, kDirect, kBatchKinds
+    kResidualMax, kSmooth, kResidualRestrict, kProlongSmooth, kDirect,
+    // level 0 four cells per thread (link field, nx % 4 == 0): tiles of 32 x 8 threads
+    kL0Smooth, kL0ProlongSmooth, kL0ResidualRestrict, kL0ResidualMax, kBatchKinds
 };
+constexpr bool is_l0_kind(int k) { return k >= kL0Smooth && k <= kL0ResidualMax; }
+constexpr int kL0Cells = 4, kL0Rows = 8, kL0Slices = 8;   // cells per thread along x, rows per tile, z per thread
 
 // Internal descriptor builders and launchers of the batched passes. A builder
 // writes the descriptor of one domain to `out` (when not NULL) and returns its
@@ -147,9 +152,20 @@ cudaError_t residual_restrict(const BatchMap& M, const void* descs, BatchState* 
 cudaError_t prolong_smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st);
 cudaError_t direct(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st);
 cudaError_t tail(const BatchMap& M, const void* descs, BatchState* state, cudaStream_t st);
+// Level 0, four cells per thread (ffx_level0.cu): whether a level and its
+// fields qualify; descriptor (p, coarse iterate for the prolongation, rhs,
+// output: the sweep's or the restriction's coarse rhs, coarse iterate to clear).
+bool l0_eligible(const FfxGraphLevel& lv, std::initializer_list<const void*> f4);
+size_t l0_desc(const FfxGraphLevel& lv, const float* p, const float* coarse, const float* rhs, float* out, float* zero,
+               void* dst);
+cudaError_t l0_smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st);
+cudaError_t l0_prolong_smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st);
+cudaError_t l0_residual_restrict(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st);
+cudaError_t l0_residual_max(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st);
 // Resident blocks per SM of a pass kind's kernel (0: not this file's kind).
 int advect_resident_blocks(int kind);
 int project_resident_blocks(int kind);
+int level0_resident_blocks(int kind);
 }  // namespace batch
 
 }  // namespace ffx

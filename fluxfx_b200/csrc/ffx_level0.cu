@@ -23,6 +23,10 @@
 // linked, and diag + 0 == diag, nb + 0 * v == nb for finite v, so the sums are
 // the same (nb never holds -0: it starts at +0 and an exact cancellation
 // rounds to +0).
+#include <algorithm>
+#include <cstring>
+
+#include "ffx_batch.cuh"
 #include "ffx_common.cuh"
 #include "ffx_host.cuh"
 #include "ffx_level0.cuh"
@@ -33,6 +37,8 @@ namespace {
 constexpr unsigned kXm = 1u, kXp = 2u, kYm = 4u, kYp = 8u, kZm = 16u, kZp = 32u, kFluid = 64u;
 constexpr int kZ4 = 8;           // slices per thread column (even: the restriction pairs slices)
 constexpr int kRows = 8;         // warps (rows) per block
+static_assert(kZ4 == kL0Slices && kRows == kL0Rows && 32 * kRows == kBatchThreads,
+              "the batched level-0 tiles are this file's blocks");
 
 struct L0 {
     int nx, ny, nz, nx4;
@@ -168,13 +174,17 @@ __device__ __forceinline__ void block_sum_d(double* out, double v) {
 // written. Block (32, kRows): lane = x4 within a 128-cell row segment, warp =
 // row; blockIdx.z = column of kZ4 slices. Threads outside the grid stay in the
 // loop (with zero data) so that shuffles and the block reduction see every lane.
+//
+// The body takes the block's coordinates (bx, by, bz) and the thread's lane
+// and row (warp), so the same code runs as its own launch (level0_kernel) and
+// as a tile of a batched persistent launch over many domains.
 template <It K, Ep E>
-__global__ void __launch_bounds__(32 * kRows, 4) level0_kernel(L0 g, ItArgs A, EpArgs P) {
-    const int lane = threadIdx.x;
-    const int x4 = blockIdx.x * 32 + lane, y = blockIdx.y * kRows + threadIdx.y;
+__device__ __forceinline__ void level0_body(const L0& g, const ItArgs& A, const EpArgs& P, int bx, int by, int bz,
+                                            int lane, int row) {
+    const int x4 = bx * 32 + lane, y = by * kRows + row;
     const bool active = x4 < g.nx4 && y < g.ny;
     const int x0 = 4 * x4;
-    const int z0 = blockIdx.z * kZ4, zend = min(z0 + kZ4, g.nz);
+    const int z0 = bz * kZ4, zend = min(z0 + kZ4, g.nz);
     const int row4 = g.nx4, slice4 = g.nx4 * g.ny;
     int i4 = x4 + row4 * (y + g.ny * z0);
     const float one_minus = 1.f - P.omega;
@@ -255,6 +265,12 @@ __global__ void __launch_bounds__(32 * kRows, 4) level0_kernel(L0 g, ItArgs A, E
     if constexpr (E == Ep::ResidualMax) block_max_to(P.fmax, m);
 }
 
+template <It K, Ep E>
+__global__ void __launch_bounds__(32 * kRows, 4) level0_kernel(L0 g, ItArgs A, EpArgs P) {
+    level0_body<K, E>(g, A, P, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)threadIdx.x,
+                      (int)threadIdx.y);
+}
+
 // First sweep from a zero iterate (graph_smooth_zero_kernel): no iterate is
 // read, so this is a plain stream over links and rhs.
 __global__ void __launch_bounds__(256) level0_smooth_zero_kernel(L0 g, const float* __restrict__ rhs, float omega,
@@ -279,15 +295,13 @@ __global__ void __launch_bounds__(256) level0_smooth_zero_kernel(L0 g, const flo
 // a thread owns a 4 x 2 (x, y) patch, i.e. two coarse cells along x, and walks
 // pairs of slices; each coarse value sums its eight children's residuals in
 // the scalar kernel's order (dz, then dy, then dx) and divides by 8.
-__global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0 g, const float* __restrict__ p,
-                                                                             const float* __restrict__ rhs,
-                                                                             float* __restrict__ coarse,
-                                                                             float* __restrict__ zero) {
-    const int lane = threadIdx.x;
-    const int x4 = blockIdx.x * 32 + lane, ya = 2 * (blockIdx.y * kRows + threadIdx.y), yb = ya + 1;
+__device__ __forceinline__ void level0_restrict_body(const L0& g, const float* __restrict__ p,
+                                                     const float* __restrict__ rhs, float* __restrict__ coarse,
+                                                     float* __restrict__ zero, int bx, int by, int bz, int lane,
+                                                     int row) {
+    const int x4 = bx * 32 + lane, ya = 2 * (by * kRows + row), yb = ya + 1;
     const bool active = x4 < g.nx4 && ya < g.ny;
-    const int x0 = 4 * x4;
-    const int z0 = blockIdx.z * kZ4, zend = min(z0 + kZ4, g.nz);
+    const int z0 = bz * kZ4, zend = min(z0 + kZ4, g.nz);
     const int row4 = g.nx4, slice4 = g.nx4 * g.ny;
     int ia = x4 + row4 * (ya + g.ny * z0);
     float4 lo_a = zero4(), c_a = zero4(), lo_b = zero4(), c_b = zero4();
@@ -346,6 +360,14 @@ __global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0
     }
 }
 
+__global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0 g, const float* __restrict__ p,
+                                                                             const float* __restrict__ rhs,
+                                                                             float* __restrict__ coarse,
+                                                                             float* __restrict__ zero) {
+    level0_restrict_body(g, p, rhs, coarse, zero, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z,
+                         (int)threadIdx.x, (int)threadIdx.y);
+}
+
 __global__ void __launch_bounds__(256) links_kernel(int nx, int ny, int nz, const uint8_t* __restrict__ solid,
                                                    uint8_t* __restrict__ links) {
     int x, y, z;
@@ -363,6 +385,76 @@ __global__ void __launch_bounds__(256) links_kernel(int nx, int ny, int nz, cons
         if (z + 1 < nz && __ldg(solid + i + sz) == 0) b |= kZp;
     }
     links[i] = (uint8_t)b;
+}
+
+// ------------------------------------------------- batched level-0 passes
+// Level 0 of many domains in one persistent launch: every domain contributes
+// the blocks of its own level0_kernel launch (32 lanes x kRows rows, kZ4
+// slices per thread; the batched map's tiles are 32 x kRows threads), so each
+// domain's cells are computed exactly as in its stand-alone launch.
+constexpr float kL0Omega = (float)(2.0 / 3.0);   // the weighted-Jacobi factor of the batched sweeps
+
+struct L0Desc {
+    L0 g;
+    const float* p;        // iterate
+    const float* coarse;   // prolongation: the coarse iterate
+    const float* rhs;
+    float* out;            // sweep output, or the coarse right-hand side (restriction)
+    float* zero;           // restriction: coarse iterate to clear (optional)
+};
+
+__global__ void __launch_bounds__(kBatchThreads) batch_l0_smooth_kernel(const __grid_constant__ BatchMap M,
+                                                                        const L0Desc* descs,
+                                                                        const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [](const L0Desc& D, const Blk& b, int) {
+        const EpArgs E{D.rhs, kL0Omega, D.out, nullptr, nullptr, 0.0, nullptr};
+        level0_body<It::Plain, Ep::Smooth>(D.g, ItArgs{D.p, nullptr, nullptr, nullptr}, E, b.x, b.y, b.z,
+                                           (int)threadIdx.x & 31, (int)threadIdx.x >> 5);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_l0_prolong_smooth_kernel(const __grid_constant__ BatchMap M,
+                                                                                const L0Desc* descs,
+                                                                                const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [](const L0Desc& D, const Blk& b, int) {
+        const EpArgs E{D.rhs, kL0Omega, D.out, nullptr, nullptr, 0.0, nullptr};
+        level0_body<It::Prolonged, Ep::Smooth>(D.g, ItArgs{D.p, D.coarse, nullptr, nullptr}, E, b.x, b.y, b.z,
+                                               (int)threadIdx.x & 31, (int)threadIdx.x >> 5);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_l0_residual_restrict_kernel(
+    const __grid_constant__ BatchMap M, const L0Desc* descs, const BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [](const L0Desc& D, const Blk& b, int) {
+        level0_restrict_body(D.g, D.p, D.rhs, D.out, D.zero, b.x, b.y, b.z, (int)threadIdx.x & 31,
+                             (int)threadIdx.x >> 5);
+    });
+}
+
+__global__ void __launch_bounds__(kBatchThreads) batch_l0_residual_max_kernel(const __grid_constant__ BatchMap M,
+                                                                              const L0Desc* descs,
+                                                                              BatchState* state) {
+    for_tiles(M, descs, state, true, NoPrep{}, [state](const L0Desc& D, const Blk& b, int slot) {
+        const int lane = (int)threadIdx.x & 31, row = (int)threadIdx.x >> 5;
+        if (state[slot].scale == 0.f) {
+            // rhs == 0: the solve's result is the zero pressure (and no cycle runs)
+            const int x4 = b.x * 32 + lane, y = b.y * kRows + row;
+            if (x4 < D.g.nx4 && y < D.g.ny)
+                for (int z = b.z * kZ4; z < min(b.z * kZ4 + kZ4, D.g.nz); ++z)
+                    reinterpret_cast<float4*>(const_cast<float*>(D.p))[x4 + D.g.nx4 * (y + D.g.ny * z)] = zero4();
+            return;
+        }
+        const EpArgs E{D.rhs, 0.f, nullptr, nullptr, nullptr, 0.0, &state[slot].res};
+        level0_body<It::Plain, Ep::ResidualMax>(D.g, ItArgs{D.p, nullptr, nullptr, nullptr}, E, b.x, b.y, b.z, lane,
+                                                row);
+    });
+}
+
+template <class K>
+int occupancy_l0(K kernel) {
+    int n = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, kernel, kBatchThreads, 0);
+    return n;
 }
 
 bool aligned(const void* p, uintptr_t a) { return ((uintptr_t)p & (a - 1)) == 0; }
@@ -453,5 +545,56 @@ int level0_links(int nx, int ny, int nz, const uint8_t* solid, uint8_t* links, c
     links_kernel<<<cell_grid(nx, ny, nz), cell_block(), 0, st>>>(nx, ny, nz, solid, links);
     return launch_status("links_kernel");
 }
+
+namespace batch {
+
+bool l0_eligible(const FfxGraphLevel& lv, std::initializer_list<const void*> f4) { return level0_x4(&lv, f4); }
+
+size_t l0_desc(const FfxGraphLevel& lv, const float* p, const float* coarse, const float* rhs, float* out, float* zero,
+               void* dst) {
+    if (dst) {
+        L0Desc D;
+        memset(&D, 0, sizeof D);
+        D.g = make_l0(&lv);
+        D.p = p;
+        D.coarse = coarse;
+        D.rhs = rhs;
+        D.out = out;
+        D.zero = zero;
+        memcpy(dst, &D, sizeof D);
+    }
+    return sizeof(L0Desc);
+}
+
+static unsigned l0_blocks(const BatchMap& M, int grid) { return (unsigned)(grid > 0 ? std::min(grid, M.total) : M.total); }
+
+cudaError_t l0_smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_l0_smooth_kernel<<<l0_blocks(M, grid), kBatchThreads, 0, st>>>(M, (const L0Desc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t l0_prolong_smooth(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_l0_prolong_smooth_kernel<<<l0_blocks(M, grid), kBatchThreads, 0, st>>>(M, (const L0Desc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t l0_residual_restrict(const BatchMap& M, const void* descs, BatchState* state, int grid,
+                                 cudaStream_t st) {
+    batch_l0_residual_restrict_kernel<<<l0_blocks(M, grid), kBatchThreads, 0, st>>>(M, (const L0Desc*)descs, state);
+    return cudaGetLastError();
+}
+cudaError_t l0_residual_max(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
+    batch_l0_residual_max_kernel<<<l0_blocks(M, grid), kBatchThreads, 0, st>>>(M, (const L0Desc*)descs, state);
+    return cudaGetLastError();
+}
+int level0_resident_blocks(int kind) {
+    switch (kind) {
+        case kL0Smooth: return occupancy_l0(batch_l0_smooth_kernel);
+        case kL0ProlongSmooth: return occupancy_l0(batch_l0_prolong_smooth_kernel);
+        case kL0ResidualRestrict: return occupancy_l0(batch_l0_residual_restrict_kernel);
+        case kL0ResidualMax: return occupancy_l0(batch_l0_residual_max_kernel);
+        default: return 0;
+    }
+}
+
+}  // namespace batch
 
 }  // namespace ffx

@@ -501,7 +501,10 @@ int ffx_batch_create(const FfxBatchDomain* domains, int32_t count, void* workspa
 enum {
     FFX_PASS_PREDICTOR = 0, FFX_PASS_VELOCITY, FFX_PASS_DIVERGENCE, FFX_PASS_SCALE, FFX_PASS_GRADIENT,
     FFX_PASS_SCALAR_PREDICTOR, FFX_PASS_SCALAR_REVERSE, FFX_PASS_SCALAR_FINAL, FFX_PASS_RESIDUAL_MAX,
-    FFX_PASS_SMOOTH, FFX_PASS_RESIDUAL_RESTRICT, FFX_PASS_PROLONG_SMOOTH, FFX_PASS_DIRECT, FFX_PASS_KINDS
+    FFX_PASS_SMOOTH, FFX_PASS_RESIDUAL_RESTRICT, FFX_PASS_PROLONG_SMOOTH, FFX_PASS_DIRECT,
+    /* level 0 four cells per thread (link field, nx % 4 == 0; fixed 32 x 8 tiles, grid tuned) */
+    FFX_PASS_L0_SMOOTH, FFX_PASS_L0_PROLONG_SMOOTH, FFX_PASS_L0_RESIDUAL_RESTRICT, FFX_PASS_L0_RESIDUAL_MAX,
+    FFX_PASS_KINDS
 };
 /* Tile shape (0: 32x8, 1: 64x4, 2: 128x2, 3: 16x16 threads) and persistent grid
  * (0: one block per tile; m >= 1: m x the resident blocks of the GPU) of one
