@@ -131,6 +131,77 @@ __device__ __forceinline__ float sample_closed(const Dev& d, const uint8_t* soli
     return zz0 * gz + zz1 * fz;
 }
 
+// sample_closed split in two for several scalars sampled at one point: the
+// stencil (clamped corners, fractions and, with colliders, which corners are
+// fluid and the sum of their weights) is formed once, then applied to each
+// field with sample_closed's operations in its order, so every channel's
+// value is sample_closed's.
+struct ClosedStencil {
+    int rows[4];          // cidx(0, y, z) of (y0, z0), (y1, z0), (y0, z1), (y1, z1)
+    int x0, x1;
+    float fx, fy, fz;
+    unsigned fluid;       // MASK: bit k set when corner k (z, y, x order) is fluid
+    float total;          // MASK: sum of the fluid corners' weights
+};
+
+template <bool MASK>
+__device__ __forceinline__ ClosedStencil closed_stencil(const Dev& d, const uint8_t* solid, float qx, float qy,
+                                                        float qz) {
+    ClosedStencil S;
+    float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
+    S.fx = qx - bx;
+    S.fy = qy - by;
+    S.fz = qz - bz;
+    int ix = floor_int(qx), iy = floor_int(qy), iz = floor_int(qz);
+    S.x0 = min(max(ix, 0), d.nx - 1);
+    S.x1 = min(max(ix + 1, 0), d.nx - 1);
+    const int y0 = min(max(iy, 0), d.ny - 1), y1 = min(max(iy + 1, 0), d.ny - 1);
+    const int z0 = min(max(iz, 0), d.nz - 1), z1 = min(max(iz + 1, 0), d.nz - 1);
+    S.rows[0] = cidx(d, 0, y0, z0);
+    S.rows[1] = cidx(d, 0, y1, z0);
+    S.rows[2] = cidx(d, 0, y0, z1);
+    S.rows[3] = cidx(d, 0, y1, z1);
+    S.fluid = 0u;
+    S.total = 0.f;
+    if (MASK) {
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            const int c = S.rows[k >> 1] + ((k & 1) ? S.x1 : S.x0);
+            if (__ldg(solid + c)) continue;
+            const float wz = (k & 4) ? S.fz : 1.f - S.fz, wy = (k & 2) ? S.fy : 1.f - S.fy,
+                        wx = (k & 1) ? S.fx : 1.f - S.fx;
+            S.fluid |= 1u << k;
+            S.total = S.total + wx * wy * wz;
+        }
+    }
+    return S;
+}
+
+template <typename T, bool MASK>
+__device__ __forceinline__ float apply_closed(const ClosedStencil& S, const T* __restrict__ f) {
+    if (MASK) {
+        float value = 0.f;
+#pragma unroll
+        for (int k = 0; k < 8; ++k) {
+            if (!(S.fluid & (1u << k))) continue;
+            const float wz = (k & 4) ? S.fz : 1.f - S.fz, wy = (k & 2) ? S.fy : 1.f - S.fy,
+                        wx = (k & 1) ? S.fx : 1.f - S.fx;
+            value = value + wx * wy * wz * Store<T>::ld(f, S.rows[k >> 1] + ((k & 1) ? S.x1 : S.x0));
+        }
+        return S.total > 1e-8f ? value / S.total : 0.f;
+    }
+    float f000 = Store<T>::ld(f, S.rows[0] + S.x0), f100 = Store<T>::ld(f, S.rows[0] + S.x1);
+    float f010 = Store<T>::ld(f, S.rows[1] + S.x0), f110 = Store<T>::ld(f, S.rows[1] + S.x1);
+    float f001 = Store<T>::ld(f, S.rows[2] + S.x0), f101 = Store<T>::ld(f, S.rows[2] + S.x1);
+    float f011 = Store<T>::ld(f, S.rows[3] + S.x0), f111 = Store<T>::ld(f, S.rows[3] + S.x1);
+    const float fx = S.fx, fy = S.fy, fz = S.fz;
+    float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
+    float a0 = f000 * gx + f100 * fx, a1 = f010 * gx + f110 * fx;
+    float b0 = f001 * gx + f101 * fx, b1 = f011 * gx + f111 * fx;
+    float zz0 = a0 * gy + a1 * fy, zz1 = b0 * gy + b1 * fy;
+    return zz0 * gz + zz1 * fz;
+}
+
 // ------------------------------------------------------------ face predictor
 template <typename T>
 struct PredParams {
@@ -376,8 +447,8 @@ __device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, c
     F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, P.dt);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
-    for (int c = 0; c < P.count; ++c)
-        Store<T>::st(P.out[c], i, sample_closed<T, MASK>(d, P.solid, P.in[c], qx, qy, qz));
+    const ClosedStencil S = closed_stencil<MASK>(d, P.solid, qx, qy, qz);
+    for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, apply_closed<T, MASK>(S, P.in[c]));
     if (P.dep) {
         P.dep[i] = dep.x;
         P.dep[i + P.n] = dep.y;
@@ -464,10 +535,13 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
                 rows[3] = cidx(d, 0, cy1, cz1);
             }
             const SrcDev& S = P.src;
+            // the semi-Lagrangian sample (the stored predictor value when it is the same)
+            const bool stored = reuse && sizeof(T) == 4;
+            ClosedStencil St;
+            if (!stored) St = closed_stencil<MASK>(d, P.solid, qx, qy, qz);
             for (int c = 0; c < P.count; ++c) {
                 const Channel<T>& C = P.ch[c];
-                float value = (reuse && sizeof(T) == 4) ? Store<T>::ld(C.pred, i)
-                                                        : sample_closed<T, MASK>(d, P.solid, C.field, qx, qy, qz);
+                float value = stored ? Store<T>::ld(C.pred, i) : apply_closed<T, MASK>(St, C.field);
                 if (ok) {
                     float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
                     float lo = Store<T>::ld(C.field, rows[0] + cx0), hi = lo;
