@@ -265,6 +265,26 @@ def grid_struct(shape, extent):
     return FfxGrid(nx, ny, nz, *[float(e) for e in extent], *inv)
 
 
+def face_starts_match(shape, extent):
+    """True when the face predictor's start point (x + o) h and the velocity
+    correction's (x + o) e / n (times 1/n on power-of-two grids) are the same
+    FP32 value for every face coordinate x + o (o = 0, 1/2) of every axis --
+    the library's own test (ffx_common.cuh, face_starts_match) in NumPy FP32.
+    The correction then reuses the predictor's face departure points."""
+    import numpy as np
+    p2 = grid_pow2(shape, extent)
+    for n, e in zip(shape, extent):
+        e32, n32 = np.float32(e), np.float32(n)
+        h32 = np.float32(e32 / n32)
+        x = (np.arange(n + 1, dtype=np.float32)[:, None] + np.array([0.0, 0.5], dtype=np.float32)).ravel()
+        a = x * h32
+        xe = x * e32
+        b = xe * np.float32(np.float32(1.0) / n32) if p2 else xe / n32
+        if not np.array_equal(a, b):
+            return False
+    return True
+
+
 def grid_pow2(shape, extent):
     """True when every FP32 extent, cell count and spacing (extent / count in
     FP32) is a power of two: the kernels then divide by exact reciprocals and

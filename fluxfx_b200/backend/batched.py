@@ -137,9 +137,9 @@ class BatchedSmoke:
         D.warm_start = int(st.solid_warm_start)
         D.tolerance = st.pressure_tolerance
         # departure points of the predictor passes, reused by the correction passes
-        # (faces on power-of-two grids only), as the single-domain step does
+        # (faces where both passes form the same start points), as the single-domain step does
         dev = s.device.device
-        if D.velocity_corrected and det.reuse_traces and det._pow2:
+        if D.velocity_corrected and det.reuse_traces and det._face_reuse:
             if det.face_trace is None:
                 det.face_trace = [torch.empty(3 * prod(sh), dtype=torch.float32, device=dev)
                                   for sh in s.grid.face_shapes]

@@ -29,11 +29,11 @@ class DetailPasses:
         self.face_predictor = None
         self.curl = None
         # departure points of the predictor passes, reused by the correction passes
-        # (faces only on power-of-two grids, where both passes trace the same point)
+        # (faces only where both passes form the same start point at every face)
         self.reuse_traces = True
         self.face_trace = None
         self.cell_trace = None
-        self._pow2 = N.grid_pow2(grid.shape, grid.extent)
+        self._face_reuse = N.face_starts_match(grid.shape, grid.extent)
 
     @property
     def allocated_bytes(self):
@@ -76,7 +76,7 @@ class DetailPasses:
         """Predict each signed face component; the reverse sample is fused with the correction."""
         if self.face_predictor is None:
             self.face_predictor = [self.device.texture(s, dtype=self.dtype) for s in self.grid.face_shapes]
-        if self.reuse_traces and self._pow2 and self.face_trace is None:
+        if self.reuse_traces and self._face_reuse and self.face_trace is None:
             self.face_trace = [torch.empty(3 * prod(s), dtype=torch.float32, device=self.device.device)
                                for s in self.grid.face_shapes]
         self.device.call('ffx_face_predictor_trace', C.byref(self._g), C.byref(self._solids), self._storage,
@@ -85,7 +85,7 @@ class DetailPasses:
 
     def face_traces(self):
         """The face departure points as a C array of three pointers, or NULL."""
-        if not (self.reuse_traces and self._pow2 and self.face_trace is not None):
+        if not (self.reuse_traces and self._face_reuse and self.face_trace is not None):
             return None
         return (C.c_void_p * 3)(*[t.data_ptr() for t in self.face_trace])
 

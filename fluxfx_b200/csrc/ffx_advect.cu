@@ -285,10 +285,11 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
                 dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
         F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * f.x + (axis != 0), 2 * f.y + (axis != 1),
                                          2 * f.z + (axis != 2));
-        // The predictor pass traced the same start point on power-of-two grids
-        // (there (x + o) h and (x + o) e / n are the same exact product), so its
-        // departure point, and in FP32 storage its sample, are this pass's.
-        const bool reuse = P2 && P.corrected && P.dep[axis] != nullptr;
+        // The host passes the predictor's departure points only when both passes
+        // form the same start point at every face (face_starts_match); the
+        // predictor then traced this face's start point with the same velocity,
+        // so its departure point, and in FP32 storage its sample, are this pass's.
+        const bool reuse = P.corrected && P.dep[axis] != nullptr;
         F3 dep;
         if (reuse) {
             const float* D = P.dep[axis];
@@ -727,6 +728,8 @@ int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
                 "must both be given for buoyancy");
     FFX_REQUIRE(blend >= 0.f && blend <= 1.f, "ffx_advect_velocity: blend must lie in [0, 1]");
     Dev d = make_dev(*g);
+    // departure points are reused only where both passes form the same start points
+    const bool starts = dep && corrected && face_starts_match(d);
     dim3 blocks = face_grid(d.nx, d.ny, d.nz), threads = cell_block();
     cudaStream_t st = as_stream(stream);
     FFX_DISPATCH_STORAGE(storage, T, {
@@ -747,7 +750,7 @@ int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
         P.out[0] = (T*)ou; P.out[1] = (T*)ov; P.out[2] = (T*)ow;
         P.walls = make_walls(s);
         for (int a = 0; a < 3; ++a) {
-            P.dep[a] = (dep && corrected) ? dep[a] : nullptr;
+            P.dep[a] = (dep && corrected && starts) ? dep[a] : nullptr;
             P.nf[a] = (d.nx + (a == 0)) * (d.ny + (a == 1)) * (d.nz + (a == 2));
         }
         const float extent[3] = {g->ex, g->ey, g->ez};
@@ -1052,8 +1055,9 @@ size_t velocity_desc(const FfxBatchDomain& D, int parity, void* out) {
         P.out[0] = D.bu; P.out[1] = D.bv; P.out[2] = D.bw;
         P.walls = make_walls(nullptr);
         const int nx = D.grid.nx, ny = D.grid.ny, nz = D.grid.nz;
+        const bool starts = D.velocity_corrected && face_starts_match(P.d);
         for (int a = 0; a < 3; ++a) {
-            P.dep[a] = D.velocity_corrected ? D.face_trace[a] : nullptr;
+            P.dep[a] = starts ? D.face_trace[a] : nullptr;
             P.nf[a] = (nx + (a == 0)) * (ny + (a == 1)) * (nz + (a == 2));
         }
         const float extent[3] = {D.grid.ex, D.grid.ey, D.grid.ez};

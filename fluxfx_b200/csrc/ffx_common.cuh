@@ -68,6 +68,28 @@ inline Dev make_dev(const FfxGrid& g) {
     return d;
 }
 
+// Whether the face predictor's start point (x + o) * h and the velocity
+// correction's (x + o) * e / n (times the exact 1/n on power-of-two grids) are
+// the same float for every face coordinate x + o (o = 0 or 1/2) of every axis,
+// evaluated exactly as the kernels evaluate them (FP32, no contraction). The
+// correction may then reuse the predictor's departure points: both passes
+// trace the same point with the same velocity and time step. True on
+// power-of-two grids, and whenever the spacing e / n is a power of two that
+// e / n rounds to exactly, for moderate n (each product then has few bits).
+inline bool face_starts_match(const Dev& d) {
+    const int n[3] = {d.nx, d.ny, d.nz};
+    for (int i = 0; i < 3; ++i)
+        for (int k = 0; k <= n[i]; ++k)
+            for (int o = 0; o < 2; ++o) {
+                const volatile float X = (float)k + (o ? 0.5f : 0.f);
+                const volatile float a = X * d.h[i];
+                const volatile float xe = X * d.e[i];
+                const volatile float b = d.pow2 ? xe * d.rn[i] : xe / d.nf[i];
+                if (a != b) return false;
+            }
+    return true;
+}
+
 // Division by the grid constants e, n and h. When every one of them is a power
 // of two (e.g. a 256^3 unit cube) dividing is an exact rescaling, so it is done
 // as a multiplication by the exact reciprocal -- bit-identical to the IEEE
