@@ -776,6 +776,85 @@ __global__ void __launch_bounds__(kTmThreads, 1) conv3_tma_kernel(const __grid_c
         asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(P.cols));
 }
 
+// ------------------------------- narrow per-voxel convolutions (CUDA cores)
+// 1^3 convolutions and transposed 2^3 stride-2 convolutions with 8 or 16
+// output channels: each output voxel is one dot product of its input (parent)
+// voxel's channels with the weights of its tap, and a tensor-core tile of 128
+// voxels x 16 channels would be mostly idle. A thread computes one output
+// voxel: the input channels in 16-byte groups, the weights of all taps as FP32
+// in shared memory, FP32 fused multiply-adds in channel order, then the bias,
+// ReLU, accumulation and BF16 / FP32 stores of the implicit-GEMM epilogue.
+constexpr int kDirectThreads = 256;
+constexpr int kDirectMaxWeights = 12288;   // taps x cin x cout FP32 values (48 KB)
+
+template <int COUT>
+__global__ void __launch_bounds__(kDirectThreads) conv_direct_kernel(const __grid_constant__ Conv a) {
+    extern __shared__ float ws[];          // [taps][cin][COUT]
+    const int taps = a.transposed ? 8 : 1;
+    const int nw = taps * a.cin * COUT;
+    for (int i = threadIdx.x; i < nw; i += kDirectThreads) ws[i] = __bfloat162float(a.w[i]);
+    __syncthreads();
+    const long long o = (long long)blockIdx.x * kDirectThreads + threadIdx.x;
+    if (o >= (long long)a.batch * a.od * a.oh * a.ow) return;
+    const RowPos p = decode(o, a.od, a.oh, a.ow);
+    int tap = 0;
+    long long q = o;
+    if (a.transposed) {
+        // output voxel 2 q + j is tap j of input voxel q
+        tap = ((p.z & 1) << 2) | ((p.y & 1) << 1) | (p.x & 1);
+        q = (((long long)p.b * a.id + (p.z >> 1)) * a.ih + (p.y >> 1)) * a.iw + (p.x >> 1);
+    }
+    const float* W = ws + tap * a.cin * COUT;
+    const bf16* x = a.in1.p + q * a.in1.pitch + a.in1.offset;
+    float acc[COUT];
+#pragma unroll
+    for (int n = 0; n < COUT; ++n) acc[n] = 0.f;
+    for (int c8 = 0; c8 < a.cin; c8 += 8) {
+        const uint4 raw = *reinterpret_cast<const uint4*>(x + c8);
+        const __nv_bfloat162* h = reinterpret_cast<const __nv_bfloat162*>(&raw);
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            const float2 f = __bfloat1622float2(h[e]);
+            const float* w0 = W + (c8 + 2 * e) * COUT;
+#pragma unroll
+            for (int n = 0; n < COUT; ++n) acc[n] = __fmaf_rn(f.x, w0[n], acc[n]);
+#pragma unroll
+            for (int n = 0; n < COUT; ++n) acc[n] = __fmaf_rn(f.y, w0[COUT + n], acc[n]);
+        }
+    }
+#pragma unroll
+    for (int n = 0; n < COUT; ++n) {
+        if (a.bias) acc[n] += __ldg(a.bias + n);
+        if (a.relu) acc[n] = fmaxf(acc[n], 0.f);
+    }
+    if (a.out) {
+        uint4* dst = reinterpret_cast<uint4*>(a.out + o * a.out_pitch + a.out_offset);
+#pragma unroll
+        for (int g = 0; g < COUT / 8; ++g) {
+            if (a.accumulate) {
+                const uint4 prev = dst[g];
+                const __nv_bfloat162* pv = reinterpret_cast<const __nv_bfloat162*>(&prev);
+#pragma unroll
+                for (int e = 0; e < 4; ++e) {
+                    const float2 f = __bfloat1622float2(pv[e]);
+                    acc[8 * g + 2 * e] += f.x;
+                    acc[8 * g + 2 * e + 1] += f.y;
+                }
+            }
+            uint4 pk;
+            __nv_bfloat162* pp = reinterpret_cast<__nv_bfloat162*>(&pk);
+#pragma unroll
+            for (int e = 0; e < 4; ++e) pp[e] = __floats2bfloat162_rn(acc[8 * g + 2 * e], acc[8 * g + 2 * e + 1]);
+            dst[g] = pk;
+        }
+    }
+    if (a.out_f32) {
+        float* dst = a.out_f32 + o * a.out_f32_pitch;
+#pragma unroll
+        for (int n = 0; n < COUT; ++n) dst[n] = acc[n];
+    }
+}
+
 // Packed weights of the TMA convolution: w[k = tap * cin + c][cout] ->
 // [cout / BN][groups][27][BN / 8][16][8] (channels >= cin zero), the
 // MN-major core-matrix image a stage copies into shared memory as it is.
@@ -1186,7 +1265,21 @@ int ffx_conv_forward_tma(const FfxConv* c, const void* packed, void* stream) {
     Conv a;
     int e = make_conv(c, a);
     if (e) return e;
-    if (!tma_eligible(a)) return ffx_conv_forward(c, stream);   // other shapes: the mma.sync kernel
+    if (!tma_eligible(a)) {
+        // 1^3 and transposed 2^3 layers with 8 or 16 output channels: the per-voxel kernel;
+        // the remaining shapes: the mma.sync implicit GEMM
+        const bool one = !a.transposed && a.ks == 1 && a.stride == 1 && a.pad == 0;
+        if ((one || a.transposed) && (a.cout == 8 || a.cout == 16) && a.c2 == 0 &&
+            (a.transposed ? 8 : 1) * a.cin * a.cout <= kDirectMaxWeights && (a.out || a.out_f32)) {
+            const long long vox = (long long)a.batch * a.od * a.oh * a.ow;
+            const size_t smem = sizeof(float) * (size_t)(a.transposed ? 8 : 1) * a.cin * a.cout;
+            const unsigned blocks = (unsigned)((vox + kDirectThreads - 1) / kDirectThreads);
+            if (a.cout == 8) conv_direct_kernel<8><<<blocks, kDirectThreads, smem, as_stream(stream)>>>(a);
+            else conv_direct_kernel<16><<<blocks, kDirectThreads, smem, as_stream(stream)>>>(a);
+            return launch_status("conv_direct_kernel");
+        }
+        return ffx_conv_forward(c, stream);
+    }
     FFX_REQUIRE(a.out || a.out_f32, "ffx_conv_forward_tma: no output");
     FFX_REQUIRE(packed && ((uintptr_t)packed & 15) == 0,
                 "ffx_conv_forward_tma: packed weights (ffx_conv_pack_weights, 16-byte aligned)");

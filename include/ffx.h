@@ -558,8 +558,9 @@ int ffx_conv_forward_tc(const FfxConv* conv, void* stream);
  * input halo tile by TMA tensor loads (cp.async.bulk.tensor, zero fill = padding) and runs
  * every tap as a shifted shared-memory descriptor into tcgen05.mma (accumulators in tensor
  * memory). The weights come pre-packed (ffx_conv_pack_weights, `packed_bytes` from
- * ffx_conv_packed_bytes; 0 for shapes the kernel does not tile). Other shapes (2^3
- * stride 2, transposed, 1x1) run the ffx_conv_forward kernel and ignore `packed`. */
+ * ffx_conv_packed_bytes; 0 for shapes the kernel does not tile). 1x1 and transposed 2^3
+ * layers with 8 or 16 output channels run a per-voxel CUDA-core kernel, the other shapes
+ * (2^3 stride 2, wider layers) the ffx_conv_forward kernel; both ignore `packed`. */
 int ffx_conv_packed_bytes(const FfxConv* conv, int64_t* packed_bytes);
 int ffx_conv_pack_weights(const FfxConv* conv, void* packed, void* stream);
 int ffx_conv_forward_tma(const FfxConv* conv, const void* packed, void* stream);

@@ -210,6 +210,62 @@ def test_tma_convolution_other_shapes_use_the_gather_kernel(lib):
     assert rel_err(out32, ref.permute(0, 2, 3, 4, 1)) < 1e-5
 
 
+@pytest.mark.parametrize('case', [
+    # (kind, cin, cout, bf16 output, relu, accumulate)
+    ('head', 16, 8, False, 0, 0),      # the network's head: FP32 output
+    ('head', 8, 16, True, 0, 1),       # the head's data gradient form, accumulated into a view
+    ('up', 32, 16, True, 1, 0),        # up-sampling to the finest level
+    ('up', 32, 16, True, 0, 1),        # the down-sampling's data gradient (accumulated)
+])
+def test_narrow_convolutions_match_torch(lib, case):
+    """1^3 and transposed 2^3 convolutions with 8 or 16 output channels run the
+    per-voxel kernel through the TMA entry point: against torch FP64 on the
+    same BF16 values, with ragged grids, channel views, bias, ReLU and
+    accumulation into the existing output."""
+    kind, cin, cout, out_bf16, relu, acc = case
+    g = torch.Generator().manual_seed(cin + 3 * cout + acc)
+    B, D, H, W = 2, 6, 10, 14
+    ind = (D // 2, H // 2, W // 2) if kind == 'up' else (D, H, W)
+    outd = (D, H, W)
+    taps = 8 if kind == 'up' else 1
+    pitch, off = cin + 8, 8
+    x = bf(torch.randn((B, *ind, pitch), generator=g))
+    w = bf(torch.randn((taps, cin, cout), generator=g) / (taps * cin) ** 0.5)
+    bias = torch.randn(cout, generator=g)
+    opitch, ooff = cout + 16, 8
+    prior = bf(torch.randn((B, *outd, opitch), generator=g))
+    out16 = prior.clone().cuda()
+    out32 = torch.zeros((B, *outd, cout), device='cuda')
+    dx, dw, db = x.cuda(), w.cuda(), bias.cuda()
+    ks, stride = (2, 2) if kind == 'up' else (1, 1)
+    c = conv_struct(B, ind, outd, cin, 0, cout, ks, stride, 0, int(kind == 'up'), dx, pitch, off, None, 0, 0, dw, db,
+                    relu, out16 if out_bf16 else None, opitch, ooff, None if out_bf16 else out32, cout,
+                    accumulate=acc)
+    nbytes = N.i64(-1)
+    N.check(lib.ffx_conv_packed_bytes(C.byref(c), C.byref(nbytes)))
+    assert nbytes.value == 0
+    N.check(lib.ffx_conv_forward_tma(C.byref(c), None, None))
+    torch.cuda.synchronize()
+    xt = x[..., off:off + cin].double().permute(0, 4, 1, 2, 3)
+    wt = U.torch_weight('up' if kind == 'up' else 'head', w.double())
+    if kind == 'up':
+        ref = F.conv_transpose3d(xt, wt, bias.double(), stride=2)
+    else:
+        ref = F.conv3d(xt, wt, bias.double())
+    ref = ref.permute(0, 2, 3, 4, 1)
+    if relu:
+        ref = torch.relu(ref)
+    if not out_bf16:
+        assert rel_err(out32, ref) < 1e-5, rel_err(out32, ref)
+        return
+    if acc:
+        ref = ref + prior[..., ooff:ooff + cout].double()
+    got = out16.cpu()
+    assert rel_err(got[..., ooff:ooff + cout].float(), ref) < 8e-3
+    assert torch.equal(got[..., :ooff], prior[..., :ooff]) and torch.equal(got[..., ooff + cout:],
+                                                                            prior[..., ooff + cout:])
+
+
 @pytest.mark.parametrize('kind', ['conv3', 'down', 'up'])
 def test_weight_gradients_match_torch(lib, kind):
     g = torch.Generator().manual_seed(2)
