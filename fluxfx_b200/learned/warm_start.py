@@ -3,11 +3,12 @@
 ``LearnedWarmStart(grid, colliders, device)`` predicts the impulse pressure of
 a projection from its divergence (``projector.before``) and the collider
 mask. Grids up to 128 cells per axis run the network at their own
-resolution; larger grids (dimensions divisible by 16) run it on the 2x2x2
-average of the divergence over a half-resolution grid whose collider mask is
-restricted from the solver's (a coarse cell is solid when at least four of its
-children are, so moving colliders are followed at every guess), and the
-prediction is prolonged trilinearly. Every pass is a library kernel
+resolution; larger grids run it on 2x2x2 averages of the divergence, halving
+the resolution until no axis exceeds 128 cells (dimensions divisible by 8 x
+the factor), with the collider mask restricted alongside (a coarse cell is
+solid when at least four of its children are, so moving colliders are followed
+at every guess); the prediction is prolonged back trilinearly, one halving at a
+time. Every pass is a library kernel
 (``ffx_mg_restrict``, ``ffx_mask_restrict``, ``ffx_max_abs``,
 ``ffx_pack_input`` + the convolutions, ``ffx_unpack_channel``,
 ``ffx_mg_prolong``); torch only allocates.
@@ -44,26 +45,35 @@ class LearnedWarmStart:
         base = getattr(device, 'base', device)
         self.device = base
         self.grid = grid
-        self.factor = 1 if max(grid.shape) <= MAX_NATIVE else 2
+        # the network runs at most MAX_NATIVE cells per axis: on the grid itself, or on
+        # restrictions by 2 per step (factor 2, 4, ...) with prolongations back
+        self.factor = 1
+        while max(grid.shape) // self.factor > MAX_NATIVE:
+            self.factor *= 2
         shape = tuple(n // self.factor for n in grid.shape)
         if any(n % 8 for n in shape) or any(n % self.factor for n in grid.shape):
-            raise ValueError('the network needs grid dimensions divisible by 8 (by 16 above 128 cells)')
+            raise ValueError('the network needs grid dimensions divisible by 8 x the restriction factor')
         self.shape = shape
+        dev = base.device
+        # shapes of the chain: the grid, then every restriction by 2 down to the network's
+        self.shapes = [tuple(grid.shape)]
+        while self.shapes[-1] != shape:
+            self.shapes.append(tuple(n // 2 for n in self.shapes[-1]))
         self.fine_mask = getattr(device, 'mask', None) if colliders else None
-        if self.fine_mask is not None and self.factor == 1:
-            self.mask = self.fine_mask
-        else:
-            self.mask = torch.zeros(shape[::-1], dtype=torch.uint8, device=base.device)
+        self.masks = [self.fine_mask] + [
+            torch.zeros(sh[::-1], dtype=torch.uint8, device=dev) if self.fine_mask is not None else None
+            for sh in self.shapes[1:]]
+        self.mask = self.masks[-1] if self.fine_mask is not None else torch.zeros(shape[::-1], dtype=torch.uint8,
+                                                                                  device=dev)
         self.weight = weight_of(shape, grid.extent)
         self.net = net or UNet(base.device, seed=0)
         if net is None:
             state = torch.load(weights or WEIGHTS)
             self.net.load_state_dict(state)
-        dev = base.device
-        nx, ny, nz = shape
-        self.div = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev) if self.factor > 1 else None
-        self.coarse = torch.empty((nz, ny, nx), dtype=torch.float32, device=dev) if self.factor > 1 else None
-        self.zero = torch.zeros(tuple(grid.shape[::-1]), dtype=torch.float32, device=dev) if self.factor > 1 else None
+        # restricted divergences and prolonged predictions per coarse level, a zero field per fine level
+        self.divs = [None] + [torch.empty(sh[::-1], dtype=torch.float32, device=dev) for sh in self.shapes[1:]]
+        self.coarses = [None] + [torch.empty(sh[::-1], dtype=torch.float32, device=dev) for sh in self.shapes[1:]]
+        self.zeros = [torch.zeros(sh[::-1], dtype=torch.float32, device=dev) for sh in self.shapes[:-1]]
         self._max = torch.zeros(1, dtype=torch.float32, device=dev)
 
     def guess(self, before, out):
@@ -71,24 +81,28 @@ class LearnedWarmStart:
         dev = self.device
         s = dev.s
         src = before
-        if self.factor > 1:
-            dev.call('ffx_mg_restrict', N.n3(*self.grid.shape), ptr(before), ptr(self.div), s)
-            src = self.div
+        for k in range(1, len(self.shapes)):
+            dev.call('ffx_mg_restrict', N.n3(*self.shapes[k - 1]), ptr(src), ptr(self.divs[k]), s)
+            src = self.divs[k]
             if self.fine_mask is not None:
-                dev.call('ffx_mask_restrict', N.n3(*self.shape), ptr(self.fine_mask), 4, ptr(self.mask), s)
+                dev.call('ffx_mask_restrict', N.n3(*self.shapes[k]), ptr(self.masks[k - 1]), 4, ptr(self.masks[k]), s)
         # the input scale 1 / max|div| stays on the device (no readback in the step);
         # a zero divergence gives a zero guess through the zero unpacking factor
         dev.call('ffx_max_abs', src.numel(), N.FFX_F32, ptr(src), ptr(self._max), s)
         calls = self.net.calls
         pred = self.net.forward(src.unsqueeze(0), self.mask.unsqueeze(0), None, s.value or 0, max_abs=self._max)
         dev.calls += self.net.calls - calls     # the network's launches count with the solver's
-        target = self.coarse if self.factor > 1 else out
+        last = len(self.shapes) - 1
+        target = self.coarses[last] if last > 0 else out
         dev.call('ffx_unpack_channel_scaled', src.numel(), ptr(self.net.pred), HEAD_CHANNELS, ptr(self._max),
                  float(self.weight), ptr(target), s)
-        if self.factor > 1:
-            dev.call('ffx_mg_prolong', N.n3(*self.grid.shape), ptr(self.zero), ptr(self.coarse), ptr(out), s)
+        for k in range(last, 0, -1):
+            fine = out if k == 1 else self.coarses[k - 1]
+            dev.call('ffx_mg_prolong', N.n3(*self.shapes[k - 1]), ptr(self.zeros[k - 1]), ptr(self.coarses[k]),
+                     ptr(fine), s)
         return pred
 
     def close(self):
         self.net = None
         self.fine_mask = self.mask = None
+        self.masks = self.divs = self.coarses = self.zeros = []
