@@ -153,6 +153,8 @@ _PROTOTYPES = {
     'ffx_divergence': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp]),
     'ffx_walls_divergence': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]),
     'ffx_gradient': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, f32, vp, vp, vp, vp, vp, vp]),
+    'ffx_gradient_links': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, f32, vp, vp, vp, vp, vp, vp,
+                                     vp]),
     'ffx_jacobi': (C.c_int, [n3, f3, vp, vp, vp, f32, f32, vp, vp]),
     'ffx_scale': (C.c_int, [i64, vp, f32, vp, vp]),
     'ffx_mg_residual': (C.c_int, [n3, f3, vp, vp, f32, vp, vp]),

@@ -117,11 +117,22 @@ class PressureProjector:
             self.device.call('ffx_scale', self.pressure.numel(), ptr(self.pressure), dt / previous_dt,
                              ptr(self.pressure), self.device.s)
         self.solve_pressure(solve_dt, previous_solve_dt)
-        self.device.call('ffx_gradient', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
-                         ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),
-                         ptr(self._scalars[0:3]), self.device.s)
+        links = self.gradient_links()
+        if links is not None:
+            self.device.call('ffx_gradient_links', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
+                             ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),
+                             ptr(self._scalars[0:3]), ptr(links), self.device.s)
+        else:
+            self.device.call('ffx_gradient', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
+                             ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),
+                             ptr(self._scalars[0:3]), self.device.s)
         self.last_dt = dt
         self.ready = True
+
+    def gradient_links(self):
+        """Level-0 link bytes of the collider mask (ffx_graph_links) for the
+        gradient pass, or None: the pass then tests the mask itself."""
+        return None
 
     def solve_pressure(self, dt, previous_dt):
         if previous_dt != dt:

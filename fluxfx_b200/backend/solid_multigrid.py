@@ -434,6 +434,12 @@ class SolidMultigridProjector(SolidPressureProjector):
                     self.last_cycles += 1
         self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
 
+    def gradient_links(self):
+        # the link bytes follow the mask (recomputed on every collider move)
+        if len(self.levels) > 1 and getattr(self, '_links', None) is not None and self.device.mask is not None:
+            return self._links
+        return None
+
     def attach_learned(self, model):
         """Pressure guess used when ``learned_warm_start`` is set
         (``fluxfx_b200.learned.LearnedWarmStart``)."""

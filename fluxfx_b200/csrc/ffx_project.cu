@@ -110,6 +110,7 @@ struct GradDesc {
     float dt;
     T* out[3];
     float* div;
+    const uint8_t* links;   // optional level-0 link bytes of the same mask (ffx_graph_links), MASK only
 };
 
 template <typename T, bool MASK>
@@ -133,11 +134,21 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
         const int iw = i;
         const int sy = d.nx, sz = d.nx * d.ny;
         float pc = __ldg(p + i);
-        // face between cells (face - e_axis) and (face); phi / plo are their pressures
+        // With the link byte of the cell, bit 2a (2a + 1) says whether the face to the lower
+        // (upper) neighbour along axis a joins two fluid cells inside the domain -- exactly the
+        // test below (interior face, neither adjacent cell solid) -- and bit 6 that the cell is fluid.
+        const unsigned lk = (MASK && P.links) ? (unsigned)__ldg(P.links + i) : 0u;
+        // face between cells (face - e_axis) and (face); phi / plo are their pressures;
+        // bit: the face's link bit in this cell's byte
         auto face_out = [&](const T* f, int idx, int c, int nf, int fx, int fy, int fz, int axis, float phi,
-                            float plo) -> float {
-            bool open = c > 0 && c < nf - 1;
-            if (MASK) open = open && !solid_face(d, solid, fx, fy, fz, axis);
+                            float plo, unsigned bit) -> float {
+            bool open;
+            if (MASK && P.links) {
+                open = (lk & bit) != 0u;
+            } else {
+                open = c > 0 && c < nf - 1;
+                if (MASK) open = open && !solid_face(d, solid, fx, fy, fz, axis);
+            }
             if (!open) return wall_value(W, axis, idx);
             float gr = (phi - plo) * d.inv[axis];
             return Store<T>::ld(f, idx) - dt * gr;
@@ -145,12 +156,12 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
         float p_xm = x > 0 ? __ldg(p + i - 1) : 0.f, p_xp = x + 1 < d.nx ? __ldg(p + i + 1) : 0.f;
         float p_ym = y > 0 ? __ldg(p + i - sy) : 0.f, p_yp = y + 1 < d.ny ? __ldg(p + i + sy) : 0.f;
         float p_zm = z > 0 ? __ldg(p + i - sz) : 0.f, p_zp = z + 1 < d.nz ? __ldg(p + i + sz) : 0.f;
-        float ul = rt<T>(face_out(F.u, iu, x, d.nx + 1, x, y, z, 0, pc, p_xm));
-        float vl = rt<T>(face_out(F.v, iv, y, d.ny + 1, x, y, z, 1, pc, p_ym));
-        float wl = rt<T>(face_out(F.w, iw, z, d.nz + 1, x, y, z, 2, pc, p_zm));
-        float uu = rt<T>(face_out(F.u, iu + 1, x + 1, d.nx + 1, x + 1, y, z, 0, p_xp, pc));
-        float vu = rt<T>(face_out(F.v, iv + d.nx, y + 1, d.ny + 1, x, y + 1, z, 1, p_yp, pc));
-        float wu = rt<T>(face_out(F.w, iw + sz, z + 1, d.nz + 1, x, y, z + 1, 2, p_zp, pc));
+        float ul = rt<T>(face_out(F.u, iu, x, d.nx + 1, x, y, z, 0, pc, p_xm, 1u));
+        float vl = rt<T>(face_out(F.v, iv, y, d.ny + 1, x, y, z, 1, pc, p_ym, 4u));
+        float wl = rt<T>(face_out(F.w, iw, z, d.nz + 1, x, y, z, 2, pc, p_zm, 16u));
+        float uu = rt<T>(face_out(F.u, iu + 1, x + 1, d.nx + 1, x + 1, y, z, 0, p_xp, pc, 2u));
+        float vu = rt<T>(face_out(F.v, iv + d.nx, y + 1, d.ny + 1, x, y + 1, z, 1, p_yp, pc, 8u));
+        float wu = rt<T>(face_out(F.w, iw + sz, z + 1, d.nz + 1, x, y, z + 1, 2, p_zp, pc, 32u));
         Store<T>::st(ou, iu, ul);
         Store<T>::st(ov, iv, vl);
         Store<T>::st(ow, iw, wl);
@@ -160,7 +171,7 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
         if (z == d.nz - 1) { Store<T>::st(ow, iw + sz, wu); mx[2] = fmaxf(mx[2], finite_abs(wu)); }
         if (div) {
             float dv = (uu - ul) * d.inv[0] + (vu - vl) * d.inv[1] + (wu - wl) * d.inv[2];
-            if (MASK && __ldg(solid + i)) dv = 0.f;
+            if (MASK && (P.links ? (lk & 64u) == 0u : __ldg(solid + i) != 0)) dv = 0.f;
             div[i] = dv;
         }
     }
@@ -175,8 +186,9 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
 template <typename T, bool MASK>
 __global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Walls W,
                                                       Faces<T> F, const float* __restrict__ p, float dt, T* ou,
-                                                      T* ov, T* ow, float* div, float* maxima) {
-    gradient_body<T, MASK>(GradDesc<T>{d, solid, W, F, p, dt, {ou, ov, ow}, div}, hw_blk(), maxima);
+                                                      T* ov, T* ow, float* div, float* maxima,
+                                                      const uint8_t* __restrict__ links) {
+    gradient_body<T, MASK>(GradDesc<T>{d, solid, W, F, p, dt, {ou, ov, ow}, div, links}, hw_blk(), maxima);
 }
 
 // ---------------------------------------------------------------- Jacobi
@@ -992,9 +1004,9 @@ int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage, cons
     return launch_status("walls_divergence_kernel");
 }
 
-int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
-                 const float* pressure, float dt, void* ou, void* ov, void* ow, float* div_after, float* maxima,
-                 void* stream) {
+static int gradient_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                         const void* w, const float* pressure, float dt, void* ou, void* ov, void* ow,
+                         float* div_after, float* maxima, const uint8_t* links, void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && pressure && ou && ov && ow,
                 "ffx_gradient: invalid arguments");
     FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_gradient: outputs must not alias inputs");
@@ -1008,11 +1020,23 @@ int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* 
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
         if (has_mask(s)) gradient_kernel<T, true><<<grid, block, 0, st>>>(d, s->solid, make_walls(s), F, pressure, dt, (T*)ou,
-                                                                          (T*)ov, (T*)ow, div_after, maxima);
+                                                                          (T*)ov, (T*)ow, div_after, maxima, links);
         else gradient_kernel<T, false><<<grid, block, 0, st>>>(d, nullptr, Walls{}, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow,
-                                                               div_after, maxima);
+                                                               div_after, maxima, nullptr);
     });
     return launch_status("gradient_kernel");
+}
+
+int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
+                 const float* pressure, float dt, void* ou, void* ov, void* ow, float* div_after, float* maxima,
+                 void* stream) {
+    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, nullptr, stream);
+}
+
+int ffx_gradient_links(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                       const void* w, const float* pressure, float dt, void* ou, void* ov, void* ow,
+                       float* div_after, float* maxima, const uint8_t* links, void* stream) {
+    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, links, stream);
 }
 
 int ffx_jacobi(const int32_t n[3], const float inv[3], const uint8_t* solid, const float* p_in, const float* rhs,
@@ -1490,6 +1514,7 @@ size_t gradient_desc(const FfxBatchDomain& D, float* u, float* v, float* w, void
         P.dt = 1.0f;   // impulse form: the solve used dt = 1
         P.out[0] = u; P.out[1] = v; P.out[2] = w;
         P.div = D.after;
+        P.links = D.level[0].level.links;   // level-0 link bytes of the same mask (or NULL)
         memcpy(out, &P, sizeof P);
     }
     return sizeof(GradDesc<float>);

@@ -221,6 +221,13 @@ int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage,
 int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage,
                  const void* u, const void* v, const void* w, const float* pressure, float dt,
                  void* ou, void* ov, void* ow, float* div_after, float* maxima, void* stream);
+/* The same with the collider test read from the level-0 link bytes of the same mask
+ * (ffx_graph_links: one byte per cell, the open-face bits and the fluid bit): one load
+ * per cell instead of twelve mask loads, the same result. */
+int ffx_gradient_links(const FfxGrid* g, const FfxSolids* s, int storage,
+                       const void* u, const void* v, const void* w, const float* pressure, float dt,
+                       void* ou, void* ov, void* ow, float* div_after, float* maxima,
+                       const uint8_t* links, void* stream);
 /* One weighted-Jacobi sweep of the (masked) Neumann Laplacian on a level of
  * shape n[3] with 1/h = inv[3]; solid may be NULL. Replaces
  * shaders/pressure_jacobi.glsl. p_out must not alias p_in. */
