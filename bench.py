@@ -480,7 +480,8 @@ def cpu_baseline(args, sample_n=None, sample_steps=1):
         ref.step(0.02, sources=table)
     dt = time.perf_counter() - t0
     rate = sample_steps * n ** 3 / dt
-    return {"value": rate / args.size ** 3, "unit": UNIT, "cores": 1, "kind": "port",
+    return {"value": rate / args.size ** 3, "unit": UNIT, "cores": 1, "host_cpu_count": os.cpu_count(),
+            "threads_note": "NumPy element-wise passes run on one thread", "kind": "port",
             "sample": f"{sample_steps} step(s) of the same scene at {n}^3 on the NumPy restatement of the "
                       f"reference ({dt:.1f} s, {ref.projector.last_cycles} V-cycles); cell-update rate scaled "
                       f"to {args.size}^3"}
@@ -500,7 +501,8 @@ def run_reference(args):
         "data": "synthetic (seeded scene)",
         "config": {"workload": f"dense smoke step {args.size}^3 scene, reference algorithm, "
                                f"bounded CPU sample at {args.cpu_sample}^3"},
-        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "kind": "port", "sample": samples[-1]['sample']},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": 1, "host_cpu_count": os.cpu_count(), "kind": "port",
+                         "sample": samples[-1]['sample']},
         "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}), flush=True)
 
 

@@ -3,6 +3,7 @@
 #include <cstring>
 
 #include "ffx_host.cuh"
+#include "ffx_stats.cuh"
 
 namespace ffx {
 
@@ -112,61 +113,6 @@ __global__ void max_abs_kernel(int64_t n, const T* __restrict__ x, float* out) {
     block_max_to(out, m);
 }
 
-// Deterministic divergence statistics: per-block FP64 partials in a fixed
-// order, then one block combines them in index order.
-constexpr int kStatsThreads = 256;
-constexpr int kStatsBlocks = 1184;   // 8 x 148 SMs
-
-__device__ __forceinline__ double warp_sum(double v) {
-    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-    return v;
-}
-__device__ __forceinline__ double warp_maxd(double v) {
-    for (int o = 16; o > 0; o >>= 1) v = fmax(v, __shfl_down_sync(0xffffffffu, v, o));
-    return v;
-}
-
-__global__ void stats_partial_kernel(int64_t n, const float* __restrict__ b, const float* __restrict__ a,
-                                     double* part) {
-    double s[6] = {0, 0, 0, 0, 0, 0};   // b2, a2, max b, max a, sum b, sum a
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        double vb = b[i], va = a[i];
-        s[0] += vb * vb; s[1] += va * va;
-        s[2] = fmax(s[2], fabs(vb)); s[3] = fmax(s[3], fabs(va));
-        s[4] += vb; s[5] += va;
-    }
-    __shared__ double sh[6][kStatsThreads / 32];
-    int lane = threadIdx.x & 31, wid = threadIdx.x >> 5;
-    for (int k = 0; k < 6; ++k) {
-        double v = (k == 2 || k == 3) ? warp_maxd(s[k]) : warp_sum(s[k]);
-        if (lane == 0) sh[k][wid] = v;
-    }
-    __syncthreads();
-    if (threadIdx.x < 6) {
-        int k = threadIdx.x;
-        double v = sh[k][0];
-        for (int w = 1; w < kStatsThreads / 32; ++w) v = (k == 2 || k == 3) ? fmax(v, sh[k][w]) : v + sh[k][w];
-        part[(int64_t)blockIdx.x * 6 + k] = v;
-    }
-}
-
-__global__ void stats_final_kernel(int nblocks, const double* part, int64_t n, double* out) {
-    int k = threadIdx.x;
-    if (k >= 6) return;
-    double v = part[k];
-    for (int bidx = 1; bidx < nblocks; ++bidx) {
-        double x = part[(int64_t)bidx * 6 + k];
-        v = (k == 2 || k == 3) ? fmax(v, x) : v + x;
-    }
-    out[k] = v;
-    if (k == 0) { out[6] = (double)n; out[7] = 0.0; }
-}
-
-int stats_blocks(int64_t n) {
-    int64_t b = (n + kStatsThreads - 1) / kStatsThreads;
-    return (int)(b < kStatsBlocks ? (b < 1 ? 1 : b) : kStatsBlocks);
-}
-
 }  // namespace
 }  // namespace ffx
 
@@ -265,7 +211,7 @@ int ffx_max_abs(int64_t count, int storage, const void* x, float* out, void* str
 }
 
 size_t ffx_divergence_stats_workspace(int64_t count) {
-    return (size_t)stats_blocks(count < 1 ? 1 : count) * 6 * sizeof(double);
+    return (size_t)stats::blocks(count < 1 ? 1 : count) * 6 * sizeof(double);
 }
 
 int ffx_divergence_stats(int64_t count, const float* before, const float* after, double* out, void* workspace,
@@ -275,13 +221,8 @@ int ffx_divergence_stats(int64_t count, const float* before, const float* after,
     FFX_REQUIRE(workspace && workspace_bytes >= need,
                 "ffx_divergence_stats: workspace of %zu bytes required, %zu given", need, workspace_bytes);
     FFX_REQUIRE(((uintptr_t)workspace & 7) == 0, "ffx_divergence_stats: workspace must be 8-byte aligned");
-    int nb = stats_blocks(count);
-    cudaStream_t s = as_stream(stream);
-    stats_partial_kernel<<<nb, kStatsThreads, 0, s>>>(count, before, after, (double*)workspace);
-    int st = launch_status("stats_partial_kernel");
-    if (st) return st;
-    stats_final_kernel<<<1, 32, 0, s>>>(nb, (const double*)workspace, count, out);
-    return launch_status("stats_final_kernel");
+    stats::launch(count, before, after, (double*)workspace, out, as_stream(stream));
+    return launch_status("divergence stats kernels");
 }
 
 }  // extern "C"

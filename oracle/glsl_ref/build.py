@@ -2,6 +2,10 @@
 
     python oracle/glsl_ref/build.py [/path/to/FluxFX_Source/fluxfx/shaders]
 
+The reference checkout is the directory FLUXFX_SOURCE names (its
+``FluxFX_Source`` folder); without it, the recipe looks in the checkout
+location of the development container (``REFERENCE_CHECKOUT``).
+
 Reads the shader sources where they lie in the reference checkout, writes
 build inputs and the library only under ``oracle/_ref/``:
 
@@ -15,6 +19,7 @@ build inputs and the library only under ``oracle/_ref/``:
 Nothing here is part of the product; the library travels with the checkout so
 the CPU reference leg can run where the reference sources are absent.
 """
+import os
 import re
 import subprocess
 import sys
@@ -24,7 +29,8 @@ HERE = Path(__file__).resolve().parent
 OUT = HERE.parent / '_ref'
 GEN = OUT / 'gen'
 LIB = OUT / 'libglsl_ref.so'
-DEFAULT_SHADERS = Path('/root/reference/FluxFX_Source/fluxfx/shaders')
+REFERENCE_CHECKOUT = Path(os.environ.get('FLUXFX_SOURCE', '/root/reference/FluxFX_Source'))
+DEFAULT_SHADERS = REFERENCE_CHECKOUT / 'fluxfx' / 'shaders'
 OUT_PARAM = re.compile(r'\bout\s+(float|int|vec2|vec3|vec4|ivec3)\s+(\w+)')
 SWIZZLE_XYZ = re.compile(r'(?<!gl_GlobalInvocationID)\.xyz\b(?!\s*\()')
 

@@ -147,4 +147,6 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
-    main(Path(sys.argv[1]) if len(sys.argv) > 1 else Path('/root/reference/FluxFX_Source'))
+    sys.path.insert(0, str(Path(__file__).resolve().parents[2]))
+    from oracle.glsl_ref.build import REFERENCE_CHECKOUT
+    main(Path(sys.argv[1]) if len(sys.argv) > 1 else REFERENCE_CHECKOUT)

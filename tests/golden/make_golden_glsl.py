@@ -206,5 +206,6 @@ def main(ref_root):
 
 
 if __name__ == '__main__':
+    from oracle.glsl_ref.build import REFERENCE_CHECKOUT
     args = [a for a in sys.argv[1:] if not a.startswith('--')]
-    main(Path(args[0]) if args else Path('/root/reference/FluxFX_Source'))
+    main(Path(args[0]) if args else REFERENCE_CHECKOUT)
