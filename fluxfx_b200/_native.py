@@ -12,6 +12,7 @@ LIB_PATH = Path(__file__).resolve().parent / '_lib' / 'libffx_core.so'
 
 FFX_OK, FFX_ERR_INVALID, FFX_ERR_LAUNCH, FFX_ERR_NOT_CONVERGED, FFX_ERR_TIMEOUT, FFX_ERR_CUDA = range(6)
 FFX_F32, FFX_BF16 = 0, 1
+FFX_PACK_U8 = 2
 STATUS_NAMES = {0: 'OK', 1: 'INVALID', 2: 'LAUNCH', 3: 'NOT_CONVERGED', 4: 'TIMEOUT', 5: 'CUDA'}
 
 vp = C.c_void_p
@@ -132,6 +133,17 @@ _PROTOTYPES = {
     'ffx_dilate_mask': (C.c_int, [P(FfxGrid), vp, vp, vp]),
     'ffx_solid_clear': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp]),
     'ffx_face_predictor': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
+    'ffx_set_transport_tiling': (C.c_int, [C.c_int]),
+    'ffx_pack_channels': (C.c_int, [i64, C.c_int, P(vp), P(C.c_int), vp, vp]),
+    'ffx_loop_begin': (C.c_int, [vp, P(vp)]),
+    'ffx_loop_decide': (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, vp, vp]),
+    'ffx_loop_reset_counter': (C.c_int, [vp, vp]),
+    'ffx_zero_if_unscaled': (C.c_int, [vp, vp, i64, vp]),
+    'ffx_loop_while': (C.c_int, [vp, P(vp)]),
+    'ffx_loop_end_while': (C.c_int, [vp]),
+    'ffx_loop_end': (C.c_int, [vp]),
+    'ffx_loop_launch': (C.c_int, [vp, vp]),
+    'ffx_loop_destroy': (C.c_int, [vp]),
     'ffx_face_predictor_trace': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, P(vp),
                                            vp]),
     'ffx_advect_velocity': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, f32, C.c_int, f32,

@@ -9,6 +9,7 @@
 // stays close to one read of each field per pass.
 #include "ffx_host.cuh"
 #include "ffx_batch.cuh"
+#include "ffx_tile.cuh"
 
 namespace ffx {
 namespace {
@@ -51,9 +52,6 @@ constexpr int kThreads = 256;
 #else
 #define FFX_LB_SCALARS __launch_bounds__(kThreads)
 #endif
-__device__ __forceinline__ int floor_int(float v) {
-    return (int)fmaxf(fminf(floorf(v), 1.0e9f), -1.0e9f);
-}
 
 struct FaceIdx {
     int axis, x, y, z, sx, sy, sz;
@@ -131,77 +129,6 @@ __device__ __forceinline__ float sample_closed(const Dev& d, const uint8_t* soli
     return zz0 * gz + zz1 * fz;
 }
 
-// sample_closed split in two for several scalars sampled at one point: the
-// stencil (clamped corners, fractions and, with colliders, which corners are
-// fluid and the sum of their weights) is formed once, then applied to each
-// field with sample_closed's operations in its order, so every channel's
-// value is sample_closed's.
-struct ClosedStencil {
-    int rows[4];          // cidx(0, y, z) of (y0, z0), (y1, z0), (y0, z1), (y1, z1)
-    int x0, x1;
-    float fx, fy, fz;
-    unsigned fluid;       // MASK: bit k set when corner k (z, y, x order) is fluid
-    float total;          // MASK: sum of the fluid corners' weights
-};
-
-template <bool MASK>
-__device__ __forceinline__ ClosedStencil closed_stencil(const Dev& d, const uint8_t* solid, float qx, float qy,
-                                                        float qz) {
-    ClosedStencil S;
-    float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
-    S.fx = qx - bx;
-    S.fy = qy - by;
-    S.fz = qz - bz;
-    int ix = floor_int(qx), iy = floor_int(qy), iz = floor_int(qz);
-    S.x0 = min(max(ix, 0), d.nx - 1);
-    S.x1 = min(max(ix + 1, 0), d.nx - 1);
-    const int y0 = min(max(iy, 0), d.ny - 1), y1 = min(max(iy + 1, 0), d.ny - 1);
-    const int z0 = min(max(iz, 0), d.nz - 1), z1 = min(max(iz + 1, 0), d.nz - 1);
-    S.rows[0] = cidx(d, 0, y0, z0);
-    S.rows[1] = cidx(d, 0, y1, z0);
-    S.rows[2] = cidx(d, 0, y0, z1);
-    S.rows[3] = cidx(d, 0, y1, z1);
-    S.fluid = 0u;
-    S.total = 0.f;
-    if (MASK) {
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            const int c = S.rows[k >> 1] + ((k & 1) ? S.x1 : S.x0);
-            if (__ldg(solid + c)) continue;
-            const float wz = (k & 4) ? S.fz : 1.f - S.fz, wy = (k & 2) ? S.fy : 1.f - S.fy,
-                        wx = (k & 1) ? S.fx : 1.f - S.fx;
-            S.fluid |= 1u << k;
-            S.total = S.total + wx * wy * wz;
-        }
-    }
-    return S;
-}
-
-template <typename T, bool MASK>
-__device__ __forceinline__ float apply_closed(const ClosedStencil& S, const T* __restrict__ f) {
-    if (MASK) {
-        float value = 0.f;
-#pragma unroll
-        for (int k = 0; k < 8; ++k) {
-            if (!(S.fluid & (1u << k))) continue;
-            const float wz = (k & 4) ? S.fz : 1.f - S.fz, wy = (k & 2) ? S.fy : 1.f - S.fy,
-                        wx = (k & 1) ? S.fx : 1.f - S.fx;
-            value = value + wx * wy * wz * Store<T>::ld(f, S.rows[k >> 1] + ((k & 1) ? S.x1 : S.x0));
-        }
-        return S.total > 1e-8f ? value / S.total : 0.f;
-    }
-    float f000 = Store<T>::ld(f, S.rows[0] + S.x0), f100 = Store<T>::ld(f, S.rows[0] + S.x1);
-    float f010 = Store<T>::ld(f, S.rows[1] + S.x0), f110 = Store<T>::ld(f, S.rows[1] + S.x1);
-    float f001 = Store<T>::ld(f, S.rows[2] + S.x0), f101 = Store<T>::ld(f, S.rows[2] + S.x1);
-    float f011 = Store<T>::ld(f, S.rows[3] + S.x0), f111 = Store<T>::ld(f, S.rows[3] + S.x1);
-    const float fx = S.fx, fy = S.fy, fz = S.fz;
-    float gx = 1.f - fx, gy = 1.f - fy, gz = 1.f - fz;
-    float a0 = f000 * gx + f100 * fx, a1 = f010 * gx + f110 * fx;
-    float b0 = f001 * gx + f101 * fx, b1 = f011 * gx + f111 * fx;
-    float zz0 = a0 * gy + a1 * fy, zz1 = b0 * gy + b1 * fy;
-    return zz0 * gz + zz1 * fz;
-}
-
 // ------------------------------------------------------------ face predictor
 template <typename T>
 struct PredParams {
@@ -215,15 +142,34 @@ struct PredParams {
     int nf[3];
 };
 
-template <typename T, bool MASK, bool P2>
-__device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, const Blk& b) {
+// Face index of face (x, y, z) of face grid `axis`.
+__device__ __forceinline__ FaceIdx face_at(const Dev& d, int axis, int x, int y, int z) {
+    FaceIdx f;
+    f.axis = axis;
+    f.x = x;
+    f.y = y;
+    f.z = z;
+    f.sx = d.nx + (axis == 0);
+    f.sy = d.ny + (axis == 1);
+    f.sz = d.nz + (axis == 2);
+    f.i = x + f.sx * (y + f.sy * z);
+    return f;
+}
+
+// Velocity faces as sampler fields 0..2 and the second face set (the
+// predictor faces of the velocity pass) as fields 3..5.
+template <typename T>
+__device__ __forceinline__ GlobalSampler<FaceFields<T>> face_sampler(const Dev& d, const Faces<T>& F,
+                                                                    const Faces<T>& second) {
+    return GlobalSampler<FaceFields<T>>{FaceFields<T>{d, F, second}};
+}
+
+template <typename T, bool MASK, bool P2, class Smp>
+__device__ __forceinline__ void face_predictor_face(const PredParams<T>& P, const FaceIdx& f, const Smp& smp) {
     const Dev& d = P.d;
     const uint8_t* __restrict__ solid = P.solid;
     const uint8_t* __restrict__ halo = P.halo;
-    const Faces<T>& F = P.F;
     const float dt = P.dt;
-    FaceIdx f;
-    if (!face_coords(b, d, f)) return;
     T* out = P.out[f.axis];
     if (MASK && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
         Store<T>::st(out, f.i, 0.f);
@@ -231,12 +177,10 @@ __device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, cons
     }
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
-    F3 v0 = velocity_at_start<T, P2>(d, F, p, 2 * f.x + (f.axis != 0), 2 * f.y + (f.axis != 1),
-                                       2 * f.z + (f.axis != 2));
-    F3 dep = backtrace<T, MASK, P2>(d, F, solid, halo, p, v0, dt);
-    const T* src = f.axis == 0 ? F.u : (f.axis == 1 ? F.v : F.w);
-    float value = sample_face(src, f.sx, f.sy, f.sz, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
-                                dv_h<P2>(d, dep.z, 2) - oz);
+    F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * f.x + (f.axis != 0), 2 * f.y + (f.axis != 1), 2 * f.z + (f.axis != 2));
+    F3 dep = backtrace_s<MASK, P2>(d, smp, solid, halo, p, v0, dt);
+    float value = smp.sample(f.axis, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
+                             dv_h<P2>(d, dep.z, 2) - oz);
     Store<T>::st(out, f.i, value);
     if (float* D = P.dep[f.axis]) {
         const int nf = P.nf[f.axis];
@@ -244,6 +188,13 @@ __device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, cons
         D[f.i + nf] = dep.y;
         D[f.i + 2 * nf] = dep.z;
     }
+}
+
+template <typename T, bool MASK, bool P2>
+__device__ __forceinline__ void face_predictor_body(const PredParams<T>& P, const Blk& b) {
+    FaceIdx f;
+    if (!face_coords(b, P.d, f)) return;
+    face_predictor_face<T, MASK, P2>(P, f, face_sampler<T>(P.d, P.F, P.F));
 }
 
 template <typename T, bool MASK, bool P2>
@@ -270,11 +221,9 @@ struct VelParams {
     SrcDev src;
 };
 
-template <typename T, bool MASK, bool P2>
-__device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, const Blk& b) {
+template <typename T, bool MASK, bool P2, class Smp>
+__device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, const FaceIdx& f, const Smp& smp) {
     const Dev& d = P.d;
-    FaceIdx f;
-    if (!face_coords(b, d, f)) return;
     const int axis = f.axis;
     const float dt = P.dt;
     bool blocked = MASK && solid_face(d, P.solid, f.x, f.y, f.z, axis);
@@ -283,8 +232,7 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
         float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
         F3 p = {dv_n<P2>(d, ((float)f.x + off[0]) * d.e[0], 0), dv_n<P2>(d, ((float)f.y + off[1]) * d.e[1], 1),
                 dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
-        F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * f.x + (axis != 0), 2 * f.y + (axis != 1),
-                                         2 * f.z + (axis != 2));
+        F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * f.x + (axis != 0), 2 * f.y + (axis != 1), 2 * f.z + (axis != 2));
         // The host passes the predictor's departure points only when both passes
         // form the same start point at every face (face_starts_match); the
         // predictor then traced this face's start point with the same velocity,
@@ -296,13 +244,13 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
             const int nf = P.nf[axis];
             dep = {__ldg(D + f.i), __ldg(D + f.i + nf), __ldg(D + f.i + 2 * nf)};
         } else {
-            dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
+            dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt);
         }
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
         float qx = dv_h<P2>(d, dep.x, 0) - off[0], qy = dv_h<P2>(d, dep.y, 1) - off[1],
               qz = dv_h<P2>(d, dep.z, 2) - off[2];
-        float low = (reuse && sizeof(T) == 4) ? Store<T>::ld(pred, f.i) : sample_face(orig, f.sx, f.sy, f.sz, qx, qy, qz);
+        float low = (reuse && sizeof(T) == 4) ? Store<T>::ld(pred, f.i) : smp.sample(axis, qx, qy, qz);
         value = low;
         if (P.corrected) {
             // correct_velocity_fused.glsl:5-27
@@ -314,31 +262,19 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
             }
             float s = 0.5f * dt;
             F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
-            F3 vm2 = velocity_at<T, P2>(d, P.F, mid2);
+            F3 vm2 = velocity_s<P2>(d, smp, mid2);
             F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
             bool ok = !(dep.x < lob[0] || dep.y < lob[1] || dep.z < lob[2] || dep.x > hib[0] || dep.y > hib[1] ||
                         dep.z > hib[2] || arr.x < lob[0] || arr.y < lob[1] || arr.z < lob[2] || arr.x > hib[0] ||
                         arr.y > hib[1] || arr.z > hib[2]);
             if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
             if (ok) {
-                float pa = sample_face(pred, f.sx, f.sy, f.sz, dv_h<P2>(d, arr.x, 0) - off[0], dv_h<P2>(d, arr.y, 1) - off[1],
-                                       dv_h<P2>(d, arr.z, 2) - off[2]);
+                float pa = smp.sample(3 + axis, dv_h<P2>(d, arr.x, 0) - off[0], dv_h<P2>(d, arr.y, 1) - off[1],
+                                      dv_h<P2>(d, arr.z, 2) - off[2]);
                 float val = Store<T>::ld(pred, f.i) + 0.5f * (Store<T>::ld(orig, f.i) - pa);
                 // min / max of the 8 corners around the departure point, clamped to the grid
-                const int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
-                const int cx0 = min(max(bx, 0), f.sx - 1), cx1 = min(max(bx + 1, 0), f.sx - 1);
-                const int cy0 = min(max(by, 0), f.sy - 1), cy1 = min(max(by + 1, 0), f.sy - 1);
-                const int cz0 = min(max(bz, 0), f.sz - 1), cz1 = min(max(bz + 1, 0), f.sz - 1);
-                const int sxy = f.sx * f.sy;
-                const int rows[4] = {cz0 * sxy + cy0 * f.sx, cz0 * sxy + cy1 * f.sx, cz1 * sxy + cy0 * f.sx,
-                                     cz1 * sxy + cy1 * f.sx};
-                float lo = Store<T>::ld(orig, rows[0] + cx0), hi = lo;
-#pragma unroll
-                for (int k = 1; k < 8; ++k) {
-                    const float v = Store<T>::ld(orig, rows[k >> 1] + ((k & 1) ? cx1 : cx0));
-                    lo = fminf(lo, v);
-                    hi = fmaxf(hi, v);
-                }
+                float lo, hi;
+                smp.minmax8(axis, (int)floorf(qx), (int)floorf(qy), (int)floorf(qz), lo, hi);
                 float cl = fminf(fmaxf(val, lo), hi);
                 value = low * (1.f - P.blend) + cl * P.blend;
             }
@@ -384,9 +320,137 @@ __device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, cons
 }
 
 template <typename T, bool MASK, bool P2>
+__device__ __forceinline__ void advect_velocity_body(const VelParams<T>& P, const Blk& b) {
+    FaceIdx f;
+    if (!face_coords(b, P.d, f)) return;
+    advect_velocity_face<T, MASK, P2>(P, f, face_sampler<T>(P.d, P.F, P.P));
+}
+
+template <typename T, bool MASK, bool P2>
 __global__ void FFX_LB_VELOCITY advect_velocity_kernel(const __grid_constant__ VelParams<T> P) {
     advect_velocity_body<T, MASK, P2>(P, hw_blk());
 }
+
+// ------------------------------------------------- tiled face passes
+// The face predictor and the velocity pass over shared-memory windows
+// (ffx_tile.cuh): a block owns 32 x 8 (x, y) columns and a chunk of z slices;
+// at slice z a thread works the U face (x, y, z), the V face and the W face
+// of its column (the thread at x = nx - 1 also the U face x = nx, the thread
+// at y = ny - 1 also the V face y = ny; the last chunk adds z = nz for the W
+// faces). Results are bit-identical to the untiled kernels.
+#ifndef FFX_MINB_PREDICTOR_TILED
+#define FFX_MINB_PREDICTOR_TILED 6
+#endif
+#ifndef FFX_MINB_VELOCITY_TILED
+#define FFX_MINB_VELOCITY_TILED 5
+#endif
+#ifndef FFX_TILE_ZCHUNK
+#define FFX_TILE_ZCHUNK 16
+#endif
+
+// Slices [z0, z_end) of the block's chunk: the last chunk of a face pass
+// includes z = nz (W faces only).
+struct Chunk {
+    int z0, z1;
+};
+__device__ __forceinline__ Chunk face_chunk(int nz, int zchunk) {
+    const int z0 = blockIdx.z * zchunk;
+    return Chunk{z0, z0 + zchunk >= nz ? nz + 1 : z0 + zchunk};
+}
+
+// The faces of column (x, y) at slice z, in U, V, W order: up to five (U at x
+// and x + 1 = nx, V at y and y + 1 = ny, W), visited from one call site so
+// the face body is inlined once.
+template <class Face>
+__device__ __forceinline__ void column_faces(const Dev& d, int x, int y, int z, Face&& face) {
+    const bool in = x < d.nx && y < d.ny;
+#pragma unroll 1
+    for (int j = 0; j < 5; ++j) {
+        int axis, fx = x, fy = y;
+        bool active;
+        switch (j) {
+            case 0: axis = 0; active = in && z < d.nz; break;
+            case 1: axis = 0; fx = d.nx; active = x == d.nx - 1 && y < d.ny && z < d.nz; break;
+            case 2: axis = 1; active = in && z < d.nz; break;
+            case 3: axis = 1; fy = d.ny; active = y == d.ny - 1 && x < d.nx && z < d.nz; break;
+            default: axis = 2; active = in; break;
+        }
+        if (active) face(axis, fx, fy, z);
+    }
+}
+
+// Marches the block's chunk: stages the first `nfields` sampler fields slice
+// by slice (z-1 .. z+2 resident while slice z is worked) and calls work(z)
+// per slice.
+template <int NF, class Fields, class Work>
+__device__ __forceinline__ void march(TileSampler<Fields>& smp, float* ring, int nfields, Chunk c, Work&& work) {
+    const int tid = threadIdx.x + tile::kTX * threadIdx.y;
+    auto stage_all = [&](int zg) {
+#pragma unroll
+        for (int k = 0; k < NF; ++k) {
+            if (k >= nfields) break;
+            int sx, sy, sz;
+            smp.G.f.dims(k, sx, sy, sz);
+            tile::stage(ring + k * tile::kRing, smp.G.f.ptr(k), sx, sy, sz, smp.w.wx, smp.w.wy, zg, tid);
+        }
+    };
+    stage_all(c.z0 - 1);
+    stage_all(c.z0);
+    stage_all(c.z0 + 1);
+#pragma unroll 1
+    for (int z = c.z0; z < c.z1; ++z) {
+        stage_all(z + 2);
+        __syncthreads();
+        smp.w.zlo = z - 1;
+        work(z);
+        __syncthreads();
+    }
+}
+
+template <class Fields>
+__device__ __forceinline__ TileSampler<Fields> tile_sampler(const GlobalSampler<Fields>& g, float* ring) {
+    return TileSampler<Fields>{g, tile::Window{ring, (int)blockIdx.x * tile::kTX - 1, (int)blockIdx.y * tile::kTY - 1, 0}};
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(tile::kThreads, FFX_MINB_PREDICTOR_TILED)
+    face_predictor_tiled_kernel(const __grid_constant__ PredParams<T> P, int zchunk) {
+    __shared__ float ring[3 * tile::kRing];
+    auto smp = tile_sampler(face_sampler<T>(P.d, P.F, P.F), ring);
+    const int x = (int)blockIdx.x * tile::kTX + (int)threadIdx.x, y = (int)blockIdx.y * tile::kTY + (int)threadIdx.y;
+    march<3>(smp, ring, 3, face_chunk(P.d.nz, zchunk), [&](int z) {
+        column_faces(P.d, x, y, z, [&](int axis, int fx, int fy, int fz) {
+            face_predictor_face<T, MASK, P2>(P, face_at(P.d, axis, fx, fy, fz), smp);
+        });
+    });
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(tile::kThreads, FFX_MINB_VELOCITY_TILED)
+    advect_velocity_tiled_kernel(const __grid_constant__ VelParams<T> P, int zchunk) {
+    __shared__ float ring[6 * tile::kRing];
+    auto smp = tile_sampler(face_sampler<T>(P.d, P.F, P.P), ring);
+    const int x = (int)blockIdx.x * tile::kTX + (int)threadIdx.x, y = (int)blockIdx.y * tile::kTY + (int)threadIdx.y;
+    // the predictor faces are read only by the MacCormack correction
+    march<6>(smp, ring, P.corrected ? 6 : 3, face_chunk(P.d.nz, zchunk), [&](int z) {
+        column_faces(P.d, x, y, z, [&](int axis, int fx, int fy, int fz) {
+            advect_velocity_face<T, MASK, P2>(P, face_at(P.d, axis, fx, fy, fz), smp);
+        });
+    });
+}
+
+dim3 tiled_grid(int nx, int ny, int nz, int zchunk) {
+    return dim3((unsigned)((nx + tile::kTX - 1) / tile::kTX), (unsigned)((ny + tile::kTY - 1) / tile::kTY),
+                (unsigned)((nz + zchunk - 1) / zchunk));
+}
+
+// Whether the transport passes run tiled (ffx_set_transport_tiling). Off by
+// default: on the 256^3 collider scene the tiled forms measured slower than the
+// gathers (face predictor 1.98 vs 1.68 ms, velocity 2.98 vs 2.44, scalar
+// predictor + reverse 2.21 vs 1.30, scalar final 1.51 vs 1.01): the passes are
+// bound by instruction issue, and staging adds instructions and a block
+// barrier per slice without removing arithmetic.
+int g_tiling = 0;
 
 // P0.3 plain face self-advection (mac_advect_velocity.glsl).
 template <typename T>
@@ -433,28 +497,40 @@ struct ScalarXport {
     int n;
 };
 
-template <typename T, bool MASK, bool P2>
-__device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, const Blk& b) {
+// Velocity faces as sampler fields 0..2, the scalar fields C[0..2] as 3..5.
+template <typename T>
+__device__ __forceinline__ GlobalSampler<CellFields<T>> cell_sampler(const Dev& d, const Faces<T>& F,
+                                                                    const T* const* C) {
+    return GlobalSampler<CellFields<T>>{CellFields<T>{d, F, C}};
+}
+
+template <typename T, bool MASK, bool P2, class Smp>
+__device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, int x, int y, int z, const Smp& smp) {
     const Dev& d = P.d;
-    int x, y, z;
-    if (!cell_coords(b, d.nx, d.ny, x, y, z)) return;
     const int i = cidx(d, x, y, z);
     if (MASK && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, 0.f);
         return;
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-    F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
-    F3 dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, P.dt);
+    F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
+    F3 dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, P.dt);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
-    const ClosedStencil S = closed_stencil<MASK>(d, P.solid, qx, qy, qz);
-    for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, apply_closed<T, MASK>(S, P.in[c]));
+    const auto S = smp.template closed<MASK>(P.solid, qx, qy, qz);
+    for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, smp.template apply<MASK>(3 + c, S));
     if (P.dep) {
         P.dep[i] = dep.x;
         P.dep[i + P.n] = dep.y;
         P.dep[i + 2 * P.n] = dep.z;
     }
+}
+
+template <typename T, bool MASK, bool P2>
+__device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, const Blk& b) {
+    int x, y, z;
+    if (!cell_coords(b, P.d.nx, P.d.ny, x, y, z)) return;
+    scalar_transport_cell<T, MASK, P2>(P, x, y, z, cell_sampler<T>(P.d, P.F, P.in));
 }
 
 template <typename T, bool MASK, bool P2>
@@ -481,100 +557,92 @@ struct ScalarFinal {
     float dt;
     int corrected, count;
     Channel<T> ch[3];
+    const T* fields[3];   // ch[c].field, as the sampler's scalar fields
     float* maxima;
     const float* dep;   // optional: the forward predictor's departure points (same start point, reused)
     int n;
     SrcDev src;
 };
 
+// One cell of the final scalar pass; vmax[c] is raised to |result of channel c|.
+template <typename T, bool MASK, bool P2, class Smp>
+__device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int x, int y, int z, const Smp& smp,
+                                                    float vmax[3]) {
+    const Dev& d = P.d;
+    const int i = cidx(d, x, y, z);
+    if (MASK && __ldg(P.solid + i)) {
+        for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
+        return;
+    }
+    const float dt = P.dt;
+    F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
+    F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
+    // the forward predictor traced this cell's start point with the same
+    // velocity: its departure point, and in FP32 storage its samples, are this pass's
+    const bool reuse = P.corrected && P.dep != nullptr;
+    F3 dep;
+    if (reuse) dep = {__ldg(P.dep + i), __ldg(P.dep + i + P.n), __ldg(P.dep + i + 2 * P.n)};
+    else dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt);
+    float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
+          qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
+    bool ok = false;
+    if (P.corrected) {
+        // correct_scalar.glsl:1-21
+        float s = 0.5f * dt;
+        F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
+        F3 vm2 = velocity_s<P2>(d, smp, mid2);
+        F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
+        float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
+        float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
+        ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
+               dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
+               arr.y > hb[1] || arr.z > hb[2]);
+        if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
+    }
+    // lower corner of the departure cell (the clamp bounds: its 8 corners clamped to the grid)
+    const int bx = ok ? (int)floorf(qx) : 0, by = ok ? (int)floorf(qy) : 0, bz = ok ? (int)floorf(qz) : 0;
+    const SrcDev& S = P.src;
+    // the semi-Lagrangian sample (the stored predictor value when it is the same)
+    const bool stored = reuse && sizeof(T) == 4;
+    decltype(smp.template closed<MASK>(P.solid, qx, qy, qz)) St;
+    if (!stored) St = smp.template closed<MASK>(P.solid, qx, qy, qz);
+    for (int c = 0; c < P.count; ++c) {
+        const Channel<T>& C = P.ch[c];
+        float value = stored ? Store<T>::ld(C.pred, i) : smp.template apply<MASK>(3 + c, St);
+        if (ok) {
+            float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
+            float lo, hi;
+            smp.minmax8(3 + c, bx, by, bz, lo, hi);
+            value = fminf(fmaxf(val, lo), hi);
+        }
+        value = value * expf(-C.decay * dt);
+        if (S.count < 0) {
+            float w = single_weight(S, p);
+            value = C.target >= 0.f ? fmaxf(value, C.target * w) : value + dt * C.rate * w;
+        } else {
+            float tgt = 0.f;
+            for (int k = 0; k < S.count; ++k) {
+                const float* row = S.table + 16 * k;
+                float r = C.channel == 0 ? row[11] : (C.channel == 1 ? row[12] : row[15]);
+                float w = table_weight(S, k, p);
+                bool is_target = (C.channel == 0 && row[13] > 0.5f) || (C.channel == 1 && C.table_target);
+                if (is_target) tgt = fmaxf(tgt, r * w);
+                else value = value + dt * r * w;
+            }
+            if (C.channel == 0 || (C.channel == 1 && C.table_target)) value = fmaxf(value, tgt);
+        }
+        Store<T>::st(C.out, i, value);
+        vmax[c] = fmaxf(vmax[c], finite_abs(value));
+    }
+}
+
 template <typename T, bool MASK, bool P2>
 __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, const Blk& b) {
     const Dev& d = P.d;
     int x, y, z;
     float vmax[3] = {0.f, 0.f, 0.f};
-    if (cell_coords(b, d.nx, d.ny, x, y, z)) {
-        const int i = cidx(d, x, y, z);
-        if (MASK && __ldg(P.solid + i)) {
-            for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
-        } else {
-            const float dt = P.dt;
-            F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-            F3 v0 = velocity_at_start<T, P2>(d, P.F, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
-            // the forward predictor traced this cell's start point with the same
-            // velocity: its departure point, and in FP32 storage its samples, are this pass's
-            const bool reuse = P.corrected && P.dep != nullptr;
-            F3 dep;
-            if (reuse) dep = {__ldg(P.dep + i), __ldg(P.dep + i + P.n), __ldg(P.dep + i + 2 * P.n)};
-            else dep = backtrace<T, MASK, P2>(d, P.F, P.solid, P.halo, p, v0, dt);
-            float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
-                  qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
-            bool ok = false;
-            if (P.corrected) {
-                // correct_scalar.glsl:1-21
-                float s = 0.5f * dt;
-                F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
-                F3 vm2 = velocity_at<T, P2>(d, P.F, mid2);
-                F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
-                float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
-                float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
-                ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
-                       dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
-                       arr.y > hb[1] || arr.z > hb[2]);
-                if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
-            }
-            // corners of the departure cell clamped to the grid (closed boundary), shared by the channels
-            int rows[4] = {0, 0, 0, 0}, cx0 = 0, cx1 = 0;
-            if (ok) {
-                const int bx = (int)floorf(qx), by = (int)floorf(qy), bz = (int)floorf(qz);
-                cx0 = min(max(bx, 0), d.nx - 1);
-                cx1 = min(max(bx + 1, 0), d.nx - 1);
-                const int cy0 = min(max(by, 0), d.ny - 1), cy1 = min(max(by + 1, 0), d.ny - 1);
-                const int cz0 = min(max(bz, 0), d.nz - 1), cz1 = min(max(bz + 1, 0), d.nz - 1);
-                rows[0] = cidx(d, 0, cy0, cz0);
-                rows[1] = cidx(d, 0, cy1, cz0);
-                rows[2] = cidx(d, 0, cy0, cz1);
-                rows[3] = cidx(d, 0, cy1, cz1);
-            }
-            const SrcDev& S = P.src;
-            // the semi-Lagrangian sample (the stored predictor value when it is the same)
-            const bool stored = reuse && sizeof(T) == 4;
-            ClosedStencil St;
-            if (!stored) St = closed_stencil<MASK>(d, P.solid, qx, qy, qz);
-            for (int c = 0; c < P.count; ++c) {
-                const Channel<T>& C = P.ch[c];
-                float value = stored ? Store<T>::ld(C.pred, i) : apply_closed<T, MASK>(St, C.field);
-                if (ok) {
-                    float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
-                    float lo = Store<T>::ld(C.field, rows[0] + cx0), hi = lo;
-#pragma unroll
-                    for (int k = 1; k < 8; ++k) {
-                        const float v = Store<T>::ld(C.field, rows[k >> 1] + ((k & 1) ? cx1 : cx0));
-                        lo = fminf(lo, v);
-                        hi = fmaxf(hi, v);
-                    }
-                    value = fminf(fmaxf(val, lo), hi);
-                }
-                value = value * expf(-C.decay * dt);
-                if (S.count < 0) {
-                    float w = single_weight(S, p);
-                    value = C.target >= 0.f ? fmaxf(value, C.target * w) : value + dt * C.rate * w;
-                } else {
-                    float tgt = 0.f;
-                    for (int k = 0; k < S.count; ++k) {
-                        const float* row = S.table + 16 * k;
-                        float r = C.channel == 0 ? row[11] : (C.channel == 1 ? row[12] : row[15]);
-                        float w = table_weight(S, k, p);
-                        bool is_target = (C.channel == 0 && row[13] > 0.5f) || (C.channel == 1 && C.table_target);
-                        if (is_target) tgt = fmaxf(tgt, r * w);
-                        else value = value + dt * r * w;
-                    }
-                    if (C.channel == 0 || (C.channel == 1 && C.table_target)) value = fmaxf(value, tgt);
-                }
-                Store<T>::st(C.out, i, value);
-                vmax[c] = finite_abs(value);
-            }
-        }
-    }
+    if (cell_coords(b, d.nx, d.ny, x, y, z))
+        advect_scalars_cell<T, MASK, P2>(P, x, y, z, cell_sampler<T>(d, P.F, P.fields), vmax);
     if (P.maxima) {
         for (int c = 0; c < P.count; ++c) {
             block_max_to(P.maxima + c, vmax[c]);
@@ -586,6 +654,53 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
 template <typename T, bool MASK, bool P2>
 __global__ void FFX_LB_SCALARS advect_scalars_kernel(const __grid_constant__ ScalarFinal<T> P) {
     advect_scalars_body<T, MASK, P2>(P, hw_blk());
+}
+
+// ------------------------------------------------ tiled scalar passes
+// The scalar predictor/reverse and final passes over shared-memory windows of
+// the velocity faces and the transported scalars (ffx_tile.cuh); a thread
+// works the cell (x, y, z) of its column at each slice of the block's chunk.
+#ifndef FFX_MINB_SCALAR_PREDICTOR_TILED
+#define FFX_MINB_SCALAR_PREDICTOR_TILED 4
+#endif
+#ifndef FFX_MINB_SCALARS_TILED
+#define FFX_MINB_SCALARS_TILED 4
+#endif
+
+__device__ __forceinline__ Chunk cell_chunk(int nz, int zchunk) {
+    const int z0 = blockIdx.z * zchunk;
+    return Chunk{z0, min(z0 + zchunk, nz)};
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(tile::kThreads, FFX_MINB_SCALAR_PREDICTOR_TILED)
+    scalar_transport_tiled_kernel(const __grid_constant__ ScalarXport<T> P, int zchunk) {
+    __shared__ float ring[6 * tile::kRing];
+    auto smp = tile_sampler(cell_sampler<T>(P.d, P.F, P.in), ring);
+    const int x = (int)blockIdx.x * tile::kTX + (int)threadIdx.x, y = (int)blockIdx.y * tile::kTY + (int)threadIdx.y;
+    const bool in = x < P.d.nx && y < P.d.ny;
+    march<6>(smp, ring, 3 + P.count, cell_chunk(P.d.nz, zchunk), [&](int z) {
+        if (in) scalar_transport_cell<T, MASK, P2>(P, x, y, z, smp);
+    });
+}
+
+template <typename T, bool MASK, bool P2>
+__global__ void __launch_bounds__(tile::kThreads, FFX_MINB_SCALARS_TILED)
+    advect_scalars_tiled_kernel(const __grid_constant__ ScalarFinal<T> P, int zchunk) {
+    __shared__ float ring[6 * tile::kRing];
+    auto smp = tile_sampler(cell_sampler<T>(P.d, P.F, P.fields), ring);
+    const int x = (int)blockIdx.x * tile::kTX + (int)threadIdx.x, y = (int)blockIdx.y * tile::kTY + (int)threadIdx.y;
+    const bool in = x < P.d.nx && y < P.d.ny;
+    float vmax[3] = {0.f, 0.f, 0.f};
+    march<6>(smp, ring, 3 + P.count, cell_chunk(P.d.nz, zchunk), [&](int z) {
+        if (in) advect_scalars_cell<T, MASK, P2>(P, x, y, z, smp, vmax);
+    });
+    if (P.maxima) {
+        for (int c = 0; c < P.count; ++c) {
+            block_max_to(P.maxima + c, vmax[c]);
+            __syncthreads();
+        }
+    }
 }
 
 // P0.2 open-boundary transport in an analytic flow (advect.glsl).
@@ -680,6 +795,12 @@ using namespace ffx;
 
 extern "C" {
 
+int ffx_set_transport_tiling(int enable) {
+    const int previous = g_tiling;
+    g_tiling = enable ? 1 : 0;
+    return previous;
+}
+
 int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                              const void* w, float dt, void* pu, void* pv, void* pw, float* const dep[3],
                              void* stream) {
@@ -704,7 +825,13 @@ int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, 
             Q.dep[a] = dep ? dep[a] : nullptr;
             Q.nf[a] = (d.nx + (a == 0)) * (d.ny + (a == 1)) * (d.nz + (a == 2));
         }
-        FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P, (face_predictor_kernel<T, M, P><<<blocks, threads, 0, st>>>(Q)));
+        if (g_tiling) {
+            const int zc = FFX_TILE_ZCHUNK;
+            FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P,
+                                 (face_predictor_tiled_kernel<T, M, P><<<tiled_grid(d.nx, d.ny, d.nz, zc), threads, 0, st>>>(Q, zc)));
+        } else {
+            FFX_DISPATCH_MASK_P2(solid != nullptr, d.pow2 != 0, M, P, (face_predictor_kernel<T, M, P><<<blocks, threads, 0, st>>>(Q)));
+        }
     });
     return launch_status("face_predictor_kernel");
 }
@@ -756,7 +883,13 @@ int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
         const float extent[3] = {g->ex, g->ey, g->ez};
         P.src = make_src(src, extent);
         if (!src) P.src.count = 0;
-        FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_velocity_kernel<T, M, Q><<<blocks, threads, 0, st>>>(P)));
+        if (g_tiling) {
+            const int zc = FFX_TILE_ZCHUNK;
+            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
+                                 (advect_velocity_tiled_kernel<T, M, Q><<<tiled_grid(d.nx, d.ny, d.nz, zc), threads, 0, st>>>(P, zc)));
+        } else {
+            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_velocity_kernel<T, M, Q><<<blocks, threads, 0, st>>>(P)));
+        }
     });
     return launch_status("advect_velocity_kernel");
 }
@@ -818,7 +951,13 @@ int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage
         }
         P.dep = dep;
         P.n = g->nx * g->ny * g->nz;
-        FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (scalar_transport_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+        if (g_tiling) {
+            const int zc = FFX_TILE_ZCHUNK;
+            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
+                                 (scalar_transport_tiled_kernel<T, M, Q><<<tiled_grid(d.nx, d.ny, d.nz, zc), block, 0, st>>>(P, zc)));
+        } else {
+            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (scalar_transport_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+        }
     });
     return launch_status("scalar_transport_kernel");
 }
@@ -869,13 +1008,20 @@ int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage, 
                 C.table_target = H.table_target;
             }
             P.ch[c] = C;
+            P.fields[c] = C.field;
         }
         P.maxima = maxima;
         P.dep = corrected ? dep : nullptr;
         P.n = g->nx * g->ny * g->nz;
         const float extent[3] = {g->ex, g->ey, g->ez};
         P.src = make_src(src, extent);
-        FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_scalars_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+        if (g_tiling) {
+            const int zc = FFX_TILE_ZCHUNK;
+            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
+                                 (advect_scalars_tiled_kernel<T, M, Q><<<tiled_grid(d.nx, d.ny, d.nz, zc), block, 0, st>>>(P, zc)));
+        } else {
+            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (advect_scalars_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+        }
     });
     return launch_status("advect_scalars_kernel");
 }
@@ -1114,6 +1260,7 @@ size_t scalar_final_desc(const FfxBatchDomain& D, int parity, void* out) {
             C.channel = H[c]->channel;
             C.table_target = H[c]->table_target;
             P.ch[c] = C;
+            P.fields[c] = C.field;
         }
         P.maxima = nullptr;
         P.dep = D.scalar_corrected ? D.cell_trace : nullptr;

@@ -1,0 +1,169 @@
+// Device-side solve loops of the single-domain solvers: a CUDA graph whose
+// WHILE node repeats a captured body (one V-cycle, the residual maximum and
+// the decision) until the residual meets the tolerance or the cycle budget is
+// spent, so a pressure solve to a tolerance needs no host round trip. The loop
+// of backend/solid_multigrid.py:67-76 with the tolerance test of the
+// extension (while cycles < max and max|r| > tol * max|rhs|: cycle) decided on
+// the device in FP64.
+//
+// Use: ffx_loop_begin starts capturing the caller's stream; the caller issues
+// the passes before the loop, ending with ffx_loop_decide (which sets the loop
+// condition); ffx_loop_while adds the WHILE node and returns a stream that
+// captures its body, where the caller issues one iteration ending with
+// ffx_loop_decide again; ffx_loop_end_while closes the body; the caller may
+// issue passes after the loop on its stream; ffx_loop_end instantiates. Every
+// launch of the result (ffx_loop_launch) runs the whole solve.
+#include "ffx_host.cuh"
+
+struct FfxLoop {
+    cudaStream_t st = nullptr;       // the caller's stream (capturing between begin and end)
+    cudaStream_t side = nullptr;     // captures the WHILE body
+    cudaGraph_t graph = nullptr;
+    cudaGraphConditionalHandle handle = 0;
+    cudaGraphNode_t node = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    int in_body = 0;
+};
+
+namespace ffx {
+namespace {
+
+// counters[0]: cycles of the current solve (zeroed by ffx_loop_reset_counter),
+// counters[1]: cycles of all solves, counters[2]: decisions taken.
+__global__ void loop_decide_kernel(const float* rmax, const float* scale, double tol, int max_cycles,
+                                   int* counters, cudaGraphConditionalHandle handle) {
+    const double r = (double)*rmax, s = (double)*scale;
+    const bool go = counters[0] < max_cycles && s > 0.0 && r > tol * s;
+    if (go) {
+        counters[0] += 1;
+        counters[1] += 1;
+    }
+    counters[2] += 1;
+    cudaGraphSetConditional(handle, go ? 1u : 0u);
+}
+
+__global__ void loop_reset_kernel(int* counters) { counters[0] = 0; }
+
+// p = 0 where the right-hand side is all zero (scale == 0): the solve of a
+// zero right-hand side is zero pressure, whatever the warm start held.
+__global__ void zero_if_unscaled_kernel(const float* scale, float* p, int64_t n) {
+    if (*scale != 0.f) return;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = 0.f;
+}
+
+}  // namespace
+}  // namespace ffx
+
+using namespace ffx;
+
+extern "C" {
+
+int ffx_loop_begin(void* stream, FfxLoop** out) {
+    FFX_REQUIRE(stream && out, "ffx_loop_begin: a stream (not the legacy default stream) and an output are required");
+    FfxLoop* L = new FfxLoop;
+    L->st = as_stream(stream);
+    int rc = cuda_status(cudaStreamCreateWithFlags(&L->side, cudaStreamNonBlocking), "ffx_loop_begin: stream");
+    if (!rc) rc = cuda_status(cudaStreamBeginCapture(L->st, cudaStreamCaptureModeRelaxed), "ffx_loop_begin: capture");
+    if (!rc) {
+        cudaStreamCaptureStatus status;
+        rc = cuda_status(cudaStreamGetCaptureInfo(L->st, &status, nullptr, &L->graph, nullptr, nullptr),
+                         "ffx_loop_begin: capture info");
+        if (!rc && status != cudaStreamCaptureStatusActive) rc = fail(FFX_ERR_CUDA, "ffx_loop_begin: not capturing");
+    }
+    if (!rc)
+        rc = cuda_status(cudaGraphConditionalHandleCreate(&L->handle, L->graph, 0, cudaGraphCondAssignDefault),
+                         "ffx_loop_begin: conditional handle");
+    if (rc) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(L->st, &g);
+        if (g) cudaGraphDestroy(g);
+        if (L->side) cudaStreamDestroy(L->side);
+        delete L;
+        return rc;
+    }
+    *out = L;
+    return FFX_OK;
+}
+
+int ffx_loop_decide(FfxLoop* L, const float* rmax, const float* scale, double tol, int32_t max_cycles,
+                    int32_t* counters, void* stream) {
+    FFX_REQUIRE(L && rmax && scale && counters && max_cycles >= 0 && tol >= 0.0, "ffx_loop_decide: invalid arguments");
+    loop_decide_kernel<<<1, 1, 0, as_stream(stream)>>>(rmax, scale, tol, max_cycles, counters, L->handle);
+    return launch_status("loop_decide_kernel");
+}
+
+int ffx_loop_reset_counter(int32_t* counters, void* stream) {
+    FFX_REQUIRE(counters, "ffx_loop_reset_counter: invalid arguments");
+    loop_reset_kernel<<<1, 1, 0, as_stream(stream)>>>(counters);
+    return launch_status("loop_reset_kernel");
+}
+
+int ffx_zero_if_unscaled(const float* scale, float* p, int64_t count, void* stream) {
+    FFX_REQUIRE(scale && p && count >= 1, "ffx_zero_if_unscaled: invalid arguments");
+    const int64_t want = (count + 255) / 256;
+    zero_if_unscaled_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(scale, p, count);
+    return launch_status("zero_if_unscaled_kernel");
+}
+
+int ffx_loop_while(FfxLoop* L, void** body_stream) {
+    FFX_REQUIRE(L && body_stream && !L->in_body && !L->node, "ffx_loop_while: one loop per graph, after begin");
+    cudaStreamCaptureStatus status;
+    cudaGraph_t graph = nullptr;
+    const cudaGraphNode_t* deps = nullptr;
+    size_t ndeps = 0;
+    int rc = cuda_status(cudaStreamGetCaptureInfo(L->st, &status, nullptr, &graph, &deps, &ndeps),
+                         "ffx_loop_while: capture info");
+    if (rc) return rc;
+    cudaGraphNodeParams params = {cudaGraphNodeTypeConditional};
+    params.conditional.handle = L->handle;
+    params.conditional.type = cudaGraphCondTypeWhile;
+    params.conditional.size = 1;
+    rc = cuda_status(cudaGraphAddNode(&L->node, graph, deps, ndeps, &params), "ffx_loop_while: node");
+    if (rc) return rc;
+    cudaGraph_t body = params.conditional.phGraph_out[0];
+    rc = cuda_status(cudaStreamBeginCaptureToGraph(L->side, body, nullptr, nullptr, 0, cudaStreamCaptureModeRelaxed),
+                     "ffx_loop_while: body capture");
+    if (rc) return rc;
+    L->in_body = 1;
+    *body_stream = L->side;
+    return FFX_OK;
+}
+
+int ffx_loop_end_while(FfxLoop* L) {
+    FFX_REQUIRE(L && L->in_body, "ffx_loop_end_while: no open loop body");
+    cudaGraph_t captured = nullptr;
+    int rc = cuda_status(cudaStreamEndCapture(L->side, &captured), "ffx_loop_end_while: end of body capture");
+    L->in_body = 0;
+    if (rc) return rc;
+    return cuda_status(cudaStreamUpdateCaptureDependencies(L->st, &L->node, 1, cudaStreamSetCaptureDependencies),
+                       "ffx_loop_end_while: dependencies");
+}
+
+int ffx_loop_end(FfxLoop* L) {
+    FFX_REQUIRE(L && !L->in_body && L->node && !L->exec, "ffx_loop_end: the loop body must be closed");
+    cudaGraph_t graph = nullptr;
+    int rc = cuda_status(cudaStreamEndCapture(L->st, &graph), "ffx_loop_end: end capture");
+    if (!rc) rc = cuda_status(cudaGraphInstantiate(&L->exec, graph, 0), "ffx_loop_end: instantiate");
+    if (graph) cudaGraphDestroy(graph);
+    return rc;
+}
+
+int ffx_loop_launch(FfxLoop* L, void* stream) {
+    FFX_REQUIRE(L && L->exec, "ffx_loop_launch: not instantiated");
+    return cuda_status(cudaGraphLaunch(L->exec, as_stream(stream)), "ffx_loop_launch");
+}
+
+int ffx_loop_destroy(FfxLoop* L) {
+    if (!L) return FFX_OK;
+    if (L->in_body) {
+        cudaGraph_t g = nullptr;
+        cudaStreamEndCapture(L->side, &g);
+    }
+    if (L->exec) cudaGraphExecDestroy(L->exec);
+    if (L->side) cudaStreamDestroy(L->side);
+    delete L;
+    return FFX_OK;
+}
+
+}  // extern "C"

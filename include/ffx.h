@@ -113,6 +113,13 @@ int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const v
                     void* out, void* stream);
 
 /* ---------------------------------------------------------- velocity passes */
+/* The transport passes (face predictor, velocity, scalar predictor/reverse and
+ * final scalar pass) run as global-memory gathers by default (enable = 0), or,
+ * with enable != 0, over shared-memory windows of a rolling z slab (measured
+ * slower on B200: the passes are bound by instruction issue). Both forms give
+ * bit-identical results; the switch is process-wide and returns the previous
+ * setting. No counterpart in the reference (an A/B switch). */
+int ffx_set_transport_tiling(int enable);
 /* MacCormack predictor of all three face components in one launch; replaces
  * backend/detail.py:27-37 + shaders/transport_face.glsl. */
 int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
@@ -387,15 +394,56 @@ int ffx_divergence_stats(int64_t count, const float* before, const float* after,
  * real-time callback where cudaMalloc -- which may synchronise the device -- is
  * not allowed, a C caller with no allocator). No counterpart in the reference.
  * Allocates nothing: the block partials live in a fixed 56,832-byte array of
- * the library, reserved on every GPU that loads it until the library is
- * unloaded. count must lie in [1, 2^31 - 1]; larger counts are rejected with
- * FFX_ERR_INVALID (use ffx_divergence_stats). The first call on a device looks
- * up that array's device address (cudaGetSymbolAddress) with the device
- * current; make that first call before any stream capture. All calls share the
- * array: calls whose kernels overlap on the GPU race; calls ordered on one
- * stream do not, since each call rewrites every partial it reads. */
+ * the library (at most 1184 blocks of six FP64 partials, whatever the count),
+ * reserved on every GPU that loads it until the library is unloaded. Any
+ * count >= 1 is accepted (count < 1 gives FFX_ERR_INVALID), and the result is
+ * bit-identical to ffx_divergence_stats'. The first call on a device looks up
+ * that array's device address (cudaGetSymbolAddress) with the device current;
+ * make that first call before any stream capture. The address is cached per
+ * device: after cudaDeviceReset it is stale, so reload the library. All calls
+ * share the array: calls whose kernels overlap on the GPU race; calls ordered
+ * on one stream do not, since each call rewrites every partial it reads. */
 int ffx_divergence_stats_static(int64_t count, const float* before, const float* after,
                                 double* out, void* stream);
+
+/* ------------------------------------------------------- device solve loops */
+/* A pressure solve to a tolerance as one CUDA graph with a WHILE node, so it
+ * needs no host round trip (the V-cycle loop of backend/solid_multigrid.py:67-76
+ * with the tolerance test decided on the device). ffx_loop_begin starts
+ * capturing `stream` (a created stream, not the legacy default stream); the
+ * caller issues the passes before the loop, the last of them ffx_loop_decide;
+ * ffx_loop_while adds the WHILE node and returns in *body_stream a stream that
+ * captures the loop body (one iteration, again ending with ffx_loop_decide);
+ * ffx_loop_end_while closes the body; passes after the loop go to `stream`;
+ * ffx_loop_end instantiates the graph and ffx_loop_launch runs the whole solve.
+ * ffx_loop_decide: continue while counters[0] < max_cycles and
+ * max|r| (*rmax) > tol * (*scale) with *scale > 0, in FP64; a continuing
+ * decision adds one to counters[0] (this solve) and counters[1] (all solves);
+ * counters[2] counts decisions. The loop ends by the cycle budget at the latest.
+ * ffx_loop_reset_counter sets counters[0] = 0; ffx_zero_if_unscaled zeroes p
+ * when *scale == 0 (a zero right-hand side). */
+typedef struct FfxLoop FfxLoop;
+int ffx_loop_begin(void* stream, FfxLoop** loop);
+int ffx_loop_decide(FfxLoop* loop, const float* rmax, const float* scale, double tol,
+                    int32_t max_cycles, int32_t* counters, void* stream);
+int ffx_loop_reset_counter(int32_t* counters, void* stream);
+int ffx_zero_if_unscaled(const float* scale, float* p, int64_t count, void* stream);
+int ffx_loop_while(FfxLoop* loop, void** body_stream);
+int ffx_loop_end_while(FfxLoop* loop);
+int ffx_loop_end(FfxLoop* loop);
+int ffx_loop_launch(FfxLoop* loop, void* stream);
+int ffx_loop_destroy(FfxLoop* loop);
+
+/* ------------------------------------------------------------- bake readback */
+/* Storage code of a uint8 field (the collider mask) for ffx_pack_channels. */
+enum { FFX_PACK_U8 = 2 };
+/* Packs `channels` (1..8) fields of `count` values each -- kinds[c] is FFX_F32,
+ * FFX_BF16 or FFX_PACK_U8 -- into out[c * count + i] as FP32: the frame layout of
+ * the playback cache (channel after channel, x-fast), so one device-to-host copy
+ * of `out` carries a whole baked frame. Replaces the per-channel texture reads of
+ * backend/cache.py:7-11 (capture). */
+int ffx_pack_channels(int64_t count, int channels, const void* const* fields, const int* kinds,
+                      float* out, void* stream);
 
 /* ------------------------------------------------------ fire configuration */
 /* Cell vorticity (omega.xyz, |omega|) as float4 per cell, central differences of
