@@ -10,9 +10,10 @@ density and temperature; aggregation multigrid projection until the relative
 max-norm divergence is <= 1e-4; dt = min(0.02, 0.5 dx / max|u|). Initial
 velocity: zero plus seeded uniform +-1e-3 noise on every face.
 
-One "step" = one DenseProjectedSmoke.step plus the next-dt selection (one
-readback of three floats). Solver variants, all to the same tolerance from the
-same seeded start after the same warm-up:
+One "step" = one DenseProjectedSmoke.step_cfl: the step plus the next-dt
+selection on the device (the pressure solve's V-cycle loop also runs on the
+device), so a step is queued without any host readback. Solver variants, all
+to the same tolerance from the same seeded start after the same warm-up:
 
 * plain   -- the reference algorithm: stand-alone aggregation V-cycles (4/4
              Jacobi sweeps), pressure cold-started every step, FP32 storage;
@@ -61,6 +62,8 @@ VARIANTS = {
     'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9),
     'learned_plain': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
     'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
+    'learned_warm': dict(pressure_method='VCYCLE', solid_warm_start=True, learned_warm_start=True,
+                         learned_correction=True, mg_coarse_scale=1.9),
 }
 
 # Algorithmic bytes per cell of each pass (inputs read once, outputs written
@@ -223,13 +226,10 @@ class Run:
         self.h = 1.0 / args.size
         self.dt = 0.02
 
-    def next_dt(self):
-        umax = max(self.solver.projector.velocity_maxima())
-        return min(0.02, 0.5 * self.h / umax) if umax > 0 else 0.02
-
     def step(self):
-        self.solver.step(self.dt, sources=self.emitters)
-        self.dt = self.next_dt()
+        """One step with dt = min(0.02, 0.5 dx / max|u|) chosen on the device
+        from the previous step's velocity (first step 0.02): no host readback."""
+        self.solver.step_cfl(0.5, 0.02, sources=self.emitters)
 
     def warm(self, count):
         for _ in range(count):
@@ -245,17 +245,18 @@ class Run:
         solver = self.solver
         self.pass_timer = PassTimer(stream) if passes else None
         solver.pass_timer = self.pass_timer
-        self.cycles = []
         graphs0 = len(getattr(solver.projector, '_graphs', ()))
         calls0 = self.device.calls
+        cycles0 = solver.projector.total_cycles()
         torch.cuda.synchronize()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
         for _ in range(count):
             self.step()
-            self.cycles.append(solver.projector.last_cycles)
         end.record(stream)
         torch.cuda.synchronize()
+        # the solves count their cycles on the device: read once, after the timed region
+        self.cycles = (solver.projector.total_cycles() - cycles0) / count
         self.launches = self.device.calls - calls0
         self.captures = len(getattr(solver.projector, '_graphs', ())) - graphs0
         solver.pass_timer = None
@@ -393,23 +394,23 @@ def run_b200(args):
                                    f"{args.storage} storage",
                        "cells": cells, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}",
-                       "v_cycles_mean": statistics.mean(head['cycles']), "v_cycles_max": max(head['cycles']),
+                       "v_cycles_mean": head['cycles'], "host_syncs_per_step": 0,
                        "graph_captures_in_timed_steps": head['captures'],
                        "final_rel_div_inf": rel_div,
                        "plain_fp32_mg": None if plain is None else {
                            "steps_per_s": job_rate(world, plain['steps'], p_el), "steps": plain['steps'],
-                           "v_cycles_mean": statistics.mean(plain['cycles']),
+                           "v_cycles_mean": plain['cycles'],
                            "final_rel_div_inf": plain['rel_div']},
                        "speedup_vs_plain": None if plain is None else
                        job_rate(world, args.steps, elapsed) / job_rate(world, plain['steps'], p_el),
                        "fast_previous_pressure_mg": None if fast is None else {
                            "steps_per_s": job_rate(world, fast['steps'], f_el), "steps": fast['steps'],
-                           "v_cycles_mean": statistics.mean(fast['cycles']),
+                           "v_cycles_mean": fast['cycles'],
                            "final_rel_div_inf": fast['rel_div'], "storage": args.storage,
                            "method": "over-corrected V(4,4) cycles from the previous step's pressure"},
                        "plain_cycles_from_network": None if learned is None else {
                            "steps_per_s": job_rate(world, learned['steps'], l_el), "steps": learned['steps'],
-                           "v_cycles_mean": statistics.mean(learned['cycles']),
+                           "v_cycles_mean": learned['cycles'],
                            "final_rel_div_inf": learned['rel_div'], "storage": args.storage,
                            "method": "the reference's V(4,4) cycles from the U-Net's guess (net on the 128^3 "
                                      "restriction, trilinear prolongation)"}},

@@ -159,6 +159,17 @@ _PROTOTYPES = {
                                      C.c_int, P(FfxScalarChannel), vp, vp]),
     'ffx_advect_scalars_trace': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, C.c_int,
                                            P(FfxSources), C.c_int, P(FfxScalarChannel), vp, vp, vp]),
+    # the same passes with the time step read on the device (a float pointer in place of dt)
+    'ffx_face_predictor_dt': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp, P(vp), vp]),
+    'ffx_advect_velocity_dt': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp, C.c_int,
+                                         f32, P(FfxSources), vp, vp, f32, f32, C.c_int, vp, vp, vp, P(vp), vp]),
+    'ffx_scalar_transport_dt': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, f32, C.c_int, P(vp),
+                                          P(vp), vp, vp]),
+    'ffx_advect_scalars_dt': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, C.c_int,
+                                        P(FfxSources), C.c_int, P(FfxScalarChannel), vp, vp, vp]),
+    'ffx_next_dt': (C.c_int, [vp, vp, vp, C.c_double, C.c_double, C.c_double, vp]),
+    'ffx_add': (C.c_int, [i64, vp, vp, vp, vp]),
+    'ffx_scale_by_ratio': (C.c_int, [i64, vp, vp, vp]),
     'ffx_advect_open': (C.c_int, [P(FfxGrid), C.c_int, vp, f32, f3, f32, f3, f32, f32, f32, vp, vp]),
     'ffx_mac_advect_density': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f3, f32, f32, f32, vp, vp]),
     'ffx_walls': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp]),

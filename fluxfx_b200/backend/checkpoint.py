@@ -46,7 +46,7 @@ FORMAT_COLLIDERS = 'fluxfx-checkpoint-1+colliders'
 # Settings this build adds to the reference's PressureSettings.
 EXTENSION_SETTINGS = ('pressure_tolerance', 'pressure_max_cycles', 'mg_pre_sweeps', 'mg_post_sweeps',
                       'mg_max_levels', 'heat_mode', 'velocity_blend', 'storage', 'solid_warm_start',
-                      'pressure_method', 'learned_warm_start', 'mg_coarse_scale')
+                      'pressure_method', 'learned_warm_start', 'mg_coarse_scale', 'learned_correction')
 _TUPLES = ('velocity', 'source_center')
 
 
@@ -66,7 +66,7 @@ def save_checkpoint(solver, path):
         extensions['axis_limit'] = solver.grid.axis_limit
     meta = {'format': FORMAT if solver.solids is None else FORMAT_COLLIDERS, 'settings': settings,
             'grid': {'shape': list(solver.grid.shape), 'extent': list(solver.grid.extent)},
-            'time': solver.time, 'steps': solver.steps, 'last_dt': solver.projector.last_dt,
+            'time': solver.time, 'steps': solver.steps, 'last_dt': solver.projector.previous_dt(),
             'extensions': extensions}
     if solver.solids is not None:
         meta['colliders'] = [{'shape': c.shape, 'inverse_rows': [list(r) for r in c.inverse_rows]}

@@ -50,9 +50,10 @@ class DetailPasses:
             self.reverses = [self.device.texture(self.grid.shape, dtype=self.dtype) for _ in range(count)]
             self.predictor, self.reverse = self.predictors[0], self.reverses[0]
 
-    def transport_many(self, fields, velocities, dt):
+    def transport_many(self, fields, velocities, dt, dt_device=None):
         """Predictor (+dt) and reverse (-dt) of up to three scalars; returns
-        (predictors, reverses) tensors aligned with ``fields``."""
+        (predictors, reverses) tensors aligned with ``fields``. ``dt_device``:
+        a device float holding dt (``ffx_*_dt`` entry points) instead of ``dt``."""
         count = len(fields)
         self._ensure_scalar(count)
         vel = [ptr(velocities[name]) if isinstance(velocities, dict) else ptr(velocities[i])
@@ -64,24 +65,31 @@ class DetailPasses:
         if self.reuse_traces and self.cell_trace is None:
             self.cell_trace = torch.empty(3 * prod(self.grid.shape), dtype=torch.float32, device=self.device.device)
         trace = ptr(self.cell_trace) if self.reuse_traces else None
-        self.device.call('ffx_scalar_transport_trace', gp, sp, self._storage, *vel, dt, count, ins, preds, trace, s)
-        self.device.call('ffx_scalar_transport', gp, sp, self._storage, *vel, -dt, count, preds, revs, s)
+        if dt_device is not None:
+            self.device.call('ffx_scalar_transport_dt', gp, sp, self._storage, *vel, dt_device, 1.0, count, ins, preds,
+                             trace, s)
+            self.device.call('ffx_scalar_transport_dt', gp, sp, self._storage, *vel, dt_device, -1.0, count, preds,
+                             revs, None, s)
+        else:
+            self.device.call('ffx_scalar_transport_trace', gp, sp, self._storage, *vel, dt, count, ins, preds, trace,
+                             s)
+            self.device.call('ffx_scalar_transport', gp, sp, self._storage, *vel, -dt, count, preds, revs, s)
         return self.predictors[:count], self.reverses[:count]
 
     def transport(self, field, velocities, dt):
         preds, revs = self.transport_many([field], velocities, dt)
         return {'predictorField': preds[0], 'reverseField': revs[0]}
 
-    def transport_velocity(self, fields, dt):
+    def transport_velocity(self, fields, dt, dt_device=None):
         """Predict each signed face component; the reverse sample is fused with the correction."""
         if self.face_predictor is None:
             self.face_predictor = [self.device.texture(s, dtype=self.dtype) for s in self.grid.face_shapes]
         if self.reuse_traces and self._face_reuse and self.face_trace is None:
             self.face_trace = [torch.empty(3 * prod(s), dtype=torch.float32, device=self.device.device)
                                for s in self.grid.face_shapes]
-        self.device.call('ffx_face_predictor_trace', C.byref(self._g), C.byref(self._solids), self._storage,
-                         *[ptr(f) for f in fields], dt, *[ptr(p) for p in self.face_predictor],
-                         self.face_traces(), self.device.s)
+        name, step = ('ffx_face_predictor_dt', dt_device) if dt_device is not None else ('ffx_face_predictor_trace', dt)
+        self.device.call(name, C.byref(self._g), C.byref(self._solids), self._storage, *[ptr(f) for f in fields],
+                         step, *[ptr(p) for p in self.face_predictor], self.face_traces(), self.device.s)
 
     def face_traces(self):
         """The face departure points as a C array of three pointers, or NULL."""

@@ -105,18 +105,31 @@ class PressureProjector:
         self.compute_divergence(self.bounded, self.before)
         self._finish(outputs, dt)
 
-    def _finish(self, outputs, dt):
+    def project_bounded_device(self, outputs, clock):
+        """``project_bounded`` with the time step on the device: ``clock`` is the
+        solver's float32 device pair (dt, previous dt). Needs the impulse form
+        (the solve is dt-independent; only the warm start's dt / previous dt
+        rescaling reads the clock, on the device)."""
+        if not self.uses_impulse:
+            raise ValueError('Device time steps need the impulse pressure form (multigrid or colliders)')
+        self.compute_divergence(self.bounded, self.before)
         self.ready = False
-        previous_dt, self.last_dt = self.last_dt, None
-        impulse = self.uses_impulse
-        solve_dt = 1.0 if impulse else dt
-        previous_solve_dt = (1.0 if previous_dt is not None else None) if impulse else previous_dt
-        if impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
-            # The incremental pressure force scales with physical dt: rescale the
-            # guess (in place, so the pressure keeps its buffer from step to step).
-            self.device.call('ffx_scale', self.pressure.numel(), ptr(self.pressure), dt / previous_dt,
-                             ptr(self.pressure), self.device.s)
-        self.solve_pressure(solve_dt, previous_solve_dt)
+        previous = self.last_dt is not None
+        if previous:
+            self.device.call('ffx_scale_by_ratio', self.pressure.numel(), ptr(self.pressure), ptr(clock),
+                             self.device.s)
+        self.solve_pressure(1.0, 1.0 if previous else None)
+        self._gradient(outputs, 1.0)
+        self.last_dt = clock        # the previous dt now lives on the device (clock[1] after the step)
+        self.ready = True
+
+    def previous_dt(self):
+        """The last projection's dt on the host (one readback after device steps)."""
+        if self.last_dt is None or isinstance(self.last_dt, float):
+            return self.last_dt
+        return float(self.last_dt[1].item())
+
+    def _gradient(self, outputs, solve_dt):
         links = self.gradient_links()
         if links is not None:
             self.device.call('ffx_gradient_links', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
@@ -126,6 +139,20 @@ class PressureProjector:
             self.device.call('ffx_gradient', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
                              ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),
                              ptr(self._scalars[0:3]), self.device.s)
+
+    def _finish(self, outputs, dt):
+        self.ready = False
+        previous_dt, self.last_dt = self.previous_dt(), None
+        impulse = self.uses_impulse
+        solve_dt = 1.0 if impulse else dt
+        previous_solve_dt = (1.0 if previous_dt is not None else None) if impulse else previous_dt
+        if impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
+            # The incremental pressure force scales with physical dt: rescale the
+            # guess (in place, so the pressure keeps its buffer from step to step).
+            self.device.call('ffx_scale', self.pressure.numel(), ptr(self.pressure), dt / previous_dt,
+                             ptr(self.pressure), self.device.s)
+        self.solve_pressure(solve_dt, previous_solve_dt)
+        self._gradient(outputs, solve_dt)
         self.last_dt = dt
         self.ready = True
 

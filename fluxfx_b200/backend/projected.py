@@ -79,7 +79,25 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             self.combustion = CombustionPasses(self.grid, self.device, self._field_dtype)
         self._solids = solids_struct(self.solids) if self.solids is not None else N.FfxSolids()
         self._maxima = torch.zeros(3, dtype=torch.float32, device=self.device.device)
+        # device-side time step (step_cfl): clock = (dt, previous dt), time in FP64
+        self._clock = torch.zeros(2, dtype=torch.float32, device=self.device.device)
+        self._clock_time = torch.zeros(1, dtype=torch.float64, device=self.device.device)
+        self._clock_live = False
         self.reset()
+
+    # Simulation time: host steps add dt here; device-timed steps (step_cfl)
+    # accumulate it on the device, read (once, synchronising) when asked.
+    @property
+    def time(self):
+        if getattr(self, '_clock_live', False):
+            return self._time_host + float(self._clock_time.item())
+        return self._time_host
+
+    @time.setter
+    def time(self, value):
+        self._time_host = float(value)
+        if getattr(self, '_clock_live', False):
+            self._clock_time.zero_()
 
     @property
     def allocated_bytes(self):
@@ -89,6 +107,7 @@ class DenseProjectedSmoke(DenseThermalAdvection):
 
     def reset(self, seed=True):
         super().reset(seed)
+        self._clock_live = False      # the next step_cfl starts again from dt_max
         self.faulted = False
         if self.combustion is not None:
             self.combustion.reset()
@@ -151,6 +170,46 @@ class DenseProjectedSmoke(DenseThermalAdvection):
     def measure_projection(self):
         return self.projector.metrics() | {"step": self.steps, "simulation_time": self.time}
 
+    def step_cfl(self, cfl=0.5, dt_max=0.02, emission=None, sources=None):
+        """One step whose time step lives on the device: the first step of a
+        run (after construction or ``reset``) uses ``dt_max``; every step ends
+        by setting the next dt = min(dt_max, cfl * cell / max|u|) on the device
+        from the face maxima of its corrected velocity (cell = the smallest cell
+        spacing), in FP64 -- the rule the workloads state. Nothing is read back:
+        with the device-side V-cycle loop a step is queued without waiting for
+        the GPU. ``time`` and ``current_dt()`` read the clock when asked. Needs
+        the impulse pressure form (multigrid or colliders); not with
+        confinement, combustion or moving colliders."""
+        if not (0 < cfl <= 10 and 0 < dt_max <= 0.1):
+            raise ValueError('cfl must lie in (0, 10] and dt_max in (0, 0.1]')
+        s = self.settings
+        if s.vorticity_strength > 0 or self.combustion is not None or s.moving_colliders:
+            raise ValueError('Device time steps cover the smoke step without confinement, combustion '
+                             'or moving colliders')
+        if sources is not None:
+            self._prepare_sources(sources)
+        if self.faulted:
+            raise RuntimeError("Reset required after a failed GPU step")
+        if not self._clock_live:
+            previous = self.projector.previous_dt()
+            self._clock[0] = dt_max
+            self._clock[1] = previous if previous is not None else 0.0
+            self._clock_time.zero_()
+            self._clock_live = True
+        try:
+            self._step(None, emission or Emission(self.settings.source_center), sources, clock=self._clock)
+            cell = min(e / n for e, n in zip(self.grid.extent, self.grid.shape))
+            self.device.call('ffx_next_dt', ptr(self.projector._scalars[0:3]), ptr(self._clock),
+                             ptr(self._clock_time), cell, float(cfl), float(dt_max), self.device.s)
+        except Exception:
+            self.faulted = True
+            self.projector.ready = False
+            raise
+
+    def current_dt(self):
+        """The dt the next ``step_cfl`` will take (one readback)."""
+        return float(self._clock[0].item())
+
     def step(self, dt=1.0 / 30.0, emission=None, sources=None):
         validate_dt(dt)
         if sources is not None:
@@ -191,7 +250,9 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         if self.pass_timer is not None:
             self.pass_timer.mark(name)
 
-    def _step(self, dt, emission, emitters=None):
+    def _step(self, dt, emission, emitters=None, clock=None):
+        """One step with the time step ``dt``, or, with ``clock``, the device
+        float clock[0] (the ``ffx_*_dt`` forms of the passes)."""
         s = self.settings
         dev = self.device
         gp = C.byref(self._g)
@@ -200,9 +261,14 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         src = self._fill_sources(emission, emitters)
         corrected_v = s.velocity_advection == "MACCORMACK"
         vel = [ptr(f) for f in self._velocity]
+        dtp = ptr(clock[0:1]) if clock is not None else None
+        if clock is None and self._clock_live:
+            # a host step after device steps: fold the device time into the host time
+            self.time = self.time
+            self._clock_live = False
         self._mark('start')
         if corrected_v:
-            self.detail.transport_velocity(self._velocity, dt)
+            self.detail.transport_velocity(self._velocity, dt, dtp)
             pred = [ptr(f) for f in self.detail.face_predictor]
             self._mark('velocity_predictor')
         else:
@@ -211,16 +277,18 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         confine = s.vorticity_strength > 0
         # with confinement the wall condition waits for the projection, as in
         # the reference (confinement reads the provisional, unwalled faces)
-        dev.call('ffx_advect_velocity_trace', gp, sp, self._storage, *vel, *pred, dt, int(corrected_v),
-                 s.velocity_blend, C.byref(src), ptr(self._front), ptr(self._temperature), s.thermal_lift,
-                 s.density_weight, int(not confine), *[ptr(b) for b in proj.bounded],
-                 self.detail.face_traces() if corrected_v else None, st)
+        dev.call('ffx_advect_velocity_dt' if dtp is not None else 'ffx_advect_velocity_trace', gp, sp, self._storage,
+                 *vel, *pred, dtp if dtp is not None else dt, int(corrected_v), s.velocity_blend, C.byref(src),
+                 ptr(self._front), ptr(self._temperature), s.thermal_lift, s.density_weight, int(not confine),
+                 *[ptr(b) for b in proj.bounded], self.detail.face_traces() if corrected_v else None, st)
         self._mark('velocity_transport')
         # The old velocity is consumed: the corrected field is written over it.
         if confine:
             self.detail.confine(proj.bounded, self._velocity, dt, s.vorticity_strength, s.vorticity_limit)
             self._mark('confinement')
             proj.project(self._velocity, self._velocity, dt)
+        elif clock is not None:
+            proj.project_bounded_device(self._velocity, clock)
         else:
             proj.project_bounded(self._velocity, dt)
         self._mark('projection')
@@ -229,7 +297,7 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         if self.combustion is not None:
             fields.append(self.combustion.fuel)
         if corrected_s:
-            preds, revs = self.detail.transport_many(fields, self._velocity, dt)
+            preds, revs = self.detail.transport_many(fields, self._velocity, dt, dtp)
             self._mark('scalar_predictor_reverse')
         else:
             preds = revs = fields
@@ -245,9 +313,9 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             chans.append(N.FfxScalarChannel(ptr(fields[2]), ptr(preds[2]), ptr(revs[2]), ptr(self.combustion.spare),
                                             s.fuel_source_rate, 0.0, -1.0, 2, 0))
         arr = (N.FfxScalarChannel * len(chans))(*chans)
-        dev.call('ffx_advect_scalars_trace', gp, sp, self._storage, *[ptr(f) for f in self._velocity], dt,
-                 int(corrected_s), C.byref(src), len(chans), arr, ptr(self._maxima),
-                 self.detail.cell_traces() if corrected_s else None, st)
+        dev.call('ffx_advect_scalars_dt' if dtp is not None else 'ffx_advect_scalars_trace', gp, sp, self._storage,
+                 *[ptr(f) for f in self._velocity], dtp if dtp is not None else dt, int(corrected_s), C.byref(src),
+                 len(chans), arr, ptr(self._maxima), self.detail.cell_traces() if corrected_s else None, st)
         self._mark('scalar_transport')
         self._front, self._back = self._back, self._front
         self._temperature, self._temperature_back = self._temperature_back, self._temperature
@@ -256,7 +324,8 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             c.fuel, c.spare = c.spare, c.fuel
             c.react(self, dt)
             self._mark('combustion')
-        self.time += dt
+        if clock is None:
+            self.time += dt
         self.steps += 1
 
     def scalar_maxima(self):

@@ -93,8 +93,45 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.learned = None
         self.use_graphs = True
         self.use_tail = True
+        # tolerance solves in V-cycle mode run as one graph with a device-side
+        # WHILE loop (no host round trip per cycle); False keeps the host loop
+        self.use_device_loop = True
+        self._loops = {}
+        # [cycles of the last solve, cycles of all device-loop solves, decisions]
+        self._counters = torch.zeros(3, dtype=torch.int32, device=dev.device)
+        self._host_total = 0
+        self._sweeps_per_cycle = 0
         self._build_hierarchy()
         self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
+
+    # The cycle count of the last solve lives on the device after a device-loop
+    # solve; reading it synchronises once.
+    @property
+    def last_cycles(self):
+        if getattr(self, '_cycles_on_device', False):
+            self._cycles_host = int(self._counters[0].item())
+            self._cycles_on_device = False
+            self._iterations_host = self._cycles_host * self._sweeps_per_cycle
+        return self._cycles_host
+
+    @last_cycles.setter
+    def last_cycles(self, value):
+        self._cycles_on_device = False
+        self._cycles_host = value
+
+    @property
+    def last_iterations(self):
+        if getattr(self, '_cycles_on_device', False):
+            return self.last_cycles * self._sweeps_per_cycle
+        return self._iterations_host
+
+    @last_iterations.setter
+    def last_iterations(self, value):
+        self._iterations_host = value
+
+    def total_cycles(self):
+        """V-cycles (or PCG iterations) of every solve so far (one readback)."""
+        return self._host_total + int(self._counters[1].item())
 
     def _shapes(self):
         """Level shapes the grid allows (halving while all dims are even and >= 8)."""
@@ -136,18 +173,29 @@ class SolidMultigridProjector(SolidPressureProjector):
             graph.coarse_scale = s.mg_coarse_scale
             self.levels.append(dict(shape=coarse_shape, edges=edges, graph=graph, p=dev.texture(coarse_shape),
                                     q=dev.texture(coarse_shape), rhs=dev.texture(coarse_shape)))
+        self.coarse_matrix = None
         self._coarse_solve()
         self._graphs = {}
+        if getattr(self, '_loops', None):
+            torch.cuda.synchronize(dev.device)
+            self._free_loops()
         self._tail, self.tail_start = self._make_tail()
 
     def _coarse_solve(self):
+        """FP64 pseudoinverse of the coarsest level. A matrix of the same size is
+        updated in place, so captured graphs (which hold its address) stay valid."""
         s = self.settings
-        self.coarse_matrix = self.coarse_kernel = None
         last = self.levels[-1]
         if prod(last['shape']) <= DIRECT_LIMIT and s.coarse_solver == 'DIRECT' and len(self.levels) > 1:
-            inv = graph_pseudoinverse(last['shape'], last['edges'].cpu().numpy())
-            self.coarse_matrix = torch.as_tensor(inv, dtype=torch.float64).to(self.device.device)
+            inv = torch.as_tensor(graph_pseudoinverse(last['shape'], last['edges'].cpu().numpy()), dtype=torch.float64)
+            old = getattr(self, 'coarse_matrix', None)
+            if old is not None and old.shape == inv.shape:
+                old.copy_(inv.to(old.device))
+            else:
+                self.coarse_matrix = inv.to(self.device.device)
             self.coarse_kernel = KernelHandle('solid_mg_direct.glsl')
+        else:
+            self.coarse_matrix = self.coarse_kernel = None
 
     def refresh_hierarchy(self):
         """Follow a collider mask that changed in place (moving colliders): the
@@ -395,7 +443,11 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.last_cycles = 0
         if len(self.levels) == 1:
             return super().solve_pressure(dt, previous_dt)
-        if s.learned_warm_start and not (s.solid_warm_start and previous_dt is not None):
+        warm = s.solid_warm_start and previous_dt is not None
+        if warm and s.learned_warm_start and s.learned_correction and self.learned is not None:
+            # learned correction of the warm start: p += N(rhs - L p)
+            self._learned_correction()
+        elif s.learned_warm_start and not warm:
             if self.learned is None:
                 raise ValueError('learned_warm_start needs a model: projector.attach_learned(LearnedWarmStart(...))')
             self.learned.guess(self.before, self.pressure)
@@ -416,6 +468,10 @@ class SolidMultigridProjector(SolidPressureProjector):
             else:
                 self._solve_krylov(scale, budget)
             self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
+            self._host_total += self.last_cycles
+            return
+        if s.pressure_tolerance > 0 and self.use_device_loop and self.use_graphs and self.timer is None:
+            self._device_solve()
             return
         one_cycle = lambda: self._replayed(('vcycle', self.levels[0]['p'].data_ptr()), lambda: self.cycle(0))
         if s.pressure_tolerance <= 0:
@@ -433,12 +489,103 @@ class SolidMultigridProjector(SolidPressureProjector):
                     one_cycle()
                     self.last_cycles += 1
         self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
+        self._host_total += self.last_cycles
+
+    # ------------------------------------------------------ device-side loop
+    def _device_solve(self):
+        """The tolerance solve as one graph launch: max|rhs|, the residual
+        maximum, and WHILE (cycles < max and max|r| > tol * max|rhs|) {V-cycle,
+        residual maximum} decided on the device; the cycle count stays on the
+        device until read."""
+        dev = self.device
+        key = ('loop', self.levels[0]['p'].data_ptr(), self.levels[0]['q'].data_ptr())
+        entry = self._loops.get(key)
+        if entry is None:
+            entry = self._capture_loop()
+            self._loops[key] = entry
+        handle, per_cycle, calls = entry
+        dev.call('ffx_loop_launch', handle, dev.s)
+        dev.calls += calls - 1
+        self._sweeps_per_cycle = per_cycle
+        self._cycles_on_device = True
+        self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
+
+    def _capture_loop(self):
+        """Capture the solve loop (see ``_device_solve``) into a graph; returns
+        (loop handle, sweeps per cycle, native passes per cycle)."""
+        s = self.settings
+        dev = self.device
+        level = self.levels[0]
+        n = self.before.numel()
+        tol = float(s.pressure_tolerance)
+        limit = int(s.pressure_max_cycles)
+        counters = ptr(self._counters)
+        loop = C.c_void_p()
+        # the stream lives on the underlying CudaDevice (a SolidDevice delegates to it)
+        root = dev.__dict__.get('base', dev)
+        side = torch.cuda.Stream(root.device)
+        side.wait_stream(root.stream)
+        saved, saved_iters, saved_calls = root.stream, self._iterations_host, dev.calls
+        p0, q0 = level['p'], level['q']
+        try:
+            root.stream = side
+            with torch.cuda.stream(side):
+                N.check(dev.lib.ffx_loop_begin(dev.s, C.byref(loop)))
+                dev.call('ffx_loop_reset_counter', counters, dev.s)
+                dev.call('ffx_max_abs', n, N.FFX_F32, ptr(self.before), ptr(self._rmax[1:2]), dev.s)
+                dev.call('ffx_zero_if_unscaled', ptr(self._rmax[1:2]), ptr(level['p']), n, dev.s)
+                dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                         ptr(self._rmax[0:1]), dev.s)
+                dev.call('ffx_loop_decide', loop, ptr(self._rmax[0:1]), ptr(self._rmax[1:2]), tol, limit, counters,
+                         dev.s)
+                body = C.c_void_p()
+                N.check(dev.lib.ffx_loop_while(loop, C.byref(body)))
+            inner = torch.cuda.ExternalStream(body.value, device=root.device)
+            root.stream = inner
+            calls0 = dev.calls
+            self._iterations_host = 0
+            with torch.cuda.stream(inner):
+                self.cycle(0)
+                dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                         ptr(self._rmax[0:1]), dev.s)
+                dev.call('ffx_loop_decide', loop, ptr(self._rmax[0:1]), ptr(self._rmax[1:2]), tol, limit, counters,
+                         dev.s)
+            per_cycle, calls = self._iterations_host, dev.calls - calls0
+            if level['p'] is not p0 or level['q'] is not q0:
+                raise RuntimeError('a V-cycle must leave the level-0 buffer roles unchanged')
+            N.check(dev.lib.ffx_loop_end_while(loop))
+            root.stream = side
+            N.check(dev.lib.ffx_loop_end(loop))
+        except Exception:
+            if loop.value:
+                dev.lib.ffx_loop_destroy(loop)
+            raise
+        finally:
+            root.stream = saved
+            self._iterations_host = saved_iters
+            dev.calls = saved_calls
+        return loop, per_cycle, calls
+
+    def _free_loops(self):
+        for handle, _, _ in self._loops.values():
+            self.device.lib.ffx_loop_destroy(handle)
+        self._loops = {}
 
     def gradient_links(self):
         # the link bytes follow the mask (recomputed on every collider move)
         if len(self.levels) > 1 and getattr(self, '_links', None) is not None and self.device.mask is not None:
             return self._links
         return None
+
+    def _learned_correction(self):
+        dev = self.device
+        level = self.levels[0]
+        if getattr(self, '_corr', None) is None:
+            self._corr = (dev.texture(level['shape']), dev.texture(level['shape']))
+        r, e = self._corr
+        dev.call('ffx_graph_residual', C.byref(level['graph']), ptr(self.pressure), ptr(self.before), ptr(r), dev.s)
+        self.learned.guess(r, e)
+        dev.call('ffx_add', self.pressure.numel(), ptr(self.pressure), ptr(e), ptr(self.pressure), dev.s)
 
     def attach_learned(self, model):
         """Pressure guess used when ``learned_warm_start`` is set
@@ -470,6 +617,9 @@ class SolidMultigridProjector(SolidPressureProjector):
             'aggregation': 'connected_children_only'}
 
     def close(self):
+        if getattr(self, '_loops', None):
+            torch.cuda.synchronize(self.device.device)
+            self._free_loops()
         self._graphs = {}
         self._kry = None
         if self.learned is not None:

@@ -129,6 +129,13 @@ __device__ __forceinline__ float sample_closed(const Dev& d, const uint8_t* soli
     return zz0 * gz + zz1 * fz;
 }
 
+// The time step of a pass: the launch parameter, or the value a device-side
+// time-step rule left at dtp (a step that never reads dt back to the host).
+template <class Pm>
+__device__ __forceinline__ float step_dt(const Pm& P) {
+    return P.dtp ? P.dt_sign * __ldg(P.dtp) : P.dt;
+}
+
 // ------------------------------------------------------------ face predictor
 template <typename T>
 struct PredParams {
@@ -137,6 +144,8 @@ struct PredParams {
     const uint8_t* halo;
     Faces<T> F;
     float dt;
+    const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
+    float dt_sign;
     T* out[3];
     float* dep[3];    // optional: departure points per face grid (three planes of nf floats), for reuse
     int nf[3];
@@ -169,7 +178,7 @@ __device__ __forceinline__ void face_predictor_face(const PredParams<T>& P, cons
     const Dev& d = P.d;
     const uint8_t* __restrict__ solid = P.solid;
     const uint8_t* __restrict__ halo = P.halo;
-    const float dt = P.dt;
+    const float dt = step_dt(P);
     T* out = P.out[f.axis];
     if (MASK && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
         Store<T>::st(out, f.i, 0.f);
@@ -211,6 +220,8 @@ struct VelParams {
     Faces<T> F;       // velocity at the start of the step
     Faces<T> P;       // MacCormack predictor
     float dt, blend, lift, weight;
+    const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
+    float dt_sign;
     int corrected, apply_walls;
     const T* density;
     const T* temperature;
@@ -225,7 +236,7 @@ template <typename T, bool MASK, bool P2, class Smp>
 __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, const FaceIdx& f, const Smp& smp) {
     const Dev& d = P.d;
     const int axis = f.axis;
-    const float dt = P.dt;
+    const float dt = step_dt(P);
     bool blocked = MASK && solid_face(d, P.solid, f.x, f.y, f.z, axis);
     float value = 0.f;
     if (!blocked) {
@@ -490,6 +501,8 @@ struct ScalarXport {
     const uint8_t* halo;
     Faces<T> F;
     float dt;
+    const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
+    float dt_sign;
     int count;
     const T* in[3];
     T* out[3];
@@ -514,7 +527,7 @@ __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, i
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
-    F3 dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, P.dt);
+    F3 dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P));
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     const auto S = smp.template closed<MASK>(P.solid, qx, qy, qz);
@@ -555,6 +568,8 @@ struct ScalarFinal {
     const uint8_t* halo;
     Faces<T> F;
     float dt;
+    const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
+    float dt_sign;
     int corrected, count;
     Channel<T> ch[3];
     const T* fields[3];   // ch[c].field, as the sampler's scalar fields
@@ -574,7 +589,7 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
         return;
     }
-    const float dt = P.dt;
+    const float dt = step_dt(P);
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
     // the forward predictor traced this cell's start point with the same
@@ -801,9 +816,9 @@ int ffx_set_transport_tiling(int enable) {
     return previous;
 }
 
-int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                             const void* w, float dt, void* pu, void* pv, void* pw, float* const dep[3],
-                             void* stream) {
+static int face_predictor_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                               const void* w, float dt, const float* dtp, void* pu, void* pv, void* pw,
+                               float* const dep[3], void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && pu && pv && pw,
                 "ffx_face_predictor: invalid arguments");
     FFX_REQUIRE(pu != u && pv != v && pw != w, "ffx_face_predictor: outputs must not alias inputs");
@@ -820,6 +835,8 @@ int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, 
         Q.halo = halo;
         Q.F = F;
         Q.dt = dt;
+        Q.dtp = dtp;
+        Q.dt_sign = 1.f;
         Q.out[0] = (T*)pu; Q.out[1] = (T*)pv; Q.out[2] = (T*)pw;
         for (int a = 0; a < 3; ++a) {
             Q.dep[a] = dep ? dep[a] : nullptr;
@@ -836,16 +853,30 @@ int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, 
     return launch_status("face_predictor_kernel");
 }
 
+int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                             const void* w, float dt, void* pu, void* pv, void* pw, float* const dep[3],
+                             void* stream) {
+    return face_predictor_impl(g, s, storage, u, v, w, dt, nullptr, pu, pv, pw, dep, stream);
+}
+
+int ffx_face_predictor_dt(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                          const void* w, const float* dt, void* pu, void* pv, void* pw, float* const dep[3],
+                          void* stream) {
+    FFX_REQUIRE(dt, "ffx_face_predictor_dt: NULL time step");
+    return face_predictor_impl(g, s, storage, u, v, w, 0.f, dt, pu, pv, pw, dep, stream);
+}
+
 int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                        const void* w, float dt, void* pu, void* pv, void* pw, void* stream) {
     return ffx_face_predictor_trace(g, s, storage, u, v, w, dt, pu, pv, pw, nullptr, stream);
 }
 
-int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                              const void* w, const void* pu, const void* pv, const void* pw, float dt,
-                              int corrected, float blend, const FfxSources* src, const void* density,
-                              const void* temperature, float lift, float weight, int apply_walls, void* ou,
-                              void* ov, void* ow, const float* const dep[3], void* stream) {
+static int advect_velocity_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                                const void* w, const void* pu, const void* pv, const void* pw, float dt,
+                                const float* dtp, int corrected, float blend, const FfxSources* src,
+                                const void* density, const void* temperature, float lift, float weight,
+                                int apply_walls, void* ou, void* ov, void* ow, const float* const dep[3],
+                                void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && ou && ov && ow,
                 "ffx_advect_velocity: invalid arguments");
     FFX_REQUIRE(!corrected || (pu && pv && pw), "ffx_advect_velocity: MacCormack needs the predictor faces");
@@ -867,6 +898,8 @@ int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.P = corrected ? Faces<T>{(const T*)pu, (const T*)pv, (const T*)pw} : P.F;
         P.dt = dt;
+        P.dtp = dtp;
+        P.dt_sign = 1.f;
         P.blend = blend;
         P.lift = lift;
         P.weight = weight;
@@ -892,6 +925,25 @@ int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
         }
     });
     return launch_status("advect_velocity_kernel");
+}
+
+int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                              const void* w, const void* pu, const void* pv, const void* pw, float dt,
+                              int corrected, float blend, const FfxSources* src, const void* density,
+                              const void* temperature, float lift, float weight, int apply_walls, void* ou,
+                              void* ov, void* ow, const float* const dep[3], void* stream) {
+    return advect_velocity_impl(g, s, storage, u, v, w, pu, pv, pw, dt, nullptr, corrected, blend, src, density,
+                                temperature, lift, weight, apply_walls, ou, ov, ow, dep, stream);
+}
+
+int ffx_advect_velocity_dt(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                           const void* w, const void* pu, const void* pv, const void* pw, const float* dt,
+                           int corrected, float blend, const FfxSources* src, const void* density,
+                           const void* temperature, float lift, float weight, int apply_walls, void* ou,
+                           void* ov, void* ow, const float* const dep[3], void* stream) {
+    FFX_REQUIRE(dt, "ffx_advect_velocity_dt: NULL time step");
+    return advect_velocity_impl(g, s, storage, u, v, w, pu, pv, pw, 0.f, dt, corrected, blend, src, density,
+                                temperature, lift, weight, apply_walls, ou, ov, ow, dep, stream);
 }
 
 int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
@@ -927,9 +979,9 @@ int ffx_buoyancy(const FfxGrid* g, int storage, const void* w_in, const void* de
     return launch_status("buoyancy_kernel");
 }
 
-int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                               const void* w, float dt, int count, const void* const* in, void* const* out,
-                               float* dep, void* stream) {
+static int scalar_transport_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                                 const void* w, float dt, const float* dtp, float sign, int count,
+                                 const void* const* in, void* const* out, float* dep, void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 && in &&
                 out, "ffx_scalar_transport: invalid arguments");
     for (int c = 0; c < count; ++c)
@@ -944,6 +996,8 @@ int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage
         P.halo = has_mask(s) ? s->halo : nullptr;
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.dt = dt;
+        P.dtp = dtp;
+        P.dt_sign = sign;
         P.count = count;
         for (int c = 0; c < 3; ++c) {
             P.in[c] = c < count ? (const T*)in[c] : nullptr;
@@ -962,14 +1016,28 @@ int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage
     return launch_status("scalar_transport_kernel");
 }
 
+int ffx_scalar_transport_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                               const void* w, float dt, int count, const void* const* in, void* const* out,
+                               float* dep, void* stream) {
+    return scalar_transport_impl(g, s, storage, u, v, w, dt, nullptr, 1.f, count, in, out, dep, stream);
+}
+
+int ffx_scalar_transport_dt(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                            const void* w, const float* dt, float sign, int count, const void* const* in,
+                            void* const* out, float* dep, void* stream) {
+    FFX_REQUIRE(dt && (sign == 1.f || sign == -1.f), "ffx_scalar_transport_dt: NULL time step or sign not +-1");
+    return scalar_transport_impl(g, s, storage, u, v, w, 0.f, dt, sign, count, in, out, dep, stream);
+}
+
 int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                          const void* w, float dt, int count, const void* const* in, void* const* out, void* stream) {
     return ffx_scalar_transport_trace(g, s, storage, u, v, w, dt, count, in, out, nullptr, stream);
 }
 
-int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
-                             const void* w, float dt, int corrected, const FfxSources* src, int count,
-                             const FfxScalarChannel* channels, float* maxima, const float* dep, void* stream) {
+static int advect_scalars_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                               const void* w, float dt, const float* dtp, int corrected, const FfxSources* src,
+                               int count, const FfxScalarChannel* channels, float* maxima, const float* dep,
+                               void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 &&
                 channels && src && src->count <= 8, "ffx_advect_scalars: invalid arguments");
     for (int c = 0; c < count; ++c) {
@@ -991,6 +1059,8 @@ int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage, 
         P.halo = has_mask(s) ? s->halo : nullptr;
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.dt = dt;
+        P.dtp = dtp;
+        P.dt_sign = 1.f;
         P.corrected = corrected;
         P.count = count;
         for (int c = 0; c < 3; ++c) {
@@ -1024,6 +1094,21 @@ int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage, 
         }
     });
     return launch_status("advect_scalars_kernel");
+}
+
+int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                             const void* w, float dt, int corrected, const FfxSources* src, int count,
+                             const FfxScalarChannel* channels, float* maxima, const float* dep, void* stream) {
+    return advect_scalars_impl(g, s, storage, u, v, w, dt, nullptr, corrected, src, count, channels, maxima, dep,
+                               stream);
+}
+
+int ffx_advect_scalars_dt(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                          const void* w, const float* dt, int corrected, const FfxSources* src, int count,
+                          const FfxScalarChannel* channels, float* maxima, const float* dep, void* stream) {
+    FFX_REQUIRE(dt, "ffx_advect_scalars_dt: NULL time step");
+    return advect_scalars_impl(g, s, storage, u, v, w, 0.f, dt, corrected, src, count, channels, maxima, dep,
+                               stream);
 }
 
 int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,

@@ -52,6 +52,34 @@ __global__ void zero_if_unscaled_kernel(const float* scale, float* p, int64_t n)
         p[i] = 0.f;
 }
 
+// Device-side time-step rule (the adaptive step of backend/timestep.py:35-53 in
+// the form the workloads use): clock = {dt, previous dt}, time in FP64.
+// previous dt = dt; time += dt; dt = min(dt_max, cfl * cell / max|u|) in FP64
+// from the face maxima of the step's corrected velocity (dt_max when they are
+// all zero; a non-finite velocity has a huge finite maximum, so dt stays > 0).
+__global__ void next_dt_kernel(const float* maxima, float* clock, double* time, double cell, double cfl,
+                               double dt_max) {
+    const float dt = clock[0];
+    time[0] += (double)dt;
+    clock[1] = dt;
+    const float umax = fmaxf(fmaxf(maxima[0], maxima[1]), maxima[2]);
+    const double r = cfl * cell / (double)umax;
+    clock[0] = (float)(umax > 0.f ? (r < dt_max ? r : dt_max) : dt_max);
+}
+
+// p *= dt / previous dt when they differ by more than 1e-6 relative (the
+// impulse warm start of backend/pressure.py:63-75), decided in FP64 on the
+// device; no previous step (previous dt <= 0) leaves p unchanged.
+__global__ void scale_by_ratio_kernel(int64_t n, float* p, const float* clock) {
+    const float dt = clock[0], prev = clock[1];
+    if (!(prev > 0.f)) return;
+    const double ratio = (double)dt / (double)prev;
+    if (!(fabs(ratio - 1.0) > 1e-6)) return;
+    const float f = (float)ratio;
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        p[i] = p[i] * f;
+}
+
 }  // namespace
 }  // namespace ffx
 
@@ -104,6 +132,21 @@ int ffx_zero_if_unscaled(const float* scale, float* p, int64_t count, void* stre
     const int64_t want = (count + 255) / 256;
     zero_if_unscaled_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(scale, p, count);
     return launch_status("zero_if_unscaled_kernel");
+}
+
+int ffx_next_dt(const float* maxima, float* clock, double* time, double cell, double cfl, double dt_max,
+                void* stream) {
+    FFX_REQUIRE(maxima && clock && time && cell > 0.0 && cfl > 0.0 && dt_max > 0.0 && dt_max <= 0.1,
+                "ffx_next_dt: invalid arguments (cell, cfl > 0; dt_max in (0, 0.1])");
+    next_dt_kernel<<<1, 1, 0, as_stream(stream)>>>(maxima, clock, time, cell, cfl, dt_max);
+    return launch_status("next_dt_kernel");
+}
+
+int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream) {
+    FFX_REQUIRE(count >= 1 && p && clock, "ffx_scale_by_ratio: invalid arguments");
+    const int64_t want = (count + 255) / 256;
+    scale_by_ratio_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(count, p, clock);
+    return launch_status("scale_by_ratio_kernel");
 }
 
 int ffx_loop_while(FfxLoop* L, void** body_stream) {

@@ -238,6 +238,11 @@ __global__ void scale_kernel(int64_t n, const float* in, float f, float* out) {
     if (i < n) out[i] = in[i] * f;
 }
 
+__global__ void add_kernel(int64_t n, const float* a, const float* b, float* out) {
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+        out[i] = a[i] + b[i];
+}
+
 // ---------------------------------------------------- geometric multigrid
 // Laplacian term of mg_residual.glsl at cell (x, y, z), index i.
 __device__ __forceinline__ float neumann_lap(const Lvl& L, const float* __restrict__ p, int i, int x, int y, int z) {
@@ -1056,6 +1061,13 @@ int ffx_scale(int64_t count, const float* in, float factor, float* out, void* st
     if (count == 0) return FFX_OK;
     scale_kernel<<<blocks_for(count, 256), 256, 0, as_stream(stream)>>>(count, in, factor, out);
     return launch_status("scale_kernel");
+}
+
+int ffx_add(int64_t count, const float* a, const float* b, float* out, void* stream) {
+    FFX_REQUIRE(count >= 1 && a && b && out, "ffx_add: invalid arguments");
+    const int64_t want = (count + 255) / 256;
+    add_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(count, a, b, out);
+    return launch_status("add_kernel");
 }
 
 int ffx_mg_residual(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt, float* r,

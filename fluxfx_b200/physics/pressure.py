@@ -19,6 +19,10 @@ Extensions (all default to the reference's behaviour):
   (arithmetic is FP32 either way).
 * ``solid_warm_start`` -- reuse the previous step's pressure with colliders
   instead of the reference's cold start.
+* ``learned_correction`` -- with ``learned_warm_start`` and
+  ``solid_warm_start``: on warm starts, add the network's answer for the
+  residual of the previous pressure to it (a learned correction) instead of
+  using the previous pressure alone.
 * ``pressure_method`` -- "VCYCLE" (reference: stand-alone V-cycles) or "PCG"
   (conjugate gradients preconditioned by the same symmetric aggregation
   V-cycle; collider multigrid only). Both solve the same system to the same
@@ -102,6 +106,7 @@ class PressureSettings(ThermalSettings):
     pressure_method: str = "VCYCLE"
     learned_warm_start: bool = False
     mg_coarse_scale: float = 1.0
+    learned_correction: bool = False
 
     def __post_init__(self):
         super().__post_init__()
@@ -140,6 +145,8 @@ class PressureSettings(ThermalSettings):
             raise ValueError("Velocity blend must lie in [0, 1]")
         if type(self.solid_warm_start) is not bool:
             raise ValueError("Collider warm start must be boolean")
+        if type(self.learned_correction) is not bool:
+            raise ValueError("Learned correction must be boolean")
         if type(self.learned_warm_start) is not bool:
             raise ValueError("Learned warm start must be boolean")
         if not isfinite(self.mg_coarse_scale) or not 0 < self.mg_coarse_scale < 2:

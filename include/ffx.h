@@ -200,6 +200,28 @@ int ffx_advect_scalars_trace(const FfxGrid* g, const FfxSolids* s, int storage,
                              const void* u, const void* v, const void* w, float dt, int corrected,
                              const FfxSources* src, int count, const FfxScalarChannel* channels,
                              float* maxima, const float* dep, void* stream);
+/* The four transport passes above with the time step read on the device: `dt`
+ * points at a float (the solver's clock, ffx_next_dt) that the kernels read,
+ * times `sign` (+1 or -1: the reverse scalar pass) for ffx_scalar_transport_dt,
+ * so a step whose dt the device chose needs no host readback. Results equal the
+ * host-dt forms given the same dt value. */
+int ffx_face_predictor_dt(const FfxGrid* g, const FfxSolids* s, int storage,
+                          const void* u, const void* v, const void* w, const float* dt,
+                          void* pu, void* pv, void* pw, float* const dep[3], void* stream);
+int ffx_advect_velocity_dt(const FfxGrid* g, const FfxSolids* s, int storage,
+                           const void* u, const void* v, const void* w,
+                           const void* pu, const void* pv, const void* pw, const float* dt,
+                           int corrected, float blend, const FfxSources* src,
+                           const void* density, const void* temperature, float lift, float weight,
+                           int apply_walls, void* ou, void* ov, void* ow, const float* const dep[3],
+                           void* stream);
+int ffx_scalar_transport_dt(const FfxGrid* g, const FfxSolids* s, int storage,
+                            const void* u, const void* v, const void* w, const float* dt, float sign,
+                            int count, const void* const* in, void* const* out, float* dep, void* stream);
+int ffx_advect_scalars_dt(const FfxGrid* g, const FfxSolids* s, int storage,
+                          const void* u, const void* v, const void* w, const float* dt, int corrected,
+                          const FfxSources* src, int count, const FfxScalarChannel* channels,
+                          float* maxima, const float* dep, void* stream);
 /* P0.2 open-boundary transport in an analytic flow; replaces shaders/advect.glsl. */
 int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt,
                     const float base[3], float angular, const float center[3], float radius,
@@ -243,6 +265,8 @@ int ffx_jacobi(const int32_t n[3], const float inv[3], const uint8_t* solid,
                void* stream);
 /* out[i] = in[i] * factor; replaces shaders/pressure_scale.glsl. */
 int ffx_scale(int64_t count, const float* in, float factor, float* out, void* stream);
+/* out = a + b elementwise (FP32; out may alias a or b). */
+int ffx_add(int64_t count, const float* a, const float* b, float* out, void* stream);
 
 /* ------------------------------------------------- geometric multigrid (MG) */
 /* r = rhs/dt - L p; replaces shaders/mg_residual.glsl. */
@@ -433,6 +457,16 @@ int ffx_loop_end_while(FfxLoop* loop);
 int ffx_loop_end(FfxLoop* loop);
 int ffx_loop_launch(FfxLoop* loop, void* stream);
 int ffx_loop_destroy(FfxLoop* loop);
+/* Device-side time-step rule (backend/timestep.py:35-53 in the workloads' form):
+ * clock = float[2] {dt, previous dt}, time = one double. Sets previous dt = dt,
+ * time += dt, and dt = min(dt_max, cfl * cell / max(maxima[0..2])) in FP64
+ * (dt_max when the maxima are zero); cell, cfl > 0, dt_max in (0, 0.1]. */
+int ffx_next_dt(const float* maxima, float* clock, double* time, double cell, double cfl,
+                double dt_max, void* stream);
+/* p *= clock[0] / clock[1] when clock[1] > 0 and the ratio differs from 1 by more
+ * than 1e-6 (FP64): the impulse warm start's rescaling (backend/pressure.py:63-75)
+ * with the time steps on the device. */
+int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream);
 
 /* ------------------------------------------------------------- bake readback */
 /* Storage code of a uint8 field (the collider mask) for ffx_pack_channels. */

@@ -397,7 +397,8 @@ def test_graph_replay_matches_eager_launches(D, method):
         assert graphed.last_iterations == eager.last_iterations
         for a in range(3):
             assert np.array_equal(n(out_g[a]), n(out_e[a])), a
-    assert graphed._graphs and not eager._graphs
+    # V-cycle tolerance solves replay one device-loop graph; PCG iterations replay captured iterations
+    assert (graphed._graphs or graphed._loops) and not eager._graphs and not eager._loops
     graphed.close()
     eager.close()
 
