@@ -131,7 +131,15 @@ class PressureProjector:
 
     def _gradient(self, outputs, solve_dt):
         links = self.gradient_links()
-        if links is not None:
+        if self._field_dtype == torch.bfloat16:
+            # BF16 storage: also the divergence of the FP32 result before rounding
+            if getattr(self, 'after_fp32', None) is None:
+                self.after_fp32 = self.device.texture(self.grid.shape)
+            self.device.call('ffx_gradient_ex', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
+                             ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),
+                             ptr(self._scalars[0:3]), ptr(links) if links is not None else None,
+                             ptr(self.after_fp32), self.device.s)
+        elif links is not None:
             self.device.call('ffx_gradient_links', self._gp, self._sp, self._storage, *[ptr(b) for b in self.bounded],
                              ptr(self.pressure), solve_dt, *[ptr(o) for o in outputs], ptr(self.after),
                              ptr(self._scalars[0:3]), ptr(links), self.device.s)
@@ -190,9 +198,16 @@ class PressureProjector:
         b2, a2, mb, ma, sb, sa, count, _ = out.cpu().tolist()
         rms_b, rms_a = (b2 / count) ** 0.5, (a2 / count) ** 0.5
         ratio = rms_a / rms_b if rms_b > 0 else (0.0 if rms_a == 0 else None)
-        return {"rms_before": rms_b, "rms_after": rms_a, "ratio": ratio, "max_before": mb, "max_after": ma,
-                "mean_before": sb / count, "mean_after": sa / count,
-                "rel_div_inf": (ma / mb) if mb > 0 else 0.0}
+        out = {"rms_before": rms_b, "rms_after": rms_a, "ratio": ratio, "max_before": mb, "max_after": ma,
+               "mean_before": sb / count, "mean_after": sa / count,
+               "rel_div_inf": (ma / mb) if mb > 0 else 0.0}
+        exact = getattr(self, 'after_fp32', None)
+        if exact is not None:
+            # BF16 storage: rel_div_inf is of the stored (rounded) faces; this one is
+            # of the projection's FP32 result before rounding, the solve's own measure
+            ma32 = float(exact.abs().max())
+            out.update(max_after_fp32=ma32, rel_div_inf_fp32=(ma32 / mb) if mb > 0 else 0.0)
+        return out
 
     def metrics(self):
         """Explicit synchronous readback; never invoked by the step itself."""

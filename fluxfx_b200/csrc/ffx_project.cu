@@ -111,6 +111,7 @@ struct GradDesc {
     T* out[3];
     float* div;
     const uint8_t* links;   // optional level-0 link bytes of the same mask (ffx_graph_links), MASK only
+    float* div_exact;       // optional: divergence of the corrected faces before rounding to storage
 };
 
 template <typename T, bool MASK>
@@ -156,12 +157,14 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
         float p_xm = x > 0 ? __ldg(p + i - 1) : 0.f, p_xp = x + 1 < d.nx ? __ldg(p + i + 1) : 0.f;
         float p_ym = y > 0 ? __ldg(p + i - sy) : 0.f, p_yp = y + 1 < d.ny ? __ldg(p + i + sy) : 0.f;
         float p_zm = z > 0 ? __ldg(p + i - sz) : 0.f, p_zp = z + 1 < d.nz ? __ldg(p + i + sz) : 0.f;
-        float ul = rt<T>(face_out(F.u, iu, x, d.nx + 1, x, y, z, 0, pc, p_xm, 1u));
-        float vl = rt<T>(face_out(F.v, iv, y, d.ny + 1, x, y, z, 1, pc, p_ym, 4u));
-        float wl = rt<T>(face_out(F.w, iw, z, d.nz + 1, x, y, z, 2, pc, p_zm, 16u));
-        float uu = rt<T>(face_out(F.u, iu + 1, x + 1, d.nx + 1, x + 1, y, z, 0, p_xp, pc, 2u));
-        float vu = rt<T>(face_out(F.v, iv + d.nx, y + 1, d.ny + 1, x, y + 1, z, 1, p_yp, pc, 8u));
-        float wu = rt<T>(face_out(F.w, iw + sz, z + 1, d.nz + 1, x, y, z + 1, 2, p_zp, pc, 32u));
+        const float ul0 = face_out(F.u, iu, x, d.nx + 1, x, y, z, 0, pc, p_xm, 1u);
+        const float vl0 = face_out(F.v, iv, y, d.ny + 1, x, y, z, 1, pc, p_ym, 4u);
+        const float wl0 = face_out(F.w, iw, z, d.nz + 1, x, y, z, 2, pc, p_zm, 16u);
+        const float uu0 = face_out(F.u, iu + 1, x + 1, d.nx + 1, x + 1, y, z, 0, p_xp, pc, 2u);
+        const float vu0 = face_out(F.v, iv + d.nx, y + 1, d.ny + 1, x, y + 1, z, 1, p_yp, pc, 8u);
+        const float wu0 = face_out(F.w, iw + sz, z + 1, d.nz + 1, x, y, z + 1, 2, p_zp, pc, 32u);
+        float ul = rt<T>(ul0), vl = rt<T>(vl0), wl = rt<T>(wl0);
+        float uu = rt<T>(uu0), vu = rt<T>(vu0), wu = rt<T>(wu0);
         Store<T>::st(ou, iu, ul);
         Store<T>::st(ov, iv, vl);
         Store<T>::st(ow, iw, wl);
@@ -173,6 +176,12 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
             float dv = (uu - ul) * d.inv[0] + (vu - vl) * d.inv[1] + (wu - wl) * d.inv[2];
             if (MASK && (P.links ? (lk & 64u) == 0u : __ldg(solid + i) != 0)) dv = 0.f;
             div[i] = dv;
+        }
+        if (P.div_exact) {
+            // the projection's own result, before the storage rounding (BF16 storage rounds the faces)
+            float dv = (uu0 - ul0) * d.inv[0] + (vu0 - vl0) * d.inv[1] + (wu0 - wl0) * d.inv[2];
+            if (MASK && (P.links ? (lk & 64u) == 0u : __ldg(solid + i) != 0)) dv = 0.f;
+            P.div_exact[i] = dv;
         }
     }
     if (maxima) {
@@ -187,8 +196,9 @@ template <typename T, bool MASK>
 __global__ void __launch_bounds__(256) gradient_kernel(Dev d, const uint8_t* __restrict__ solid, Walls W,
                                                       Faces<T> F, const float* __restrict__ p, float dt, T* ou,
                                                       T* ov, T* ow, float* div, float* maxima,
-                                                      const uint8_t* __restrict__ links) {
-    gradient_body<T, MASK>(GradDesc<T>{d, solid, W, F, p, dt, {ou, ov, ow}, div, links}, hw_blk(), maxima);
+                                                      const uint8_t* __restrict__ links, float* div_exact) {
+    gradient_body<T, MASK>(GradDesc<T>{d, solid, W, F, p, dt, {ou, ov, ow}, div, links, div_exact}, hw_blk(),
+                           maxima);
 }
 
 // ---------------------------------------------------------------- Jacobi
@@ -1011,7 +1021,8 @@ int ffx_walls_divergence(const FfxGrid* g, const FfxSolids* s, int storage, cons
 
 static int gradient_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                          const void* w, const float* pressure, float dt, void* ou, void* ov, void* ow,
-                         float* div_after, float* maxima, const uint8_t* links, void* stream) {
+                         float* div_after, float* maxima, const uint8_t* links, float* div_exact,
+                         void* stream) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && pressure && ou && ov && ow,
                 "ffx_gradient: invalid arguments");
     FFX_REQUIRE(ou != u && ov != v && ow != w, "ffx_gradient: outputs must not alias inputs");
@@ -1025,9 +1036,10 @@ static int gradient_impl(const FfxGrid* g, const FfxSolids* s, int storage, cons
     FFX_DISPATCH_STORAGE(storage, T, {
         Faces<T> F = {(const T*)u, (const T*)v, (const T*)w};
         if (has_mask(s)) gradient_kernel<T, true><<<grid, block, 0, st>>>(d, s->solid, make_walls(s), F, pressure, dt, (T*)ou,
-                                                                          (T*)ov, (T*)ow, div_after, maxima, links);
+                                                                          (T*)ov, (T*)ow, div_after, maxima, links,
+                                                                          div_exact);
         else gradient_kernel<T, false><<<grid, block, 0, st>>>(d, nullptr, Walls{}, F, pressure, dt, (T*)ou, (T*)ov, (T*)ow,
-                                                               div_after, maxima, nullptr);
+                                                               div_after, maxima, nullptr, div_exact);
     });
     return launch_status("gradient_kernel");
 }
@@ -1035,13 +1047,22 @@ static int gradient_impl(const FfxGrid* g, const FfxSolids* s, int storage, cons
 int ffx_gradient(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
                  const float* pressure, float dt, void* ou, void* ov, void* ow, float* div_after, float* maxima,
                  void* stream) {
-    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, nullptr, stream);
+    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, nullptr, nullptr,
+                         stream);
 }
 
 int ffx_gradient_links(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                        const void* w, const float* pressure, float dt, void* ou, void* ov, void* ow,
                        float* div_after, float* maxima, const uint8_t* links, void* stream) {
-    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, links, stream);
+    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, links, nullptr,
+                         stream);
+}
+
+int ffx_gradient_ex(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v, const void* w,
+                    const float* pressure, float dt, void* ou, void* ov, void* ow, float* div_after, float* maxima,
+                    const uint8_t* links, float* div_unrounded, void* stream) {
+    return gradient_impl(g, s, storage, u, v, w, pressure, dt, ou, ov, ow, div_after, maxima, links, div_unrounded,
+                         stream);
 }
 
 int ffx_jacobi(const int32_t n[3], const float inv[3], const uint8_t* solid, const float* p_in, const float* rhs,

@@ -257,6 +257,14 @@ int ffx_gradient_links(const FfxGrid* g, const FfxSolids* s, int storage,
                        const void* u, const void* v, const void* w, const float* pressure, float dt,
                        void* ou, void* ov, void* ow, float* div_after, float* maxima,
                        const uint8_t* links, void* stream);
+/* Either of the two (links may be NULL), also writing to div_unrounded (may be
+ * NULL) the divergence of the corrected faces before they are rounded to the
+ * storage type: with BF16 storage the projection's FP32 result, which meets the
+ * solve tolerance where the stored faces cannot (a BF16 face holds ~3 digits). */
+int ffx_gradient_ex(const FfxGrid* g, const FfxSolids* s, int storage,
+                    const void* u, const void* v, const void* w, const float* pressure, float dt,
+                    void* ou, void* ov, void* ow, float* div_after, float* maxima,
+                    const uint8_t* links, float* div_unrounded, void* stream);
 /* One weighted-Jacobi sweep of the (masked) Neumann Laplacian on a level of
  * shape n[3] with 1/h = inv[3]; solid may be NULL. Replaces
  * shaders/pressure_jacobi.glsl. p_out must not alias p_in. */
