@@ -70,19 +70,31 @@ VARIANTS = {
                          learned_correction=True, mg_coarse_scale=1.9),
 }
 
-# Algorithmic bytes per cell of each pass (inputs read once, outputs written
-# once; s = bytes per stored velocity/scalar value, masks 1 B each).
-def pass_bytes(s, face_trace=True):
-    """Per cell; the departure points the predictor passes store and the
-    correction passes read are 3 FP32 values per face (3 faces per cell, on
-    power-of-two grids) and per cell."""
-    ft = 36 if face_trace else 0
+# Algorithmic bytes per cell of each pass: the compulsory traffic of the
+# passes as the scope table states it (inputs read once, outputs written once,
+# face grids as 3 values per cell, one mask byte; s = bytes per stored
+# velocity/scalar value): A1 predictor 6s + m, A2 velocity correction 9s + 2s
+# + m (velocity, predictor and output faces, density and temperature), S1
+# scalar predictor (+ reverse, per pass) 3s + 4s + m, S2 scalar correction
+# 3s + 6s + m. The departure points that this design stores in the predictor
+# passes and reads in the correction passes (3 FP32 values per face and per
+# cell) are extra traffic of the design, reported separately.
+def pass_bytes(s):
+    m = 1
     return {
-        'velocity_predictor': 3 * s + 2 + 3 * s + ft,             # U,V,W + solid,halo -> 3 predictor faces (+trace)
-        'velocity_transport': 3 * s + 3 * s + 2 * s + 2 + 3 * s + ft,  # U,V,W, predictors, rho,T, masks (+trace) -> faces
-        'scalar_predictor_reverse': 2 * (3 * s + 2 * s + 2 + 2 * s) + 12,
-        'scalar_transport': 3 * s + 6 * s + 2 + 2 * s + 12,       # U,V,W, 3 fields x 2 scalars, masks, trace -> 2
+        'velocity_predictor': 6 * s + m,
+        'velocity_transport': 9 * s + 2 * s + m,
+        'scalar_predictor_reverse': 2 * (3 * s + 4 * s + m),
+        'scalar_transport': 3 * s + 6 * s + m,
     }
+
+
+def trace_bytes(face_trace=True):
+    """Per cell, the departure points written by the predictors and read by the
+    corrections (faces only where both passes form the same start points)."""
+    ft = 36 if face_trace else 0
+    return {'velocity_predictor': ft, 'velocity_transport': ft, 'scalar_predictor_reverse': 12,
+            'scalar_transport': 12}
 
 
 def peaks():
@@ -227,6 +239,11 @@ class Run:
                 overrides['mg_coarse_scale'] = args.coarse_scale
             overrides.update(parse_settings(args.set))
         self.solver, self.emitters = build_solver(args.size, storage, args.seed + rank, device, **overrides)
+        if args.host_loop:
+            # the V-cycle loop on the host (one residual readback per cycle): the same
+            # kernels, launched from replayed graphs -- for profilers that do not list
+            # the kernels inside a conditional graph node
+            self.solver.projector.use_device_loop = False
         self.h = 1.0 / args.size
         self.dt = 0.02
 
@@ -378,13 +395,14 @@ def run_b200(args):
         hbm, peak_kind = peaks()
         s = 4 if args.storage == 'FP32' else 2
         ft = N.grid_pow2((n, n, n), (1.0, 1.0, 1.0))
-        pb = pass_bytes(s, ft)
+        pb, tb = pass_bytes(s), trace_bytes(ft)
         pass_report = {}
         for name, ms in passes.items():
             per_step = ms / args.steps
             entry = {"ms_per_step": per_step}
             if name in pb:
                 entry["algorithmic_bytes_per_cell"] = pb[name]
+                entry["design_trace_bytes_per_cell"] = tb[name]
                 entry["achieved_GBps"] = pb[name] * cells / (per_step / 1e3) / 1e9
                 entry["frac_of_peak"] = entry["achieved_GBps"] / hbm
             pass_report[name] = entry
@@ -402,7 +420,8 @@ def run_b200(args):
                                    f"{args.storage} storage",
                        "cells": cells, "l2": "inputs larger than L2 (no flush)",
                        "parallelism": f"replicas x{world}",
-                       "v_cycles_mean": head['cycles'], "host_syncs_per_step": 0,
+                       "v_cycles_mean": head['cycles'],
+                       "host_syncs_per_step": "one per V-cycle (--host-loop)" if args.host_loop else 0,
                        "graph_captures_in_timed_steps": head['captures'],
                        "final_rel_div_inf": rel_div,
                        "final_rel_div_inf_fp32": rel_div32,
@@ -453,29 +472,32 @@ def run_b200(args):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one advect_velocity_kernel
-# launch (reading the stored departure points), from an ncu capture of this
-# bench's scene (fast variant, FP32).
-MEASURED_TRAFFIC = {(256, 4): 1.835e9}
+# launch (reading the stored departure points), from ncu captures of this
+# bench's scene: FP32 storage (fast variant) and BF16 storage (learned).
+MEASURED_TRAFFIC = {(256, 4): 1.835e9, (256, 2): 1.169733888e9 + 0.099842816e9}
 
 
 def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True):
     """The dominant kernel of the step, advect_velocity_kernel (one launch per
     step; its time comes from the events bracketing that launch in the timed
-    steps): algorithmic bytes per launch / launch time against the measured
-    copy bandwidth. The kernel is bound by instruction issue, not by HBM
-    (about 2000 instructions per face: three trilinear velocity samples per
-    trace, two traces, trace clipping), hence the low fraction."""
+    steps): algorithmic bytes per launch (the scope table's 9s + 2s + m per
+    cell) / launch time against the measured copy bandwidth. The kernel is
+    bound by instruction issue, not by HBM (about 1250 instructions per face in
+    the reference's FP32 evaluation order: three trilinear velocity samples for
+    the forward trace, the predictor sample, the 8-corner clamp, the collider
+    tests, emitters, buoyancy and walls), hence the low fraction."""
     ms = passes.get('velocity_transport', 0.0) / steps
-    per_cell = pass_bytes(s, face_trace)['velocity_transport']
+    per_cell = pass_bytes(s)['velocity_transport']
     achieved = per_cell * cells / (ms / 1e3) / 1e9 if ms else None
     return {"bound": "hbm", "kernel": "advect_velocity_kernel (MacCormack velocity transport + emission + "
                                       "buoyancy + walls, one launch per step)",
             "achieved": achieved, "peak": hbm, "peak_kind": f"{peak_kind} (MEASURED_PEAKS hbm_gbs)", "unit": "GB/s",
             "frac": (achieved / hbm) if achieved else None,
             "traffic": MEASURED_TRAFFIC.get((round(cells ** (1 / 3)), s)),
-            "traffic_source": "ncu dram read+write of one launch (same scene), not measured in this run",
-            "algorithmic_bytes_per_launch": per_cell * cells, "avg_launch_ms": ms,
-            "limiter": "instruction issue",
+            "traffic_source": "ncu dram read+write of one launch (same scene and storage), not measured in this run",
+            "algorithmic_bytes_per_launch": per_cell * cells,
+            "design_trace_bytes_per_launch": trace_bytes(face_trace)['velocity_transport'] * cells,
+            "avg_launch_ms": ms, "limiter": "instruction issue",
             "timing": "CUDA events bracketing the launch in every timed step"}
 
 
@@ -666,25 +688,29 @@ def fire_scene(storage, seed, fast):
 
 
 def run_fire(args):
-    """Four fire domains stepped in turn on one GPU (the batched plan covers the
-    static-collider step only), fast form against the plain FP32 multigrid form
-    on the same dt sequence; error of the fast fields against the plain ones."""
+    """Four fire domains on one GPU, each on its own CUDA stream so their
+    passes overlap (the batched plan covers the static-collider step only),
+    fast form against the plain FP32 multigrid form on the same dt sequence;
+    error of the fast fields against the plain ones."""
     import torch
     from fluxfx_b200.backend.device import CudaDevice
     from fluxfx_b200.backend.projected import DenseProjectedSmoke
     from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
     from fluxfx_b200.learned import attach
-    device = CudaDevice()
     domains, steps = 4, args.steps
+    devices = [CudaDevice(stream=torch.cuda.Stream()) for _ in range(domains)]
+    main = torch.cuda.current_stream()
     h = 1.0 / 192
 
     def build(fast):
         out = []
         for d in range(domains):
             grid, settings, pose, noise = fire_scene(args.storage, args.seed + d, fast)
-            s = DenseProjectedSmoke(grid, settings, device, projector_class=SolidMultigridProjector, colliders=pose(0))
+            s = DenseProjectedSmoke(grid, settings, devices[d], projector_class=SolidMultigridProjector,
+                                    colliders=pose(0))
             if fast:
                 attach(s, pose(0))
+                s.projector.defer_refresh_check = True
             s.upload(torch.zeros(grid.cells))
             s.upload_temperature(torch.zeros(grid.cells))
             s.upload_velocity([torch.as_tensor(v) for v in noise])
@@ -693,23 +719,29 @@ def run_fire(args):
 
     def run(solvers, dts=None):
         record = []
-        cycles = 0
-        stream = device.stream
+        totals = [s.projector.total_cycles() for s, _ in solvers]
         torch.cuda.synchronize()
         a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        a.record(stream)
+        a.record(main)
+        for dev in devices:
+            dev.stream.wait_event(a)
         for k in range(steps):
             row = []
             for d, (s, pose) in enumerate(solvers):
                 dt = dts[k][d] if dts else (record[-1][d] if record else 0.02)
                 s.move_colliders(pose(k + 1), dt)
                 s.step(dt)
-                cycles += s.projector.last_cycles
-                umax = max(s.projector.velocity_maxima())
-                row.append(min(0.02, 0.5 * h / umax) if umax > 0 else 0.02)
+                if dts is None:
+                    # the plain run chooses the time steps (one readback); the fast
+                    # runs replay them and read nothing back
+                    umax = max(s.projector.velocity_maxima())
+                    row.append(min(0.02, 0.5 * h / umax) if umax > 0 else 0.02)
             record.append(row)
-        b.record(stream)
+        for dev in devices:
+            main.wait_stream(dev.stream)
+        b.record(main)
         torch.cuda.synchronize()
+        cycles = sum(s.projector.total_cycles() - t for (s, _), t in zip(solvers, totals))
         used = [[0.02] * domains] + record[:-1] if dts is None else dts
         return a.elapsed_time(b) / 1e3, cycles / (steps * domains), used
 
@@ -804,6 +836,8 @@ def main():
     ap.add_argument('--size', type=int, default=256)
     ap.add_argument('--storage', default='BF16', choices=('FP32', 'BF16'),
                     help='field storage of the headline variant (default BF16: the mixed-precision form)')
+    ap.add_argument('--host-loop', action='store_true',
+                    help='run the V-cycle loop on the host (for kernel-listing profilers)')
     ap.add_argument('--no-compare-storage', dest='compare_storage', action='store_false',
                     help='skip the headline variant with FP32 storage')
     ap.add_argument('--variant', default='learned', choices=tuple(VARIANTS))

@@ -96,6 +96,11 @@ class SolidMultigridProjector(SolidPressureProjector):
         # tolerance solves in V-cycle mode run as one graph with a device-side
         # WHILE loop (no host round trip per cycle); False keeps the host loop
         self.use_device_loop = True
+        # moving colliders: check a refresh's coarsening flags at the next refresh
+        # (read back asynchronously) instead of waiting for them (coarse direct
+        # solves are refreshed at once, as they need the new records on the host)
+        self.defer_refresh_check = False
+        self._pending_refresh = None
         self._loops = {}
         # [cycles of the last solve, cycles of all device-loop solves, decisions]
         self._counters = torch.zeros(3, dtype=torch.int32, device=dev.device)
@@ -176,6 +181,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.coarse_matrix = None
         self._coarse_solve()
         self._graphs = {}
+        self._pending_refresh = None
         if getattr(self, '_loops', None):
             torch.cuda.synchronize(dev.device)
             self._free_loops()
@@ -205,6 +211,18 @@ class SolidMultigridProjector(SolidPressureProjector):
         hierarchy is rebuilt. An extension: the reference keeps masked Jacobi
         for moving colliders."""
         dev = self.device
+        if self.defer_refresh_check:
+            # the previous refresh's flags, copied back while the steps ran: rebuild
+            # now if they asked for it (a V-cycle on a stale hierarchy still reaches
+            # the tolerance, only more slowly)
+            pending = self._pending_refresh
+            self._pending_refresh = None
+            if pending is not None:
+                event, host, n_then, probe_then = pending
+                event.synchronize()
+                f = host.tolist()
+                if len(self.levels) == n_then and (any(f[1:n_then]) or (probe_then and not f[n_then])):
+                    self._build_hierarchy()
         shapes = self._shapes()
         n = len(self.levels)
         probe = n < len(shapes)           # the hierarchy stopped early: could it go deeper now?
@@ -218,6 +236,14 @@ class SolidMultigridProjector(SolidPressureProjector):
             scratch = torch.empty((cz, cy, cx, 4), dtype=torch.float32, device=dev.device)
             dev.call('ffx_graph_coarsen', C.byref(self.levels[n - 1]['graph']), ptr(scratch), ptr(flags[n:n + 1]),
                      dev.s)
+        if self.defer_refresh_check and self.coarse_matrix is None:
+            host = torch.empty(n + 1, dtype=torch.int32, pin_memory=True)
+            with torch.cuda.stream(dev.stream):
+                host.copy_(flags, non_blocking=True)
+                event = torch.cuda.Event()
+                event.record(dev.stream)
+            self._pending_refresh = (event, host, n, probe)
+            return
         f = flags.cpu().tolist()
         if any(f[1:n]) or (probe and not f[n]):
             self._build_hierarchy()
