@@ -75,6 +75,19 @@ class FfxGraphTail(C.Structure):
                 ('levels', FfxTailLevel * TAIL_LEVELS)]
 
 
+class FfxBrickStats(C.Structure):
+    _fields_ = [("capacity", C.c_uint32), ("active", C.c_uint32), ("metadata_bytes", C.c_uint64)]
+
+
+class FfxArenaStats(C.Structure):
+    _fields_ = [(k, C.c_uint64) for k in ("capacity", "used", "peak", "allocations", "live", "largest_free")]
+
+
+class FfxSparseLevel(C.Structure):
+    _fields_ = [("n", C.c_int32), ("side", C.c_int32), ("mode", C.c_int32), ("sparse", C.c_int32),
+                ("map", C.c_void_p), ("active", C.c_void_p), ("coords", C.c_void_p), ("count", C.c_int32)]
+
+
 class FfxTensorView(C.Structure):
     _fields_ = [('data', vp), ('pitch', i32), ('offset', i32)]
 
@@ -169,6 +182,27 @@ _PROTOTYPES = {
                                         P(FfxSources), C.c_int, P(FfxScalarChannel), vp, vp, vp]),
     'ffx_next_dt': (C.c_int, [vp, vp, vp, C.c_double, C.c_double, C.c_double, vp]),
     'ffx_add': (C.c_int, [i64, vp, vp, vp, vp]),
+    'ffx_bricks_create': (C.c_int, [C.c_uint32, P(vp)]),
+    'ffx_bricks_destroy': (C.c_int, [vp]),
+    'ffx_bricks_lookup': (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32)]),
+    'ffx_bricks_activate': (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32)]),
+    'ffx_bricks_deactivate': (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32)]),
+    'ffx_bricks_neighbors': (C.c_int, [vp, C.c_int32, C.c_int32, C.c_int32, P(C.c_int32)]),
+    'ffx_bricks_activate_box': (C.c_int, [vp, P(C.c_int32), P(C.c_int32)]),
+    'ffx_bricks_stats': (C.c_int, [vp, P(FfxBrickStats)]),
+    'ffx_bricks_active': (C.c_int, [vp, P(C.c_int32), P(C.c_int32), C.c_uint32]),
+    'ffx_arena_create': (C.c_int, [C.c_uint64, P(vp)]),
+    'ffx_arena_destroy': (C.c_int, [vp]),
+    'ffx_arena_allocate': (C.c_int, [vp, C.c_uint64, P(C.c_uint64)]),
+    'ffx_arena_get': (C.c_int, [vp, C.c_uint64, P(C.c_uint64), P(C.c_uint64), P(C.c_uint64)]),
+    'ffx_arena_release': (C.c_int, [vp, C.c_uint64]),
+    'ffx_arena_stats': (C.c_int, [vp, P(FfxArenaStats)]),
+    'ffx_sparse_divergence': (C.c_int, [P(FfxSparseLevel), vp, C.c_int32, vp, vp]),
+    'ffx_sparse_jacobi': (C.c_int, [P(FfxSparseLevel), vp, vp, vp, vp]),
+    'ffx_sparse_residual': (C.c_int, [P(FfxSparseLevel), vp, vp, vp, vp]),
+    'ffx_sparse_gradient': (C.c_int, [P(FfxSparseLevel), vp, vp, C.c_int32, vp, vp]),
+    'ffx_sparse_restrict': (C.c_int, [P(FfxSparseLevel), vp, P(FfxSparseLevel), vp, vp]),
+    'ffx_sparse_prolong': (C.c_int, [P(FfxSparseLevel), vp, P(FfxSparseLevel), vp, vp]),
     'ffx_gradient_ex': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, f32, vp, vp, vp, vp, vp, vp, vp,
                                   vp]),
     'ffx_scale_by_ratio': (C.c_int, [i64, vp, vp, vp]),

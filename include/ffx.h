@@ -476,6 +476,70 @@ int ffx_next_dt(const float* maxima, float* clock, double* time, double cell, do
  * with the time steps on the device. */
 int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream);
 
+/* ------------------------------------------------------- sparse brick path */
+/* Brick pool: the topology of FluxFX_Source/native/bricks.hpp:14-94 (fixed
+ * capacity 1..262144, brick coordinates in [-2^20, 2^20 - 1], open addressing with
+ * tombstones, a removed slot is the next one handed out, atomic box activation
+ * with a capacity preflight). Host memory only. */
+typedef struct FfxBrickPool FfxBrickPool;
+typedef struct FfxBrickStats {
+    uint32_t capacity, active;
+    uint64_t metadata_bytes;   /* constant after creation: all storage is reserved */
+} FfxBrickStats;
+int ffx_bricks_create(uint32_t capacity, FfxBrickPool** pool);
+int ffx_bricks_destroy(FfxBrickPool* pool);
+int ffx_bricks_lookup(const FfxBrickPool* pool, int32_t x, int32_t y, int32_t z, int32_t* slot);
+int ffx_bricks_activate(FfxBrickPool* pool, int32_t x, int32_t y, int32_t z, int32_t* slot);
+int ffx_bricks_deactivate(FfxBrickPool* pool, int32_t x, int32_t y, int32_t z, int32_t* was_active);
+/* slots of the -x, +x, -y, +y, -z, +z neighbours (-1: inactive) */
+int ffx_bricks_neighbors(const FfxBrickPool* pool, int32_t x, int32_t y, int32_t z, int32_t out[6]);
+int ffx_bricks_activate_box(FfxBrickPool* pool, const int32_t lo[3], const int32_t extent[3]);
+int ffx_bricks_stats(const FfxBrickPool* pool, FfxBrickStats* out);
+/* active slots (stats.active of them) and the coordinates of every slot (3 per
+ * slot); both arrays hold room >= capacity entries */
+int ffx_bricks_active(const FfxBrickPool* pool, int32_t* slots, int32_t* coords_by_slot, uint32_t room);
+/* Arena: a GPU-independent suballocator of one buffer (FluxFX_Source/native/
+ * arena.hpp:12-57): capacity a positive multiple of 256; spans aligned to 256 bytes,
+ * first fit in address order, adjacent free spans merged on release; handles are
+ * unique across all arenas and never reused; at most 65536 live spans. */
+typedef struct FfxArena FfxArena;
+typedef struct FfxArenaStats {
+    uint64_t capacity, used, peak, allocations, live, largest_free;
+} FfxArenaStats;
+int ffx_arena_create(uint64_t capacity, FfxArena** arena);
+int ffx_arena_destroy(FfxArena* arena);
+int ffx_arena_allocate(FfxArena* arena, uint64_t bytes, uint64_t* handle);
+int ffx_arena_get(const FfxArena* arena, uint64_t handle, uint64_t* offset, uint64_t* bytes, uint64_t* requested);
+int ffx_arena_release(FfxArena* arena, uint64_t handle);
+int ffx_arena_stats(const FfxArena* arena, FfxArenaStats* out);
+/* One level of the sparse projection (FluxFX_Source/native/projection.mm:15-120):
+ * n^3 unit cells (n a multiple of side, side 8 or 16), solve region `mode` (0 all,
+ * 1 the central box [n/4, 3n/4)^3, 2 the boxes [n/8, 3n/8)^3 and [5n/8, 7n/8)^3).
+ * sparse != 0: fields hold side^3 values per brick slot, local (z*side + y)*side + x,
+ * faces the side^3 faces at the lower side of each cell per axis (upper-wall faces
+ * are zero, not stored); map = (n/side)^3 slots (-1 inactive), active = the
+ * `count` slots to sweep, coords = 3 per slot. sparse == 0: n^3 cells and
+ * (n+1) n^2 faces per axis, x-fast. `faces` is the per-axis stride of a face
+ * array. Sparse and dense give identical values on the solve region. */
+typedef struct FfxSparseLevel {
+    int32_t n, side, mode, sparse;
+    const int32_t* map;
+    const int32_t* active;
+    const int32_t* coords;
+    int32_t count;
+} FfxSparseLevel;
+int ffx_sparse_divergence(const FfxSparseLevel* l, const float* u, int32_t faces, float* out, void* stream);
+/* out = q + 2/3 ((sum of in-domain neighbours - rhs) / their count - q) on solve cells, 0 elsewhere */
+int ffx_sparse_jacobi(const FfxSparseLevel* l, const float* q, const float* rhs, float* out, void* stream);
+int ffx_sparse_residual(const FfxSparseLevel* l, const float* q, const float* rhs, float* out, void* stream);
+/* out = u - (q(c) - q(c - e)) on faces with a solve cell beside them, 0 elsewhere */
+int ffx_sparse_gradient(const FfxSparseLevel* l, const float* u, const float* q, int32_t faces, float* out,
+                        void* stream);
+int ffx_sparse_restrict(const FfxSparseLevel* fine, const float* residual, const FfxSparseLevel* coarse,
+                        float* coarse_rhs, void* stream);
+int ffx_sparse_prolong(const FfxSparseLevel* coarse, const float* correction, const FfxSparseLevel* fine,
+                       float* q, void* stream);
+
 /* ------------------------------------------------------------- bake readback */
 /* Storage code of a uint8 field (the collider mask) for ffx_pack_channels. */
 enum { FFX_PACK_U8 = 2 };
