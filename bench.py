@@ -66,6 +66,8 @@ VARIANTS = {
     'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9),
     'learned_plain': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
     'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
+    'learned_ir': dict(pressure_method='IR', solid_warm_start=False, learned_warm_start=True, mg_coarse_scale=1.9),
+    'fast_ir': dict(pressure_method='IR', solid_warm_start=True, mg_coarse_scale=1.9),
     'learned_warm': dict(pressure_method='VCYCLE', solid_warm_start=True, learned_warm_start=True,
                          learned_correction=True, mg_coarse_scale=1.9),
 }

@@ -46,7 +46,8 @@ FORMAT_COLLIDERS = 'fluxfx-checkpoint-1+colliders'
 # Settings this build adds to the reference's PressureSettings.
 EXTENSION_SETTINGS = ('pressure_tolerance', 'pressure_max_cycles', 'mg_pre_sweeps', 'mg_post_sweeps',
                       'mg_max_levels', 'heat_mode', 'velocity_blend', 'storage', 'solid_warm_start',
-                      'pressure_method', 'learned_warm_start', 'mg_coarse_scale', 'learned_correction')
+                      'pressure_method', 'learned_warm_start', 'mg_coarse_scale', 'learned_correction',
+                      'ir_inner_cycles')
 _TUPLES = ('velocity', 'source_center')
 
 

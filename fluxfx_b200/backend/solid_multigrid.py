@@ -106,6 +106,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         self._counters = torch.zeros(3, dtype=torch.int32, device=dev.device)
         self._host_total = 0
         self._sweeps_per_cycle = 0
+        self._cycle_factor = s.ir_inner_cycles if s.pressure_method == 'IR' else 1
         self._build_hierarchy()
         self._rmax = torch.zeros(2, dtype=torch.float32, device=dev.device)
 
@@ -114,9 +115,10 @@ class SolidMultigridProjector(SolidPressureProjector):
     @property
     def last_cycles(self):
         if getattr(self, '_cycles_on_device', False):
-            self._cycles_host = int(self._counters[0].item())
+            # iterative refinement counts outer iterations of ir_inner_cycles V-cycles each
+            self._cycles_host = int(self._counters[0].item()) * self._cycle_factor
             self._cycles_on_device = False
-            self._iterations_host = self._cycles_host * self._sweeps_per_cycle
+            self._iterations_host = self._cycles_host // self._cycle_factor * self._sweeps_per_cycle
         return self._cycles_host
 
     @last_cycles.setter
@@ -127,7 +129,7 @@ class SolidMultigridProjector(SolidPressureProjector):
     @property
     def last_iterations(self):
         if getattr(self, '_cycles_on_device', False):
-            return self.last_cycles * self._sweeps_per_cycle
+            return self.last_cycles // self._cycle_factor * self._sweeps_per_cycle
         return self._iterations_host
 
     @last_iterations.setter
@@ -136,7 +138,7 @@ class SolidMultigridProjector(SolidPressureProjector):
 
     def total_cycles(self):
         """V-cycles (or PCG iterations) of every solve so far (one readback)."""
-        return self._host_total + int(self._counters[1].item())
+        return self._host_total + int(self._counters[1].item()) * self._cycle_factor
 
     def _shapes(self):
         """Level shapes the grid allows (halving while all dims are even and >= 8)."""
@@ -496,6 +498,11 @@ class SolidMultigridProjector(SolidPressureProjector):
             self.levels[0]['p'], self.levels[0]['q'] = self.pressure, self.spare
             self._host_total += self.last_cycles
             return
+        if s.pressure_method == 'IR':
+            if not (s.pressure_tolerance > 0):
+                raise ValueError("pressure_method 'IR' needs a pressure tolerance")
+            self._device_solve(refine=True)
+            return
         if s.pressure_tolerance > 0 and self.use_device_loop and self.use_graphs and self.timer is None:
             self._device_solve()
             return
@@ -518,16 +525,17 @@ class SolidMultigridProjector(SolidPressureProjector):
         self._host_total += self.last_cycles
 
     # ------------------------------------------------------ device-side loop
-    def _device_solve(self):
+    def _device_solve(self, refine=False):
         """The tolerance solve as one graph launch: max|rhs|, the residual
         maximum, and WHILE (cycles < max and max|r| > tol * max|rhs|) {V-cycle,
         residual maximum} decided on the device; the cycle count stays on the
-        device until read."""
+        device until read. ``refine``: the iterative-refinement form, whose
+        loop counts outer iterations (see ``_capture_loop``)."""
         dev = self.device
-        key = ('loop', self.levels[0]['p'].data_ptr(), self.levels[0]['q'].data_ptr())
+        key = ('refine' if refine else 'loop', self.levels[0]['p'].data_ptr(), self.levels[0]['q'].data_ptr())
         entry = self._loops.get(key)
         if entry is None:
-            entry = self._capture_loop()
+            entry = self._capture_loop(refine)
             self._loops[key] = entry
         handle, per_cycle, calls = entry
         dev.call('ffx_loop_launch', handle, dev.s)
@@ -536,9 +544,15 @@ class SolidMultigridProjector(SolidPressureProjector):
         self._cycles_on_device = True
         self.pressure, self.spare = self.levels[0]['p'], self.levels[0]['q']
 
-    def _capture_loop(self):
+    def _capture_loop(self, refine=False):
         """Capture the solve loop (see ``_device_solve``) into a graph; returns
-        (loop handle, sweeps per cycle, native passes per cycle)."""
+        (loop handle, sweeps per cycle, native passes per cycle).
+
+        ``refine``: iterative refinement. The loop tests the true FP32 residual
+        r = rhs - L p (kept in a buffer); each iteration solves L e = r from
+        e = 0 with ``ir_inner_cycles`` V-cycles and sets p = p + e, so the
+        pressure is only ever updated by whole corrections and every decision
+        reads a freshly computed residual."""
         s = self.settings
         dev = self.device
         level = self.levels[0]
@@ -555,13 +569,24 @@ class SolidMultigridProjector(SolidPressureProjector):
         p0, q0 = level['p'], level['q']
         try:
             root.stream = side
+            if refine:
+                if getattr(self, '_ir', None) is None:
+                    self._ir = tuple(dev.texture(level['shape']) for _ in range(3))   # r, e, e spare
+                r, e, e2 = self._ir
+
+                def true_residual():
+                    dev.call('ffx_graph_residual', C.byref(level['graph']), ptr(p0), ptr(self.before), ptr(r), dev.s)
+                    dev.call('ffx_max_abs', n, N.FFX_F32, ptr(r), ptr(self._rmax[0:1]), dev.s)
             with torch.cuda.stream(side):
                 N.check(dev.lib.ffx_loop_begin(dev.s, C.byref(loop)))
                 dev.call('ffx_loop_reset_counter', counters, dev.s)
                 dev.call('ffx_max_abs', n, N.FFX_F32, ptr(self.before), ptr(self._rmax[1:2]), dev.s)
                 dev.call('ffx_zero_if_unscaled', ptr(self._rmax[1:2]), ptr(level['p']), n, dev.s)
-                dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
-                         ptr(self._rmax[0:1]), dev.s)
+                if refine:
+                    true_residual()
+                else:
+                    dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                             ptr(self._rmax[0:1]), dev.s)
                 dev.call('ffx_loop_decide', loop, ptr(self._rmax[0:1]), ptr(self._rmax[1:2]), tol, limit, counters,
                          dev.s)
                 body = C.c_void_p()
@@ -571,9 +596,21 @@ class SolidMultigridProjector(SolidPressureProjector):
             calls0 = dev.calls
             self._iterations_host = 0
             with torch.cuda.stream(inner):
-                self.cycle(0)
-                dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
-                         ptr(self._rmax[0:1]), dev.s)
+                if refine:
+                    # the correction equation L e = r from e = 0, then p += e
+                    level['p'], level['q'], level['rhs'] = e, e2, r
+                    try:
+                        for k in range(s.ir_inner_cycles):
+                            self.cycle(0, zero_init=(k == 0))
+                    finally:
+                        corr = level['p']
+                        level['p'], level['q'], level['rhs'] = p0, q0, self.before
+                    dev.call('ffx_add', n, ptr(p0), ptr(corr), ptr(p0), dev.s)
+                    true_residual()
+                else:
+                    self.cycle(0)
+                    dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                             ptr(self._rmax[0:1]), dev.s)
                 dev.call('ffx_loop_decide', loop, ptr(self._rmax[0:1]), ptr(self._rmax[1:2]), tol, limit, counters,
                          dev.s)
             per_cycle, calls = self._iterations_host, dev.calls - calls0

@@ -26,7 +26,10 @@ Extensions (all default to the reference's behaviour):
 * ``pressure_method`` -- "VCYCLE" (reference: stand-alone V-cycles) or "PCG"
   (conjugate gradients preconditioned by the same symmetric aggregation
   V-cycle; collider multigrid only). Both solve the same system to the same
-  tolerance.
+  tolerance. "IR": iterative refinement -- every outer iteration recomputes the
+  true FP32 residual of the pressure, decides convergence in FP64, solves the
+  correction equation from zero with ``ir_inner_cycles`` V-cycles and adds the
+  correction (collider multigrid with a tolerance).
 """
 from dataclasses import dataclass
 from math import fsum, isfinite, sqrt
@@ -44,7 +47,7 @@ _CHOICES = {
     "pressure_solver": ({"AUTO", "JACOBI", "MULTIGRID"}, "Unknown pressure solver"),
     "heat_mode": ({"RATE", "TARGET"}, "Unknown heat emission mode"),
     "storage": ({"FP32", "BF16"}, "Unknown field storage"),
-    "pressure_method": ({"VCYCLE", "PCG"}, "Unknown pressure method"),
+    "pressure_method": ({"VCYCLE", "PCG", "IR"}, "Unknown pressure method"),
 }
 
 _TURBULENCE_RANGES = (
@@ -59,6 +62,7 @@ _INT_RANGES = (
     ("mg_pre_sweeps", 0, 16, "Multigrid sweeps must be integers in [0, 16]"),
     ("mg_post_sweeps", 0, 16, "Multigrid sweeps must be integers in [0, 16]"),
     ("mg_max_levels", 0, 16, "Multigrid level cap must be an integer in [0, 16]"),
+    ("ir_inner_cycles", 1, 16, "Inner refinement cycles must be an integer in [1, 16]"),
 )
 
 
@@ -107,6 +111,7 @@ class PressureSettings(ThermalSettings):
     learned_warm_start: bool = False
     mg_coarse_scale: float = 1.0
     learned_correction: bool = False
+    ir_inner_cycles: int = 1
 
     def __post_init__(self):
         super().__post_init__()

@@ -114,3 +114,28 @@ def test_device_steps_read_nothing_back():
     assert a.steps == 4 and a.projector.last_cycles > 0
     assert a.measure_projection()['rel_div_inf'] <= 1e-4
     a.close()
+
+
+@pytest.mark.parametrize('inner', [1, 2])
+def test_iterative_refinement_reaches_the_tolerance(inner):
+    """pressure_method='IR': every outer iteration recomputes the true FP32
+    residual, decides in FP64, solves the correction equation from zero with
+    `inner` V-cycles and adds the correction. It reaches the same tolerance as
+    the V-cycle loop with about the same V-cycles, and the two solutions differ
+    by what the tolerance allows (both corrected velocities have relative
+    divergence <= 1e-4, their difference is a discrete gradient)."""
+    D = dev()
+    a, em = _solver(D, 'fast')
+    b, _ = _solver(D, 'fast', pressure_method='IR', ir_inner_cycles=inner)
+    for k in range(4):
+        a.step(0.02, sources=em)
+        b.step(0.02, sources=em)
+        ma, mb = a.measure_projection(), b.measure_projection()
+        assert ma['rel_div_inf'] <= 1e-4 and mb['rel_div_inf'] <= 1e-4, (k, ma, mb)
+        ca, cb = a.projector.last_cycles, b.projector.last_cycles
+        assert cb % inner == 0 and abs(cb - ca) <= inner + 1, (k, ca, cb)
+        for x, y in zip(a._velocity, b._velocity):
+            scale = float(y.abs().max())
+            assert float((x - y).abs().max()) <= 2e-3 * scale, k
+    a.close()
+    b.close()
