@@ -83,6 +83,18 @@ class CudaDevice:
     def synchronize(self):
         self.stream.synchronize()
 
+    def ordered(self):
+        """Context in which torch ops run on this device's stream, after the
+        passes queued there (a solver may run on a stream other than torch's
+        current one)."""
+        return torch.cuda.stream(self.stream)
+
+    def fetch(self, tensor):
+        """Synchronous host copy of a device tensor, ordered after the passes
+        queued on this device's stream."""
+        with torch.cuda.stream(self.stream):
+            return tensor.cpu()
+
     def capture(self, fn):
         """Record the passes ``fn`` enqueues into a CUDA graph (not executed now).
 

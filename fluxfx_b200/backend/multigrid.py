@@ -117,7 +117,7 @@ class MultigridPressureProjector(PressureProjector):
         level = self.levels[0]
         self.device.call('ffx_mg_residual_max', self._n3(level), self._inv3(level), ptr(level['p']),
                          ptr(level['rhs']), dt, ptr(self._rmax[0:1]), self.device.s)
-        return float(self._rmax[0].item())
+        return float(self.device.fetch(self._rmax[0]))
 
     def _run_cycles(self, dt, budget):
         s = self.settings
@@ -129,7 +129,7 @@ class MultigridPressureProjector(PressureProjector):
             return
         self.device.call('ffx_max_abs', self.before.numel(), N.FFX_F32, ptr(self.before), ptr(self._rmax[1:2]),
                          self.device.s)
-        scale = float(self._rmax[1].item()) / dt
+        scale = float(self.device.fetch(self._rmax[1])) / dt
         if scale == 0:
             self.levels[0]['p'].zero_()
             return

@@ -127,7 +127,7 @@ class PressureProjector:
         """The last projection's dt on the host (one readback after device steps)."""
         if self.last_dt is None or isinstance(self.last_dt, float):
             return self.last_dt
-        return float(self.last_dt[1].item())
+        return float(self.device.fetch(self.last_dt[1]))
 
     def _gradient(self, outputs, solve_dt):
         links = self.gradient_links()
@@ -185,10 +185,14 @@ class PressureProjector:
     # ------------------------------------------------------------- diagnostics
     def velocity_maxima(self):
         """max |u|, |v|, |w| of the last corrected velocity (one readback)."""
-        return [float(v) for v in self._scalars[0:3].cpu()]
+        return [float(v) for v in self.device.fetch(self._scalars[0:3])]
 
     def divergence_summary(self):
         """FP64 statistics of ``before``/``after`` on the device (one readback)."""
+        with self.device.ordered():
+            return self._divergence_summary()
+
+    def _divergence_summary(self):
         n = self.before.numel()
         ws = torch.empty(int(self.device.lib.ffx_divergence_stats_workspace(n)) // 8 + 1,
                          dtype=torch.float64, device=self.device.device)

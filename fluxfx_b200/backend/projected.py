@@ -90,7 +90,7 @@ class DenseProjectedSmoke(DenseThermalAdvection):
     @property
     def time(self):
         if getattr(self, '_clock_live', False):
-            return self._time_host + float(self._clock_time.item())
+            return self._time_host + float(self.device.fetch(self._clock_time))
         return self._time_host
 
     @time.setter
@@ -106,42 +106,46 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         return super().allocated_bytes + extra + self.projector.allocated_bytes + self.detail.allocated_bytes
 
     def reset(self, seed=True):
-        super().reset(seed)
-        self._clock_live = False      # the next step_cfl starts again from dt_max
-        self.faulted = False
-        if self.combustion is not None:
-            self.combustion.reset()
-        if self.solids is not None:
-            self.solids.clear_solid(self._front, self._back)
-            self._front, self._back = self._back, self._front
-            if self._temperature is not None:
-                self.solids.clear_solid(self._temperature, self._temperature_back)
-                self._temperature, self._temperature_back = self._temperature_back, self._temperature
-        if self.projector is not None:
-            self.projector.reset()
-            self.projector.enforce_walls(self._velocity, self._velocity_back)
-            self._velocity, self._velocity_back = self._velocity_back, self._velocity
+        with self.device.ordered():
+            super().reset(seed)
+            self._clock_live = False      # the next step_cfl starts again from dt_max
+            self.faulted = False
+            if self.combustion is not None:
+                self.combustion.reset()
+            if self.solids is not None:
+                self.solids.clear_solid(self._front, self._back)
+                self._front, self._back = self._back, self._front
+                if self._temperature is not None:
+                    self.solids.clear_solid(self._temperature, self._temperature_back)
+                    self._temperature, self._temperature_back = self._temperature_back, self._temperature
+            if self.projector is not None:
+                self.projector.reset()
+                self.projector.enforce_walls(self._velocity, self._velocity_back)
+                self._velocity, self._velocity_back = self._velocity_back, self._velocity
 
     def upload_velocity(self, components):
-        super().upload_velocity(components)
-        if self.solids is not None:
-            self.projector.enforce_walls(self._velocity, self._velocity_back)
-            self._velocity, self._velocity_back = self._velocity_back, self._velocity
-        self.projector.reset()
+        with self.device.ordered():
+            super().upload_velocity(components)
+            if self.solids is not None:
+                self.projector.enforce_walls(self._velocity, self._velocity_back)
+                self._velocity, self._velocity_back = self._velocity_back, self._velocity
+            self.projector.reset()
 
     def upload(self, values):
-        super().upload(values)
-        if self.solids is not None:
-            self.solids.clear_solid(self._front, self._back)
-            self._front, self._back = self._back, self._front
-        self.projector.reset()
+        with self.device.ordered():
+            super().upload(values)
+            if self.solids is not None:
+                self.solids.clear_solid(self._front, self._back)
+                self._front, self._back = self._back, self._front
+            self.projector.reset()
 
     def upload_temperature(self, values):
-        super().upload_temperature(values)
-        if self.solids is not None:
-            self.solids.clear_solid(self._temperature, self._temperature_back)
-            self._temperature, self._temperature_back = self._temperature_back, self._temperature
-        self.projector.reset()
+        with self.device.ordered():
+            super().upload_temperature(values)
+            if self.solids is not None:
+                self.solids.clear_solid(self._temperature, self._temperature_back)
+                self._temperature, self._temperature_back = self._temperature_back, self._temperature
+            self.projector.reset()
 
     def update_settings(self, settings):
         """Apply live parameters between steps, preserving all fields and pressure."""
@@ -151,21 +155,22 @@ class DenseProjectedSmoke(DenseThermalAdvection):
 
     def move_colliders(self, colliders, dt):
         """New collider poses before a step (``projected.py:103-115``)."""
-        if not self.settings.moving_colliders or self.solids is None:
-            raise ValueError('Enable Moving colliders and Reset first')
-        validate_dt(dt)
-        if self.faulted:
-            raise RuntimeError('Reset required after a failed GPU step')
-        try:
-            self.solids.update(colliders, dt)
-            self.solids.remap(self)
-            refresh = getattr(self.projector, 'refresh_hierarchy', None)
-            if refresh is not None:
-                refresh()            # multigrid with moving colliders (extension): follow the new mask
-            self.projector.ready = False
-        except Exception:
-            self.faulted = True
-            raise
+        with self.device.ordered():
+            if not self.settings.moving_colliders or self.solids is None:
+                raise ValueError('Enable Moving colliders and Reset first')
+            validate_dt(dt)
+            if self.faulted:
+                raise RuntimeError('Reset required after a failed GPU step')
+            try:
+                self.solids.update(colliders, dt)
+                self.solids.remap(self)
+                refresh = getattr(self.projector, 'refresh_hierarchy', None)
+                if refresh is not None:
+                    refresh()            # multigrid with moving colliders (extension): follow the new mask
+                self.projector.ready = False
+            except Exception:
+                self.faulted = True
+                raise
 
     def measure_projection(self):
         return self.projector.metrics() | {"step": self.steps, "simulation_time": self.time}
@@ -180,48 +185,50 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         the GPU. ``time`` and ``current_dt()`` read the clock when asked. Needs
         the impulse pressure form (multigrid or colliders); not with
         confinement, combustion or moving colliders."""
-        if not (0 < cfl <= 10 and 0 < dt_max <= 0.1):
-            raise ValueError('cfl must lie in (0, 10] and dt_max in (0, 0.1]')
-        s = self.settings
-        if s.vorticity_strength > 0 or self.combustion is not None or s.moving_colliders:
-            raise ValueError('Device time steps cover the smoke step without confinement, combustion '
-                             'or moving colliders')
-        if sources is not None:
-            self._prepare_sources(sources)
-        if self.faulted:
-            raise RuntimeError("Reset required after a failed GPU step")
-        if not self._clock_live:
-            previous = self.projector.previous_dt()
-            self._clock[0] = dt_max
-            self._clock[1] = previous if previous is not None else 0.0
-            self._clock_time.zero_()
-            self._clock_live = True
-        try:
-            self._step(None, emission or Emission(self.settings.source_center), sources, clock=self._clock)
-            cell = min(e / n for e, n in zip(self.grid.extent, self.grid.shape))
-            self.device.call('ffx_next_dt', ptr(self.projector._scalars[0:3]), ptr(self._clock),
-                             ptr(self._clock_time), cell, float(cfl), float(dt_max), self.device.s)
-        except Exception:
-            self.faulted = True
-            self.projector.ready = False
-            raise
+        with self.device.ordered():
+            if not (0 < cfl <= 10 and 0 < dt_max <= 0.1):
+                raise ValueError('cfl must lie in (0, 10] and dt_max in (0, 0.1]')
+            s = self.settings
+            if s.vorticity_strength > 0 or self.combustion is not None or s.moving_colliders:
+                raise ValueError('Device time steps cover the smoke step without confinement, combustion '
+                                 'or moving colliders')
+            if sources is not None:
+                self._prepare_sources(sources)
+            if self.faulted:
+                raise RuntimeError("Reset required after a failed GPU step")
+            if not self._clock_live:
+                previous = self.projector.previous_dt()
+                self._clock[0] = dt_max
+                self._clock[1] = previous if previous is not None else 0.0
+                self._clock_time.zero_()
+                self._clock_live = True
+            try:
+                self._step(None, emission or Emission(self.settings.source_center), sources, clock=self._clock)
+                cell = min(e / n for e, n in zip(self.grid.extent, self.grid.shape))
+                self.device.call('ffx_next_dt', ptr(self.projector._scalars[0:3]), ptr(self._clock),
+                                 ptr(self._clock_time), cell, float(cfl), float(dt_max), self.device.s)
+            except Exception:
+                self.faulted = True
+                self.projector.ready = False
+                raise
 
     def current_dt(self):
         """The dt the next ``step_cfl`` will take (one readback)."""
-        return float(self._clock[0].item())
+        return float(self.device.fetch(self._clock[0]))
 
     def step(self, dt=1.0 / 30.0, emission=None, sources=None):
-        validate_dt(dt)
-        if sources is not None:
-            self._prepare_sources(sources)
-        if self.faulted:
-            raise RuntimeError("Reset required after a failed GPU step")
-        try:
-            self._step(dt, emission or Emission(self.settings.source_center), sources)
-        except Exception:
-            self.faulted = True
-            self.projector.ready = False
-            raise
+        with self.device.ordered():
+            validate_dt(dt)
+            if sources is not None:
+                self._prepare_sources(sources)
+            if self.faulted:
+                raise RuntimeError("Reset required after a failed GPU step")
+            try:
+                self._step(dt, emission or Emission(self.settings.source_center), sources)
+            except Exception:
+                self.faulted = True
+                self.projector.ready = False
+                raise
 
     def _prepare_sources(self, sources):
         data = pack_sources(sources)
@@ -330,7 +337,7 @@ class DenseProjectedSmoke(DenseThermalAdvection):
 
     def scalar_maxima(self):
         """max |density|, |temperature| of the last step (one readback)."""
-        return [float(v) for v in self._maxima[0:2].cpu()]
+        return [float(v) for v in self.device.fetch(self._maxima[0:2])]
 
     def preview_field(self, channel):
         if channel == 'COLLISION':

@@ -116,7 +116,7 @@ class SolidMultigridProjector(SolidPressureProjector):
     def last_cycles(self):
         if getattr(self, '_cycles_on_device', False):
             # iterative refinement counts outer iterations of ir_inner_cycles V-cycles each
-            self._cycles_host = int(self._counters[0].item()) * self._cycle_factor
+            self._cycles_host = int(self.device.fetch(self._counters[0])) * self._cycle_factor
             self._cycles_on_device = False
             self._iterations_host = self._cycles_host // self._cycle_factor * self._sweeps_per_cycle
         return self._cycles_host
@@ -138,7 +138,7 @@ class SolidMultigridProjector(SolidPressureProjector):
 
     def total_cycles(self):
         """V-cycles (or PCG iterations) of every solve so far (one readback)."""
-        return self._host_total + int(self._counters[1].item()) * self._cycle_factor
+        return self._host_total + int(self.device.fetch(self._counters[1])) * self._cycle_factor
 
     def _shapes(self):
         """Level shapes the grid allows (halving while all dims are even and >= 8)."""
@@ -174,7 +174,7 @@ class SolidMultigridProjector(SolidPressureProjector):
             cx, cy, cz = coarse_shape
             edges = torch.empty((cz, cy, cx, 4), dtype=torch.float32, device=dev.device)
             dev.call('ffx_graph_coarsen', C.byref(self.levels[-1]['graph']), ptr(edges), ptr(flag), dev.s)
-            if int(flag.item()):
+            if int(self.device.fetch(flag)):
                 break   # an aggregate would join disconnected children: stop here
             graph = N.FfxGraphLevel(*coarse_shape, ptr(edges), None, N.f3(0.0, 0.0, 0.0))
             graph.coarse_scale = s.mg_coarse_scale
@@ -195,7 +195,8 @@ class SolidMultigridProjector(SolidPressureProjector):
         s = self.settings
         last = self.levels[-1]
         if prod(last['shape']) <= DIRECT_LIMIT and s.coarse_solver == 'DIRECT' and len(self.levels) > 1:
-            inv = torch.as_tensor(graph_pseudoinverse(last['shape'], last['edges'].cpu().numpy()), dtype=torch.float64)
+            edges = self.device.fetch(last['edges']).numpy()
+            inv = torch.as_tensor(graph_pseudoinverse(last['shape'], edges), dtype=torch.float64)
             old = getattr(self, 'coarse_matrix', None)
             if old is not None and old.shape == inv.shape:
                 old.copy_(inv.to(old.device))
@@ -246,7 +247,7 @@ class SolidMultigridProjector(SolidPressureProjector):
                 event.record(dev.stream)
             self._pending_refresh = (event, host, n, probe)
             return
-        f = flags.cpu().tolist()
+        f = dev.fetch(flags).tolist()
         if any(f[1:n]) or (probe and not f[n]):
             self._build_hierarchy()
         elif self.coarse_matrix is not None:
@@ -371,7 +372,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         level = self.levels[0]
         self.device.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
                          ptr(self._rmax[0:1]), self.device.s)
-        return float(self._rmax[0].item())
+        return float(self.device.fetch(self._rmax[0]))
 
     # ------------------------------------------------------------ graph replay
     def _replayed(self, key, fn):
@@ -443,7 +444,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         for _restart in range(2):
             dev.call('ffx_graph_residual', g, ptr(x), ptr(self.before), ptr(B['res']), dev.s)
             dev.call('ffx_max_abs', n, N.FFX_F32, ptr(B['res']), ptr(B['rmax']), dev.s)
-            if float(B['rmax'].item()) <= tol:
+            if float(self.device.fetch(B['rmax'])) <= tol:
                 return
             k = 0
             while self.last_cycles < budget:
@@ -453,13 +454,13 @@ class SolidMultigridProjector(SolidPressureProjector):
                     self._replayed(('pcg', x.data_ptr(), k % 2), lambda kk=k: self._pcg_iteration(B, x, kk))
                 self.last_cycles += 1
                 k += 1
-                if float(B['rmax'].item()) <= tol:
+                if float(self.device.fetch(B['rmax'])) <= tol:
                     break
             if tol < 0 or self.last_cycles >= budget:
                 return
             # the recursively updated residual drifts in FP32: confirm on the true one
             dev.call('ffx_graph_residual_max', g, ptr(x), ptr(self.before), ptr(B['rmax']), dev.s)
-            if float(B['rmax'].item()) <= tol:
+            if float(self.device.fetch(B['rmax'])) <= tol:
                 return
 
     def solve_pressure(self, dt, previous_dt):
@@ -489,7 +490,7 @@ class SolidMultigridProjector(SolidPressureProjector):
             if s.pressure_tolerance > 0:
                 self.device.call('ffx_max_abs', self.before.numel(), N.FFX_F32, ptr(self.before),
                                  ptr(self._rmax[1:2]), self.device.s)
-                scale = float(self._rmax[1].item())
+                scale = float(self.device.fetch(self._rmax[1]))
                 budget = s.pressure_max_cycles
             if s.pressure_tolerance > 0 and scale == 0:
                 self.pressure.zero_()
@@ -514,7 +515,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         else:
             self.device.call('ffx_max_abs', self.before.numel(), N.FFX_F32, ptr(self.before),
                              ptr(self._rmax[1:2]), self.device.s)
-            scale = float(self._rmax[1].item())
+            scale = float(self.device.fetch(self._rmax[1]))
             if scale == 0:
                 self.levels[0]['p'].zero_()
             else:
@@ -666,11 +667,11 @@ class SolidMultigridProjector(SolidPressureProjector):
         """Host copy of a level's (+x, +y, +z, active) records, x-fast."""
         level = self.levels[index]
         if level['edges'] is not None:
-            return level['edges'].cpu().numpy()
+            return self.device.fetch(level['edges']).numpy()
         nz, ny, nx = self.levels[0]['p'].shape
         out = torch.empty((nz, ny, nx, 4), dtype=torch.float32, device=self.device.device)
         self.device.call('ffx_graph_level0_edges', C.byref(level['graph']), ptr(out), self.device.s)
-        return out.cpu().numpy()
+        return self.device.fetch(out).numpy()
 
     def metrics(self):
         return super().metrics() | {

@@ -29,7 +29,7 @@ class AdaptiveTimestep:
         for k, f in enumerate(fields):
             code = N.FFX_F32 if f.dtype == torch.float32 else N.FFX_BF16
             self.device.call('ffx_max_abs', f.numel(), code, ptr(f), ptr(self._out[k:k + 1]), self.device.s)
-        maxima = [float(v) for v in self._out.cpu()]
+        maxima = [float(v) for v in self.device.fetch(self._out)]
         if any(not isfinite(v) or v >= 1e30 for v in maxima):
             raise RuntimeError('Nonfinite or excessive field values; reset simulation')
         return maxima
