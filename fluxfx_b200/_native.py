@@ -39,7 +39,7 @@ class FfxGrid(C.Structure):
 
 
 class FfxSolids(C.Structure):
-    _fields_ = [('solid', vp), ('halo', vp), ('wall', vp * 3)]
+    _fields_ = [('solid', vp), ('halo', vp), ('wall', vp * 3), ('clear', vp)]
 
 
 class FfxSources(C.Structure):
@@ -144,6 +144,7 @@ _PROTOTYPES = {
     'ffx_seed_faces': (C.c_int, [P(FfxGrid), C.c_int, f3, f32, vp, vp, vp, vp]),
     'ffx_raster_colliders': (C.c_int, [P(FfxGrid), C.c_double * 3, C.c_int, vp, vp, vp]),
     'ffx_dilate_mask': (C.c_int, [P(FfxGrid), vp, vp, vp]),
+    'ffx_clearance': (C.c_int, [P(FfxGrid), vp, vp, vp]),
     'ffx_solid_clear': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp]),
     'ffx_face_predictor': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
     'ffx_set_transport_tiling': (C.c_int, [C.c_int]),

@@ -52,6 +52,10 @@ class SolidDevice:
         self.base.call('ffx_raster_colliders', C.byref(g), (C.c_double * 3)(*grid.extent), len(colliders),
                        ptr(rows), ptr(self.mask), self.base.s)
         self.base.call('ffx_dilate_mask', C.byref(g), ptr(self.mask), ptr(self.halo), self.base.s)
+        # cells with no collider or wall within three cells: the transport passes
+        # skip their collider tests (ffx_clearance); refreshed with the mask
+        self.clear = torch.zeros((nz, ny, nx), dtype=torch.uint8, device=dev)
+        self.base.call('ffx_clearance', C.byref(g), ptr(self.halo), ptr(self.clear), self.base.s)
         self._rows = rows
         self.colliders = tuple(colliders)
 
@@ -71,7 +75,7 @@ class SolidDevice:
 
     @property
     def allocated_bytes(self):
-        return 2 * prod(self.grid.shape)
+        return 3 * prod(self.grid.shape)
 
     def kernel(self, filename, constants=(), sample_input=False, samplers=(), includes=(), output_format='R32F'):
         handle = self.base.kernel(filename, constants)
@@ -89,7 +93,7 @@ class SolidDevice:
         self.base.call('ffx_solid_clear', C.byref(g), code, ptr(self.mask), ptr(source), ptr(target), self.base.s)
 
     def close(self):
-        self.mask = self.halo = None
+        self.mask = self.halo = self.clear = None
         self.decorated = []
         self.mesh_sdf = None
         self.mesh_reports = []

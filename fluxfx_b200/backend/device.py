@@ -208,7 +208,10 @@ def solids_struct(device):
     mask = getattr(device, 'mask', None)
     halo = getattr(device, 'halo', None)
     walls = getattr(device, 'walls', None)
+    clear = getattr(device, 'clear', None)
     s = N.FfxSolids(ptr(mask) if mask is not None else None, ptr(halo) if halo is not None else None)
+    if clear is not None and mask is not None:
+        s.clear = clear.data_ptr()
     if walls is not None:
         for a in range(3):
             s.wall[a] = walls[a].data_ptr()

@@ -37,7 +37,7 @@ class MovingSolidDevice(SolidDevice):
 
     @property
     def allocated_bytes(self):
-        return 3 * prod(self.grid.shape) + 4 * sum(prod(s) for s in self.grid.face_shapes)
+        return 4 * prod(self.grid.shape) + 4 * sum(prod(s) for s in self.grid.face_shapes)
 
     def _owner_mask(self, colliders):
         rows, box = collider_rows12(colliders)
@@ -47,6 +47,7 @@ class MovingSolidDevice(SolidDevice):
         self.base.call('ffx_moving_mask', C.byref(self._g), len(colliders), rows_h, box_h, ptr(self.mask),
                        self.base.s)
         self.base.call('ffx_dilate_mask', C.byref(self._g), ptr(self.mask), ptr(self.halo), self.base.s)
+        self.base.call('ffx_clearance', C.byref(self._g), ptr(self.halo), ptr(self.clear), self.base.s)
 
     def update(self, colliders, dt):
         """New poses: owner mask, dilated mask and wall velocities, in place."""

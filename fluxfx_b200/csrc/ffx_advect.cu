@@ -142,6 +142,7 @@ struct PredParams {
     Dev d;
     const uint8_t* solid;
     const uint8_t* halo;
+    const uint8_t* clear;     // optional: ffx_clearance of the mask (collider tests skipped in clear cells)
     Faces<T> F;
     float dt;
     const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
@@ -180,14 +181,16 @@ __device__ __forceinline__ void face_predictor_face(const PredParams<T>& P, cons
     const uint8_t* __restrict__ halo = P.halo;
     const float dt = step_dt(P);
     T* out = P.out[f.axis];
-    if (MASK && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
+    // a clear cell and its lower neighbours are fluid: the face is open
+    const bool clear = MASK && home_clear(P.clear, d, f.x, f.y, f.z);
+    if (MASK && !clear && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
         Store<T>::st(out, f.i, 0.f);
         return;
     }
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
-    F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * f.x + (f.axis != 0), 2 * f.y + (f.axis != 1), 2 * f.z + (f.axis != 2));
-    F3 dep = backtrace_s<MASK, P2>(d, smp, solid, halo, p, v0, dt);
+    F3 v0 = start_velocity_face<P2>(d, smp, p, f.axis, f.x, f.y, f.z);
+    F3 dep = backtrace_s<MASK, P2>(d, smp, solid, halo, p, v0, dt, clear);
     float value = smp.sample(f.axis, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
                              dv_h<P2>(d, dep.z, 2) - oz);
     Store<T>::st(out, f.i, value);
@@ -217,6 +220,7 @@ struct VelParams {
     Dev d;
     const uint8_t* solid;
     const uint8_t* halo;
+    const uint8_t* clear;   // optional: ffx_clearance of the mask
     Faces<T> F;       // velocity at the start of the step
     Faces<T> P;       // MacCormack predictor
     float dt, blend, lift, weight;
@@ -236,14 +240,25 @@ template <typename T, bool MASK, bool P2, class Smp>
 __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, const FaceIdx& f, const Smp& smp) {
     const Dev& d = P.d;
     const int axis = f.axis;
+    if (P.apply_walls) {
+        // a boundary face ends as its wall value whatever was advected into it
+        // (the wall condition below), so its advection is skipped
+        const int c = axis == 0 ? f.x : (axis == 1 ? f.y : f.z);
+        const int n = axis == 0 ? f.sx : (axis == 1 ? f.sy : f.sz);
+        if (c == 0 || c == n - 1) {
+            Store<T>::st(P.out[axis], f.i, wall_value(P.walls, axis, f.i));
+            return;
+        }
+    }
     const float dt = step_dt(P);
-    bool blocked = MASK && solid_face(d, P.solid, f.x, f.y, f.z, axis);
+    const bool clear = MASK && home_clear(P.clear, d, f.x, f.y, f.z);
+    bool blocked = MASK && !clear && solid_face(d, P.solid, f.x, f.y, f.z, axis);
     float value = 0.f;
     if (!blocked) {
         float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
         F3 p = {dv_n<P2>(d, ((float)f.x + off[0]) * d.e[0], 0), dv_n<P2>(d, ((float)f.y + off[1]) * d.e[1], 1),
                 dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
-        F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * f.x + (axis != 0), 2 * f.y + (axis != 1), 2 * f.z + (axis != 2));
+        F3 v0 = start_velocity_face<P2>(d, smp, p, axis, f.x, f.y, f.z);
         // The host passes the predictor's departure points only when both passes
         // form the same start point at every face (face_starts_match); the
         // predictor then traced this face's start point with the same velocity,
@@ -255,7 +270,7 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
             const int nf = P.nf[axis];
             dep = {__ldg(D + f.i), __ldg(D + f.i + nf), __ldg(D + f.i + 2 * nf)};
         } else {
-            dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt);
+            dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, clear);
         }
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
@@ -278,7 +293,7 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
             bool ok = !(dep.x < lob[0] || dep.y < lob[1] || dep.z < lob[2] || dep.x > hib[0] || dep.y > hib[1] ||
                         dep.z > hib[2] || arr.x < lob[0] || arr.y < lob[1] || arr.z < lob[2] || arr.x > hib[0] ||
                         arr.y > hib[1] || arr.z > hib[2]);
-            if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
+            if (MASK && ok) ok = safe_correction_from<P2>(d, P.solid, P.halo, clear, p, dep, mid2, arr);
             if (ok) {
                 float pa = smp.sample(3 + axis, dv_h<P2>(d, arr.x, 0) - off[0], dv_h<P2>(d, arr.y, 1) - off[1],
                                       dv_h<P2>(d, arr.z, 2) - off[2]);
@@ -499,6 +514,7 @@ struct ScalarXport {
     Dev d;
     const uint8_t* solid;
     const uint8_t* halo;
+    const uint8_t* clear;   // optional: ffx_clearance of the mask
     Faces<T> F;
     float dt;
     const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
@@ -521,13 +537,14 @@ template <typename T, bool MASK, bool P2, class Smp>
 __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, int x, int y, int z, const Smp& smp) {
     const Dev& d = P.d;
     const int i = cidx(d, x, y, z);
-    if (MASK && __ldg(P.solid + i)) {
+    const bool clear = MASK && home_clear(P.clear, d, x, y, z);
+    if (MASK && !clear && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, 0.f);
         return;
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
-    F3 dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P));
+    F3 dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P), clear);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     const auto S = smp.template closed<MASK>(P.solid, qx, qy, qz);
@@ -566,6 +583,7 @@ struct ScalarFinal {
     Dev d;
     const uint8_t* solid;
     const uint8_t* halo;
+    const uint8_t* clear;   // optional: ffx_clearance of the mask
     Faces<T> F;
     float dt;
     const float* dtp;     // optional: the time step read on the device (times dt_sign) instead of dt
@@ -585,7 +603,8 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
                                                     float vmax[3]) {
     const Dev& d = P.d;
     const int i = cidx(d, x, y, z);
-    if (MASK && __ldg(P.solid + i)) {
+    const bool clear = MASK && home_clear(P.clear, d, x, y, z);
+    if (MASK && !clear && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
         return;
     }
@@ -597,7 +616,7 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
     const bool reuse = P.corrected && P.dep != nullptr;
     F3 dep;
     if (reuse) dep = {__ldg(P.dep + i), __ldg(P.dep + i + P.n), __ldg(P.dep + i + 2 * P.n)};
-    else dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt);
+    else dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, clear);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     bool ok = false;
@@ -612,7 +631,7 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
         ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
                dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
                arr.y > hb[1] || arr.z > hb[2]);
-        if (MASK && ok) ok = safe_solid_correction<P2>(d, P.solid, P.halo, p, dep, mid2, arr);
+        if (MASK && ok) ok = safe_correction_from<P2>(d, P.solid, P.halo, clear, p, dep, mid2, arr);
     }
     // lower corner of the departure cell (the clamp bounds: its 8 corners clamped to the grid)
     const int bx = ok ? (int)floorf(qx) : 0, by = ok ? (int)floorf(qy) : 0, bz = ok ? (int)floorf(qz) : 0;
@@ -799,6 +818,7 @@ bool solids_ok(const FfxSolids* s) {
     if (!s) return true;
     const bool walls = s->wall[0] || s->wall[1] || s->wall[2];
     if (walls && !(s->wall[0] && s->wall[1] && s->wall[2] && s->solid)) return false;   // all three, with a mask
+    if (s->clear && !s->solid) return false;                  // clearance only with a mask
     return (!s->solid && !s->halo) || (s->solid && s->halo);
 }
 bool has_mask(const FfxSolids* s) { return s && s->solid; }
@@ -833,6 +853,7 @@ static int face_predictor_impl(const FfxGrid* g, const FfxSolids* s, int storage
         Q.d = d;
         Q.solid = solid;
         Q.halo = halo;
+        Q.clear = solid ? s->clear : nullptr;
         Q.F = F;
         Q.dt = dt;
         Q.dtp = dtp;
@@ -895,6 +916,7 @@ static int advect_velocity_impl(const FfxGrid* g, const FfxSolids* s, int storag
         P.d = d;
         P.solid = has_mask(s) ? s->solid : nullptr;
         P.halo = has_mask(s) ? s->halo : nullptr;
+        P.clear = has_mask(s) ? s->clear : nullptr;
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.P = corrected ? Faces<T>{(const T*)pu, (const T*)pv, (const T*)pw} : P.F;
         P.dt = dt;
@@ -994,6 +1016,7 @@ static int scalar_transport_impl(const FfxGrid* g, const FfxSolids* s, int stora
         P.d = d;
         P.solid = has_mask(s) ? s->solid : nullptr;
         P.halo = has_mask(s) ? s->halo : nullptr;
+        P.clear = has_mask(s) ? s->clear : nullptr;
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.dt = dt;
         P.dtp = dtp;
@@ -1057,6 +1080,7 @@ static int advect_scalars_impl(const FfxGrid* g, const FfxSolids* s, int storage
         P.d = d;
         P.solid = has_mask(s) ? s->solid : nullptr;
         P.halo = has_mask(s) ? s->halo : nullptr;
+        P.clear = has_mask(s) ? s->clear : nullptr;
         P.F = {(const T*)u, (const T*)v, (const T*)w};
         P.dt = dt;
         P.dtp = dtp;

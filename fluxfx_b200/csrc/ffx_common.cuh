@@ -430,6 +430,72 @@ __device__ __forceinline__ bool safe_solid_correction(const Dev& d, const uint8_
     return clipped_ok(arr, pa, true);
 }
 
+// ---------------------------------------------------------------- clearance
+// `clear` (ffx_clearance) marks the cells with no solid and no out-of-domain
+// cell within Chebyshev distance 3 (so every cell within distance 1 of them
+// lies at distance >= 3, every cell within distance 2 at distance >= 2 from
+// the nearest solid or outside cell). Let p be the start point of a face or
+// cell whose own cell c (its integer cell coordinates) is clear, and t a
+// target within 0.75 h of p on every axis:
+//  * floor(p / h * n) is c or a neighbour of c (rounding of the grid
+//    coordinate), so the trace's start cell is at distance >= 3 and t's cell,
+//    within one cell of it, at distance >= 2: both lie in the grid at least one
+//    cell from the walls, with a clear 3x3x3 block (halo 0);
+//  * clip_solid_trace(p, t) therefore takes its fast path with unclamped grid
+//    coordinates and returns t / e * n / n * e (clear_clip), which is t itself
+//    when e, n and h are powers of two (exact rescalings);
+//  * safe_solid_correction(p, dep, mid, arr) with all three near p finds every
+//    probe inside the grid with a clear halo and every segment on the fast
+//    path, so it reduces to the three distance tests of the fast values
+//    (clear_correction), always true on power-of-two grids.
+// Both forms give the functions' results bit for bit and skip their mask reads.
+__device__ __forceinline__ bool home_clear(const uint8_t* __restrict__ clear, const Dev& d, int x, int y, int z) {
+    return clear != nullptr && x < d.nx && y < d.ny && z < d.nz && __ldg(clear + cidx(d, x, y, z)) != 0;
+}
+
+__device__ __forceinline__ bool near_start(const Dev& d, F3 p, F3 t) {
+    return fabsf(t.x - p.x) <= 0.75f * d.h[0] && fabsf(t.y - p.y) <= 0.75f * d.h[1] &&
+           fabsf(t.z - p.z) <= 0.75f * d.h[2];
+}
+
+template <bool P2>
+__device__ __forceinline__ F3 clear_clip(const Dev& d, F3 t) {
+    if constexpr (P2) {
+        return t;
+    } else {
+        return F3{dv_n<P2>(d, dv_e<P2>(d, t.x, 0) * d.nf[0], 0) * d.e[0],
+                  dv_n<P2>(d, dv_e<P2>(d, t.y, 1) * d.nf[1], 1) * d.e[1],
+                  dv_n<P2>(d, dv_e<P2>(d, t.z, 2) * d.nf[2], 2) * d.e[2]};
+    }
+}
+
+template <bool P2>
+__device__ __forceinline__ bool clear_correction(const Dev& d, F3 dep, F3 mid, F3 arr) {
+    if constexpr (P2) {
+        return true;
+    } else {
+        return within_1e7(clear_clip<P2>(d, dep), dep) && within_1e7(clear_clip<P2>(d, mid), mid) &&
+               within_1e7(clear_clip<P2>(d, arr), arr);
+    }
+}
+
+// clip_solid_trace(p, t), through the clear form where it applies.
+template <bool P2>
+__device__ __forceinline__ F3 clip_from(const Dev& d, const uint8_t* solid, const uint8_t* halo, bool clear, F3 p,
+                                        F3 t) {
+    if (clear && near_start(d, p, t)) return clear_clip<P2>(d, t);
+    return clip_solid_trace<P2>(d, solid, halo, p, t);
+}
+
+// safe_solid_correction(p, dep, mid, arr), through the clear form where it applies.
+template <bool P2>
+__device__ __forceinline__ bool safe_correction_from(const Dev& d, const uint8_t* solid, const uint8_t* halo,
+                                                     bool clear, F3 p, F3 dep, F3 mid, F3 arr) {
+    if (clear && near_start(d, p, dep) && near_start(d, p, mid) && near_start(d, p, arr))
+        return clear_correction<P2>(d, dep, mid, arr);
+    return safe_solid_correction<P2>(d, solid, halo, p, dep, mid, arr);
+}
+
 // ---------------------------------------------------------------- emitters
 // Exact time average of the compact sphere profile along a linear sweep
 // (emission_weight.glsl:2-29).

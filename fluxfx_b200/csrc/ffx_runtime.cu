@@ -98,6 +98,20 @@ __global__ void dilate_kernel(Dev d, const uint8_t* __restrict__ solid, uint8_t*
     halo[i] = any;
 }
 
+// 1 where no cell of the 5x5x5 block around the cell is set in `halo` or lies
+// outside the grid (ffx_clearance).
+__global__ void clearance_kernel(Dev d, const uint8_t* __restrict__ halo, uint8_t* clear) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y * blockDim.y + threadIdx.y, z = blockIdx.z;
+    if (x >= d.nx || y >= d.ny) return;
+    bool any = x < 2 || y < 2 || z < 2 || x >= d.nx - 2 || y >= d.ny - 2 || z >= d.nz - 2;
+    for (int dz = -2; dz <= 2 && !any; ++dz)
+        for (int dy = -2; dy <= 2 && !any; ++dy) {
+            const uint8_t* row = halo + cidx(d, x, y + dy, z + dz);
+            any = row[-2] | row[-1] | row[0] | row[1] | row[2];
+        }
+    clear[cidx(d, x, y, z)] = any ? 0 : 1;
+}
+
 template <typename T>
 __global__ void solid_clear_kernel(int64_t n, const uint8_t* __restrict__ solid, const T* in, T* out) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -188,6 +202,13 @@ int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void*
     int64_t n = (int64_t)g->nx * g->ny * g->nz;
     dilate_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(d, solid, halo);
     return launch_status("dilate_kernel");
+}
+
+int ffx_clearance(const FfxGrid* g, const uint8_t* halo, uint8_t* clear, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && halo && clear && halo != clear, "ffx_clearance: invalid arguments");
+    Dev d = make_dev(*g);
+    clearance_kernel<<<cell_grid(g->nx, g->ny, g->nz), cell_block(), 0, as_stream(stream)>>>(d, halo, clear);
+    return launch_status("clearance_kernel");
 }
 
 int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const void* in, void* out,

@@ -265,6 +265,37 @@ struct GlobalSampler {
         f.dims(k, sx, sy, sz);
         return sample_face_half(f.ptr(k), sx, sy, sz, qx2, qy2, qz2);
     }
+    // sample_face_half of field k at the node whose doubled coordinates have the
+    // parities (HX, HY, HZ) and lower corner (ix, iy, iz), for a node where no
+    // coordinate is clamped (the corners ix..ix+HX etc. lie in the field): the
+    // same terms in the same order with the same power-of-two weight, with the
+    // parities known when compiling.
+    template <int HX, int HY, int HZ>
+    __device__ __forceinline__ float node(int k, int ix, int iy, int iz) const {
+        int sx, sy, sz;
+        f.dims(k, sx, sy, sz);
+        const auto* g = f.ptr(k);
+        using E = typename std::remove_cv<typename std::remove_pointer<decltype(g)>::type>::type;
+        constexpr float w = (HX ? 0.5f : 1.f) * (HY ? 0.5f : 1.f) * (HZ ? 0.5f : 1.f);
+        const int sxy = sx * sy;
+        const int b = iz * sxy + iy * sx + ix;
+        float v = 0.f;
+        v = v + w * Store<E>::ld(g, b);
+        if (HX) v = v + w * Store<E>::ld(g, b + 1);
+        if (HY) {
+            v = v + w * Store<E>::ld(g, b + sx);
+            if (HX) v = v + w * Store<E>::ld(g, b + sx + 1);
+        }
+        if (HZ) {
+            v = v + w * Store<E>::ld(g, b + sxy);
+            if (HX) v = v + w * Store<E>::ld(g, b + sxy + 1);
+            if (HY) {
+                v = v + w * Store<E>::ld(g, b + sxy + sx);
+                if (HX) v = v + w * Store<E>::ld(g, b + sxy + sx + 1);
+            }
+        }
+        return v;
+    }
     // min / max over the eight corners of field k around lower corner (bx, by,
     // bz), each index clamped to the field (correct_velocity_fused.glsl:19-24,
     // correct_scalar.glsl:12-17)
@@ -321,6 +352,10 @@ struct TileSampler {
         int sx, sy, sz;
         G.f.dims(k, sx, sy, sz);
         return tile::sample_half(w, k, G.f.ptr(k), sx, sy, sz, qx2, qy2, qz2);
+    }
+    template <int HX, int HY, int HZ>
+    __device__ __forceinline__ float node(int k, int ix, int iy, int iz) const {
+        return G.template node<HX, HY, HZ>(k, ix, iy, iz);
     }
     __device__ __forceinline__ void minmax8(int k, int bx, int by, int bz, float& lo, float& hi) const {
         // the window holds clamp(index) at every entry, so the clamped corners
@@ -422,16 +457,42 @@ __device__ __forceinline__ F3 start_velocity_s(const Dev& d, const S& smp, F3 p,
     }
 }
 
-// Midpoint backtrace through a sampler (the `backtrace` of the transport passes).
+// Velocity at the centre p of face (x, y, z) of face grid `axis`
+// (start_velocity_s at its doubled coordinates). On power-of-two grids, for a
+// face off the domain walls along its axis, no doubled coordinate is clamped
+// and the parities of every component's node are fixed by the axis: the U face
+// (2x, 2y+1, 2z+1) reads u at (x, y, z), v at (x-1..x, y..y+1, z) and w at
+// (x-1..x, y, z..z+1), and likewise for V and W faces.
+template <bool P2, class S>
+__device__ __forceinline__ F3 start_velocity_face(const Dev& d, const S& smp, F3 p, int axis, int x, int y, int z) {
+    if constexpr (P2) {
+        const int c = axis == 0 ? x : (axis == 1 ? y : z);
+        const int n = axis == 0 ? d.nx : (axis == 1 ? d.ny : d.nz);
+        if (c >= 1 && c <= n - 1) {
+            if (axis == 0)
+                return F3{smp.template node<0, 0, 0>(0, x, y, z), smp.template node<1, 1, 0>(1, x - 1, y, z),
+                          smp.template node<1, 0, 1>(2, x - 1, y, z)};
+            if (axis == 1)
+                return F3{smp.template node<1, 1, 0>(0, x, y - 1, z), smp.template node<0, 0, 0>(1, x, y, z),
+                          smp.template node<0, 1, 1>(2, x, y - 1, z)};
+            return F3{smp.template node<1, 0, 1>(0, x, y, z - 1), smp.template node<0, 1, 1>(1, x, y, z - 1),
+                      smp.template node<0, 0, 0>(2, x, y, z)};
+        }
+    }
+    return start_velocity_s<P2>(d, smp, p, 2 * x + (axis != 0), 2 * y + (axis != 1), 2 * z + (axis != 2));
+}
+
+// Midpoint backtrace through a sampler (the `backtrace` of the transport
+// passes); `clear`: the start point's own cell is clear (home_clear).
 template <bool MASK, bool P2, class S>
 __device__ __forceinline__ F3 backtrace_s(const Dev& d, const S& smp, const uint8_t* solid, const uint8_t* halo, F3 p,
-                                          F3 v0, float dt) {
+                                          F3 v0, float dt, bool clear = false) {
     const float s = 0.5f * dt;
     F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
-    if (MASK) mid = clip_solid_trace<P2>(d, solid, halo, p, mid);
+    if (MASK) mid = clip_from<P2>(d, solid, halo, clear, p, mid);
     const F3 vm = velocity_s<P2>(d, smp, mid);
     F3 dep = {p.x - dt * vm.x, p.y - dt * vm.y, p.z - dt * vm.z};
-    if (MASK) dep = clip_solid_trace<P2>(d, solid, halo, p, dep);
+    if (MASK) dep = clip_from<P2>(d, solid, halo, clear, p, dep);
     return dep;
 }
 

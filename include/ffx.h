@@ -58,6 +58,9 @@ typedef struct FfxSolids {
     const uint8_t* halo;  /* nx*ny*nz dilated mask (ffx_dilate_mask) */
     const float* wall[3]; /* moving colliders: velocity of every wall and solid face
                              (face grids, ffx_moving_walls); NULL = 0 (static walls) */
+    const uint8_t* clear; /* optional, with a mask: nx*ny*nz clearance (ffx_clearance); the
+                             transport passes skip the collider tests of traces that start
+                             in a clear cell and stay within 0.75 cells (same results) */
 } FfxSolids;
 
 /* Moving colliders per solver (the reference's wall table holds 8). */
@@ -108,6 +111,14 @@ int ffx_raster_colliders(const FfxGrid* g, const double extent[3], int count,
 /* 3x3x3 dilation with out-of-domain = solid (precomputes solidHalo,
  * shaders/solid_boundary.glsl:39-44). */
 int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void* stream);
+
+/* Clearance of a mask: clear[c] = 1 where no cell within Chebyshev distance 2
+ * of c is set in `halo` (ffx_dilate_mask of the mask) or lies outside the grid,
+ * i.e. no solid or outside cell lies within distance 3 of c; else 0. An
+ * extension with no reference counterpart: it lets the transport passes skip
+ * the collider tests (solid_boundary.glsl, correct_*.glsl) where they cannot
+ * change the result. One-time work per collider layout. */
+int ffx_clearance(const FfxGrid* g, const uint8_t* halo, uint8_t* clear, void* stream);
 /* out = solid ? 0 : in; replaces shaders/solid_clear.glsl. */
 int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const void* in,
                     void* out, void* stream);

@@ -32,7 +32,7 @@ def test_library_loads_and_exports_every_symbol():
 def test_struct_layouts_match_the_header():
     # sizes of the C structs (natural alignment, 64-bit pointers)
     assert ctypes.sizeof(N.FfxGrid) == 36
-    assert ctypes.sizeof(N.FfxSolids) == 16 + 24   # solid, halo, wall[3]
+    assert ctypes.sizeof(N.FfxSolids) == 16 + 24 + 8   # solid, halo, wall[3], clear
     assert ctypes.sizeof(N.FfxSources) == 4 * (2 + 3 + 3 + 1 + 3 + 1 + 128)
     assert ctypes.sizeof(N.FfxScalarChannel) == 4 * 8 + 4 * 5 + 4
     assert ctypes.sizeof(N.FfxGraphLevel) == 12 + 4 + 8 + 8 + 12 + 4 + 8   # ..., w[3], pad, links

@@ -1,0 +1,121 @@
+"""The clearance field (ffx_clearance) and the transport passes' clear form.
+
+* The field equals its definition computed on the host: 1 exactly where no
+  solid cell and no cell outside the grid lies within Chebyshev distance 3.
+* Steps that use the field give the fields of the same steps without it, bit
+  for bit: power-of-two and other grids, FP32 and BF16 storage, emitters,
+  static and moving colliders, and traces both within the clear form's 0.75
+  cells and far beyond it (which take the full collider tests).
+"""
+import numpy as np
+import pytest
+import torch
+from scipy.ndimage import maximum_filter
+
+from tests.gpu_helpers import dev
+
+pytestmark = pytest.mark.gpu
+
+
+def _expected_clear(solid):
+    padded = np.pad(solid.astype(np.uint8), 3, constant_values=1)      # outside counts as solid
+    near = maximum_filter(padded, size=7, mode='constant', cval=1)[3:-3, 3:-3, 3:-3]
+    return (near == 0).astype(np.uint8)
+
+
+@pytest.mark.parametrize('n', [48, 64])
+def test_clearance_matches_its_definition(n):
+    import bench
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    D = dev()
+    grid, s, colliders, _, _ = bench.scene(n, 'FP32', 1)
+    sv = DenseProjectedSmoke(grid, s, D, colliders=colliders)
+    torch.cuda.synchronize()
+    solid = sv.solids.mask.cpu().numpy() != 0
+    clear = sv.solids.clear.cpu().numpy()
+    assert np.array_equal(clear, _expected_clear(solid))
+    assert 0 < clear.sum() < clear.size
+    sv.close()
+
+
+def _without_clear(sv):
+    for owner in (sv, sv.detail, sv.projector):
+        owner._solids.clear = None
+
+
+def _pair(n, storage, variant, amp, seed=4):
+    import bench
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    D = dev()
+    out = []
+    for use_clear in (True, False):
+        grid, s, colliders, emitters, noise = bench.scene(n, storage, seed, **bench.VARIANTS[variant])
+        sv = DenseProjectedSmoke(grid, s, D, colliders=colliders)
+        if not use_clear:
+            _without_clear(sv)
+        sv.upload(torch.zeros(grid.cells))
+        sv.upload_temperature(torch.zeros(grid.cells))
+        sv.upload_velocity([torch.as_tensor(v * (amp / 1e-3)) for v in noise])
+        out.append(sv)
+    return out, emitters
+
+
+def _fields(sv):
+    torch.cuda.synchronize()
+    return [sv.density, sv.temperature, sv.projector.pressure, *sv._velocity]
+
+
+@pytest.mark.parametrize('n,storage,variant,amp', [
+    (64, 'FP32', 'plain', 1e-3),     # power-of-two grid: traces well inside 0.75 cells
+    (64, 'BF16', 'fast', 0.3),       # up to ~0.4 cells per step
+    (64, 'FP32', 'fast', 2.0),       # ~2.5 cells: the full collider tests
+    (48, 'FP32', 'plain', 0.3),      # h = 1/48: the clear form's rounding-exact fast values
+    (48, 'BF16', 'fast', 2.0),
+])
+def test_clear_form_is_bit_identical(n, storage, variant, amp):
+    (a, b), em = _pair(n, storage, variant, amp)
+    for k in range(4):
+        a.step(0.02, sources=em)
+        b.step(0.02, sources=em)
+        for x, y in zip(_fields(a), _fields(b)):
+            assert torch.equal(x, y), (n, storage, variant, amp, k)
+    a.close()
+    b.close()
+
+
+def test_clear_form_with_a_moving_collider():
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    from fluxfx_b200.backend.solid_multigrid import SolidMultigridProjector
+    from fluxfx_b200.physics.collision import primitive
+    from fluxfx_b200.physics.config import GridSpec
+    from fluxfx_b200.physics.pressure import PressureSettings
+    D = dev()
+    shape = (48, 40, 56)
+    grid = GridSpec(shape)
+    hx = 1.0 / shape[0]
+    s = PressureSettings(velocity_advection='MACCORMACK', scalar_advection='MACCORMACK', moving_colliders=True,
+                         thermal_lift=1.0, density_weight=0.05, source_center=(0.5, 0.5, 0.2), source_radius=0.1,
+                         pressure_tolerance=1e-4, pressure_max_cycles=100, vorticity_strength=0.3)
+    pose = lambda k: (primitive('SPHERE', (0.3 + 0.5 * hx * k, 0.5, 0.6), (0.15, 0.15, 0.15)),)
+    rng = np.random.default_rng(8)
+    vel = [torch.as_tensor((rng.uniform(-1, 1, (fs[2], fs[1], fs[0])) * 0.3).astype(np.float32))
+           for fs in grid.face_shapes]
+    solvers = []
+    for use_clear in (True, False):
+        sv = DenseProjectedSmoke(grid, s, D, projector_class=SolidMultigridProjector, colliders=pose(0))
+        if not use_clear:
+            _without_clear(sv)
+        sv.upload_velocity(vel)
+        solvers.append(sv)
+    a, b = solvers
+    for k in range(5):
+        for sv in solvers:
+            sv.move_colliders(pose(k + 1), 0.02)
+            sv.step(0.02)
+        torch.cuda.synchronize()
+        assert torch.equal(a.solids.clear, torch.as_tensor(_expected_clear(a.solids.mask.cpu().numpy() != 0),
+                                                           device=a.solids.clear.device)), k
+        for x, y in zip([a.density, a.temperature, *a._velocity], [b.density, b.temperature, *b._velocity]):
+            assert torch.equal(x, y), k
+    a.close()
+    b.close()
