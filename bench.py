@@ -784,7 +784,9 @@ def run_fire(args):
     f_time, f_cycles, _ = run(fast, dts)
     clock_info = clocks.stop()
     err = errors(fast)
-    f_rel = [s.measure_projection()['rel_div_inf'] for s, _ in fast]
+    f_metrics = [s.measure_projection() for s, _ in fast]
+    f_rel = [m['rel_div_inf'] for m in f_metrics]
+    f_rel32 = [m.get('rel_div_inf_fp32', m['rel_div_inf']) for m in f_metrics]
     for s, _ in fast:
         s.close()
     cells = 192 * 192 * 320 * domains
@@ -804,7 +806,10 @@ def run_fire(args):
                               "rel_error_vs_plain_fp32": err32},
         "speedup_vs_plain": p_time / f_time,
         "final_rel_div_inf_max": max(f_rel),
-        "final_rel_div_note": "measured on the stored faces (BF16 storage rounds the projected velocity)",
+        "final_rel_div_inf_fp32_max": max(f_rel32),
+        "final_rel_div_note": "final_rel_div_inf_max is measured on the stored faces (BF16 storage rounds the "
+                              "projected velocity); final_rel_div_inf_fp32_max on the projection's FP32 result "
+                              "before rounding, the solve's own tolerance measure",
         "rel_error_vs_plain_fp32": err, "clocks": clock_info,
     }
     print(json.dumps(line), flush=True)

@@ -181,6 +181,10 @@ _PROTOTYPES = {
                                           P(vp), vp, vp]),
     'ffx_advect_scalars_dt': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, C.c_int,
                                         P(FfxSources), C.c_int, P(FfxScalarChannel), vp, vp, vp]),
+    'ffx_scalar_reverse_ok': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, C.c_float, vp, C.c_int,
+                                        vp, vp, vp, vp, vp]),
+    'ffx_advect_scalars_ok': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, C.c_float, vp, C.c_int,
+                                        P(FfxSources), C.c_int, P(FfxScalarChannel), vp, vp, vp, vp]),
     'ffx_next_dt': (C.c_int, [vp, vp, vp, C.c_double, C.c_double, C.c_double, vp]),
     'ffx_add': (C.c_int, [i64, vp, vp, vp, vp]),
     'ffx_bricks_create': (C.c_int, [C.c_uint32, P(vp)]),

@@ -33,6 +33,7 @@ class DetailPasses:
         self.reuse_traces = True
         self.face_trace = None
         self.cell_trace = None
+        self.cell_ok = None       # the reverse pass's correction decisions (uint8 per cell)
         self._face_reuse = N.face_starts_match(grid.shape, grid.extent)
 
     @property
@@ -41,7 +42,8 @@ class DetailPasses:
         scalar = sum(t.numel() for t in (self.predictors or []) + (self.reverses or [])) * size
         faces = size * sum(prod(s) for s in self.grid.face_shapes) if self.face_predictor is not None else 0
         traces = sum(4 * t.numel() for t in (self.face_trace or [])) + (
-            4 * self.cell_trace.numel() if self.cell_trace is not None else 0)
+            4 * self.cell_trace.numel() if self.cell_trace is not None else 0) + (
+            self.cell_ok.numel() if self.cell_ok is not None else 0)
         return scalar + faces + traces + (self.curl.numel() * 4 if self.curl is not None else 0)
 
     def _ensure_scalar(self, count):
@@ -65,7 +67,20 @@ class DetailPasses:
         if self.reuse_traces and self.cell_trace is None:
             self.cell_trace = torch.empty(3 * prod(self.grid.shape), dtype=torch.float32, device=self.device.device)
         trace = ptr(self.cell_trace) if self.reuse_traces else None
-        if dt_device is not None:
+        if self.reuse_traces:
+            # the reverse pass also decides the final pass's corrections (cell_decisions)
+            if self.cell_ok is None:
+                nx, ny, nz = self.grid.shape
+                self.cell_ok = torch.empty((nz, ny, nx), dtype=torch.uint8, device=self.device.device)
+            if dt_device is not None:
+                self.device.call('ffx_scalar_transport_dt', gp, sp, self._storage, *vel, dt_device, 1.0, count, ins,
+                                 preds, trace, s)
+            else:
+                self.device.call('ffx_scalar_transport_trace', gp, sp, self._storage, *vel, dt, count, ins, preds,
+                                 trace, s)
+            self.device.call('ffx_scalar_reverse_ok', gp, sp, self._storage, *vel, 0.0 if dt_device is not None
+                             else -dt, dt_device, count, preds, revs, trace, ptr(self.cell_ok), s)
+        elif dt_device is not None:
             self.device.call('ffx_scalar_transport_dt', gp, sp, self._storage, *vel, dt_device, 1.0, count, ins, preds,
                              trace, s)
             self.device.call('ffx_scalar_transport_dt', gp, sp, self._storage, *vel, dt_device, -1.0, count, preds,
@@ -99,6 +114,10 @@ class DetailPasses:
 
     def cell_traces(self):
         return ptr(self.cell_trace) if (self.reuse_traces and self.cell_trace is not None) else None
+
+    def cell_decisions(self):
+        """The reverse pass's correction decisions (ffx_scalar_reverse_ok), or NULL."""
+        return ptr(self.cell_ok) if (self.reuse_traces and self.cell_ok is not None) else None
 
     def confine(self, fields, outputs, dt, strength, limit):
         """Vorticity confinement (``backend/detail.py:39-49``): cell curl

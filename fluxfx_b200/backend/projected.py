@@ -320,9 +320,17 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             chans.append(N.FfxScalarChannel(ptr(fields[2]), ptr(preds[2]), ptr(revs[2]), ptr(self.combustion.spare),
                                             s.fuel_source_rate, 0.0, -1.0, 2, 0))
         arr = (N.FfxScalarChannel * len(chans))(*chans)
-        dev.call('ffx_advect_scalars_dt' if dtp is not None else 'ffx_advect_scalars_trace', gp, sp, self._storage,
-                 *[ptr(f) for f in self._velocity], dtp if dtp is not None else dt, int(corrected_s), C.byref(src),
-                 len(chans), arr, ptr(self._maxima), self.detail.cell_traces() if corrected_s else None, st)
+        decisions = self.detail.cell_decisions() if corrected_s else None
+        if decisions is not None:
+            # the reverse pass decided the corrections (ffx_scalar_reverse_ok)
+            dev.call('ffx_advect_scalars_ok', gp, sp, self._storage, *[ptr(f) for f in self._velocity],
+                     0.0 if dtp is not None else dt, dtp, int(corrected_s), C.byref(src), len(chans), arr,
+                     ptr(self._maxima), self.detail.cell_traces(), decisions, st)
+        else:
+            dev.call('ffx_advect_scalars_dt' if dtp is not None else 'ffx_advect_scalars_trace', gp, sp,
+                     self._storage, *[ptr(f) for f in self._velocity], dtp if dtp is not None else dt,
+                     int(corrected_s), C.byref(src), len(chans), arr, ptr(self._maxima),
+                     self.detail.cell_traces() if corrected_s else None, st)
         self._mark('scalar_transport')
         self._front, self._back = self._back, self._front
         self._temperature, self._temperature_back = self._temperature_back, self._temperature

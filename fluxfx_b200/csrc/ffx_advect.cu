@@ -315,7 +315,9 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
                 // expf(+-0) = 1, so bl = 0 and the blend is value * 1 + jet * 0
                 value = value + comp(S.jet, axis) * 0.f;
             }
-        } else if (S.count > 0) {
+        } else if (S.count > 0 && !outside(S.any, p)) {
+            // (outside every row's reach all weights are +0: total stays +-0
+            // and the blend below is not taken, so the value is unchanged)
             float total = 0.f, target = 0.f;
             for (int i = 0; i < S.count; ++i) {
                 float rate = S.table[16 * i + 7] * table_weight(S, i, p);
@@ -524,7 +526,32 @@ struct ScalarXport {
     T* out[3];
     float* dep;       // optional: departure points (three planes of n floats) for the final pass
     int n;
+    // optional, on the reverse pass: the forward pass's departure points (read)
+    // and the final pass's correction decision per cell (written)
+    const float* fdep;
+    uint8_t* ok;
 };
+
+// correct_scalar.glsl:1-21's conditions for the MacCormack correction of a
+// cell: departure and arrival points at least half a cell inside the domain
+// and, with colliders, safe_solid_correction at start, departure, midpoint and
+// arrival.
+template <bool MASK, bool P2>
+__device__ __forceinline__ bool scalar_correction_ok(const Dev& d, const uint8_t* solid, const uint8_t* halo,
+                                                     bool clear, F3 p, F3 dep, F3 mid2, F3 arr) {
+    const float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
+    const float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
+    bool ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
+                dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
+                arr.y > hb[1] || arr.z > hb[2]);
+    if (MASK && ok) ok = safe_correction_from<P2>(d, solid, halo, clear, p, dep, mid2, arr);
+    return ok;
+}
+
+__device__ __forceinline__ bool same_bits(F3 a, F3 b) {
+    return __float_as_uint(a.x) == __float_as_uint(b.x) && __float_as_uint(a.y) == __float_as_uint(b.y) &&
+           __float_as_uint(a.z) == __float_as_uint(b.z);
+}
 
 // Velocity faces as sampler fields 0..2, the scalar fields C[0..2] as 3..5.
 template <typename T>
@@ -544,10 +571,31 @@ __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, i
     }
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
-    F3 dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P), clear);
+    F3 dep;
+    if (P.ok) {
+        // backtrace_s, keeping the unclipped midpoint and departure point: with
+        // the reverse step -dt they are the final pass's forward midpoint
+        // p + (dt/2) v0 and, where the midpoint was not clipped, its arrival
+        // point p + dt v(mid) (x - (-a) b == x + a b exactly), so the final
+        // pass's correction test is decided here
+        const float dtr = step_dt(P), s = 0.5f * dtr;
+        const F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
+        const F3 midc = MASK ? clip_from<P2>(d, P.solid, P.halo, clear, p, mid) : mid;
+        const F3 vm = velocity_s<P2>(d, smp, midc);
+        F3 arr = {p.x - dtr * vm.x, p.y - dtr * vm.y, p.z - dtr * vm.z};
+        dep = MASK ? clip_from<P2>(d, P.solid, P.halo, clear, p, arr) : arr;
+        if (!same_bits(midc, mid)) {
+            const F3 vm2 = velocity_s<P2>(d, smp, mid);
+            arr = {p.x - dtr * vm2.x, p.y - dtr * vm2.y, p.z - dtr * vm2.z};
+        }
+        const F3 fdep = {__ldg(P.fdep + i), __ldg(P.fdep + i + P.n), __ldg(P.fdep + i + 2 * P.n)};
+        P.ok[i] = scalar_correction_ok<MASK, P2>(d, P.solid, P.halo, clear, p, fdep, mid, arr) ? 1 : 0;
+    } else {
+        dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P), clear);
+    }
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
-    const auto S = smp.template closed<MASK>(P.solid, qx, qy, qz);
+    const auto S = smp.template closed<MASK>(P.solid, qx, qy, qz, clear && near_start(d, p, dep));
     for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, smp.template apply<MASK>(3 + c, S));
     if (P.dep) {
         P.dep[i] = dep.x;
@@ -594,6 +642,7 @@ struct ScalarFinal {
     float* maxima;
     const float* dep;   // optional: the forward predictor's departure points (same start point, reused)
     int n;
+    const uint8_t* ok;  // optional, with dep: the correction decisions of the reverse pass
     SrcDev src;
 };
 
@@ -610,46 +659,52 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
     }
     const float dt = step_dt(P);
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
-    F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
     // the forward predictor traced this cell's start point with the same
     // velocity: its departure point, and in FP32 storage its samples, are this pass's
     const bool reuse = P.corrected && P.dep != nullptr;
+    // the reverse pass decided the correction (scalar_transport_cell with ok)
+    const bool decided = reuse && P.ok != nullptr;
+    F3 v0 = {0.f, 0.f, 0.f};
+    if (!decided) v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
     F3 dep;
     if (reuse) dep = {__ldg(P.dep + i), __ldg(P.dep + i + P.n), __ldg(P.dep + i + 2 * P.n)};
     else dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, clear);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     bool ok = false;
-    if (P.corrected) {
+    if (decided) {
+        ok = __ldg(P.ok + i) != 0;
+    } else if (P.corrected) {
         // correct_scalar.glsl:1-21
         float s = 0.5f * dt;
         F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
         F3 vm2 = velocity_s<P2>(d, smp, mid2);
         F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
-        float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
-        float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
-        ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
-               dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
-               arr.y > hb[1] || arr.z > hb[2]);
-        if (MASK && ok) ok = safe_correction_from<P2>(d, P.solid, P.halo, clear, p, dep, mid2, arr);
+        ok = scalar_correction_ok<MASK, P2>(d, P.solid, P.halo, clear, p, dep, mid2, arr);
     }
     // lower corner of the departure cell (the clamp bounds: its 8 corners clamped to the grid)
     const int bx = ok ? (int)floorf(qx) : 0, by = ok ? (int)floorf(qy) : 0, bz = ok ? (int)floorf(qz) : 0;
     const SrcDev& S = P.src;
     // the semi-Lagrangian sample (the stored predictor value when it is the same)
     const bool stored = reuse && sizeof(T) == 4;
+    const bool none = S.count > 0 && outside(S.any, p);
+    // (where the correction applies it replaces the semi-Lagrangian value, which
+    // is then not formed)
     decltype(smp.template closed<MASK>(P.solid, qx, qy, qz)) St;
-    if (!stored) St = smp.template closed<MASK>(P.solid, qx, qy, qz);
+    if (!stored && !ok) St = smp.template closed<MASK>(P.solid, qx, qy, qz, clear && near_start(d, p, dep));
     for (int c = 0; c < P.count; ++c) {
         const Channel<T>& C = P.ch[c];
-        float value = stored ? Store<T>::ld(C.pred, i) : smp.template apply<MASK>(3 + c, St);
+        float value;
         if (ok) {
             float val = Store<T>::ld(C.pred, i) + 0.5f * (Store<T>::ld(C.field, i) - Store<T>::ld(C.rev, i));
             float lo, hi;
             smp.minmax8(3 + c, bx, by, bz, lo, hi);
             value = fminf(fmaxf(val, lo), hi);
+        } else {
+            value = stored ? Store<T>::ld(C.pred, i) : smp.template apply<MASK>(3 + c, St);
         }
-        value = value * expf(-C.decay * dt);
+        // expf(-0) = 1 and v * 1 = v: no decay leaves the value as it is
+        if (C.decay != 0.f) value = value * expf(-C.decay * dt);
         if (S.count < 0) {
             float w = single_weight(S, p);
             value = C.target >= 0.f ? fmaxf(value, C.target * w) : value + dt * C.rate * w;
@@ -658,7 +713,8 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
             for (int k = 0; k < S.count; ++k) {
                 const float* row = S.table + 16 * k;
                 float r = C.channel == 0 ? row[11] : (C.channel == 1 ? row[12] : row[15]);
-                float w = table_weight(S, k, p);
+                // table_weight is +0 outside every row's reach
+                float w = none ? 0.f : table_weight(S, k, p);
                 bool is_target = (C.channel == 0 && row[13] > 0.5f) || (C.channel == 1 && C.table_target);
                 if (is_target) tgt = fmaxf(tgt, r * w);
                 else value = value + dt * r * w;
@@ -1003,7 +1059,8 @@ int ffx_buoyancy(const FfxGrid* g, int storage, const void* w_in, const void* de
 
 static int scalar_transport_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                                  const void* w, float dt, const float* dtp, float sign, int count,
-                                 const void* const* in, void* const* out, float* dep, void* stream) {
+                                 const void* const* in, void* const* out, float* dep, void* stream,
+                                 const float* fdep = nullptr, uint8_t* ok = nullptr) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 && in &&
                 out, "ffx_scalar_transport: invalid arguments");
     for (int c = 0; c < count; ++c)
@@ -1028,6 +1085,8 @@ static int scalar_transport_impl(const FfxGrid* g, const FfxSolids* s, int stora
         }
         P.dep = dep;
         P.n = g->nx * g->ny * g->nz;
+        P.fdep = fdep;
+        P.ok = ok;
         if (g_tiling) {
             const int zc = FFX_TILE_ZCHUNK;
             FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
@@ -1057,10 +1116,18 @@ int ffx_scalar_transport(const FfxGrid* g, const FfxSolids* s, int storage, cons
     return ffx_scalar_transport_trace(g, s, storage, u, v, w, dt, count, in, out, nullptr, stream);
 }
 
+int ffx_scalar_reverse_ok(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                          const void* w, float dt, const float* dtp, int count, const void* const* in,
+                          void* const* out, const float* dep, uint8_t* ok, void* stream) {
+    FFX_REQUIRE(dep && ok, "ffx_scalar_reverse_ok: NULL departure points or decisions");
+    FFX_REQUIRE(dtp || dt < 0.f, "ffx_scalar_reverse_ok: the reverse pass runs with a negative time step");
+    return scalar_transport_impl(g, s, storage, u, v, w, dt, dtp, -1.f, count, in, out, nullptr, stream, dep, ok);
+}
+
 static int advect_scalars_impl(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
                                const void* w, float dt, const float* dtp, int corrected, const FfxSources* src,
                                int count, const FfxScalarChannel* channels, float* maxima, const float* dep,
-                               void* stream) {
+                               void* stream, const uint8_t* ok = nullptr) {
     FFX_REQUIRE(grid_ok(g) && storage_ok(storage) && solids_ok(s) && u && v && w && count >= 1 && count <= 3 &&
                 channels && src && src->count <= 8, "ffx_advect_scalars: invalid arguments");
     for (int c = 0; c < count; ++c) {
@@ -1107,6 +1174,7 @@ static int advect_scalars_impl(const FfxGrid* g, const FfxSolids* s, int storage
         P.maxima = maxima;
         P.dep = corrected ? dep : nullptr;
         P.n = g->nx * g->ny * g->nz;
+        P.ok = corrected ? ok : nullptr;
         const float extent[3] = {g->ex, g->ey, g->ez};
         P.src = make_src(src, extent);
         if (g_tiling) {
@@ -1140,6 +1208,15 @@ int ffx_advect_scalars(const FfxGrid* g, const FfxSolids* s, int storage, const 
                        const FfxScalarChannel* channels, float* maxima, void* stream) {
     return ffx_advect_scalars_trace(g, s, storage, u, v, w, dt, corrected, src, count, channels, maxima, nullptr,
                                     stream);
+}
+
+int ffx_advect_scalars_ok(const FfxGrid* g, const FfxSolids* s, int storage, const void* u, const void* v,
+                          const void* w, float dt, const float* dtp, int corrected, const FfxSources* src,
+                          int count, const FfxScalarChannel* channels, float* maxima, const float* dep,
+                          const uint8_t* ok, void* stream) {
+    FFX_REQUIRE(!corrected || (dep && ok), "ffx_advect_scalars_ok: NULL departure points or decisions");
+    return advect_scalars_impl(g, s, storage, u, v, w, dt, dtp, corrected, src, count, channels, maxima, dep,
+                               stream, ok);
 }
 
 int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt, const float base[3], float angular,

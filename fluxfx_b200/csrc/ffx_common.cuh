@@ -579,6 +579,7 @@ struct SrcDev {
     float radius, coupling;
     float table[128];
     Reach reach[9];   // table rows 0..7, then the single emitter
+    Reach any;        // a box holding the reach of every table row in use
 };
 
 inline SrcDev make_src(const FfxSources* s, const float* extent) {
@@ -597,6 +598,19 @@ inline SrcDev make_src(const FfxSources* s, const float* extent) {
     }
     const float c[3] = {r.center.x, r.center.y, r.center.z}, st[3] = {r.start.x, r.start.y, r.start.z};
     r.reach[8] = make_reach(c, st, r.radius, extent);
+    // the union of the rows' boxes (NaN if any bound is NaN: never outside);
+    // a point outside it is outside every row's box
+    for (int a = 0; a < 3; ++a) {
+        float lo = INFINITY, hi = -INFINITY;
+        bool nan = false;
+        for (int i = 0; i < r.count && i < 8; ++i) {
+            nan = nan || std::isnan(r.reach[i].lo[a]) || std::isnan(r.reach[i].hi[a]);
+            lo = std::fmin(lo, r.reach[i].lo[a]);
+            hi = std::fmax(hi, r.reach[i].hi[a]);
+        }
+        r.any.lo[a] = nan ? NAN : lo;
+        r.any.hi[a] = nan ? NAN : hi;
+    }
     return r;
 }
 

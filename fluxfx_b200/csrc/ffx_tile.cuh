@@ -152,9 +152,11 @@ struct ClosedStencil {
     float total;          // MASK: sum of the fluid corners' weights
 };
 
+// fluid: every corner is known to be fluid (a departure point near a clear
+// cell's centre: its corners lie within one cell of it), so the mask is not read.
 template <bool MASK>
 __device__ __forceinline__ ClosedStencil closed_stencil(const Dev& d, const uint8_t* solid, float qx, float qy,
-                                                        float qz) {
+                                                        float qz, bool fluid = false) {
     ClosedStencil S;
     float bx = floorf(qx), by = floorf(qy), bz = floorf(qz);
     S.fx = qx - bx;
@@ -175,7 +177,7 @@ __device__ __forceinline__ ClosedStencil closed_stencil(const Dev& d, const uint
 #pragma unroll
         for (int k = 0; k < 8; ++k) {
             const int c = S.rows[k >> 1] + ((k & 1) ? S.x1 : S.x0);
-            if (__ldg(solid + c)) continue;
+            if (!fluid && __ldg(solid + c)) continue;
             const float wz = (k & 4) ? S.fz : 1.f - S.fz, wy = (k & 2) ? S.fy : 1.f - S.fy,
                         wx = (k & 1) ? S.fx : 1.f - S.fx;
             S.fluid |= 1u << k;
@@ -322,8 +324,9 @@ struct GlobalSampler {
         }
     }
     template <bool MASK>
-    __device__ __forceinline__ ClosedStencil closed(const uint8_t* solid, float qx, float qy, float qz) const {
-        return closed_stencil<MASK>(f.d, solid, qx, qy, qz);
+    __device__ __forceinline__ ClosedStencil closed(const uint8_t* solid, float qx, float qy, float qz,
+                                                    bool fluid = false) const {
+        return closed_stencil<MASK>(f.d, solid, qx, qy, qz, fluid);
     }
     template <bool MASK>
     __device__ __forceinline__ float apply(int k, const ClosedStencil& S) const {
@@ -383,9 +386,10 @@ struct TileSampler {
         int s0, s1;     // slice offset + in-slice offset of the lower corner (z0 and z1 slices); s0 < 0: global
     };
     template <bool MASK>
-    __device__ __forceinline__ Stencil closed(const uint8_t* solid, float qx, float qy, float qz) const {
+    __device__ __forceinline__ Stencil closed(const uint8_t* solid, float qx, float qy, float qz,
+                                              bool fluid = false) const {
         Stencil t;
-        t.S = closed_stencil<MASK>(G.f.d, solid, qx, qy, qz);
+        t.S = closed_stencil<MASK>(G.f.d, solid, qx, qy, qz, fluid);
         const int ix = floor_int(qx), iy = floor_int(qy), iz = floor_int(qz);
         if (tile::inside(w, ix, iy, iz)) {
             const int off = (iy - w.wy) * tile::kPitch + (ix - w.wx);

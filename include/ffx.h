@@ -233,6 +233,26 @@ int ffx_advect_scalars_dt(const FfxGrid* g, const FfxSolids* s, int storage,
                           const void* u, const void* v, const void* w, const float* dt, int corrected,
                           const FfxSources* src, int count, const FfxScalarChannel* channels,
                           float* maxima, const float* dep, void* stream);
+/* The reverse scalar pass (ffx_scalar_transport with the forward pass's step
+ * negated: `dt` < 0, or dtp != NULL: minus the device float *dtp) that also
+ * decides the final pass's MacCormack correction of every fluid cell
+ * (correct_scalar.glsl's conditions): its backtrace with -dt starts with the
+ * final pass's forward midpoint and arrival point, so ok[c] = 1 exactly where
+ * ffx_advect_scalars would correct cell c. `dep`: the forward pass's departure
+ * points (ffx_scalar_transport_trace / _dt). An extension with no reference
+ * counterpart; results equal those of the passes it replaces. */
+int ffx_scalar_reverse_ok(const FfxGrid* g, const FfxSolids* s, int storage,
+                          const void* u, const void* v, const void* w, float dt, const float* dtp,
+                          int count, const void* const* in, void* const* out, const float* dep,
+                          uint8_t* ok, void* stream);
+/* The final scalar pass reading those decisions (and the forward departure
+ * points) instead of tracing forward again: the result of ffx_advect_scalars_trace
+ * (dtp == NULL) or ffx_advect_scalars_dt (dtp != NULL) with the same arguments. */
+int ffx_advect_scalars_ok(const FfxGrid* g, const FfxSolids* s, int storage,
+                          const void* u, const void* v, const void* w, float dt, const float* dtp,
+                          int corrected, const FfxSources* src, int count,
+                          const FfxScalarChannel* channels, float* maxima, const float* dep,
+                          const uint8_t* ok, void* stream);
 /* P0.2 open-boundary transport in an analytic flow; replaces shaders/advect.glsl. */
 int ffx_advect_open(const FfxGrid* g, int storage, const void* in, float dt,
                     const float base[3], float angular, const float center[3], float radius,

@@ -47,3 +47,39 @@ def test_velocity_trace_reuse_is_bit_identical(shape, extent, matches):
     assert reused == matches
     for x, y in zip(a, b):
         assert torch.equal(x, y), float((x - y).abs().max())
+
+
+@pytest.mark.parametrize('storage', ['FP32', 'BF16'])
+@pytest.mark.parametrize('device_dt, amp', [(False, 0.3), (False, 2.0), (True, 0.3)])
+def test_scalar_decisions_of_the_reverse_pass_are_bit_identical(storage, device_dt, amp):
+    """The final scalar pass reading the reverse pass's correction decisions
+    (ffx_scalar_reverse_ok, ffx_advect_scalars_ok) gives the fields of the final
+    pass that traces forward again, bit for bit: the collider scene with traces
+    of under half a cell and of about 2.5 cells (midpoints clipped at the
+    colliders), host and device time steps, FP32 and BF16 storage."""
+    import bench
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    D = dev()
+    runs = []
+    for decide in (True, False):
+        grid, s, colliders, emitters, noise = bench.scene(64, storage, 2, **bench.VARIANTS['fast'])
+        sv = DenseProjectedSmoke(grid, s, D, colliders=colliders)
+        if not decide:
+            sv.detail.cell_decisions = lambda: None
+        sv.upload(torch.zeros(grid.cells))
+        sv.upload_temperature(torch.zeros(grid.cells))
+        sv.upload_velocity([torch.as_tensor(v * (amp / 1e-3)) for v in noise])
+        runs.append((sv, emitters))
+    for k in range(4):
+        for sv, em in runs:
+            if device_dt:
+                sv.step_cfl(0.5, 0.02, sources=em)
+            else:
+                sv.step(0.02, sources=em)
+        torch.cuda.synchronize()
+        (a, _), (b, _) = runs
+        assert a.detail.cell_decisions() is not None
+        for x, y in zip([a.density, a.temperature, *a._velocity], [b.density, b.temperature, *b._velocity]):
+            assert torch.equal(x, y), (storage, device_dt, amp, k)
+    for sv, _ in runs:
+        sv.close()
