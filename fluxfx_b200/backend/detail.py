@@ -100,7 +100,9 @@ class DetailPasses:
         if self.face_predictor is None:
             self.face_predictor = [self.device.texture(s, dtype=self.dtype) for s in self.grid.face_shapes]
         if self.reuse_traces and self._face_reuse and self.face_trace is None:
-            self.face_trace = [torch.empty(3 * prod(s), dtype=torch.float32, device=self.device.device)
+            # x, y, z of each departure point, plus (16-bit storage) the unrounded sample
+            planes = 3 if self.dtype == torch.float32 else 4
+            self.face_trace = [torch.empty(planes * prod(s), dtype=torch.float32, device=self.device.device)
                                for s in self.grid.face_shapes]
         name, step = ('ffx_face_predictor_dt', dt_device) if dt_device is not None else ('ffx_face_predictor_trace', dt)
         self.device.call(name, C.byref(self._g), C.byref(self._solids), self._storage, *[ptr(f) for f in fields],

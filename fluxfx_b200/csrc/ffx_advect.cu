@@ -199,6 +199,9 @@ __device__ __forceinline__ void face_predictor_face(const PredParams<T>& P, cons
         D[f.i] = dep.x;
         D[f.i + nf] = dep.y;
         D[f.i + 2 * nf] = dep.z;
+        // 16-bit storage rounds the stored predictor: its FP32 value, the
+        // correction's semi-Lagrangian sample, goes to a fourth plane
+        if (sizeof(T) == 2) D[f.i + 3 * nf] = value;
     }
 }
 
@@ -276,7 +279,10 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
         float qx = dv_h<P2>(d, dep.x, 0) - off[0], qy = dv_h<P2>(d, dep.y, 1) - off[1],
               qz = dv_h<P2>(d, dep.z, 2) - off[2];
-        float low = (reuse && sizeof(T) == 4) ? Store<T>::ld(pred, f.i) : smp.sample(axis, qx, qy, qz);
+        // the predictor's sample at the same departure point: the stored value
+        // (FP32) or its unrounded copy in the fourth trace plane (BF16)
+        float low = !reuse ? smp.sample(axis, qx, qy, qz)
+                           : (sizeof(T) == 4 ? Store<T>::ld(pred, f.i) : __ldg(P.dep[axis] + f.i + 3 * P.nf[axis]));
         value = low;
         if (P.corrected) {
             // correct_velocity_fused.glsl:5-27

@@ -137,7 +137,10 @@ int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
                        const void* u, const void* v, const void* w, float dt,
                        void* pu, void* pv, void* pw, void* stream);
 /* The same, also storing each open face's departure point in dep[axis] (three
- * planes of (nx+a0)(ny+a1)(nz+a2) floats: x, y, z) for ffx_advect_velocity_trace. */
+ * planes of (nx+a0)(ny+a1)(nz+a2) floats: x, y, z) for ffx_advect_velocity_trace.
+ * With storage FFX_BF16 each dep[axis] holds a fourth plane: the face's sample
+ * before rounding to storage, which the velocity correction reads as its
+ * semi-Lagrangian value. */
 int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage,
                              const void* u, const void* v, const void* w, float dt,
                              void* pu, void* pv, void* pw, float* const dep[3], void* stream);
@@ -156,8 +159,9 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage,
 /* The same, reusing the predictor's departure points `dep` (ffx_face_predictor_trace
  * of the same faces and dt) instead of tracing again; used on grids whose extent, cell
  * count and spacing are powers of two, where both passes form the same start point, so
- * the result is unchanged (and in FP32 storage the semi-Lagrangian sample is the
- * predictor's value). dep == NULL or other grids: ffx_advect_velocity. */
+ * the result is unchanged (and the semi-Lagrangian sample is the predictor's value:
+ * the stored face in FP32 storage, the fourth trace plane in BF16 storage).
+ * dep == NULL or other grids: ffx_advect_velocity. */
 int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
                               const void* u, const void* v, const void* w,
                               const void* pu, const void* pv, const void* pw,

@@ -17,11 +17,11 @@ from tests.gpu_helpers import dev
 pytestmark = pytest.mark.gpu
 
 
-def _run(grid, reuse, steps=3):
+def _run(grid, reuse, steps=3, storage='FP32'):
     from fluxfx_b200.backend.projected import DenseProjectedSmoke
     settings = PressureSettings(velocity_advection='MACCORMACK', scalar_advection='MACCORMACK',
                                 thermal_lift=0.5, density_weight=0.1, source_center=(.3, .4, .25),
-                                source_radius=.12, heat_source_rate=10.0)
+                                source_radius=.12, heat_source_rate=10.0, storage=storage)
     colliders = (primitive('SPHERE', (.55, .5, .5), (.2,) * 3),)
     s = DenseProjectedSmoke(grid, settings, dev(), colliders=colliders)
     s.detail.reuse_traces = reuse
@@ -39,11 +39,13 @@ def _run(grid, reuse, steps=3):
     ((32, 32, 32), (1.0, 1.0, 1.0), True),                 # power-of-two grid
     ((24, 20, 16), (1.3, 0.8, 1.7), False),                # start points differ: no face reuse
 ])
-def test_velocity_trace_reuse_is_bit_identical(shape, extent, matches):
+@pytest.mark.parametrize('storage', ['FP32', 'BF16'])
+def test_velocity_trace_reuse_is_bit_identical(shape, extent, matches, storage):
+    # BF16: the correction reads the predictor's unrounded sample from the fourth trace plane
     assert N.face_starts_match(shape, extent) == matches
     grid = GridSpec(shape, extent)
-    a, reused = _run(grid, True)
-    b, _ = _run(grid, False)
+    a, reused = _run(grid, True, storage=storage)
+    b, _ = _run(grid, False, storage=storage)
     assert reused == matches
     for x, y in zip(a, b):
         assert torch.equal(x, y), float((x - y).abs().max())
