@@ -566,7 +566,9 @@ __device__ __forceinline__ GlobalSampler<CellFields<T>> cell_sampler(const Dev& 
     return GlobalSampler<CellFields<T>>{CellFields<T>{d, F, C}};
 }
 
-template <typename T, bool MASK, bool P2, class Smp>
+// DECIDE: the reverse pass that also writes P.ok (its own instantiation, so
+// the other passes keep their registers).
+template <typename T, bool MASK, bool P2, class Smp, bool DECIDE = false>
 __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, int x, int y, int z, const Smp& smp) {
     const Dev& d = P.d;
     const int i = cidx(d, x, y, z);
@@ -578,7 +580,7 @@ __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, i
     F3 p = {((float)x + 0.5f) * d.h[0], ((float)y + 0.5f) * d.h[1], ((float)z + 0.5f) * d.h[2]};
     F3 v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
     F3 dep;
-    if (P.ok) {
+    if (DECIDE) {
         // backtrace_s, keeping the unclipped midpoint and departure point: with
         // the reverse step -dt they are the final pass's forward midpoint
         // p + (dt/2) v0 and, where the midpoint was not clipped, its arrival
@@ -610,16 +612,31 @@ __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, i
     }
 }
 
-template <typename T, bool MASK, bool P2>
+template <typename T, bool MASK, bool P2, bool DECIDE = false>
 __device__ __forceinline__ void scalar_transport_body(const ScalarXport<T>& P, const Blk& b) {
     int x, y, z;
     if (!cell_coords(b, P.d.nx, P.d.ny, x, y, z)) return;
-    scalar_transport_cell<T, MASK, P2>(P, x, y, z, cell_sampler<T>(P.d, P.F, P.in));
+    using S = GlobalSampler<CellFields<T>>;
+    scalar_transport_cell<T, MASK, P2, S, DECIDE>(P, x, y, z, cell_sampler<T>(P.d, P.F, P.in));
 }
 
 template <typename T, bool MASK, bool P2>
 __global__ void FFX_LB_SCALAR_PREDICTOR scalar_transport_kernel(const __grid_constant__ ScalarXport<T> P) {
     scalar_transport_body<T, MASK, P2>(P, hw_blk());
+}
+
+#ifndef FFX_MINB_SCALAR_REVERSE
+#define FFX_MINB_SCALAR_REVERSE 0
+#endif
+#if FFX_MINB_SCALAR_REVERSE > 0
+#define FFX_LB_SCALAR_REVERSE __launch_bounds__(kThreads, FFX_MINB_SCALAR_REVERSE)
+#else
+#define FFX_LB_SCALAR_REVERSE __launch_bounds__(kThreads)
+#endif
+
+template <typename T, bool MASK, bool P2>
+__global__ void FFX_LB_SCALAR_REVERSE scalar_reverse_ok_kernel(const __grid_constant__ ScalarXport<T> P) {
+    scalar_transport_body<T, MASK, P2, true>(P, hw_blk());
 }
 
 template <typename T>
@@ -775,8 +792,11 @@ __global__ void __launch_bounds__(tile::kThreads, FFX_MINB_SCALAR_PREDICTOR_TILE
     auto smp = tile_sampler(cell_sampler<T>(P.d, P.F, P.in), ring);
     const int x = (int)blockIdx.x * tile::kTX + (int)threadIdx.x, y = (int)blockIdx.y * tile::kTY + (int)threadIdx.y;
     const bool in = x < P.d.nx && y < P.d.ny;
+    using S = decltype(smp);
     march<6>(smp, ring, 3 + P.count, cell_chunk(P.d.nz, zchunk), [&](int z) {
-        if (in) scalar_transport_cell<T, MASK, P2>(P, x, y, z, smp);
+        if (!in) return;
+        if (P.ok) scalar_transport_cell<T, MASK, P2, S, true>(P, x, y, z, smp);
+        else scalar_transport_cell<T, MASK, P2, S, false>(P, x, y, z, smp);
     });
 }
 
@@ -1098,7 +1118,13 @@ static int scalar_transport_impl(const FfxGrid* g, const FfxSolids* s, int stora
             FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
                                  (scalar_transport_tiled_kernel<T, M, Q><<<tiled_grid(d.nx, d.ny, d.nz, zc), block, 0, st>>>(P, zc)));
         } else {
-            FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q, (scalar_transport_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+            if (ok) {
+                FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
+                                     (scalar_reverse_ok_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+            } else {
+                FFX_DISPATCH_MASK_P2(P.solid != nullptr, d.pow2 != 0, M, Q,
+                                     (scalar_transport_kernel<T, M, Q><<<grid, block, 0, st>>>(P)));
+            }
         }
     });
     return launch_status("scalar_transport_kernel");
