@@ -84,7 +84,8 @@ class SolidDevice:
         return handle
 
     def dispatch(self, shader, output, shape, uniforms=None, input_field=None, sources=None):
-        self.base.dispatch(shader, output, shape, uniforms, input_field, sources)
+        # through this device, so the passes read its mask (the collider variants)
+        CudaDevice.dispatch(self, shader, output, shape, uniforms, input_field, sources)
 
     def clear_solid(self, source, target):
         """target = source outside solids, 0 inside (``solid_clear.glsl``)."""

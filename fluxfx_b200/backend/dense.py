@@ -47,6 +47,12 @@ class DenseAdvection:
     def density(self):
         return self._front
 
+    def _source_uniforms(self):
+        """The seed/source uniforms of the reference's passes (``backend/dense.py:29-31``),
+        for scripts that drive single passes through ``device.dispatch``."""
+        return {"domainExtent": self.grid.extent, "sourceCenter": self.settings.source_center,
+                "sourceRadius": self.settings.source_radius}
+
     def reset(self, seed=True):
         self._front.zero_()
         self._back.zero_()

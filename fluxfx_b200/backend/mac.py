@@ -29,6 +29,11 @@ class DenseMACAdvection(DenseAdvection):
     def allocated_bytes(self):
         return self.grid.mac_bytes
 
+    def _face_uniforms(self, axis):
+        """The face-pass uniforms of the reference (``backend/mac.py:33-35``)."""
+        return {"domainExtent": self.grid.extent, "cellCount": self.grid.shape,
+                "faceOffset": FACE_OFFSETS[axis], "axisMask": AXIS_MASKS[axis]}
+
     def _face_ptrs(self, faces):
         return [ptr(f) for f in faces]
 

@@ -78,6 +78,12 @@ class DenseProjectedSmoke(DenseThermalAdvection):
             from .combustion import CombustionPasses
             self.combustion = CombustionPasses(self.grid, self.device, self._field_dtype)
         self._solids = solids_struct(self.solids) if self.solids is not None else N.FfxSolids()
+        # the reference's pass handles, for scripts that drive single passes
+        # through device.dispatch (backend/projected.py:47-54, 135-146)
+        self._closed_scalar = self.device.kernel('closed_advect_scalar.glsl')
+        self._emitting_velocity = self.device.kernel('emitting_advect_velocity.glsl')
+        self._multi_scalar = self._multi_velocity = None
+        self._source_table = None
         self._maxima = torch.zeros(3, dtype=torch.float32, device=self.device.device)
         # device-side time step (step_cfl): clock = (dt, previous dt), time in FP64
         self._clock = torch.zeros(2, dtype=torch.float32, device=self.device.device)
@@ -234,6 +240,14 @@ class DenseProjectedSmoke(DenseThermalAdvection):
         data = pack_sources(sources)
         if data != self._source_data:
             self._source_data = data
+            # the table as a device field (the reference's sourceTable texture), for
+            # single-pass dispatch of the table forms
+            with self.device.ordered():
+                self._source_table = torch.tensor(list(data) + [0.0] * (128 - len(data)), dtype=torch.float32,
+                                                  device=self.device.device)
+            if self._multi_velocity is None:
+                self._multi_velocity = self.device.kernel('multi_advect_velocity.glsl')
+                self._multi_scalar = self.device.kernel('multi_advect_scalar.glsl')
         self._source_count = len(sources)
 
     def _fill_sources(self, emission, emitters):
