@@ -626,7 +626,7 @@ __global__ void FFX_LB_SCALAR_PREDICTOR scalar_transport_kernel(const __grid_con
 }
 
 #ifndef FFX_MINB_SCALAR_REVERSE
-#define FFX_MINB_SCALAR_REVERSE 0
+#define FFX_MINB_SCALAR_REVERSE 5
 #endif
 #if FFX_MINB_SCALAR_REVERSE > 0
 #define FFX_LB_SCALAR_REVERSE __launch_bounds__(kThreads, FFX_MINB_SCALAR_REVERSE)
