@@ -100,6 +100,8 @@ class SolidMultigridProjector(SolidPressureProjector):
         # (read back asynchronously) instead of waiting for them (coarse direct
         # solves are refreshed at once, as they need the new records on the host)
         self.defer_refresh_check = False
+        # level-0 sweeps in fused pairs (ffx_graph_smooth2; same results)
+        self.fuse_sweeps = True
         self._pending_refresh = None
         self._loops = {}
         # [cycles of the last solve, cycles of all device-loop solves, decisions]
@@ -283,16 +285,39 @@ class SolidMultigridProjector(SolidPressureProjector):
         links = self._links.numel() if self._links is not None else 0
         return super().allocated_bytes + coarse + direct + links
 
-    def smooth(self, level, count):
+    def _fuse_cycle(self, level, zero_init, dot):
+        """Whether this cycle runs its level-0 sweeps in fused pairs
+        (ffx_graph_smooth2, ffx_graph_prolong_smooth2; same results): level 0
+        with its link field on rows of four cells, outside the Krylov cycles,
+        when the fused cycle swaps the level's p/q roles as often, modulo 2, as
+        the sweep-by-sweep one (a cycle then leaves the iterate in the same
+        buffer either way)."""
+        if (not self.fuse_sweeps or dot is not None or level is not self.levels[0] or self._links is None
+                or level['shape'][0] % 4):
+            return False
+        pre, post = self.pre_sweeps, self.post_sweeps
+        pairs = lambda n: n // 2 + n % 2
+        fused = (1 + pairs(pre - 1) if zero_init and pre > 0 else pairs(pre)) + \
+            (1 + pairs(post - 2) if post >= 2 else post)
+        return (fused - pre - post) % 2 == 0
+
+    def smooth(self, level, count, fused=False):
         timer = self.timer if level is self.levels[0] else None
-        for _ in range(count):
+        while count > 0:
+            pair = fused and count >= 2
             started = timer.begin() if timer is not None else None
-            self.device.call('ffx_graph_smooth', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
-                             2.0 / 3.0, ptr(level['q']), self.device.s)
+            if pair:
+                # two sweeps in one pass, bit-identical to two ffx_graph_smooth launches
+                self.device.call('ffx_graph_smooth2', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                                 2.0 / 3.0, None, ptr(level['q']), self.device.s)
+            else:
+                self.device.call('ffx_graph_smooth', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                                 2.0 / 3.0, ptr(level['q']), self.device.s)
             if timer is not None:
                 timer.end(started)
             level['p'], level['q'] = level['q'], level['p']
-            self.last_iterations += 1
+            self.last_iterations += 2 if pair else 1
+            count -= 2 if pair else 1
 
     def cycle(self, index, zero_init=False, dot=None):
         """One V-cycle from ``index`` down (``backend/solid_multigrid.py:46-65``).
@@ -316,6 +341,7 @@ class SolidMultigridProjector(SolidPressureProjector):
                 dev.call('ffx_dot', level['p'].numel(), ptr(level['rhs']), ptr(level['p']), -1.0, ptr(dot), dev.s)
             return
         pre = self.pre_sweeps
+        fuse = self._fuse_cycle(level, zero_init, dot)
         if zero_init:
             if pre > 0:
                 dev.call('ffx_graph_smooth_zero', C.byref(level['graph']), ptr(level['rhs']), 2.0 / 3.0,
@@ -325,7 +351,7 @@ class SolidMultigridProjector(SolidPressureProjector):
                 pre -= 1
             else:
                 level['p'].zero_()
-        self.smooth(level, pre)
+        self.smooth(level, pre, fuse)
         coarse = self.levels[index + 1]
         tail = self.use_tail and index + 1 == self.tail_start
         # the coarse iterate starts from zero: the restriction pass clears it
@@ -344,7 +370,14 @@ class SolidMultigridProjector(SolidPressureProjector):
             level['p'], level['q'] = level['q'], level['p']
             self.last_iterations += 1
             return
-        if self.post_sweeps > 0:
+        if fuse and self.post_sweeps > 1:
+            # prolongation + the first two post-sweeps in one pass (ffx_graph_prolong_smooth2)
+            dev.call('ffx_graph_prolong_smooth2', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
+                     ptr(level['rhs']), 2.0 / 3.0, None, ptr(level['q']), dev.s)
+            level['p'], level['q'] = level['q'], level['p']
+            self.last_iterations += 2
+            self.smooth(level, self.post_sweeps - 2, fuse)
+        elif self.post_sweeps > 0:
             dev.call('ffx_graph_prolong_smooth', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), dev.s)
             level['p'], level['q'] = level['q'], level['p']

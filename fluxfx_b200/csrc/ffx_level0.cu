@@ -271,6 +271,129 @@ __global__ void __launch_bounds__(32 * kRows, 4) level0_kernel(L0 g, ItArgs A, E
                       (int)threadIdx.y);
 }
 
+// ------------------------------------------------ two sweeps in one pass
+// out = S(S(p)), S being the weighted-Jacobi sweep of level0_body<K, Smooth>
+// (the first sweep reads the iterate of kind K, the second the first's output).
+// A block owns 128 x kRows2 x kZ2 cells. Its kRows2 + 2 warps march the slices
+// z0 - 1 .. z0 + kZ2: each warp computes the first sweep of its row (the
+// block's rows and one halo row on either side) at slice z into a ring of three
+// slices in shared memory, 128 cells a row plus the cell on either side
+// (lanes 0 and 31 compute those one at a time); after a barrier the inner warps
+// compute the second sweep of slice z - 1 from the ring, with the link byte and
+// right-hand side they loaded for it one slice earlier. Every value of the
+// first sweep is formed by S's operations in S's order from the same inputs,
+// so the result equals two launches of S bit for bit while the iterate, the
+// right-hand side and the links are read from memory once for two sweeps.
+constexpr int kRows2 = 8;             // output rows per block
+constexpr int kWarps2 = kRows2 + 2;   // + one halo row on either side
+constexpr int kZ2 = 16;               // output slices per block
+constexpr int kOff2 = 4;              // ring column of cell x0 (16-byte aligned); x0 - 1 at kOff2 - 1
+constexpr int kPitch2 = kOff2 + 128 + 4;
+
+// S at one cell from its neighbours' iterate values (terms4's per-cell terms,
+// in its order, and the Smooth epilogue).
+__device__ __forceinline__ float sweep1(const L0& g, unsigned b, float c, float xm, float xp, float ym, float yp,
+                                        float zm, float zp, float r, float omega, float one_minus) {
+    float d = 0.f, s = 0.f;
+    if (b & kXm) { d = d + g.wx; s = s + g.wx * xm; }
+    if (b & kXp) { d = d + g.wx; s = s + g.wx * xp; }
+    if (b & kYm) { d = d + g.wy; s = s + g.wy * ym; }
+    if (b & kYp) { d = d + g.wy; s = s + g.wy * yp; }
+    if (b & kZm) { d = d + g.wz; s = s + g.wz * zm; }
+    if (b & kZp) { d = d + g.wz; s = s + g.wz * zp; }
+    return d > 0.f ? c * one_minus + ((s - r) / d) * omega : 0.f;
+}
+
+__device__ __forceinline__ float4 sweep4(const L0& g, uint32_t lk, float left, const float4& c, float right,
+                                         const float4& ym, const float4& yp, const float4& lo, const float4& hi,
+                                         const float4& r, float omega, float one_minus) {
+    float diag[4], nb[4];
+    terms4(g, lk, left, c, right, ym, yp, lo, hi, diag, nb);
+    float4 o;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const float d = diag[k];
+        set_el(o, k, d > 0.f ? el(c, k) * one_minus + ((nb[k] - el(r, k)) / d) * omega : 0.f);
+    }
+    return o;
+}
+
+template <It K>
+__global__ void __launch_bounds__(32 * kWarps2) level0_smooth2_kernel(L0 g, ItArgs A, const float* __restrict__ rhs,
+                                                                      float omega, float* __restrict__ out) {
+    __shared__ __align__(16) float ring[3][kWarps2][kPitch2];
+    const int lane = threadIdx.x, w = threadIdx.y;
+    const int x4 = blockIdx.x * 32 + lane, x0 = 4 * x4;
+    const int y = (int)blockIdx.y * kRows2 - 1 + w;
+    const int z0 = blockIdx.z * kZ2, zend = min(z0 + kZ2, g.nz);
+    const bool row = y >= 0 && y < g.ny;
+    const bool active = row && x4 < g.nx4;
+    const bool inner = w >= 1 && w <= kRows2 && active;
+    const int row4 = g.nx4;
+    const float one_minus = 1.f - omega;
+    // the iterate (of kind K) at this thread's four cells of row yy, slice z, or zeros outside
+    auto it_row = [&](int yy, int z) -> float4 {
+        return (x4 < g.nx4 && yy >= 0 && yy < g.ny && z >= 0 && z < g.nz)
+                   ? it4<K>(g, A, 0.f, x4 + row4 * (yy + g.ny * z), x4, yy, z) : zero4();
+    };
+    auto it_cell = [&](int x, int yy, int z) -> float {
+        return (x >= 0 && x < g.nx && yy >= 0 && yy < g.ny && z >= 0 && z < g.nz)
+                   ? it1<K>(g, A, 0.f, x + g.nx * (yy + g.ny * z), x, yy, z) : 0.f;
+    };
+    // the first sweep at the single cell (xe, y, z) (the ring's halo columns)
+    auto edge = [&](int xe, int z) -> float {
+        if (!row || xe < 0 || xe >= g.nx || z < 0 || z >= g.nz) return 0.f;
+        const int i = xe + g.nx * (y + g.ny * z);
+        return sweep1(g, __ldg(g.links + i), it_cell(xe, y, z), it_cell(xe - 1, y, z), it_cell(xe + 1, y, z),
+                      it_cell(xe, y - 1, z), it_cell(xe, y + 1, z), it_cell(xe, y, z - 1), it_cell(xe, y, z + 1),
+                      __ldg(rhs + i), omega, one_minus);
+    };
+    float4 lo = it_row(y, z0 - 2), c = it_row(y, z0 - 1);
+    uint32_t lk_prev = 0u;
+    float4 r_prev = zero4();
+    for (int z = z0 - 1; z <= zend; ++z) {
+        const float4 hi = it_row(y, z + 1);
+        // first sweep of (row y, slice z)
+        const bool zin = z >= 0 && z < g.nz;
+        const int i4 = x4 + row4 * (y + g.ny * z);
+        uint32_t lk = 0u;
+        float4 r = zero4(), o = zero4();
+        if (active && zin) {
+            lk = ld_links(g, i4);
+            r = ld4(rhs, i4);
+        }
+        float left = __shfl_up_sync(0xffffffffu, c.w, 1);
+        float right = __shfl_down_sync(0xffffffffu, c.x, 1);
+        if (lane == 0) left = it_cell(x0 - 1, y, z);
+        if (lane == 31) right = it_cell(x0 + 4, y, z);
+        if (active && zin) o = sweep4(g, lk, left, c, right, it_row(y - 1, z), it_row(y + 1, z), lo, hi, r, omega,
+                                      one_minus);
+        float* slot = ring[(z + 3) % 3][w];
+        *reinterpret_cast<float4*>(slot + kOff2 + 4 * lane) = o;
+        if (lane == 0) slot[kOff2 - 1] = edge(x0 - 1, z);
+        if (lane == 31) slot[kOff2 + 128] = edge(x0 + 4, z);
+        __syncthreads();
+        // second sweep of (row y, slice z - 1)
+        const int zo = z - 1;
+        if (inner && zo >= z0 && zo < zend) {
+            const float* mid = ring[(zo + 3) % 3][w];
+            const float4 c2 = *reinterpret_cast<const float4*>(mid + kOff2 + 4 * lane);
+            const float4 ym2 = *reinterpret_cast<const float4*>(ring[(zo + 3) % 3][w - 1] + kOff2 + 4 * lane);
+            const float4 yp2 = *reinterpret_cast<const float4*>(ring[(zo + 3) % 3][w + 1] + kOff2 + 4 * lane);
+            const float4 lo2 = *reinterpret_cast<const float4*>(ring[(zo + 2) % 3][w] + kOff2 + 4 * lane);
+            const float4 hi2 = *reinterpret_cast<const float4*>(ring[(zo + 4) % 3][w] + kOff2 + 4 * lane);
+            const float4 o2 = sweep4(g, lk_prev, mid[kOff2 + 4 * lane - 1], c2, mid[kOff2 + 4 * lane + 4], ym2, yp2,
+                                     lo2, hi2, r_prev, omega, one_minus);
+            reinterpret_cast<float4*>(out)[x4 + row4 * (y + g.ny * zo)] = o2;
+        }
+        __syncthreads();
+        lk_prev = lk;
+        r_prev = r;
+        lo = c;
+        c = hi;
+    }
+}
+
 // First sweep from a zero iterate (graph_smooth_zero_kernel): no iterate is
 // read, so this is a plain stream over links and rhs.
 __global__ void __launch_bounds__(256) level0_smooth_zero_kernel(L0 g, const float* __restrict__ rhs, float omega,
@@ -504,6 +627,26 @@ int level0_prolong_smooth_dot(const FfxGraphLevel* lv, const float* p, const flo
     EpArgs P{rhs, omega, out, nullptr, dot, scale, nullptr};
     return launch<It::Prolonged, Ep::SmoothDot>(make_l0(lv), ItArgs{p, coarse, nullptr, nullptr}, P, st,
                                                 "level0_prolong_smooth_dot_kernel");
+}
+
+int level0_smooth2(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega, float* out,
+                   cudaStream_t st) {
+    const L0 g = make_l0(lv);
+    const dim3 grid((unsigned)((g.nx4 + 31) / 32), (unsigned)((g.ny + kRows2 - 1) / kRows2),
+                    (unsigned)((g.nz + kZ2 - 1) / kZ2));
+    level0_smooth2_kernel<It::Plain><<<grid, dim3(32, kWarps2), 0, st>>>(g, ItArgs{p, nullptr, nullptr, nullptr}, rhs,
+                                                                          omega, out);
+    return launch_status("level0_smooth2_kernel");
+}
+
+int level0_prolong_smooth2(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                           float omega, float* out, cudaStream_t st) {
+    const L0 g = make_l0(lv);
+    const dim3 grid((unsigned)((g.nx4 + 31) / 32), (unsigned)((g.ny + kRows2 - 1) / kRows2),
+                    (unsigned)((g.nz + kZ2 - 1) / kZ2));
+    level0_smooth2_kernel<It::Prolonged><<<grid, dim3(32, kWarps2), 0, st>>>(g, ItArgs{p, coarse, nullptr, nullptr},
+                                                                              rhs, omega, out);
+    return launch_status("level0_prolong_smooth2_kernel");
 }
 
 int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st) {

@@ -21,6 +21,10 @@ int level0_prolong_smooth(const FfxGraphLevel* lv, const float* p, const float* 
                           float omega, float* out, cudaStream_t st);
 int level0_prolong_smooth_dot(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
                               float omega, float* out, double* dot, double scale, cudaStream_t st);
+int level0_smooth2(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega, float* out,
+                   cudaStream_t st);
+int level0_prolong_smooth2(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                           float omega, float* out, cudaStream_t st);
 int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st);
 int level0_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, cudaStream_t st);
 int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse,

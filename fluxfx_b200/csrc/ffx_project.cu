@@ -1163,6 +1163,28 @@ int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rh
     return launch_status("graph_smooth_kernel");
 }
 
+int ffx_graph_smooth2(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega, float* tmp,
+                      float* p_out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p_in && rhs && p_out && p_in != p_out && (!tmp || (tmp != p_in && tmp != p_out)),
+                "ffx_graph_smooth2: invalid arguments");
+    if (level0_x4(lv, {p_in, rhs, p_out})) return level0_smooth2(lv, p_in, rhs, omega, p_out, as_stream(stream));
+    FFX_REQUIRE(tmp, "ffx_graph_smooth2: this level needs the intermediate buffer");
+    const int e = ffx_graph_smooth(lv, p_in, rhs, omega, tmp, stream);
+    return e ? e : ffx_graph_smooth(lv, tmp, rhs, omega, p_out, stream);
+}
+
+int ffx_graph_prolong_smooth2(const FfxGraphLevel* lv, const float* p, const float* coarse, const float* rhs,
+                              float omega, float* tmp, float* p_out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && coarse && rhs && p_out && p != p_out && lv->nx % 2 == 0 && lv->ny % 2 == 0 &&
+                lv->nz % 2 == 0 && (!tmp || (tmp != p && tmp != p_out)),
+                "ffx_graph_prolong_smooth2: invalid arguments");
+    if (level0_x4(lv, {p, rhs, p_out}) && ((uintptr_t)coarse & 7) == 0)
+        return level0_prolong_smooth2(lv, p, coarse, rhs, omega, p_out, as_stream(stream));
+    FFX_REQUIRE(tmp, "ffx_graph_prolong_smooth2: this level needs the intermediate buffer");
+    const int e = ffx_graph_prolong_smooth(lv, p, coarse, rhs, omega, tmp, stream);
+    return e ? e : ffx_graph_smooth(lv, tmp, rhs, omega, p_out, stream);
+}
+
 int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, void* stream) {
     FFX_REQUIRE(glvl_ok(lv) && p && rhs && r && r != p, "ffx_graph_residual: invalid arguments");
     if (level0_x4(lv, {p, rhs, r})) return level0_residual(lv, p, rhs, r, as_stream(stream));

@@ -388,6 +388,17 @@ int ffx_graph_links(const FfxGraphLevel* lv, uint8_t* links, void* stream);
  * (omega = 2/3 there). p_out must not alias p_in. */
 int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rhs,
                      float omega, float* p_out, void* stream);
+/* Two sweeps of ffx_graph_smooth in one pass: p_out = S(S(p_in)), bit-identical
+ * to two ffx_graph_smooth launches. On a level-0 field with links (nx % 4 == 0,
+ * aligned rows) the first sweep stays in shared memory (the iterate, right-hand
+ * side and links are read once); on other levels it runs as two launches
+ * through `tmp` (a field of the level's size, distinct from p_in and p_out; may
+ * be NULL on level 0). An extension with no reference counterpart. */
+int ffx_graph_smooth2(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega,
+                      float* tmp, float* p_out, void* stream);
+/* The same for ffx_graph_prolong_smooth followed by one ffx_graph_smooth. */
+int ffx_graph_prolong_smooth2(const FfxGraphLevel* lv, const float* p, const float* coarse,
+                              const float* rhs, float omega, float* tmp, float* p_out, void* stream);
 /* r = rhs - L p on active cells; replaces shaders/solid_mg_residual.glsl. */
 int ffx_graph_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r,
                        void* stream);
