@@ -44,13 +44,15 @@ def test_fused_sweeps_equal_two_sweeps(shape):
     lv.links = links.data_ptr()
     cell = (nz, ny, nx)
     p, rhs = t(rng.uniform(-1, 1, cell)), t(rng.uniform(-1, 1, cell))
-    coarse = t(rng.uniform(-1, 1, (nz // 2, ny // 2, nx // 2)))
+    coarse = t(rng.uniform(-1, 1, (max(nz // 2, 1), max(ny // 2, 1), max(nx // 2, 1))))
     for omega in (2 / 3, 0.8):
         mid, two, fused = (t(np.full(cell, np.nan)) for _ in range(3))
         D.call('ffx_graph_smooth', C.byref(lv), ptr(p), ptr(rhs), omega, ptr(mid), D.s)
         D.call('ffx_graph_smooth', C.byref(lv), ptr(mid), ptr(rhs), omega, ptr(two), D.s)
         D.call('ffx_graph_smooth2', C.byref(lv), ptr(p), ptr(rhs), omega, None, ptr(fused), D.s)
         assert np.array_equal(_bits(two), _bits(fused)), (shape, omega)
+        if nx % 2 or ny % 2 or nz % 2:
+            continue     # the prolongation needs even extents
         mid, two, fused = (t(np.full(cell, np.nan)) for _ in range(3))
         D.call('ffx_graph_prolong_smooth', C.byref(lv), ptr(p), ptr(coarse), ptr(rhs), omega, ptr(mid), D.s)
         D.call('ffx_graph_smooth', C.byref(lv), ptr(mid), ptr(rhs), omega, ptr(two), D.s)
