@@ -100,8 +100,8 @@ class SolidMultigridProjector(SolidPressureProjector):
         # (read back asynchronously) instead of waiting for them (coarse direct
         # solves are refreshed at once, as they need the new records on the host)
         self.defer_refresh_check = False
-        # level-0 sweeps in fused pairs (ffx_graph_smooth2; same results)
-        self.fuse_sweeps = True
+        # level-0 sweeps in fused pairs (ffx_graph_smooth2; same results; off: measured slower)
+        self.fuse_sweeps = False
         self._pending_refresh = None
         self._loops = {}
         # [cycles of the last solve, cycles of all device-loop solves, decisions]

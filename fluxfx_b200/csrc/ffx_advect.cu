@@ -715,7 +715,10 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
     // is then not formed)
     decltype(smp.template closed<MASK>(P.solid, qx, qy, qz)) St;
     if (!stored && !ok) St = smp.template closed<MASK>(P.solid, qx, qy, qz, clear && near_start(d, p, dep));
-    for (int c = 0; c < P.count; ++c) {
+    // at most three channels, unrolled: per-channel state stays in registers
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+        if (c >= P.count) break;
         const Channel<T>& C = P.ch[c];
         float value;
         if (ok) {
@@ -757,10 +760,8 @@ __device__ __forceinline__ void advect_scalars_body(const ScalarFinal<T>& P, con
     if (cell_coords(b, d.nx, d.ny, x, y, z))
         advect_scalars_cell<T, MASK, P2>(P, x, y, z, cell_sampler<T>(d, P.F, P.fields), vmax);
     if (P.maxima) {
-        for (int c = 0; c < P.count; ++c) {
-            block_max_to(P.maxima + c, vmax[c]);
-            __syncthreads();
-        }
+        block_max_to_n<3>(P.maxima, vmax, P.count);
+        __syncthreads();
     }
 }
 
@@ -812,10 +813,8 @@ __global__ void __launch_bounds__(tile::kThreads, FFX_MINB_SCALARS_TILED)
         if (in) advect_scalars_cell<T, MASK, P2>(P, x, y, z, smp, vmax);
     });
     if (P.maxima) {
-        for (int c = 0; c < P.count; ++c) {
-            block_max_to(P.maxima + c, vmax[c]);
-            __syncthreads();
-        }
+        block_max_to_n<3>(P.maxima, vmax, P.count);
+        __syncthreads();
     }
 }
 

@@ -654,4 +654,30 @@ __device__ __forceinline__ void block_max_to(float* out, float v) {
     }
 }
 
+// out[k] raised to the block-wide max of v[k] for k < count (count <= K), with
+// one barrier for all of them (the same maxima as K calls of block_max_to). A
+// caller that runs it again in the same block (a persistent loop) puts a
+// barrier in between.
+template <int K>
+__device__ __forceinline__ void block_max_to_n(float* out, const float (&v)[K], int count) {
+    __shared__ float part[K][32];
+    const int tid = threadIdx.x + blockDim.x * (threadIdx.y + blockDim.y * threadIdx.z);
+    const int lane = tid & 31, wid = tid >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const float w = warp_max(v[k]);
+        if (lane == 0) part[k][wid] = w;
+    }
+    __syncthreads();
+    if (wid == 0) {
+        const int nw = (blockDim.x * blockDim.y * blockDim.z + 31) >> 5;
+#pragma unroll
+        for (int k = 0; k < K; ++k) {
+            float m = lane < nw ? part[k][lane] : 0.f;
+            m = warp_max(m);
+            if (k < count && lane == 0 && m > 0.f) atomic_max_nonneg(out + k, m);
+        }
+    }
+}
+
 }  // namespace ffx

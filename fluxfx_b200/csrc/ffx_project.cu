@@ -185,10 +185,8 @@ __device__ __forceinline__ void gradient_body(const GradDesc<T>& P, const Blk& b
         }
     }
     if (maxima) {
-        for (int a = 0; a < 3; ++a) {
-            block_max_to(maxima + a, mx[a]);
-            __syncthreads();
-        }
+        block_max_to_n<3>(maxima, mx, 3);
+        __syncthreads();
     }
 }
 
