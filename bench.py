@@ -478,7 +478,7 @@ def run_b200(args):
                             "pinned host memory on a copy stream, overlapped with the next step (the step after "
                             "that, which overwrites the field, waits for the read)"},
             "gpu_launches": head['launches'],
-            "roofline": roofline(passes, args.steps, cells, s, hbm, peak_kind, ft),
+            "roofline": roofline(passes, args.steps, cells, s, hbm, peak_kind, ft, clock_info.get('sm_mhz')),
             "clocks": clock_info,
         }
         if args.cpu_baseline:
@@ -494,9 +494,28 @@ def run_b200(args):
 # predictor's unrounded samples), from an ncu capture of this bench's scene
 # (fast variant, BF16 storage; the kernel is the same for every solver variant).
 MEASURED_TRAFFIC = {(256, 2): 1419564800 + 97425664}
+# smsp__inst_executed.sum (warp instructions) of the same launch, same capture
+MEASURED_WARP_INSTRUCTIONS = {(256, 2): 1.660e9}
+B200_SMS, SCHEDULERS_PER_SM = 148, 4     # one warp instruction per scheduler per cycle
 
 
-def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True):
+def issue_roofline(ms, cells, s, sm_mhz):
+    """The instruction-issue roofline of the same kernel: its warp
+    instructions per launch (ncu) over the GPU's issue rate at the clock seen
+    in the timed region give the shortest launch that instruction count
+    allows; frac = that floor / the measured launch time."""
+    inst = MEASURED_WARP_INSTRUCTIONS.get((round(cells ** (1 / 3)), s))
+    if not inst or not ms or not sm_mhz:
+        return None
+    rate = B200_SMS * SCHEDULERS_PER_SM * sm_mhz * 1e6      # warp instructions per second
+    floor_ms = inst / rate * 1e3
+    return {"bound": "issue", "warp_instructions_per_launch": inst,
+            "peak_warp_instructions_per_s": rate, "floor_ms": floor_ms, "achieved_ms": ms, "frac": floor_ms / ms,
+            "source": "ncu smsp__inst_executed.sum of one launch (profiles/transport_256_bf16.txt); clock from "
+                      "this run's samples"}
+
+
+def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True, sm_mhz=None):
     """The dominant kernel of the step, advect_velocity_kernel (one launch per
     step; its time comes from the events bracketing that launch in the timed
     steps): algorithmic bytes per launch (the scope table's 9s + 2s + m per
@@ -517,6 +536,7 @@ def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True):
             "algorithmic_bytes_per_launch": per_cell * cells,
             "design_trace_bytes_per_launch": trace_bytes(face_trace)['velocity_transport'] * cells,
             "avg_launch_ms": ms, "limiter": "instruction issue",
+            "issue": issue_roofline(ms, cells, s, sm_mhz),
             "timing": "CUDA events bracketing the launch in every timed step"}
 
 

@@ -37,3 +37,17 @@ def test_single_rank_needs_no_process_group():
     import bench
     assert bench.max_over_ranks([3.0, 4.0], 1) == [3.0, 4.0]
     assert bench.job_rate(1, 20, 2.0) == 10.0
+
+
+def test_issue_roofline_of_the_dominant_kernel():
+    """The instruction-issue roofline: warp instructions of one launch over 148
+    SMs x 4 schedulers x the clock give the floor time; frac = floor / measured."""
+    import bench
+    cells = 256 ** 3
+    r = bench.issue_roofline(2.0, cells, 2, 1965.0)
+    rate = 148 * 4 * 1965.0e6
+    assert r['bound'] == 'issue' and r['peak_warp_instructions_per_s'] == rate
+    assert abs(r['floor_ms'] - bench.MEASURED_WARP_INSTRUCTIONS[(256, 2)] / rate * 1e3) < 1e-12
+    assert abs(r['frac'] - r['floor_ms'] / 2.0) < 1e-12
+    assert bench.issue_roofline(2.0, 64 ** 3, 2, 1965.0) is None      # no capture of that size
+    assert bench.issue_roofline(2.0, cells, 2, None) is None           # no clock sampled
