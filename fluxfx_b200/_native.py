@@ -229,6 +229,7 @@ _PROTOTYPES = {
     'ffx_mg_residual_max': (C.c_int, [n3, f3, vp, vp, f32, vp, vp]),
     'ffx_graph_smooth': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp]),
     'ffx_graph_smooth2': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp, vp]),
+    'ffx_graph_residual_max_smooth': (C.c_int, [P(FfxGraphLevel), vp, vp, f32, vp, vp, vp]),
     'ffx_graph_prolong_smooth2': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, f32, vp, vp, vp]),
     'ffx_graph_residual': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),
     'ffx_graph_residual_restrict': (C.c_int, [P(FfxGraphLevel), vp, vp, vp, vp]),

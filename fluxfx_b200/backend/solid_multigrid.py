@@ -102,6 +102,9 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.defer_refresh_check = False
         # level-0 sweeps in fused pairs (ffx_graph_smooth2; same results; off: measured slower)
         self.fuse_sweeps = False
+        # the device loop's convergence test also makes the next cycle's first
+        # pre-sweep (ffx_graph_residual_max_smooth; same results)
+        self.speculate = True
         self._pending_refresh = None
         self._loops = {}
         # [cycles of the last solve, cycles of all device-loop solves, decisions]
@@ -319,12 +322,14 @@ class SolidMultigridProjector(SolidPressureProjector):
             self.last_iterations += 2 if pair else 1
             count -= 2 if pair else 1
 
-    def cycle(self, index, zero_init=False, dot=None):
+    def cycle(self, index, zero_init=False, dot=None, first_pre=False):
         """One V-cycle from ``index`` down (``backend/solid_multigrid.py:46-65``).
 
         ``zero_init``: the level's iterate is zero, so the first sweep reads none.
         ``dot``: FP64 device slot receiving -rhs . result from the last sweep
-        (used by the Krylov solve)."""
+        (used by the Krylov solve). ``first_pre``: the first pre-sweep's result
+        is already in the level's spare buffer (ffx_graph_residual_max_smooth,
+        run with the convergence test before the cycle)."""
         level = self.levels[index]
         dev = self.device
         if index == len(self.levels) - 1:
@@ -341,8 +346,12 @@ class SolidMultigridProjector(SolidPressureProjector):
                 dev.call('ffx_dot', level['p'].numel(), ptr(level['rhs']), ptr(level['p']), -1.0, ptr(dot), dev.s)
             return
         pre = self.pre_sweeps
-        fuse = self._fuse_cycle(level, zero_init, dot)
-        if zero_init:
+        fuse = not first_pre and self._fuse_cycle(level, zero_init, dot)
+        if first_pre and pre > 0:
+            level['p'], level['q'] = level['q'], level['p']
+            self.last_iterations += 1
+            pre -= 1
+        elif zero_init:
             if pre > 0:
                 dev.call('ffx_graph_smooth_zero', C.byref(level['graph']), ptr(level['rhs']), 2.0 / 3.0,
                          ptr(level['q']), dev.s)
@@ -601,6 +610,11 @@ class SolidMultigridProjector(SolidPressureProjector):
         side.wait_stream(root.stream)
         saved, saved_iters, saved_calls = root.stream, self._iterations_host, dev.calls
         p0, q0 = level['p'], level['q']
+
+        def check_and_sweep():
+            # max |rhs - L p| for the decision and, from the same pass, the sweep of p into q
+            dev.call('ffx_graph_residual_max_smooth', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
+                     2.0 / 3.0, ptr(self._rmax[0:1]), ptr(level['q']), dev.s)
         try:
             root.stream = side
             if refine:
@@ -616,8 +630,11 @@ class SolidMultigridProjector(SolidPressureProjector):
                 dev.call('ffx_loop_reset_counter', counters, dev.s)
                 dev.call('ffx_max_abs', n, N.FFX_F32, ptr(self.before), ptr(self._rmax[1:2]), dev.s)
                 dev.call('ffx_zero_if_unscaled', ptr(self._rmax[1:2]), ptr(level['p']), n, dev.s)
+                speculate = not refine and self.speculate and self.pre_sweeps > 0
                 if refine:
                     true_residual()
+                elif speculate:
+                    check_and_sweep()
                 else:
                     dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
                              ptr(self._rmax[0:1]), dev.s)
@@ -641,6 +658,11 @@ class SolidMultigridProjector(SolidPressureProjector):
                         level['p'], level['q'], level['rhs'] = p0, q0, self.before
                     dev.call('ffx_add', n, ptr(p0), ptr(corr), ptr(p0), dev.s)
                     true_residual()
+                elif speculate:
+                    # the cycle starts from the sweep the test made; the test after it
+                    # makes the next cycle's (discarded when the loop stops)
+                    self.cycle(0, first_pre=True)
+                    check_and_sweep()
                 else:
                     self.cycle(0)
                     dev.call('ffx_graph_residual_max', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),

@@ -141,7 +141,7 @@ __device__ __forceinline__ float it1(const L0& g, const ItArgs& A, float beta, i
 }
 
 // ------------------------------------------------------------ epilogues
-enum class Ep { Smooth, SmoothDot, Apply, Residual, ResidualMax };
+enum class Ep { Smooth, SmoothDot, Apply, Residual, ResidualMax, ResidualMaxSmooth };
 
 struct EpArgs {
     const float* rhs;
@@ -242,17 +242,28 @@ __device__ __forceinline__ void level0_body(const L0& g, const ItArgs& A, const 
             } else {
                 const float4 r = cur.r;
                 float4 o;
+                if constexpr (E == Ep::ResidualMaxSmooth) {
+                    // the residual maximum of the iterate and, from the same terms, its sweep
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
-                    const float rk = el(r, k), d = diag[k];
-                    float v;
-                    if constexpr (E == Ep::Residual || E == Ep::ResidualMax)
-                        v = d > 0.f ? (rk - nb[k]) + d * el(c, k) : 0.f;
-                    else
-                        v = d > 0.f ? el(c, k) * one_minus + ((nb[k] - rk) / d) * P.omega : 0.f;
-                    set_el(o, k, v);
-                    if constexpr (E == Ep::SmoothDot) acc += P.scale * (double)rk * (double)v;
-                    if constexpr (E == Ep::ResidualMax) m = fmaxf(m, finite_abs(v));
+                    for (int k = 0; k < 4; ++k) {
+                        const float rk = el(r, k), d = diag[k];
+                        const float res = d > 0.f ? (rk - nb[k]) + d * el(c, k) : 0.f;
+                        m = fmaxf(m, finite_abs(res));
+                        set_el(o, k, d > 0.f ? el(c, k) * one_minus + ((nb[k] - rk) / d) * P.omega : 0.f);
+                    }
+                } else {
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        const float rk = el(r, k), d = diag[k];
+                        float v;
+                        if constexpr (E == Ep::Residual || E == Ep::ResidualMax)
+                            v = d > 0.f ? (rk - nb[k]) + d * el(c, k) : 0.f;
+                        else
+                            v = d > 0.f ? el(c, k) * one_minus + ((nb[k] - rk) / d) * P.omega : 0.f;
+                        set_el(o, k, v);
+                        if constexpr (E == Ep::SmoothDot) acc += P.scale * (double)rk * (double)v;
+                        if constexpr (E == Ep::ResidualMax) m = fmaxf(m, finite_abs(v));
+                    }
                 }
                 if constexpr (E != Ep::ResidualMax) reinterpret_cast<float4*>(P.out)[i4] = o;
             }
@@ -262,7 +273,7 @@ __device__ __forceinline__ void level0_body(const L0& g, const ItArgs& A, const 
         cur = nxt;
     }
     if constexpr (E == Ep::SmoothDot || E == Ep::Apply) block_sum_d(P.dsum, acc);
-    if constexpr (E == Ep::ResidualMax) block_max_to(P.fmax, m);
+    if constexpr (E == Ep::ResidualMax || E == Ep::ResidualMaxSmooth) block_max_to(P.fmax, m);
 }
 
 template <It K, Ep E>
@@ -647,6 +658,13 @@ int level0_prolong_smooth2(const FfxGraphLevel* lv, const float* p, const float*
     level0_smooth2_kernel<It::Prolonged><<<grid, dim3(32, kWarps2), 0, st>>>(g, ItArgs{p, coarse, nullptr, nullptr},
                                                                               rhs, omega, out);
     return launch_status("level0_prolong_smooth2_kernel");
+}
+
+int level0_residual_max_smooth(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega, float* out,
+                               float* p_out, cudaStream_t st) {
+    EpArgs P{rhs, omega, p_out, nullptr, nullptr, 0.0, out};
+    return launch<It::Plain, Ep::ResidualMaxSmooth>(make_l0(lv), ItArgs{p, nullptr, nullptr, nullptr}, P, st,
+                                                    "level0_residual_max_smooth_kernel");
 }
 
 int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st) {

@@ -27,6 +27,8 @@ int level0_prolong_smooth2(const FfxGraphLevel* lv, const float* p, const float*
                            float omega, float* out, cudaStream_t st);
 int level0_residual(const FfxGraphLevel* lv, const float* p, const float* rhs, float* r, cudaStream_t st);
 int level0_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, cudaStream_t st);
+int level0_residual_max_smooth(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega, float* out,
+                               float* p_out, cudaStream_t st);
 int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse,
                              float* zero, cudaStream_t st);
 int level0_direction_apply(const FfxGraphLevel* lv, const float* z, const float* p_old, const double* rz_new,

@@ -1242,6 +1242,19 @@ int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float*
     return launch_status("graph_residual_max_kernel");
 }
 
+int ffx_graph_residual_max_smooth(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega,
+                                  float* out, float* p_out, void* stream) {
+    FFX_REQUIRE(glvl_ok(lv) && p && rhs && out && p_out && p_out != p,
+                "ffx_graph_residual_max_smooth: invalid arguments");
+    cudaStream_t st = as_stream(stream);
+    if (level0_x4(lv, {p, rhs, p_out})) {
+        int e = cuda_status(cudaMemsetAsync(out, 0, sizeof(float), st), "ffx_graph_residual_max_smooth memset");
+        return e ? e : level0_residual_max_smooth(lv, p, rhs, omega, out, p_out, st);
+    }
+    const int e = ffx_graph_residual_max(lv, p, rhs, out, stream);
+    return e ? e : ffx_graph_smooth(lv, p, rhs, omega, p_out, stream);
+}
+
 int ffx_graph_coarsen(const FfxGraphLevel* fine, float* coarse_edges, int32_t* disconnected, void* stream) {
     FFX_REQUIRE(glvl_ok(fine) && coarse_edges && disconnected && ((uintptr_t)coarse_edges & 15) == 0 &&
                 fine->nx % 2 == 0 && fine->ny % 2 == 0 && fine->nz % 2 == 0,

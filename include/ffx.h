@@ -388,6 +388,14 @@ int ffx_graph_links(const FfxGraphLevel* lv, uint8_t* links, void* stream);
  * (omega = 2/3 there). p_out must not alias p_in. */
 int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rhs,
                      float omega, float* p_out, void* stream);
+/* ffx_graph_residual_max and ffx_graph_smooth of the same p in one pass: out[0]
+ * = max |rhs - L p| (out is set first) and p_out = the sweep of p, both
+ * bit-identical to the two entry points (on level 0 with links the terms are
+ * formed once; other levels run the two launches). A solve loop that tests
+ * convergence with it has the next cycle's first pre-sweep ready when it goes
+ * on. An extension with no reference counterpart. */
+int ffx_graph_residual_max_smooth(const FfxGraphLevel* lv, const float* p, const float* rhs,
+                                  float omega, float* out, float* p_out, void* stream);
 /* Two sweeps of ffx_graph_smooth in one pass: p_out = S(S(p_in)), bit-identical
  * to two ffx_graph_smooth launches. On a level-0 field with links (nx % 4 == 0,
  * aligned rows) the first sweep stays in shared memory (the iterate, right-hand

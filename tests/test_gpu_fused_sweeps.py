@@ -59,6 +59,13 @@ def test_fused_sweeps_equal_two_sweeps(shape):
         D.call('ffx_graph_prolong_smooth2', C.byref(lv), ptr(p), ptr(coarse), ptr(rhs), omega, None, ptr(fused),
                D.s)
         assert np.array_equal(_bits(two), _bits(fused)), (shape, omega, 'prolonged')
+    # the convergence test with the speculative sweep: the residual maximum and the sweep
+    m1, m2 = torch.full((1,), -1.0, device='cuda'), torch.full((1,), -1.0, device='cuda')
+    one, both = t(np.full(cell, np.nan)), t(np.full(cell, np.nan))
+    D.call('ffx_graph_residual_max', C.byref(lv), ptr(p), ptr(rhs), ptr(m1), D.s)
+    D.call('ffx_graph_smooth', C.byref(lv), ptr(p), ptr(rhs), 2 / 3, ptr(one), D.s)
+    D.call('ffx_graph_residual_max_smooth', C.byref(lv), ptr(p), ptr(rhs), 2 / 3, ptr(m2), ptr(both), D.s)
+    assert float(m1[0]) == float(m2[0]) > 0 and np.array_equal(_bits(one), _bits(both))
     # without the link field the level takes the one-cell kernels, two launches through tmp
     scalar = N.FfxGraphLevel(*shape, None, ptr(solid_t), N.f3(*w))
     tmp, fused = t(np.full(cell, np.nan)), t(np.full(cell, np.nan))
@@ -93,5 +100,38 @@ def test_solve_with_fused_sweeps_equals_sweep_by_sweep(variant, sweeps):
         for x, y in zip([a.density, a.temperature, a.projector.pressure, *a._velocity],
                         [b.density, b.temperature, b.projector.pressure, *b._velocity]):
             assert torch.equal(x, y), (variant, sweeps, k)
+    for sv, _ in runs:
+        sv.close()
+
+
+@pytest.mark.parametrize('variant, storage', [('fast', 'BF16'), ('plain', 'FP32'), ('learned', 'FP32')])
+def test_speculative_sweep_in_the_solve_loop(variant, storage):
+    """The device loop whose convergence test also makes the next cycle's first
+    pre-sweep (ffx_graph_residual_max_smooth) gives the cycle counts and fields
+    of the loop without it, bit for bit."""
+    import bench
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    D = dev()
+    runs = []
+    for speculate in (True, False):
+        grid, s, colliders, emitters, noise = bench.scene(64, storage, 7, **bench.VARIANTS[variant])
+        sv = DenseProjectedSmoke(grid, s, D, colliders=colliders)
+        if s.learned_warm_start:
+            from fluxfx_b200.learned import attach
+            attach(sv, colliders)
+        sv.projector.speculate = speculate
+        sv.upload(torch.zeros(grid.cells))
+        sv.upload_temperature(torch.zeros(grid.cells))
+        sv.upload_velocity([torch.as_tensor(v * 300) for v in noise])
+        runs.append((sv, emitters))
+    for k in range(4):
+        for sv, em in runs:
+            sv.step_cfl(0.5, 0.02, sources=em)
+        (a, _), (b, _) = runs
+        assert a.projector.last_cycles == b.projector.last_cycles > 0, k
+        torch.cuda.synchronize()
+        for x, y in zip([a.density, a.temperature, a.projector.pressure, *a._velocity],
+                        [b.density, b.temperature, b.projector.pressure, *b._velocity]):
+            assert torch.equal(x, y), (variant, k)
     for sv, _ in runs:
         sv.close()
