@@ -18,14 +18,21 @@ namespace ffx {
 
 // ---------------------------------------------------------------- storage
 template <typename T> struct Store;
+// Element i of a field. The 32-bit index forms (every field has fewer than
+// 2^31 elements, checked at the entry points) let the address be one wide
+// multiply-add; the 64-bit forms serve callers that index in int64_t.
 template <> struct Store<float> {
+    static __device__ __forceinline__ float ld(const float* p, int i) { return __ldg(p + i); }
     static __device__ __forceinline__ float ld(const float* p, int64_t i) { return __ldg(p + i); }
+    static __device__ __forceinline__ void st(float* p, int i, float v) { p[i] = v; }
     static __device__ __forceinline__ void st(float* p, int64_t i, float v) { p[i] = v; }
 };
 template <> struct Store<__nv_bfloat16> {
+    static __device__ __forceinline__ float ld(const __nv_bfloat16* p, int i) { return __bfloat162float(p[i]); }
     static __device__ __forceinline__ float ld(const __nv_bfloat16* p, int64_t i) {
         return __bfloat162float(p[i]);
     }
+    static __device__ __forceinline__ void st(__nv_bfloat16* p, int i, float v) { p[i] = __float2bfloat16_rn(v); }
     static __device__ __forceinline__ void st(__nv_bfloat16* p, int64_t i, float v) {
         p[i] = __float2bfloat16_rn(v);
     }
