@@ -126,7 +126,8 @@ class FfxBatchDomain(C.Structure):
                 ('heat_channel', FfxScalarChannel), ('cell', C.c_double), ('cfl', C.c_double),
                 ('dt_max', C.c_double), ('dt0', f32), ('levels', i32), ('level', FfxBatchLevel * BATCH_LEVELS),
                 ('tail_start', i32), ('inverse', vp), ('pre', i32), ('post', i32), ('max_cycles', i32),
-                ('warm_start', i32), ('tolerance', C.c_double), ('face_trace', vp * 3), ('cell_trace', vp)]
+                ('warm_start', i32), ('tolerance', C.c_double), ('face_trace', vp * 3), ('cell_trace', vp),
+                ('clear', vp), ('cell_ok', vp)]
 
 
 class FfxBatchStats(C.Structure):

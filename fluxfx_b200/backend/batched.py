@@ -102,6 +102,8 @@ class BatchedSmoke:
         det._ensure_scalar(2)
         D.grid = s._g
         D.solid, D.halo = s.solids.mask.data_ptr(), s.solids.halo.data_ptr()
+        clear = getattr(s.solids, 'clear', None)
+        D.clear = clear.data_ptr() if clear is not None else None
         D.u, D.v, D.w = [f.data_ptr() for f in s._velocity]
         D.pu, D.pv, D.pw = [f.data_ptr() for f in det.face_predictor]
         D.bu, D.bv, D.bw = [f.data_ptr() for f in p.bounded]
@@ -149,6 +151,11 @@ class BatchedSmoke:
             if det.cell_trace is None:
                 det.cell_trace = torch.empty(3 * prod(s.grid.shape), dtype=torch.float32, device=dev)
             D.cell_trace = det.cell_trace.data_ptr()
+            # the reverse pass decides the final pass's corrections, as the single-domain step does
+            if det.cell_ok is None:
+                nx, ny, nz = s.grid.shape
+                det.cell_ok = torch.empty((nz, ny, nx), dtype=torch.uint8, device=dev)
+            D.cell_ok = det.cell_ok.data_ptr()
 
     # ------------------------------------------------------------ running
     @property

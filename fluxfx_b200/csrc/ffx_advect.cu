@@ -1356,6 +1356,25 @@ __global__ void __launch_bounds__(kBatchThreads) batch_scalar_transport_kernel(c
     });
 }
 
+// The reverse pass: domains with decision buffers decide the final pass's corrections.
+__global__ void __launch_bounds__(kBatchThreads) batch_scalar_reverse_kernel(const __grid_constant__ BatchMap M,
+                                                                             const ScalarXport<float>* descs,
+                                                                             const BatchState* state) {
+    using S = GlobalSampler<CellFields<float>>;
+    for_tiles(M, descs, state, false, DeviceDt{state, -1.f}, [](const ScalarXport<float>& P, const Blk& b, int) {
+        int x, y, z;
+        if (!cell_coords(b, P.d.nx, P.d.ny, x, y, z)) return;
+        const auto smp = cell_sampler<float>(P.d, P.F, P.in);
+        if (P.ok) {
+            if (P.d.pow2) scalar_transport_cell<float, true, true, S, true>(P, x, y, z, smp);
+            else scalar_transport_cell<float, true, false, S, true>(P, x, y, z, smp);
+        } else {
+            if (P.d.pow2) scalar_transport_cell<float, true, true, S, false>(P, x, y, z, smp);
+            else scalar_transport_cell<float, true, false, S, false>(P, x, y, z, smp);
+        }
+    });
+}
+
 __global__ void FFX_LB_BATCH_SCALARS batch_scalars_kernel(const __grid_constant__ BatchMap M,
                                                                       const ScalarFinal<float>* descs,
                                                                       const BatchState* state) {
@@ -1385,6 +1404,7 @@ size_t predictor_desc(const FfxBatchDomain& D, void* out) {
         P.d = make_dev(D.grid);
         P.solid = D.solid;
         P.halo = D.halo;
+        P.clear = D.clear;
         P.F = {D.u, D.v, D.w};
         P.dt = 0.f;
         P.out[0] = D.pu; P.out[1] = D.pv; P.out[2] = D.pw;
@@ -1405,6 +1425,7 @@ size_t velocity_desc(const FfxBatchDomain& D, int parity, void* out) {
         P.d = make_dev(D.grid);
         P.solid = D.solid;
         P.halo = D.halo;
+        P.clear = D.clear;
         P.F = {D.u, D.v, D.w};
         P.P = D.velocity_corrected ? Faces<float>{D.pu, D.pv, D.pw} : P.F;
         P.dt = 0.f;
@@ -1446,6 +1467,11 @@ size_t scalar_xport_desc(const FfxBatchDomain& D, int parity, int reverse, void*
         P.out[1] = reverse ? D.reverse[1] : D.predictor[1];
         P.dep = reverse ? nullptr : D.cell_trace;     // the forward pass stores its departure points
         P.n = D.grid.nx * D.grid.ny * D.grid.nz;
+        P.clear = D.clear;
+        if (reverse && D.cell_trace && D.cell_ok) {  // the reverse pass decides the final pass's corrections
+            P.fdep = D.cell_trace;
+            P.ok = D.cell_ok;
+        }
         memcpy(out, &P, sizeof P);
     }
     return sizeof(ScalarXport<float>);
@@ -1482,6 +1508,8 @@ size_t scalar_final_desc(const FfxBatchDomain& D, int parity, void* out) {
         P.maxima = nullptr;
         P.dep = D.scalar_corrected ? D.cell_trace : nullptr;
         P.n = D.grid.nx * D.grid.ny * D.grid.nz;
+        P.clear = D.clear;
+        P.ok = (D.scalar_corrected && D.cell_trace) ? D.cell_ok : nullptr;
         const float extent[3] = {D.grid.ex, D.grid.ey, D.grid.ez};
         P.src = make_src(&D.sources, extent);
         memcpy(out, &P, sizeof P);
@@ -1499,8 +1527,12 @@ cudaError_t advect_velocity(const BatchMap& M, const void* descs, BatchState* st
 }
 cudaError_t scalar_transport(const BatchMap& M, const void* descs, BatchState* state, int reverse, int grid,
                              cudaStream_t st) {
-    batch_scalar_transport_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(
-        M, (const ScalarXport<float>*)descs, state, reverse ? -1.f : 1.f);
+    if (reverse)
+        batch_scalar_reverse_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(M, (const ScalarXport<float>*)descs,
+                                                                               state);
+    else
+        batch_scalar_transport_kernel<<<grid_of(M, grid), kBatchThreads, 0, st>>>(
+            M, (const ScalarXport<float>*)descs, state, 1.f);
     return cudaGetLastError();
 }
 cudaError_t advect_scalars(const BatchMap& M, const void* descs, BatchState* state, int grid, cudaStream_t st) {
@@ -1513,7 +1545,7 @@ int advect_resident_blocks(int kind) {
         case kPredictor: return occupancy(batch_predictor_kernel);
         case kVelocity: return occupancy(batch_velocity_kernel);
         case kScalarPredictor:
-        case kScalarReverse: return occupancy(batch_scalar_transport_kernel);
+        case kScalarReverse: return occupancy(batch_scalar_reverse_kernel);
         case kScalarFinal: return occupancy(batch_scalars_kernel);
         default: return 0;
     }

@@ -698,6 +698,9 @@ typedef struct FfxBatchDomain {
                                           velocity pass as in ffx_advect_velocity_trace */
     float* cell_trace;                 /* optional departure points of the scalar predictor (three
                                           planes of cells), reused by the final scalar pass */
+    const uint8_t* clear;              /* optional clearance of the mask (ffx_clearance), as FfxSolids.clear */
+    uint8_t* cell_ok;                  /* optional, with cell_trace: one byte per cell, the reverse scalar
+                                          pass's correction decisions (as ffx_scalar_reverse_ok) */
 } FfxBatchDomain;
 typedef struct FfxBatchStats {
     float dt, last_dt;                 /* dt of the next step, of the last step */
