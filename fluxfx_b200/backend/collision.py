@@ -51,11 +51,11 @@ class SolidDevice:
         g = N.grid_struct(grid.shape, grid.extent)
         self.base.call('ffx_raster_colliders', C.byref(g), (C.c_double * 3)(*grid.extent), len(colliders),
                        ptr(rows), ptr(self.mask), self.base.s)
-        self.base.call('ffx_dilate_mask', C.byref(g), ptr(self.mask), ptr(self.halo), self.base.s)
-        # cells with no collider or wall within three cells: the transport passes
-        # skip their collider tests (ffx_clearance); refreshed with the mask
+        # the dilated mask and the cells with no collider or wall within three cells
+        # (the transport passes skip their collider tests there), refreshed with the mask
         self.clear = torch.zeros((nz, ny, nx), dtype=torch.uint8, device=dev)
-        self.base.call('ffx_clearance', C.byref(g), ptr(self.halo), ptr(self.clear), self.base.s)
+        self.base.call('ffx_halo_clearance', C.byref(g), ptr(self.mask), ptr(self.halo), ptr(self.clear),
+                       self.base.s)
         self._rows = rows
         self.colliders = tuple(colliders)
 

@@ -46,8 +46,8 @@ class MovingSolidDevice(SolidDevice):
         box_h = (C.c_int32 * len(box))(*box)
         self.base.call('ffx_moving_mask', C.byref(self._g), len(colliders), rows_h, box_h, ptr(self.mask),
                        self.base.s)
-        self.base.call('ffx_dilate_mask', C.byref(self._g), ptr(self.mask), ptr(self.halo), self.base.s)
-        self.base.call('ffx_clearance', C.byref(self._g), ptr(self.halo), ptr(self.clear), self.base.s)
+        self.base.call('ffx_halo_clearance', C.byref(self._g), ptr(self.mask), ptr(self.halo), ptr(self.clear),
+                       self.base.s)
 
     def update(self, colliders, dt):
         """New poses: owner mask, dilated mask and wall velocities, in place."""

@@ -112,6 +112,58 @@ __global__ void clearance_kernel(Dev d, const uint8_t* __restrict__ halo, uint8_
     clear[cidx(d, x, y, z)] = any ? 0 : 1;
 }
 
+// The dilated mask and the clearance of a mask in one pass (ffx_halo_clearance):
+// halo = any solid or outside cell in the 3x3x3 block (dilate_kernel's field),
+// clear = no solid or outside cell in the 7x7x7 block (clearance_kernel's
+// field of that halo: no halo or outside cell within distance 2 means no solid
+// or outside cell within distance 3). A block owns 32 x 8 columns and a chunk of
+// kHZ slices; per slice it stages the 38 x 14 window of the mask (outside = 1),
+// dilates it along x and then y in shared memory, and every thread keeps the
+// last seven slices' (x, y) dilations as bits, so the z dilation is a mask of
+// those bits.
+constexpr int kHX = 32, kHY = 8, kHZ = 16, kHR = 3;
+constexpr int kWinX = kHX + 2 * kHR, kWinY = kHY + 2 * kHR;
+
+__global__ void __launch_bounds__(kHX * kHY) halo_clear_kernel(Dev d, const uint8_t* __restrict__ solid,
+                                                               uint8_t* __restrict__ halo, uint8_t* __restrict__ clear) {
+    __shared__ uint8_t win[kWinY][kWinX];
+    __shared__ uint8_t rx1[kWinY][kHX], rx3[kWinY][kHX];
+    const int tx = threadIdx.x, ty = threadIdx.y, tid = ty * kHX + tx;
+    const int x0 = blockIdx.x * kHX, y0 = blockIdx.y * kHY, z0 = blockIdx.z * kHZ;
+    const int x = x0 + tx, y = y0 + ty;
+    const int zend = min(z0 + kHZ, d.nz);
+    unsigned h1 = 0u, h3 = 0u;   // bit k: the (x, y) dilation of slice zs - k
+    for (int zs = z0 - kHR; zs < zend + kHR; ++zs) {
+        for (int e = tid; e < kWinY * kWinX; e += kHX * kHY) {
+            const int wy = e / kWinX, wx = e - wy * kWinX;
+            const int gx = x0 - kHR + wx, gy = y0 - kHR + wy;
+            const bool out = gx < 0 || gy < 0 || zs < 0 || gx >= d.nx || gy >= d.ny || zs >= d.nz;
+            win[wy][wx] = out ? 1 : (__ldg(solid + cidx(d, gx, gy, zs)) != 0);
+        }
+        __syncthreads();
+        for (int e = tid; e < kWinY * kHX; e += kHX * kHY) {
+            const int wy = e / kHX, cx = e - wy * kHX;
+            const uint8_t* r = win[wy] + cx;    // r[0 .. 6]: x - 3 .. x + 3
+            rx1[wy][cx] = r[2] | r[3] | r[4];
+            rx3[wy][cx] = r[0] | r[1] | r[2] | r[3] | r[4] | r[5] | r[6];
+        }
+        __syncthreads();
+        const unsigned d1 = rx1[ty + 2][tx] | rx1[ty + 3][tx] | rx1[ty + 4][tx];
+        unsigned d3 = 0u;
+#pragma unroll
+        for (int k = 0; k < 2 * kHR + 1; ++k) d3 |= rx3[ty + k][tx];
+        h1 = (h1 << 1) | d1;
+        h3 = (h3 << 1) | d3;
+        const int z = zs - kHR;   // slices z - 3 .. z + 3 are bits 6 .. 0
+        if (z >= z0 && z < zend && x < d.nx && y < d.ny) {
+            const int i = cidx(d, x, y, z);
+            halo[i] = ((h1 >> 2) & 7u) != 0u;
+            clear[i] = (h3 & 0x7fu) == 0u;
+        }
+        __syncthreads();
+    }
+}
+
 template <typename T>
 __global__ void solid_clear_kernel(int64_t n, const uint8_t* __restrict__ solid, const T* in, T* out) {
     int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
@@ -202,6 +254,16 @@ int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void*
     int64_t n = (int64_t)g->nx * g->ny * g->nz;
     dilate_kernel<<<blocks_for(n, 256), 256, 0, as_stream(stream)>>>(d, solid, halo);
     return launch_status("dilate_kernel");
+}
+
+int ffx_halo_clearance(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, uint8_t* clear, void* stream) {
+    FFX_REQUIRE(grid_ok(g) && solid && halo && clear && solid != halo && solid != clear && halo != clear,
+                "ffx_halo_clearance: invalid arguments");
+    Dev d = make_dev(*g);
+    const dim3 grid((unsigned)((g->nx + kHX - 1) / kHX), (unsigned)((g->ny + kHY - 1) / kHY),
+                    (unsigned)((g->nz + kHZ - 1) / kHZ));
+    halo_clear_kernel<<<grid, dim3(kHX, kHY), 0, as_stream(stream)>>>(d, solid, halo, clear);
+    return launch_status("halo_clear_kernel");
 }
 
 int ffx_clearance(const FfxGrid* g, const uint8_t* halo, uint8_t* clear, void* stream) {

@@ -119,6 +119,10 @@ int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void*
  * the collider tests (solid_boundary.glsl, correct_*.glsl) where they cannot
  * change the result. One-time work per collider layout. */
 int ffx_clearance(const FfxGrid* g, const uint8_t* halo, uint8_t* clear, void* stream);
+/* ffx_dilate_mask and ffx_clearance of a mask in one pass: the same halo and
+ * clearance fields, bit for bit, from the mask alone (an extension: moving
+ * colliders refresh both after every move). */
+int ffx_halo_clearance(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, uint8_t* clear, void* stream);
 /* out = solid ? 0 : in; replaces shaders/solid_clear.glsl. */
 int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const void* in,
                     void* out, void* stream);

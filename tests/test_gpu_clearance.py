@@ -119,3 +119,27 @@ def test_clear_form_with_a_moving_collider():
             assert torch.equal(x, y), k
     a.close()
     b.close()
+
+
+@pytest.mark.parametrize('shape', [(64, 64, 64), (37, 9, 21), (1, 1, 1), (33, 17, 40), (200, 3, 5)])
+def test_one_pass_halo_and_clearance(shape):
+    """ffx_halo_clearance equals ffx_dilate_mask followed by ffx_clearance, bit
+    for bit, on grids whose extents are and are not multiples of its tile
+    (32 x 8 x 16 cells), with sparse and dense random masks."""
+    import ctypes as C
+    from fluxfx_b200 import _native as N
+    D = dev()
+    nx, ny, nz = shape
+    g = N.grid_struct(shape, (1.0, 1.0, 1.0))
+    rng = np.random.default_rng(nx + 5 * ny + 11 * nz)
+    for density in (0.0, 0.002, 0.05):
+        mask = torch.as_tensor((rng.uniform(size=(nz, ny, nx)) < density).astype(np.uint8), device='cuda')
+        halo2, clear2, halo1, clear1 = (torch.full((nz, ny, nx), 7, dtype=torch.uint8, device='cuda')
+                                        for _ in range(4))
+        p = lambda x: C.c_void_p(x.data_ptr())
+        D.call('ffx_dilate_mask', C.byref(g), p(mask), p(halo2), D.s)
+        D.call('ffx_clearance', C.byref(g), p(halo2), p(clear2), D.s)
+        D.call('ffx_halo_clearance', C.byref(g), p(mask), p(halo1), p(clear1), D.s)
+        torch.cuda.synchronize()
+        assert torch.equal(halo1, halo2) and torch.equal(clear1, clear2), (shape, density)
+        assert np.array_equal(clear1.cpu().numpy(), _expected_clear(mask.cpu().numpy() != 0))
