@@ -147,6 +147,7 @@ _PROTOTYPES = {
     'ffx_dilate_mask': (C.c_int, [P(FfxGrid), vp, vp, vp]),
     'ffx_clearance': (C.c_int, [P(FfxGrid), vp, vp, vp]),
     'ffx_halo_clearance': (C.c_int, [P(FfxGrid), vp, vp, vp, vp]),
+    'ffx_division_mismatches': (C.c_int, [f32, vp, vp]),
     'ffx_solid_clear': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp]),
     'ffx_face_predictor': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
     'ffx_set_transport_tiling': (C.c_int, [C.c_int]),

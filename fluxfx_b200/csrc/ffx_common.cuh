@@ -45,7 +45,7 @@ struct Dev {
     float e[3];              // extent
     float h[3];              // e / n (FP32 division, as the shaders compute it)
     float inv[3];            // host-side 1/h rounded to FP32 (the invCell uniform)
-    float re[3], rn[3], rh[3];   // 1/e, 1/n, 1/h (exact when pow2)
+    float re[3], rn[3], rh[3];   // 1/e, 1/n, 1/h rounded to nearest (exact when pow2)
     int pow2;                // every e, n and h is a power of two
 };
 
@@ -97,18 +97,44 @@ inline bool face_starts_match(const Dev& d) {
     return true;
 }
 
+// a / b rounded to nearest, as the IEEE division gives it, for a divisor b in
+// [2^-30, 2^30] known in advance, with y = 1/b rounded to nearest (the host's
+// IEEE division). Markstein's correction (P. W. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Dev. 34(1), 1990): when y is 1/b rounded to nearest and q lies within one
+// ulp of a / b, the remainder r = a - b q is exact in one FMA and RN(q + r y)
+// is a / b rounded to nearest. q0 = RN(a y) lies within 1.5 ulp of a / b; the
+// first correction brings it within half an ulp plus a term of relative size
+// 2^-23 (so within one ulp), the second rounds it correctly. No branch: the
+// sign copy makes -0 / b = -0, and |a| > 2^96 (infinities included) returns
+// a y, which is the IEEE infinity for an infinite a; NaN stays NaN. The
+// quotient is the IEEE one, bit for bit, for +-0, +-inf, NaN and every finite
+// a with 2^-96 <= |a| <= 2^96, where no intermediate underflows or overflows:
+// checked over all 2^32 inputs per divisor (ffx_division_mismatches). Grid
+// positions are 0 or at least an ulp of half a cell, so the excluded
+// magnitudes (nonzero below 2^-96, finite above 2^96) never reach it.
+__device__ __forceinline__ float div_rn(float a, float b, float y) {
+    float q = a * y;
+    float r = fmaf(-q, b, a);
+    q = fmaf(r, y, q);
+    r = fmaf(-q, b, a);
+    q = copysignf(fmaf(r, y, q), a);
+    return fabsf(a) > 0x1p96f ? a * y : q;
+}
+
 // Division by the grid constants e, n and h. When every one of them is a power
 // of two (e.g. a 256^3 unit cube) dividing is an exact rescaling, so it is done
-// as a multiplication by the exact reciprocal -- bit-identical to the IEEE
-// division, and several times cheaper. P2 is chosen per launch from Dev::pow2.
+// as a multiplication by the exact reciprocal; otherwise by div_rn. Both are
+// bit-identical to the IEEE division and several times cheaper. P2 is chosen
+// per launch from Dev::pow2.
 template <bool P2> __device__ __forceinline__ float dv_e(const Dev& d, float x, int i) {
-    return P2 ? x * d.re[i] : x / d.e[i];
+    return P2 ? x * d.re[i] : div_rn(x, d.e[i], d.re[i]);
 }
 template <bool P2> __device__ __forceinline__ float dv_n(const Dev& d, float x, int i) {
-    return P2 ? x * d.rn[i] : x / d.nf[i];
+    return P2 ? x * d.rn[i] : div_rn(x, d.nf[i], d.rn[i]);
 }
 template <bool P2> __device__ __forceinline__ float dv_h(const Dev& d, float x, int i) {
-    return P2 ? x * d.rh[i] : x / d.h[i];
+    return P2 ? x * d.rh[i] : div_rn(x, d.h[i], d.rh[i]);
 }
 
 // Every field has fewer than 2^31 elements (checked at the entry points), so

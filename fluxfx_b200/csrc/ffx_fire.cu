@@ -119,9 +119,9 @@ struct MovingColliders {
 __global__ void __launch_bounds__(256) moving_mask_kernel(Dev d, MovingColliders C, uint8_t* owners) {
     int x, y, z;
     if (!cell_coords(d.nx, d.ny, x, y, z)) return;
-    const float px = (((float)x + 0.5f) * d.e[0]) / d.nf[0];
-    const float py = (((float)y + 0.5f) * d.e[1]) / d.nf[1];
-    const float pz = (((float)z + 0.5f) * d.e[2]) / d.nf[2];
+    const float px = dv_n<false>(d, ((float)x + 0.5f) * d.e[0], 0);
+    const float py = dv_n<false>(d, ((float)y + 0.5f) * d.e[1], 1);
+    const float pz = dv_n<false>(d, ((float)z + 0.5f) * d.e[2], 2);
     unsigned value = 0;
     for (int k = 0; k < C.count && value == 0; ++k) {
         const float* r = C.rows[k];
@@ -158,9 +158,9 @@ __global__ void __launch_bounds__(256) moving_wall_kernel(Dev d, const uint8_t* 
         const int owner = lo > 0 ? lo : hi;
         if (owner > 0 && owner <= FFX_MOVING_MAX) {
             const float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
-            const float px = (((float)x + off[0]) * d.e[0]) / d.nf[0];
-            const float py = (((float)y + off[1]) * d.e[1]) / d.nf[1];
-            const float pz = (((float)z + off[2]) * d.e[2]) / d.nf[2];
+            const float px = dv_n<false>(d, ((float)x + off[0]) * d.e[0], 0);
+            const float py = dv_n<false>(d, ((float)y + off[1]) * d.e[1], 1);
+            const float pz = dv_n<false>(d, ((float)z + off[2]) * d.e[2], 2);
             const float* r = W.rows[owner - 1][axis];
             value = ((r[0] * px + r[1] * py) + r[2] * pz) + r[3] * 1.0f;
         }

@@ -34,9 +34,14 @@ inline int cuda_status(cudaError_t e, const char* what) {
 
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
+// Extents within [2^-18, 2^30]: with at most 4096 cells per axis every
+// extent, cell count and spacing then lies in [2^-30, 2^30], the divisor range
+// of the kernels' division by grid constants.
+inline bool extent_ok(float e) { return e >= 0x1p-18f && e <= 0x1p30f; }
+
 inline bool grid_ok(const FfxGrid* g) {
     return g && g->nx >= 1 && g->ny >= 1 && g->nz >= 1 && g->nx <= 4096 && g->ny <= 4096 && g->nz <= 4096 &&
-           g->ex > 0.f && g->ey > 0.f && g->ez > 0.f &&
+           extent_ok(g->ex) && extent_ok(g->ey) && extent_ok(g->ez) &&
            (int64_t)(g->nx + 1) * (g->ny + 1) * (g->nz + 1) < (int64_t(1) << 31);
 }
 

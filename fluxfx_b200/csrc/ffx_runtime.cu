@@ -256,6 +256,38 @@ int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void*
     return launch_status("dilate_kernel");
 }
 
+// Inputs a, over all 2^32 bit patterns, whose div_rn quotient by b differs
+// from the IEEE division a / b (NaN against NaN counts as equal): count[0]
+// those in div_rn's exact class (+-0, +-inf, NaN, 2^-96 <= |a| <= 2^96),
+// count[1] the others.
+__global__ void __launch_bounds__(256) division_check_kernel(float b, float y, unsigned long long* count) {
+    unsigned long long bad[2] = {0, 0};
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t k = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; k < (1ull << 32); k += stride) {
+        const float a = __uint_as_float((uint32_t)k);
+        const float q = div_rn(a, b, y), ref = a / b;
+        const bool same = __float_as_uint(q) == __float_as_uint(ref) || (q != q && ref != ref);
+        const float m = fabsf(a);
+        const bool exact_class = m == 0.f || m == INFINITY || a != a || (m >= 0x1p-96f && m <= 0x1p96f);
+        bad[exact_class ? 0 : 1] += !same;
+    }
+    for (int j = 0; j < 2; ++j) {
+        unsigned long long v = bad[j];
+        for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+        if ((threadIdx.x & 31) == 0 && v) atomicAdd(count + j, v);
+    }
+}
+
+int ffx_division_mismatches(float divisor, int64_t* count, void* stream) {
+    FFX_REQUIRE(count && divisor >= 0x1p-30f && divisor <= 0x1p30f, "ffx_division_mismatches: invalid arguments");
+    cudaStream_t st = as_stream(stream);
+    int e = cuda_status(cudaMemsetAsync(count, 0, 2 * sizeof(int64_t), st), "ffx_division_mismatches: clear");
+    if (e) return e;
+    division_check_kernel<<<148 * 8, 256, 0, st>>>(divisor, 1.f / divisor,
+                                                    reinterpret_cast<unsigned long long*>(count));
+    return launch_status("division_check_kernel");
+}
+
 int ffx_halo_clearance(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, uint8_t* clear, void* stream) {
     FFX_REQUIRE(grid_ok(g) && solid && halo && clear && solid != halo && solid != clear && halo != clear,
                 "ffx_halo_clearance: invalid arguments");

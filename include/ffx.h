@@ -46,8 +46,8 @@ typedef enum FfxStatus {
 enum { FFX_F32 = 0, FFX_BF16 = 1 };
 
 typedef struct FfxGrid {
-    int32_t nx, ny, nz;   /* cells per axis */
-    float ex, ey, ez;     /* domain extent in metres */
+    int32_t nx, ny, nz;   /* cells per axis, 1 to 4096 */
+    float ex, ey, ez;     /* domain extent in metres, 2^-18 to 2^30 */
     float ix, iy, iz;     /* 1/h of divergence and gradient (the reference's
                              invCell uniform: 1/(extent/n) in FP64, rounded);
                              0 = derive it from ex..ez */
@@ -123,6 +123,15 @@ int ffx_clearance(const FfxGrid* g, const uint8_t* halo, uint8_t* clear, void* s
  * clearance fields, bit for bit, from the mask alone (an extension: moving
  * colliders refresh both after every move). */
 int ffx_halo_clearance(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, uint8_t* clear, void* stream);
+/* Counts the inputs a, over all 2^32 FP32 bit patterns, whose quotient by
+ * `divisor` (in [2^-30, 2^30]) as the kernels form it on grids that are not
+ * powers of two (a reciprocal with two remainder corrections) differs from the
+ * IEEE division a / divisor: count[0] (device int64) over the inputs the form
+ * is exact for (+-0, +-inf, NaN and 2^-96 <= |a| <= 2^96; must be 0),
+ * count[1] over the others (nonzero |a| < 2^-96, finite |a| > 2^96; no grid
+ * position). A check of the library's own arithmetic: no reference
+ * counterpart. */
+int ffx_division_mismatches(float divisor, int64_t* count, void* stream);
 /* out = solid ? 0 : in; replaces shaders/solid_clear.glsl. */
 int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const void* in,
                     void* out, void* stream);
