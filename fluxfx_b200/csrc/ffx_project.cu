@@ -639,6 +639,109 @@ __global__ void __launch_bounds__(256) graph_prolong_smooth_kernel(GLvl g, const
     graph_prolong_smooth_body(g, p, coarse, rhs, omega, out, hw_blk());
 }
 
+// ------------------------------------------ coarse (edge-record) levels: residual + restriction
+// graph_residual_restrict_zero_kernel's pass on levels with edge records,
+// streamed along z (ffx_set_edge_streaming, on by default): every fine
+// residual is formed by the same operations in graph_terms' order (x-, x+, y-,
+// y+, z-, z+) and the eight are added in the restriction's order, so the
+// coarse fields are bit-identical. Measured at 256^3 (levels 128^3 .. 8^3):
+// 18.2 -> 14.4 us on 128^3 and 6.2 -> 4.6-5.1 us on the small levels. The
+// same streaming of the sweep and of prolongation + sweep (x neighbours by
+// shuffle, the slice below carried) was slower than one cell per thread
+// (15.2 against 13.7 us on 128^3; 6.2 against 4.5-5.2 us for the small
+// prolongations): with eight slices per thread the level keeps too few threads
+// in flight to hide L2 latency, so those passes keep their one-cell kernels.
+int g_edge_streaming = 1;   // ffx_set_edge_streaming
+
+__device__ __forceinline__ float edge_comp(const GLvl& g, int i, int c) {
+    return __ldg(reinterpret_cast<const float*>(g.edges) + 4 * i + c);
+}
+
+// Residual + restriction: a thread owns one coarse column (its 2 x 2 fine
+// cells per slice) and walks 2 * chunk fine slices, carrying the iterate and z
+// edge weights of the fine slice below. Each fine slice's four residuals are
+// formed as graph_res forms them and added in the restriction's order
+// (dz, dy, dx).
+__device__ __forceinline__ void graph_residual_restrict_edges_body(const GLvl& g, const float* __restrict__ p,
+                                                                   const float* __restrict__ rhs, float* c,
+                                                                   float* zero, int chunk, const Blk& b) {
+    const int cx = g.nx / 2, cy = g.ny / 2, cz = g.nz / 2;
+    const int X = b.x * b.bw + b.ox, Y = b.y * b.bh + b.oy;
+    if (X >= cx || Y >= cy) return;
+    const int Z0 = b.z * chunk, Zend = min(Z0 + chunk, cz);
+    const int sy = g.nx, sz = g.nx * g.ny;
+    const int x0 = 2 * X, y0 = 2 * Y;
+    // k = 2 * dy + dx indexes the four fine cells of a slice
+    float p_lo[4], wz_lo[4], p_c[4];
+    int base = x0 + g.nx * (y0 + g.ny * (2 * Z0));
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        const int j = base + (k & 1) + sy * (k >> 1);
+        p_c[k] = __ldg(p + j);
+        p_lo[k] = Z0 > 0 ? __ldg(p + j - sz) : 0.f;
+        wz_lo[k] = Z0 > 0 ? edge_comp(g, j - sz, 2) : 0.f;
+    }
+    float v = 0.f;
+    for (int fz = 2 * Z0; fz < 2 * Zend; ++fz, base += sz) {
+        const bool up = fz + 1 < g.nz;
+        float p_hi[4], res[4];
+        float4 E[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int j = base + (k & 1) + sy * (k >> 1);
+            E[k] = __ldg(g.edges + j);
+            p_hi[k] = up ? __ldg(p + j + sz) : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const int dx = k & 1, dy = k >> 1;
+            const int fx = x0 + dx, fy = y0 + dy;
+            const int j = base + dx + sy * dy;
+            const float4 here = E[k];
+            float diag = 0.f, nb = 0.f;
+            if (fx > 0) {
+                const float w = dx ? E[k - 1].x : edge_comp(g, j - 1, 0);
+                diag = diag + w;
+                nb = nb + w * (dx ? p_c[k - 1] : __ldg(p + j - 1));
+            }
+            if (fx + 1 < g.nx) { diag = diag + here.x; nb = nb + here.x * (dx ? __ldg(p + j + 1) : p_c[k + 1]); }
+            if (fy > 0) {
+                const float w = dy ? E[k - 2].y : edge_comp(g, j - sy, 1);
+                diag = diag + w;
+                nb = nb + w * (dy ? p_c[k - 2] : __ldg(p + j - sy));
+            }
+            if (fy + 1 < g.ny) { diag = diag + here.y; nb = nb + here.y * (dy ? __ldg(p + j + sy) : p_c[k + 2]); }
+            if (fz > 0) { diag = diag + wz_lo[k]; nb = nb + wz_lo[k] * p_lo[k]; }
+            if (up) { diag = diag + here.z; nb = nb + here.z * p_hi[k]; }
+            res[k] = diag > 0.f ? (__ldg(rhs + j) - nb) + diag * p_c[k] : 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) v = v + res[k];
+        if (fz & 1) {
+            const int ci = X + cx * (Y + cy * (fz >> 1));
+            c[ci] = v / 8.0f;
+            if (zero) zero[ci] = 0.f;
+            v = 0.f;
+        }
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            p_lo[k] = p_c[k];
+            p_c[k] = p_hi[k];
+            wz_lo[k] = E[k].z;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(256) graph_residual_restrict_edges_kernel(GLvl g, const float* __restrict__ p,
+                                                                           const float* __restrict__ rhs, float* c,
+                                                                           float* zero, int chunk) {
+    graph_residual_restrict_edges_body(g, p, rhs, c, zero, chunk, hw_blk());
+}
+
+// Fine z slices per thread of the streamed restriction: long columns where the
+// level has enough columns to fill the GPU, short ones on small levels.
+inline int edge_chunk(int nx, int ny, int nz) { return (int64_t)nx * ny * nz >= (1 << 20) ? 8 : 2; }
+
 // physics/solid_hierarchy.py:27-53 for one coarse cell.
 __global__ void __launch_bounds__(256) graph_coarsen_kernel(GLvl g, float4* coarse, int* disconnected) {
     const int cx = g.nx / 2, cy = g.ny / 2;
@@ -1199,6 +1302,12 @@ int ffx_graph_residual_restrict_zero(const FfxGraphLevel* lv, const float* p, co
     if (level0_x4(lv, {p, rhs}) && ((uintptr_t)coarse_rhs & 7) == 0 && ((uintptr_t)coarse_p & 7) == 0)
         return level0_residual_restrict(lv, p, rhs, coarse_rhs, coarse_p, as_stream(stream));
     GLvl g = make_glvl(lv);
+    if (g_edge_streaming && g.edges) {
+        const int cz = g.nz / 2, chunk = edge_chunk(g.nx, g.ny, g.nz) / 2;
+        graph_residual_restrict_edges_kernel<<<cell_grid(g.nx / 2, g.ny / 2, (cz + chunk - 1) / chunk), cell_block(),
+                                               0, as_stream(stream)>>>(g, p, rhs, coarse_rhs, coarse_p, chunk);
+        return launch_status("graph_residual_restrict_edges_kernel");
+    }
     graph_residual_restrict_zero_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0,
                                           as_stream(stream)>>>(g, p, rhs, coarse_rhs, coarse_p);
     return launch_status("graph_residual_restrict_kernel");
@@ -1227,6 +1336,12 @@ int ffx_graph_prolong_smooth(const FfxGraphLevel* lv, const float* p, const floa
     graph_prolong_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(
         g, p, coarse, rhs, omega, p_out);
     return launch_status("graph_prolong_smooth_kernel");
+}
+
+int ffx_set_edge_streaming(int enable) {
+    const int previous = g_edge_streaming;
+    g_edge_streaming = enable ? 1 : 0;
+    return previous;
 }
 
 int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float* rhs, float* out, void* stream) {

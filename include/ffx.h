@@ -144,6 +144,10 @@ int ffx_solid_clear(const FfxGrid* g, int storage, const uint8_t* solid, const v
  * bit-identical results; the switch is process-wide and returns the previous
  * setting. No counterpart in the reference (an A/B switch). */
 int ffx_set_transport_tiling(int enable);
+/* Whether the edge-record (coarse) multigrid levels run the residual +
+ * restriction streamed along z (default on) or one coarse cell per thread.
+ * Both give the same fields bit for bit; returns the previous setting. */
+int ffx_set_edge_streaming(int enable);
 /* MacCormack predictor of all three face components in one launch; replaces
  * backend/detail.py:27-37 + shaders/transport_face.glsl. */
 int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
