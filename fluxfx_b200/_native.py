@@ -152,6 +152,7 @@ _PROTOTYPES = {
     'ffx_face_predictor': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, f32, vp, vp, vp, vp]),
     'ffx_set_transport_tiling': (C.c_int, [C.c_int]),
     'ffx_set_edge_streaming': (C.c_int, [C.c_int]),
+    'ffx_set_dependent_launch': (C.c_int, [C.c_int]),
     'ffx_pack_channels': (C.c_int, [i64, C.c_int, P(vp), P(C.c_int), vp, vp]),
     'ffx_loop_begin': (C.c_int, [vp, P(vp)]),
     'ffx_loop_decide': (C.c_int, [vp, vp, vp, C.c_double, C.c_int32, vp, vp]),

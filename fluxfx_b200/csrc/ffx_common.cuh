@@ -179,6 +179,17 @@ inline dim3 face_grid(int nx, int ny, int nz) {
     return dim3((unsigned)((nx + 1 + kBX - 1) / kBX), (unsigned)((ny + 1 + kBY - 1) / kBY), (unsigned)(3 * (nz + 1)));
 }
 
+// Programmatic dependent launch (launch_pdl): a multigrid pass launched that
+// way may be scheduled while the pass before it in the stream is still
+// running. Its first statement lets the pass after it be scheduled the same
+// way, then waits until the pass before it has finished and its memory is
+// visible; only then does it read or write any field. For a pass launched
+// normally both instructions have no effect.
+__device__ __forceinline__ void pdl_enter() {
+    asm volatile("griddepcontrol.launch_dependents;" ::: "memory");
+    asm volatile("griddepcontrol.wait;" ::: "memory");
+}
+
 struct F3 { float x, y, z; };
 __device__ __forceinline__ float comp(const F3& v, int a) { return a == 0 ? v.x : (a == 1 ? v.y : v.z); }
 __device__ __forceinline__ float dot3(const F3& a, const F3& b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }

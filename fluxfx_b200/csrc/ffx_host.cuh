@@ -32,6 +32,34 @@ inline int cuda_status(cudaError_t e, const char* what) {
     return FFX_OK;
 }
 
+// Whether launch_pdl launches with programmatic stream serialization
+// (ffx_set_dependent_launch; on by default).
+extern int g_pdl;
+
+// Launches a kernel that begins with pdl_enter() so that it may be scheduled
+// while the kernel before it in the stream finishes; launch errors map like
+// launch_status.
+template <typename... KArgs, typename... Args>
+inline int launch_pdl(const char* what, void (*kernel)(KArgs...), dim3 grid, dim3 block, cudaStream_t st,
+                      Args... args) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = grid;
+    cfg.blockDim = block;
+    cfg.dynamicSmemBytes = 0;
+    cfg.stream = st;
+    cudaLaunchAttribute attr[1];
+    attr[0].id = cudaLaunchAttributeProgrammaticStreamSerialization;
+    attr[0].val.programmaticStreamSerializationAllowed = 1;
+    cfg.attrs = attr;
+    cfg.numAttrs = g_pdl ? 1 : 0;
+    const cudaError_t e = cudaLaunchKernelEx(&cfg, kernel, static_cast<KArgs>(args)...);
+    if (e != cudaSuccess) {
+        (void)cudaGetLastError();
+        return fail(FFX_ERR_LAUNCH, "%s: %s", what, cudaGetErrorString(e));
+    }
+    return launch_status(what);
+}
+
 inline cudaStream_t as_stream(void* s) { return reinterpret_cast<cudaStream_t>(s); }
 
 // Extents within [2^-18, 2^30]: with at most 4096 cells per axis every

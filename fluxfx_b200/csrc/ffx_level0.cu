@@ -278,6 +278,7 @@ __device__ __forceinline__ void level0_body(const L0& g, const ItArgs& A, const 
 
 template <It K, Ep E>
 __global__ void __launch_bounds__(32 * kRows, 4) level0_kernel(L0 g, ItArgs A, EpArgs P) {
+    pdl_enter();
     level0_body<K, E>(g, A, P, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z, (int)threadIdx.x,
                       (int)threadIdx.y);
 }
@@ -409,6 +410,7 @@ __global__ void __launch_bounds__(32 * kWarps2) level0_smooth2_kernel(L0 g, ItAr
 // read, so this is a plain stream over links and rhs.
 __global__ void __launch_bounds__(256) level0_smooth_zero_kernel(L0 g, const float* __restrict__ rhs, float omega,
                                                                 float* __restrict__ out, int n4) {
+    pdl_enter();
     const int i4 = blockIdx.x * blockDim.x + threadIdx.x;
     if (i4 >= n4) return;
     const uint32_t lk = ld_links(g, i4);
@@ -498,6 +500,7 @@ __global__ void __launch_bounds__(32 * kRows) level0_residual_restrict_kernel(L0
                                                                              const float* __restrict__ rhs,
                                                                              float* __restrict__ coarse,
                                                                              float* __restrict__ zero) {
+    pdl_enter();
     level0_restrict_body(g, p, rhs, coarse, zero, (int)blockIdx.x, (int)blockIdx.y, (int)blockIdx.z,
                          (int)threadIdx.x, (int)threadIdx.y);
 }
@@ -600,8 +603,7 @@ dim3 l0_grid(const L0& g) {
 
 template <It K, Ep E>
 int launch(const L0& g, const ItArgs& A, const EpArgs& P, cudaStream_t st, const char* name) {
-    level0_kernel<K, E><<<l0_grid(g), dim3(32, kRows), 0, st>>>(g, A, P);
-    return launch_status(name);
+    return launch_pdl(name, level0_kernel<K, E>, l0_grid(g), dim3(32, kRows), st, g, A, P);
 }
 
 }  // namespace
@@ -689,8 +691,8 @@ int level0_direction_apply(const FfxGraphLevel* lv, const float* z, const float*
 int level0_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega, float* out, cudaStream_t st) {
     const L0 g = make_l0(lv);
     const int n4 = g.nx4 * g.ny * g.nz;
-    level0_smooth_zero_kernel<<<(unsigned)((n4 + 255) / 256), 256, 0, st>>>(g, rhs, omega, out, n4);
-    return launch_status("level0_smooth_zero_kernel");
+    return launch_pdl("level0_smooth_zero_kernel", level0_smooth_zero_kernel, dim3((unsigned)((n4 + 255) / 256)),
+                      dim3(256), st, g, rhs, omega, out, n4);
 }
 
 int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse,
@@ -698,8 +700,8 @@ int level0_residual_restrict(const FfxGraphLevel* lv, const float* p, const floa
     const L0 g = make_l0(lv);
     const dim3 grid((unsigned)((g.nx4 + 31) / 32), (unsigned)((g.ny / 2 + kRows - 1) / kRows),
                     (unsigned)((g.nz + kZ4 - 1) / kZ4));
-    level0_residual_restrict_kernel<<<grid, dim3(32, kRows), 0, st>>>(g, p, rhs, coarse, zero);
-    return launch_status("level0_residual_restrict_kernel");
+    return launch_pdl("level0_residual_restrict_kernel", level0_residual_restrict_kernel, grid, dim3(32, kRows), st,
+                      g, p, rhs, coarse, zero);
 }
 
 int level0_links(int nx, int ny, int nz, const uint8_t* solid, uint8_t* links, cudaStream_t st) {

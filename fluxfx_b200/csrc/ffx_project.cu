@@ -361,6 +361,7 @@ __global__ void __launch_bounds__(256) mg_prolong_kernel(int nx, int ny, int nz,
 // Dense FP64 mat-vec, one warp per row (coarse_pressure.glsl, solid_mg_direct.glsl).
 __global__ void direct_kernel(int n, const double* __restrict__ inv, const float* __restrict__ rhs, float dt,
                               float* p) {
+    pdl_enter();
     int warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5, lane = threadIdx.x & 31;
     if (warp >= n) return;
     const double* row = inv + (int64_t)warp * n;
@@ -467,6 +468,7 @@ __device__ __forceinline__ void graph_smooth_body(const GLvl& g, const float* __
 
 __global__ void __launch_bounds__(256) graph_smooth_kernel(GLvl g, const float* __restrict__ p,
                                                           const float* __restrict__ rhs, float omega, float* out) {
+    pdl_enter();
     graph_smooth_body(g, p, rhs, omega, out, hw_blk());
 }
 
@@ -537,6 +539,7 @@ __device__ __forceinline__ void graph_smooth_level0_body(const GLvl& g, const fl
 __global__ void __launch_bounds__(256) graph_smooth_level0_kernel(GLvl g, const float* __restrict__ p,
                                                                  const float* __restrict__ rhs, float omega,
                                                                  float* out) {
+    pdl_enter();
     graph_smooth_level0_body(g, p, rhs, omega, out, hw_blk());
 }
 
@@ -569,6 +572,7 @@ __device__ __forceinline__ void graph_residual_max_body(const GLvl& g, const flo
 
 __global__ void __launch_bounds__(256) graph_residual_max_kernel(GLvl g, const float* __restrict__ p,
                                                                 const float* __restrict__ rhs, float* out) {
+    pdl_enter();
     graph_residual_max_body(g, p, rhs, out, hw_blk());
 }
 
@@ -595,6 +599,7 @@ __device__ __forceinline__ void graph_residual_restrict_body(const GLvl& g, cons
 __global__ void __launch_bounds__(256) graph_residual_restrict_zero_kernel(GLvl g, const float* __restrict__ p,
                                                                           const float* __restrict__ rhs, float* c,
                                                                           float* zero) {
+    pdl_enter();
     graph_residual_restrict_body(g, p, rhs, c, zero, hw_blk());
 }
 
@@ -636,6 +641,7 @@ __global__ void __launch_bounds__(256) graph_prolong_smooth_kernel(GLvl g, const
                                                                   const float* __restrict__ coarse,
                                                                   const float* __restrict__ rhs, float omega,
                                                                   float* out) {
+    pdl_enter();
     graph_prolong_smooth_body(g, p, coarse, rhs, omega, out, hw_blk());
 }
 
@@ -735,6 +741,7 @@ __device__ __forceinline__ void graph_residual_restrict_edges_body(const GLvl& g
 __global__ void __launch_bounds__(256) graph_residual_restrict_edges_kernel(GLvl g, const float* __restrict__ p,
                                                                            const float* __restrict__ rhs, float* c,
                                                                            float* zero, int chunk) {
+    pdl_enter();
     graph_residual_restrict_edges_body(g, p, rhs, c, zero, chunk, hw_blk());
 }
 
@@ -930,6 +937,7 @@ __device__ __forceinline__ void graph_tail_body(const TailArgs& A) {
 }
 
 __global__ void __launch_bounds__(kTailThreads) graph_tail_kernel(const __grid_constant__ TailArgs A) {
+    pdl_enter();
     graph_tail_body(A);
 }
 
@@ -999,6 +1007,7 @@ __global__ void __launch_bounds__(256) graph_prolong_smooth_dot_kernel(GLvl g, c
 // First sweep from a zero iterate: p_out = omega * (0 - rhs) / diag on active cells.
 __global__ void __launch_bounds__(256) graph_smooth_zero_kernel(GLvl g, const float* __restrict__ rhs, float omega,
                                                                float* out) {
+    pdl_enter();
     int x, y, z;
     if (!cell_coords(g.nx, g.ny, x, y, z)) return;
     const int i = x + g.nx * (y + g.ny * z);
@@ -1231,8 +1240,8 @@ int ffx_direct_solve(int32_t n, const double* inverse, const float* rhs, float d
                 "ffx_direct_solve: invalid arguments (n in [1, 1024])");
     int threads = 256;
     int blocks = (n * 32 + threads - 1) / threads;
-    direct_kernel<<<blocks, threads, 0, as_stream(stream)>>>(n, inverse, rhs, dt, p);
-    return launch_status("direct_kernel");
+    return launch_pdl("direct_kernel", direct_kernel, dim3(blocks), dim3(threads), as_stream(stream), n, inverse, rhs,
+                      dt, p);
 }
 
 int ffx_mg_residual_max(const int32_t n[3], const float inv[3], const float* p, const float* rhs, float dt,
@@ -1256,12 +1265,11 @@ int ffx_graph_smooth(const FfxGraphLevel* lv, const float* p_in, const float* rh
     GLvl g = make_glvl(lv);
     if (!g.edges) {
         dim3 grid = cell_grid(g.nx, g.ny, (g.nz + kZ - 1) / kZ);
-        graph_smooth_level0_kernel<<<grid, cell_block(), 0, as_stream(stream)>>>(g, p_in, rhs, omega, p_out);
-        return launch_status("graph_smooth_level0_kernel");
+        return launch_pdl("graph_smooth_level0_kernel", graph_smooth_level0_kernel, grid, cell_block(),
+                          as_stream(stream), g, p_in, rhs, omega, p_out);
     }
-    graph_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, p_in, rhs, omega,
-                                                                                             p_out);
-    return launch_status("graph_smooth_kernel");
+    return launch_pdl("graph_smooth_kernel", graph_smooth_kernel, cell_grid(g.nx, g.ny, g.nz), cell_block(),
+                      as_stream(stream), g, p_in, rhs, omega, p_out);
 }
 
 int ffx_graph_smooth2(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega, float* tmp,
@@ -1304,13 +1312,13 @@ int ffx_graph_residual_restrict_zero(const FfxGraphLevel* lv, const float* p, co
     GLvl g = make_glvl(lv);
     if (g_edge_streaming && g.edges) {
         const int cz = g.nz / 2, chunk = edge_chunk(g.nx, g.ny, g.nz) / 2;
-        graph_residual_restrict_edges_kernel<<<cell_grid(g.nx / 2, g.ny / 2, (cz + chunk - 1) / chunk), cell_block(),
-                                               0, as_stream(stream)>>>(g, p, rhs, coarse_rhs, coarse_p, chunk);
-        return launch_status("graph_residual_restrict_edges_kernel");
+        return launch_pdl("graph_residual_restrict_edges_kernel", graph_residual_restrict_edges_kernel,
+                          cell_grid(g.nx / 2, g.ny / 2, (cz + chunk - 1) / chunk), cell_block(), as_stream(stream), g,
+                          p, rhs, coarse_rhs, coarse_p, chunk);
     }
-    graph_residual_restrict_zero_kernel<<<cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), 0,
-                                          as_stream(stream)>>>(g, p, rhs, coarse_rhs, coarse_p);
-    return launch_status("graph_residual_restrict_kernel");
+    return launch_pdl("graph_residual_restrict_kernel", graph_residual_restrict_zero_kernel,
+                      cell_grid(g.nx / 2, g.ny / 2, g.nz / 2), cell_block(), as_stream(stream), g, p, rhs, coarse_rhs,
+                      coarse_p);
 }
 
 int ffx_graph_residual_restrict(const FfxGraphLevel* lv, const float* p, const float* rhs, float* coarse_rhs,
@@ -1333,9 +1341,8 @@ int ffx_graph_prolong_smooth(const FfxGraphLevel* lv, const float* p, const floa
     if (level0_x4(lv, {p, rhs, p_out}) && ((uintptr_t)coarse & 7) == 0)
         return level0_prolong_smooth(lv, p, coarse, rhs, omega, p_out, as_stream(stream));
     GLvl g = make_glvl(lv);
-    graph_prolong_smooth_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(
-        g, p, coarse, rhs, omega, p_out);
-    return launch_status("graph_prolong_smooth_kernel");
+    return launch_pdl("graph_prolong_smooth_kernel", graph_prolong_smooth_kernel, cell_grid(g.nx, g.ny, g.nz),
+                      cell_block(), as_stream(stream), g, p, coarse, rhs, omega, p_out);
 }
 
 int ffx_set_edge_streaming(int enable) {
@@ -1353,8 +1360,7 @@ int ffx_graph_residual_max(const FfxGraphLevel* lv, const float* p, const float*
     if (level0_x4(lv, {p, rhs})) return level0_residual_max(lv, p, rhs, out, st);
     dim3 grid = cell_grid(g.nx, g.ny, 1);
     grid.z = reduce_z(g.nz);
-    graph_residual_max_kernel<<<grid, cell_block(), 0, st>>>(g, p, rhs, out);
-    return launch_status("graph_residual_max_kernel");
+    return launch_pdl("graph_residual_max_kernel", graph_residual_max_kernel, grid, cell_block(), st, g, p, rhs, out);
 }
 
 int ffx_graph_residual_max_smooth(const FfxGraphLevel* lv, const float* p, const float* rhs, float omega,
@@ -1410,8 +1416,7 @@ int ffx_graph_tail(const FfxGraphTail* t, void* stream) {
         A.lv[k].n = lv.nx * lv.ny * lv.nz;
     }
     FFX_REQUIRE(!t->inverse || A.lv[t->count - 1].n <= 1024, "ffx_graph_tail: direct solve limited to 1024 cells");
-    graph_tail_kernel<<<1, kTailThreads, 0, as_stream(stream)>>>(A);
-    return launch_status("graph_tail_kernel");
+    return launch_pdl("graph_tail_kernel", graph_tail_kernel, dim3(1), dim3(kTailThreads), as_stream(stream), A);
 }
 
 int ffx_graph_links(const FfxGraphLevel* lv, uint8_t* links, void* stream) {
@@ -1455,8 +1460,8 @@ int ffx_graph_smooth_zero(const FfxGraphLevel* lv, const float* rhs, float omega
     FFX_REQUIRE(glvl_ok(lv) && rhs && p_out && rhs != p_out, "ffx_graph_smooth_zero: invalid arguments");
     if (level0_x4(lv, {rhs, p_out})) return level0_smooth_zero(lv, rhs, omega, p_out, as_stream(stream));
     GLvl g = make_glvl(lv);
-    graph_smooth_zero_kernel<<<cell_grid(g.nx, g.ny, g.nz), cell_block(), 0, as_stream(stream)>>>(g, rhs, omega, p_out);
-    return launch_status("graph_smooth_zero_kernel");
+    return launch_pdl("graph_smooth_zero_kernel", graph_smooth_zero_kernel, cell_grid(g.nx, g.ny, g.nz), cell_block(),
+                      as_stream(stream), g, rhs, omega, p_out);
 }
 
 int ffx_graph_smooth_dot(const FfxGraphLevel* lv, const float* p_in, const float* rhs, float omega, float* p_out,

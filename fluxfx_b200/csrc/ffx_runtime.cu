@@ -12,6 +12,8 @@ std::string& last_error_buffer() {
     return buf;
 }
 
+int g_pdl = 1;
+
 namespace {
 
 __global__ void probe_kernel(float* out) {
@@ -189,6 +191,12 @@ extern "C" {
 int ffx_abi_version(void) { return FFX_ABI_VERSION; }
 
 const char* ffx_last_error(void) { return last_error_buffer().c_str(); }
+
+int ffx_set_dependent_launch(int enable) {
+    const int previous = g_pdl;
+    g_pdl = enable ? 1 : 0;
+    return previous;
+}
 
 int ffx_device_info(int device, FfxDeviceInfo* out) {
     FFX_REQUIRE(out, "ffx_device_info: out is NULL");

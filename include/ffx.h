@@ -148,6 +148,12 @@ int ffx_set_transport_tiling(int enable);
  * restriction streamed along z (default on) or one coarse cell per thread.
  * Both give the same fields bit for bit; returns the previous setting. */
 int ffx_set_edge_streaming(int enable);
+/* Whether the multigrid passes of the collider solver (level-0 and coarse
+ * sweeps, residual + restriction, prolongation + sweep, the single-block tail,
+ * the convergence test) are launched as programmatic dependent launches, so a
+ * pass is scheduled while the one before it finishes (default on). Results are
+ * the same either way; returns the previous setting. */
+int ffx_set_dependent_launch(int enable);
 /* MacCormack predictor of all three face components in one launch; replaces
  * backend/detail.py:27-37 + shaders/transport_face.glsl. */
 int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
