@@ -181,16 +181,18 @@ __device__ __forceinline__ void face_predictor_face(const PredParams<T>& P, cons
     const uint8_t* __restrict__ halo = P.halo;
     const float dt = step_dt(P);
     T* out = P.out[f.axis];
-    // a clear cell and its lower neighbours are fluid: the face is open
-    const bool clear = MASK && home_clear(P.clear, d, f.x, f.y, f.z);
-    if (MASK && !clear && solid_face(d, solid, f.x, f.y, f.z, f.axis)) {
+    // a clear cell and its lower neighbours are fluid: the face is open (but
+    // for the lower grid wall next to a cell of clearance 2)
+    const int cv = MASK ? home_clearance(P.clear, d, f.x, f.y, f.z) : 0;
+    if (MASK && (cv == 0 ? solid_face(d, solid, f.x, f.y, f.z, f.axis)
+                         : clear_face_blocked(cv, f.x, f.y, f.z, f.axis))) {
         Store<T>::st(out, f.i, 0.f);
         return;
     }
     float ox = f.axis == 0 ? 0.f : 0.5f, oy = f.axis == 1 ? 0.f : 0.5f, oz = f.axis == 2 ? 0.f : 0.5f;
     F3 p = {((float)f.x + ox) * d.h[0], ((float)f.y + oy) * d.h[1], ((float)f.z + oz) * d.h[2]};
     F3 v0 = start_velocity_face<P2>(d, smp, p, f.axis, f.x, f.y, f.z);
-    F3 dep = backtrace_s<MASK, P2>(d, smp, solid, halo, p, v0, dt, clear);
+    F3 dep = backtrace_s<MASK, P2>(d, smp, solid, halo, p, v0, dt, cv);
     float value = smp.sample(f.axis, dv_h<P2>(d, dep.x, 0) - ox, dv_h<P2>(d, dep.y, 1) - oy,
                              dv_h<P2>(d, dep.z, 2) - oz);
     Store<T>::st(out, f.i, value);
@@ -254,8 +256,9 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
         }
     }
     const float dt = step_dt(P);
-    const bool clear = MASK && home_clear(P.clear, d, f.x, f.y, f.z);
-    bool blocked = MASK && !clear && solid_face(d, P.solid, f.x, f.y, f.z, axis);
+    const int cv = MASK ? home_clearance(P.clear, d, f.x, f.y, f.z) : 0;
+    bool blocked = MASK && (cv == 0 ? solid_face(d, P.solid, f.x, f.y, f.z, axis)
+                                    : clear_face_blocked(cv, f.x, f.y, f.z, axis));
     float value = 0.f;
     if (!blocked) {
         float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
@@ -273,7 +276,7 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
             const int nf = P.nf[axis];
             dep = {__ldg(D + f.i), __ldg(D + f.i + nf), __ldg(D + f.i + 2 * nf)};
         } else {
-            dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, clear);
+            dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, cv);
         }
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);
         const T* pred = axis == 0 ? P.P.u : (axis == 1 ? P.P.v : P.P.w);
@@ -299,7 +302,7 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
             bool ok = !(dep.x < lob[0] || dep.y < lob[1] || dep.z < lob[2] || dep.x > hib[0] || dep.y > hib[1] ||
                         dep.z > hib[2] || arr.x < lob[0] || arr.y < lob[1] || arr.z < lob[2] || arr.x > hib[0] ||
                         arr.y > hib[1] || arr.z > hib[2]);
-            if (MASK && ok) ok = safe_correction_from<P2>(d, P.solid, P.halo, clear, p, dep, mid2, arr);
+            if (MASK && ok) ok = safe_correction_from<P2>(d, P.solid, P.halo, cv, p, dep, mid2, arr);
             if (ok) {
                 float pa = smp.sample(3 + axis, dv_h<P2>(d, arr.x, 0) - off[0], dv_h<P2>(d, arr.y, 1) - off[1],
                                       dv_h<P2>(d, arr.z, 2) - off[2]);
@@ -544,13 +547,13 @@ struct ScalarXport {
 // arrival.
 template <bool MASK, bool P2>
 __device__ __forceinline__ bool scalar_correction_ok(const Dev& d, const uint8_t* solid, const uint8_t* halo,
-                                                     bool clear, F3 p, F3 dep, F3 mid2, F3 arr) {
+                                                     int cv, F3 p, F3 dep, F3 mid2, F3 arr) {
     const float lb[3] = {0.5f * d.h[0], 0.5f * d.h[1], 0.5f * d.h[2]};
     const float hb[3] = {d.e[0] - 0.5f * d.h[0], d.e[1] - 0.5f * d.h[1], d.e[2] - 0.5f * d.h[2]};
     bool ok = !(dep.x < lb[0] || dep.y < lb[1] || dep.z < lb[2] || dep.x > hb[0] || dep.y > hb[1] ||
                 dep.z > hb[2] || arr.x < lb[0] || arr.y < lb[1] || arr.z < lb[2] || arr.x > hb[0] ||
                 arr.y > hb[1] || arr.z > hb[2]);
-    if (MASK && ok) ok = safe_correction_from<P2>(d, solid, halo, clear, p, dep, mid2, arr);
+    if (MASK && ok) ok = safe_correction_from<P2>(d, solid, halo, cv, p, dep, mid2, arr);
     return ok;
 }
 
@@ -572,7 +575,8 @@ template <typename T, bool MASK, bool P2, class Smp, bool DECIDE = false>
 __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, int x, int y, int z, const Smp& smp) {
     const Dev& d = P.d;
     const int i = cidx(d, x, y, z);
-    const bool clear = MASK && home_clear(P.clear, d, x, y, z);
+    const int cv = MASK ? home_clearance(P.clear, d, x, y, z) : 0;
+    const bool clear = cv != 0;
     if (MASK && !clear && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.out[c], i, 0.f);
         return;
@@ -588,18 +592,18 @@ __device__ __forceinline__ void scalar_transport_cell(const ScalarXport<T>& P, i
         // pass's correction test is decided here
         const float dtr = step_dt(P), s = 0.5f * dtr;
         const F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
-        const F3 midc = MASK ? clip_from<P2>(d, P.solid, P.halo, clear, p, mid) : mid;
+        const F3 midc = MASK ? clip_from<P2>(d, P.solid, P.halo, cv, p, mid) : mid;
         const F3 vm = velocity_s<P2>(d, smp, midc);
         F3 arr = {p.x - dtr * vm.x, p.y - dtr * vm.y, p.z - dtr * vm.z};
-        dep = MASK ? clip_from<P2>(d, P.solid, P.halo, clear, p, arr) : arr;
+        dep = MASK ? clip_from<P2>(d, P.solid, P.halo, cv, p, arr) : arr;
         if (!same_bits(midc, mid)) {
             const F3 vm2 = velocity_s<P2>(d, smp, mid);
             arr = {p.x - dtr * vm2.x, p.y - dtr * vm2.y, p.z - dtr * vm2.z};
         }
         const F3 fdep = {__ldg(P.fdep + i), __ldg(P.fdep + i + P.n), __ldg(P.fdep + i + 2 * P.n)};
-        P.ok[i] = scalar_correction_ok<MASK, P2>(d, P.solid, P.halo, clear, p, fdep, mid, arr) ? 1 : 0;
+        P.ok[i] = scalar_correction_ok<MASK, P2>(d, P.solid, P.halo, cv, p, fdep, mid, arr) ? 1 : 0;
     } else {
-        dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P), clear);
+        dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, step_dt(P), cv);
     }
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
@@ -675,7 +679,8 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
                                                     float vmax[3]) {
     const Dev& d = P.d;
     const int i = cidx(d, x, y, z);
-    const bool clear = MASK && home_clear(P.clear, d, x, y, z);
+    const int cv = MASK ? home_clearance(P.clear, d, x, y, z) : 0;
+    const bool clear = cv != 0;
     if (MASK && !clear && __ldg(P.solid + i)) {
         for (int c = 0; c < P.count; ++c) Store<T>::st(P.ch[c].out, i, 0.f);
         return;
@@ -691,7 +696,7 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
     if (!decided) v0 = start_velocity_s<P2>(d, smp, p, 2 * x + 1, 2 * y + 1, 2 * z + 1);
     F3 dep;
     if (reuse) dep = {__ldg(P.dep + i), __ldg(P.dep + i + P.n), __ldg(P.dep + i + 2 * P.n)};
-    else dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, clear);
+    else dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, cv);
     float qx = dv_h<P2>(d, dep.x, 0) - 0.5f, qy = dv_h<P2>(d, dep.y, 1) - 0.5f,
           qz = dv_h<P2>(d, dep.z, 2) - 0.5f;
     bool ok = false;
@@ -703,7 +708,7 @@ __device__ __forceinline__ void advect_scalars_cell(const ScalarFinal<T>& P, int
         F3 mid2 = {p.x + s * v0.x, p.y + s * v0.y, p.z + s * v0.z};
         F3 vm2 = velocity_s<P2>(d, smp, mid2);
         F3 arr = {p.x + dt * vm2.x, p.y + dt * vm2.y, p.z + dt * vm2.z};
-        ok = scalar_correction_ok<MASK, P2>(d, P.solid, P.halo, clear, p, dep, mid2, arr);
+        ok = scalar_correction_ok<MASK, P2>(d, P.solid, P.halo, cv, p, dep, mid2, arr);
     }
     // lower corner of the departure cell (the clamp bounds: its 8 corners clamped to the grid)
     const int bx = ok ? (int)floorf(qx) : 0, by = ok ? (int)floorf(qy) : 0, bz = ok ? (int)floorf(qz) : 0;

@@ -475,26 +475,42 @@ __device__ __forceinline__ bool safe_solid_correction(const Dev& d, const uint8_
 }
 
 // ---------------------------------------------------------------- clearance
-// `clear` (ffx_clearance) marks the cells with no solid and no out-of-domain
-// cell within Chebyshev distance 3 (so every cell within distance 1 of them
-// lies at distance >= 3, every cell within distance 2 at distance >= 2 from
-// the nearest solid or outside cell). Let p be the start point of a face or
-// cell whose own cell c (its integer cell coordinates) is clear, and t a
-// target within 0.75 h of p on every axis:
-//  * floor(p / h * n) is c or a neighbour of c (rounding of the grid
-//    coordinate), so the trace's start cell is at distance >= 3 and t's cell,
-//    within one cell of it, at distance >= 2: both lie in the grid at least one
-//    cell from the walls, with a clear 3x3x3 block (halo 0);
-//  * clip_solid_trace(p, t) therefore takes its fast path with unclamped grid
-//    coordinates and returns t / e * n / n * e (clear_clip), which is t itself
-//    when e, n and h are powers of two (exact rescalings);
-//  * safe_solid_correction(p, dep, mid, arr) with all three near p finds every
+// `clear` (ffx_clearance, ffx_halo_clearance) holds one byte per cell:
+//   1  no solid and no out-of-domain cell within Chebyshev distance 3;
+//   2  no solid cell within distance 3, but an out-of-domain one (the cell lies
+//      within three cells of a wall); ffx_clearance, which sees only the
+//      dilated mask, never writes 2;
+//   0  otherwise.
+// Let p be the start point of a face or cell whose own cell c (its integer
+// cell coordinates) has a nonzero value, and t a target within 0.75 h of p on
+// every axis. floor(p / h * n) is c or a neighbour of c (rounding of the grid
+// coordinate), and t's cell lies within one cell of that.
+//  * Value 1: both cells lie at distance >= 2 from every solid or outside
+//    cell, with a clear 3x3x3 block (halo 0), so clip_solid_trace(p, t) takes
+//    its fast path with unclamped grid coordinates and returns t / e * n / n *
+//    e (clear_clip), which is t itself when e, n and h are powers of two; and
+//    safe_solid_correction(p, dep, mid, arr) with all three near p finds every
 //    probe inside the grid with a clear halo and every segment on the fast
 //    path, so it reduces to the three distance tests of the fast values
 //    (clear_correction), always true on power-of-two grids.
+//  * Value 2: every cell the functions visit lies within distance 3 of c and
+//    is not a solid; only the grid's walls can matter. The clip's grid
+//    coordinates are clamped to [1e-4, n - 1e-4], so a traversal of at most
+//    0.75 cells (plus rounding) never crosses a wall: the crossing parameter
+//    of a wall exceeds 1 by at least 1e-4 / 0.76, far beyond rounding. So
+//    clip_solid_trace(p, t), fast path or traversal, returns the clamped
+//    rescale (wall_clip). In safe_solid_correction a probe cell has halo 0
+//    exactly when it lies in [1, n - 2] on every axis (inner); when p's cell
+//    does, the midpoint is at least 0.25 cells from the walls and unclamped,
+//    as are the departure and arrival points whose cells do, so the test
+//    reduces to inner(p), inner(dep), inner(arr) and clear_correction
+//    (wall_correction). A face of the cell is blocked only at the lower grid
+//    wall (its lower cell lies outside); the cell itself is fluid, and so are
+//    the clamped corners of a scalar sample within 0.75 h.
 // Both forms give the functions' results bit for bit and skip their mask reads.
-__device__ __forceinline__ bool home_clear(const uint8_t* __restrict__ clear, const Dev& d, int x, int y, int z) {
-    return clear != nullptr && x < d.nx && y < d.ny && z < d.nz && __ldg(clear + cidx(d, x, y, z)) != 0;
+__device__ __forceinline__ int home_clearance(const uint8_t* __restrict__ clear, const Dev& d, int x, int y,
+                                              int z) {
+    return clear != nullptr && x < d.nx && y < d.ny && z < d.nz ? (int)__ldg(clear + cidx(d, x, y, z)) : 0;
 }
 
 __device__ __forceinline__ bool near_start(const Dev& d, F3 p, F3 t) {
@@ -513,6 +529,34 @@ __device__ __forceinline__ F3 clear_clip(const Dev& d, F3 t) {
     }
 }
 
+// clip_solid_trace's value for a cell of clearance 2 (its fast-path formula
+// with the wall clamp).
+template <bool P2>
+__device__ __forceinline__ F3 wall_clip(const Dev& d, F3 t) {
+    const float tt[3] = {t.x, t.y, t.z};
+    float r[3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const float b = fminf(fmaxf(dv_e<P2>(d, tt[i], i) * d.nf[i], 0.0001f), d.nf[i] - 0.0001f);
+        r[i] = dv_n<P2>(d, b, i) * d.e[i];
+    }
+    return F3{r[0], r[1], r[2]};
+}
+
+// The probe cell of t (probe_inside) lies in [1, n - 2] on every axis.
+template <bool P2>
+__device__ __forceinline__ bool inner_cell(const Dev& d, F3 t) {
+    const float tt[3] = {t.x, t.y, t.z};
+    const int n[3] = {d.nx, d.ny, d.nz};
+    bool in = true;
+#pragma unroll
+    for (int i = 0; i < 3; ++i) {
+        const int c = (int)fmaxf(fminf(floorf(dv_e<P2>(d, tt[i], i) * d.nf[i]), 1.0e9f), -1.0e9f);
+        in = in && c >= 1 && c <= n[i] - 2;
+    }
+    return in;
+}
+
 template <bool P2>
 __device__ __forceinline__ bool clear_correction(const Dev& d, F3 dep, F3 mid, F3 arr) {
     if constexpr (P2) {
@@ -523,21 +567,29 @@ __device__ __forceinline__ bool clear_correction(const Dev& d, F3 dep, F3 mid, F
     }
 }
 
-// clip_solid_trace(p, t), through the clear form where it applies.
+// clip_solid_trace(p, t), through the clear forms where they apply (cv: the
+// start cell's clearance).
 template <bool P2>
-__device__ __forceinline__ F3 clip_from(const Dev& d, const uint8_t* solid, const uint8_t* halo, bool clear, F3 p,
+__device__ __forceinline__ F3 clip_from(const Dev& d, const uint8_t* solid, const uint8_t* halo, int cv, F3 p,
                                         F3 t) {
-    if (clear && near_start(d, p, t)) return clear_clip<P2>(d, t);
+    if (cv != 0 && near_start(d, p, t)) return cv == 1 ? clear_clip<P2>(d, t) : wall_clip<P2>(d, t);
     return clip_solid_trace<P2>(d, solid, halo, p, t);
 }
 
-// safe_solid_correction(p, dep, mid, arr), through the clear form where it applies.
+// safe_solid_correction(p, dep, mid, arr), through the clear forms where they apply.
 template <bool P2>
 __device__ __forceinline__ bool safe_correction_from(const Dev& d, const uint8_t* solid, const uint8_t* halo,
-                                                     bool clear, F3 p, F3 dep, F3 mid, F3 arr) {
-    if (clear && near_start(d, p, dep) && near_start(d, p, mid) && near_start(d, p, arr))
-        return clear_correction<P2>(d, dep, mid, arr);
+                                                     int cv, F3 p, F3 dep, F3 mid, F3 arr) {
+    if (cv != 0 && near_start(d, p, dep) && near_start(d, p, mid) && near_start(d, p, arr))
+        return (cv == 1 || (inner_cell<P2>(d, p) && inner_cell<P2>(d, dep) && inner_cell<P2>(d, arr))) &&
+               clear_correction<P2>(d, dep, mid, arr);
     return safe_solid_correction<P2>(d, solid, halo, p, dep, mid, arr);
+}
+
+// solid_face for a face whose own cell has a nonzero clearance cv: only the
+// lower grid wall (the face's lower cell outside) can block it.
+__device__ __forceinline__ bool clear_face_blocked(int cv, int x, int y, int z, int axis) {
+    return cv == 2 && (axis == 0 ? x : (axis == 1 ? y : z)) == 0;
 }
 
 // ---------------------------------------------------------------- emitters

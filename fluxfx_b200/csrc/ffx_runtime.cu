@@ -115,14 +115,15 @@ __global__ void clearance_kernel(Dev d, const uint8_t* __restrict__ halo, uint8_
 }
 
 // The dilated mask and the clearance of a mask in one pass (ffx_halo_clearance):
-// halo = any solid or outside cell in the 3x3x3 block (dilate_kernel's field),
-// clear = no solid or outside cell in the 7x7x7 block (clearance_kernel's
-// field of that halo: no halo or outside cell within distance 2 means no solid
-// or outside cell within distance 3). A block owns 32 x 8 columns and a chunk of
-// kHZ slices; per slice it stages the 38 x 14 window of the mask (outside = 1),
+// halo = any solid or outside cell in the 3x3x3 block (dilate_kernel's field);
+// clear = 1 where the 7x7x7 block holds no solid and no outside cell
+// (clearance_kernel's value), 2 where it holds no solid but reaches outside the
+// grid, 0 where it holds a solid. A block owns 32 x 8 columns and a chunk of
+// kHZ slices; per slice it stages the 38 x 14 window of the mask (outside = 0),
 // dilates it along x and then y in shared memory, and every thread keeps the
 // last seven slices' (x, y) dilations as bits, so the z dilation is a mask of
-// those bits.
+// those bits; the outside cells within distance 1 or 3 follow from the cell's
+// coordinates.
 constexpr int kHX = 32, kHY = 8, kHZ = 16, kHR = 3;
 constexpr int kWinX = kHX + 2 * kHR, kWinY = kHY + 2 * kHR;
 
@@ -140,7 +141,7 @@ __global__ void __launch_bounds__(kHX * kHY) halo_clear_kernel(Dev d, const uint
             const int wy = e / kWinX, wx = e - wy * kWinX;
             const int gx = x0 - kHR + wx, gy = y0 - kHR + wy;
             const bool out = gx < 0 || gy < 0 || zs < 0 || gx >= d.nx || gy >= d.ny || zs >= d.nz;
-            win[wy][wx] = out ? 1 : (__ldg(solid + cidx(d, gx, gy, zs)) != 0);
+            win[wy][wx] = out ? 0 : (__ldg(solid + cidx(d, gx, gy, zs)) != 0);
         }
         __syncthreads();
         for (int e = tid; e < kWinY * kHX; e += kHX * kHY) {
@@ -159,8 +160,10 @@ __global__ void __launch_bounds__(kHX * kHY) halo_clear_kernel(Dev d, const uint
         const int z = zs - kHR;   // slices z - 3 .. z + 3 are bits 6 .. 0
         if (z >= z0 && z < zend && x < d.nx && y < d.ny) {
             const int i = cidx(d, x, y, z);
-            halo[i] = ((h1 >> 2) & 7u) != 0u;
-            clear[i] = (h3 & 0x7fu) == 0u;
+            const bool wall1 = x < 1 || y < 1 || z < 1 || x > d.nx - 2 || y > d.ny - 2 || z > d.nz - 2;
+            const bool wall3 = x < 3 || y < 3 || z < 3 || x > d.nx - 4 || y > d.ny - 4 || z > d.nz - 4;
+            halo[i] = wall1 || ((h1 >> 2) & 7u) != 0u;
+            clear[i] = (h3 & 0x7fu) != 0u ? 0 : (wall3 ? 2 : 1);
         }
         __syncthreads();
     }

@@ -487,16 +487,16 @@ __device__ __forceinline__ F3 start_velocity_face(const Dev& d, const S& smp, F3
 }
 
 // Midpoint backtrace through a sampler (the `backtrace` of the transport
-// passes); `clear`: the start point's own cell is clear (home_clear).
+// passes); `cv`: the clearance of the start point's own cell (home_clearance).
 template <bool MASK, bool P2, class S>
 __device__ __forceinline__ F3 backtrace_s(const Dev& d, const S& smp, const uint8_t* solid, const uint8_t* halo, F3 p,
-                                          F3 v0, float dt, bool clear = false) {
+                                          F3 v0, float dt, int cv = 0) {
     const float s = 0.5f * dt;
     F3 mid = {p.x - s * v0.x, p.y - s * v0.y, p.z - s * v0.z};
-    if (MASK) mid = clip_from<P2>(d, solid, halo, clear, p, mid);
+    if (MASK) mid = clip_from<P2>(d, solid, halo, cv, p, mid);
     const F3 vm = velocity_s<P2>(d, smp, mid);
     F3 dep = {p.x - dt * vm.x, p.y - dt * vm.y, p.z - dt * vm.z};
-    if (MASK) dep = clip_from<P2>(d, solid, halo, clear, p, dep);
+    if (MASK) dep = clip_from<P2>(d, solid, halo, cv, p, dep);
     return dep;
 }
 

@@ -58,9 +58,11 @@ typedef struct FfxSolids {
     const uint8_t* halo;  /* nx*ny*nz dilated mask (ffx_dilate_mask) */
     const float* wall[3]; /* moving colliders: velocity of every wall and solid face
                              (face grids, ffx_moving_walls); NULL = 0 (static walls) */
-    const uint8_t* clear; /* optional, with a mask: nx*ny*nz clearance (ffx_clearance); the
-                             transport passes skip the collider tests of traces that start
-                             in a clear cell and stay within 0.75 cells (same results) */
+    const uint8_t* clear; /* optional, with a mask: nx*ny*nz clearance (ffx_clearance: 0/1;
+                             ffx_halo_clearance: 0/1/2, 2 = no solid within three cells but
+                             a wall); the transport passes skip the collider tests of traces
+                             that start in a cell of nonzero clearance and stay within 0.75
+                             cells (same results) */
 } FfxSolids;
 
 /* Moving colliders per solver (the reference's wall table holds 8). */
@@ -119,9 +121,12 @@ int ffx_dilate_mask(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, void*
  * the collider tests (solid_boundary.glsl, correct_*.glsl) where they cannot
  * change the result. One-time work per collider layout. */
 int ffx_clearance(const FfxGrid* g, const uint8_t* halo, uint8_t* clear, void* stream);
-/* ffx_dilate_mask and ffx_clearance of a mask in one pass: the same halo and
- * clearance fields, bit for bit, from the mask alone (an extension: moving
- * colliders refresh both after every move). */
+/* ffx_dilate_mask and the clearance of a mask in one pass (an extension:
+ * moving colliders refresh both after every move). halo is ffx_dilate_mask's
+ * field bit for bit; clear is 1 where ffx_clearance writes 1 (no solid and no
+ * outside cell within distance 3), 2 where no solid but an outside cell lies
+ * within distance 3, 0 elsewhere. The transport passes take both nonzero
+ * values through FfxSolids.clear. */
 int ffx_halo_clearance(const FfxGrid* g, const uint8_t* solid, uint8_t* halo, uint8_t* clear, void* stream);
 /* Counts the inputs a, over all 2^32 FP32 bit patterns, whose quotient by
  * `divisor` (in [2^-30, 2^30]) as the kernels form it on grids that are not
