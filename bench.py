@@ -92,10 +92,12 @@ def pass_bytes(s):
     }
 
 
-def trace_bytes(face_trace=True):
-    """Per cell, the departure points written by the predictors and read by the
-    corrections (faces only where both passes form the same start points)."""
-    ft = 36 if face_trace else 0
+def trace_bytes(face_trace=True, storage='BF16'):
+    """Per cell, the traces written by the predictors and read by the
+    corrections (faces only where both passes form the same start points): per
+    face the departure point and the start velocity, and in BF16 storage the
+    unrounded sample, 4 bytes each, for three faces per cell."""
+    ft = 3 * 4 * (7 if storage == 'BF16' else 6) if face_trace else 0
     return {'velocity_predictor': ft, 'velocity_transport': ft, 'scalar_predictor_reverse': 12,
             'scalar_transport': 12}
 
@@ -401,7 +403,7 @@ def run_b200(args):
         hbm, peak_kind = peaks()
         s = 4 if args.storage == 'FP32' else 2
         ft = N.grid_pow2((n, n, n), (1.0, 1.0, 1.0))
-        pb, tb = pass_bytes(s), trace_bytes(ft)
+        pb, tb = pass_bytes(s), trace_bytes(ft, args.storage)
         pass_report = {}
         for name, ms in passes.items():
             per_step = ms / args.steps
@@ -534,7 +536,7 @@ def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True, sm_mhz=No
             "traffic": MEASURED_TRAFFIC.get((round(cells ** (1 / 3)), s)),
             "traffic_source": "ncu dram read+write of one launch (same scene and storage), not measured in this run",
             "algorithmic_bytes_per_launch": per_cell * cells,
-            "design_trace_bytes_per_launch": trace_bytes(face_trace)['velocity_transport'] * cells,
+            "design_trace_bytes_per_launch": trace_bytes(face_trace, 'FP32' if s == 4 else 'BF16')['velocity_transport'] * cells,
             "avg_launch_ms": ms, "limiter": "instruction issue",
             "issue": issue_roofline(ms, cells, s, sm_mhz),
             "timing": "CUDA events bracketing the launch in every timed step"}

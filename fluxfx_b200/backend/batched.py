@@ -143,7 +143,7 @@ class BatchedSmoke:
         dev = s.device.device
         if D.velocity_corrected and det.reuse_traces and det._face_reuse:
             if det.face_trace is None:
-                det.face_trace = [torch.empty(3 * prod(sh), dtype=torch.float32, device=dev)
+                det.face_trace = [torch.empty(6 * prod(sh), dtype=torch.float32, device=dev)
                                   for sh in s.grid.face_shapes]
             for a in range(3):
                 D.face_trace[a] = det.face_trace[a].data_ptr()

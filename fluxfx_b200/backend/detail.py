@@ -101,7 +101,8 @@ class DetailPasses:
             self.face_predictor = [self.device.texture(s, dtype=self.dtype) for s in self.grid.face_shapes]
         if self.reuse_traces and self._face_reuse and self.face_trace is None:
             # x, y, z of each departure point, plus (16-bit storage) the unrounded sample
-            planes = 3 if self.dtype == torch.float32 else 4
+            # departure point, (BF16) the unrounded sample, start velocity
+            planes = 6 if self.dtype == torch.float32 else 7
             self.face_trace = [torch.empty(planes * prod(s), dtype=torch.float32, device=self.device.device)
                                for s in self.grid.face_shapes]
         name, step = ('ffx_face_predictor_dt', dt_device) if dt_device is not None else ('ffx_face_predictor_trace', dt)

@@ -204,6 +204,11 @@ __device__ __forceinline__ void face_predictor_face(const PredParams<T>& P, cons
         // 16-bit storage rounds the stored predictor: its FP32 value, the
         // correction's semi-Lagrangian sample, goes to a fourth plane
         if (sizeof(T) == 2) D[f.i + 3 * nf] = value;
+        // the start velocity, which the correction would form again at the same point
+        constexpr int kV0 = sizeof(T) == 2 ? 4 : 3;
+        D[f.i + kV0 * nf] = v0.x;
+        D[f.i + (kV0 + 1) * nf] = v0.y;
+        D[f.i + (kV0 + 2) * nf] = v0.z;
     }
 }
 
@@ -264,18 +269,21 @@ __device__ __forceinline__ void advect_velocity_face(const VelParams<T>& P, cons
         float off[3] = {axis == 0 ? 0.f : 0.5f, axis == 1 ? 0.f : 0.5f, axis == 2 ? 0.f : 0.5f};
         F3 p = {dv_n<P2>(d, ((float)f.x + off[0]) * d.e[0], 0), dv_n<P2>(d, ((float)f.y + off[1]) * d.e[1], 1),
                 dv_n<P2>(d, ((float)f.z + off[2]) * d.e[2], 2)};
-        F3 v0 = start_velocity_face<P2>(d, smp, p, axis, f.x, f.y, f.z);
-        // The host passes the predictor's departure points only when both passes
-        // form the same start point at every face (face_starts_match); the
-        // predictor then traced this face's start point with the same velocity,
-        // so its departure point, and in FP32 storage its sample, are this pass's.
+        // The host passes the predictor's traces only when both passes form the
+        // same start point at every face (face_starts_match); the predictor then
+        // traced this face's start point with the same velocity, so its start
+        // velocity, its departure point, and in FP32 storage its sample, are this
+        // pass's.
         const bool reuse = P.corrected && P.dep[axis] != nullptr;
-        F3 dep;
+        F3 v0, dep;
         if (reuse) {
             const float* D = P.dep[axis];
             const int nf = P.nf[axis];
+            constexpr int kV0 = sizeof(T) == 2 ? 4 : 3;
             dep = {__ldg(D + f.i), __ldg(D + f.i + nf), __ldg(D + f.i + 2 * nf)};
+            v0 = {__ldg(D + f.i + kV0 * nf), __ldg(D + f.i + (kV0 + 1) * nf), __ldg(D + f.i + (kV0 + 2) * nf)};
         } else {
+            v0 = start_velocity_face<P2>(d, smp, p, axis, f.x, f.y, f.z);
             dep = backtrace_s<MASK, P2>(d, smp, P.solid, P.halo, p, v0, dt, cv);
         }
         const T* orig = axis == 0 ? P.F.u : (axis == 1 ? P.F.v : P.F.w);

@@ -164,11 +164,12 @@ int ffx_set_dependent_launch(int enable);
 int ffx_face_predictor(const FfxGrid* g, const FfxSolids* s, int storage,
                        const void* u, const void* v, const void* w, float dt,
                        void* pu, void* pv, void* pw, void* stream);
-/* The same, also storing each open face's departure point in dep[axis] (three
- * planes of (nx+a0)(ny+a1)(nz+a2) floats: x, y, z) for ffx_advect_velocity_trace.
- * With storage FFX_BF16 each dep[axis] holds a fourth plane: the face's sample
- * before rounding to storage, which the velocity correction reads as its
- * semi-Lagrangian value. */
+/* The same, also storing each open face's trace in dep[axis], planes of
+ * (nx+a0)(ny+a1)(nz+a2) floats for ffx_advect_velocity_trace: FFX_F32 storage
+ * six planes (departure point x, y, z; start velocity x, y, z), FFX_BF16 seven
+ * (departure point x, y, z; the face's sample before rounding to storage, which
+ * the velocity correction reads as its semi-Lagrangian value; start velocity
+ * x, y, z). */
 int ffx_face_predictor_trace(const FfxGrid* g, const FfxSolids* s, int storage,
                              const void* u, const void* v, const void* w, float dt,
                              void* pu, void* pv, void* pw, float* const dep[3], void* stream);
@@ -188,7 +189,8 @@ int ffx_advect_velocity(const FfxGrid* g, const FfxSolids* s, int storage,
  * of the same faces and dt) instead of tracing again; used on grids whose extent, cell
  * count and spacing are powers of two, where both passes form the same start point, so
  * the result is unchanged (and the semi-Lagrangian sample is the predictor's value:
- * the stored face in FP32 storage, the fourth trace plane in BF16 storage).
+ * the stored face in FP32 storage, the fourth trace plane in BF16 storage; the
+ * start velocity is the predictor's too).
  * dep == NULL or other grids: ffx_advect_velocity. */
 int ffx_advect_velocity_trace(const FfxGrid* g, const FfxSolids* s, int storage,
                               const void* u, const void* v, const void* w,
@@ -721,9 +723,10 @@ typedef struct FfxBatchDomain {
     int32_t warm_start;                /* 1: start each solve from the previous step's pressure scaled by
                                           dt / previous dt (backend/pressure.py:63-75), 0: from zero */
     double tolerance;                  /* relative max-norm residual target (> 0) */
-    float* face_trace[3];              /* optional departure points of the face predictor (three planes
-                                          per face grid; power-of-two grids only), reused by the
-                                          velocity pass as in ffx_advect_velocity_trace */
+    float* face_trace[3];              /* optional traces of the face predictor (six planes per face
+                                          grid, the FP32 layout of ffx_face_predictor_trace;
+                                          power-of-two grids only), reused by the velocity pass as in
+                                          ffx_advect_velocity_trace */
     float* cell_trace;                 /* optional departure points of the scalar predictor (three
                                           planes of cells), reused by the final scalar pass */
     const uint8_t* clear;              /* optional clearance of the mask (ffx_clearance), as FfxSolids.clear */
