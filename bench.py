@@ -141,6 +141,12 @@ def scene(n, storage='FP32', seed=0, **overrides):
     return grid, settings, (sphere, box), emitters, noise
 
 
+def replica_seed(seed, rank):
+    """Seed of rank ``rank``'s domain: with --gpus N every rank advances its own
+    independent replica of the scene (no data crosses ranks on the step path)."""
+    return seed + rank
+
+
 def build_solver(n, storage, seed, device, **overrides):
     import torch
     from fluxfx_b200.backend.projected import DenseProjectedSmoke
@@ -243,7 +249,8 @@ class Run:
             if args.coarse_scale is not None:
                 overrides['mg_coarse_scale'] = args.coarse_scale
             overrides.update(parse_settings(args.set))
-        self.solver, self.emitters = build_solver(args.size, storage, args.seed + rank, device, **overrides)
+        self.solver, self.emitters = build_solver(args.size, storage, replica_seed(args.seed, rank), device,
+                                                  **overrides)
         if args.host_loop:
             # the V-cycle loop on the host (one residual readback per cycle): the same
             # kernels, launched from replayed graphs -- for profilers that do not list
