@@ -65,6 +65,8 @@ VARIANTS = {
     'plain': dict(pressure_method='VCYCLE', solid_warm_start=False),
     'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True, mg_coarse_scale=1.9),
     'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9),
+    'extrapolated': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9,
+                         warm_start_extrapolation=1.0),
     'learned_plain': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
     'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
     'learned_ir': dict(pressure_method='IR', solid_warm_start=False, learned_warm_start=True, mg_coarse_scale=1.9),
@@ -400,12 +402,15 @@ def run_b200(args):
     # (beside the previous-pressure headline), or the previous pressure
     alt_variant = 'learned' if args.variant != 'learned' else 'fast'
     fast = compare(alt_variant, args.compare_fast, args.storage)
+    # the extrapolated start against the previous pressure alone
+    previous = compare('fast', args.compare_fast and args.variant == 'extrapolated', args.storage)
     learned = compare('learned_plain', args.compare_learned, args.storage)
     learned32 = compare(args.variant, args.compare_storage, 'FP32')
 
-    elapsed, e2e_time, p_el, f_el, l_el, s_el = max_over_ranks(
+    elapsed, e2e_time, p_el, f_el, l_el, s_el, v_el = max_over_ranks(
         [elapsed, e2e_time, plain['elapsed'] if plain else 0.0, fast['elapsed'] if fast else 0.0,
-         learned['elapsed'] if learned else 0.0, learned32['elapsed'] if learned32 else 0.0], world)
+         learned['elapsed'] if learned else 0.0, learned32['elapsed'] if learned32 else 0.0,
+         previous['elapsed'] if previous else 0.0], world)
     if rank == 0:
         hbm, peak_kind = peaks()
         s = 4 if args.storage == 'FP32' else 2
@@ -462,11 +467,26 @@ def run_b200(args):
                                       "trilinear prolongation) as the start of every solve, then over-corrected "
                                       "V(4,4) cycles" if alt_variant == 'learned' else
                                       "over-corrected V(4,4) cycles from the previous step's pressure (no network)")},
-                       "headline_note": ("variant fast: the previous step's pressure (times dt / previous dt) starts "
-                                         "every solve, over-corrected V(4,4) cycles (alpha 1.9); measured beside it, "
-                                         "the U-Net guess every step (learned_every_step) saves a fraction of a "
-                                         "V-cycle against the previous pressure and costs more than it saves, so "
-                                         "the faster form is the headline" if args.variant == 'fast' else None),
+                       "previous_pressure_start": None if previous is None else {
+                           "steps_per_s": job_rate(world, previous['steps'], v_el), "steps": previous['steps'],
+                           "v_cycles_mean": previous['cycles'], "final_rel_div_inf": previous['rel_div'],
+                           "final_rel_div_inf_fp32": previous['rel_div32'], "storage": previous['storage'],
+                           "speedup_vs_plain": None if plain is None else
+                           job_rate(world, previous['steps'], v_el) / job_rate(world, plain['steps'], p_el),
+                           "method": "variant fast: the previous step's pressure times dt / previous dt alone "
+                                     "starts every solve (no extrapolation)"},
+                       "headline_note": ({
+                           'fast': "variant fast: the previous step's pressure (times dt / previous dt) starts "
+                                   "every solve, over-corrected V(4,4) cycles (alpha 1.9); measured beside it, "
+                                   "the U-Net guess every step (learned_every_step) saves a fraction of a "
+                                   "V-cycle against the previous pressure and costs more than it saves, so "
+                                   "the faster form is the headline",
+                           'extrapolated': "variant extrapolated: the last two solves' pressures, extrapolated "
+                                           "linearly in time, start every solve; over-corrected V(4,4) cycles "
+                                           "(alpha 1.9); measured beside it, the previous pressure alone "
+                                           "(previous_pressure_start) and the U-Net guess every step "
+                                           "(learned_every_step), which saves a fraction of a V-cycle against the "
+                                           "previous pressure and costs more than it saves"}.get(args.variant)),
                        "same_solver_fp32_storage": None if learned32 is None else {
                            "steps_per_s": job_rate(world, learned32['steps'], s_el), "steps": learned32['steps'],
                            "v_cycles_mean": learned32['cycles'], "final_rel_div_inf": learned32['rel_div'],
@@ -893,7 +913,7 @@ def main():
                     help='run the V-cycle loop on the host (for kernel-listing profilers)')
     ap.add_argument('--no-compare-storage', dest='compare_storage', action='store_false',
                     help='skip the headline variant with FP32 storage')
-    ap.add_argument('--variant', default='fast', choices=tuple(VARIANTS))
+    ap.add_argument('--variant', default='extrapolated', choices=tuple(VARIANTS))
     ap.add_argument('--seed', type=int, default=0)
     ap.add_argument('--cpu-sample', type=int, default=64)
     ap.add_argument('--no-cpu-baseline', dest='cpu_baseline', action='store_false')

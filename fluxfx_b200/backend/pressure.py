@@ -41,6 +41,11 @@ class PressureProjector:
         self.before = dev.texture(grid.shape)
         self.after = dev.texture(grid.shape)
         self._scalars = torch.zeros(8, dtype=torch.float32, device=dev.device)   # device-side maxima
+        # warm-start extrapolation: the previous solve's pressure per unit time
+        # (allocated on first use) and whether it holds one
+        self._history = None
+        self._history_valid = False
+        self._host_clock = None
         self.ready = False
         self.last_dt = None
         self.last_iterations = 0
@@ -79,6 +84,7 @@ class PressureProjector:
         self.ready = False
         self.last_dt = None
         self.last_iterations = 0
+        self._history_valid = False
         for t in (self.pressure, self.spare, self.before, self.after, *self.bounded):
             t.zero_()
 
@@ -115,9 +121,13 @@ class PressureProjector:
         self.compute_divergence(self.bounded, self.before)
         self.ready = False
         previous = self.last_dt is not None
-        if previous:
+        if previous and self.extrapolation_beta() > 0:
+            self._extrapolate(clock)
+        elif previous:
             self.device.call('ffx_scale_by_ratio', self.pressure.numel(), ptr(self.pressure), ptr(clock),
                              self.device.s)
+        else:
+            self._history_valid = False
         self.solve_pressure(1.0, 1.0 if previous else None)
         self._gradient(outputs, 1.0)
         self.last_dt = clock        # the previous dt now lives on the device (clock[1] after the step)
@@ -154,15 +164,39 @@ class PressureProjector:
         impulse = self.uses_impulse
         solve_dt = 1.0 if impulse else dt
         previous_solve_dt = (1.0 if previous_dt is not None else None) if impulse else previous_dt
-        if impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
+        if impulse and previous_dt is not None and self.extrapolation_beta() > 0:
+            if self._host_clock is None:
+                self._host_clock = torch.zeros(2, dtype=torch.float32, device=self.device.device)
+            self._host_clock.copy_(torch.tensor([dt, previous_dt], dtype=torch.float32))
+            self._extrapolate(self._host_clock)
+        elif impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
             # The incremental pressure force scales with physical dt: rescale the
             # guess (in place, so the pressure keeps its buffer from step to step).
             self.device.call('ffx_scale', self.pressure.numel(), ptr(self.pressure), dt / previous_dt,
                              ptr(self.pressure), self.device.s)
+        if previous_dt is None:
+            self._history_valid = False
         self.solve_pressure(solve_dt, previous_solve_dt)
         self._gradient(outputs, solve_dt)
         self.last_dt = dt
         self.ready = True
+
+    def extrapolation_beta(self):
+        """beta of the warm start extrapolated in time, or 0 where the solve
+        does not start from the previous pressure."""
+        return 0.0
+
+    def _extrapolate(self, clock):
+        """Start the next solve from the last two pressures extrapolated in
+        time (ffx_extrapolate_pressure; ``clock`` = device (dt, previous dt)).
+        The first call after a cold solve has one pressure only and applies the
+        ratio rule."""
+        if self._history is None:
+            self._history = self.device.texture(self.grid.shape)
+        self.device.call('ffx_extrapolate_pressure', self.pressure.numel(), ptr(self.pressure), ptr(self._history),
+                         ptr(clock), float(self.extrapolation_beta()), 0 if self._history_valid else 1,
+                         self.device.s)
+        self._history_valid = True
 
     def gradient_links(self):
         """Level-0 link bytes of the collider mask (ffx_graph_links) for the

@@ -706,6 +706,12 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.learned.guess(r, e)
         dev.call('ffx_add', self.pressure.numel(), ptr(self.pressure), ptr(e), ptr(self.pressure), dev.s)
 
+    def extrapolation_beta(self):
+        s = self.settings
+        if s.warm_start_extrapolation > 0 and s.solid_warm_start and not s.learned_warm_start and len(self.levels) > 1:
+            return s.warm_start_extrapolation
+        return 0.0
+
     def attach_learned(self, model):
         """Pressure guess used when ``learned_warm_start`` is set
         (``fluxfx_b200.learned.LearnedWarmStart``)."""

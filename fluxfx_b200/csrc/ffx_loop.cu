@@ -13,6 +13,9 @@
 // ffx_loop_decide again; ffx_loop_end_while closes the body; the caller may
 // issue passes after the loop on its stream; ffx_loop_end instantiates. Every
 // launch of the result (ffx_loop_launch) runs the whole solve.
+#include <cmath>
+#include <cstdint>
+
 #include "ffx_host.cuh"
 
 struct FfxLoop {
@@ -78,6 +81,46 @@ __global__ void scale_by_ratio_kernel(int64_t n, float* p, const float* clock) {
     const float f = (float)ratio;
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
         p[i] = p[i] * f;
+}
+
+// Warm start extrapolated linearly in time. The impulse pressure of a solve is
+// dt times the pressure per unit time, P. With P1 = p / d1 (the last solve,
+// d1 = previous dt) and P2 = hist (the solve before it, stored by the previous
+// call), the next solve (dt = d0) starts from d0 * (P1 + beta * (d0 / d1) *
+// (P1 - P2)), and hist becomes P1. `first` (no older solve): P2 is not used,
+// so p takes the ratio rule of scale_by_ratio_kernel and hist becomes P1.
+// Coefficients in FP64, the update in FP32, four cells per thread.
+__device__ __forceinline__ void extrapolate_cell(float& p, float& h, float c1, float c2, float inv, bool first) {
+    const float v = p;
+    p = first ? v * c1 : c1 * v - c2 * h;
+    h = v * inv;
+}
+
+__global__ void extrapolate_kernel(int64_t n, float* p, float* hist, const float* clock, float beta, int first) {
+    const float dt = clock[0], prev = clock[1];
+    if (!(prev > 0.f)) return;
+    const double d0 = dt, d1 = prev, r = d0 / d1;
+    const float inv = (float)(1.0 / d1);
+    const float c1 = first ? (fabs(r - 1.0) > 1e-6 ? (float)r : 1.f) : (float)(d0 * (1.0 + (double)beta * r) / d1);
+    const float c2 = first ? 0.f : (float)(d0 * (double)beta * r);
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t quads = n / 4;
+    float4* p4 = reinterpret_cast<float4*>(p);
+    float4* h4 = reinterpret_cast<float4*>(hist);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < quads; i += stride) {
+        float4 v = p4[i], h = first ? make_float4(0.f, 0.f, 0.f, 0.f) : h4[i];
+        extrapolate_cell(v.x, h.x, c1, c2, inv, first);
+        extrapolate_cell(v.y, h.y, c1, c2, inv, first);
+        extrapolate_cell(v.z, h.z, c1, c2, inv, first);
+        extrapolate_cell(v.w, h.w, c1, c2, inv, first);
+        p4[i] = v;
+        h4[i] = h;
+    }
+    for (int64_t i = 4 * quads + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float h = first ? 0.f : hist[i];
+        extrapolate_cell(p[i], h, c1, c2, inv, first);
+        hist[i] = h;
+    }
 }
 
 }  // namespace
@@ -147,6 +190,19 @@ int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream
     const int64_t want = (count + 255) / 256;
     scale_by_ratio_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(count, p, clock);
     return launch_status("scale_by_ratio_kernel");
+}
+
+int ffx_extrapolate_pressure(int64_t count, float* p, float* hist, const float* clock, float beta, int32_t first,
+                             void* stream) {
+    FFX_REQUIRE(count >= 1 && p && hist && clock && p != hist && std::isfinite(beta) && beta >= 0.f && beta <= 1.f &&
+                    (first == 0 || first == 1),
+                "ffx_extrapolate_pressure: invalid arguments (beta in [0, 1], first 0 or 1, distinct buffers)");
+    FFX_REQUIRE(reinterpret_cast<uintptr_t>(p) % 16 == 0 && reinterpret_cast<uintptr_t>(hist) % 16 == 0,
+                "ffx_extrapolate_pressure: p and hist must be 16-byte aligned");
+    const int64_t want = (count / 4 + 255) / 256;
+    const int64_t blocks = want < 1 ? 1 : (want < 148 * 8 ? want : 148 * 8);
+    extrapolate_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(count, p, hist, clock, beta, first);
+    return launch_status("extrapolate_kernel");
 }
 
 int ffx_loop_while(FfxLoop* L, void** body_stream) {

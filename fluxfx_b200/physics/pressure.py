@@ -30,6 +30,11 @@ Extensions (all default to the reference's behaviour):
   true FP32 residual of the pressure, decides convergence in FP64, solves the
   correction equation from zero with ``ir_inner_cycles`` V-cycles and adds the
   correction (collider multigrid with a tolerance).
+* ``warm_start_extrapolation`` -- with ``solid_warm_start`` (and no learned
+  warm start): beta in [0, 1]. The solve starts from the previous two
+  pressures extrapolated linearly in time, P1 + beta (dt / dt1) (P1 - P2) in
+  pressure per unit time, instead of the previous pressure alone (0, the
+  default). Same system, same tolerance; only the start differs.
 """
 from dataclasses import dataclass
 from math import fsum, isfinite, sqrt
@@ -112,6 +117,7 @@ class PressureSettings(ThermalSettings):
     mg_coarse_scale: float = 1.0
     learned_correction: bool = False
     ir_inner_cycles: int = 1
+    warm_start_extrapolation: float = 0.0
 
     def __post_init__(self):
         super().__post_init__()
@@ -156,6 +162,9 @@ class PressureSettings(ThermalSettings):
             raise ValueError("Learned warm start must be boolean")
         if not isfinite(self.mg_coarse_scale) or not 0 < self.mg_coarse_scale < 2:
             raise ValueError("Coarse-correction factor must lie in (0, 2)")
+        if (type(self.warm_start_extrapolation) not in (int, float) or not isfinite(self.warm_start_extrapolation)
+                or not 0 <= self.warm_start_extrapolation <= 1):
+            raise ValueError("Warm-start extrapolation must lie in [0, 1]")
 
 
 def divergence_stats(before, after):

@@ -559,6 +559,16 @@ int ffx_next_dt(const float* maxima, float* clock, double* time, double cell, do
  * than 1e-6 (FP64): the impulse warm start's rescaling (backend/pressure.py:63-75)
  * with the time steps on the device. */
 int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream);
+/* Warm start extrapolated linearly in time (an extension; the reference's warm
+ * start is the ratio rule of ffx_scale_by_ratio, backend/pressure.py:63-75). The
+ * impulse pressure is dt times the pressure per unit time P. With P1 = p / clock[1]
+ * (the last solve) and P2 = hist (the same quantity from the solve before), sets
+ * p = clock[0] * (P1 + beta * (clock[0] / clock[1]) * (P1 - P2)) and hist = P1.
+ * first = 1 (no older solve): p takes ffx_scale_by_ratio's rule and hist = P1.
+ * Nothing changes when clock[1] <= 0. beta in [0, 1]; p and hist distinct,
+ * 16-byte aligned, count floats each. */
+int ffx_extrapolate_pressure(int64_t count, float* p, float* hist, const float* clock, float beta,
+                             int32_t first, void* stream);
 
 /* ------------------------------------------------------- sparse brick path */
 /* Brick pool: the topology of FluxFX_Source/native/bricks.hpp:14-94 (fixed

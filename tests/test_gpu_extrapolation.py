@@ -1,0 +1,122 @@
+"""Warm start extrapolated in time (warm_start_extrapolation, an extension).
+
+The kernel (ffx_extrapolate_pressure) against its formula, bit for bit (the
+library is built without FMA contraction, so c1*v - c2*h rounds like NumPy's
+FP32 products and difference); the solver with the extrapolated start against
+the same solver started from the previous pressure: every step meets the
+tolerance, the extrapolated start needs no more V-cycles, and the two runs
+stay within what the solve tolerance allows of each other."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from fluxfx_b200 import _native as N
+from tests.gpu_helpers import dev, n
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope='module')
+def D():
+    return dev()
+
+
+def _ptr(t):
+    return C.c_void_p(t.data_ptr())
+
+
+def _expected(p, hist, dt, prev, beta, first):
+    d0, d1 = float(np.float32(dt)), float(np.float32(prev))
+    r = d0 / d1
+    inv = np.float32(1.0 / d1)
+    if first:
+        c1 = np.float32(r) if abs(r - 1.0) > 1e-6 else np.float32(1.0)
+        return p * c1, p * inv
+    c1 = np.float32(d0 * (1.0 + beta * r) / d1)
+    c2 = np.float32(d0 * beta * r)
+    return c1 * p - c2 * hist, p * inv
+
+
+@pytest.mark.parametrize('count', [4096, 1001])
+@pytest.mark.parametrize('first', [0, 1])
+@pytest.mark.parametrize('clock', [(0.0019, 0.0021), (0.02, 0.02), (0.02, 0.02 * (1 + 1e-7))])
+def test_extrapolate_kernel_matches_its_formula(D, count, first, clock):
+    lib = N.load()
+    rng = np.random.default_rng(count + first)
+    p0 = rng.normal(size=count).astype(np.float32) * 3e-3
+    h0 = rng.normal(size=count).astype(np.float32)
+    beta = 1.0
+    p, h = torch.as_tensor(p0).cuda(), torch.as_tensor(h0).cuda()
+    ck = torch.tensor(clock, dtype=torch.float32, device='cuda')
+    N.check(lib.ffx_extrapolate_pressure(count, _ptr(p), _ptr(h), _ptr(ck), beta, first, None))
+    torch.cuda.synchronize()
+    want_p, want_h = _expected(p0, h0, clock[0], clock[1], beta, first)
+    assert np.array_equal(p.cpu().numpy(), want_p)
+    assert np.array_equal(h.cpu().numpy(), want_h)
+
+
+def test_extrapolate_kernel_without_previous_step_and_invalid_arguments(D):
+    lib = N.load()
+    p = torch.ones(64, device='cuda')
+    h = torch.full((64,), 2.0, device='cuda')
+    ck = torch.tensor([0.02, 0.0], dtype=torch.float32, device='cuda')   # no previous dt
+    N.check(lib.ffx_extrapolate_pressure(64, _ptr(p), _ptr(h), _ptr(ck), 1.0, 0, None))
+    torch.cuda.synchronize()
+    assert (p.cpu() == 1).all() and (h.cpu() == 2).all()
+    bad = [(64, p, h, 1.5, 0), (64, p, h, -0.1, 0), (64, p, p, 1.0, 0), (0, p, h, 1.0, 0), (64, p, h, 1.0, 2)]
+    for count, a, b, beta, first in bad:
+        rc = lib.ffx_extrapolate_pressure(count, _ptr(a), _ptr(b), _ptr(ck), beta, first, None)
+        assert rc == N.FFX_ERR_INVALID
+    # a pointer off the 16-byte grid is rejected before any launch
+    rc = lib.ffx_extrapolate_pressure(60, C.c_void_p(p.data_ptr() + 4), _ptr(h), _ptr(ck), 1.0, 0, None)
+    assert rc == N.FFX_ERR_INVALID
+    assert b'16-byte' in lib.ffx_last_error()
+
+
+def _solver(D, size, beta):
+    import bench
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    grid, s, colliders, emitters, noise = bench.scene(size, 'FP32', 0, **bench.VARIANTS['fast'],
+                                                      warm_start_extrapolation=beta)
+    solver = DenseProjectedSmoke(grid, s, D, colliders=colliders)
+    zeros = torch.zeros(grid.cells)
+    solver.upload(zeros)
+    solver.upload_temperature(zeros)
+    solver.upload_velocity([torch.as_tensor(v) for v in noise])
+    return solver, emitters
+
+
+def _rel_l2(a, b):
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize('device_steps', [True, False])
+def test_extrapolated_warm_start_meets_tolerance_with_fewer_cycles(D, device_steps):
+    """Both runs solve the same systems to relative max-norm divergence
+    <= 1e-4 every step; they start each solve from different guesses, so
+    their fields separate only by the accumulated solve error (the bounds of
+    the headline-solver test: 1e-3 relative L2 for the scalars, 1e-2 for the
+    velocity)."""
+    size, steps = 64, 12
+    runs = {beta: _solver(D, size, beta) for beta in (0.0, 1.0)}
+    cycles = {beta: [] for beta in runs}
+    for k in range(steps):
+        for beta, (solver, emitters) in runs.items():
+            if device_steps:
+                solver.step_cfl(0.5, 0.02, sources=emitters)
+            else:
+                solver.step(0.02 if k == 0 else min(0.02, 0.5 / size / max(solver.projector.velocity_maxima())),
+                            sources=emitters)
+            assert solver.measure_projection()['rel_div_inf'] <= 1e-4, (beta, k)
+            cycles[beta].append(solver.projector.last_cycles)
+    print('cycles per step: previous pressure %s, extrapolated %s' % (cycles[0.0], cycles[1.0]))
+    assert sum(cycles[1.0][3:]) < sum(cycles[0.0][3:])
+    A, B = runs[1.0][0], runs[0.0][0]
+    assert _rel_l2(n(A.density), n(B.density)) <= 1e-3
+    assert _rel_l2(n(A.temperature), n(B.temperature)) <= 1e-3
+    for a in range(3):
+        assert _rel_l2(n(A._velocity[a]), n(B._velocity[a])) <= 1e-2, a
+    for solver, _ in runs.values():
+        solver.close()

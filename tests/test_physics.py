@@ -186,3 +186,12 @@ def test_rigid_collider_motion_rows():
         validate_motion((a,), (primitive('BOX', (0.4, 0.5, 0.5), (0.1, 0.3, 0.1)),))
     with pytest.raises(ValueError):
         validate_motion((a,), (a, b))
+
+
+def test_warm_start_extrapolation_setting():
+    assert PressureSettings().warm_start_extrapolation == 0.0     # the reference's start by default
+    assert PressureSettings(warm_start_extrapolation=1).warm_start_extrapolation == 1
+    assert PressureSettings(warm_start_extrapolation=0.5, solid_warm_start=True).warm_start_extrapolation == 0.5
+    for bad in (-0.1, 1.5, math.nan, math.inf, '1', True):
+        with pytest.raises(ValueError):
+            PressureSettings(warm_start_extrapolation=bad)
