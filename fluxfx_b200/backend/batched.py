@@ -52,8 +52,10 @@ def _check_solver(i, s):
         problems.append('needs the collider multigrid with at least two levels')
     elif not p.uses_impulse:
         problems.append('needs the impulse pressure form')
-    if st.pressure_method != 'VCYCLE' or st.learned_warm_start:
+    if st.pressure_method != 'VCYCLE' or st.learned_warm_start or st.warm_start_extrapolation > 0:
         problems.append('stand-alone V-cycles required (from zero or the previous pressure)')
+    if st.mg_coarse_sweeps and st.mg_coarse_sweeps != p.pre_sweeps or st.mg_coarse_sweeps and p.pre_sweeps != p.post_sweeps:
+        problems.append('the same sweep counts on every level required')
     if not st.pressure_tolerance > 0:
         problems.append('a pressure tolerance is required')
     if st.moving_colliders or st.vorticity_strength > 0 or s.combustion is not None:

@@ -88,6 +88,9 @@ class SolidMultigridProjector(SolidPressureProjector):
         self.prolong_kernel = KernelHandle('solid_mg_prolong.glsl')
         self.pre_sweeps = s.mg_pre_sweeps or 4
         self.post_sweeps = s.mg_post_sweeps or 4
+        # sweeps on the levels below level 0 (the same counts unless mg_coarse_sweeps is set)
+        self.coarse_pre = s.mg_coarse_sweeps or self.pre_sweeps
+        self.coarse_post = s.mg_coarse_sweeps or self.post_sweeps
         self.last_cycles = 0
         self.timer = None
         self.learned = None
@@ -263,7 +266,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         the levels from the first one (below level 0) with at most TAIL_CELLS
         cells down to the coarsest, at most eight of them. Needs an even number
         of sweeps per level and cycle, so buffer roles repeat."""
-        if (self.pre_sweeps + self.post_sweeps) % 2 or len(self.levels) < 3:
+        if (self.coarse_pre + self.coarse_post) % 2 or len(self.levels) < 3:
             return None, None
         start = next((k for k in range(1, len(self.levels)) if prod(self.levels[k]['shape']) <= TAIL_CELLS), None)
         if start is None or (start == len(self.levels) - 1 and self.coarse_matrix is not None):
@@ -273,7 +276,7 @@ class SolidMultigridProjector(SolidPressureProjector):
         start = max(start, len(self.levels) - N.TAIL_LEVELS)
         tail = N.FfxGraphTail()
         tail.count = len(self.levels) - start
-        tail.pre, tail.post, tail.omega = self.pre_sweeps, self.post_sweeps, 2.0 / 3.0
+        tail.pre, tail.post, tail.omega = self.coarse_pre, self.coarse_post, 2.0 / 3.0
         tail.inverse = self.coarse_matrix.data_ptr() if self.coarse_matrix is not None else None
         for k, level in enumerate(self.levels[start:]):
             slot = tail.levels[k]
@@ -345,7 +348,7 @@ class SolidMultigridProjector(SolidPressureProjector):
             if dot is not None:
                 dev.call('ffx_dot', level['p'].numel(), ptr(level['rhs']), ptr(level['p']), -1.0, ptr(dot), dev.s)
             return
-        pre = self.pre_sweeps
+        pre, post = (self.pre_sweeps, self.post_sweeps) if index == 0 else (self.coarse_pre, self.coarse_post)
         fuse = not first_pre and self._fuse_cycle(level, zero_init, dot)
         if first_pre and pre > 0:
             level['p'], level['q'] = level['q'], level['p']
@@ -373,32 +376,32 @@ class SolidMultigridProjector(SolidPressureProjector):
             self.last_iterations += self._tail_sweeps()
         else:
             self.cycle(index + 1)
-        if self.post_sweeps == 1 and dot is not None:
+        if post == 1 and dot is not None:
             dev.call('ffx_graph_prolong_smooth_dot', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), ptr(dot), -1.0, dev.s)
             level['p'], level['q'] = level['q'], level['p']
             self.last_iterations += 1
             return
-        if fuse and self.post_sweeps > 1:
+        if fuse and post > 1:
             # prolongation + the first two post-sweeps in one pass (ffx_graph_prolong_smooth2)
             dev.call('ffx_graph_prolong_smooth2', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['rhs']), 2.0 / 3.0, None, ptr(level['q']), dev.s)
             level['p'], level['q'] = level['q'], level['p']
             self.last_iterations += 2
-            self.smooth(level, self.post_sweeps - 2, fuse)
-        elif self.post_sweeps > 0:
+            self.smooth(level, post - 2, fuse)
+        elif post > 0:
             dev.call('ffx_graph_prolong_smooth', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['rhs']), 2.0 / 3.0, ptr(level['q']), dev.s)
             level['p'], level['q'] = level['q'], level['p']
             self.last_iterations += 1
-            if dot is not None and self.post_sweeps > 1:
-                self.smooth(level, self.post_sweeps - 2)
+            if dot is not None and post > 1:
+                self.smooth(level, post - 2)
                 dev.call('ffx_graph_smooth_dot', C.byref(level['graph']), ptr(level['p']), ptr(level['rhs']),
                          2.0 / 3.0, ptr(level['q']), ptr(dot), -1.0, dev.s)
                 level['p'], level['q'] = level['q'], level['p']
                 self.last_iterations += 1
                 return
-            self.smooth(level, self.post_sweeps - 1)
+            self.smooth(level, post - 1)
         else:
             dev.call('ffx_graph_prolong', C.byref(level['graph']), ptr(level['p']), ptr(coarse['p']),
                      ptr(level['q']), dev.s)
@@ -408,7 +411,7 @@ class SolidMultigridProjector(SolidPressureProjector):
 
     def _tail_sweeps(self):
         n = len(self.levels) - self.tail_start - 1
-        return n * (self.pre_sweeps + self.post_sweeps) + (0 if self.coarse_matrix is not None else 80)
+        return n * (self.coarse_pre + self.coarse_post) + (0 if self.coarse_matrix is not None else 80)
 
     def _residual_max(self):
         level = self.levels[0]

@@ -9,6 +9,9 @@ Extensions (all default to the reference's behaviour):
   ``pressure_max_cycles``.
 * ``mg_pre_sweeps`` / ``mg_post_sweeps`` -- 0 keeps the reference's sweeps
   (3/3 geometric, 4/4 collider aggregation).
+* ``mg_coarse_sweeps`` -- collider multigrid: 0 keeps the level-0 sweep counts
+  on every level (the reference); N runs N pre- and N post-sweeps on every
+  level below level 0 (level 0 keeps ``mg_pre_sweeps`` / ``mg_post_sweeps``).
 * ``mg_max_levels`` -- 0 keeps the reference's hierarchy (halve while all axes
   are even and the smallest is >= 8); N caps it at N levels.
 * ``heat_mode`` -- "RATE" (reference: temperature emission is additive) or
@@ -67,6 +70,7 @@ _INT_RANGES = (
     ("mg_pre_sweeps", 0, 16, "Multigrid sweeps must be integers in [0, 16]"),
     ("mg_post_sweeps", 0, 16, "Multigrid sweeps must be integers in [0, 16]"),
     ("mg_max_levels", 0, 16, "Multigrid level cap must be an integer in [0, 16]"),
+    ("mg_coarse_sweeps", 0, 16, "Coarse-level sweeps must be an integer in [0, 16]"),
     ("ir_inner_cycles", 1, 16, "Inner refinement cycles must be an integer in [1, 16]"),
 )
 
@@ -118,6 +122,7 @@ class PressureSettings(ThermalSettings):
     learned_correction: bool = False
     ir_inner_cycles: int = 1
     warm_start_extrapolation: float = 0.0
+    mg_coarse_sweeps: int = 0
 
     def __post_init__(self):
         super().__post_init__()

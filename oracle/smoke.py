@@ -961,9 +961,11 @@ def graph_prolong(p, coarse, edges, alpha=1.0):
 class SolidMG:
     """Aggregation V-cycle (``backend/solid_multigrid.py:7-76``)."""
 
-    def __init__(self, levels, pre=4, post=4, coarse_solver='DIRECT', dtype=np.float32, alpha=1.0):
+    def __init__(self, levels, pre=4, post=4, coarse_solver='DIRECT', dtype=np.float32, alpha=1.0, coarse_sweeps=0):
         self.levels = levels
         self.pre, self.post = pre, post
+        # the coarse-sweeps extension: N pre- and post-sweeps below level 0 (0: the same as level 0)
+        self.cpre, self.cpost = (coarse_sweeps, coarse_sweeps) if coarse_sweeps else (pre, post)
         self.alpha = alpha
         self.dtype = np.dtype(dtype)
         shape, edges = levels[-1]
@@ -986,12 +988,13 @@ class SolidMG:
                 return (self.inverse @ r).astype(self.dtype).reshape(rhs.shape)
             return self.smooth(level, p, rhs, 80)
         edges = self.levels[level][1]
-        p = self.smooth(level, p, rhs, self.pre)
+        pre, post = (self.pre, self.post) if level == 0 else (self.cpre, self.cpost)
+        p = self.smooth(level, p, rhs, pre)
         r = graph_residual(p, rhs, edges)
         crhs = restrict(r)
         cp = self.cycle(level + 1, np.zeros_like(crhs), crhs)
         p = graph_prolong(p, cp, edges, self.alpha)
-        return self.smooth(level, p, rhs, self.post)
+        return self.smooth(level, p, rhs, post)
 
 
 def raster_mask(g, colliders):

@@ -31,6 +31,7 @@ class OracleProjector:
         self.s = settings
         self.kind = kind                      # JACOBI | MULTIGRID | SOLID_JACOBI | SOLID_MULTIGRID
         self.pressure = g.zeros(g.cell_shape)
+        self.history = None          # the extrapolated warm start's previous pressure per unit time
         self.last_dt = None
         self.last_iterations = 0
         self.last_cycles = 0
@@ -58,7 +59,7 @@ class OracleProjector:
             hier = S.build_hierarchy(g.shape, g.extent64, g.mask, s.mg_max_levels)
             self.levels = [h[0] for h in hier]
             self.mg = S.SolidMG(hier, s.mg_pre_sweeps or 4, s.mg_post_sweeps or 4, s.coarse_solver, g.dt,
-                                getattr(s, 'mg_coarse_scale', 1.0))
+                                getattr(s, 'mg_coarse_scale', 1.0), getattr(s, 'mg_coarse_sweeps', 0))
 
     @property
     def uses_impulse(self):
@@ -69,6 +70,7 @@ class OracleProjector:
 
     def reset(self):
         self.pressure = self.g.zeros(self.g.cell_shape)
+        self.history = None
         self.last_dt = None
         self.last_iterations = 0
         self.last_cycles = 0
@@ -156,13 +158,40 @@ class OracleProjector:
         impulse = self.uses_impulse
         solve_dt = 1.0 if impulse else dt
         previous_solve = (1.0 if previous_dt is not None else None) if impulse else previous_dt
-        if impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
+        beta = getattr(self.s, 'warm_start_extrapolation', 0.0)
+        extrapolates = (beta > 0 and self.kind == 'SOLID_MULTIGRID' and len(self.levels) > 1
+                        and self.s.solid_warm_start and not getattr(self.s, 'learned_warm_start', False))
+        if impulse and previous_dt is not None and extrapolates:
+            self.pressure, self.history = extrapolate(self.pressure, self.history, dt, previous_dt, beta)
+        elif impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
             self.pressure = self.pressure * g.f(dt / previous_dt)
+        if previous_dt is None:
+            self.history = None
         self.solve(before, solve_dt, previous_solve)
         out = S.gradient(g, bounded, self.pressure, solve_dt)
         after = S.divergence(g, out)
         self.last_dt = dt
         return out, before, after
+
+
+def extrapolate(p, history, dt, previous_dt, beta):
+    """The extrapolated warm start (an extension of the solver, not in the
+    reference): with P1 = p / previous dt and P2 = history, the start is
+    dt (P1 + beta (dt / previous dt) (P1 - P2)); returns (start, P1). The time
+    steps are rounded to FP32 first (the device keeps them as floats), the
+    coefficients formed in FP64 and the update done in FP32, as the device
+    pass does; without a history (the first warm solve) the start is the
+    dt / previous dt rescale."""
+    d0, d1 = float(np.float32(dt)), float(np.float32(previous_dt))
+    r = d0 / d1
+    p = np.asarray(p, np.float32)
+    new_history = p * np.float32(1.0 / d1)
+    if history is None:
+        c1 = np.float32(r) if abs(r - 1.0) > 1e-6 else np.float32(1.0)
+        return p * c1, new_history
+    c1 = np.float32(d0 * (1.0 + beta * r) / d1)
+    c2 = np.float32(d0 * beta * r)
+    return c1 * p - c2 * np.asarray(history, np.float32), new_history
 
 
 def projector_kind(grid_shape, settings, has_mask):

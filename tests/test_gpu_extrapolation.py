@@ -120,3 +120,42 @@ def test_extrapolated_warm_start_meets_tolerance_with_fewer_cycles(D, device_ste
         assert _rel_l2(n(A._velocity[a]), n(B._velocity[a])) <= 1e-2, a
     for solver, _ in runs.values():
         solver.close()
+
+
+@pytest.mark.parametrize('coarse_sweeps', [0, 2])
+def test_extended_solver_matches_oracle_on_collider_scene(D, coarse_sweeps):
+    """The collider scene at 64^3 with the extrapolated start (beta = 1) and,
+    optionally, two pre- and post-sweeps on the levels below level 0, against
+    the CPU oracle with the same settings: per step and field within 1e-5 of
+    the field's maximum, the same V-cycle counts. Host steps (dt from the
+    device's face maxima on both sides), six steps: the extrapolation starts
+    at the third."""
+    import bench
+    from fluxfx_b200.backend.projected import DenseProjectedSmoke
+    from fluxfx_b200.physics.emission import pack_sources
+    from oracle import solver as O
+    from tests.test_gpu_configs import cfl_dt, compare_step
+    grid, s, colliders, emitters, noise = bench.scene(64, 'FP32', 0, **bench.VARIANTS['extrapolated'],
+                                                      mg_coarse_sweeps=coarse_sweeps)
+    solver = DenseProjectedSmoke(grid, s, D, colliders=colliders)
+    if coarse_sweeps:
+        assert solver.projector.coarse_pre == solver.projector.coarse_post == coarse_sweeps
+    mask = n(solver.solids.mask).astype(bool)
+    ref = O.OracleSmoke(grid.shape, grid.extent, s, np.float32, mask=mask)
+    zeros = np.zeros(grid.cells, np.float32)
+    solver.upload(torch.as_tensor(zeros))
+    solver.upload_temperature(torch.as_tensor(zeros))
+    solver.upload_velocity([torch.as_tensor(v) for v in noise])
+    ref.upload(density=zeros, temperature=zeros, velocity=noise)
+    table = (pack_sources(emitters), len(emitters))
+    dt, cycles = 0.02, []
+    for k in range(6):
+        solver.step(dt, sources=emitters)
+        ref.step(dt, sources=table)
+        assert solver.projector.last_cycles == ref.projector.last_cycles, k
+        cycles.append(ref.projector.last_cycles)
+        compare_step(solver, ref, k)
+        assert solver.measure_projection()['rel_div_inf'] <= 1e-4
+        dt = cfl_dt(max(solver.projector.velocity_maxima()), 1.0 / 64)
+    print(f'coarse sweeps {coarse_sweeps}: cycles {cycles}')
+    solver.close()

@@ -195,3 +195,11 @@ def test_warm_start_extrapolation_setting():
     for bad in (-0.1, 1.5, math.nan, math.inf, '1', True):
         with pytest.raises(ValueError):
             PressureSettings(warm_start_extrapolation=bad)
+
+
+def test_coarse_sweeps_setting():
+    assert PressureSettings().mg_coarse_sweeps == 0      # the reference: the same sweeps on every level
+    assert PressureSettings(mg_coarse_sweeps=2).mg_coarse_sweeps == 2
+    for bad in (-1, 17, 2.0, True):
+        with pytest.raises(ValueError):
+            PressureSettings(mg_coarse_sweeps=bad)
