@@ -519,12 +519,12 @@ def run_b200(args):
 
 
 # dram__bytes_read.sum + dram__bytes_write.sum of one advect_velocity_kernel
-# launch (reading the stored departure points and, in BF16 storage, the
-# predictor's unrounded samples), from an ncu capture of this bench's scene
-# (fast variant, BF16 storage; the kernel is the same for every solver variant).
-MEASURED_TRAFFIC = {(256, 2): 1331289600 + 96822784}
+# launch (reading the stored departure points, start velocities and, in BF16
+# storage, the predictor's unrounded samples), from an ncu capture of this
+# bench's scene (BF16 storage; the kernel is the same for every solver variant).
+MEASURED_TRAFFIC = {(256, 2): 1929255936 + 97080320}
 # smsp__inst_executed.sum (warp instructions) of the same launch, same capture
-MEASURED_WARP_INSTRUCTIONS = {(256, 2): 1.577e9}
+MEASURED_WARP_INSTRUCTIONS = {(256, 2): 1.486e9}
 B200_SMS, SCHEDULERS_PER_SM = 148, 4     # one warp instruction per scheduler per cycle
 
 
@@ -549,7 +549,7 @@ def roofline(passes, steps, cells, s, hbm, peak_kind, face_trace=True, sm_mhz=No
     step; its time comes from the events bracketing that launch in the timed
     steps): algorithmic bytes per launch (the scope table's 9s + 2s + m per
     cell) / launch time against the measured copy bandwidth. The kernel is
-    bound by instruction issue, not by HBM (about 1250 instructions per face in
+    bound by instruction issue, not by HBM (about 940 instructions per face in
     the reference's FP32 evaluation order: three trilinear velocity samples for
     the forward trace, the predictor sample, the 8-corner clamp, the collider
     tests, emitters, buoyancy and walls), hence the low fraction."""
