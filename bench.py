@@ -66,7 +66,7 @@ VARIANTS = {
     'learned': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True, mg_coarse_scale=1.9),
     'fast': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9),
     'extrapolated': dict(pressure_method='VCYCLE', solid_warm_start=True, mg_coarse_scale=1.9,
-                         warm_start_extrapolation=1.0),
+                         warm_start_extrapolation=1.0, warm_start_order=2),
     'learned_plain': dict(pressure_method='VCYCLE', solid_warm_start=False, learned_warm_start=True),
     'pcg': dict(pressure_method='PCG', solid_warm_start=True, mg_pre_sweeps=1, mg_post_sweeps=1),
     'learned_ir': dict(pressure_method='IR', solid_warm_start=False, learned_warm_start=True, mg_coarse_scale=1.9),
@@ -481,8 +481,8 @@ def run_b200(args):
                                    "the U-Net guess every step (learned_every_step) saves a fraction of a "
                                    "V-cycle against the previous pressure and costs more than it saves, so "
                                    "the faster form is the headline",
-                           'extrapolated': "variant extrapolated: the last two solves' pressures, extrapolated "
-                                           "linearly in time, start every solve; over-corrected V(4,4) cycles "
+                           'extrapolated': "variant extrapolated: the last three solves' pressures, extrapolated "
+                                           "in time by their quadratic, start every solve; over-corrected V(4,4) cycles "
                                            "(alpha 1.9); measured beside it, the previous pressure alone "
                                            "(previous_pressure_start) and the U-Net guess every step "
                                            "(learned_every_step), which saves a fraction of a V-cycle against the "

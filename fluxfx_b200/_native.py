@@ -217,6 +217,7 @@ _PROTOTYPES = {
                                   vp]),
     'ffx_scale_by_ratio': (C.c_int, [i64, vp, vp, vp]),
     'ffx_extrapolate_pressure': (C.c_int, [i64, vp, vp, vp, C.c_float, C.c_int32, vp]),
+    'ffx_extrapolate_pressure2': (C.c_int, [i64, vp, vp, vp, vp, vp, vp, C.c_float, C.c_int32, vp]),
     'ffx_advect_open': (C.c_int, [P(FfxGrid), C.c_int, vp, f32, f3, f32, f3, f32, f32, f32, vp, vp]),
     'ffx_mac_advect_density': (C.c_int, [P(FfxGrid), C.c_int, vp, vp, vp, vp, f32, f3, f32, f32, f32, vp, vp]),
     'ffx_walls': (C.c_int, [P(FfxGrid), P(FfxSolids), C.c_int, vp, vp, vp, vp, vp, vp, vp]),

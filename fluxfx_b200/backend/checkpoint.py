@@ -47,7 +47,8 @@ FORMAT_COLLIDERS = 'fluxfx-checkpoint-1+colliders'
 EXTENSION_SETTINGS = ('pressure_tolerance', 'pressure_max_cycles', 'mg_pre_sweeps', 'mg_post_sweeps',
                       'mg_max_levels', 'heat_mode', 'velocity_blend', 'storage', 'solid_warm_start',
                       'pressure_method', 'learned_warm_start', 'mg_coarse_scale', 'learned_correction',
-                      'ir_inner_cycles', 'warm_start_extrapolation', 'mg_coarse_sweeps')
+                      'ir_inner_cycles', 'warm_start_extrapolation', 'mg_coarse_sweeps',
+                      'warm_start_order')
 _TUPLES = ('velocity', 'source_center')
 
 

@@ -46,6 +46,11 @@ class PressureProjector:
         self._history = None
         self._history_valid = False
         self._host_clock = None
+        # quadratic form: two stored solves (newest first), their count, and the
+        # previous dt in two alternating device slots
+        self._histories = None
+        self._history_count = 0
+        self._dprev = None
         self.ready = False
         self.last_dt = None
         self.last_iterations = 0
@@ -85,6 +90,7 @@ class PressureProjector:
         self.last_dt = None
         self.last_iterations = 0
         self._history_valid = False
+        self._history_count = 0
         for t in (self.pressure, self.spare, self.before, self.after, *self.bounded):
             t.zero_()
 
@@ -128,6 +134,7 @@ class PressureProjector:
                              self.device.s)
         else:
             self._history_valid = False
+            self._history_count = 0
         self.solve_pressure(1.0, 1.0 if previous else None)
         self._gradient(outputs, 1.0)
         self.last_dt = clock        # the previous dt now lives on the device (clock[1] after the step)
@@ -176,6 +183,7 @@ class PressureProjector:
                              ptr(self.pressure), self.device.s)
         if previous_dt is None:
             self._history_valid = False
+            self._history_count = 0
         self.solve_pressure(solve_dt, previous_solve_dt)
         self._gradient(outputs, solve_dt)
         self.last_dt = dt
@@ -191,6 +199,20 @@ class PressureProjector:
         time (ffx_extrapolate_pressure; ``clock`` = device (dt, previous dt)).
         The first call after a cold solve has one pressure only and applies the
         ratio rule."""
+        if self.settings.warm_start_order == 2:
+            if self._histories is None:
+                self._histories = [self.device.texture(self.grid.shape) for _ in range(2)]
+                self._dprev = torch.zeros(2, dtype=torch.float32, device=self.device.device)
+            newest, oldest = self._histories
+            k = self._history_count
+            self.device.call('ffx_extrapolate_pressure2', self.pressure.numel(), ptr(self.pressure), ptr(newest),
+                             ptr(oldest), ptr(clock), ptr(self._dprev[(k + 1) % 2:(k + 1) % 2 + 1]),
+                             ptr(self._dprev[k % 2:k % 2 + 1]), float(self.extrapolation_beta()), min(k, 2),
+                             self.device.s)
+            # the pass wrote the last solve over the oldest: it is now the newest
+            self._histories = [oldest, newest]
+            self._history_count = k + 1
+            return
         if self._history is None:
             self._history = self.device.texture(self.grid.shape)
         self.device.call('ffx_extrapolate_pressure', self.pressure.numel(), ptr(self.pressure), ptr(self._history),

@@ -123,6 +123,46 @@ __global__ void extrapolate_kernel(int64_t n, float* p, float* hist, const float
     }
 }
 
+// Quadratic form of the same start, through the last three solves. P1 = p / d1
+// and the two stored quantities P2 = h_new (solve before) and P3 = h_old (the
+// one before that), taken at times 0, -d1 and -d1 - d2; the Lagrange quadratic
+// through them, evaluated at d0, gives Q, and the start is
+// d0 * (P1 + beta * (Q - P1)). `have` = stored solves (0: the ratio rule; 1:
+// the linear form with h_new; 2: the quadratic). Every form writes P1 over
+// h_old (which becomes the newest stored quantity; the caller swaps the roles)
+// and d1 into dprev_w; d2 is read from dprev_r (written by the previous call).
+// Coefficients in FP64, the update ((a0 v + a1 h_new) + a2 h_old) in FP32.
+__global__ void extrapolate2_kernel(int64_t n, float* p, const float* h_new, float* h_old, const float* clock,
+                                    const float* dprev_r, float* dprev_w, float beta, int have) {
+    const float dt = clock[0], prev = clock[1];
+    if (!(prev > 0.f)) return;
+    const double d0 = dt, d1 = prev, r = d0 / d1, b = beta;
+    float a0, a1 = 0.f, a2 = 0.f;
+    if (have == 0) {
+        a0 = fabs(r - 1.0) > 1e-6 ? (float)r : 1.f;
+    } else if (have == 1) {
+        a0 = (float)(d0 * (1.0 + b * r) / d1);
+        a1 = (float)(-d0 * b * r);
+    } else {
+        const double d2 = *dprev_r;
+        const double l0 = (d0 + d1) * (d0 + d1 + d2) / (d1 * (d1 + d2));
+        const double l1 = -d0 * (d0 + d1 + d2) / (d1 * d2);
+        const double l2 = d0 * (d0 + d1) / ((d1 + d2) * d2);
+        a0 = (float)(d0 * (1.0 + b * (l0 - 1.0)) / d1);
+        a1 = (float)(d0 * b * l1);
+        a2 = (float)(d0 * b * l2);
+    }
+    const float inv = (float)(1.0 / d1);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
+        const float v = p[i];
+        const float h1 = have >= 1 ? h_new[i] : 0.f;
+        const float h2 = have >= 2 ? h_old[i] : 0.f;
+        p[i] = have == 0 ? v * a0 : (have == 1 ? a0 * v + a1 * h1 : (a0 * v + a1 * h1) + a2 * h2);
+        h_old[i] = v * inv;
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) *dprev_w = prev;
+}
+
 }  // namespace
 }  // namespace ffx
 
@@ -190,6 +230,18 @@ int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream
     const int64_t want = (count + 255) / 256;
     scale_by_ratio_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(count, p, clock);
     return launch_status("scale_by_ratio_kernel");
+}
+
+int ffx_extrapolate_pressure2(int64_t count, float* p, const float* h_new, float* h_old, const float* clock,
+                              const float* dprev_r, float* dprev_w, float beta, int32_t have, void* stream) {
+    FFX_REQUIRE(count >= 1 && p && h_new && h_old && clock && dprev_r && dprev_w && p != h_new && p != h_old &&
+                    h_new != h_old && dprev_r != dprev_w && std::isfinite(beta) && beta >= 0.f && beta <= 1.f &&
+                    have >= 0 && have <= 2,
+                "ffx_extrapolate_pressure2: invalid arguments (beta in [0, 1], have 0..2, distinct buffers)");
+    const int64_t want = (count + 255) / 256;
+    extrapolate2_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(
+        count, p, h_new, h_old, clock, dprev_r, dprev_w, beta, have);
+    return launch_status("extrapolate2_kernel");
 }
 
 int ffx_extrapolate_pressure(int64_t count, float* p, float* hist, const float* clock, float beta, int32_t first,

@@ -38,6 +38,8 @@ Extensions (all default to the reference's behaviour):
   pressures extrapolated linearly in time, P1 + beta (dt / dt1) (P1 - P2) in
   pressure per unit time, instead of the previous pressure alone (0, the
   default). Same system, same tolerance; only the start differs.
+  ``warm_start_order`` 2 extrapolates with the quadratic through the last
+  three pressures instead (P1 + beta (Q - P1)).
 """
 from dataclasses import dataclass
 from math import fsum, isfinite, sqrt
@@ -123,6 +125,7 @@ class PressureSettings(ThermalSettings):
     ir_inner_cycles: int = 1
     warm_start_extrapolation: float = 0.0
     mg_coarse_sweeps: int = 0
+    warm_start_order: int = 1
 
     def __post_init__(self):
         super().__post_init__()
@@ -170,6 +173,8 @@ class PressureSettings(ThermalSettings):
         if (type(self.warm_start_extrapolation) not in (int, float) or not isfinite(self.warm_start_extrapolation)
                 or not 0 <= self.warm_start_extrapolation <= 1):
             raise ValueError("Warm-start extrapolation must lie in [0, 1]")
+        if type(self.warm_start_order) is not int or self.warm_start_order not in (1, 2):
+            raise ValueError("Warm-start extrapolation order must be 1 or 2")
 
 
 def divergence_stats(before, after):

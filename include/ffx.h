@@ -569,6 +569,16 @@ int ffx_scale_by_ratio(int64_t count, float* p, const float* clock, void* stream
  * 16-byte aligned, count floats each. */
 int ffx_extrapolate_pressure(int64_t count, float* p, float* hist, const float* clock, float beta,
                              int32_t first, void* stream);
+/* Quadratic form (an extension): P1 = p / clock[1], P2 = h_new and P3 = h_old (the
+ * two earlier solves, per unit time) at times 0, -clock[1] and -clock[1] - *dprev_r;
+ * Q = their Lagrange quadratic at clock[0]; p = clock[0] * (P1 + beta * (Q - P1)).
+ * have = earlier solves stored: 0 applies ffx_scale_by_ratio's rule, 1 the linear
+ * form of ffx_extrapolate_pressure with h_new, 2 the quadratic. Every call writes
+ * P1 over h_old and clock[1] to *dprev_w; the caller then swaps h_new / h_old and
+ * dprev_r / dprev_w. Nothing changes when clock[1] <= 0. */
+int ffx_extrapolate_pressure2(int64_t count, float* p, const float* h_new, float* h_old,
+                              const float* clock, const float* dprev_r, float* dprev_w, float beta,
+                              int32_t have, void* stream);
 
 /* ------------------------------------------------------- sparse brick path */
 /* Brick pool: the topology of FluxFX_Source/native/bricks.hpp:14-94 (fixed

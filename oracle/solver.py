@@ -161,7 +161,12 @@ class OracleProjector:
         beta = getattr(self.s, 'warm_start_extrapolation', 0.0)
         extrapolates = (beta > 0 and self.kind == 'SOLID_MULTIGRID' and len(self.levels) > 1
                         and self.s.solid_warm_start and not getattr(self.s, 'learned_warm_start', False))
-        if impulse and previous_dt is not None and extrapolates:
+        if impulse and previous_dt is not None and extrapolates and getattr(self.s, 'warm_start_order', 1) == 2:
+            hist = self.history or []
+            self.pressure, newest = extrapolate2(self.pressure, hist, dt, previous_dt, beta)
+            # (P1, its dt) first, then the solve before it
+            self.history = [(newest, float(np.float32(previous_dt)))] + hist[:1]
+        elif impulse and previous_dt is not None and extrapolates:
             self.pressure, self.history = extrapolate(self.pressure, self.history, dt, previous_dt, beta)
         elif impulse and previous_dt is not None and abs(dt / previous_dt - 1.0) > 1e-6:
             self.pressure = self.pressure * g.f(dt / previous_dt)
@@ -192,6 +197,34 @@ def extrapolate(p, history, dt, previous_dt, beta):
     c1 = np.float32(d0 * (1.0 + beta * r) / d1)
     c2 = np.float32(d0 * beta * r)
     return c1 * p - c2 * np.asarray(history, np.float32), new_history
+
+
+def extrapolate2(p, history, dt, previous_dt, beta):
+    """The quadratic form of the extrapolated start (``warm_start_order`` 2):
+    ``history`` holds up to two earlier solves as (pressure per unit time, the
+    dt of that solve), newest first. With P1 = p / previous dt at time 0 and
+    the stored ones at -d1 and -d1 - d2, the start is d0 (P1 + beta (Q - P1))
+    with Q their Lagrange quadratic at d0 (the linear form with one stored
+    solve, the dt rescale with none). FP32 time steps, FP64 coefficients,
+    FP32 update ((a0 v + a1 h1) + a2 h2), as the device pass does; returns
+    (start, P1)."""
+    d0, d1 = float(np.float32(dt)), float(np.float32(previous_dt))
+    r, b = d0 / d1, beta
+    v = np.asarray(p, np.float32)
+    newest = v * np.float32(1.0 / d1)
+    if not history:
+        c = np.float32(r) if abs(r - 1.0) > 1e-6 else np.float32(1.0)
+        return v * c, newest
+    if len(history) == 1:
+        a0, a1 = np.float32(d0 * (1.0 + b * r) / d1), np.float32(-d0 * b * r)
+        return a0 * v + a1 * history[0][0], newest
+    d2 = history[0][1]
+    l0 = (d0 + d1) * (d0 + d1 + d2) / (d1 * (d1 + d2))
+    l1 = -d0 * (d0 + d1 + d2) / (d1 * d2)
+    l2 = d0 * (d0 + d1) / ((d1 + d2) * d2)
+    a0 = np.float32(d0 * (1.0 + b * (l0 - 1.0)) / d1)
+    a1, a2 = np.float32(d0 * b * l1), np.float32(d0 * b * l2)
+    return (a0 * v + a1 * history[0][0]) + a2 * history[1][0], newest
 
 
 def projector_kind(grid_shape, settings, has_mask):

@@ -122,21 +122,44 @@ def test_extrapolated_warm_start_meets_tolerance_with_fewer_cycles(D, device_ste
         solver.close()
 
 
-@pytest.mark.parametrize('coarse_sweeps', [0, 2])
-def test_extended_solver_matches_oracle_on_collider_scene(D, coarse_sweeps):
+@pytest.mark.parametrize('have', [0, 1, 2])
+@pytest.mark.parametrize('clock', [(0.0019, 0.0021), (0.02, 0.02)])
+def test_quadratic_extrapolate_kernel_matches_its_formula(D, have, clock):
+    from oracle.solver import extrapolate2
+    lib = N.load()
+    rng = np.random.default_rng(7 + have)
+    count, d2 = 3001, 0.0023
+    p0 = rng.normal(size=count).astype(np.float32) * 3e-3
+    h = [rng.normal(size=count).astype(np.float32) for _ in range(2)]
+    p, newest, oldest = (torch.as_tensor(a).cuda() for a in (p0, h[0], h[1]))
+    ck = torch.tensor(clock, dtype=torch.float32, device='cuda')
+    slots = torch.tensor([d2, -1.0], dtype=torch.float32, device='cuda')
+    N.check(lib.ffx_extrapolate_pressure2(count, _ptr(p), _ptr(newest), _ptr(oldest), _ptr(ck), _ptr(slots[0:1]),
+                                          _ptr(slots[1:2]), 0.75, have, None))
+    torch.cuda.synchronize()
+    history = [(h[0], float(np.float32(d2))), (h[1], 0.0)][:have]
+    want_p, want_h = extrapolate2(p0, history, clock[0], clock[1], 0.75)
+    assert np.array_equal(p.cpu().numpy(), want_p)
+    assert np.array_equal(oldest.cpu().numpy(), want_h)          # the last solve, written over the oldest
+    assert np.array_equal(newest.cpu().numpy(), h[0])
+    assert slots.cpu().tolist() == [pytest.approx(d2), float(np.float32(clock[1]))]
+
+
+@pytest.mark.parametrize('coarse_sweeps, order', [(0, 1), (2, 1), (0, 2)])
+def test_extended_solver_matches_oracle_on_collider_scene(D, coarse_sweeps, order):
     """The collider scene at 64^3 with the extrapolated start (beta = 1) and,
     optionally, two pre- and post-sweeps on the levels below level 0, against
     the CPU oracle with the same settings: per step and field within 1e-5 of
     the field's maximum, the same V-cycle counts. Host steps (dt from the
     device's face maxima on both sides), six steps: the extrapolation starts
-    at the third."""
+    at the third (the quadratic at the fourth)."""
     import bench
     from fluxfx_b200.backend.projected import DenseProjectedSmoke
     from fluxfx_b200.physics.emission import pack_sources
     from oracle import solver as O
     from tests.test_gpu_configs import cfl_dt, compare_step
-    grid, s, colliders, emitters, noise = bench.scene(64, 'FP32', 0, **bench.VARIANTS['extrapolated'],
-                                                      mg_coarse_sweeps=coarse_sweeps)
+    settings = dict(bench.VARIANTS['extrapolated'], mg_coarse_sweeps=coarse_sweeps, warm_start_order=order)
+    grid, s, colliders, emitters, noise = bench.scene(64, 'FP32', 0, **settings)
     solver = DenseProjectedSmoke(grid, s, D, colliders=colliders)
     if coarse_sweeps:
         assert solver.projector.coarse_pre == solver.projector.coarse_post == coarse_sweeps
@@ -157,5 +180,5 @@ def test_extended_solver_matches_oracle_on_collider_scene(D, coarse_sweeps):
         compare_step(solver, ref, k)
         assert solver.measure_projection()['rel_div_inf'] <= 1e-4
         dt = cfl_dt(max(solver.projector.velocity_maxima()), 1.0 / 64)
-    print(f'coarse sweeps {coarse_sweeps}: cycles {cycles}')
+    print(f'coarse sweeps {coarse_sweeps}, order {order}: cycles {cycles}')
     solver.close()

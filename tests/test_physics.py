@@ -203,3 +203,11 @@ def test_coarse_sweeps_setting():
     for bad in (-1, 17, 2.0, True):
         with pytest.raises(ValueError):
             PressureSettings(mg_coarse_sweeps=bad)
+
+
+def test_warm_start_order_setting():
+    assert PressureSettings().warm_start_order == 1
+    assert PressureSettings(warm_start_order=2).warm_start_order == 2
+    for bad in (0, 3, 2.0, True):
+        with pytest.raises(ValueError):
+            PressureSettings(warm_start_order=bad)
