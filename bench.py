@@ -725,7 +725,7 @@ def run_batched(args):
 SHAPES_NAMES = ((32, 8), (64, 4), (128, 2), (16, 16))
 
 
-def fire_scene(storage, seed, fast):
+def fire_scene(storage, seed, fast, **overrides):
     """The fire configuration: 192 x 192 x 320 cells (cells of 1/192, z up), a
     fuel emitter of radius 10 cells (fuel 1.0, temperature 0.4), combustion
     (burn rate 0.75, ignition 0.3, heat yield 1.0, smoke yield 0.5), vorticity
@@ -751,6 +751,7 @@ def fire_scene(storage, seed, fast):
                pressure_max_cycles=200, storage=storage if fast else 'FP32')
     if fast:
         cfg.update(solid_warm_start=True, mg_coarse_scale=1.9, learned_warm_start=True)
+        cfg.update(overrides)
     noise = [rng.uniform(-1e-3, 1e-3, (fs[2], fs[1], fs[0])).astype(np.float32) for fs in grid.face_shapes]
     return grid, PressureSettings(**cfg), pose, noise
 
@@ -773,7 +774,8 @@ def run_fire(args):
     def build(fast):
         out = []
         for d in range(domains):
-            grid, settings, pose, noise = fire_scene(args.storage, args.seed + d, fast)
+            grid, settings, pose, noise = fire_scene(args.storage, args.seed + d, fast,
+                                                     **(parse_settings(args.set) if fast else {}))
             s = DenseProjectedSmoke(grid, settings, devices[d], projector_class=SolidMultigridProjector,
                                     colliders=pose(0))
             if fast:

@@ -711,7 +711,10 @@ class SolidMultigridProjector(SolidPressureProjector):
 
     def extrapolation_beta(self):
         s = self.settings
-        if s.warm_start_extrapolation > 0 and s.solid_warm_start and not s.learned_warm_start and len(self.levels) > 1:
+        # warm solves start from the extrapolation; a learned guess of cold solves is
+        # compatible, a learned correction of warm ones is not
+        learned_correction = s.learned_warm_start and s.learned_correction
+        if s.warm_start_extrapolation > 0 and s.solid_warm_start and not learned_correction and len(self.levels) > 1:
             return s.warm_start_extrapolation
         return 0.0
 

@@ -153,12 +153,33 @@ __global__ void extrapolate2_kernel(int64_t n, float* p, const float* h_new, flo
         a2 = (float)(d0 * b * l2);
     }
     const float inv = (float)(1.0 / d1);
-    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
-        const float v = p[i];
-        const float h1 = have >= 1 ? h_new[i] : 0.f;
-        const float h2 = have >= 2 ? h_old[i] : 0.f;
-        p[i] = have == 0 ? v * a0 : (have == 1 ? a0 * v + a1 * h1 : (a0 * v + a1 * h1) + a2 * h2);
-        h_old[i] = v * inv;
+    auto cell = [&](float& v, float h1, float& h2) {
+        const float x = v;
+        v = have == 0 ? x * a0 : (have == 1 ? a0 * x + a1 * h1 : (a0 * x + a1 * h1) + a2 * h2);
+        h2 = x * inv;
+    };
+    const int64_t stride = (int64_t)gridDim.x * blockDim.x;
+    const int64_t quads = n / 4;
+    float4* p4 = reinterpret_cast<float4*>(p);
+    const float4* n4 = reinterpret_cast<const float4*>(h_new);
+    float4* o4 = reinterpret_cast<float4*>(h_old);
+    const float4 zero = make_float4(0.f, 0.f, 0.f, 0.f);
+    for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < quads; i += stride) {
+        float4 v = p4[i];
+        const float4 a = have >= 1 ? n4[i] : zero;
+        float4 b = have >= 2 ? o4[i] : zero;
+        cell(v.x, a.x, b.x);
+        cell(v.y, a.y, b.y);
+        cell(v.z, a.z, b.z);
+        cell(v.w, a.w, b.w);
+        p4[i] = v;
+        o4[i] = b;
+    }
+    for (int64_t i = 4 * quads + (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        float v = p[i], b = have >= 2 ? h_old[i] : 0.f;
+        cell(v, have >= 1 ? h_new[i] : 0.f, b);
+        p[i] = v;
+        h_old[i] = b;
     }
     if (blockIdx.x == 0 && threadIdx.x == 0) *dprev_w = prev;
 }
@@ -238,8 +259,12 @@ int ffx_extrapolate_pressure2(int64_t count, float* p, const float* h_new, float
                     h_new != h_old && dprev_r != dprev_w && std::isfinite(beta) && beta >= 0.f && beta <= 1.f &&
                     have >= 0 && have <= 2,
                 "ffx_extrapolate_pressure2: invalid arguments (beta in [0, 1], have 0..2, distinct buffers)");
-    const int64_t want = (count + 255) / 256;
-    extrapolate2_kernel<<<(unsigned)(want < 148 * 8 ? want : 148 * 8), 256, 0, as_stream(stream)>>>(
+    FFX_REQUIRE(reinterpret_cast<uintptr_t>(p) % 16 == 0 && reinterpret_cast<uintptr_t>(h_new) % 16 == 0 &&
+                    reinterpret_cast<uintptr_t>(h_old) % 16 == 0,
+                "ffx_extrapolate_pressure2: p, h_new and h_old must be 16-byte aligned");
+    const int64_t want = (count / 4 + 255) / 256;
+    const int64_t blocks = want < 1 ? 1 : (want < 148 * 8 ? want : 148 * 8);
+    extrapolate2_kernel<<<(unsigned)blocks, 256, 0, as_stream(stream)>>>(
         count, p, h_new, h_old, clock, dprev_r, dprev_w, beta, have);
     return launch_status("extrapolate2_kernel");
 }

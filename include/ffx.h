@@ -575,7 +575,8 @@ int ffx_extrapolate_pressure(int64_t count, float* p, float* hist, const float* 
  * have = earlier solves stored: 0 applies ffx_scale_by_ratio's rule, 1 the linear
  * form of ffx_extrapolate_pressure with h_new, 2 the quadratic. Every call writes
  * P1 over h_old and clock[1] to *dprev_w; the caller then swaps h_new / h_old and
- * dprev_r / dprev_w. Nothing changes when clock[1] <= 0. */
+ * dprev_r / dprev_w. Nothing changes when clock[1] <= 0. p, h_new and h_old are
+ * distinct, 16-byte aligned, count floats each. */
 int ffx_extrapolate_pressure2(int64_t count, float* p, const float* h_new, float* h_old,
                               const float* clock, const float* dprev_r, float* dprev_w, float beta,
                               int32_t have, void* stream);

@@ -160,7 +160,8 @@ class OracleProjector:
         previous_solve = (1.0 if previous_dt is not None else None) if impulse else previous_dt
         beta = getattr(self.s, 'warm_start_extrapolation', 0.0)
         extrapolates = (beta > 0 and self.kind == 'SOLID_MULTIGRID' and len(self.levels) > 1
-                        and self.s.solid_warm_start and not getattr(self.s, 'learned_warm_start', False))
+                        and self.s.solid_warm_start
+                        and not (getattr(self.s, 'learned_warm_start', False) and getattr(self.s, 'learned_correction', False)))
         if impulse and previous_dt is not None and extrapolates and getattr(self.s, 'warm_start_order', 1) == 2:
             hist = self.history or []
             self.pressure, newest = extrapolate2(self.pressure, hist, dt, previous_dt, beta)

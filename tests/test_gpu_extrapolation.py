@@ -122,13 +122,14 @@ def test_extrapolated_warm_start_meets_tolerance_with_fewer_cycles(D, device_ste
         solver.close()
 
 
+@pytest.mark.parametrize('count', [3001, 4096])
 @pytest.mark.parametrize('have', [0, 1, 2])
 @pytest.mark.parametrize('clock', [(0.0019, 0.0021), (0.02, 0.02)])
-def test_quadratic_extrapolate_kernel_matches_its_formula(D, have, clock):
+def test_quadratic_extrapolate_kernel_matches_its_formula(D, have, clock, count):
     from oracle.solver import extrapolate2
     lib = N.load()
     rng = np.random.default_rng(7 + have)
-    count, d2 = 3001, 0.0023
+    d2 = 0.0023
     p0 = rng.normal(size=count).astype(np.float32) * 3e-3
     h = [rng.normal(size=count).astype(np.float32) for _ in range(2)]
     p, newest, oldest = (torch.as_tensor(a).cuda() for a in (p0, h[0], h[1]))
