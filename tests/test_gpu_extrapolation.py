@@ -1,11 +1,15 @@
-"""Warm start extrapolated in time (warm_start_extrapolation, an extension).
+"""Warm start extrapolated in time (warm_start_extrapolation and
+warm_start_order, extensions of the solver).
 
-The kernel (ffx_extrapolate_pressure) against its formula, bit for bit (the
-library is built without FMA contraction, so c1*v - c2*h rounds like NumPy's
-FP32 products and difference); the solver with the extrapolated start against
-the same solver started from the previous pressure: every step meets the
-tolerance, the extrapolated start needs no more V-cycles, and the two runs
-stay within what the solve tolerance allows of each other."""
+The linear and quadratic passes (ffx_extrapolate_pressure, _pressure2) against
+their formulas, bit for bit (the library is built without FMA contraction, so
+the products and sums round like NumPy's FP32 ones); the solver with the
+extrapolated start against the same solver started from the previous
+pressure: every step meets the tolerance, the extrapolated start needs fewer
+V-cycles, and the two runs stay within what the solve tolerance allows of
+each other; and the extended solver (linear or quadratic start, optionally
+fewer coarse-level sweeps) against the CPU oracle restating the same
+extensions, step by step on the 64^3 collider scene."""
 import ctypes as C
 
 import numpy as np
